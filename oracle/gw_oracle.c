@@ -1,0 +1,391 @@
+/*
+ * gw_oracle.c -- CPU oracle for the GOWalker second-order walk step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product links or calls this file:
+ * only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg and
+ * `--impl reference` arm load it, and only as the checker or the timed CPU
+ * baseline.
+ *
+ * What it restates (reference file:line, paths inside the GOWalker project):
+ *   - Node2vec CPU step   engine/engine.hpp:158-287  (sidewalkupdate)
+ *   - SOPR/SOSR CPU step  engine/engine.hpp:289-404  (SOPR_sidewalkupdate)
+ *   - binary search of the candidate in N(prev)  engine/engine.hpp:225-243
+ *   - dead-end rule (deg == 0 -> hop = maxhop-1, next vertex 0)
+ *                                              engine/engine.hpp:196-199
+ *   - walker init, Node2vec: id = v*wps + i     engine/walk.hpp:32-49, 294-321
+ *   - walker init, SOPR (all at vertex 1) / SOSR (half at 1, half at 3)
+ *                                              engine/walk.hpp:275-293, 355-384
+ *
+ * The reference draws from RandNum::inlineRandPair (util/util.hpp:291-301),
+ * a stateful xoroshiro128+ seeded from time(NULL).  Here every draw comes from
+ * Philox4x32-10 (Salmon et al., SC'11) keyed by the walk seed and countered by
+ * (walker id, hop, attempt, 0):
+ *   lane0 -> rand_pos = lane0 % deg                     (util/util.hpp:294)
+ *   lane1 -> rand_val = float(lane1 >> 8) * 2^-24 * max_val   (one fp32 multiply)
+ *   lane2 -> SOPR/SOSR geometric termination draw at hop >= 1 (not in the
+ *            reference, whose walks have fixed length)
+ * A second keying, (walker id, running trial index), matches the shim used
+ * by oracle/ref_step_harness.cu, which drives the reference's own
+ * sidewalkupdate for the differential test.
+ *
+ * The floating-point mix of the reference is kept exactly:
+ *   Node2vec: inv_p = 1.0f/p, inv_q = 1.0f/q, all compares in fp32
+ *             (engine.hpp:169-172, 209, 216, 247, 254).
+ *   SOPR:     inv_deg = (float)((1.0 - alpha)/deg) in fp64, inv_prev_deg =
+ *             alpha / (float)prev_deg in fp32 (engine.hpp:323-326); the x==prev
+ *             compare is fp64 against (1.0-alpha)/deg (engine.hpp:341), the
+ *             others fp32 (engine.hpp:334, 368, 373).
+ * Build with -ffp-contract=off so no multiply-add is fused.
+ *
+ * Besides paths, the oracle counts the memory the step needs, in 32-byte
+ * sectors: the (beg[cur], beg[cur+1]) pair, one csr sector per trial, and the
+ * distinct sectors touched by the binary search of each trial.  These give the
+ * algorithmic bytes per step used for the roofline.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <omp.h>
+
+#define PHILOX_M0 0xD2511F53u
+#define PHILOX_M1 0xCD9E8D57u
+#define PHILOX_W0 0x9E3779B9u
+#define PHILOX_W1 0xBB67AE85u
+
+#define FNV_OFFSET 0xcbf29ce484222325ull
+#define FNV_PRIME 0x100000001b3ull
+
+#define RMAT_TAG 0x524D4154u /* 'RMAT' */
+#define INIT_TAG 0x494E4954u /* 'INIT' */
+
+enum { ALG_NODE2VEC = 0, ALG_SOPR = 1, ALG_SOSR = 2 };
+enum { INIT_PER_VERTEX = 0, INIT_SINGLE_SOURCE = 1, INIT_RANDOM = 2 };
+enum { KEY_HOP_ATTEMPT = 0, KEY_TRIAL = 1 };
+
+/* Philox4x32-10: ten rounds of the published S-box-free bijection, key bumped
+ * by the Weyl constants between rounds. */
+void oracle_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)PHILOX_M0 * c0;
+        uint64_t p1 = (uint64_t)PHILOX_M1 * c2;
+        uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+        uint32_t n1 = (uint32_t)p1;
+        uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+        uint32_t n3 = (uint32_t)p0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += PHILOX_W0;
+        k1 += PHILOX_W1;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+static inline void draw4(uint64_t seed, uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t out[4])
+{
+    uint32_t ctr[4] = {a, b, c, d};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    oracle_philox4x32_10(ctr, key, out);
+}
+
+/* ---------------------------------------------------------------- R-MAT */
+
+/* R-MAT edge sample e at `scale` levels.  Level l uses lane (l & 3) of the
+ * Philox call (e_lo, e_hi, l >> 2, 'RMAT').  thr[] are the cumulative quadrant
+ * thresholds a, a+b, a+b+c scaled to 2^32 (integers, so CPU and GPU agree). */
+static inline void rmat_one(uint32_t scale, uint64_t e, const uint32_t thr[3], uint64_t seed,
+                            uint32_t *src, uint32_t *dst)
+{
+    uint32_t s = 0, d = 0, r[4];
+    for (uint32_t l = 0; l < scale; ++l) {
+        if ((l & 3u) == 0)
+            draw4(seed, (uint32_t)e, (uint32_t)(e >> 32), l >> 2, RMAT_TAG, r);
+        uint32_t u = r[l & 3u];
+        uint32_t sb, db;
+        if (u < thr[0]) { sb = 0; db = 0; }
+        else if (u < thr[1]) { sb = 0; db = 1; }
+        else if (u < thr[2]) { sb = 1; db = 0; }
+        else { sb = 1; db = 1; }
+        s = (s << 1) | sb;
+        d = (d << 1) | db;
+    }
+    *src = s;
+    *dst = d;
+}
+
+/* Raw samples e in [first, first+count). */
+void oracle_rmat_edges(uint32_t scale, uint64_t first, uint64_t count, const uint32_t thr[3],
+                       uint64_t seed, uint32_t *src, uint32_t *dst, int nthreads)
+{
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)count; ++i)
+        rmat_one(scale, first + (uint64_t)i, thr, seed, &src[i], &dst[i]);
+}
+
+/* ---------------------------------------------------------------- walks */
+
+typedef struct {
+    uint32_t algo;       /* ALG_* (AlgorithmType order, api/types.hpp:27) */
+    uint32_t maxhops;    /* walk length (the "length" option) */
+    float p, q, alpha;   /* Node2vec p, q; SOPR/SOSR alpha */
+    float term_prob;     /* geometric termination per step at hop >= 1; 0 = off */
+    uint64_t seed;       /* walk seed (Philox key) */
+    uint32_t keying;     /* KEY_* */
+    uint32_t init_mode;  /* INIT_* */
+    uint32_t wps;        /* walkers per source vertex (INIT_PER_VERTEX) */
+    uint32_t numwalks;   /* total walkers (INIT_SINGLE_SOURCE / INIT_RANDOM) */
+} oracle_cfg;
+
+typedef struct {
+    uint64_t steps;          /* real moves (path entries after the source) */
+    uint64_t trials;         /* rejection-sampling attempts */
+    uint64_t probes;         /* binary-search reads of N(prev) */
+    uint64_t search_sectors; /* distinct 32-B sectors per trial's search, summed */
+    uint64_t off_sectors;    /* sectors of (beg[cur], beg[cur+1]) per step */
+    uint64_t dead_ends;      /* walks stopped by the deg==0 rule */
+    uint64_t terminated;     /* walks stopped by the termination draw */
+} oracle_stats;
+
+/* Source vertex of walker `wid` (engine/walk.hpp init kernels). */
+uint32_t oracle_walker_source(const oracle_cfg *c, uint32_t nverts, uint32_t wid)
+{
+    switch (c->init_mode) {
+    case INIT_PER_VERTEX:
+        return wid / c->wps;
+    case INIT_SINGLE_SOURCE:
+        if (c->algo == ALG_SOSR)
+            return wid < c->numwalks / 2 ? 1u : 3u;
+        return 1u;
+    default: {
+        uint32_t r[4];
+        draw4(c->seed, wid, 0xFFFFFFFFu, 0, INIT_TAG, r);
+        return r[0] % nverts;
+    }
+    }
+}
+
+typedef struct {
+    uint32_t deg;
+    uint32_t maxv_bits;
+    uint32_t pos;
+    uint32_t rv_bits;
+} oracle_trial;
+
+static inline uint32_t f2u(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+
+/* Membership of x in the sorted run csr[lo, hi), by the reference's binary
+ * search (engine/engine.hpp:225-243), counting reads and distinct sectors. */
+static inline int search_sorted(const uint32_t *csr, uint64_t lo, uint64_t hi, uint32_t x,
+                                uint64_t *probes, uint64_t *sectors)
+{
+    int64_t left = (int64_t)lo, right = (int64_t)hi - 1;
+    uint64_t seen[72];
+    int nseen = 0;
+    while (left <= right) {
+        int64_t mid = left + ((right - left) >> 1);
+        uint64_t sec = ((uint64_t)mid * 4u) >> 5;
+        int dup = 0;
+        for (int i = 0; i < nseen; ++i)
+            if (seen[i] == sec) { dup = 1; break; }
+        if (!dup && nseen < 72) seen[nseen++] = sec;
+        (*probes)++;
+        uint32_t v = csr[mid];
+        if (v == x) { *sectors += (uint64_t)nseen; return 1; }
+        if (v < x) left = mid + 1;
+        else right = mid - 1;
+    }
+    *sectors += (uint64_t)nseen;
+    return 0;
+}
+
+/* One walk from an explicit state.  Returns the number of real moves.
+ * path (may be NULL) receives the vertices visited after `cur`.
+ * trace (may be NULL, capacity trace_cap) receives every trial. */
+static uint32_t walk_from(const uint64_t *beg, const uint32_t *csr, const oracle_cfg *c,
+                          uint32_t wid, uint32_t *pprev, uint32_t *pcur, uint32_t *phop,
+                          uint64_t *phash, uint32_t *path, oracle_stats *st,
+                          oracle_trial *trace, uint64_t trace_cap, uint64_t *ntrace,
+                          uint64_t *trial_counter)
+{
+    uint32_t prev = *pprev, cur = *pcur, hop = *phop;
+    uint64_t h = *phash;
+    uint32_t moves = 0;
+    const uint32_t maxhops = c->maxhops;
+
+    /* Node2vec constants, engine/engine.hpp:169-172 */
+    const float inv_p = 1.0f / c->p;
+    const float inv_q = 1.0f / c->q;
+    const float t_iq1 = (inv_q < 1.0f) ? 1.0f : inv_q; /* std::max(inv_q, 1.0f) */
+    const float n2v_max = (inv_p < t_iq1) ? t_iq1 : inv_p;
+    const float t_iq2 = (1.0f < inv_q) ? 1.0f : inv_q; /* std::min(inv_q, 1.0f) */
+    const float n2v_min = (t_iq2 < inv_p) ? t_iq2 : inv_p;
+
+    while (hop < maxhops) {
+        uint32_t r[4];
+        if (c->term_prob > 0.0f && hop > 0 && c->keying == KEY_HOP_ATTEMPT) {
+            draw4(c->seed, wid, hop, 0, 0, r);
+            float u = (float)(r[2] >> 8) * 0x1p-24f;
+            if (u < c->term_prob) { st->terminated++; break; }
+        }
+        uint64_t head = beg[cur], tail = beg[cur + 1];
+        st->off_sectors += (((uint64_t)cur * 8u) >> 5) != (((uint64_t)cur * 8u + 15u) >> 5) ? 2 : 1;
+        uint64_t deg = tail - head;
+        if (deg == 0) {
+            /* engine/engine.hpp:196-199: hop = maxhop-1, next vertex 0, then hop++ */
+            prev = cur;
+            cur = 0;
+            hop = maxhops;
+            st->dead_ends++;
+            break;
+        }
+        uint64_t phead = beg[prev], ptail = beg[prev + 1];
+        uint64_t pdeg = ptail - phead;
+
+        float maxv, minv, t_prev_f = 0.f, t_found, t_notfound;
+        double t_prev_d = 0.0;
+        if (c->algo == ALG_NODE2VEC) {
+            maxv = n2v_max;
+            minv = n2v_min;
+            t_prev_f = inv_p;
+            t_found = 1.0f;
+            t_notfound = inv_q;
+        } else {
+            /* engine/engine.hpp:323-326, 341, 368, 373 */
+            t_prev_d = (1.0 - (double)c->alpha) / (double)deg;
+            float inv_deg = (float)t_prev_d;
+            float inv_prev_deg = c->alpha / (float)pdeg;
+            float sum = inv_deg + inv_prev_deg;
+            maxv = (inv_deg < sum) ? sum : inv_deg;
+            minv = (sum < inv_deg) ? sum : inv_deg;
+            t_found = sum;
+            t_notfound = inv_deg;
+        }
+
+        uint32_t attempt = 0, x;
+        for (;;) {
+            if (c->keying == KEY_HOP_ATTEMPT)
+                draw4(c->seed, wid, hop, attempt, 0, r);
+            else
+                draw4(c->seed, wid, (uint32_t)*trial_counter, (uint32_t)(*trial_counter >> 32), 0, r);
+            attempt++;
+            (*trial_counter)++;
+            st->trials++;
+            uint32_t pos = (uint32_t)((uint64_t)r[0] % deg);
+            float rv = ((float)(r[1] >> 8) * 0x1p-24f) * maxv;
+            if (trace && *ntrace < trace_cap) {
+                oracle_trial *t = &trace[*ntrace];
+                t->deg = (uint32_t)deg;
+                t->maxv_bits = f2u(maxv);
+                t->pos = pos;
+                t->rv_bits = f2u(rv);
+            }
+            if (ntrace) (*ntrace)++;
+            x = csr[head + pos];
+            if (rv <= minv) break;
+            if (x == prev) {
+                int acc = (c->algo == ALG_NODE2VEC) ? (rv < t_prev_f) : ((double)rv < t_prev_d);
+                if (acc) break;
+                continue;
+            }
+            int found;
+            if (prev == cur)
+                found = 1; /* x is drawn from N(cur) = N(prev): the search must succeed */
+            else
+                found = search_sorted(csr, phead, ptail, x, &st->probes, &st->search_sectors);
+            if (found ? (rv < t_found) : (rv < t_notfound)) break;
+        }
+        (void)pdeg;
+        prev = cur;
+        cur = x;
+        hop++;
+        h = (h ^ (uint64_t)x) * FNV_PRIME;
+        if (path) path[moves] = x;
+        moves++;
+        st->steps++;
+    }
+    *pprev = prev;
+    *pcur = cur;
+    *phop = hop;
+    *phash = h;
+    return moves;
+}
+
+uint64_t oracle_hash_init(uint32_t source)
+{
+    return (FNV_OFFSET ^ (uint64_t)source) * FNV_PRIME;
+}
+
+/* Walk walkers [wid_begin, wid_begin + count) from their initial state.
+ *   paths:  count x (maxhops+1) u32 or NULL (source first)
+ *   lens:   count u32 (vertices recorded) or NULL
+ *   hashes: count u64 (FNV-1a over the path's 32-bit vertices) or NULL
+ *   finals: count x 3 u32 (prev, cur, hop) after the walk, or NULL */
+int oracle_walk(const uint64_t *beg, const uint32_t *csr, uint32_t nverts, const oracle_cfg *c,
+                uint32_t wid_begin, uint32_t count, uint32_t *paths, uint32_t *lens,
+                uint64_t *hashes, uint32_t *finals, oracle_stats *stats, int nthreads)
+{
+    if (c->algo > ALG_SOSR || c->maxhops == 0) return -1;
+    if (c->init_mode == INIT_PER_VERTEX && c->wps == 0) return -1;
+    memset(stats, 0, sizeof(*stats));
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    const uint64_t stride = (uint64_t)c->maxhops + 1;
+#pragma omp parallel
+    {
+        oracle_stats st;
+        memset(&st, 0, sizeof(st));
+#pragma omp for schedule(dynamic, 1024)
+        for (int64_t i = 0; i < (int64_t)count; ++i) {
+            uint32_t wid = wid_begin + (uint32_t)i;
+            uint32_t src = oracle_walker_source(c, nverts, wid);
+            uint32_t prev = src, cur = src, hop = 0;
+            uint64_t h = oracle_hash_init(src);
+            uint64_t tc = 0;
+            uint32_t *path = paths ? paths + (uint64_t)i * stride : NULL;
+            if (path) path[0] = src;
+            uint32_t moves = walk_from(beg, csr, c, wid, &prev, &cur, &hop, &h, path ? path + 1 : NULL,
+                                       &st, NULL, 0, NULL, &tc);
+            if (lens) lens[i] = moves + 1;
+            if (hashes) hashes[i] = h;
+            if (finals) {
+                finals[3 * i + 0] = prev;
+                finals[3 * i + 1] = cur;
+                finals[3 * i + 2] = hop;
+            }
+        }
+#pragma omp critical
+        {
+            stats->steps += st.steps;
+            stats->trials += st.trials;
+            stats->probes += st.probes;
+            stats->search_sectors += st.search_sectors;
+            stats->off_sectors += st.off_sectors;
+            stats->dead_ends += st.dead_ends;
+            stats->terminated += st.terminated;
+        }
+    }
+    return 0;
+}
+
+/* Single walker from an explicit state (prev, cur, hop) with a trial trace,
+ * for the differential test against the reference's sidewalkupdate.
+ * Returns the number of moves; *ntrace receives the number of trials. */
+uint32_t oracle_walk_traced(const uint64_t *beg, const uint32_t *csr, const oracle_cfg *c,
+                            uint32_t wid, uint32_t prev, uint32_t cur, uint32_t hop,
+                            uint32_t *path, oracle_trial *trace, uint64_t trace_cap,
+                            uint64_t *ntrace, uint32_t *final3)
+{
+    oracle_stats st;
+    memset(&st, 0, sizeof(st));
+    uint64_t h = 0, tc = 0;
+    *ntrace = 0;
+    uint32_t moves = walk_from(beg, csr, c, wid, &prev, &cur, &hop, &h, path, &st, trace, trace_cap,
+                               ntrace, &tc);
+    if (final3) {
+        final3[0] = prev;
+        final3[1] = cur;
+        final3[2] = hop;
+    }
+    return moves;
+}

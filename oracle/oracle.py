@@ -1,0 +1,341 @@
+"""CPU oracle for the GOWalker walk step -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU legs import this
+module, and only as the checker or the timed CPU baseline.  The product
+(gowalker_b200) never imports it.
+
+Contents:
+  * ctypes wrappers over liboracle.so (gw_oracle.c): Philox4x32-10, the
+    counter-based R-MAT sampler and the Node2vec / SOPR / SOSR whole-walk
+    restatement of engine/engine.hpp:158-404;
+  * a numpy CSR builder (drop self loops, optional symmetrisation, dedup,
+    sorted adjacency) for the synthetic R-MAT graphs;
+  * writers for the reference's on-disk format: ``<base>.beg`` (u64, V+1),
+    ``<base>.csr`` (u32, E), ``<base>.meta`` (packed u32 nvertices, u64 nedges,
+    u32 min_vert; preprocess/graph_converter.hpp finalize()), and the block
+    files ``sowalker_<MB>/<name>_<MB>MB.{vert,edge}.blocks``
+    (util/util.hpp:148-165, preprocess/split.hpp:74-84);
+  * a restatement of the reference's block splitter
+    (preprocess/split.hpp:15-87) and the equal-edge-mass splitter;
+  * a loader for oracle/_ref/libref_step*.so, the harness that runs the
+    reference's own sidewalkupdate.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+ALG_NODE2VEC, ALG_SOPR, ALG_SOSR = 0, 1, 2
+INIT_PER_VERTEX, INIT_SINGLE_SOURCE, INIT_RANDOM = 0, 1, 2
+KEY_HOP_ATTEMPT, KEY_TRIAL = 0, 1
+
+RMAT_ABC = (0.57, 0.19, 0.19)
+
+
+class Cfg(ctypes.Structure):
+    _fields_ = [
+        ("algo", ctypes.c_uint32),
+        ("maxhops", ctypes.c_uint32),
+        ("p", ctypes.c_float),
+        ("q", ctypes.c_float),
+        ("alpha", ctypes.c_float),
+        ("term_prob", ctypes.c_float),
+        ("seed", ctypes.c_uint64),
+        ("keying", ctypes.c_uint32),
+        ("init_mode", ctypes.c_uint32),
+        ("wps", ctypes.c_uint32),
+        ("numwalks", ctypes.c_uint32),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("steps", ctypes.c_uint64),
+        ("trials", ctypes.c_uint64),
+        ("probes", ctypes.c_uint64),
+        ("search_sectors", ctypes.c_uint64),
+        ("off_sectors", ctypes.c_uint64),
+        ("dead_ends", ctypes.c_uint64),
+        ("terminated", ctypes.c_uint64),
+    ]
+
+    def as_dict(self):
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
+_LIB = None
+
+
+def build_oracle(with_ref: bool = False) -> None:
+    """Compile liboracle.so (and the reference harness when asked)."""
+    target = "all" if with_ref else "oracle"
+    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build_oracle()
+        L = ctypes.CDLL(path)
+        u32p = ctypes.POINTER(ctypes.c_uint32)
+        u64p = ctypes.POINTER(ctypes.c_uint64)
+        L.oracle_philox4x32_10.argtypes = [u32p, u32p, u32p]
+        L.oracle_rmat_edges.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, u32p,
+                                        ctypes.c_uint64, u32p, u32p, ctypes.c_int]
+        L.oracle_walk.argtypes = [u64p, u32p, ctypes.c_uint32, ctypes.POINTER(Cfg), ctypes.c_uint32,
+                                  ctypes.c_uint32, u32p, u32p, u64p, u32p, ctypes.POINTER(Stats),
+                                  ctypes.c_int]
+        L.oracle_walk.restype = ctypes.c_int
+        L.oracle_walk_traced.argtypes = [u64p, u32p, ctypes.POINTER(Cfg), ctypes.c_uint32,
+                                         ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, u32p,
+                                         u32p, ctypes.c_uint64, u64p, u32p]
+        L.oracle_walk_traced.restype = ctypes.c_uint32
+        L.oracle_walker_source.argtypes = [ctypes.POINTER(Cfg), ctypes.c_uint32, ctypes.c_uint32]
+        L.oracle_walker_source.restype = ctypes.c_uint32
+        L.oracle_hash_init.argtypes = [ctypes.c_uint32]
+        L.oracle_hash_init.restype = ctypes.c_uint64
+        _LIB = L
+    return _LIB
+
+
+def _p(a, ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+# ------------------------------------------------------------------ Philox
+
+def philox(ctr, key) -> np.ndarray:
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint32)
+    lib().oracle_philox4x32_10(_p(c, ctypes.c_uint32), _p(k, ctypes.c_uint32), _p(out, ctypes.c_uint32))
+    return out
+
+
+# ------------------------------------------------------------------ graphs
+
+def rmat_thresholds(a: float, b: float, c: float) -> np.ndarray:
+    """Cumulative quadrant thresholds a, a+b, a+b+c scaled to 2^32, as u32."""
+    t = [int(a * 4294967296.0), int((a + b) * 4294967296.0), int((a + b + c) * 4294967296.0)]
+    return np.array([min(x, 0xFFFFFFFF) for x in t], dtype=np.uint32)
+
+
+def rmat_edges(scale: int, first: int, count: int, seed: int = 1, abc=RMAT_ABC, nthreads: int = 0):
+    thr = rmat_thresholds(*abc)
+    src = np.empty(count, dtype=np.uint32)
+    dst = np.empty(count, dtype=np.uint32)
+    lib().oracle_rmat_edges(scale, first, count, _p(thr, ctypes.c_uint32), seed,
+                            _p(src, ctypes.c_uint32), _p(dst, ctypes.c_uint32), nthreads)
+    return src, dst
+
+
+def build_csr(nverts: int, src: np.ndarray, dst: np.ndarray, symmetric: bool = True):
+    """CSR with u64 offsets and sorted, duplicate-free u32 adjacency; self loops
+    dropped (preprocess/graph_converter.hpp:362-363)."""
+    src = src.astype(np.uint64)
+    dst = dst.astype(np.uint64)
+    keep = src != dst
+    src, dst = src[keep], dst[keep]
+    if symmetric:
+        src, dst = np.concatenate([src, dst]), np.concatenate([dst, src])
+    keys = np.unique((src << np.uint64(32)) | dst)
+    s = (keys >> np.uint64(32)).astype(np.int64)
+    csr = (keys & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+    beg = np.zeros(nverts + 1, dtype=np.uint64)
+    beg[1:] = np.cumsum(np.bincount(s, minlength=nverts)).astype(np.uint64)
+    return beg, csr
+
+
+def rmat_graph(scale: int, edgefactor: int = 16, seed: int = 1, abc=RMAT_ABC, symmetric: bool = True):
+    """Synthetic R-MAT graph: (edgefactor << scale) counter-based samples."""
+    n = edgefactor << scale
+    src, dst = rmat_edges(scale, 0, n, seed, abc)
+    return build_csr(1 << scale, src, dst, symmetric)
+
+
+def check_csr(beg: np.ndarray, csr: np.ndarray) -> None:
+    assert beg.dtype == np.uint64 and csr.dtype == np.uint32
+    assert int(beg[0]) == 0 and int(beg[-1]) == len(csr)
+    assert np.all(np.diff(beg.astype(np.int64)) >= 0)
+
+
+# ------------------------------------------------------------------ walks
+
+def make_cfg(algo=ALG_NODE2VEC, maxhops=80, p=2.0, q=0.5, alpha=0.2, term_prob=0.0, seed=42,
+             keying=KEY_HOP_ATTEMPT, init_mode=INIT_PER_VERTEX, wps=1, numwalks=0) -> Cfg:
+    return Cfg(algo, maxhops, p, q, alpha, term_prob, seed, keying, init_mode, wps, numwalks)
+
+
+def walk(beg, csr, cfg: Cfg, wid_begin: int, count: int, paths: bool = True, finals: bool = False,
+         nthreads: int = 0):
+    """Walk walkers [wid_begin, wid_begin+count).  Returns a dict with
+    paths (count x maxhops+1, zero padded), lens, hashes, finals, stats."""
+    nverts = len(beg) - 1
+    stride = cfg.maxhops + 1
+    P = np.zeros((count, stride), dtype=np.uint32) if paths else None
+    L = np.zeros(count, dtype=np.uint32)
+    H = np.zeros(count, dtype=np.uint64)
+    F = np.zeros((count, 3), dtype=np.uint32) if finals else None
+    st = Stats()
+    rc = lib().oracle_walk(_p(beg, ctypes.c_uint64), _p(csr, ctypes.c_uint32), nverts, ctypes.byref(cfg),
+                           wid_begin, count, _p(P, ctypes.c_uint32), _p(L, ctypes.c_uint32),
+                           _p(H, ctypes.c_uint64), _p(F, ctypes.c_uint32), ctypes.byref(st), nthreads)
+    if rc != 0:
+        raise ValueError("oracle_walk rejected the configuration")
+    return {"paths": P, "lens": L, "hashes": H, "finals": F, "stats": st.as_dict()}
+
+
+def walk_traced(beg, csr, cfg: Cfg, wid: int, prev: int, cur: int, hop: int, cap: int = 1 << 16):
+    path = np.zeros(cfg.maxhops + 1, dtype=np.uint32)
+    trace = np.zeros((cap, 4), dtype=np.uint32)
+    n = ctypes.c_uint64(0)
+    final = np.zeros(3, dtype=np.uint32)
+    moves = lib().oracle_walk_traced(_p(beg, ctypes.c_uint64), _p(csr, ctypes.c_uint32), ctypes.byref(cfg),
+                                     wid, prev, cur, hop, _p(path, ctypes.c_uint32),
+                                     _p(trace, ctypes.c_uint32), cap, ctypes.byref(n),
+                                     _p(final, ctypes.c_uint32))
+    return int(moves), path[:moves], trace[: min(int(n.value), cap)], final
+
+
+def path_hash(path) -> int:
+    """FNV-1a over 32-bit vertex ids (the engine's per-walker path hash)."""
+    h = 0xCBF29CE484222325
+    for v in path:
+        h = ((h ^ int(v)) * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+# ------------------------------------------------------------------ files
+
+def block_names(base: str, blocksize_mb: int):
+    folder = os.path.join(os.path.dirname(base) or ".", "sowalker_%d" % blocksize_mb)
+    name = os.path.basename(base)
+    vb = os.path.join(folder, "%s_%dMB.vert.blocks" % (name, blocksize_mb))
+    eb = os.path.join(folder, "%s_%dMB.edge.blocks" % (name, blocksize_mb))
+    return folder, vb, eb
+
+
+def write_dataset(base: str, beg: np.ndarray, csr: np.ndarray, min_vert: int = 0) -> None:
+    beg.astype(np.uint64).tofile(base + ".beg")
+    csr.astype(np.uint32).tofile(base + ".csr")
+    meta = np.zeros(16, dtype=np.uint8)
+    meta[0:4] = np.frombuffer(np.uint32(len(beg) - 1).tobytes(), np.uint8)
+    meta[4:12] = np.frombuffer(np.uint64(len(csr)).tobytes(), np.uint8)
+    meta[12:16] = np.frombuffer(np.uint32(min_vert).tobytes(), np.uint8)
+    meta.tofile(base + ".meta")
+
+
+def write_blocks(base: str, blocksize_mb: int, vblocks, eblocks) -> None:
+    folder, vb, eb = block_names(base, blocksize_mb)
+    os.makedirs(folder, exist_ok=True)
+    np.asarray(vblocks, dtype=np.uint32).tofile(vb)
+    np.asarray(eblocks, dtype=np.uint64).tofile(eb)
+
+
+def split_blocks_reference(beg: np.ndarray, block_size: int):
+    """Restatement of split_blocks (preprocess/split.hpp:15-87): walk beg[] and
+    cut a block when its edges exceed block_size/4 (the cut goes one vertex
+    back) or its vertices reach block_size/8."""
+    max_nedges = block_size // 4
+    max_nverts = block_size // 8
+    nv = len(beg)  # the file holds V+1 offsets; the reference calls that nvertices
+    vblocks, eblocks = [0], [0]
+    cur_pos, rd_edges = 0, 0
+    for v in range(nv):
+        if int(beg[v]) - rd_edges > max_nedges:
+            cur_pos = v - 1
+            vblocks.append(cur_pos)
+            rd_edges = int(beg[v - 1])
+            eblocks.append(rd_edges)
+        elif v - cur_pos >= max_nverts:
+            cur_pos = v
+            vblocks.append(cur_pos)
+            rd_edges = int(beg[v])
+            eblocks.append(rd_edges)
+    vblocks.append(nv - 1)
+    eblocks.append(int(beg[nv - 1]))
+    return np.array(vblocks, dtype=np.uint32), np.array(eblocks, dtype=np.uint64)
+
+
+def split_equal_edge_mass(beg: np.ndarray, nblocks: int):
+    """Vertex-range blocks of (nearly) equal edge mass: block b ends at the
+    first vertex whose offset reaches b*E/nblocks."""
+    V = len(beg) - 1
+    E = int(beg[-1])
+    targets = (np.arange(1, nblocks, dtype=np.float64) * E / nblocks).astype(np.uint64)
+    cuts = np.searchsorted(beg[:-1], targets, side="left").astype(np.int64)
+    cuts = np.maximum.accumulate(np.clip(cuts, 1, max(V - 1, 1)))
+    vb = np.concatenate([[0], cuts, [V]]).astype(np.int64)
+    vb = np.maximum.accumulate(vb)
+    vb = vb.astype(np.uint32)
+    eb = beg[vb.astype(np.int64)].astype(np.uint64)
+    return vb, eb
+
+
+# ------------------------------------------------------------------ reference harness
+
+def ref_lib(unmodified: bool = False):
+    """Load the harness built from the reference's own headers."""
+    name = "libref_step_unmod.so" if unmodified else "libref_step.so"
+    path = os.path.join(REF_DIR, name)
+    if not os.path.exists(path):
+        return None
+    L = ctypes.CDLL(path)
+    u32p = ctypes.POINTER(ctypes.c_uint32)
+    L.ref_open.argtypes = [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                           ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
+    L.ref_open.restype = ctypes.c_int
+    L.ref_set_seed.argtypes = [ctypes.c_uint64]
+    L.ref_walk.argtypes = [ctypes.c_uint32] * 6 + [u32p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64),
+                                                   ctypes.POINTER(ctypes.c_int), u32p]
+    L.ref_walk.restype = ctypes.c_int
+    L.ref_get_block.argtypes = [ctypes.c_uint32]
+    L.ref_get_block.restype = ctypes.c_uint32
+    return L
+
+
+def ref_walk(L, wid, prev, cur, hop, prev_blk, cur_blk, cap=1 << 16):
+    trace = np.zeros((cap, 4), dtype=np.uint32)
+    n = ctypes.c_uint64(0)
+    pushed = ctypes.c_int(0)
+    state = np.zeros(5, dtype=np.uint32)
+    run = L.ref_walk(wid, prev, cur, hop, prev_blk, cur_blk, _p(trace, ctypes.c_uint32), cap,
+                     ctypes.byref(n), ctypes.byref(pushed), _p(state, ctypes.c_uint32))
+    return run, trace[: min(int(n.value), cap)], bool(pushed.value), state
+
+
+def ref_scenario(base: str, algo: int, p: float, q: float, alpha: float, maxhops: int, blocksize_mb: int,
+                 seed: int, starts, unmodified: bool = False, cpu_batch: int = 1):
+    """Open the reference harness on the dataset at `base` and run one
+    sidewalkupdate per start tuple (wid, prev, cur, hop, prev_blk, cur_blk).
+    The harness keeps global state, so call this in a fresh process
+    (multiprocessing 'spawn')."""
+    L = ref_lib(unmodified)
+    if L is None:
+        raise FileNotFoundError("oracle/_ref harness not built")
+    nb = L.ref_open(base.encode(), algo, p, q, alpha, maxhops, blocksize_mb, cpu_batch)
+    L.ref_set_seed(seed)
+    return nb, [ref_walk(L, *s) for s in starts]
+
+
+def harness_graph(beg: np.ndarray, csr: np.ndarray):
+    """Graph G' for driving the reference's cross-block loop from a walk's
+    first step: vertex V+v is a copy of v's adjacency (nothing points to it),
+    so a walker at (prev=V+v, cur=v) takes exactly the step that (prev=v,
+    cur=v) takes, while prev and cur sit in different one-vertex blocks."""
+    V = len(beg) - 1
+    beg2 = np.concatenate([beg, beg[-1] + beg[1:]]).astype(np.uint64)
+    csr2 = np.concatenate([csr, csr]).astype(np.uint32)
+    vblocks = np.arange(2 * V + 1, dtype=np.uint32)
+    eblocks = beg2.copy()
+    return beg2, csr2, vblocks, eblocks
