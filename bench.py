@@ -1,0 +1,380 @@
+#!/usr/bin/env python3
+"""Walk-engine benchmark: walk steps/s on one B200 (per rank), JSON on one line.
+
+Workload (default, `--config c2`): SOPR walks (reference transition rule,
+alpha 0.2), termination probability 0.15 per step, at most 20 steps, 4
+walkers per vertex, on a synthetic R-MAT graph of scale 24 (16,777,216
+vertices, edge factor 16, (a,b,c,d) = (0.57,0.19,0.19,0.05), generator seed 1,
+symmetrised, ~500 M directed edges, u32 ids, u64 offsets), in-core, walk seed
+42.  `--config c1` is the Node2vec scale-20 workload (p=2, q=0.5, length 80).
+
+One bench step = one full run of every walker of the workload (gw_run).
+  value : steps/s with the graph resident in HBM (gw_device_graph), timed with
+          CUDA events on the engine's launching stream.
+  e2e   : the same through the C ABI with the graph in pinned HOST blocks: each
+          step drops the device cache (gw_cache_reset), so the run copies the
+          CSR host->device, validates it, walks, and reads the counters back.
+
+Under torchrun each rank runs the workload with walk seed 42+rank (walkers are
+independent: no data-path collective); value = all ranks' steps / max time.
+
+`--impl reference` times the oracle (the reference CPU step rule restated in
+C, OpenMP over all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "c2": dict(name="C2: SOPR alpha=0.2, termination 0.15, max length 20, 4 walkers/vertex, "
+                    "R-MAT scale 24 ef 16 symmetrised, in-core",
+               scale=24, ef=16, algo=1, maxhops=20, wps=4, p=0.5, q=2.0, alpha=0.2, term=0.15),
+    "c1": dict(name="C1: Node2vec p=2 q=0.5 length 80, 1 walker/vertex, R-MAT scale 20 ef 16 symmetrised, in-core",
+               scale=20, ef=16, algo=0, maxhops=80, wps=1, p=2.0, q=0.5, alpha=0.2, term=0.0),
+}
+L2_BYTES = 126 * 1024 * 1024
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def profile_bytes_per_step(workload):
+    """dram bytes per walk step from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "walk_incore_%s.md" % workload)
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"dram_bytes_per_step:\s*([0-9.]+)", txt)
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- helpers
+
+def build_graph(gw, wl):
+    t0 = time.time()
+    dg = gw.DeviceGraph(wl["scale"], edgefactor=wl["ef"], seed=1, symmetric=True)
+    log("graph: V=%d E=%d built on device in %.1fs" % (dg.nverts, dg.nedges, time.time() - t0))
+    return dg
+
+
+def host_graph(dg):
+    beg_t, csr_t = dg.to_host(pinned=True)
+    beg = beg_t.numpy().view(np.uint64)
+    csr = csr_t.numpy().view(np.uint32)[: dg.nedges]
+    return beg_t, csr_t, beg, csr
+
+
+def oracle_sample(O, beg, csr, wl, seed, target_s, nchunks=32, threads=0):
+    """Time the oracle on an evenly spread sample of the workload's walkers,
+    sized to take about target_s seconds.  Returns (steps, seconds, stats,
+    walkers, description)."""
+    V = len(beg) - 1
+    nwalk = V * wl["wps"]
+    cfg = O.make_cfg(algo=wl["algo"], maxhops=wl["maxhops"], p=wl["p"], q=wl["q"], alpha=wl["alpha"],
+                     term_prob=wl["term"], seed=seed, wps=wl["wps"])
+    # calibration
+    t0 = time.time()
+    r = O.walk(beg, csr, cfg, nwalk // 3, 20000, paths=False, nthreads=threads)
+    dt = max(time.time() - t0, 1e-3)
+    per_walker = dt / 20000
+    count = int(max(nchunks * 64, min(nwalk, target_s / per_walker)))
+    chunk = max(1, count // nchunks)
+    starts = [int(i * (nwalk - chunk) / max(nchunks - 1, 1)) for i in range(nchunks)]
+    tot = {k: 0 for k in r["stats"]}
+    t0 = time.time()
+    for s in starts:
+        rr = O.walk(beg, csr, cfg, s, chunk, paths=False, nthreads=threads)
+        for k, v in rr["stats"].items():
+            tot[k] += v
+    secs = time.time() - t0
+    desc = "%d walkers in %d evenly spaced runs of %d (of %d)" % (chunk * nchunks, nchunks, chunk, nwalk)
+    return tot["steps"], secs, tot, chunk * nchunks, desc
+
+
+def algorithmic_bytes(stats, walkers, paths):
+    """Bytes the walk must move: 32-B sectors for (beg[cur], beg[cur+1]), one csr
+    sector per trial, the distinct sectors of each trial's search of N(prev),
+    plus the per-walker outputs (hash 8 B, length 4 B, path entries 4 B)."""
+    b = 32 * (stats["off_sectors"] + stats["trials"] + stats["search_sectors"])
+    b += 12 * walkers
+    if paths:
+        b += 4 * (stats["steps"] + walkers)
+    return b
+
+
+# ---------------------------------------------------------------- arms
+
+def run_reference_arm(args, wl):
+    """The reference's CPU walk step (oracle port) on the host cores."""
+    import gowalker_b200 as gw
+    from oracle import oracle as O
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    dg = build_graph(gw, wl)
+    _, _, beg, csr = host_graph(dg)[:4]
+    dg.free()
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        oracle_sample(O, beg, csr, wl, 42, 0.5, threads=threads)
+    steps = secs = 0.0
+    desc = ""
+    for _ in range(args.steps):
+        s, t, _, _, desc = oracle_sample(O, beg, csr, wl, 42, args.ref_seconds, threads=threads)
+        steps += s
+        secs += t
+    v = steps / secs
+    line = {"impl": "reference", "metric": "walk steps/sec", "value": v, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32+fp32/fp64 compares",
+            "data": "synthetic", "config": {"workload": wl["name"]},
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port",
+                             "sample": "per step: " + desc},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, wl):
+    import torch
+    import gowalker_b200 as gw
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    seed = 42 + rank
+    paths = 1 if args.paths else 0
+
+    dg = build_graph(gw, wl)
+    cfgkw = dict(algorithm=wl["algo"], maxhops=wl["maxhops"], p=wl["p"], q=wl["q"], alpha=wl["alpha"],
+                 term_prob=wl["term"], seed=seed, walkpersource=wl["wps"], record_paths=paths, device=local,
+                 cache_size=1 << 40)
+    eng = gw.WalkEngine(**cfgkw)
+    eng.set_device_graph(dg.nverts, dg.nedges, dg.beg_ptr, dg.csr_ptr)
+    stream = torch.cuda.ExternalStream(eng.stream_handle(), device=local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident runs
+    for _ in range(args.warmup):
+        eng.init_walkers(wl["algo"], wl["wps"], seed)
+        eng.run()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    steps = 0
+    kernel_ms = 0.0
+    launches = 0
+    for _ in range(args.steps):
+        eng.init_walkers(wl["algo"], wl["wps"], seed)
+        st = eng.run()
+        steps += st["steps"]
+        kernel_ms += st["kernel_ms"]
+        launches += st["launches"]
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    hash_sum, steps_last = eng.checksum()
+    nwalkers = eng.num_walkers()
+
+    # ---- end to end through the C ABI with host blocks
+    beg_t, csr_t, beg, csr = host_graph(dg)
+    eng2 = gw.WalkEngine(**cfgkw)
+    eng2.set_host_graph(beg_t, csr_t[: dg.nedges])
+    stream2 = torch.cuda.ExternalStream(eng2.stream_handle(), device=local)
+    for _ in range(max(1, args.warmup)):
+        eng2.cache_reset()
+        eng2.init_walkers(wl["algo"], wl["wps"], seed)
+        eng2.run()
+    barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream2)
+    e2e_steps = h2d = d2h = 0
+    for _ in range(args.steps):
+        eng2.cache_reset()
+        eng2.init_walkers(wl["algo"], wl["wps"], seed)
+        st2 = eng2.run()
+        e2e_steps += st2["steps"]
+        h2d += st2["h2d_bytes"]
+        d2h += st2["d2h_bytes"]
+        launches += 0
+    hs2, _ = eng2.checksum()
+    f1.record(stream2)
+    barrier()
+    ms2 = f0.elapsed_time(f1)
+    if hs2 != hash_sum:
+        log("warning: e2e checksum differs from the device-resident run")
+
+    # max over ranks
+    t = torch.tensor([ms, ms2, float(steps), float(e2e_steps)], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        tmax = t.clone()
+        dist.all_reduce(tmax[:2], op=dist.ReduceOp.MAX)
+        tsum = t.clone()
+        dist.all_reduce(tsum[2:], op=dist.ReduceOp.SUM)
+        ms, ms2 = float(tmax[0]), float(tmax[1])
+        steps_all, e2e_all = float(tsum[2]), float(tsum[3])
+    else:
+        steps_all, e2e_all = float(steps), float(e2e_steps)
+
+    if rank == 0:
+        peaks, peak_kind = measured_peaks()
+        value = steps_all / (ms / 1000.0)
+        line = {
+            "metric": "walk steps/sec", "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32 gathers, fp32/fp64 accept compares", "data": "synthetic",
+            "config": {"workload": wl["name"], "vertices": dg.nverts, "edges": dg.nedges, "walkers": nwalkers,
+                       "csr_bytes": (dg.nverts + 1) * 8 + dg.nedges * 4,
+                       "l2": "inputs larger than L2 (CSR %.2f GB vs 126 MB L2); no flush"
+                             % (((dg.nverts + 1) * 8 + dg.nedges * 4) / 1e9),
+                       "paths_recorded": bool(paths), "walk_seed": "42+rank", "generator_seed": 1,
+                       "parallelism": "walker replicas per rank" if world > 1 else "1 GPU"},
+            "gpu_launches": launches,
+            "e2e": {"value": e2e_all / (ms2 / 1000.0), "unit": "steps/s",
+                    "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps},
+            "checksum": {"path_hash_sum": hash_sum, "steps_per_run": steps_last},
+        }
+        if clk:
+            line["clocks"] = clk
+        # roofline of the step kernel from the oracle's exact sector counts on a sample
+        from oracle import oracle as O
+        O.lib()
+        threads = os.cpu_count() or 1
+        s_steps, s_secs, s_stats, s_walk, s_desc = oracle_sample(O, beg, csr, wl, seed, args.cpu_seconds,
+                                                                 threads=threads)
+        bpstep = algorithmic_bytes(s_stats, s_walk, paths) / max(s_steps, 1)
+        kernel_s = kernel_ms / 1000.0 / args.steps
+        steps_per_launch = steps / args.steps
+        achieved = bpstep * steps_per_launch / kernel_s / 1e9
+        dram_ps = profile_bytes_per_step(args.config)
+        line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                            "frac": achieved / peaks["hbm_gbs"],
+                            "traffic": (dram_ps * steps_per_launch) if dram_ps else None,
+                            "peak_source": peak_kind,
+                            "algorithmic_bytes_per_step": bpstep, "kernel_ms_per_launch": kernel_ms / args.steps,
+                            "kernel": "k_walk_incore"}
+        line["cpu_baseline"] = {"value": s_steps / s_secs, "unit": "steps/s", "cores": threads, "kind": "port",
+                                "sample": s_desc}
+        print(json.dumps(line), flush=True)
+    eng.close()
+    eng2.close()
+    dg.free()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--scale", type=int, default=None, help="override the graph scale (smaller smoke runs)")
+    ap.add_argument("--paths", type=int, default=1, help="record full paths (1) or hashes only (0)")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-seconds", type=float, default=8.0)
+    args = ap.parse_args()
+    wl = dict(WORKLOADS[args.config])
+    if args.scale:
+        wl["scale"] = args.scale
+        wl["name"] = wl["name"].replace("scale %d" % WORKLOADS[args.config]["scale"], "scale %d" % args.scale)
+    if args.warmup < 3:
+        log("note: fewer than 3 warm-up steps")
+    if args.impl == "reference":
+        return run_reference_arm(args, wl)
+    return run_ours(args, wl)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

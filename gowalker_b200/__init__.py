@@ -1,0 +1,17 @@
+"""gowalker_b200 -- a B200-native second-order random-walk engine with the
+interface of GOWalker's walk path (Node2vec / SOPR / SOSR).
+
+The engine itself is libgowalker.so (C ABI in include/gowalker.h, kernels in
+gowalker_b200/csrc).  This package is its Python binding; importing it loads
+the library and fails loudly when it has not been built.
+"""
+from ._abi import (GW_INIT_PER_VERTEX, GW_INIT_RANDOM, GW_INIT_SINGLE_SOURCE, GW_NODE2VEC, GW_PATHS_FULL,
+                   GW_PATHS_NONE, GW_POLICY_LEARNED, GW_POLICY_PLAIN, GW_SOPR, GW_SOSR, GwConfig, GwError,
+                   GwStats, LIB_PATH, load)
+from .engine import DeviceGraph, WalkEngine, default_config
+
+__all__ = [
+    "GW_NODE2VEC", "GW_SOPR", "GW_SOSR", "GW_INIT_PER_VERTEX", "GW_INIT_SINGLE_SOURCE", "GW_INIT_RANDOM",
+    "GW_POLICY_PLAIN", "GW_POLICY_LEARNED", "GW_PATHS_NONE", "GW_PATHS_FULL", "GwConfig", "GwStats",
+    "GwError", "WalkEngine", "DeviceGraph", "default_config", "load", "LIB_PATH",
+]

@@ -1,0 +1,68 @@
+// Launch interfaces of the engine's kernels (internal to libgowalker.so).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "gw_step.cuh"
+
+namespace gw {
+
+constexpr int kWalkThreads = 256;   // threads per CTA of the walk kernels
+constexpr uint32_t kChunk = 64;     // walkers a warp claims per atomic
+
+// Work / statistics counters of one run (device, zeroed per run).
+enum Counter : int {
+    kCtrCursor = 0,   // next walker index to hand out
+    kCtrSteps = 1,
+    kCtrTrials = 2,
+    kCtrDone = 3,
+    kCtrHashSum = 4,  // wrapping sum of finished walkers' path hashes
+    kCtrCount = 8
+};
+
+// Error word bits set by kernels instead of trapping.
+enum ErrBit : uint32_t {
+    kErrVertexRange = 1u,   // a neighbour id >= nverts
+    kErrSource = 2u,        // a walker source >= nverts
+    kErrBlock = 4u,         // a vertex outside every block
+    kErrTrials = 8u,        // a step exceeded kMaxAttempts rejection trials
+};
+
+// Rejection trials allowed for one step before the walker is stopped with
+// kErrTrials.  Only degenerate parameters get near it (e.g. alpha = 1 on a
+// directed graph whose N(cur) and N(prev) are disjoint): the worst R-MAT case
+// of the SOPR rule, a step from a degree-1 vertex into a hub of degree d,
+// needs 1 + alpha*d/(1-alpha) trials on average (~1.3e6 for d = 5e6), so a
+// cap of 2^26 is never reached by a valid walk.
+constexpr uint32_t kMaxAttempts = 1u << 26;
+
+struct WalkerInit {
+    uint32_t mode;       // GW_INIT_*
+    uint32_t algo;       // GW_NODE2VEC / GW_SOPR / GW_SOSR
+    uint32_t wps;        // walkers per vertex
+    uint32_t numwalks;   // total walkers (single-source / random)
+    uint32_t nverts;
+    uint32_t key0, key1; // walk seed (random init)
+};
+
+struct IncoreArgs {
+    StepConsts c;
+    WalkerInit init;
+    const uint64_t *beg;       // nverts+1 global offsets
+    const uint32_t *csr;       // nedges neighbour ids
+    uint32_t nverts;
+    uint32_t nwalkers;
+    uint32_t *paths;           // nwalkers x stride, or null
+    uint32_t stride;           // maxhops + 1
+    uint32_t *lens;            // vertices per path
+    uint64_t *hashes;          // FNV-1a per path
+    unsigned long long *ctr;   // Counter slots
+    uint32_t *err;             // ErrBit word
+};
+
+// Grid size (CTAs) for a persistent walk kernel on this device.
+int incore_grid(bool sopr, bool paths, int num_sms);
+cudaError_t launch_walk_incore(const IncoreArgs &a, bool sopr, int grid, cudaStream_t s);
+cudaError_t launch_validate_csr(const uint64_t *beg, const uint32_t *csr, uint32_t nverts, uint64_t nedges,
+                                uint32_t *err, int num_sms, cudaStream_t s);
+
+}  // namespace gw

@@ -1,0 +1,115 @@
+// The second-order walk step, shared by every walk kernel.
+//
+// Semantics follow the reference CPU step (GOWalker engine/engine.hpp:158-404)
+// with every draw taken from Philox4x32-10 keyed by the walk seed and
+// countered by (walker id, hop, attempt, 0):
+//   lane x -> rand_pos = x % deg                                (util/util.hpp:294)
+//   lane y -> rand_val = float(y >> 8) * 2^-24 * max_val        (one fp32 multiply)
+//   lane z -> SOPR/SOSR termination draw at hop >= 1 (attempt 0)
+// Acceptance keeps the reference's precision mix:
+//   Node2vec: fp32 thresholds 1/p, 1, 1/q, min and max of the three
+//             (engine/engine.hpp:169-172, 209-258)
+//   SOPR/SOSR: inv_deg = (float)((1-alpha)/deg) in fp64, inv_prev_deg =
+//             alpha/(float)prev_deg in fp32 (323-326); the x==prev compare is
+//             fp64 (341), the others fp32 (334, 368, 373).
+// Every rounding step is an explicit _rn intrinsic so no contraction or
+// fast-math flag can change a bit.
+#pragma once
+#include <cstdint>
+#include "gw_philox.cuh"
+
+namespace gw {
+
+// Per-run constants, computed on the host.
+struct StepConsts {
+    uint32_t maxhops;
+    uint32_t key0, key1;
+    float n2v_maxv, n2v_minv;  // max / min of {1/p, 1/q, 1}
+    float inv_p, inv_q;        // 1.0f/p, 1.0f/q
+    float alpha;               // SOPR/SOSR
+    float term_prob;           // 0 = no termination draw
+    double one_m_alpha;        // 1.0 - (double)alpha
+};
+
+// Thresholds of one step (depend on deg / prev_deg for SOPR).
+struct StepThr {
+    float maxv, minv;
+    float t_prev;      // Node2vec: x == prev accepts below 1/p
+    float t_found;     // x in N(prev)
+    float t_notfound;  // otherwise
+    double t_prev_d;   // SOPR: x == prev accepts below (1-alpha)/deg in fp64
+};
+
+template <bool SOPR>
+__device__ __forceinline__ StepThr step_thresholds(const StepConsts &c, uint64_t deg, uint64_t pdeg)
+{
+    StepThr t;
+    if constexpr (!SOPR) {
+        t.maxv = c.n2v_maxv;
+        t.minv = c.n2v_minv;
+        t.t_prev = c.inv_p;
+        t.t_found = 1.0f;
+        t.t_notfound = c.inv_q;
+        t.t_prev_d = 0.0;
+    } else {
+        const double tp = __ddiv_rn(c.one_m_alpha, (double)deg);
+        const float inv_deg = __double2float_rn(tp);
+        const float inv_prev = __fdiv_rn(c.alpha, __ull2float_rn((unsigned long long)pdeg));
+        const float sum = __fadd_rn(inv_deg, inv_prev);
+        t.maxv = (inv_deg < sum) ? sum : inv_deg;   // std::max(inv_deg, sum)
+        t.minv = (sum < inv_deg) ? sum : inv_deg;   // std::min(inv_deg, sum)
+        t.t_prev = 0.f;
+        t.t_found = sum;
+        t.t_notfound = inv_deg;
+        t.t_prev_d = tp;
+    }
+    return t;
+}
+
+__device__ __forceinline__ U4 draw(const StepConsts &c, uint32_t wid, uint32_t hop, uint32_t attempt)
+{
+    return philox4x32_10(wid, hop, attempt, kTagWalk, c.key0, c.key1);
+}
+
+__device__ __forceinline__ float rand_val(uint32_t y, float maxv)
+{
+    return __fmul_rn(__uint2float_rn(y >> 8) * 0x1p-24f, maxv);
+}
+
+__device__ __forceinline__ bool terminates(const StepConsts &c, uint32_t z)
+{
+    return c.term_prob > 0.0f && __uint2float_rn(z >> 8) * 0x1p-24f < c.term_prob;
+}
+
+// Membership of x in the sorted run base[0, n): plain binary search.
+__device__ __forceinline__ bool search_sorted(const uint32_t *__restrict__ base, uint32_t n, uint32_t x)
+{
+    int32_t lo = 0, hi = (int32_t)n - 1;
+    while (lo <= hi) {
+        const int32_t mid = lo + ((hi - lo) >> 1);
+        const uint32_t v = __ldg(base + mid);
+        if (v == x) return true;
+        if (v < x) lo = mid + 1;
+        else hi = mid - 1;
+    }
+    return false;
+}
+
+// Acceptance of candidate x drawn with rand value rv (engine/engine.hpp:209-258,
+// 334-375).  `searched` gets the membership result when a search ran.
+template <bool SOPR>
+__device__ __forceinline__ bool accept_candidate(const StepThr &t, float rv, uint32_t x, uint32_t prev,
+                                                 uint32_t cur, const uint32_t *__restrict__ prev_adj,
+                                                 uint32_t pdeg)
+{
+    if (rv <= t.minv) return true;
+    if (x == prev) {
+        if constexpr (SOPR) return (double)rv < t.t_prev_d;
+        else return rv < t.t_prev;
+    }
+    // x is drawn from N(cur); when prev == cur the search must succeed.
+    const bool found = (prev == cur) ? true : search_sorted(prev_adj, pdeg, x);
+    return found ? (rv < t.t_found) : (rv < t.t_notfound);
+}
+
+}  // namespace gw

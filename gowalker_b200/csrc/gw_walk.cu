@@ -1,0 +1,236 @@
+// Step kernels of the walk engine (replace GOWalker gpu/gpuwalk.hpp:87-319).
+//
+// In-core kernel: one persistent grid sized to fill the SMs.  Each lane owns
+// one walker at a time and takes it to the end; a warp claims walker ids in
+// chunks of kChunk with one atomic and hands them to its idle lanes, so lanes
+// whose walks end early (SOPR termination, dead ends) pick up new walkers
+// instead of idling -- the work-stealing loop that replaces the reference's
+// grid-stride loop (gpu/gpuwalk.hpp:200) and its one-walker-per-thread
+// imbalance.  The loop body is one rejection-sampling trial, so lanes of a
+// warp stay converged at trial granularity whatever their walk lengths.
+//
+// Walkers of the in-core kernel are generated from their id on the fly
+// (engine/walk.hpp:32-49 for per-vertex init), so no walker record is read
+// or written; per walker the kernel writes its path row (optional), length
+// and 64-bit path hash.
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "gw_kernels.cuh"
+#include "../../include/gowalker.h"
+
+namespace gw {
+
+__device__ __forceinline__ uint32_t walker_source(const WalkerInit &in, uint32_t wid)
+{
+    if (in.mode == GW_INIT_PER_VERTEX) return wid / in.wps;
+    if (in.mode == GW_INIT_SINGLE_SOURCE) {
+        if (in.algo == GW_SOSR) return wid < in.numwalks / 2 ? 1u : 3u;
+        return 1u;
+    }
+    const U4 r = philox4x32_10(wid, 0xFFFFFFFFu, 0u, kTagInit, in.key0, in.key1);
+    return r.x % in.nverts;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+    return v;
+}
+
+template <bool SOPR, bool PATHS>
+__global__ void __launch_bounds__(kWalkThreads) k_walk_incore(const IncoreArgs a)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint64_t *__restrict__ beg = a.beg;
+    const uint32_t *__restrict__ csr = a.csr;
+    const uint32_t maxhops = a.c.maxhops;
+
+    uint32_t q_next = 0, q_end = 0;  // warp-uniform claimed range
+    bool exhausted = false;          // warp-uniform
+    bool active = false;
+
+    uint32_t wid = 0, prev = 0, cur = 0, hop = 0, attempt = 0;
+    uint32_t deg = 0, pdeg = 0;
+    uint64_t head = 0, phead = 0, h = 0;
+    U4 r{0, 0, 0, 0};
+    StepThr t{};
+    uint32_t *prow = nullptr;
+    unsigned long long n_steps = 0, n_trials = 0, n_done = 0, hsum = 0;
+
+    auto finish = [&]() {
+        a.hashes[wid] = h;
+        a.lens[wid] = hop + 1;
+        hsum += h;
+        n_done++;
+        active = false;
+    };
+
+    for (;;) {
+        // Hand walkers to idle lanes.
+        for (;;) {
+            const unsigned need = __ballot_sync(0xFFFFFFFFu, !active);
+            if (need == 0 || exhausted) break;
+            if (q_next >= q_end) {
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(&a.ctr[kCtrCursor], (unsigned long long)kChunk);
+                base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                if (base >= a.nwalkers) {
+                    exhausted = true;
+                    break;
+                }
+                q_next = (uint32_t)base;
+                q_end = (uint32_t)min(base + kChunk, (unsigned long long)a.nwalkers);
+            }
+            const uint32_t avail = q_end - q_next;
+            const uint32_t rank = __popc(need & lt_mask);
+            if (!active && rank < avail) {
+                wid = q_next + rank;
+                const uint32_t src = walker_source(a.init, wid);
+                prev = cur = src;
+                hop = 0;
+                h = hash_init(src);
+                if (PATHS) {
+                    prow = a.paths + (uint64_t)wid * a.stride;
+                    prow[0] = src;
+                }
+                if (src >= a.nverts) {
+                    atomicOr(a.err, kErrSource);
+                    finish();
+                } else if (maxhops == 0) {
+                    finish();
+                } else {
+                    head = __ldg(beg + src);
+                    deg = (uint32_t)(__ldg(beg + src + 1) - head);
+                    if (deg == 0) {
+                        finish();  // dead end (engine/engine.hpp:196-199)
+                    } else {
+                        phead = head;
+                        pdeg = deg;
+                        t = step_thresholds<SOPR>(a.c, deg, pdeg);
+                        r = draw(a.c, wid, 0, 0);
+                        attempt = 1;
+                        active = true;
+                    }
+                }
+            }
+            q_next += min((uint32_t)__popc(need), avail);
+        }
+        if (!__any_sync(0xFFFFFFFFu, active)) break;
+        if (!active) continue;
+
+        // One rejection-sampling trial.
+        const uint32_t pos = r.x % deg;
+        const float rv = rand_val(r.y, t.maxv);
+        const uint32_t x = __ldg(csr + head + pos);
+        n_trials++;
+        if (accept_candidate<SOPR>(t, rv, x, prev, cur, csr + phead, pdeg)) {
+            hop++;
+            n_steps++;
+            h = hash_step(h, x);
+            if (PATHS) prow[hop] = x;
+            prev = cur;
+            phead = head;
+            pdeg = deg;
+            cur = x;
+            if (hop >= maxhops) {
+                finish();
+            } else if (x >= a.nverts) {
+                atomicOr(a.err, kErrVertexRange);
+                finish();
+            } else if (a.c.term_prob > 0.0f) {
+                r = draw(a.c, wid, hop, 0);
+                attempt = 1;
+                if (terminates(a.c, r.z)) {
+                    finish();
+                } else {
+                    head = __ldg(beg + x);
+                    deg = (uint32_t)(__ldg(beg + x + 1) - head);
+                    if (deg == 0) finish();
+                    else t = step_thresholds<SOPR>(a.c, deg, pdeg);
+                }
+            } else {
+                head = __ldg(beg + x);
+                const uint64_t tail = __ldg(beg + x + 1);
+                r = draw(a.c, wid, hop, 0);
+                attempt = 1;
+                deg = (uint32_t)(tail - head);
+                if (deg == 0) finish();
+                else t = step_thresholds<SOPR>(a.c, deg, pdeg);
+            }
+        } else if (attempt >= kMaxAttempts) {
+            atomicOr(a.err, kErrTrials);
+            finish();
+        } else {
+            r = draw(a.c, wid, hop, attempt);
+            attempt++;
+        }
+    }
+
+    n_steps = warp_sum(n_steps);
+    n_trials = warp_sum(n_trials);
+    n_done = warp_sum(n_done);
+    hsum = warp_sum(hsum);
+    if (lane == 0) {
+        atomicAdd(&a.ctr[kCtrSteps], n_steps);
+        atomicAdd(&a.ctr[kCtrTrials], n_trials);
+        atomicAdd(&a.ctr[kCtrDone], n_done);
+        atomicAdd(&a.ctr[kCtrHashSum], hsum);
+    }
+}
+
+// Memory-safety check of a resident CSR before any walk reads it: offsets
+// non-decreasing and within [0, nedges], every neighbour id < nverts.
+// (Adjacency order is a precondition -- the reference's `sorted` option --
+// and affects results, not safety.)
+__global__ void k_validate_csr(const uint64_t *__restrict__ beg, const uint32_t *__restrict__ csr,
+                               uint32_t nverts, uint64_t nedges, uint32_t *err)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool bad = false;
+    for (uint64_t v = t0; v < nverts; v += stride) {
+        const uint64_t a = beg[v], b = beg[v + 1];
+        bad |= (a > b) | (b > nedges);
+    }
+    for (uint64_t i = t0; i < nedges; i += stride) bad |= csr[i] >= nverts;
+    if (__any_sync(0xFFFFFFFFu, bad) && (threadIdx.x & 31u) == 0) atomicOr(err, kErrVertexRange);
+}
+
+cudaError_t launch_validate_csr(const uint64_t *beg, const uint32_t *csr, uint32_t nverts, uint64_t nedges,
+                                uint32_t *err, int num_sms, cudaStream_t s)
+{
+    k_validate_csr<<<num_sms * 8, 256, 0, s>>>(beg, csr, nverts, nedges, err);
+    return cudaGetLastError();
+}
+
+template <bool SOPR, bool PATHS>
+static int grid_for(int num_sms)
+{
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_incore<SOPR, PATHS>, kWalkThreads, 0);
+    if (per_sm < 1) per_sm = 1;
+    return per_sm * num_sms;
+}
+
+int incore_grid(bool sopr, bool paths, int num_sms)
+{
+    if (sopr) return paths ? grid_for<true, true>(num_sms) : grid_for<true, false>(num_sms);
+    return paths ? grid_for<false, true>(num_sms) : grid_for<false, false>(num_sms);
+}
+
+cudaError_t launch_walk_incore(const IncoreArgs &a, bool sopr, int grid, cudaStream_t s)
+{
+    const bool paths = a.paths != nullptr;
+    if (sopr) {
+        if (paths) k_walk_incore<true, true><<<grid, kWalkThreads, 0, s>>>(a);
+        else k_walk_incore<true, false><<<grid, kWalkThreads, 0, s>>>(a);
+    } else {
+        if (paths) k_walk_incore<false, true><<<grid, kWalkThreads, 0, s>>>(a);
+        else k_walk_incore<false, false><<<grid, kWalkThreads, 0, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace gw

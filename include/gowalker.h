@@ -1,0 +1,215 @@
+/*
+ * gowalker.h -- C ABI of the B200 walk engine (libgowalker.so).
+ *
+ * The engine is a drop-in for the walk path of GOWalker: the Node2vec / SOPR /
+ * SOSR second-order random-walk step, walker bucketing by (prev block, cur
+ * block), the device block cache fed from pinned host memory, and block
+ * choice.  GOWalker itself has no binary interface (each app is one nvcc
+ * translation unit); every entry point below names the reference call site it
+ * stands in for, as file:line inside the GOWalker sources.
+ *
+ * Conventions
+ *   - Every call returns int status: GW_OK (0) or a negative GW_ERR_*; no call
+ *     exits the process (the reference's checkCudaError calls exit(),
+ *     api/types.hpp:28-35).  gw_last_error() gives the message of the last
+ *     failure on a handle.
+ *   - Plain pointers and sizes only.  Host buffers passed to gw_host_block are
+ *     borrowed for the life of the handle (the reference keeps every block in
+ *     pinned host memory, engine/engine.hpp:74-77); pin them (cudaHostAlloc or
+ *     cudaHostRegister) for full copy bandwidth.
+ *   - One host thread per handle.  The handle owns its device memory and its
+ *     CUDA streams.
+ *   - Walks are bit-identical to the reference CPU step rule
+ *     (engine/engine.hpp:158-404) driven by a Philox4x32-10 stream keyed by
+ *     (seed, walker id, hop, attempt), whatever the block schedule, cache size
+ *     or launch shape.
+ */
+#ifndef GOWALKER_H
+#define GOWALKER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GW_ABI_VERSION 1
+
+/* status codes */
+#define GW_OK 0
+#define GW_ERR_ARG (-1)      /* bad argument or configuration */
+#define GW_ERR_CUDA (-2)     /* a CUDA runtime call failed */
+#define GW_ERR_NOMEM (-3)    /* device or pinned allocation refused */
+#define GW_ERR_STATE (-4)    /* call out of order (e.g. run before graph) */
+#define GW_ERR_TIMEOUT (-5)  /* a bounded device wait gave up */
+#define GW_ERR_DEVICE (-6)   /* a kernel reported an error word */
+#define GW_ERR_GRAPH (-7)    /* graph data failed validation */
+
+/* algorithms, in AlgorithmType order (api/types.hpp:27) */
+#define GW_NODE2VEC 0u
+#define GW_SOPR 1u
+#define GW_SOSR 2u
+
+/* walker initialisation */
+#define GW_INIT_PER_VERTEX 0u    /* walkpersource walkers per vertex, id = v*wps+i
+                                    (engine/walk.hpp:32-49) */
+#define GW_INIT_SINGLE_SOURCE 1u /* SOPR: all at vertex 1; SOSR: first half at 1,
+                                    rest at 3 (engine/walk.hpp:275-293, 355-384) */
+#define GW_INIT_RANDOM 2u        /* numwalks walkers at Philox-drawn vertices
+                                    (stands in for engine/walk.hpp:64-80) */
+
+/* block-choice policies */
+#define GW_POLICY_PLAIN 0u   /* GOwalker_scheduler_t::max_choose_blocks
+                                (engine/schedule.hpp:70-138) on the device */
+#define GW_POLICY_LEARNED 1u /* MLP demand predictor, plain policy as fallback */
+
+/* path recording */
+#define GW_PATHS_NONE 0u   /* per-walker hash and length only */
+#define GW_PATHS_FULL 1u   /* every vertex, walker-major rows of maxhops+1 */
+
+typedef struct gw_handle gw_handle;
+
+/* Run parameters.  The fields that have a graph_config counterpart
+ * (engine/config.hpp:7-34) keep its meaning and default (apps/Node2vec.cu:35-59). */
+typedef struct gw_config {
+    uint64_t cache_size;      /* device block-cache bytes ("memory", GB on the CLI) */
+    uint64_t blocksize;       /* bytes per block ("blocksize", MB on the CLI) */
+    uint32_t algorithm;       /* GW_NODE2VEC / GW_SOPR / GW_SOSR */
+    float p, q;               /* Node2vec return / in-out parameters */
+    float alpha;              /* SOPR/SOSR restart weight */
+    uint32_t maxhops;         /* walk length ("length") */
+    uint32_t walkpersource;   /* walkers per vertex */
+    uint32_t numwalks;        /* total walkers for SINGLE_SOURCE / RANDOM init */
+    uint32_t blockpergrid;    /* 0 = chosen by the autotuner */
+    uint32_t threadperblock;  /* 0 = chosen by the autotuner */
+    uint32_t zero_threshold;  /* walkers a block must attract to be loaded */
+    uint32_t zero_copy;       /* 1: finish stragglers reading mapped host CSR */
+    uint32_t init_mode;       /* GW_INIT_* */
+    float term_prob;          /* geometric termination per step at hop >= 1 (0 = off) */
+    uint64_t seed;            /* Philox key of the walk stream */
+    uint32_t record_paths;    /* GW_PATHS_* */
+    int32_t device;           /* CUDA device ordinal */
+    uint32_t reserved[8];
+} gw_config;
+
+/* Per-run counters. */
+typedef struct gw_stats {
+    uint64_t steps;           /* real moves taken by all walkers */
+    uint64_t trials;          /* rejection-sampling attempts */
+    uint64_t walkers;         /* walkers finished */
+    uint64_t h2d_bytes;       /* host->device bytes (blocks + walker records) */
+    uint64_t d2h_bytes;       /* device->host bytes */
+    uint64_t block_loads;     /* block copies into cache slots */
+    uint64_t zero_copy_steps; /* steps taken in the mapped-host tail mode */
+    uint32_t iterations;      /* scheduler iterations */
+    uint32_t launches;        /* kernels launched by this run */
+    float kernel_ms;          /* time inside the step kernels (CUDA events) */
+    float total_ms;           /* whole run (CUDA events) */
+    uint32_t reserved[8];
+} gw_stats;
+
+/* ------------------------------------------------------------------ basics */
+
+int gw_version(void);
+const char *gw_status_string(int status);
+
+/* Defaults of apps/Node2vec.cu:35-59 (p 0.5, q 2.0, alpha 0.2, length 30,
+ * blocksize 1024 MB, memory 4 GB, walkpersource 1). */
+int gw_config_default(gw_config *cfg);
+
+/* Replaces the graph_engine constructor's device set-up
+ * (engine/engine.hpp:54-102: initgpugraph, initgpucache, cudarand, initwalk). */
+int gw_create(const gw_config *cfg, gw_handle **out);
+
+/* Frees everything the handle owns (the reference never frees its device
+ * state: gpu/memory.hpp:179-207 are never called). */
+int gw_destroy(gw_handle *h);
+
+int gw_last_error(gw_handle *h, char *buf, size_t n);
+
+/* Update p, q, alpha, length, seed, termination or path mode between runs. */
+int gw_set_config(gw_handle *h, const gw_config *cfg);
+
+/* The handle's compute stream (a cudaStream_t), on which every step kernel
+ * is launched; callers may record their own CUDA events on it.  The three
+ * streams of the reference (gpu_stream, api/types.hpp:174-187) become one
+ * compute stream and one copy stream. */
+int gw_stream(gw_handle *h, void **stream);
+
+/* ------------------------------------------------------------------ graph */
+
+/* Block table: graph_block (engine/cache.hpp:150-175) from the .vert.blocks /
+ * .edge.blocks files (vblocks: nblocks+1 u32, eblocks: nblocks+1 u64). */
+int gw_set_graph_meta(gw_handle *h, uint32_t nverts, uint64_t nedges, uint32_t nblocks,
+                      const uint32_t *vblocks, const uint64_t *eblocks);
+
+/* Host copy of block blk: beg = its nverts+1 u64 offsets as stored in the
+ * .beg file (absolute), csr = its nedges u32 neighbours.  Stands in for
+ * graph_driver::load_block_info_all (engine/driver.hpp:71-90); the engine
+ * copies from these buffers into device slots (gpu/memory.hpp:124-139). */
+int gw_host_block(gw_handle *h, uint32_t blk, const uint64_t *beg, const uint32_t *csr);
+
+/* Whole graph already resident on this device (d_beg: nverts+1, d_csr:
+ * nedges), borrowed.  The engine then runs in-core without host copies. */
+int gw_device_graph(gw_handle *h, const uint64_t *d_beg, const uint32_t *d_csr);
+
+/* Drop every cached block so the next run copies the graph from the host
+ * blocks again. */
+int gw_cache_reset(gw_handle *h);
+
+/* ------------------------------------------------------------------ walks */
+
+/* Replaces graph_walk::gpu_createwalk (engine/walk.hpp:272-389): sets the
+ * walker population; walkers are generated on the device. */
+int gw_init_walkers(gw_handle *h, uint32_t algo, uint32_t walkpersource, uint64_t seed);
+
+/* Runs every walker to the end.  Replaces graph_engine::pipe_run
+ * (engine/engine.hpp:517-638) with its pipeline / zero_gpujob launches
+ * (406-515): the plain or learned block policy, device bucketing, and the
+ * step kernels of gpu/gpuwalk.hpp. */
+int gw_run(gw_handle *h, uint32_t policy, gw_stats *stats);
+
+/* Walker count of the current population. */
+int gw_num_walkers(gw_handle *h, uint64_t *n);
+
+/* Paths of walkers [first, first+n): out = n rows of maxhops+1 u32 (zero
+ * padded), lens = vertices per row.  Needs record_paths = GW_PATHS_FULL. */
+int gw_get_paths(gw_handle *h, uint64_t first, uint64_t n, uint32_t *out, uint32_t *lens);
+
+/* 64-bit FNV-1a hash of each walker's path over its 32-bit vertex ids. */
+int gw_path_hashes(gw_handle *h, uint64_t first, uint64_t n, uint64_t *out);
+
+/* Hash of all path hashes (order-independent sum) and total steps, read back
+ * as 16 bytes: the per-run checksum. */
+int gw_checksum(gw_handle *h, uint64_t *hash_sum, uint64_t *steps);
+
+/* Walker counts of the nblocks*nblocks (prev block, cur block) buckets after
+ * the last scheduler iteration (walk_block::num, engine/walk.hpp:104-209). */
+int gw_bucket_counts(gw_handle *h, uint32_t *out);
+
+/* ------------------------------------------------------------------ graphs on the device */
+
+/* Counter-based R-MAT graph built on the device: samples e in [0, nsamples)
+ * take `scale` quadrant choices from Philox(e, level/4) against the u32
+ * thresholds thr = {a, a+b, a+b+c} * 2^32.  Samples with an endpoint >=
+ * nverts are rejected, self loops dropped, the edge set symmetrised when
+ * `symmetric`, duplicates removed, adjacency sorted.  When target_edges is
+ * non-zero the sorted unique edge list is thinned evenly to exactly that
+ * many edges.  Allocates *d_beg (nverts+1 u64) and *d_csr (nedges u32) with
+ * cudaMalloc on the current device; free them with gw_device_free. */
+int gw_rmat_csr(uint32_t scale, uint32_t nverts, uint64_t nsamples, const uint32_t thr[3], uint64_t seed,
+                int symmetric, uint64_t target_edges, uint64_t **d_beg, uint32_t **d_csr, uint64_t *nedges);
+
+int gw_device_free(void *p);
+
+/* Plain copy between any two host / device pointers (cudaMemcpyDefault),
+ * synchronous: lets callers without their own CUDA runtime move the buffers
+ * gw_rmat_csr returns. */
+int gw_memcpy(void *dst, const void *src, uint64_t bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GOWALKER_H */

@@ -1,0 +1,212 @@
+"""GPU parity tests: the CUDA walk path (through the C ABI) against the oracle.
+
+Bit-exact: paths, lengths and 64-bit path hashes are integer data, so every
+comparison is equality.
+"""
+import ctypes
+import glob
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def run_engine(gw, beg, csr, algo, maxhops, wps=1, p=0.5, q=2.0, alpha=0.2, term=0.0, seed=42, paths=True,
+               init_mode=0, numwalks=0, blocks=None, **cfg):
+    eng = gw.WalkEngine(algorithm=algo, maxhops=maxhops, p=p, q=q, alpha=alpha, term_prob=term, seed=seed,
+                        walkpersource=wps, record_paths=1 if paths else 0, init_mode=init_mode,
+                        numwalks=numwalks, cache_size=1 << 34, **cfg)
+    vb, eb = (None, None) if blocks is None else blocks
+    eng.set_host_graph(beg, csr, vb, eb)
+    eng.init_walkers(algo, wps, seed)
+    st = eng.run()
+    return eng, st
+
+
+def oracle_cfg(O, algo, maxhops, wps=1, p=0.5, q=2.0, alpha=0.2, term=0.0, seed=42, init_mode=0, numwalks=0):
+    return O.make_cfg(algo=algo, maxhops=maxhops, p=p, q=q, alpha=alpha, term_prob=term, seed=seed, wps=wps,
+                      init_mode=init_mode, numwalks=numwalks)
+
+
+def test_device_philox_matches_curand_and_oracle(oracle, tmp_path):
+    so = tmp_path / "probe.so"
+    subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-shared", "-Xcompiler", "-fPIC",
+                    "-I", os.path.join(ROOT, "gowalker_b200", "csrc"), "-o", str(so),
+                    os.path.join(ROOT, "tests", "cuda", "philox_curand.cu")], check=True)
+    L = ctypes.CDLL(str(so))
+    n = 4096
+    ours = np.zeros((n, 8), dtype=np.uint32)
+    theirs = np.zeros((n, 8), dtype=np.uint32)
+    seed, sub0 = 0x0123456789ABCDEF, (1 << 32) - 100
+    assert L.probe_philox(ctypes.c_uint64(seed), ctypes.c_uint64(sub0), n, ours.ctypes.data_as(ctypes.c_void_p),
+                          theirs.ctypes.data_as(ctypes.c_void_p)) == 0
+    assert np.array_equal(ours, theirs)
+    key = [seed & 0xFFFFFFFF, seed >> 32]
+    for i in range(0, n, 257):
+        sub = sub0 + i
+        assert np.array_equal(oracle.philox([0, 0, sub & 0xFFFFFFFF, sub >> 32], key), ours[i, :4])
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*_s8.npz"))))
+def test_golden_fixtures(gw, path):
+    z = np.load(path)
+    eng, st = run_engine(gw, z["beg"], z["csr"], int(z["algo"]), int(z["maxhops"]), wps=int(z["wps"]),
+                         p=float(z["p"]), q=float(z["q"]), alpha=float(z["alpha"]), seed=int(z["seed"]))
+    P, L = eng.paths()
+    assert np.array_equal(L, z["lens"])
+    assert np.array_equal(P, z["paths"])
+    assert np.array_equal(eng.hashes(), z["hashes"])
+    assert st["steps"] == int(z["steps"])
+    eng.close()
+
+
+SWEEP = [
+    # algo, scale, ef, symmetric, maxhops, wps, p, q, alpha, term
+    (0, 11, 16, True, 40, 1, 2.0, 0.5, 0.2, 0.0),
+    (0, 11, 16, True, 25, 2, 0.25, 4.0, 0.2, 0.0),
+    (0, 11, 8, False, 30, 1, 1.0, 1.0, 0.2, 0.0),
+    (1, 11, 16, True, 20, 4, 0.5, 2.0, 0.2, 0.15),
+    (2, 10, 16, False, 20, 2, 0.5, 2.0, 0.35, 0.15),
+    (1, 12, 4, True, 12, 1, 0.5, 2.0, 0.9, 0.0),
+]
+
+
+@pytest.mark.parametrize("case", SWEEP)
+def test_sweep_vs_oracle(gw, oracle, case):
+    algo, scale, ef, sym, maxhops, wps, p, q, alpha, term = case
+    beg, csr = oracle.rmat_graph(scale, ef, seed=5, symmetric=sym)
+    V = len(beg) - 1
+    eng, st = run_engine(gw, beg, csr, algo, maxhops, wps, p, q, alpha, term, seed=1234)
+    cfg = oracle_cfg(oracle, algo, maxhops, wps, p, q, alpha, term, seed=1234)
+    ref = oracle.walk(beg, csr, cfg, 0, V * wps, paths=True)
+    P, L = eng.paths()
+    assert np.array_equal(L, ref["lens"])
+    assert np.array_equal(P, ref["paths"])
+    assert np.array_equal(eng.hashes(), ref["hashes"])
+    assert st["steps"] == ref["stats"]["steps"]
+    assert st["trials"] == ref["stats"]["trials"]
+    hs, steps = eng.checksum()
+    assert hs == int(ref["hashes"].astype(np.uint64).sum(dtype=np.uint64))
+    eng.close()
+
+
+@pytest.mark.parametrize("algo,init_mode", [(1, 1), (2, 1), (0, 2)])
+def test_init_modes_vs_oracle(gw, oracle, algo, init_mode):
+    beg, csr = oracle.rmat_graph(10, 16, seed=9)
+    n = 3000
+    eng, st = run_engine(gw, beg, csr, algo, 20, wps=1, term=0.15 if algo else 0.0, seed=77, init_mode=init_mode,
+                         numwalks=n)
+    cfg = oracle_cfg(oracle, algo, 20, 1, term=0.15 if algo else 0.0, seed=77, init_mode=init_mode, numwalks=n)
+    ref = oracle.walk(beg, csr, cfg, 0, n, paths=True)
+    P, L = eng.paths()
+    assert np.array_equal(P, ref["paths"])
+    assert np.array_equal(eng.hashes(), ref["hashes"])
+    eng.close()
+
+
+def test_launch_shape_and_graph_mode_invariance(gw, oracle):
+    beg, csr = oracle.rmat_graph(12, 16, seed=2)
+    V = len(beg) - 1
+    base = None
+    for grid in (0, 1, 7, 333):
+        eng, _ = run_engine(gw, beg, csr, 0, 30, 1, 2.0, 0.5, paths=False, blockpergrid=grid)
+        h = eng.hashes()
+        eng.close()
+        base = h if base is None else base
+        assert np.array_equal(h, base)
+    # device-resident graph gives the same walks as host blocks
+    dg = gw.DeviceGraph(12, edgefactor=16, seed=2)
+    b2, c2 = dg.to_host()
+    assert np.array_equal(b2, beg) and np.array_equal(c2, csr)
+    eng = gw.WalkEngine(algorithm=0, maxhops=30, p=2.0, q=0.5, seed=42, record_paths=0)
+    eng.set_device_graph(dg.nverts, dg.nedges, dg.beg_ptr, dg.csr_ptr)
+    eng.init_walkers(0, 1, 42)
+    eng.run()
+    assert np.array_equal(eng.hashes(), base)
+    eng.close()
+    dg.free()
+
+
+def test_multiblock_host_graph_incore(gw, oracle):
+    """Blocks that all fit the cache are assembled into one resident CSR."""
+    beg, csr = oracle.rmat_graph(11, 16, seed=4)
+    vb, eb = oracle.split_equal_edge_mass(beg, 5)
+    V = len(beg) - 1
+    eng, st = run_engine(gw, beg, csr, 0, 20, 1, 2.0, 0.5, blocks=(vb, eb))
+    ref = oracle.walk(beg, csr, oracle_cfg(oracle, 0, 20, 1, 2.0, 0.5), 0, V, paths=False)
+    assert np.array_equal(eng.hashes(), ref["hashes"])
+    assert st["h2d_bytes"] == (V + 1) * 8 + len(csr) * 4
+    eng.close()
+
+
+@pytest.mark.parametrize("sym,cap,target", [(True, None, 0), (False, 3000, 0), (True, None, 50000)])
+def test_device_rmat_matches_oracle(gw, oracle, sym, cap, target):
+    scale = 12
+    V = (1 << scale) if cap is None else cap
+    n = 16 << scale
+    src, dst = oracle.rmat_edges(scale, 0, n, seed=3)
+    keep = (src < V) & (dst < V)
+    beg, csr = oracle.build_csr(V, src[keep], dst[keep], symmetric=sym)
+    if target:
+        keys = (np.repeat(np.arange(V, dtype=np.uint64), np.diff(beg.astype(np.int64))) << np.uint64(32)) | csr
+        U, k = len(keys), len(keys) - target
+        i = np.arange(U, dtype=np.uint64)
+        keep_i = (i * np.uint64(k)) // np.uint64(U) == ((i + np.uint64(1)) * np.uint64(k)) // np.uint64(U)
+        keys = keys[keep_i]
+        s = (keys >> np.uint64(32)).astype(np.int64)
+        csr = (keys & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+        beg = np.zeros(V + 1, dtype=np.uint64)
+        beg[1:] = np.cumsum(np.bincount(s, minlength=V))
+    dg = gw.DeviceGraph(scale, nverts=V, nsamples=n, seed=3, symmetric=sym, target_edges=target)
+    b2, c2 = dg.to_host()
+    dg.free()
+    assert np.array_equal(b2, beg)
+    assert np.array_equal(c2, csr)
+
+
+def test_corrupt_graph_is_rejected(gw, oracle):
+    beg, csr = oracle.rmat_graph(9, 8, seed=1)
+    bad = csr.copy()
+    bad[len(bad) // 2] = len(beg) + 5  # neighbour id beyond nverts
+    eng = gw.WalkEngine(algorithm=0, maxhops=10, cache_size=1 << 30)
+    eng.set_host_graph(beg, bad)
+    eng.init_walkers(0, 1, 1)
+    with pytest.raises(gw.GwError) as e:
+        eng.run()
+    assert e.value.status == -7
+    # the handle stays usable with a good graph
+    eng.set_host_graph(beg, csr)
+    eng.init_walkers(0, 1, 1)
+    eng.run()
+    eng.close()
+
+
+def test_c1_node2vec_sample_vs_oracle(gw, oracle):
+    """Scale-20 R-MAT, Node2vec p=2 q=0.5 length 80 (the in-core C1 workload):
+    full GPU run, first 20k walkers and a strided sample checked against the oracle."""
+    dg = gw.DeviceGraph(20, edgefactor=16, seed=1)
+    beg, csr = dg.to_host()
+    V = dg.nverts
+    eng = gw.WalkEngine(algorithm=0, maxhops=80, p=2.0, q=0.5, seed=42, record_paths=0)
+    eng.set_device_graph(dg.nverts, dg.nedges, dg.beg_ptr, dg.csr_ptr)
+    eng.init_walkers(0, 1, 42)
+    st = eng.run()
+    H = eng.hashes()
+    cfg = oracle_cfg(oracle, 0, 80, 1, 2.0, 0.5, seed=42)
+    ref = oracle.walk(beg, csr, cfg, 0, 20000, paths=False)
+    assert np.array_equal(H[:20000], ref["hashes"])
+    for w0 in range(20000, V, 97531):
+        r = oracle.walk(beg, csr, cfg, w0, 64, paths=False)
+        assert np.array_equal(H[w0:w0 + 64], r["hashes"])
+    assert st["walkers"] == V
+    hs, _ = eng.checksum()
+    assert hs == int(H.sum(dtype=np.uint64))
+    eng.close()
+    dg.free()

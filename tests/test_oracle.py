@@ -1,0 +1,131 @@
+"""CPU tests of the oracle: golden fixtures, reference harness, properties."""
+import glob
+import multiprocessing as mp
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def _cfg_from(O, z, **kw):
+    return O.make_cfg(algo=int(z["algo"]), maxhops=int(z["maxhops"]), p=float(z["p"]), q=float(z["q"]),
+                      alpha=float(z["alpha"]), seed=int(z["seed"]), wps=int(z["wps"]), **kw)
+
+
+def test_philox_fixture(oracle):
+    z = np.load(os.path.join(GOLDEN, "philox.npz"))
+    for c, k, o in zip(z["ctrs"], z["keys"], z["outs"]):
+        assert np.array_equal(oracle.philox(c, k), o)
+
+
+def test_philox_lanes_uniform(oracle):
+    """Chi-square of the top byte of 40k Philox draws (each lane)."""
+    outs = np.stack([oracle.philox([i, 7, 0, 0], [42, 0]) for i in range(10000)])
+    for lane in range(4):
+        hist = np.bincount(outs[:, lane] >> 24, minlength=256)
+        exp = len(outs) / 256.0
+        chi2 = float(((hist - exp) ** 2 / exp).sum())
+        assert chi2 < 340.0, (lane, chi2)  # 255 dof, p ~ 3e-4
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*_s8.npz"))))
+def test_golden_walks(oracle, path):
+    z = np.load(path)
+    cfg = _cfg_from(oracle, z)
+    n = len(z["hashes"])
+    r = oracle.walk(z["beg"], z["csr"], cfg, 0, n, paths=True)
+    assert np.array_equal(r["hashes"], z["hashes"])
+    assert np.array_equal(r["lens"], z["lens"])
+    assert np.array_equal(r["paths"], z["paths"])
+    assert r["stats"]["steps"] == int(z["steps"])
+
+
+def test_paths_follow_edges(oracle):
+    beg, csr = oracle.rmat_graph(10, 8, seed=3)
+    cfg = oracle.make_cfg(algo=oracle.ALG_NODE2VEC, maxhops=30, p=2.0, q=0.5, seed=7)
+    V = len(beg) - 1
+    r = oracle.walk(beg, csr, cfg, 0, V, paths=True)
+    for w in range(0, V, 37):
+        L = int(r["lens"][w])
+        p = r["paths"][w, :L]
+        assert p[0] == w
+        for a, b in zip(p[:-1], p[1:]):
+            adj = csr[int(beg[a]):int(beg[a + 1])]
+            assert b in adj
+        assert oracle.path_hash(p) == int(r["hashes"][w])
+
+
+def test_termination_length_distribution(oracle):
+    """SOPR with termination 0.15, max 20: mean length ~ (1-0.85^20)/0.15."""
+    beg, csr = oracle.rmat_graph(11, 16, seed=1)
+    V = len(beg) - 1
+    cfg = oracle.make_cfg(algo=oracle.ALG_SOPR, maxhops=20, alpha=0.2, term_prob=0.15, seed=42, wps=4)
+    r = oracle.walk(beg, csr, cfg, 0, 4 * V, paths=False)
+    deg = np.diff(beg.astype(np.int64))
+    live = np.repeat(deg > 0, 4)
+    mean = (r["lens"][live].astype(np.float64) - 1).mean()
+    expect = (1 - 0.85 ** 20) / 0.15
+    assert abs(mean - expect) < 0.08, mean
+
+
+def test_dead_end_rule(oracle):
+    """A walker reaching a vertex without out-edges stops there
+    (engine/engine.hpp:196-199: hop = maxhop-1, next vertex 0)."""
+    beg = np.array([0, 1, 2, 2], dtype=np.uint64)   # 0->1, 1->2, 2 has no out-edge
+    csr = np.array([1, 2], dtype=np.uint32)
+    cfg = oracle.make_cfg(algo=oracle.ALG_NODE2VEC, maxhops=10, p=1.0, q=1.0, seed=1)
+    r = oracle.walk(beg, csr, cfg, 0, 3, paths=True, finals=True)
+    assert list(r["paths"][0, :r["lens"][0]]) == [0, 1, 2]
+    assert list(r["finals"][0]) == [2, 0, 10]
+    assert r["lens"][2] == 1 and list(r["finals"][2]) == [2, 0, 10]
+    assert r["stats"]["dead_ends"] == 3
+
+
+def test_single_source_init(oracle):
+    cfg = oracle.make_cfg(algo=oracle.ALG_SOSR, init_mode=oracle.INIT_SINGLE_SOURCE, numwalks=10)
+    L = oracle.lib()
+    srcs = [L.oracle_walker_source(cfg, 100, w) for w in range(10)]
+    assert srcs == [1] * 5 + [3] * 5
+
+
+def test_block_splitters(oracle):
+    beg, csr = oracle.rmat_graph(12, 16, seed=1)
+    vb, eb = oracle.split_equal_edge_mass(beg, 8)
+    assert len(vb) == 9 and vb[0] == 0 and vb[-1] == len(beg) - 1
+    assert np.all(np.diff(vb.astype(np.int64)) > 0)
+    assert np.array_equal(eb, beg[vb.astype(np.int64)])
+    mass = np.diff(eb.astype(np.int64))
+    assert mass.max() < 2.5 * mass.mean()
+    vr, er = oracle.split_blocks_reference(beg, 64 * 1024)
+    assert vr[0] == 0 and vr[-1] == len(beg) - 1
+    assert np.all(np.diff(er.astype(np.int64)[:-1]) <= 64 * 1024 // 4)
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_step.so")),
+                    reason="reference harness not built (needs the GOWalker sources)")
+@pytest.mark.parametrize("algo", [0, 1])
+def test_reference_harness_matches_oracle(oracle, tmp_path, algo):
+    """The reference's own CPU step, fed the same Philox stream, takes the same
+    trials as the oracle (directed graph: dead ends included)."""
+    V = 150
+    src, dst = oracle.rmat_edges(8, 0, 6 << 8, seed=11)
+    keep = (src < V) & (dst < V)
+    beg, csr = oracle.build_csr(V, src[keep], dst[keep], symmetric=False)
+    beg2, csr2, vb, eb = oracle.harness_graph(beg, csr)
+    base = str(tmp_path / "g")
+    oracle.write_dataset(base, beg2, csr2)
+    oracle.write_blocks(base, 1, vb, eb)
+    starts = [(v, V + v, v, 0, V + v, v) for v in range(V)]
+    with mp.get_context("spawn").Pool(1) as pool:
+        _, res = pool.apply(oracle.ref_scenario, (base, algo, 0.7, 1.9, 0.25, 12, 1, 99, starts))
+    cfg = oracle.make_cfg(algo=algo, maxhops=12, p=0.7, q=1.9, alpha=0.25, seed=99, keying=oracle.KEY_TRIAL)
+    for v in range(V):
+        moves, _, trace, final = oracle.walk_traced(beg, csr, cfg, v, v, v, 0)
+        run, rtrace, _, _ = res[v]
+        dead = 1 if (moves < 12 and final[1] == 0 and final[2] == 12) else 0
+        assert np.array_equal(trace, rtrace), v
+        assert run == moves + dead, v
