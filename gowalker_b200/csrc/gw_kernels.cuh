@@ -59,6 +59,26 @@ struct IncoreArgs {
     uint32_t *err;             // ErrBit word
 };
 
+// Source vertex of walker `wid` (engine/walk.hpp:32-49 per-vertex ids
+// v*wps+i; 82-95 and 355-384 single source 1, or 1 and 3 for SOSR).
+__device__ __forceinline__ uint32_t walker_source(const WalkerInit &in, uint32_t wid)
+{
+    if (in.mode == 0u) return wid / in.wps;
+    if (in.mode == 1u) {
+        if (in.algo == 2u) return wid < in.numwalks / 2 ? 1u : 3u;
+        return 1u;
+    }
+    const U4 r = philox4x32_10(wid, 0xFFFFFFFFu, 0u, kTagInit, in.key0, in.key1);
+    return r.x % in.nverts;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+    return v;
+}
+
 // Grid size (CTAs) for a persistent walk kernel on this device.
 int incore_grid(bool sopr, bool paths, int num_sms);
 cudaError_t launch_walk_incore(const IncoreArgs &a, bool sopr, int grid, cudaStream_t s);

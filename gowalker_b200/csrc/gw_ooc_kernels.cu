@@ -1,0 +1,569 @@
+// Out-of-core kernels (replace GOWalker gpu/gpuwalk.hpp:87-372 and the host
+// block choice of engine/schedule.hpp:70-138).
+//
+//  k_init_walkers  walker records from ids (engine/walk.hpp:32-95)
+//  k_count         walkers per (prev block, cur block) bucket, warp-aggregated
+//                  atomics (one atomic per distinct bucket per warp instead of
+//                  one per walker, gpu/gpuwalk.hpp:179)
+//  k_scan          exclusive scan of the nblocks^2 bucket counts in one CTA
+//                  (the reference scans them on one thread, gpu/gpuwalk.hpp:321-338)
+//  k_scatter       walkers into bucket order, finished walkers dropped
+//                  (gpu/gpuwalk.hpp:340-360 + the spill of engine/walk.hpp:484-525)
+//  k_runnable      ranges of the buckets whose two blocks are resident
+//  k_schedule      GOwalker_scheduler_t::max_choose_blocks on the device
+//  k_walk_ooc      the step kernel over runnable walkers; a walker stops when
+//                  its next vertex lies in a block that is not resident
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "gw_ooc_kernels.cuh"
+
+namespace gw {
+
+constexpr uint32_t kNoBucket = 0xFFFFFFFFu;
+
+__device__ __forceinline__ uint32_t block_of(const uint32_t *vs, uint32_t nb, uint32_t v)
+{
+    // largest b with vs[b] <= v (vs[nb] = nverts > v)
+    uint32_t lo = 0, hi = nb;  // invariant vs[lo] <= v < vs[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (vs[mid] <= v) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_init_walkers(WalkerInit in, const uint32_t *__restrict__ vstart, uint32_t nb, uint64_t n,
+                               WalkerRec *__restrict__ out, uint32_t *__restrict__ paths, uint32_t stride)
+{
+    __shared__ uint32_t s_vs[kMaxBlocks + 1];
+    for (uint32_t i = threadIdx.x; i <= nb; i += blockDim.x) s_vs[i] = vstart[i];
+    __syncthreads();
+    const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += step) {
+        const uint32_t wid = (uint32_t)i;
+        const uint32_t src = walker_source(in, wid);
+        const uint32_t b = block_of(s_vs, nb, src);
+        const uint64_t h = hash_init(src);
+        WalkerRec r;
+        r.wid = wid;
+        r.prev = src;
+        r.cur = src;
+        r.hop = 0;
+        r.prev_blk = b;
+        r.cur_blk = b;
+        r.hash_lo = (uint32_t)h;
+        r.hash_hi = (uint32_t)(h >> 32);
+        out[i] = r;
+        if (paths) paths[(uint64_t)wid * stride] = src;
+    }
+}
+
+__device__ __forceinline__ uint32_t bucket_of(const WalkerRec &r, uint32_t nb)
+{
+    return r.prev_blk == kFinished ? kNoBucket : r.prev_blk * nb + r.cur_blk;
+}
+
+__global__ void k_count(const WalkerRec *__restrict__ w, uint64_t n, uint32_t nb, uint32_t *__restrict__ counts)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull; base < n; base += step) {
+        const uint64_t i = base + lane;
+        const uint32_t b = (i < n) ? bucket_of(w[i], nb) : kNoBucket;
+        const unsigned grp = __match_any_sync(0xFFFFFFFFu, b);
+        if (b != kNoBucket && lane == (uint32_t)(__ffs(grp) - 1)) atomicAdd(&counts[b], (uint32_t)__popc(grp));
+    }
+}
+
+__global__ void k_scatter(const WalkerRec *__restrict__ in, uint64_t n, uint32_t nb,
+                          const uint32_t *__restrict__ offsets, uint32_t *__restrict__ cursor,
+                          WalkerRec *__restrict__ out)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull; base < n; base += step) {
+        const uint64_t i = base + lane;
+        WalkerRec r{};
+        uint32_t b = kNoBucket;
+        if (i < n) {
+            r = in[i];
+            b = bucket_of(r, nb);
+        }
+        const unsigned grp = __match_any_sync(0xFFFFFFFFu, b);
+        if (b != kNoBucket) {
+            const uint32_t leader = (uint32_t)(__ffs(grp) - 1);
+            uint32_t pos = 0;
+            if (lane == leader) pos = atomicAdd(&cursor[b], (uint32_t)__popc(grp));
+            pos = __shfl_sync(grp, pos, leader) + (uint32_t)__popc(grp & lt);
+            out[offsets[b] + pos] = r;
+        }
+    }
+}
+
+// One-CTA scans over at most 2^20 entries (nblocks <= 1024).
+constexpr int kScanThreads = 1024;
+
+__device__ __forceinline__ uint32_t cta_exclusive_scan(uint32_t v, uint32_t *total)
+{
+    __shared__ uint32_t s_w[32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) s_w[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = (lane < (blockDim.x >> 5)) ? s_w[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+            if (lane >= (uint32_t)o) w += y;
+        }
+        s_w[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t before = (warp > 0 ? s_w[warp - 1] : 0) + x - v;
+    if (total) *total = s_w[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return before;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan(const uint32_t *__restrict__ in, uint32_t n,
+                                                       uint32_t *__restrict__ out)
+{
+    const uint32_t per = (n + kScanThreads - 1) / kScanThreads;
+    const uint32_t lo = min(threadIdx.x * per, n), hi = min(lo + per, n);
+    uint32_t sum = 0;
+    for (uint32_t i = lo; i < hi; ++i) sum += in[i];
+    uint32_t total = 0;
+    uint32_t run = cta_exclusive_scan(sum, &total);
+    for (uint32_t i = lo; i < hi; ++i) {
+        const uint32_t c = in[i];
+        out[i] = run;
+        run += c;
+    }
+    if (threadIdx.x == 0) out[n] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_runnable(const uint32_t *__restrict__ counts,
+                                                           const uint32_t *__restrict__ offsets,
+                                                           const uint64_t *const *__restrict__ blk_beg, uint32_t nb,
+                                                           uint32_t *__restrict__ run_pre,
+                                                           uint32_t *__restrict__ run_off, uint32_t *__restrict__ nrun)
+{
+    __shared__ uint8_t s_res[kMaxBlocks];
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) s_res[i] = blk_beg[i] != nullptr;
+    __syncthreads();
+    const uint32_t n = nb * nb;
+    const uint32_t per = (n + kScanThreads - 1) / kScanThreads;
+    const uint32_t lo = min(threadIdx.x * per, n), hi = min(lo + per, n);
+    uint32_t cnt = 0, sum = 0;
+    for (uint32_t b = lo; b < hi; ++b) {
+        const uint32_t c = counts[b];
+        if (c && s_res[b / nb] && s_res[b % nb]) {
+            cnt++;
+            sum += c;
+        }
+    }
+    uint32_t tot_cnt = 0, tot_sum = 0;
+    uint32_t k = cta_exclusive_scan(cnt, &tot_cnt);
+    uint32_t run = cta_exclusive_scan(sum, &tot_sum);
+    for (uint32_t b = lo; b < hi; ++b) {
+        const uint32_t c = counts[b];
+        if (c && s_res[b / nb] && s_res[b % nb]) {
+            run_off[k] = offsets[b];
+            run_pre[k] = run;
+            run += c;
+            k++;
+        }
+    }
+    if (threadIdx.x == 0) {
+        *nrun = tot_cnt;
+        run_pre[tot_cnt] = tot_sum;
+    }
+}
+
+// Block choice, GOwalker_scheduler_t::max_choose_blocks (engine/schedule.hpp:70-138):
+//  cache not full: for every uncached block i, score = sum over cached c of
+//    walkers(i,c) + walkers(c,i), plus walkers(i,i); the best block is added.
+//  cache full: for every uncached i, s_j = walkers(i,c_j) + walkers(c_j,i);
+//    score = sum_j s_j - min_j s_j and i replaces the cached block with the
+//    smallest s_j (first such j).
+//  A block is taken only if its score is > 0 and > zero_threshold; ties go to
+//  the lowest block id (the reference's std::sort leaves their order open).
+// Rescue choice, for runs without the zero-copy tail (where the reference
+// would switch to it): the fullest bucket with an absent block; load its first
+// absent block, evicting the cached block with the fewest incident walkers
+// outside that bucket -- after at most two rescues the bucket runs, so every
+// run ends.  `pred` (optional) replaces the scores by predicted demand scaled
+// by pred_weight: the learned policy.
+__global__ void __launch_bounds__(1024) k_schedule(const uint32_t *__restrict__ counts,
+                                                   const uint32_t *__restrict__ offsets, uint32_t nb,
+                                                   const uint32_t *__restrict__ cached, uint32_t ncached,
+                                                   uint32_t nslots, uint32_t zero_threshold,
+                                                   const float *__restrict__ pred, float pred_weight,
+                                                   Decision *__restrict__ out)
+{
+    __shared__ uint8_t s_cached[kMaxBlocks];
+    __shared__ uint32_t s_list[kMaxBlocks];
+    __shared__ uint32_t s_pos[kMaxBlocks];
+    __shared__ unsigned long long s_inc[kMaxBlocks];
+    __shared__ unsigned long long s_best, s_bucket;
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) s_cached[i] = 0;
+    if (threadIdx.x == 0) {
+        s_best = 0;
+        s_bucket = 0;
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < ncached; j += blockDim.x) {
+        s_list[j] = cached[j];
+        s_cached[cached[j]] = 1;
+    }
+    __syncthreads();
+    const bool full = ncached >= nslots;
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+        uint64_t incident = 0;  // walkers in buckets touching i (row + column, diagonal once)
+        for (uint32_t c = 0; c < nb; ++c) incident += (uint64_t)counts[i * nb + c] + (c != i ? counts[c * nb + i] : 0u);
+        s_inc[i] = incident;
+        if (s_cached[i]) continue;
+        uint64_t score = 0;
+        uint32_t pos = 0;
+        if (!full) {
+            for (uint32_t j = 0; j < ncached; ++j) {
+                const uint32_t c = s_list[j];
+                score += (uint64_t)counts[i * nb + c] + counts[c * nb + i];
+            }
+            score += counts[i * nb + i];
+        } else {
+            uint64_t all = 0, mn = 0xFFFFFFFFull;
+            for (uint32_t j = 0; j < ncached; ++j) {
+                const uint32_t c = s_list[j];
+                const uint64_t v = (uint64_t)counts[i * nb + c] + counts[c * nb + i];
+                all += v;
+                if (v < mn) {
+                    mn = v;
+                    pos = j;
+                }
+            }
+            score = all - mn;
+        }
+        if (pred) score = (uint64_t)fmaxf(0.f, pred_weight * pred[i]) + (score > 0 ? 1 : 0);
+        s_pos[i] = pos;
+        atomicMax(&s_best, (score << 11) | (2047u - i));
+    }
+    // fullest bucket with an absent block
+    const uint32_t nbk = nb * nb;
+    for (uint32_t b = threadIdx.x; b < nbk; b += blockDim.x) {
+        const uint32_t c = counts[b];
+        if (c && !(s_cached[b / nb] && s_cached[b % nb]))
+            atomicMax(&s_bucket, ((unsigned long long)c << 21) | (0x1FFFFFu - b));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Decision d{};
+        const uint64_t best = s_best >> 11;
+        const int32_t bi = (int32_t)(2047u - (uint32_t)(s_best & 2047u));
+        d.score = best;
+        d.live = offsets[nbk];
+        if (s_best != 0 && best > 0 && best > zero_threshold) {
+            d.action = full ? 2 : 1;
+            d.block = bi;
+            d.position = full ? (int32_t)s_pos[bi] : (int32_t)ncached;
+        } else {
+            d.action = 0;
+            d.block = -1;
+            d.position = -1;
+        }
+        d.rescue_block = -1;
+        d.rescue_position = -1;
+        if (s_bucket) {
+            const uint32_t b = 0x1FFFFFu - (uint32_t)(s_bucket & 0x1FFFFFu);
+            const uint32_t p = b / nb, c = b % nb;
+            d.rescue_block = (int32_t)(s_cached[p] ? c : p);
+            if (full) {
+                unsigned long long mn = ~0ull;
+                for (uint32_t j = 0; j < ncached; ++j) {
+                    const uint32_t blk = s_list[j];
+                    if (blk == p || blk == c) continue;
+                    if (s_inc[blk] < mn) {
+                        mn = s_inc[blk];
+                        d.rescue_position = (int32_t)j;
+                    }
+                }
+            }
+        }
+        *out = d;
+    }
+}
+
+template <bool SOPR, bool PATHS>
+__global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const OocStepArgs a)
+{
+    __shared__ uint32_t s_vs[kMaxBlocks + 1];
+    for (uint32_t i = threadIdx.x; i <= a.nb; i += blockDim.x) s_vs[i] = a.vstart[i];
+    __syncthreads();
+
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint32_t nrun = *a.nrun;
+    const uint32_t total = a.run_pre[nrun];
+    const uint32_t maxhops = a.c.maxhops;
+
+    uint32_t q_next = 0, q_end = 0;
+    bool exhausted = false;
+    bool active = false;
+
+    uint32_t wid = 0, prev = 0, cur = 0, hop = 0, attempt = 0, pb = 0, cb = 0, deg = 0, pdeg = 0;
+    uint64_t idx = 0, head = 0, phead = 0, h = 0;
+    const uint32_t *ccsr = nullptr, *pcsr = nullptr;
+    U4 r{0, 0, 0, 0};
+    StepThr t{};
+    uint32_t *prow = nullptr;
+    unsigned long long n_steps = 0, n_trials = 0, n_done = 0, hsum = 0;
+
+    auto finish = [&]() {
+        a.hashes[wid] = h;
+        a.lens[wid] = hop + 1;
+        a.walkers[idx].prev_blk = kFinished;
+        hsum += h;
+        n_done++;
+        active = false;
+    };
+    // Enter a step at vertex cur (block cb), prev adjacency already set:
+    // termination draw, then cur's offsets (the order of the in-core kernel).
+    auto enter = [&]() {
+        r = draw(a.c, wid, hop, 0);
+        attempt = 1;
+        if (hop > 0 && terminates(a.c, r.z)) {
+            finish();
+            return;
+        }
+        const uint64_t *cbeg = a.blk_beg[cb];
+        ccsr = a.blk_csr[cb];
+        const uint32_t off = cur - s_vs[cb];
+        const uint64_t e0 = a.estart[cb];
+        const uint64_t b0 = __ldg(cbeg + off), b1 = __ldg(cbeg + off + 1);
+        head = b0 - e0;
+        deg = (uint32_t)(b1 - b0);
+        if (deg == 0) {
+            finish();
+            return;
+        }
+        t = step_thresholds<SOPR>(a.c, deg, pdeg);
+        active = true;
+    };
+
+    for (;;) {
+        for (;;) {
+            const unsigned need = __ballot_sync(0xFFFFFFFFu, !active);
+            if (need == 0 || exhausted) break;
+            if (q_next >= q_end) {
+                uint32_t base = 0;
+                if (lane == 0) base = (uint32_t)atomicAdd(&a.ctr[kCtrCursor], (unsigned long long)kChunk);
+                base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                if (base >= total) {
+                    exhausted = true;
+                    break;
+                }
+                q_next = base;
+                q_end = min(base + kChunk, total);
+            }
+            const uint32_t avail = q_end - q_next;
+            const uint32_t rank = __popc(need & lt_mask);
+            if (!active && rank < avail) {
+                const uint32_t g = q_next + rank;
+                uint32_t lo = 0, hi = nrun;  // run_pre[lo] <= g < run_pre[hi]
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (__ldg(a.run_pre + mid) <= g) lo = mid;
+                    else hi = mid;
+                }
+                idx = (uint64_t)__ldg(a.run_off + lo) + (g - __ldg(a.run_pre + lo));
+                const WalkerRec rec = a.walkers[idx];
+                wid = rec.wid;
+                prev = rec.prev;
+                cur = rec.cur;
+                hop = rec.hop;
+                pb = rec.prev_blk;
+                cb = rec.cur_blk;
+                h = ((uint64_t)rec.hash_hi << 32) | rec.hash_lo;
+                if (PATHS) prow = a.paths + (uint64_t)wid * a.stride;
+                if (hop >= maxhops) {
+                    finish();
+                } else {
+                    const uint64_t *pbeg = a.blk_beg[pb];
+                    pcsr = a.blk_csr[pb];
+                    const uint32_t poff = prev - s_vs[pb];
+                    const uint64_t p0 = __ldg(pbeg + poff), p1 = __ldg(pbeg + poff + 1);
+                    phead = p0 - a.estart[pb];
+                    pdeg = (uint32_t)(p1 - p0);
+                    enter();
+                }
+            }
+            q_next += min((uint32_t)__popc(need), avail);
+        }
+        if (!__any_sync(0xFFFFFFFFu, active)) break;
+
+        // hard steps: the whole warp evaluates 32 attempts per round
+        for (unsigned hm = __ballot_sync(0xFFFFFFFFu, active && attempt > kHardAttempts); hm; hm &= hm - 1) {
+            const int L = __ffs(hm) - 1;
+            const uint32_t p0 = __shfl_sync(0xFFFFFFFFu, attempt, L) - 1;
+            const uint64_t hd = shfl64(head, L), ph = shfl64(phead, L);
+            const uint32_t *cc = shfl_ptr(ccsr, L), *pc = shfl_ptr(pcsr, L);
+            uint32_t xs;
+            const uint32_t astar = warp_first_accept<SOPR>(
+                a.c, shfl_thr(t, L), __shfl_sync(0xFFFFFFFFu, wid, L), __shfl_sync(0xFFFFFFFFu, hop, L), p0,
+                kMaxAttempts, cc + hd, __shfl_sync(0xFFFFFFFFu, deg, L), __shfl_sync(0xFFFFFFFFu, prev, L),
+                __shfl_sync(0xFFFFFFFFu, cur, L), pc + ph, __shfl_sync(0xFFFFFFFFu, pdeg, L), &xs);
+            if (lane == (uint32_t)L) {
+                n_trials += astar - p0;
+                if (astar >= kMaxAttempts) {
+                    atomicOr(a.err, kErrTrials);
+                    finish();
+                } else {
+                    r = draw(a.c, wid, hop, astar);
+                    attempt = astar + 1;
+                }
+            }
+        }
+        if (!active) continue;
+
+        const uint32_t pos = r.x % deg;
+        const float rv = rand_val(r.y, t.maxv);
+        const uint32_t x = __ldg(ccsr + head + pos);
+        n_trials++;
+        if (accept_candidate<SOPR>(t, rv, x, prev, cur, pcsr + phead, pdeg)) {
+            hop++;
+            n_steps++;
+            h = hash_step(h, x);
+            if (PATHS) prow[hop] = x;
+            prev = cur;
+            pb = cb;
+            phead = head;
+            pdeg = deg;
+            pcsr = ccsr;
+            cur = x;
+            if (hop >= maxhops) {
+                finish();
+            } else if (x >= a.nverts) {
+                atomicOr(a.err, kErrVertexRange);
+                finish();
+            } else {
+                const uint32_t nbx = (x >= s_vs[cb] && x < s_vs[cb + 1]) ? cb : block_of(s_vs, a.nb, x);
+                if (a.blk_beg[nbx] == nullptr) {
+                    // next block absent: park the walker in bucket (cb, nbx)
+                    WalkerRec rec;
+                    rec.wid = wid;
+                    rec.prev = prev;
+                    rec.cur = cur;
+                    rec.hop = hop;
+                    rec.prev_blk = pb;
+                    rec.cur_blk = nbx;
+                    rec.hash_lo = (uint32_t)h;
+                    rec.hash_hi = (uint32_t)(h >> 32);
+                    a.walkers[idx] = rec;
+                    active = false;
+                } else {
+                    cb = nbx;
+                    enter();
+                }
+            }
+        } else if (attempt >= kMaxAttempts) {
+            atomicOr(a.err, kErrTrials);
+            finish();
+        } else {
+            r = draw(a.c, wid, hop, attempt);
+            attempt++;
+        }
+    }
+
+    n_steps = warp_sum(n_steps);
+    n_trials = warp_sum(n_trials);
+    n_done = warp_sum(n_done);
+    hsum = warp_sum(hsum);
+    if (lane == 0) {
+        atomicAdd(&a.ctr[kCtrSteps], n_steps);
+        atomicAdd(&a.ctr[kCtrTrials], n_trials);
+        atomicAdd(&a.ctr[kCtrDone], n_done);
+        atomicAdd(&a.ctr[kCtrHashSum], hsum);
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+
+cudaError_t launch_init_walkers(const WalkerInit &in, const uint32_t *vstart, uint32_t nb, uint64_t n,
+                                WalkerRec *out, uint32_t *paths, uint32_t stride, int num_sms, cudaStream_t s)
+{
+    k_init_walkers<<<num_sms * 8, 256, 0, s>>>(in, vstart, nb, n, out, paths, stride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_count(const WalkerRec *w, uint64_t n, uint32_t nb, uint32_t *counts, int num_sms,
+                         cudaStream_t s)
+{
+    k_count<<<num_sms * 8, 256, 0, s>>>(w, n, nb, counts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scan(const uint32_t *counts, uint32_t n, uint32_t *offsets, cudaStream_t s)
+{
+    k_scan<<<1, kScanThreads, 0, s>>>(counts, n, offsets);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter(const WalkerRec *in, uint64_t n, uint32_t nb, const uint32_t *offsets,
+                           uint32_t *cursor, WalkerRec *out, int num_sms, cudaStream_t s)
+{
+    k_scatter<<<num_sms * 8, 256, 0, s>>>(in, n, nb, offsets, cursor, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_runnable(const uint32_t *counts, const uint32_t *offsets, const uint64_t *const *blk_beg,
+                            uint32_t nb, uint32_t *run_pre, uint32_t *run_off, uint32_t *nrun, cudaStream_t s)
+{
+    k_runnable<<<1, kScanThreads, 0, s>>>(counts, offsets, blk_beg, nb, run_pre, run_off, nrun);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_schedule(const uint32_t *counts, const uint32_t *offsets, uint32_t nb, const uint32_t *cached,
+                            uint32_t ncached, uint32_t nslots, uint32_t zero_threshold, const float *pred,
+                            float pred_weight, Decision *out, cudaStream_t s)
+{
+    k_schedule<<<1, 1024, 0, s>>>(counts, offsets, nb, cached, ncached, nslots, zero_threshold, pred, pred_weight,
+                                  out);
+    return cudaGetLastError();
+}
+
+template <bool SOPR, bool PATHS>
+static int ooc_grid_for(int num_sms)
+{
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_ooc<SOPR, PATHS>, kWalkThreads, 0);
+    return (per_sm < 1 ? 1 : per_sm) * num_sms;
+}
+
+int ooc_grid(bool sopr, bool paths, int num_sms)
+{
+    if (sopr) return paths ? ooc_grid_for<true, true>(num_sms) : ooc_grid_for<true, false>(num_sms);
+    return paths ? ooc_grid_for<false, true>(num_sms) : ooc_grid_for<false, false>(num_sms);
+}
+
+cudaError_t launch_walk_ooc(const OocStepArgs &a, bool sopr, int grid, cudaStream_t s)
+{
+    const bool paths = a.paths != nullptr;
+    if (sopr) {
+        if (paths) k_walk_ooc<true, true><<<grid, kWalkThreads, 0, s>>>(a);
+        else k_walk_ooc<true, false><<<grid, kWalkThreads, 0, s>>>(a);
+    } else {
+        if (paths) k_walk_ooc<false, true><<<grid, kWalkThreads, 0, s>>>(a);
+        else k_walk_ooc<false, false><<<grid, kWalkThreads, 0, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace gw

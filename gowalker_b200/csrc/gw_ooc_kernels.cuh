@@ -1,0 +1,68 @@
+// Out-of-core kernels: walker records, bucketing, block choice, step kernel.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "gw_kernels.cuh"
+
+namespace gw {
+
+// Device walker record, 32 bytes like the reference's walker_t
+// (api/types.hpp:49-56): id, previous, current, hop, prev/cur block (the
+// reference's prev_index / cur_index), and the running 64-bit path hash in
+// place of the source and totblk words, which the step never reads.
+struct __align__(16) WalkerRec {
+    uint32_t wid, prev, cur, hop;
+    uint32_t prev_blk, cur_blk;
+    uint32_t hash_lo, hash_hi;
+};
+static_assert(sizeof(WalkerRec) == 32, "walker record is 32 bytes");
+
+constexpr uint32_t kFinished = 0xFFFFFFFFu;  // prev_blk of a finished walker
+constexpr uint32_t kMaxBlocks = 1024;        // block table kept in shared memory
+
+struct OocStepArgs {
+    StepConsts c;
+    const uint64_t *const *blk_beg;  // [nb] block offsets (entry 0 = vertex vstart[b]); null = absent
+    const uint32_t *const *blk_csr;  // [nb] block neighbours, indexed from estart[b]
+    const uint32_t *vstart;          // [nb+1]
+    const uint64_t *estart;          // [nb+1]
+    uint32_t nb, nverts;
+    WalkerRec *walkers;              // bucket-sorted, updated in place
+    const uint32_t *run_pre;         // [nrun+1] prefix of runnable bucket sizes
+    const uint32_t *run_off;         // [nrun] first walker of each runnable bucket
+    const uint32_t *nrun;            // runnable bucket count (device)
+    uint32_t *paths;                 // or null
+    uint32_t stride;
+    uint32_t *lens;
+    uint64_t *hashes;
+    unsigned long long *ctr;
+    uint32_t *err;
+};
+
+// Decision of the block-choice kernel.
+struct Decision {
+    int32_t action;     // 0 none, 1 add to a free slot, 2 replace the block at `position`
+    int32_t block;      // block to load
+    int32_t position;   // index in the cached list to replace
+    int32_t rescue_block;     // best block by all incident walkers (progress when nothing qualifies)
+    int32_t rescue_position;  // cached block with the fewest incident walkers
+    uint32_t live;      // live walkers after the last bucketing
+    uint64_t score;
+};
+
+cudaError_t launch_init_walkers(const WalkerInit &in, const uint32_t *vstart, uint32_t nb, uint64_t n,
+                                WalkerRec *out, uint32_t *paths, uint32_t stride, int num_sms, cudaStream_t s);
+cudaError_t launch_count(const WalkerRec *w, uint64_t n, uint32_t nb, uint32_t *counts, int num_sms,
+                         cudaStream_t s);
+cudaError_t launch_scan(const uint32_t *counts, uint32_t n, uint32_t *offsets, cudaStream_t s);
+cudaError_t launch_scatter(const WalkerRec *in, uint64_t n, uint32_t nb, const uint32_t *offsets,
+                           uint32_t *cursor, WalkerRec *out, int num_sms, cudaStream_t s);
+cudaError_t launch_runnable(const uint32_t *counts, const uint32_t *offsets, const uint64_t *const *blk_beg,
+                            uint32_t nb, uint32_t *run_pre, uint32_t *run_off, uint32_t *nrun, cudaStream_t s);
+cudaError_t launch_schedule(const uint32_t *counts, const uint32_t *offsets, uint32_t nb, const uint32_t *cached,
+                            uint32_t ncached, uint32_t nslots, uint32_t zero_threshold, const float *pred,
+                            float pred_weight, Decision *out, cudaStream_t s);
+int ooc_grid(bool sopr, bool paths, int num_sms);
+cudaError_t launch_walk_ooc(const OocStepArgs &a, bool sopr, int grid, cudaStream_t s);
+
+}  // namespace gw

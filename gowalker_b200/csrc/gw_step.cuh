@@ -112,4 +112,69 @@ __device__ __forceinline__ bool accept_candidate(const StepThr &t, float rv, uin
     return found ? (rv < t.t_found) : (rv < t.t_notfound);
 }
 
+// A walker whose step has already rejected this many attempts is served by
+// the whole warp (warp_first_accept).
+constexpr uint32_t kHardAttempts = 8;
+
+__device__ __forceinline__ uint64_t shfl64(uint64_t v, int src)
+{
+    const uint32_t lo = __shfl_sync(0xFFFFFFFFu, (uint32_t)v, src);
+    const uint32_t hi = __shfl_sync(0xFFFFFFFFu, (uint32_t)(v >> 32), src);
+    return ((uint64_t)hi << 32) | lo;
+}
+
+template <typename T>
+__device__ __forceinline__ T *shfl_ptr(T *p, int src)
+{
+    return reinterpret_cast<T *>(shfl64(reinterpret_cast<uint64_t>(p), src));
+}
+
+__device__ __forceinline__ StepThr shfl_thr(const StepThr &t, int src)
+{
+    StepThr o;
+    o.maxv = __shfl_sync(0xFFFFFFFFu, t.maxv, src);
+    o.minv = __shfl_sync(0xFFFFFFFFu, t.minv, src);
+    o.t_prev = __shfl_sync(0xFFFFFFFFu, t.t_prev, src);
+    o.t_found = __shfl_sync(0xFFFFFFFFu, t.t_found, src);
+    o.t_notfound = __shfl_sync(0xFFFFFFFFu, t.t_notfound, src);
+    o.t_prev_d = __shfl_sync(0xFFFFFFFFu, t.t_prev_d, src);
+    return o;
+}
+
+// All 32 lanes, with identical (broadcast) arguments, evaluate attempts
+// p0+lane, p0+32+lane, ... of one walker's step and return the first accepting
+// attempt in attempt order -- the one a single thread evaluating them one by
+// one would take -- and its candidate in *x_out.  Returns `limit` if none of
+// the attempts below `limit` accepts.
+template <bool SOPR>
+__device__ __forceinline__ uint32_t warp_first_accept(const StepConsts &c, const StepThr &t, uint32_t wid,
+                                                      uint32_t hop, uint32_t p0, uint32_t limit,
+                                                      const uint32_t *__restrict__ cand, uint32_t deg,
+                                                      uint32_t prev, uint32_t cur,
+                                                      const uint32_t *__restrict__ prev_adj, uint32_t pdeg,
+                                                      uint32_t *x_out)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = p0; base < limit; base += 32) {
+        const uint32_t att = base + lane;
+        bool acc = false;
+        uint32_t x = 0;
+        if (att < limit) {
+            const U4 r = draw(c, wid, hop, att);
+            const uint32_t pos = r.x % deg;
+            const float rv = rand_val(r.y, t.maxv);
+            x = __ldg(cand + pos);
+            acc = accept_candidate<SOPR>(t, rv, x, prev, cur, prev_adj, pdeg);
+        }
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, acc);
+        if (m) {
+            const int f = __ffs(m) - 1;
+            *x_out = __shfl_sync(0xFFFFFFFFu, x, f);
+            return base + (uint32_t)f;
+        }
+    }
+    *x_out = 0;
+    return limit;
+}
+
 }  // namespace gw

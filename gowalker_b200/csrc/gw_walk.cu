@@ -20,24 +20,6 @@
 
 namespace gw {
 
-__device__ __forceinline__ uint32_t walker_source(const WalkerInit &in, uint32_t wid)
-{
-    if (in.mode == GW_INIT_PER_VERTEX) return wid / in.wps;
-    if (in.mode == GW_INIT_SINGLE_SOURCE) {
-        if (in.algo == GW_SOSR) return wid < in.numwalks / 2 ? 1u : 3u;
-        return 1u;
-    }
-    const U4 r = philox4x32_10(wid, 0xFFFFFFFFu, 0u, kTagInit, in.key0, in.key1);
-    return r.x % in.nverts;
-}
-
-__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
-    return v;
-}
-
 template <bool SOPR, bool PATHS>
 __global__ void __launch_bounds__(kWalkThreads) k_walk_incore(const IncoreArgs a)
 {
@@ -118,6 +100,30 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_incore(const IncoreArgs a
             q_next += min((uint32_t)__popc(need), avail);
         }
         if (!__any_sync(0xFFFFFFFFu, active)) break;
+
+        // Walkers whose step keeps rejecting (a low-degree prev next to a hub
+        // under SOPR) are served one at a time by the whole warp, 32 attempts
+        // per round; the lane then re-takes the accepting attempt below.
+        for (unsigned hm = __ballot_sync(0xFFFFFFFFu, active && attempt > kHardAttempts); hm; hm &= hm - 1) {
+            const int L = __ffs(hm) - 1;
+            const uint32_t p0 = __shfl_sync(0xFFFFFFFFu, attempt, L) - 1;
+            const uint64_t hd = shfl64(head, L), ph = shfl64(phead, L);
+            uint32_t xs;
+            const uint32_t astar = warp_first_accept<SOPR>(
+                a.c, shfl_thr(t, L), __shfl_sync(0xFFFFFFFFu, wid, L), __shfl_sync(0xFFFFFFFFu, hop, L), p0,
+                kMaxAttempts, csr + hd, __shfl_sync(0xFFFFFFFFu, deg, L), __shfl_sync(0xFFFFFFFFu, prev, L),
+                __shfl_sync(0xFFFFFFFFu, cur, L), csr + ph, __shfl_sync(0xFFFFFFFFu, pdeg, L), &xs);
+            if (lane == (uint32_t)L) {
+                n_trials += astar - p0;
+                if (astar >= kMaxAttempts) {
+                    atomicOr(a.err, kErrTrials);
+                    finish();
+                } else {
+                    r = draw(a.c, wid, hop, astar);
+                    attempt = astar + 1;
+                }
+            }
+        }
         if (!active) continue;
 
         // One rejection-sampling trial.

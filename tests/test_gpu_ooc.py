@@ -1,0 +1,80 @@
+"""GPU tests of the out-of-core path: device block cache, bucketing, block
+choice, zero-copy tail.  Walks must be bit-identical to the oracle whatever
+the cache size or schedule (counter-based draws)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def graph(oracle, scale=13, ef=8, sym=False, cap=6000, seed=21):
+    src, dst = oracle.rmat_edges(scale, 0, ef << scale, seed=seed)
+    keep = (src < cap) & (dst < cap)
+    return oracle.build_csr(cap, src[keep], dst[keep], symmetric=sym)
+
+
+def run_ooc(gw, beg, csr, nblocks, slots, algo=0, maxhops=20, wps=1, p=0.5, q=2.0, alpha=0.2, term=0.0, seed=5,
+            zero_copy=0, zero_threshold=0, paths=1, policy=0):
+    from oracle import oracle as O
+    vb, eb = O.split_equal_edge_mass(beg, nblocks)
+    maxv = int(np.diff(vb.astype(np.int64)).max())
+    maxe = int(np.diff(eb.astype(np.int64)).max())
+    slot = ((maxv + 2) & ~1) * 8 + ((max(maxe, 1) + 3) & ~3) * 4
+    cache = slot * slots
+    eng = gw.WalkEngine(algorithm=algo, maxhops=maxhops, p=p, q=q, alpha=alpha, term_prob=term, seed=seed,
+                        walkpersource=wps, record_paths=paths, cache_size=cache, zero_copy=zero_copy,
+                        zero_threshold=zero_threshold)
+    eng.set_host_graph(beg, csr, vb, eb)
+    eng.init_walkers(algo, wps, seed)
+    st = eng.run(policy)
+    return eng, st
+
+
+@pytest.mark.parametrize("algo,term,sym", [(0, 0.0, False), (1, 0.15, False), (0, 0.0, True), (2, 0.15, True)])
+def test_ooc_matches_oracle(gw, oracle, algo, term, sym):
+    beg, csr = graph(oracle, sym=sym)
+    V = len(beg) - 1
+    eng, st = run_ooc(gw, beg, csr, 12, 3, algo=algo, term=term, wps=2)
+    cfg = oracle.make_cfg(algo=algo, maxhops=20, p=0.5, q=2.0, alpha=0.2, term_prob=term, seed=5, wps=2)
+    ref = oracle.walk(beg, csr, cfg, 0, 2 * V, paths=True)
+    P, L = eng.paths()
+    assert np.array_equal(L, ref["lens"])
+    assert np.array_equal(P, ref["paths"])
+    assert np.array_equal(eng.hashes(), ref["hashes"])
+    assert st["steps"] == ref["stats"]["steps"]
+    assert st["trials"] == ref["stats"]["trials"]
+    assert st["block_loads"] >= 3 and st["h2d_bytes"] > 0 and st["iterations"] >= 3
+    assert int(eng.bucket_counts().sum()) == 0  # every walker finished
+    eng.close()
+
+
+def test_schedule_invariance(gw, oracle):
+    """Same walks for every cache size, with and without the zero-copy tail."""
+    beg, csr = graph(oracle, scale=13, ef=12, sym=True, cap=7000, seed=3)
+    base = None
+    loads = {}
+    for slots, zc, zt in ((2, 0, 0), (4, 0, 0), (7, 0, 0), (3, 1, 400), (10, 0, 0)):
+        eng, st = run_ooc(gw, beg, csr, 10, slots, algo=1, term=0.15, wps=1, zero_copy=zc, zero_threshold=zt,
+                          paths=0)
+        h = eng.hashes()
+        loads[(slots, zc)] = (st["block_loads"], st["zero_copy_steps"])
+        eng.close()
+        base = h if base is None else base
+        assert np.array_equal(h, base), (slots, zc)
+    assert loads[(3, 1)][1] > 0          # the tail ran through mapped host memory
+    assert loads[(2, 0)][0] >= loads[(10, 0)][0]
+
+
+def test_ooc_learned_policy_same_walks(gw, oracle):
+    beg, csr = graph(oracle, scale=13, ef=8, sym=False, cap=6000, seed=8)
+    e1, s1 = run_ooc(gw, beg, csr, 12, 3, algo=0, paths=0, policy=0)
+    e2, s2 = run_ooc(gw, beg, csr, 12, 3, algo=0, paths=0, policy=1)
+    assert np.array_equal(e1.hashes(), e2.hashes())
+    e1.close()
+    e2.close()
+
+
+def test_ooc_rejects_tiny_cache(gw, oracle):
+    beg, csr = graph(oracle)
+    with pytest.raises(gw.GwError):
+        run_ooc(gw, beg, csr, 8, 1)
