@@ -43,6 +43,10 @@ WORKLOADS = {
                scale=24, ef=16, algo=1, maxhops=20, wps=4, p=0.5, q=2.0, alpha=0.2, term=0.15),
     "c1": dict(name="C1: Node2vec p=2 q=0.5 length 80, 1 walker/vertex, R-MAT scale 20 ef 16 symmetrised, in-core",
                scale=20, ef=16, algo=0, maxhops=80, wps=1, p=2.0, q=0.5, alpha=0.2, term=0.0),
+    "c3": dict(name="C3: out-of-core Node2vec p=0.5 q=2 length 80, 1 walker/vertex, directed R-MAT scale 26 "
+                    "rejecting ids >= 41.6M, thinned to 1.47B edges, 64 equal-edge-mass blocks, 1.5 GB device cache",
+               scale=26, nverts=41_600_000, target=1_470_000_000, nsamples=2_600_000_000, ef=0, algo=0, maxhops=80,
+               wps=1, p=0.5, q=2.0, alpha=0.2, term=0.0, nblocks=64, cache=1_500_000_000, ooc=True),
 }
 L2_BYTES = 126 * 1024 * 1024
 
@@ -123,6 +127,20 @@ class ClockSampler:
 
 def build_graph(gw, wl):
     t0 = time.time()
+    if wl.get("ooc"):
+        nsamples = wl["nsamples"]
+        for _ in range(4):
+            try:
+                dg = gw.DeviceGraph(wl["scale"], nverts=wl["nverts"], nsamples=nsamples, seed=1, symmetric=False,
+                                    target_edges=wl["target"])
+                break
+            except gw.GwError:
+                nsamples = int(nsamples * 1.2)  # too few unique edges: sample more
+        else:
+            raise RuntimeError("could not reach the target edge count")
+        log("graph: V=%d E=%d from %d samples, built on device in %.1fs" % (dg.nverts, dg.nedges, nsamples,
+                                                                           time.time() - t0))
+        return dg
     dg = gw.DeviceGraph(wl["scale"], edgefactor=wl["ef"], seed=1, symmetric=True)
     log("graph: V=%d E=%d built on device in %.1fs" % (dg.nverts, dg.nedges, time.time() - t0))
     return dg
@@ -203,6 +221,77 @@ def run_reference_arm(args, wl):
                              "sample": "per step: " + desc},
             "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+PCIE_GEN5_X16_GBS = 64.0  # nominal host-link peak per direction
+
+
+def run_ooc_bench(args, wl):
+    """Out-of-core workload: blocks in pinned host memory, device cache capped."""
+    import torch
+    import gowalker_b200 as gw
+    torch.cuda.set_device(0)
+    dg = build_graph(gw, wl)
+    beg_t, csr_t, beg, csr = host_graph(dg)
+    dg.free()
+    from gowalker_b200.preprocess import split_equal_edge_mass
+    vb, eb = split_equal_edge_mass(beg, wl["nblocks"])
+    policy = gw.GW_POLICY_LEARNED if args.policy == "learned" else gw.GW_POLICY_PLAIN
+    eng = gw.WalkEngine(algorithm=wl["algo"], maxhops=wl["maxhops"], p=wl["p"], q=wl["q"], alpha=wl["alpha"],
+                        term_prob=wl["term"], seed=42, walkpersource=wl["wps"], record_paths=1 if args.paths else 0,
+                        cache_size=wl["cache"], zero_copy=0)
+    eng.set_host_graph(beg_t, csr_t[: len(csr)], vb, eb)
+    stream = torch.cuda.ExternalStream(eng.stream_handle())
+    for _ in range(args.warmup):
+        eng.init_walkers(wl["algo"], wl["wps"], 42)
+        eng.run(policy)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    tot = {"steps": 0, "h2d_bytes": 0, "kernel_ms": 0.0, "block_loads": 0, "iterations": 0, "launches": 0,
+           "d2h_bytes": 0, "trials": 0}
+    for _ in range(args.steps):
+        eng.init_walkers(wl["algo"], wl["wps"], 42)
+        st = eng.run(policy)
+        for k in tot:
+            tot[k] += st[k]
+    hs, _ = eng.checksum()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    value = tot["steps"] / (ms / 1000.0)
+    h2d_step = tot["h2d_bytes"] / args.steps
+    link = h2d_step / (ms / 1000.0 / args.steps) / 1e9
+    line = {"metric": "walk steps/sec", "value": value, "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32 gathers, fp32/fp64 accept compares", "data": "synthetic",
+            "config": {"workload": wl["name"], "policy": args.policy, "vertices": len(beg) - 1, "edges": len(csr),
+                       "blocks": wl["nblocks"], "cache_bytes": wl["cache"], "walkers": eng.num_walkers(),
+                       "graph_in": "pinned host memory", "paths_recorded": bool(args.paths)},
+            "gpu_launches": tot["launches"],
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": int(h2d_step),
+                    "d2h_bytes_per_step": int(tot["d2h_bytes"] / args.steps)},
+            "h2d_bytes_per_walk_step": tot["h2d_bytes"] / max(tot["steps"], 1),
+            "block_loads_per_run": tot["block_loads"] / args.steps,
+            "iterations_per_run": tot["iterations"] / args.steps,
+            "roofline": {"bound": "host-link", "achieved": link, "peak": PCIE_GEN5_X16_GBS, "unit": "GB/s",
+                         "frac": link / PCIE_GEN5_X16_GBS, "traffic": None,
+                         "kernel_ms_per_run": tot["kernel_ms"] / args.steps},
+            "checksum": {"path_hash_sum": hs}}
+    if clk:
+        line["clocks"] = clk
+    if args.cpu_seconds > 0:
+        from oracle import oracle as O
+        threads = os.cpu_count() or 1
+        s_steps, s_secs, _, _, s_desc = oracle_sample(O, beg, csr, wl, 42, args.cpu_seconds, threads=threads)
+        line["cpu_baseline"] = {"value": s_steps / s_secs, "unit": "steps/s", "cores": threads, "kind": "port",
+                                "sample": s_desc}
+    print(json.dumps(line), flush=True)
+    eng.close()
     return 0
 
 
@@ -364,6 +453,7 @@ def main():
     ap.add_argument("--paths", type=int, default=1, help="record full paths (1) or hashes only (0)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
+    ap.add_argument("--policy", default="plain", choices=["plain", "learned"], help="block policy (out-of-core)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.config])
     if args.scale:
@@ -373,6 +463,8 @@ def main():
         log("note: fewer than 3 warm-up steps")
     if args.impl == "reference":
         return run_reference_arm(args, wl)
+    if wl.get("ooc"):
+        return run_ooc_bench(args, wl)
     return run_ours(args, wl)
 
 

@@ -476,10 +476,11 @@ int gw_handle::run_incore(gw_stats *stats)
     a.ctr = d_ctr;
     a.err = d_err;
     const bool sopr = cfg.algorithm != GW_NODE2VEC;
+    const bool coop = needs_coop(cfg.algorithm, a.c);
     int grid = (int)cfg.blockpergrid;
-    if (grid <= 0) grid = incore_grid(sopr, a.paths != nullptr, num_sms);
+    if (grid <= 0) grid = incore_grid(sopr, a.paths != nullptr, coop, num_sms);
     if ((st = cuda(cudaEventRecord(ev_kernel0, s), "event"))) return st;
-    if ((st = cuda(launch_walk_incore(a, sopr, grid, s), "walk kernel launch"))) return st;
+    if ((st = cuda(launch_walk_incore(a, sopr, coop, grid, s), "walk kernel launch"))) return st;
     if ((st = cuda(cudaEventRecord(ev_kernel1, s), "event"))) return st;
     if ((st = cuda(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(unsigned long long) * kCtrCount, cudaMemcpyDeviceToHost, s),
                    "counters D2H")))

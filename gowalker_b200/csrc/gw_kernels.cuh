@@ -80,8 +80,17 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
 }
 
 // Grid size (CTAs) for a persistent walk kernel on this device.
-int incore_grid(bool sopr, bool paths, int num_sms);
-cudaError_t launch_walk_incore(const IncoreArgs &a, bool sopr, int grid, cudaStream_t s);
+int incore_grid(bool sopr, bool paths, bool coop, int num_sms);
+cudaError_t launch_walk_incore(const IncoreArgs &a, bool sopr, bool coop, int grid, cudaStream_t s);
+
+// Whether a run needs the warp-cooperative path for hard steps: always for
+// SOPR/SOSR (acceptance ~ deg(prev)/deg(cur) next to hubs); for Node2vec
+// only when max/min of {1/p, 1/q, 1} exceeds 8 (otherwise a step accepts
+// within 1/ratio >= 1/8 per trial and never gets hard).
+inline bool needs_coop(uint32_t algo, const StepConsts &c)
+{
+    return algo != 0u || c.n2v_maxv > 8.0f * c.n2v_minv;
+}
 cudaError_t launch_validate_csr(const uint64_t *beg, const uint32_t *csr, uint32_t nverts, uint64_t nedges,
                                 uint32_t *err, int num_sms, cudaStream_t s);
 

@@ -313,8 +313,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     a.hashes = d_hashes;
     a.ctr = d_ctr;
     a.err = d_err;
+    const bool coop = needs_coop(cfg.algorithm, a.c);
     int grid = (int)cfg.blockpergrid;
-    if (grid <= 0) grid = ooc_grid(sopr, paths, num_sms);
+    if (grid <= 0) grid = ooc_grid(sopr, paths, coop, num_sms);
 
     cudaEvent_t k0 = nullptr, k1 = nullptr;
     cudaEventCreate(&k0);
@@ -327,7 +328,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if ((e = cuda(cudaMemsetAsync(d_ctr + kCtrCursor, 0, sizeof(unsigned long long), s), "memset"))) return e;
         a.walkers = o.w_a;
         if ((e = cuda(cudaEventRecord(k0, s), "event"))) return e;
-        if ((e = cuda(launch_walk_ooc(a, sopr, grid, s), "walk kernel"))) return e;
+        if ((e = cuda(launch_walk_ooc(a, sopr, coop, grid, s), "walk kernel"))) return e;
         if ((e = cuda(cudaEventRecord(k1, s), "event"))) return e;
         launches += 2;
         return GW_OK;

@@ -301,10 +301,11 @@ __global__ void __launch_bounds__(1024) k_schedule(const uint32_t *__restrict__ 
     }
 }
 
-template <bool SOPR, bool PATHS>
+template <bool SOPR, bool PATHS, bool COOP>
 __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const OocStepArgs a)
 {
     __shared__ uint32_t s_vs[kMaxBlocks + 1];
+    __shared__ uint32_t s_iv[kWalkThreads / 32][64];
     for (uint32_t i = threadIdx.x; i <= a.nb; i += blockDim.x) s_vs[i] = a.vstart[i];
     __syncthreads();
 
@@ -410,7 +411,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const OocStepArgs a)
         if (!__any_sync(0xFFFFFFFFu, active)) break;
 
         // hard steps: the whole warp evaluates 32 attempts per round
-        for (unsigned hm = __ballot_sync(0xFFFFFFFFu, active && attempt > kHardAttempts); hm; hm &= hm - 1) {
+        for (unsigned hm = COOP ? __ballot_sync(0xFFFFFFFFu, active && attempt > kHardAttempts) : 0u; hm;
+             hm &= hm - 1) {
             const int L = __ffs(hm) - 1;
             const uint32_t p0 = __shfl_sync(0xFFFFFFFFu, attempt, L) - 1;
             const uint64_t hd = shfl64(head, L), ph = shfl64(phead, L);
@@ -419,7 +421,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const OocStepArgs a)
             const uint32_t astar = warp_first_accept<SOPR>(
                 a.c, shfl_thr(t, L), __shfl_sync(0xFFFFFFFFu, wid, L), __shfl_sync(0xFFFFFFFFu, hop, L), p0,
                 kMaxAttempts, cc + hd, __shfl_sync(0xFFFFFFFFu, deg, L), __shfl_sync(0xFFFFFFFFu, prev, L),
-                __shfl_sync(0xFFFFFFFFu, cur, L), pc + ph, __shfl_sync(0xFFFFFFFFu, pdeg, L), &xs);
+                __shfl_sync(0xFFFFFFFFu, cur, L), pc + ph, __shfl_sync(0xFFFFFFFFu, pdeg, L), s_iv[threadIdx.x >> 5],
+                &xs);
             if (lane == (uint32_t)L) {
                 n_trials += astar - p0;
                 if (astar >= kMaxAttempts) {
@@ -539,29 +542,47 @@ cudaError_t launch_schedule(const uint32_t *counts, const uint32_t *offsets, uin
     return cudaGetLastError();
 }
 
-template <bool SOPR, bool PATHS>
+template <bool SOPR, bool PATHS, bool COOP>
 static int ooc_grid_for(int num_sms)
 {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_ooc<SOPR, PATHS>, kWalkThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_ooc<SOPR, PATHS, COOP>, kWalkThreads, 0);
     return (per_sm < 1 ? 1 : per_sm) * num_sms;
 }
 
-int ooc_grid(bool sopr, bool paths, int num_sms)
+template <bool SOPR, bool PATHS, bool COOP>
+static void ooc_launch_one(const OocStepArgs &a, int grid, cudaStream_t s)
 {
-    if (sopr) return paths ? ooc_grid_for<true, true>(num_sms) : ooc_grid_for<true, false>(num_sms);
-    return paths ? ooc_grid_for<false, true>(num_sms) : ooc_grid_for<false, false>(num_sms);
+    k_walk_ooc<SOPR, PATHS, COOP><<<grid, kWalkThreads, 0, s>>>(a);
 }
 
-cudaError_t launch_walk_ooc(const OocStepArgs &a, bool sopr, int grid, cudaStream_t s)
+int ooc_grid(bool sopr, bool paths, bool coop, int num_sms)
 {
-    const bool paths = a.paths != nullptr;
-    if (sopr) {
-        if (paths) k_walk_ooc<true, true><<<grid, kWalkThreads, 0, s>>>(a);
-        else k_walk_ooc<true, false><<<grid, kWalkThreads, 0, s>>>(a);
-    } else {
-        if (paths) k_walk_ooc<false, true><<<grid, kWalkThreads, 0, s>>>(a);
-        else k_walk_ooc<false, false><<<grid, kWalkThreads, 0, s>>>(a);
+    const int v = (sopr ? 4 : 0) | (paths ? 2 : 0) | (coop ? 1 : 0);
+    switch (v) {
+    case 0: return ooc_grid_for<false, false, false>(num_sms);
+    case 1: return ooc_grid_for<false, false, true>(num_sms);
+    case 2: return ooc_grid_for<false, true, false>(num_sms);
+    case 3: return ooc_grid_for<false, true, true>(num_sms);
+    case 4: return ooc_grid_for<true, false, false>(num_sms);
+    case 5: return ooc_grid_for<true, false, true>(num_sms);
+    case 6: return ooc_grid_for<true, true, false>(num_sms);
+    default: return ooc_grid_for<true, true, true>(num_sms);
+    }
+}
+
+cudaError_t launch_walk_ooc(const OocStepArgs &a, bool sopr, bool coop, int grid, cudaStream_t s)
+{
+    const int v = (sopr ? 4 : 0) | (a.paths ? 2 : 0) | (coop ? 1 : 0);
+    switch (v) {
+    case 0: ooc_launch_one<false, false, false>(a, grid, s); break;
+    case 1: ooc_launch_one<false, false, true>(a, grid, s); break;
+    case 2: ooc_launch_one<false, true, false>(a, grid, s); break;
+    case 3: ooc_launch_one<false, true, true>(a, grid, s); break;
+    case 4: ooc_launch_one<true, false, false>(a, grid, s); break;
+    case 5: ooc_launch_one<true, false, true>(a, grid, s); break;
+    case 6: ooc_launch_one<true, true, false>(a, grid, s); break;
+    default: ooc_launch_one<true, true, true>(a, grid, s); break;
     }
     return cudaGetLastError();
 }

@@ -62,7 +62,7 @@ cudaError_t launch_runnable(const uint32_t *counts, const uint32_t *offsets, con
 cudaError_t launch_schedule(const uint32_t *counts, const uint32_t *offsets, uint32_t nb, const uint32_t *cached,
                             uint32_t ncached, uint32_t nslots, uint32_t zero_threshold, const float *pred,
                             float pred_weight, Decision *out, cudaStream_t s);
-int ooc_grid(bool sopr, bool paths, int num_sms);
-cudaError_t launch_walk_ooc(const OocStepArgs &a, bool sopr, int grid, cudaStream_t s);
+int ooc_grid(bool sopr, bool paths, bool coop, int num_sms);
+cudaError_t launch_walk_ooc(const OocStepArgs &a, bool sopr, bool coop, int grid, cudaStream_t s);
 
 }  // namespace gw

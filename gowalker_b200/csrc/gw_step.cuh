@@ -146,14 +146,101 @@ __device__ __forceinline__ StepThr shfl_thr(const StepThr &t, int src)
 // attempt in attempt order -- the one a single thread evaluating them one by
 // one would take -- and its candidate in *x_out.  Returns `limit` if none of
 // the attempts below `limit` accepts.
+// First index in the sorted run a[0, n) whose value is >= y.
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *__restrict__ a, uint32_t n, uint32_t y)
+{
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(a + mid) < y) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Hard steps whose prev has fewer than 32 neighbours are decided without
+// touching the candidate: a trial's verdict depends on x = cand[pos] only
+// through "x == prev" and "x in N(prev)", i.e. through whether pos falls in
+// the run of prev, or of some y in N(prev), inside the sorted N(cur).  Those
+// runs are located once per step (one lower-bound search per lane); the
+// trials are then Philox + a lookup in `iv`, a 64-word per-warp scratch in
+// shared memory.
+template <bool SOPR>
+__device__ __forceinline__ uint32_t warp_first_accept_runs(const StepConsts &c, const StepThr &t, uint32_t wid,
+                                                           uint32_t hop, uint32_t p0, uint32_t limit,
+                                                           const uint32_t *__restrict__ cand, uint32_t deg,
+                                                           uint32_t prev, const uint32_t *__restrict__ prev_adj,
+                                                           uint32_t pdeg, uint32_t *iv, uint32_t *x_out)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    // lane k < pdeg: run of N(prev)[k]; lane pdeg: run of prev
+    uint32_t lo = 0, hi = 0;
+    if (lane <= pdeg) {
+        const uint32_t y = (lane < pdeg) ? __ldg(prev_adj + lane) : prev;
+        lo = lower_bound_u32(cand, deg, y);
+        hi = lo;
+        while (hi < deg && __ldg(cand + hi) == y) hi++;
+    }
+    if (lane < pdeg) {
+        iv[lane] = lo;
+        iv[32 + lane] = hi;
+    }
+    __syncwarp();
+    const uint32_t plo = __shfl_sync(0xFFFFFFFFu, lo, (int)pdeg), phi = __shfl_sync(0xFFFFFFFFu, hi, (int)pdeg);
+    for (uint32_t base = p0; base < limit; base += 32) {
+        const uint32_t att = base + lane;
+        bool acc = false;
+        uint32_t pos = 0;
+        if (att < limit) {
+            const U4 r = draw(c, wid, hop, att);
+            pos = r.x % deg;
+            const float rv = rand_val(r.y, t.maxv);
+            if (rv <= t.minv) {
+                acc = true;
+            } else if (pos >= plo && pos < phi) {
+                if constexpr (SOPR) acc = (double)rv < t.t_prev_d;
+                else acc = rv < t.t_prev;
+            } else {
+                // last run whose start is <= pos (runs are in N(prev) order, so sorted)
+                int k = -1;
+                uint32_t a = 0, b = pdeg;
+                while (a < b) {
+                    const uint32_t m = (a + b) >> 1;
+                    if (iv[m] <= pos) {
+                        k = (int)m;
+                        a = m + 1;
+                    } else {
+                        b = m;
+                    }
+                }
+                const bool found = k >= 0 && pos < iv[32 + k];
+                acc = found ? (rv < t.t_found) : (rv < t.t_notfound);
+            }
+        }
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, acc);
+        if (m) {
+            const int f = __ffs(m) - 1;
+            const uint32_t pf = __shfl_sync(0xFFFFFFFFu, pos, f);
+            *x_out = __ldg(cand + pf);
+            __syncwarp();
+            return base + (uint32_t)f;
+        }
+    }
+    *x_out = 0;
+    __syncwarp();
+    return limit;
+}
+
 template <bool SOPR>
 __device__ __forceinline__ uint32_t warp_first_accept(const StepConsts &c, const StepThr &t, uint32_t wid,
                                                       uint32_t hop, uint32_t p0, uint32_t limit,
                                                       const uint32_t *__restrict__ cand, uint32_t deg,
                                                       uint32_t prev, uint32_t cur,
                                                       const uint32_t *__restrict__ prev_adj, uint32_t pdeg,
-                                                      uint32_t *x_out)
+                                                      uint32_t *iv, uint32_t *x_out)
 {
+    if (pdeg < 32 && prev != cur)
+        return warp_first_accept_runs<SOPR>(c, t, wid, hop, p0, limit, cand, deg, prev, prev_adj, pdeg, iv, x_out);
     const uint32_t lane = threadIdx.x & 31u;
     for (uint32_t base = p0; base < limit; base += 32) {
         const uint32_t att = base + lane;

@@ -20,9 +20,10 @@
 
 namespace gw {
 
-template <bool SOPR, bool PATHS>
+template <bool SOPR, bool PATHS, bool COOP>
 __global__ void __launch_bounds__(kWalkThreads) k_walk_incore(const IncoreArgs a)
 {
+    __shared__ uint32_t s_iv[kWalkThreads / 32][64];  // per-warp scratch of warp_first_accept
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint64_t *__restrict__ beg = a.beg;
@@ -104,7 +105,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_incore(const IncoreArgs a
         // Walkers whose step keeps rejecting (a low-degree prev next to a hub
         // under SOPR) are served one at a time by the whole warp, 32 attempts
         // per round; the lane then re-takes the accepting attempt below.
-        for (unsigned hm = __ballot_sync(0xFFFFFFFFu, active && attempt > kHardAttempts); hm; hm &= hm - 1) {
+        for (unsigned hm = COOP ? __ballot_sync(0xFFFFFFFFu, active && attempt > kHardAttempts) : 0u; hm;
+             hm &= hm - 1) {
             const int L = __ffs(hm) - 1;
             const uint32_t p0 = __shfl_sync(0xFFFFFFFFu, attempt, L) - 1;
             const uint64_t hd = shfl64(head, L), ph = shfl64(phead, L);
@@ -112,7 +114,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_incore(const IncoreArgs a
             const uint32_t astar = warp_first_accept<SOPR>(
                 a.c, shfl_thr(t, L), __shfl_sync(0xFFFFFFFFu, wid, L), __shfl_sync(0xFFFFFFFFu, hop, L), p0,
                 kMaxAttempts, csr + hd, __shfl_sync(0xFFFFFFFFu, deg, L), __shfl_sync(0xFFFFFFFFu, prev, L),
-                __shfl_sync(0xFFFFFFFFu, cur, L), csr + ph, __shfl_sync(0xFFFFFFFFu, pdeg, L), &xs);
+                __shfl_sync(0xFFFFFFFFu, cur, L), csr + ph, __shfl_sync(0xFFFFFFFFu, pdeg, L), s_iv[threadIdx.x >> 5],
+                &xs);
             if (lane == (uint32_t)L) {
                 n_trials += astar - p0;
                 if (astar >= kMaxAttempts) {
@@ -211,30 +214,48 @@ cudaError_t launch_validate_csr(const uint64_t *beg, const uint32_t *csr, uint32
     return cudaGetLastError();
 }
 
-template <bool SOPR, bool PATHS>
+template <bool SOPR, bool PATHS, bool COOP>
 static int grid_for(int num_sms)
 {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_incore<SOPR, PATHS>, kWalkThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_incore<SOPR, PATHS, COOP>, kWalkThreads, 0);
     if (per_sm < 1) per_sm = 1;
     return per_sm * num_sms;
 }
 
-int incore_grid(bool sopr, bool paths, int num_sms)
+template <bool SOPR, bool PATHS, bool COOP>
+static void launch_one(const IncoreArgs &a, int grid, cudaStream_t s)
 {
-    if (sopr) return paths ? grid_for<true, true>(num_sms) : grid_for<true, false>(num_sms);
-    return paths ? grid_for<false, true>(num_sms) : grid_for<false, false>(num_sms);
+    k_walk_incore<SOPR, PATHS, COOP><<<grid, kWalkThreads, 0, s>>>(a);
 }
 
-cudaError_t launch_walk_incore(const IncoreArgs &a, bool sopr, int grid, cudaStream_t s)
+int incore_grid(bool sopr, bool paths, bool coop, int num_sms)
 {
-    const bool paths = a.paths != nullptr;
-    if (sopr) {
-        if (paths) k_walk_incore<true, true><<<grid, kWalkThreads, 0, s>>>(a);
-        else k_walk_incore<true, false><<<grid, kWalkThreads, 0, s>>>(a);
-    } else {
-        if (paths) k_walk_incore<false, true><<<grid, kWalkThreads, 0, s>>>(a);
-        else k_walk_incore<false, false><<<grid, kWalkThreads, 0, s>>>(a);
+    const int v = (sopr ? 4 : 0) | (paths ? 2 : 0) | (coop ? 1 : 0);
+    switch (v) {
+    case 0: return grid_for<false, false, false>(num_sms);
+    case 1: return grid_for<false, false, true>(num_sms);
+    case 2: return grid_for<false, true, false>(num_sms);
+    case 3: return grid_for<false, true, true>(num_sms);
+    case 4: return grid_for<true, false, false>(num_sms);
+    case 5: return grid_for<true, false, true>(num_sms);
+    case 6: return grid_for<true, true, false>(num_sms);
+    default: return grid_for<true, true, true>(num_sms);
+    }
+}
+
+cudaError_t launch_walk_incore(const IncoreArgs &a, bool sopr, bool coop, int grid, cudaStream_t s)
+{
+    const int v = (sopr ? 4 : 0) | (a.paths ? 2 : 0) | (coop ? 1 : 0);
+    switch (v) {
+    case 0: launch_one<false, false, false>(a, grid, s); break;
+    case 1: launch_one<false, false, true>(a, grid, s); break;
+    case 2: launch_one<false, true, false>(a, grid, s); break;
+    case 3: launch_one<false, true, true>(a, grid, s); break;
+    case 4: launch_one<true, false, false>(a, grid, s); break;
+    case 5: launch_one<true, false, true>(a, grid, s); break;
+    case 6: launch_one<true, true, false>(a, grid, s); break;
+    default: launch_one<true, true, true>(a, grid, s); break;
     }
     return cudaGetLastError();
 }

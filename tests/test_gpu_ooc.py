@@ -15,8 +15,8 @@ def graph(oracle, scale=13, ef=8, sym=False, cap=6000, seed=21):
 
 def run_ooc(gw, beg, csr, nblocks, slots, algo=0, maxhops=20, wps=1, p=0.5, q=2.0, alpha=0.2, term=0.0, seed=5,
             zero_copy=0, zero_threshold=0, paths=1, policy=0):
-    from oracle import oracle as O
-    vb, eb = O.split_equal_edge_mass(beg, nblocks)
+    from gowalker_b200.preprocess import split_equal_edge_mass
+    vb, eb = split_equal_edge_mass(beg, nblocks)
     maxv = int(np.diff(vb.astype(np.int64)).max())
     maxe = int(np.diff(eb.astype(np.int64)).max())
     slot = ((maxv + 2) & ~1) * 8 + ((max(maxe, 1) + 3) & ~3) * 4

@@ -129,3 +129,40 @@ def test_reference_harness_matches_oracle(oracle, tmp_path, algo):
         dead = 1 if (moves < 12 and final[1] == 0 and final[2] == 12) else 0
         assert np.array_equal(trace, rtrace), v
         assert run == moves + dead, v
+
+
+def test_product_splitters_match_oracle(oracle):
+    from gowalker_b200 import preprocess as P
+    beg, csr = oracle.rmat_graph(12, 16, seed=1)
+    for nb in (1, 3, 8, 64):
+        a = P.split_equal_edge_mass(beg, nb)
+        b = oracle.split_equal_edge_mass(beg, nb)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    for bs in (16 * 1024, 64 * 1024):
+        a = P.split_blocks(beg, bs)
+        b = oracle.split_blocks_reference(beg, bs)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_dataset_files_roundtrip(oracle, tmp_path):
+    from gowalker_b200 import preprocess as P
+    beg, csr = oracle.rmat_graph(10, 8, seed=2)
+    base = str(tmp_path / "g")
+    P.write_dataset(base, beg, csr)
+    assert os.path.getsize(base + ".meta") == 16
+    assert P.read_meta(base) == (len(beg) - 1, len(csr), 0)
+    b2, c2 = P.load_dataset(base)
+    assert np.array_equal(b2, beg) and np.array_equal(c2, csr)
+    vb, eb = P.split_equal_edge_mass(beg, 4)
+    P.write_blocks(base, 64, vb, eb)
+    v2, e2 = P.load_blocks(base, 64)
+    assert np.array_equal(v2, vb) and np.array_equal(e2, eb)
+    # oracle writer produces byte-identical files
+    base2 = str(tmp_path / "h")
+    oracle.write_dataset(base2, beg, csr)
+    for ext in (".beg", ".csr", ".meta"):
+        assert open(base + ext, "rb").read() == open(base2 + ext, "rb").read()
+    with open(base + ".meta", "wb") as f:
+        f.write(b"\0" * 5)
+    with pytest.raises(ValueError):
+        P.load_dataset(base)
