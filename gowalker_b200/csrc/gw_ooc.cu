@@ -16,6 +16,8 @@
 #include <algorithm>
 #include <cstring>
 #include <vector>
+#include <iterator>
+#include <map>
 #include "gw_engine.cuh"
 #include "gw_ooc_kernels.cuh"
 
@@ -49,7 +51,7 @@ struct OocState {
     // zero-copy: device views of the host blocks, and what we registered
     std::vector<const uint64_t *> map_beg;
     std::vector<const uint32_t *> map_csr;
-    std::vector<void *> registered;
+    std::map<uintptr_t, uintptr_t> reg;  // page ranges we registered: start -> end
     bool mapped = false;
 
     bool ready = false;
@@ -96,7 +98,7 @@ void gw_handle::ooc_release()
     if (o.h_blk_csr) cudaFreeHost((void *)o.h_blk_csr);
     if (o.h_cached) cudaFreeHost(o.h_cached);
     if (o.h_dec) cudaFreeHost(o.h_dec);
-    for (void *p : o.registered) cudaHostUnregister(p);
+    for (auto &r : o.reg) cudaHostUnregister((void *)r.first);
     delete ooc;
     ooc = nullptr;
 }
@@ -106,8 +108,8 @@ void gw_handle::ooc_invalidate()
     // host blocks changed: drop mappings so they are rebuilt on demand
     if (!ooc) return;
     cudaSetDevice(cfg.device);
-    for (void *p : ooc->registered) cudaHostUnregister(p);
-    ooc->registered.clear();
+    for (auto &r : ooc->reg) cudaHostUnregister((void *)r.first);
+    ooc->reg.clear();
     ooc->mapped = false;
 }
 
@@ -180,35 +182,80 @@ static int ooc_walkers(gw_handle *h)
     return GW_OK;
 }
 
+// Make [p, p+bytes) readable by the device at address p.  Blocks handed to
+// gw_host_block are often slices of one array: neighbouring blocks share a
+// page (their offset ranges even share an entry), and a registration may not
+// overlap an earlier one, so only the pages no registration covers yet are
+// registered.  Memory that is already pinned (cudaHostAlloc, or registered by
+// the caller) is used as it is.  Needs a device that reads registered host
+// memory at its host address (checked by the caller).
+static int map_range(gw_handle *h, OocState &o, const void *p, uint64_t bytes)
+{
+    if (!p || !bytes) return GW_OK;
+    cudaPointerAttributes a0{}, a1{};
+    const char *last = (const char *)p + bytes - 1;
+    if (cudaPointerGetAttributes(&a0, p) == cudaSuccess && a0.type == cudaMemoryTypeHost &&
+        cudaPointerGetAttributes(&a1, last) == cudaSuccess && a1.type == cudaMemoryTypeHost &&
+        a0.devicePointer == p) {
+        // both ends pinned, device address = host address: a block is one
+        // array, so one pinned allocation covers it
+        return GW_OK;
+    }
+    cudaGetLastError();
+    const uintptr_t page = 4096;
+    uintptr_t a = (uintptr_t)p & ~(page - 1);
+    const uintptr_t b = ((uintptr_t)p + bytes + page - 1) & ~(page - 1);
+    while (a < b) {
+        // skip pages inside one of our registrations
+        auto it = o.reg.upper_bound(a);
+        if (it != o.reg.begin()) {
+            auto pr = std::prev(it);
+            if (pr->second > a) {
+                a = pr->second;
+                continue;
+            }
+        }
+        uintptr_t end = b;
+        if (it != o.reg.end() && it->first < end) end = it->first;
+        // pages of the gap that somebody else already pinned are fine as they are
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, (const void *)a) == cudaSuccess && at.type == cudaMemoryTypeHost) {
+            a += page;
+            continue;
+        }
+        cudaGetLastError();
+        const cudaError_t e = cudaHostRegister((void *)a, end - a, cudaHostRegisterMapped | cudaHostRegisterReadOnly);
+        if (e == cudaErrorHostMemoryAlreadyRegistered) {
+            cudaGetLastError();  // pinned elsewhere in the range: take it page by page
+            a += page;
+            continue;
+        }
+        if (e != cudaSuccess) return h->cuda(e, "cudaHostRegister (zero-copy)");
+        o.reg[a] = end;
+        a = end;
+    }
+    return GW_OK;
+}
+
 // Map every host block for device reads (zero-copy tail).
 static int ooc_map_host(gw_handle *h)
 {
     OocState &o = *h->ooc;
     if (o.mapped) return GW_OK;
+    int direct = 0;
+    cudaDeviceGetAttribute(&direct, cudaDevAttrCanUseHostPointerForRegisteredMem, h->cfg.device);
+    if (!direct)
+        return h->fail(GW_ERR_STATE, "zero-copy needs a device that reads registered host memory at its host address");
     o.map_beg.assign(o.nb, nullptr);
     o.map_csr.assign(o.nb, nullptr);
     for (uint32_t b = 0; b < o.nb; ++b) {
         const uint64_t nv = (uint64_t)h->vblocks[b + 1] - h->vblocks[b];
         const uint64_t ne = h->eblocks[b + 1] - h->eblocks[b];
-        const void *ptrs[2] = {h->host_beg[b], h->host_csr[b]};
-        const uint64_t sizes[2] = {(nv + 1) * 8, ne * 4};
-        void *dev[2] = {nullptr, nullptr};
-        for (int k = 0; k < 2; ++k) {
-            if (!ptrs[k] || sizes[k] == 0) continue;
-            void *p = const_cast<void *>(ptrs[k]);
-            cudaError_t e = cudaHostRegister(p, sizes[k], cudaHostRegisterMapped | cudaHostRegisterReadOnly);
-            if (e == cudaSuccess) {
-                o.registered.push_back(p);
-            } else if (e == cudaErrorHostMemoryAlreadyRegistered) {
-                cudaGetLastError();
-            } else {
-                return h->cuda(e, "cudaHostRegister (zero-copy)");
-            }
-            int st = h->cuda(cudaHostGetDevicePointer(&dev[k], p, 0), "cudaHostGetDevicePointer");
-            if (st) return st;
-        }
-        o.map_beg[b] = (const uint64_t *)dev[0];
-        o.map_csr[b] = (const uint32_t *)dev[1];
+        int st;
+        if ((st = map_range(h, o, h->host_beg[b], (nv + 1) * 8))) return st;
+        if ((st = map_range(h, o, h->host_csr[b], ne * 4))) return st;
+        o.map_beg[b] = h->host_beg[b];
+        o.map_csr[b] = h->host_csr[b];
     }
     o.mapped = true;
     return GW_OK;
