@@ -22,7 +22,7 @@ EXPORTS = (
     "gw_version", "gw_status_string", "gw_config_default", "gw_create", "gw_destroy", "gw_last_error",
     "gw_set_config", "gw_stream", "gw_set_graph_meta", "gw_host_block", "gw_device_graph", "gw_cache_reset",
     "gw_init_walkers", "gw_run", "gw_num_walkers", "gw_get_paths", "gw_path_hashes", "gw_checksum",
-    "gw_bucket_counts", "gw_rmat_csr", "gw_device_free", "gw_memcpy",
+    "gw_bucket_counts", "gw_rmat_csr", "gw_device_free", "gw_memcpy", "gw_walk_noalloc",
 )
 
 
@@ -110,6 +110,8 @@ def load():
         "gw_rmat_csr": ([u32, u32, u64, u32p, u64, i32, u64, ctypes.POINTER(vp), ctypes.POINTER(vp), u64p], i32),
         "gw_device_free": ([vp], i32),
         "gw_memcpy": ([vp, vp, u64], i32),
+        "gw_walk_noalloc": ([ctypes.POINTER(GwConfig), vp, vp, u32, u64, u64, vp, vp, vp, vp,
+                             ctypes.POINTER(GwStats)], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

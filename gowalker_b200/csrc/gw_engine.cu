@@ -36,7 +36,7 @@ int gw_handle::cuda(cudaError_t e, const char *what)
     return fail(st, "%s: %s", what, cudaGetErrorString(e));
 }
 
-static void consts_from_config(const gw_config &c, StepConsts &k)
+void gw::consts_from_config(const gw_config &c, StepConsts &k)
 {
     k.maxhops = c.maxhops;
     k.key0 = (uint32_t)c.seed;

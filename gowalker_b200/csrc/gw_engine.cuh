@@ -10,6 +10,9 @@
 
 namespace gw {
 struct OocState;
+// Step constants of a configuration (fp32 thresholds computed as the
+// reference writes them, engine/engine.hpp:169-172).
+void consts_from_config(const gw_config &c, StepConsts &k);
 }
 
 struct gw_handle {

@@ -203,6 +203,41 @@ int gw_rmat_csr(uint32_t scale, uint32_t nverts, uint64_t nsamples, const uint32
 
 int gw_device_free(void *p);
 
+/* ------------------------------------------------------------------ no-allocation walk */
+
+/* No counterpart in the reference: an entry point for callers that cannot
+ * let a library allocate device memory -- a plugin whose host owns all device
+ * memory through its own pool, a runtime that forbids allocation after
+ * start-up, a host language that manages the buffers itself.
+ *
+ * Walks every walker of `cfg` (algorithm, p, q, alpha, maxhops, term_prob,
+ * seed, init_mode, walkpersource, numwalks, record_paths, blockpergrid,
+ * device) over a CSR already on the device (d_beg: nverts+1 u64 offsets,
+ * d_csr: nedges u32 ids, sorted per vertex), writing the caller's buffers:
+ * d_hashes (nwalkers u64), d_lens (nwalkers u32) and, when record_paths is
+ * GW_PATHS_FULL, d_paths (nwalkers rows of maxhops+1 u32).  The walks are the
+ * ones gw_run produces for the same configuration, bit for bit.
+ *
+ * Allocates nothing: no cudaMalloc, no cudaFree, no allocating library call.
+ * Its only other memory is a 256-byte array in the library (the run's work
+ * cursor and counters, and the error word), which every device that loads
+ * the library holds until the process exits and which this call clears
+ * before use.  That array never grows: the size limits are the walk's own --
+ * nwalkers must equal the population cfg implies and stay below 2^32 (walker
+ * ids are 32-bit), otherwise the call returns GW_ERR_ARG without touching the
+ * device.
+ *
+ * The first call on a device looks up the array's device address with that
+ * device current; make that first call before any stream capture.  The call
+ * runs on `stream` (a cudaStream_t, 0 for the default stream) and returns
+ * after the walk has finished; it first checks the CSR (GW_ERR_GRAPH if
+ * offsets are not monotone or an id is out of range).  Every call shares the
+ * one array, so calls that overlap on the same device -- from two host
+ * threads -- race: serialise them.  `stats` may be NULL. */
+int gw_walk_noalloc(const gw_config *cfg, const uint64_t *d_beg, const uint32_t *d_csr, uint32_t nverts,
+                    uint64_t nedges, uint64_t nwalkers, uint64_t *d_hashes, uint32_t *d_lens, uint32_t *d_paths,
+                    void *stream, gw_stats *stats);
+
 /* Plain copy between any two host / device pointers (cudaMemcpyDefault),
  * synchronous: lets callers without their own CUDA runtime move the buffers
  * gw_rmat_csr returns. */
