@@ -252,12 +252,14 @@ def run_ooc_bench(args, wl):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     tot = {"steps": 0, "h2d_bytes": 0, "kernel_ms": 0.0, "block_loads": 0, "iterations": 0, "launches": 0,
-           "d2h_bytes": 0, "trials": 0}
+           "d2h_bytes": 0, "trials": 0, "learned_iterations": 0, "policy_reverted": 0}
+    last = {}
     for _ in range(args.steps):
         eng.init_walkers(wl["algo"], wl["wps"], 42)
         st = eng.run(policy)
         for k in tot:
             tot[k] += st[k]
+        last = st
     hs, _ = eng.checksum()
     e1.record(stream)
     torch.cuda.synchronize()
@@ -278,6 +280,10 @@ def run_ooc_bench(args, wl):
             "h2d_bytes_per_walk_step": tot["h2d_bytes"] / max(tot["steps"], 1),
             "block_loads_per_run": tot["block_loads"] / args.steps,
             "iterations_per_run": tot["iterations"] / args.steps,
+            "learned": {"iterations_per_run": tot["learned_iterations"] / args.steps,
+                        "reverted_runs": tot["policy_reverted"], "train_loss": last.get("train_loss"),
+                        "pred_error": last.get("pred_error")},
+            "trials_per_step": tot["trials"] / max(tot["steps"], 1),
             "roofline": {"bound": "host-link", "achieved": link, "peak": PCIE_GEN5_X16_GBS, "unit": "GB/s",
                          "frac": link / PCIE_GEN5_X16_GBS, "traffic": None,
                          "kernel_ms_per_run": tot["kernel_ms"] / args.steps},
@@ -339,11 +345,15 @@ def run_ours(args, wl):
     steps = 0
     kernel_ms = 0.0
     launches = 0
+    trials = 0
+    variant = -1
     for _ in range(args.steps):
         eng.init_walkers(wl["algo"], wl["wps"], seed)
         st = eng.run()
         steps += st["steps"]
         kernel_ms += st["kernel_ms"]
+        trials += st["trials"]
+        variant = st["kernel_variant"]
         launches += st["launches"]
     e1.record(stream)
     barrier()
@@ -410,6 +420,8 @@ def run_ours(args, wl):
             "e2e": {"value": e2e_all / (ms2 / 1000.0), "unit": "steps/s",
                     "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps},
             "checksum": {"path_hash_sum": hash_sum, "steps_per_run": steps_last},
+            "trials_per_step": trials / max(steps, 1),
+            "kernel_variant": variant,
         }
         if clk:
             line["clocks"] = clk

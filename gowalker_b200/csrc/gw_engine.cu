@@ -5,6 +5,7 @@
 // creation of engine/walk.hpp:272-389.  Every failure returns a status and
 // records a message; nothing exits the process.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -454,8 +455,6 @@ int gw_handle::run_incore(gw_stats *stats)
                         (unsigned long long)ends[0], (unsigned long long)ends[1]);
         validated = true;
     }
-    if ((st = cuda(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * kCtrCount, s), "memset"))) return st;
-
     IncoreArgs a{};
     consts_from_config(cfg, a.c);
     a.init.mode = cfg.init_mode;
@@ -477,10 +476,42 @@ int gw_handle::run_incore(gw_stats *stats)
     a.err = d_err;
     const bool sopr = cfg.algorithm != GW_NODE2VEC;
     const bool coop = needs_coop(cfg.algorithm, a.c);
+    const int combo = (sopr ? 4 : 0) | (a.paths ? 2 : 0) | (coop ? 1 : 0);
+    int variant = tuned_variant[combo];
+    if (cfg.blockpergrid == 0 && variant < 0) {
+        // Autotuner: time each register-cap variant on one slice of this
+        // run's walkers (their outputs are rewritten by the full run below)
+        // and keep the fastest for every later run of this kernel class.
+        const uint64_t ns = std::min<uint64_t>(nwalkers, std::max<uint64_t>((uint64_t)num_sms * 4096, nwalkers / 16));
+        IncoreArgs c = a;
+        c.wid_base = (uint32_t)((nwalkers - ns) * 3 / 8);
+        c.nwalkers = (uint32_t)ns;
+        float best = 1e30f;
+        for (int v = 0; v < kIncoreVariants; ++v) {
+            if ((st = cuda(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * kCtrCount, s), "memset"))) return st;
+            if ((st = cuda(cudaEventRecord(ev_kernel0, s), "event"))) return st;
+            if ((st = cuda(launch_walk_incore(c, sopr, coop, v, incore_grid(sopr, c.paths != nullptr, coop, v, num_sms), s),
+                           "walk kernel launch (tuning)")))
+                return st;
+            if ((st = cuda(cudaEventRecord(ev_kernel1, s), "event"))) return st;
+            if ((st = cuda(cudaEventSynchronize(ev_kernel1), "tuning"))) return st;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev_kernel0, ev_kernel1);
+            tuned_ms[combo][v] = ms;
+            if (ms < best) {
+                best = ms;
+                variant = v;
+            }
+        }
+        tuned_variant[combo] = variant;
+    }
+    if (variant < 0) variant = 1;
+    last_variant = variant;
+    if ((st = cuda(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * kCtrCount, s), "memset"))) return st;
     int grid = (int)cfg.blockpergrid;
-    if (grid <= 0) grid = incore_grid(sopr, a.paths != nullptr, coop, num_sms);
+    if (grid <= 0) grid = incore_grid(sopr, a.paths != nullptr, coop, variant, num_sms);
     if ((st = cuda(cudaEventRecord(ev_kernel0, s), "event"))) return st;
-    if ((st = cuda(launch_walk_incore(a, sopr, coop, grid, s), "walk kernel launch"))) return st;
+    if ((st = cuda(launch_walk_incore(a, sopr, coop, variant, grid, s), "walk kernel launch"))) return st;
     if ((st = cuda(cudaEventRecord(ev_kernel1, s), "event"))) return st;
     if ((st = cuda(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(unsigned long long) * kCtrCount, cudaMemcpyDeviceToHost, s),
                    "counters D2H")))
@@ -503,6 +534,7 @@ int gw_handle::run_incore(gw_stats *stats)
         stats->block_loads = h2d ? nblocks : 0;
         stats->iterations = 1;
         stats->launches = 1;
+        stats->kernel_variant = (uint32_t)variant;
         cudaEventElapsedTime(&stats->kernel_ms, ev_kernel0, ev_kernel1);
         cudaEventElapsedTime(&stats->total_ms, ev_start, ev_stop);
     }

@@ -63,6 +63,12 @@ struct gw_handle {
     uint64_t last_hash_sum = 0;
     uint64_t last_steps = 0;
 
+    // autotuner: best register-cap variant per in-core kernel class
+    // (sopr, paths, coop) and the measured times of each variant
+    int tuned_variant[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+    float tuned_ms[8][gw::kIncoreVariants] = {};
+    int last_variant = -1;
+
     // out-of-core state (gw_ooc.cu)
     gw::OocState *ooc = nullptr;
 

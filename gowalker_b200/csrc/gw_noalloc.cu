@@ -127,8 +127,10 @@ extern "C" int gw_walk_noalloc(const gw_config *cfg, const uint64_t *d_beg, cons
     a.err = err;
     const bool sopr = cfg->algorithm != GW_NODE2VEC;
     const bool coop = needs_coop(cfg->algorithm, a.c);
-    const int grid = cfg->blockpergrid ? (int)cfg->blockpergrid : incore_grid(sopr, a.paths != nullptr, coop, num_sms);
-    e = launch_walk_incore(a, sopr, coop, grid, s);
+    const int variant = 1;  // 4 CTAs per SM; this entry point keeps no tuning state
+    const int grid =
+        cfg->blockpergrid ? (int)cfg->blockpergrid : incore_grid(sopr, a.paths != nullptr, coop, variant, num_sms);
+    e = launch_walk_incore(a, sopr, coop, variant, grid, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(host_ctr, ctr, sizeof(host_ctr), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {

@@ -20,6 +20,8 @@
 #include <map>
 #include "gw_engine.cuh"
 #include "gw_ooc_kernels.cuh"
+#include "gw_mlp.cuh"
+#include <cmath>
 
 namespace gw {
 
@@ -55,7 +57,28 @@ struct OocState {
     bool mapped = false;
 
     bool ready = false;
+
+    // learned policy (gw_mlp.cu kernels): model, training traces, features
+    bool learned_ready = false, trained = false;
+    float train_loss = 0.f;
+    float *d_params = nullptr, *d_train_ws = nullptr;
+    float *d_trace_x = nullptr, *d_trace_col = nullptr, *d_trace_y = nullptr;
+    float *d_feat_x = nullptr, *d_feat_col = nullptr, *d_pred = nullptr;
+    float *d_emass = nullptr, *d_vfrac = nullptr, *d_prev_col = nullptr, *d_ema = nullptr;
+    int32_t *d_choose = nullptr, *h_choose = nullptr;
+    float *h_pred = nullptr, *h_col = nullptr;
 };
+
+// Learned policy constants: traces of 20 plain iterations (+3 of horizon for
+// the targets) train the predictor; it then loads up to 4 blocks per
+// iteration, swapping a resident block out only for one whose predicted demand
+// is higher by `kSwapMargin` (log1p scale).
+constexpr uint32_t kTraceIters = 20;
+constexpr uint32_t kHorizon = 3;
+constexpr uint32_t kMaxLoadsPerIter = 4;
+constexpr float kSwapMargin = 0.25f;
+constexpr uint32_t kTrainEpochs = 400;
+constexpr float kTrainLr = 3e-3f;
 
 __global__ void k_validate_block(const uint64_t *beg, const uint32_t *csr, uint32_t nv, uint64_t e0, uint64_t e1,
                                  uint32_t nverts, uint32_t *err)
@@ -99,8 +122,52 @@ void gw_handle::ooc_release()
     if (o.h_cached) cudaFreeHost(o.h_cached);
     if (o.h_dec) cudaFreeHost(o.h_dec);
     for (auto &r : o.reg) cudaHostUnregister((void *)r.first);
+    for (float *p : {o.d_params, o.d_train_ws, o.d_trace_x, o.d_trace_col, o.d_trace_y, o.d_feat_x, o.d_feat_col,
+                     o.d_pred, o.d_emass, o.d_vfrac, o.d_prev_col, o.d_ema})
+        cudaFree(p);
+    cudaFree(o.d_choose);
+    if (o.h_choose) cudaFreeHost(o.h_choose);
+    if (o.h_pred) cudaFreeHost(o.h_pred);
+    if (o.h_col) cudaFreeHost(o.h_col);
     delete ooc;
     ooc = nullptr;
+}
+
+static int learned_setup(gw_handle *h)
+{
+    OocState &o = *h->ooc;
+    if (o.learned_ready) return GW_OK;
+    const uint32_t nb = o.nb;
+    int st;
+    auto dalloc = [&](float **p, uint64_t n, const char *what) { return h->cuda(cudaMalloc(p, n * sizeof(float)), what); };
+    if ((st = dalloc(&o.d_params, kMlpParams, "predictor weights"))) return st;
+    if ((st = dalloc(&o.d_train_ws, (uint64_t)kMlpGradCtas * (kMlpParams + 1) + 3 * kMlpParams + 1, "training state")))
+        return st;
+    if ((st = dalloc(&o.d_trace_x, (uint64_t)kTraceIters * nb * kMlpIn, "traces"))) return st;
+    if ((st = dalloc(&o.d_trace_col, (uint64_t)(kTraceIters + kHorizon) * nb, "traces"))) return st;
+    if ((st = dalloc(&o.d_trace_y, (uint64_t)kTraceIters * nb, "targets"))) return st;
+    if ((st = dalloc(&o.d_feat_x, (uint64_t)nb * kMlpIn, "features"))) return st;
+    if ((st = dalloc(&o.d_feat_col, nb, "demand"))) return st;
+    if ((st = dalloc(&o.d_pred, nb, "predictions"))) return st;
+    if ((st = dalloc(&o.d_emass, nb, "edge shares"))) return st;
+    if ((st = dalloc(&o.d_vfrac, nb, "vertex shares"))) return st;
+    if ((st = dalloc(&o.d_prev_col, nb, "history"))) return st;
+    if ((st = dalloc(&o.d_ema, nb, "history"))) return st;
+    if ((st = h->cuda(cudaMalloc(&o.d_choose, sizeof(int32_t) * (2 * kMaxLoadsPerIter + 1)), "choice"))) return st;
+    if ((st = h->cuda(cudaMallocHost(&o.h_choose, sizeof(int32_t) * (2 * kMaxLoadsPerIter + 1)), "choice"))) return st;
+    if ((st = h->cuda(cudaMallocHost(&o.h_pred, sizeof(float) * nb), "predictions"))) return st;
+    if ((st = h->cuda(cudaMallocHost(&o.h_col, sizeof(float) * nb), "demand"))) return st;
+    std::vector<float> em(nb), vf(nb);
+    for (uint32_t b = 0; b < nb; ++b) {
+        em[b] = h->nedges ? (float)((double)(h->eblocks[b + 1] - h->eblocks[b]) / (double)h->nedges * nb) : 0.f;
+        vf[b] = (float)((double)(h->vblocks[b + 1] - h->vblocks[b]) / (double)h->nverts * nb);
+    }
+    if ((st = h->cuda(cudaMemcpy(o.d_emass, em.data(), sizeof(float) * nb, cudaMemcpyHostToDevice), "edge shares")))
+        return st;
+    if ((st = h->cuda(cudaMemcpy(o.d_vfrac, vf.data(), sizeof(float) * nb, cudaMemcpyHostToDevice), "vertex shares")))
+        return st;
+    o.learned_ready = true;
+    return GW_OK;
 }
 
 void gw_handle::ooc_invalidate()
@@ -383,25 +450,87 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
 
     const uint32_t kMaxIters = 1u << 20;
     bool done = false;
+    // learned-policy state of this run
+    if (policy == GW_POLICY_LEARNED && (st = learned_setup(this))) {
+        cudaEventDestroy(k0);
+        cudaEventDestroy(k1);
+        return st;
+    }
+    if (policy == GW_POLICY_LEARNED) {
+        if ((st = cuda(cudaMemsetAsync(o.d_prev_col, 0, sizeof(float) * nb, s), "memset")) ||
+            (st = cuda(cudaMemsetAsync(o.d_ema, 0, sizeof(float) * nb, s), "memset"))) {
+            cudaEventDestroy(k0);
+            cudaEventDestroy(k1);
+            return st;
+        }
+    }
+    uint32_t trace_t = 0, learned_iters = 0;
+    bool reverted = false, have_prev_pred = false;
+    uint64_t learned_steps = 0, learned_bytes = 0, plain_steps = 0, plain_bytes = 0;
+    uint64_t phase_steps_mark = 0, phase_bytes_mark = 0;
+    int last_phase = -1;
+    double pred_err_sum = 0.0;
+    uint32_t pred_err_n = 0;
+    std::vector<float> prev_pred;
     while (!done) {
         if (++iters > kMaxIters) {
             st = fail(GW_ERR_STATE, "out-of-core run exceeded %u scheduler iterations", kMaxIters);
             break;
         }
-        // ---- block choice on the device, decision read back
         const uint32_t ncached = (uint32_t)o.cached.size();
         for (uint32_t j = 0; j < ncached; ++j) o.h_cached[j] = o.cached[j];
         if (ncached &&
             (st = cuda(cudaMemcpyAsync(o.d_cached, o.h_cached, ncached * sizeof(uint32_t), cudaMemcpyHostToDevice, s),
                        "cached list")))
             break;
-        (void)policy;
+        // ---- learned policy: features (traces while training), prediction, choice
+        const bool learned = policy == GW_POLICY_LEARNED;
+        const bool learned_active = learned && o.trained && !reverted;
+        const bool tracing = learned && !o.trained && trace_t < kTraceIters + kHorizon;
+        if (learned_active || tracing) {
+            FeatureArgs f{};
+            f.counts = o.d_counts;
+            f.blk_beg = o.d_blk_beg;
+            f.emass = o.d_emass;
+            f.vfrac = o.d_vfrac;
+            f.prev_col = o.d_prev_col;
+            f.ema_arr = o.d_ema;
+            f.nb = nb;
+            f.iter = iters;
+            f.live_frac = (float)nlive / (float)nwalkers;
+            f.inv_live = nlive ? 1.f / (float)nlive : 0.f;
+            f.x = tracing ? o.d_trace_x + (uint64_t)std::min(trace_t, kTraceIters - 1) * nb * kMlpIn : o.d_feat_x;
+            f.col = tracing ? o.d_trace_col + (uint64_t)trace_t * nb : o.d_feat_col;
+            if ((st = cuda(launch_features(f, s), "features"))) break;
+            launches++;
+            if (learned_active) {
+                if ((st = cuda(mlp_forward(o.d_params, o.d_feat_x, nb, o.d_pred, s), "predictor"))) break;
+                if ((st = cuda(launch_learned_choose(o.d_pred, nb, o.d_blk_beg, o.d_cached, ncached,
+                                                     o.nslots, kMaxLoadsPerIter, kSwapMargin, o.d_choose, s),
+                               "learned choice")))
+                    break;
+                launches += 2;
+                if ((st = cuda(cudaMemcpyAsync(o.h_choose, o.d_choose, sizeof(int32_t) * (2 * kMaxLoadsPerIter + 1),
+                                               cudaMemcpyDeviceToHost, s), "choice")))
+                    break;
+                if ((st = cuda(cudaMemcpyAsync(o.h_pred, o.d_pred, sizeof(float) * nb, cudaMemcpyDeviceToHost, s),
+                               "predictions")))
+                    break;
+                if ((st = cuda(cudaMemcpyAsync(o.h_col, o.d_feat_col, sizeof(float) * nb, cudaMemcpyDeviceToHost, s),
+                               "demand")))
+                    break;
+            }
+        }
+        // ---- plain block choice on the device (decision, fallback and rescue), read back
         if ((st = cuda(launch_schedule(o.d_counts, o.d_offsets, nb, o.d_cached, ncached, o.nslots, cfg.zero_threshold,
                                        nullptr, 0.f, o.d_dec, s),
                        "schedule")))
             break;
         launches++;
         if ((st = cuda(cudaMemcpyAsync(o.h_dec, o.d_dec, sizeof(Decision), cudaMemcpyDeviceToHost, s), "decision")))
+            break;
+        if ((st = cuda(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(unsigned long long) * kCtrCount, cudaMemcpyDeviceToHost, s),
+                       "counters")))
             break;
         if ((st = cuda(cudaMemcpyAsync(h_ctr + kCtrCount, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
                        "error word")))
@@ -417,13 +546,47 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             break;
         }
         const Decision d = *o.h_dec;
+        // judge: host-link bytes per step of each policy since it took over
+        const uint64_t steps_now = h_ctr[kCtrSteps];
+        if (last_phase >= 0) {
+            const uint64_t ds = steps_now - phase_steps_mark, db = h2d - phase_bytes_mark;
+            if (last_phase == 1) {
+                learned_steps += ds;
+                learned_bytes += db;
+            } else if (o.cached.size() >= o.nslots) {
+                plain_steps += ds;
+                plain_bytes += db;
+            }
+        }
+        phase_steps_mark = steps_now;
+        phase_bytes_mark = h2d;
+        last_phase = -1;
+        if (learned_active) {
+            // observed demand vs the previous iteration's prediction
+            if (have_prev_pred) {
+                double e = 0.0;
+                for (uint32_t i = 0; i < nb; ++i) e += std::fabs(prev_pred[i] - std::log1p((double)o.h_col[i]));
+                pred_err_sum += e / nb;
+                pred_err_n++;
+            }
+            prev_pred.assign(o.h_pred, o.h_pred + nb);
+            have_prev_pred = true;
+            if (learned_iters >= 16 && plain_steps > 0 && learned_steps > 0 &&
+                (double)learned_bytes / (double)learned_steps > (double)plain_bytes / (double)plain_steps) {
+                reverted = true;  // the judge: learned moves more bytes per step than the plain rule
+            }
+        }
         nlive = d.live;
         if (nlive == 0) break;
 
-        int load_block = -1, position = -1;
-        if (d.action == 1 || d.action == 2) {
-            load_block = d.block;
-            position = d.action == 2 ? d.position : -1;
+        std::vector<std::pair<int, int>> todo;  // (block, cached position or -1)
+        if (learned_active && !reverted && o.h_choose[0] > 0) {
+            for (int k = 0; k < o.h_choose[0]; ++k) todo.emplace_back(o.h_choose[1 + 2 * k], o.h_choose[2 + 2 * k]);
+            learned_iters++;
+            last_phase = 1;
+        } else if (d.action == 1 || d.action == 2) {
+            todo.emplace_back(d.block, d.action == 2 ? d.position : -1);
+            last_phase = 0;
         } else if (cfg.zero_copy) {
             // ---- zero-copy tail: every absent block read through mapped host memory
             if ((st = ooc_map_host(this))) break;
@@ -434,9 +597,6 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 }
             if ((st = push_tables())) break;
             unsigned long long before[kCtrCount];
-            if ((st = cuda(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(before), cudaMemcpyDeviceToHost, s), "counters")))
-                break;
-            if ((st = cuda(cudaStreamSynchronize(s), "counters"))) break;
             memcpy(before, h_ctr, sizeof(before));
             if ((st = step())) break;
             if ((st = cuda(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(before), cudaMemcpyDeviceToHost, s), "counters")))
@@ -457,56 +617,81 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             done = true;
             break;
         } else if (d.rescue_block >= 0 && (o.cached.size() < o.nslots || d.rescue_position >= 0)) {
-            load_block = d.rescue_block;
-            position = (o.cached.size() >= o.nslots) ? d.rescue_position : -1;
+            todo.emplace_back(d.rescue_block, (o.cached.size() >= o.nslots) ? d.rescue_position : -1);
+            last_phase = 0;
         } else {
             st = fail(GW_ERR_STATE, "no block can make progress (%u live walkers)", (unsigned)nlive);
             break;
         }
 
-        // ---- load the chosen block into a slot
-        int slot = -1;
-        if (position >= 0) {
-            const uint32_t victim = o.cached[position];
-            slot = o.block_slot[victim];
-            o.block_slot[victim] = -1;
-            o.h_blk_beg[victim] = nullptr;
-            o.h_blk_csr[victim] = nullptr;
-            o.cached[position] = (uint32_t)load_block;
-        } else {
-            for (uint32_t k = 0; k < o.nslots; ++k)
-                if (o.slot_block[k] < 0) {
-                    slot = (int)k;
-                    break;
-                }
-            o.cached.push_back((uint32_t)load_block);
+        // ---- load the chosen blocks into slots
+        for (const auto &ld : todo) {
+            const int load_block = ld.first, position = ld.second;
+            int slot = -1;
+            if (position >= 0) {
+                const uint32_t victim = o.cached[position];
+                slot = o.block_slot[victim];
+                o.block_slot[victim] = -1;
+                o.h_blk_beg[victim] = nullptr;
+                o.h_blk_csr[victim] = nullptr;
+                o.cached[position] = (uint32_t)load_block;
+            } else {
+                for (uint32_t k = 0; k < o.nslots; ++k)
+                    if (o.slot_block[k] < 0) {
+                        slot = (int)k;
+                        break;
+                    }
+                o.cached.push_back((uint32_t)load_block);
+            }
+            if (slot < 0) {
+                st = fail(GW_ERR_STATE, "no free cache slot");
+                break;
+            }
+            const uint32_t b = (uint32_t)load_block;
+            const uint64_t nv = (uint64_t)vblocks[b + 1] - vblocks[b];
+            const uint64_t ne = eblocks[b + 1] - eblocks[b];
+            uint64_t *sb = o.slot_beg + (uint64_t)slot * o.slot_beg_words;
+            uint32_t *sc = o.slot_csr + (uint64_t)slot * o.slot_csr_words;
+            if ((st = cuda(cudaMemcpyAsync(sb, host_beg[b], (nv + 1) * 8, cudaMemcpyHostToDevice, s), "block offsets")))
+                break;
+            if (ne &&
+                (st = cuda(cudaMemcpyAsync(sc, host_csr[b], ne * 4, cudaMemcpyHostToDevice, s), "block neighbours")))
+                break;
+            h2d += (nv + 1) * 8 + ne * 4;
+            loads++;
+            k_validate_block<<<num_sms * 4, 256, 0, s>>>(sb, sc, (uint32_t)nv, eblocks[b], eblocks[b + 1], nverts,
+                                                         d_err);
+            launches++;
+            o.slot_block[slot] = (int)b;
+            o.block_slot[b] = slot;
+            o.h_blk_beg[b] = sb;
+            o.h_blk_csr[b] = sc;
         }
-        if (slot < 0) {
-            st = fail(GW_ERR_STATE, "no free cache slot");
-            break;
-        }
-        const uint32_t b = (uint32_t)load_block;
-        const uint64_t nv = (uint64_t)vblocks[b + 1] - vblocks[b];
-        const uint64_t ne = eblocks[b + 1] - eblocks[b];
-        uint64_t *sb = o.slot_beg + (uint64_t)slot * o.slot_beg_words;
-        uint32_t *sc = o.slot_csr + (uint64_t)slot * o.slot_csr_words;
-        if ((st = cuda(cudaMemcpyAsync(sb, host_beg[b], (nv + 1) * 8, cudaMemcpyHostToDevice, s), "block offsets")))
-            break;
-        if (ne && (st = cuda(cudaMemcpyAsync(sc, host_csr[b], ne * 4, cudaMemcpyHostToDevice, s), "block neighbours")))
-            break;
-        h2d += (nv + 1) * 8 + ne * 4;
-        loads++;
-        k_validate_block<<<num_sms * 4, 256, 0, s>>>(sb, sc, (uint32_t)nv, eblocks[b], eblocks[b + 1], nverts, d_err);
-        launches++;
-        o.slot_block[slot] = (int)b;
-        o.block_slot[b] = slot;
-        o.h_blk_beg[b] = sb;
-        o.h_blk_csr[b] = sc;
+        if (st) break;
         if ((st = push_tables())) break;
 
         // ---- walk every runnable bucket, then re-bucket
         if ((st = step())) break;
         if ((st = bucketize(nlive))) break;
+
+        // ---- predictor training after kTraceIters + kHorizon traced iterations
+        if (tracing) {
+            trace_t++;
+            if (trace_t == kTraceIters + kHorizon) {
+                if ((st = cuda(launch_targets(o.d_trace_col, kTraceIters, kHorizon, nb, o.d_trace_y, s), "targets")))
+                    break;
+                if ((st = cuda(mlp_train(o.d_params, o.d_trace_x, o.d_trace_y, kTraceIters * nb, kTrainEpochs,
+                                         kTrainLr, 0x6C6561726E6564ull, o.d_train_ws, nullptr, s),
+                               "predictor training")))
+                    break;
+                const float *loss_dev = o.d_train_ws + (uint64_t)kMlpGradCtas * (kMlpParams + 1) + 3 * kMlpParams;
+                if ((st = cuda(cudaMemcpyAsync(&o.train_loss, loss_dev, sizeof(float), cudaMemcpyDeviceToHost, s),
+                               "loss")))
+                    break;
+                launches += 2 + 3 * kTrainEpochs;
+                o.trained = true;
+            }
+        }
     }
     if (st == GW_OK) {
         if ((st = cuda(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(unsigned long long) * kCtrCount, cudaMemcpyDeviceToHost, s),
@@ -536,6 +721,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         stats->launches = launches;
         stats->kernel_ms = kernel_ms;
         cudaEventElapsedTime(&stats->total_ms, ev_start, ev_stop);
+        stats->learned_iterations = learned_iters;
+        stats->policy_reverted = reverted ? 1u : 0u;
+        stats->train_loss = (policy == GW_POLICY_LEARNED) ? o.train_loss : 0.f;
+        stats->pred_error = pred_err_n ? (float)(pred_err_sum / pred_err_n) : 0.f;
     }
     const uint32_t errw = (uint32_t)h_ctr[kCtrCount];
     if (errw) return fail(GW_ERR_DEVICE, "kernel error word 0x%x", errw);

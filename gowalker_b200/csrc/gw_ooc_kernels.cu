@@ -497,6 +497,137 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const OocStepArgs a)
     }
 }
 
+// ------------------------------------------------------------------ learned policy
+
+// Per-block features of the demand predictor (all log1p-scaled counts):
+//  0 waiting at i (cur block i)   1 leaving i (prev block i)   2 diagonal (i,i)
+//  3 walkers between i and resident blocks   4 walkers that run if i is resident
+//  5 resident   6 edge share   7 vertex share   8 arrival EMA   9 arrivals
+// 10 live fraction  11 iteration/256  12 waiting share  13 incident
+// 14 leaving, off-diagonal  15 waiting, off-diagonal
+__global__ void __launch_bounds__(1024) k_features(const FeatureArgs f)
+{
+    __shared__ uint8_t s_res[kMaxBlocks];
+    const uint32_t nb = f.nb;
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) s_res[i] = f.blk_beg[i] != nullptr;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+        uint64_t col = 0, row = 0, cross = 0, ready = 0;
+        for (uint32_t p = 0; p < nb; ++p) {
+            const uint32_t cpi = f.counts[p * nb + i], cip = f.counts[i * nb + p];
+            col += cpi;
+            row += cip;
+            if (s_res[p]) cross += (uint64_t)cpi + cip;
+            if (s_res[p] || p == i) ready += cpi;
+        }
+        const uint32_t diag = f.counts[i * nb + i];
+        const float colf = (float)col;
+        const float arr = fmaxf(colf - f.prev_col[i], 0.f);
+        const float ema = 0.7f * f.ema_arr[i] + 0.3f * arr;
+        f.prev_col[i] = colf;
+        f.ema_arr[i] = ema;
+        float *x = f.x + (uint64_t)i * 16;
+        x[0] = log1pf(colf);
+        x[1] = log1pf((float)row);
+        x[2] = log1pf((float)diag);
+        x[3] = log1pf((float)cross);
+        x[4] = log1pf((float)ready);
+        x[5] = s_res[i] ? 1.f : 0.f;
+        x[6] = f.emass[i];
+        x[7] = f.vfrac[i];
+        x[8] = log1pf(ema);
+        x[9] = log1pf(arr);
+        x[10] = f.live_frac;
+        x[11] = fminf((float)f.iter, 256.f) * (1.f / 256.f);
+        x[12] = colf * f.inv_live * (float)nb;
+        x[13] = log1pf((float)(row + col - diag));
+        x[14] = log1pf((float)(row - diag));
+        x[15] = log1pf((float)(col - diag));
+        f.col[i] = colf;
+    }
+}
+
+__global__ void k_targets(const float *col_hist, uint32_t T, uint32_t k, uint32_t nb, float *y)
+{
+    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= T * nb) return;
+    const uint32_t t = idx / nb, i = idx % nb;
+    float s = 0.f;
+    for (uint32_t d = 1; d <= k; ++d) s += col_hist[(uint64_t)(t + d) * nb + i];
+    y[idx] = log1pf(s / (float)k);
+}
+
+// One thread: fill free slots with the highest predicted uncached blocks, then
+// swap while the best uncached block's predicted demand beats the worst
+// resident one's by `margin` (log scale); blocks chosen this round stay.
+__global__ void k_learned_choose(const float *__restrict__ pred, uint32_t nb, const uint64_t *const *blk_beg,
+                                 const uint32_t *__restrict__ cached, uint32_t ncached, uint32_t nslots,
+                                 uint32_t lmax, float margin, int32_t *out)
+{
+    __shared__ uint8_t s_state[kMaxBlocks];  // 0 absent, 1 resident, 2 chosen now, 3 evicted now
+    __shared__ int32_t s_pos[kMaxBlocks];
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+        s_state[i] = blk_beg[i] != nullptr ? 1 : 0;
+        s_pos[i] = -1;
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < ncached; j += blockDim.x) s_pos[cached[j]] = (int32_t)j;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    uint32_t n = 0, used = ncached;
+    while (n < lmax) {
+        int bi = -1;
+        float bp = -1e30f;
+        for (uint32_t i = 0; i < nb; ++i)
+            if (s_state[i] == 0 && pred[i] > bp) {
+                bp = pred[i];
+                bi = (int)i;
+            }
+        if (bi < 0 || bp <= 0.05f) break;  // nothing worth a copy
+        int32_t pos = -1;
+        if (used >= nslots) {
+            int wj = -1;
+            float wp = 1e30f;
+            for (uint32_t i = 0; i < nb; ++i)
+                if (s_state[i] == 1 && s_pos[i] >= 0 && pred[i] < wp) {
+                    wp = pred[i];
+                    wj = (int)i;
+                }
+            if (wj < 0 || bp <= wp + margin) break;
+            pos = s_pos[wj];
+            s_state[wj] = 3;
+        } else {
+            used++;
+        }
+        s_state[bi] = 2;
+        out[1 + 2 * n] = bi;
+        out[2 + 2 * n] = pos;
+        n++;
+    }
+    out[0] = (int32_t)n;
+}
+
+cudaError_t launch_features(const FeatureArgs &f, cudaStream_t s)
+{
+    k_features<<<1, 1024, 0, s>>>(f);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_targets(const float *col_hist, uint32_t T, uint32_t k, uint32_t nb, float *y, cudaStream_t s)
+{
+    const uint32_t n = T * nb;
+    k_targets<<<(n + 255) / 256, 256, 0, s>>>(col_hist, T, k, nb, y);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_learned_choose(const float *pred, uint32_t nb, const uint64_t *const *blk_beg,
+                                  const uint32_t *cached, uint32_t ncached, uint32_t nslots, uint32_t lmax,
+                                  float margin, int32_t *out, cudaStream_t s)
+{
+    k_learned_choose<<<1, 256, 0, s>>>(pred, nb, blk_beg, cached, ncached, nslots, lmax, margin, out);
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ launchers
 
 cudaError_t launch_init_walkers(const WalkerInit &in, const uint32_t *vstart, uint32_t nb, uint64_t n,

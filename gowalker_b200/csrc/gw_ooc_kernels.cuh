@@ -62,6 +62,27 @@ cudaError_t launch_runnable(const uint32_t *counts, const uint32_t *offsets, con
 cudaError_t launch_schedule(const uint32_t *counts, const uint32_t *offsets, uint32_t nb, const uint32_t *cached,
                             uint32_t ncached, uint32_t nslots, uint32_t zero_threshold, const float *pred,
                             float pred_weight, Decision *out, cudaStream_t s);
+// ---- learned policy: per-block features, training targets, decisions
+
+struct FeatureArgs {
+    const uint32_t *counts;            // [nb*nb] bucket counts after the last bucketing
+    const uint64_t *const *blk_beg;    // residency (non-null = resident)
+    const float *emass, *vfrac;        // edge / vertex share of each block, times nb
+    float *prev_col, *ema_arr;         // per-block history, updated in place
+    uint32_t nb, iter;
+    float live_frac, inv_live;
+    float *x;                          // [nb][16] features out
+    float *col;                        // [nb] walkers waiting with cur block = i (demand) out
+};
+cudaError_t launch_features(const FeatureArgs &f, cudaStream_t s);
+// y[t][i] = log1p(mean over t' in (t, t+k] of col_hist[t'][i]) for t < T
+cudaError_t launch_targets(const float *col_hist, uint32_t T, uint32_t k, uint32_t nb, float *y, cudaStream_t s);
+// Up to lmax (block, cached position or -1 for a free slot) pairs by
+// predicted demand; out[0] = count, then the pairs.
+cudaError_t launch_learned_choose(const float *pred, uint32_t nb, const uint64_t *const *blk_beg,
+                                  const uint32_t *cached, uint32_t ncached, uint32_t nslots, uint32_t lmax,
+                                  float margin, int32_t *out, cudaStream_t s);
+
 int ooc_grid(bool sopr, bool paths, bool coop, int num_sms);
 cudaError_t launch_walk_ooc(const OocStepArgs &a, bool sopr, bool coop, int grid, cudaStream_t s);
 

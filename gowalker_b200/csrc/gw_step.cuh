@@ -187,43 +187,46 @@ __device__ __forceinline__ uint32_t warp_first_accept_runs(const StepConsts &c, 
     }
     __syncwarp();
     const uint32_t plo = __shfl_sync(0xFFFFFFFFu, lo, (int)pdeg), phi = __shfl_sync(0xFFFFFFFFu, hi, (int)pdeg);
-    for (uint32_t base = p0; base < limit; base += 32) {
-        const uint32_t att = base + lane;
-        bool acc = false;
-        uint32_t pos = 0;
-        if (att < limit) {
-            const U4 r = draw(c, wid, hop, att);
-            pos = r.x % deg;
-            const float rv = rand_val(r.y, t.maxv);
-            if (rv <= t.minv) {
-                acc = true;
-            } else if (pos >= plo && pos < phi) {
-                if constexpr (SOPR) acc = (double)rv < t.t_prev_d;
-                else acc = rv < t.t_prev;
+    // verdict of attempt `att` from its draw alone
+    auto judge = [&](uint32_t att, uint32_t &pos) -> bool {
+        if (att >= limit) return false;
+        const U4 r = draw(c, wid, hop, att);
+        pos = r.x % deg;
+        const float rv = rand_val(r.y, t.maxv);
+        if (rv <= t.minv) return true;
+        if (pos >= plo && pos < phi) {
+            if constexpr (SOPR) return (double)rv < t.t_prev_d;
+            else return rv < t.t_prev;
+        }
+        // last run whose start is <= pos (runs are in N(prev) order, so sorted)
+        int k = -1;
+        uint32_t a = 0, b = pdeg;
+        while (a < b) {
+            const uint32_t m = (a + b) >> 1;
+            if (iv[m] <= pos) {
+                k = (int)m;
+                a = m + 1;
             } else {
-                // last run whose start is <= pos (runs are in N(prev) order, so sorted)
-                int k = -1;
-                uint32_t a = 0, b = pdeg;
-                while (a < b) {
-                    const uint32_t m = (a + b) >> 1;
-                    if (iv[m] <= pos) {
-                        k = (int)m;
-                        a = m + 1;
-                    } else {
-                        b = m;
-                    }
-                }
-                const bool found = k >= 0 && pos < iv[32 + k];
-                acc = found ? (rv < t.t_found) : (rv < t.t_notfound);
+                b = m;
             }
         }
-        const unsigned m = __ballot_sync(0xFFFFFFFFu, acc);
-        if (m) {
-            const int f = __ffs(m) - 1;
-            const uint32_t pf = __shfl_sync(0xFFFFFFFFu, pos, f);
+        const bool found = k >= 0 && pos < iv[32 + k];
+        return found ? (rv < t.t_found) : (rv < t.t_notfound);
+    };
+    // 64 attempts per round, two independent Philox chains per lane
+    for (uint32_t base = p0; base < limit; base += 64) {
+        uint32_t pos0 = 0, pos1 = 0;
+        const bool acc0 = judge(base + lane, pos0);
+        const bool acc1 = judge(base + 32 + lane, pos1);
+        const unsigned m0 = __ballot_sync(0xFFFFFFFFu, acc0);
+        const unsigned m1 = __ballot_sync(0xFFFFFFFFu, acc1);
+        if (m0 | m1) {
+            const bool first_half = m0 != 0;
+            const int f = __ffs(first_half ? m0 : m1) - 1;
+            const uint32_t pf = __shfl_sync(0xFFFFFFFFu, first_half ? pos0 : pos1, f);
             *x_out = __ldg(cand + pf);
             __syncwarp();
-            return base + (uint32_t)f;
+            return base + (first_half ? 0u : 32u) + (uint32_t)f;
         }
     }
     *x_out = 0;

@@ -20,8 +20,8 @@
 
 namespace gw {
 
-template <bool SOPR, bool PATHS, bool COOP>
-__global__ void __launch_bounds__(kWalkThreads) k_walk_incore(const IncoreArgs a)
+template <bool SOPR, bool PATHS, bool COOP, int MINB>
+__global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const IncoreArgs a)
 {
     __shared__ uint32_t s_iv[kWalkThreads / 32][64];  // per-warp scratch of warp_first_accept
     const uint32_t lane = threadIdx.x & 31u;
@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_incore(const IncoreArgs a
             const uint32_t avail = q_end - q_next;
             const uint32_t rank = __popc(need & lt_mask);
             if (!active && rank < avail) {
-                wid = q_next + rank;
+                wid = a.wid_base + q_next + rank;
                 const uint32_t src = walker_source(a.init, wid);
                 prev = cur = src;
                 hop = 0;
@@ -214,48 +214,73 @@ cudaError_t launch_validate_csr(const uint64_t *beg, const uint32_t *csr, uint32
     return cudaGetLastError();
 }
 
-template <bool SOPR, bool PATHS, bool COOP>
+// Register-cap variants the autotuner chooses between: at 256 threads per CTA,
+// 3, 4 or 6 resident CTAs per SM (<= 85, 64, 40 registers per thread).
+template <int V>
+struct MinBlocks;
+template <> struct MinBlocks<0> { static constexpr int value = 3; };
+template <> struct MinBlocks<1> { static constexpr int value = 4; };
+template <> struct MinBlocks<2> { static constexpr int value = 6; };
+
+template <bool SOPR, bool PATHS, bool COOP, int V>
 static int grid_for(int num_sms)
 {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_incore<SOPR, PATHS, COOP>, kWalkThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_incore<SOPR, PATHS, COOP, MinBlocks<V>::value>,
+                                                  kWalkThreads, 0);
     if (per_sm < 1) per_sm = 1;
     return per_sm * num_sms;
 }
 
-template <bool SOPR, bool PATHS, bool COOP>
+template <bool SOPR, bool PATHS, bool COOP, int V>
 static void launch_one(const IncoreArgs &a, int grid, cudaStream_t s)
 {
-    k_walk_incore<SOPR, PATHS, COOP><<<grid, kWalkThreads, 0, s>>>(a);
+    k_walk_incore<SOPR, PATHS, COOP, MinBlocks<V>::value><<<grid, kWalkThreads, 0, s>>>(a);
 }
 
-int incore_grid(bool sopr, bool paths, bool coop, int num_sms)
+template <bool SOPR, bool PATHS, bool COOP>
+static int grid_v(int variant, int num_sms)
+{
+    if (variant == 0) return grid_for<SOPR, PATHS, COOP, 0>(num_sms);
+    if (variant == 1) return grid_for<SOPR, PATHS, COOP, 1>(num_sms);
+    return grid_for<SOPR, PATHS, COOP, 2>(num_sms);
+}
+
+template <bool SOPR, bool PATHS, bool COOP>
+static void launch_v(const IncoreArgs &a, int variant, int grid, cudaStream_t s)
+{
+    if (variant == 0) launch_one<SOPR, PATHS, COOP, 0>(a, grid, s);
+    else if (variant == 1) launch_one<SOPR, PATHS, COOP, 1>(a, grid, s);
+    else launch_one<SOPR, PATHS, COOP, 2>(a, grid, s);
+}
+
+int incore_grid(bool sopr, bool paths, bool coop, int variant, int num_sms)
 {
     const int v = (sopr ? 4 : 0) | (paths ? 2 : 0) | (coop ? 1 : 0);
     switch (v) {
-    case 0: return grid_for<false, false, false>(num_sms);
-    case 1: return grid_for<false, false, true>(num_sms);
-    case 2: return grid_for<false, true, false>(num_sms);
-    case 3: return grid_for<false, true, true>(num_sms);
-    case 4: return grid_for<true, false, false>(num_sms);
-    case 5: return grid_for<true, false, true>(num_sms);
-    case 6: return grid_for<true, true, false>(num_sms);
-    default: return grid_for<true, true, true>(num_sms);
+    case 0: return grid_v<false, false, false>(variant, num_sms);
+    case 1: return grid_v<false, false, true>(variant, num_sms);
+    case 2: return grid_v<false, true, false>(variant, num_sms);
+    case 3: return grid_v<false, true, true>(variant, num_sms);
+    case 4: return grid_v<true, false, false>(variant, num_sms);
+    case 5: return grid_v<true, false, true>(variant, num_sms);
+    case 6: return grid_v<true, true, false>(variant, num_sms);
+    default: return grid_v<true, true, true>(variant, num_sms);
     }
 }
 
-cudaError_t launch_walk_incore(const IncoreArgs &a, bool sopr, bool coop, int grid, cudaStream_t s)
+cudaError_t launch_walk_incore(const IncoreArgs &a, bool sopr, bool coop, int variant, int grid, cudaStream_t s)
 {
     const int v = (sopr ? 4 : 0) | (a.paths ? 2 : 0) | (coop ? 1 : 0);
     switch (v) {
-    case 0: launch_one<false, false, false>(a, grid, s); break;
-    case 1: launch_one<false, false, true>(a, grid, s); break;
-    case 2: launch_one<false, true, false>(a, grid, s); break;
-    case 3: launch_one<false, true, true>(a, grid, s); break;
-    case 4: launch_one<true, false, false>(a, grid, s); break;
-    case 5: launch_one<true, false, true>(a, grid, s); break;
-    case 6: launch_one<true, true, false>(a, grid, s); break;
-    default: launch_one<true, true, true>(a, grid, s); break;
+    case 0: launch_v<false, false, false>(a, variant, grid, s); break;
+    case 1: launch_v<false, false, true>(a, variant, grid, s); break;
+    case 2: launch_v<false, true, false>(a, variant, grid, s); break;
+    case 3: launch_v<false, true, true>(a, variant, grid, s); break;
+    case 4: launch_v<true, false, false>(a, variant, grid, s); break;
+    case 5: launch_v<true, false, true>(a, variant, grid, s); break;
+    case 6: launch_v<true, true, false>(a, variant, grid, s); break;
+    default: launch_v<true, true, true>(a, variant, grid, s); break;
     }
     return cudaGetLastError();
 }

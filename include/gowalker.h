@@ -106,7 +106,12 @@ typedef struct gw_stats {
     uint32_t launches;        /* kernels launched by this run */
     float kernel_ms;          /* time inside the step kernels (CUDA events) */
     float total_ms;           /* whole run (CUDA events) */
-    uint32_t reserved[8];
+    uint32_t learned_iterations; /* iterations decided by the predictor */
+    uint32_t policy_reverted;    /* 1 when the judge sent the run back to the plain policy */
+    float train_loss;            /* predictor training loss (mean squared, log1p scale) */
+    float pred_error;            /* mean |predicted - observed| demand, log1p scale */
+    uint32_t kernel_variant;     /* register-cap variant the autotuner picked (in-core) */
+    uint32_t reserved[3];
 } gw_stats;
 
 /* ------------------------------------------------------------------ basics */
@@ -202,6 +207,32 @@ int gw_rmat_csr(uint32_t scale, uint32_t nverts, uint64_t nsamples, const uint32
                 int symmetric, uint64_t target_edges, uint64_t **d_beg, uint32_t **d_csr, uint64_t *nedges);
 
 int gw_device_free(void *p);
+
+/* ------------------------------------------------------------------ block-demand predictor */
+
+/* No counterpart in the reference (its block choice is the fixed rule of
+ * engine/schedule.hpp:70-138): the learned policy's network, a 16 -> 64 ->
+ * 64 -> 1 ReLU MLP in fp32 (GW_MLP_PARAMS weights, layout W1[64][16], b1[64],
+ * W2[64][64], b2[64], W3[64], b3).  These calls run its hand-written kernels on
+ * caller-owned device buffers (synchronous, default stream); the engine uses
+ * the same kernels internally for GW_POLICY_LEARNED. */
+#define GW_MLP_INPUTS 16
+#define GW_MLP_PARAMS 5313
+#define GW_MLP_GRAD_WS_FLOATS (32 * (GW_MLP_PARAMS + 1))
+
+/* y[i] = mlp(x[i]) for n rows of GW_MLP_INPUTS floats. */
+int gw_mlp_forward(const float *d_params, const float *d_x, uint32_t n, float *d_y);
+
+/* Gradient of the mean squared error over n rows: d_grad (GW_MLP_PARAMS
+ * floats), d_loss (1 float), workspace d_ws (GW_MLP_GRAD_WS_FLOATS floats). */
+int gw_mlp_grad(const float *d_params, const float *d_x, const float *d_t, uint32_t n, float *d_grad, float *d_loss,
+                float *d_ws);
+
+/* Full-batch Adam for `epochs` steps at learning rate lr; seed != 0 first
+ * re-initialises d_params.  d_ws holds GW_MLP_GRAD_WS_FLOATS + 3 *
+ * GW_MLP_PARAMS + 1 floats.  *loss_out receives the final loss. */
+int gw_mlp_train(float *d_params, const float *d_x, const float *d_t, uint32_t n, uint32_t epochs, float lr,
+                 uint64_t seed, float *d_ws, float *loss_out);
 
 /* ------------------------------------------------------------------ no-allocation walk */
 

@@ -66,10 +66,24 @@ def test_schedule_invariance(gw, oracle):
 
 
 def test_ooc_learned_policy_same_walks(gw, oracle):
-    beg, csr = graph(oracle, scale=13, ef=8, sym=False, cap=6000, seed=8)
-    e1, s1 = run_ooc(gw, beg, csr, 12, 3, algo=0, paths=0, policy=0)
-    e2, s2 = run_ooc(gw, beg, csr, 12, 3, algo=0, paths=0, policy=1)
-    assert np.array_equal(e1.hashes(), e2.hashes())
+    """The learned policy trains on the first plain iterations, then decides;
+    the walks stay those of the plain policy and of the oracle."""
+    beg, csr = graph(oracle, scale=14, ef=8, sym=False, cap=12000, seed=8)
+    e1, s1 = run_ooc(gw, beg, csr, 16, 4, algo=0, maxhops=30, paths=0, policy=0)
+    e2, s2 = run_ooc(gw, beg, csr, 16, 4, algo=0, maxhops=30, paths=0, policy=1)
+    h1, h2 = e1.hashes(), e2.hashes()
+    assert np.array_equal(h1, h2)
+    V = len(beg) - 1
+    ref = oracle.walk(beg, csr, oracle.make_cfg(algo=0, maxhops=30, p=0.5, q=2.0, seed=5), 0, V, paths=False)
+    assert np.array_equal(h2, ref["hashes"])
+    assert s1["learned_iterations"] == 0
+    if s2["iterations"] > 23:
+        assert s2["train_loss"] > 0.0
+        assert s2["learned_iterations"] > 0 or s2["policy_reverted"] == 1
+    # a second learned run reuses the trained model from its first iteration
+    e2.init_walkers(0, 1, 5)
+    s3 = e2.run(1)
+    assert np.array_equal(e2.hashes(), h1)
     e1.close()
     e2.close()
 

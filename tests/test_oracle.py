@@ -166,3 +166,19 @@ def test_dataset_files_roundtrip(oracle, tmp_path):
         f.write(b"\0" * 5)
     with pytest.raises(ValueError):
         P.load_dataset(base)
+
+
+def test_mlp_oracle_gradient_by_finite_differences():
+    from oracle import mlp_oracle as M
+    rng = np.random.default_rng(0)
+    p = rng.normal(0, 0.2, M.NPARAMS)
+    x = rng.normal(0, 1, (20, M.IN))
+    t = rng.normal(0, 1, 20)
+    _, g = M.loss_and_grad(p, x, t)
+    for idx in rng.choice(M.NPARAMS, 12, replace=False):
+        pp = p.copy()
+        pp[idx] += 1e-6
+        lp, _ = M.loss_and_grad(pp, x, t)
+        pp[idx] -= 2e-6
+        lm, _ = M.loss_and_grad(pp, x, t)
+        assert abs((lp - lm) / 2e-6 - g[idx]) < 1e-5 * max(1.0, abs(g[idx]))
