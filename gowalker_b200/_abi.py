@@ -23,7 +23,7 @@ EXPORTS = (
     "gw_set_config", "gw_stream", "gw_set_graph_meta", "gw_host_block", "gw_device_graph", "gw_cache_reset",
     "gw_init_walkers", "gw_run", "gw_num_walkers", "gw_get_paths", "gw_path_hashes", "gw_checksum",
     "gw_bucket_counts", "gw_rmat_csr", "gw_device_free", "gw_memcpy", "gw_walk_noalloc",
-    "gw_mlp_forward", "gw_mlp_grad", "gw_mlp_train",
+    "gw_mlp_forward", "gw_mlp_grad", "gw_mlp_train", "gw_host_alloc", "gw_host_free",
 )
 GW_MLP_INPUTS = 16
 GW_MLP_PARAMS = 5313
@@ -121,6 +121,8 @@ def load():
         "gw_memcpy": ([vp, vp, u64], i32),
         "gw_walk_noalloc": ([ctypes.POINTER(GwConfig), vp, vp, u32, u64, u64, vp, vp, vp, vp,
                              ctypes.POINTER(GwStats)], i32),
+        "gw_host_alloc": ([u64, ctypes.POINTER(vp)], i32),
+        "gw_host_free": ([vp], i32),
         "gw_mlp_forward": ([vp, vp, u32, vp], i32),
         "gw_mlp_grad": ([vp, vp, vp, u32, vp, vp, vp], i32),
         "gw_mlp_train": ([vp, vp, vp, u32, u32, ctypes.c_float, u64, vp, ctypes.POINTER(ctypes.c_float)], i32),

@@ -1,0 +1,5 @@
+// The Node2vec app: apps/Node2vec.cu of GOWalker, same flags, walks on the B200
+// engine through libgowalker.so.
+#include "gowalker_host.hpp"
+
+int main(int argc, const char *argv[]) { return walk_app_main(argc, argv, node2vec); }

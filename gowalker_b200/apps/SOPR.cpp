@@ -1,0 +1,5 @@
+// The SOPR app: apps/SOPR.cu of GOWalker, same flags, walks on the B200
+// engine through libgowalker.so.
+#include "gowalker_host.hpp"
+
+int main(int argc, const char *argv[]) { return walk_app_main(argc, argv, SOPR); }

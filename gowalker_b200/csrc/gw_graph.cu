@@ -157,6 +157,25 @@ extern "C" int gw_device_free(void *p)
     return cudaFree(p) == cudaSuccess ? GW_OK : GW_ERR_CUDA;
 }
 
+extern "C" int gw_host_alloc(uint64_t bytes, void **out)
+{
+    if (!out || bytes == 0) return GW_ERR_ARG;
+    *out = nullptr;
+    const cudaError_t e = cudaHostAlloc(out, bytes, cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return e == cudaErrorMemoryAllocation ? GW_ERR_NOMEM : GW_ERR_CUDA;
+    }
+    return GW_OK;
+}
+
+extern "C" int gw_host_free(void *p)
+{
+    if (!p) return GW_OK;
+    return cudaFreeHost(p) == cudaSuccess ? GW_OK : GW_ERR_CUDA;
+}
+
 extern "C" int gw_memcpy(void *dst, const void *src, uint64_t bytes)
 {
     if ((!dst || !src) && bytes) return GW_ERR_ARG;

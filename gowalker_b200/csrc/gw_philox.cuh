@@ -62,6 +62,22 @@ GW_HD U4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint3
     return U4{c0, c1, c2, c3};
 }
 
+// Exact a % d for 32-bit a and d >= 1 by direct computation (Lemire, Kaser and
+// Kurz, "Faster remainder by direct computation", 2019): with the 64-bit
+// fraction M = ceil(2^64 / d), a % d = high64((M * a mod 2^64) * d).  M costs one
+// 64-bit division, so it pays off when one divisor serves many draws -- the
+// warp-uniform degree of a cooperative step.
+GW_HD uint64_t fastmod_magic(uint32_t d) { return ~0ull / d + 1; }
+GW_HD uint32_t fastmod(uint32_t a, uint64_t M, uint32_t d)
+{
+    const uint64_t low = M * (uint64_t)a;
+#if defined(__CUDA_ARCH__)
+    return (uint32_t)__umul64hi(low, (uint64_t)d);
+#else
+    return (uint32_t)(((unsigned __int128)low * d) >> 64);
+#endif
+}
+
 // FNV-1a over 32-bit words: the per-walker path hash.
 constexpr uint64_t kFnvOffset = 0xcbf29ce484222325ull;
 constexpr uint64_t kFnvPrime = 0x100000001b3ull;

@@ -114,7 +114,7 @@ __device__ __forceinline__ bool accept_candidate(const StepThr &t, float rv, uin
 
 // A walker whose step has already rejected this many attempts is served by
 // the whole warp (warp_first_accept).
-constexpr uint32_t kHardAttempts = 8;
+constexpr uint32_t kHardAttempts = 4;
 
 __device__ __forceinline__ uint64_t shfl64(uint64_t v, int src)
 {
@@ -141,11 +141,6 @@ __device__ __forceinline__ StepThr shfl_thr(const StepThr &t, int src)
     return o;
 }
 
-// All 32 lanes, with identical (broadcast) arguments, evaluate attempts
-// p0+lane, p0+32+lane, ... of one walker's step and return the first accepting
-// attempt in attempt order -- the one a single thread evaluating them one by
-// one would take -- and its candidate in *x_out.  Returns `limit` if none of
-// the attempts below `limit` accepts.
 // First index in the sorted run a[0, n) whose value is >= y.
 __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *__restrict__ a, uint32_t n, uint32_t y)
 {
@@ -187,11 +182,12 @@ __device__ __forceinline__ uint32_t warp_first_accept_runs(const StepConsts &c, 
     }
     __syncwarp();
     const uint32_t plo = __shfl_sync(0xFFFFFFFFu, lo, (int)pdeg), phi = __shfl_sync(0xFFFFFFFFu, hi, (int)pdeg);
+    const uint64_t M = fastmod_magic(deg);
     // verdict of attempt `att` from its draw alone
     auto judge = [&](uint32_t att, uint32_t &pos) -> bool {
         if (att >= limit) return false;
         const U4 r = draw(c, wid, hop, att);
-        pos = r.x % deg;
+        pos = fastmod(r.x, M, deg);
         const float rv = rand_val(r.y, t.maxv);
         if (rv <= t.minv) return true;
         if (pos >= plo && pos < phi) {
@@ -234,6 +230,11 @@ __device__ __forceinline__ uint32_t warp_first_accept_runs(const StepConsts &c, 
     return limit;
 }
 
+// All 32 lanes, with identical (broadcast) arguments, evaluate attempts
+// p0+lane, p0+32+lane, ... of one walker's step and return the first accepting
+// attempt in attempt order -- the one a single thread evaluating them one by
+// one would take -- and its candidate in *x_out.  Returns `limit` if none of
+// the attempts below `limit` accepts.
 template <bool SOPR>
 __device__ __forceinline__ uint32_t warp_first_accept(const StepConsts &c, const StepThr &t, uint32_t wid,
                                                       uint32_t hop, uint32_t p0, uint32_t limit,
@@ -245,13 +246,14 @@ __device__ __forceinline__ uint32_t warp_first_accept(const StepConsts &c, const
     if (pdeg < 32 && prev != cur)
         return warp_first_accept_runs<SOPR>(c, t, wid, hop, p0, limit, cand, deg, prev, prev_adj, pdeg, iv, x_out);
     const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t M = fastmod_magic(deg);
     for (uint32_t base = p0; base < limit; base += 32) {
         const uint32_t att = base + lane;
         bool acc = false;
         uint32_t x = 0;
         if (att < limit) {
             const U4 r = draw(c, wid, hop, att);
-            const uint32_t pos = r.x % deg;
+            const uint32_t pos = fastmod(r.x, M, deg);
             const float rv = rand_val(r.y, t.maxv);
             x = __ldg(cand + pos);
             acc = accept_candidate<SOPR>(t, rv, x, prev, cur, prev_adj, pdeg);

@@ -208,6 +208,13 @@ int gw_rmat_csr(uint32_t scale, uint32_t nverts, uint64_t nsamples, const uint32
 
 int gw_device_free(void *p);
 
+/* Pinned host memory for graph blocks and walker batches, in place of the
+ * reference's cudaHostAlloc calls (engine/cache.hpp:106-120,
+ * api/graph_buffer.hpp:26-32), so a host program needs no CUDA runtime of its
+ * own. */
+int gw_host_alloc(uint64_t bytes, void **out);
+int gw_host_free(void *p);
+
 /* ------------------------------------------------------------------ block-demand predictor */
 
 /* No counterpart in the reference (its block choice is the fixed rule of

@@ -60,3 +60,13 @@ def test_null_handle_rejected(gw):
     L = gw.load()
     assert L.gw_run(None, 0, None) == -1
     assert L.gw_destroy(None) == -1
+
+
+def test_fastmod_is_exact(tmp_path):
+    """The direct-computation remainder used by cooperative steps equals %."""
+    import subprocess
+    exe = tmp_path / "fastmod"
+    subprocess.run(["/usr/bin/g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "gowalker_b200", "csrc"),
+                    "-o", str(exe), os.path.join(ROOT, "tests", "cuda", "fastmod_check.cpp")], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0 and out.stdout.startswith("ok"), out.stdout
