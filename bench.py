@@ -347,9 +347,12 @@ def run_ours(args, wl):
     launches = 0
     trials = 0
     variant = -1
+    coop = [0, 0, 0, 0]
     for _ in range(args.steps):
         eng.init_walkers(wl["algo"], wl["wps"], seed)
         st = eng.run()
+        for i, k in enumerate(("coop_small_steps", "coop_small_attempts", "coop_large_steps", "coop_large_attempts")):
+            coop[i] += st[k]
         steps += st["steps"]
         kernel_ms += st["kernel_ms"]
         trials += st["trials"]
@@ -422,6 +425,8 @@ def run_ours(args, wl):
             "checksum": {"path_hash_sum": hash_sum, "steps_per_run": steps_last},
             "trials_per_step": trials / max(steps, 1),
             "kernel_variant": variant,
+            "hard_steps": {"by_position": coop[0] // args.steps, "by_position_attempts": coop[1] // args.steps,
+                           "by_search": coop[2] // args.steps, "by_search_attempts": coop[3] // args.steps},
         }
         if clk:
             line["clocks"] = clk

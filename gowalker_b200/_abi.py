@@ -73,6 +73,10 @@ class GwStats(ctypes.Structure):
         ("pred_error", ctypes.c_float),
         ("kernel_variant", ctypes.c_uint32),
         ("reserved", ctypes.c_uint32 * 3),
+        ("coop_small_steps", ctypes.c_uint64),
+        ("coop_small_attempts", ctypes.c_uint64),
+        ("coop_large_steps", ctypes.c_uint64),
+        ("coop_large_attempts", ctypes.c_uint64),
     ]
 
     def as_dict(self):

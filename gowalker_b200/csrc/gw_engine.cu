@@ -535,6 +535,10 @@ int gw_handle::run_incore(gw_stats *stats)
         stats->iterations = 1;
         stats->launches = 1;
         stats->kernel_variant = (uint32_t)variant;
+        stats->coop_small_steps = h_ctr[kCtrCoopSmall];
+        stats->coop_small_attempts = h_ctr[kCtrCoopSmallAtt];
+        stats->coop_large_steps = h_ctr[kCtrCoopLarge];
+        stats->coop_large_attempts = h_ctr[kCtrCoopLargeAtt];
         cudaEventElapsedTime(&stats->kernel_ms, ev_kernel0, ev_kernel1);
         cudaEventElapsedTime(&stats->total_ms, ev_start, ev_stop);
     }

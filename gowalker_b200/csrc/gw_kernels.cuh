@@ -16,7 +16,11 @@ enum Counter : int {
     kCtrTrials = 2,
     kCtrDone = 3,
     kCtrHashSum = 4,  // wrapping sum of finished walkers' path hashes
-    kCtrCount = 8
+    kCtrCoopSmall = 5,     // hard steps decided from candidate positions (prev degree < 32)
+    kCtrCoopSmallAtt = 6,  // attempts those steps took
+    kCtrCoopLarge = 7,     // hard steps evaluated with candidate loads and searches
+    kCtrCoopLargeAtt = 8,  // attempts those steps took
+    kCtrCount = 12
 };
 
 // Error word bits set by kernels instead of trapping.

@@ -305,7 +305,7 @@ template <bool SOPR, bool PATHS, bool COOP>
 __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const OocStepArgs a)
 {
     __shared__ uint32_t s_vs[kMaxBlocks + 1];
-    __shared__ uint32_t s_iv[kWalkThreads / 32][64];
+    __shared__ uint32_t s_iv[kWalkThreads / 32][kCoopScratchWords];
     for (uint32_t i = threadIdx.x; i <= a.nb; i += blockDim.x) s_vs[i] = a.vstart[i];
     __syncthreads();
 

@@ -153,13 +153,42 @@ __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *__restrict__
     return lo;
 }
 
+// Per-warp shared scratch of a cooperative step, in 32-bit words: run starts
+// (32), run ends (32), and a filter of 2^kFilterBits buckets, one bit each.
+constexpr uint32_t kFilterBits = 12;
+constexpr int kCoopScratchWords = 64 + (1 << kFilterBits) / 32;
+
+// Smallest k in [0, 2^24] for which `pred(k)` fails, where pred holds on a
+// prefix of [0, 2^24).  rand_val(k << 8, maxv) is non-decreasing in k (an
+// exact scaling followed by one rounded multiply by a positive constant), so
+// every "rv <= T" / "rv < T" test of a step is such a prefix, and comparing
+// k = y >> 8 with its bound gives the same verdict bit for bit.
+template <class Pred>
+__device__ __forceinline__ uint32_t rand_prefix(Pred pred)
+{
+    uint32_t lo = 0, hi = 1u << 24;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (pred(mid)) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
 // Hard steps whose prev has fewer than 32 neighbours are decided without
 // touching the candidate: a trial's verdict depends on x = cand[pos] only
 // through "x == prev" and "x in N(prev)", i.e. through whether pos falls in
 // the run of prev, or of some y in N(prev), inside the sorted N(cur).  Those
-// runs are located once per step (one lower-bound search per lane); the
-// trials are then Philox + a lookup in `iv`, a 64-word per-warp scratch in
-// shared memory.
+// runs are located once per step (one lower-bound search per lane).
+//
+// Trials then run on integers only.  The rand-value tests become bounds on
+// k = y >> 8 (rand_prefix).  pos = x mod deg is never formed on the common
+// path: with Lemire's fraction f = M*x mod 2^64 (M = ceil(2^64/deg)), pos =
+// floor(f*deg / 2^64), so f lies in [pos, pos+1) * 2^64/deg and its top
+// kFilterBits bits name a bucket of positions.  A per-warp bitmap marks every
+// bucket a run can reach; a trial whose bucket is unmarked is in no run and
+// its verdict is k < max(k_min, k_notfound).  Only marked buckets take the
+// exact path (pos, run lookup in `iv`).
 template <bool SOPR>
 __device__ __forceinline__ uint32_t warp_first_accept_runs(const StepConsts &c, const StepThr &t, uint32_t wid,
                                                            uint32_t hop, uint32_t p0, uint32_t limit,
@@ -168,6 +197,9 @@ __device__ __forceinline__ uint32_t warp_first_accept_runs(const StepConsts &c, 
                                                            uint32_t pdeg, uint32_t *iv, uint32_t *x_out)
 {
     const uint32_t lane = threadIdx.x & 31u;
+    uint32_t *bm = iv + 64;
+    constexpr uint32_t kFilterWords = (1u << kFilterBits) / 32;
+    for (uint32_t w = lane; w < kFilterWords; w += 32) bm[w] = 0;
     // lane k < pdeg: run of N(prev)[k]; lane pdeg: run of prev
     uint32_t lo = 0, hi = 0;
     if (lane <= pdeg) {
@@ -180,47 +212,87 @@ __device__ __forceinline__ uint32_t warp_first_accept_runs(const StepConsts &c, 
         iv[lane] = lo;
         iv[32 + lane] = hi;
     }
-    __syncwarp();
-    const uint32_t plo = __shfl_sync(0xFFFFFFFFu, lo, (int)pdeg), phi = __shfl_sync(0xFFFFFFFFu, hi, (int)pdeg);
     const uint64_t M = fastmod_magic(deg);
-    // verdict of attempt `att` from its draw alone
-    auto judge = [&](uint32_t att, uint32_t &pos) -> bool {
-        if (att >= limit) return false;
-        const U4 r = draw(c, wid, hop, att);
-        pos = fastmod(r.x, M, deg);
-        const float rv = rand_val(r.y, t.maxv);
-        if (rv <= t.minv) return true;
-        if (pos >= plo && pos < phi) {
-            if constexpr (SOPR) return (double)rv < t.t_prev_d;
-            else return rv < t.t_prev;
+    __syncwarp();
+    if (hi > lo) {
+        // buckets floor(p * 2^B / deg) for p in [lo, hi], widened by one below
+        // (umul64hi(M, P) exceeds floor(P / deg) by at most one); deg = 1 has
+        // M = 0 and covers everything.
+        uint32_t b0 = 0, b1 = (1u << kFilterBits) - 1;
+        if (deg > 1) {
+            const uint32_t e0 = (uint32_t)__umul64hi(M, (uint64_t)lo << kFilterBits);
+            const uint32_t e1 = (uint32_t)__umul64hi(M, (uint64_t)hi << kFilterBits);
+            b0 = e0 > 0 ? e0 - 1 : 0;
+            b1 = min(e1, b1);
         }
+        for (uint32_t w = b0 >> 5; w <= (b1 >> 5); ++w) {
+            const uint32_t from = (w == (b0 >> 5)) ? (b0 & 31u) : 0u;
+            const uint32_t to = (w == (b1 >> 5)) ? (b1 & 31u) : 31u;
+            const uint32_t mask = (0xFFFFFFFFu >> (31u - to)) & (0xFFFFFFFFu << from);
+            atomicOr(bm + w, mask);
+        }
+    }
+    // integer bounds of the four rand-value tests, one per lane of a quad
+    uint32_t kq;
+    {
+        const uint32_t which = lane & 3u;
+        kq = rand_prefix([&](uint32_t k) {
+            const float rv = rand_val(k << 8, t.maxv);
+            bool prev_ok;
+            if constexpr (SOPR) prev_ok = (double)rv < t.t_prev_d;
+            else prev_ok = rv < t.t_prev;
+            return which == 0 ? (rv <= t.minv) : which == 1 ? prev_ok : which == 2 ? (rv < t.t_found)
+                                                                                    : (rv < t.t_notfound);
+        });
+    }
+    const uint32_t k_min = __shfl_sync(0xFFFFFFFFu, kq, 0), k_prev = __shfl_sync(0xFFFFFFFFu, kq, 1);
+    const uint32_t k_found = __shfl_sync(0xFFFFFFFFu, kq, 2), k_nf = __shfl_sync(0xFFFFFFFFu, kq, 3);
+    const uint32_t k_fast = max(k_min, k_nf);
+    const uint32_t plo = __shfl_sync(0xFFFFFFFFu, lo, (int)pdeg), phi = __shfl_sync(0xFFFFFFFFu, hi, (int)pdeg);
+    const uint32_t m_lo = (uint32_t)M, m_hi = (uint32_t)(M >> 32);
+    __syncwarp();
+
+    // exact verdict of a trial whose bucket is marked
+    auto exact = [&](uint32_t x, uint32_t k) -> bool {
+        if (k < k_min) return true;
+        const uint32_t pos = fastmod(x, M, deg);
+        if (pos >= plo && pos < phi) return k < k_prev;
         // last run whose start is <= pos (runs are in N(prev) order, so sorted)
-        int k = -1;
+        int r = -1;
         uint32_t a = 0, b = pdeg;
         while (a < b) {
             const uint32_t m = (a + b) >> 1;
             if (iv[m] <= pos) {
-                k = (int)m;
+                r = (int)m;
                 a = m + 1;
             } else {
                 b = m;
             }
         }
-        const bool found = k >= 0 && pos < iv[32 + k];
-        return found ? (rv < t.t_found) : (rv < t.t_notfound);
+        const bool found = r >= 0 && pos < iv[32 + r];
+        return found ? (k < k_found) : (k < k_nf);
+    };
+    auto judge = [&](uint32_t att, uint32_t &xr) -> bool {
+        if (att >= limit) return false;
+        const U4 r = draw(c, wid, hop, att);
+        xr = r.x;
+        const uint32_t k = r.y >> 8;
+        const uint32_t b = (m_hi * r.x + __umulhi(m_lo, r.x)) >> (32 - kFilterBits);
+        if ((bm[b >> 5] >> (b & 31u)) & 1u) return exact(r.x, k);
+        return k < k_fast;
     };
     // 64 attempts per round, two independent Philox chains per lane
     for (uint32_t base = p0; base < limit; base += 64) {
-        uint32_t pos0 = 0, pos1 = 0;
-        const bool acc0 = judge(base + lane, pos0);
-        const bool acc1 = judge(base + 32 + lane, pos1);
+        uint32_t x0 = 0, x1 = 0;
+        const bool acc0 = judge(base + lane, x0);
+        const bool acc1 = judge(base + 32 + lane, x1);
         const unsigned m0 = __ballot_sync(0xFFFFFFFFu, acc0);
         const unsigned m1 = __ballot_sync(0xFFFFFFFFu, acc1);
         if (m0 | m1) {
             const bool first_half = m0 != 0;
             const int f = __ffs(first_half ? m0 : m1) - 1;
-            const uint32_t pf = __shfl_sync(0xFFFFFFFFu, first_half ? pos0 : pos1, f);
-            *x_out = __ldg(cand + pf);
+            const uint32_t xf = __shfl_sync(0xFFFFFFFFu, first_half ? x0 : x1, f);
+            *x_out = __ldg(cand + fastmod(xf, M, deg));
             __syncwarp();
             return base + (first_half ? 0u : 32u) + (uint32_t)f;
         }

@@ -23,7 +23,7 @@ namespace gw {
 template <bool SOPR, bool PATHS, bool COOP, int MINB>
 __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const IncoreArgs a)
 {
-    __shared__ uint32_t s_iv[kWalkThreads / 32][64];  // per-warp scratch of warp_first_accept
+    __shared__ uint32_t s_iv[kWalkThreads / 32][kCoopScratchWords];  // per-warp scratch of warp_first_accept
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint64_t *__restrict__ beg = a.beg;
@@ -41,6 +41,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const Incore
     StepThr t{};
     uint32_t *prow = nullptr;
     unsigned long long n_steps = 0, n_trials = 0, n_done = 0, hsum = 0;
+    unsigned long long n_cs = 0, n_csa = 0, n_cl = 0, n_cla = 0;  // cooperative steps / attempts by path
 
     auto finish = [&]() {
         a.hashes[wid] = h;
@@ -118,6 +119,13 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const Incore
                 &xs);
             if (lane == (uint32_t)L) {
                 n_trials += astar - p0;
+                if (pdeg < 32 && prev != cur) {
+                    n_cs++;
+                    n_csa += astar - p0 + 1;
+                } else {
+                    n_cl++;
+                    n_cla += astar - p0 + 1;
+                }
                 if (astar >= kMaxAttempts) {
                     atomicOr(a.err, kErrTrials);
                     finish();
@@ -181,11 +189,21 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const Incore
     n_trials = warp_sum(n_trials);
     n_done = warp_sum(n_done);
     hsum = warp_sum(hsum);
+    n_cs = warp_sum(n_cs);
+    n_csa = warp_sum(n_csa);
+    n_cl = warp_sum(n_cl);
+    n_cla = warp_sum(n_cla);
     if (lane == 0) {
         atomicAdd(&a.ctr[kCtrSteps], n_steps);
         atomicAdd(&a.ctr[kCtrTrials], n_trials);
         atomicAdd(&a.ctr[kCtrDone], n_done);
         atomicAdd(&a.ctr[kCtrHashSum], hsum);
+        if (COOP) {
+            atomicAdd(&a.ctr[kCtrCoopSmall], n_cs);
+            atomicAdd(&a.ctr[kCtrCoopSmallAtt], n_csa);
+            atomicAdd(&a.ctr[kCtrCoopLarge], n_cl);
+            atomicAdd(&a.ctr[kCtrCoopLargeAtt], n_cla);
+        }
     }
 }
 

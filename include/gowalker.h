@@ -112,6 +112,10 @@ typedef struct gw_stats {
     float pred_error;            /* mean |predicted - observed| demand, log1p scale */
     uint32_t kernel_variant;     /* register-cap variant the autotuner picked (in-core) */
     uint32_t reserved[3];
+    uint64_t coop_small_steps;   /* hard steps decided from candidate positions (in-core) */
+    uint64_t coop_small_attempts;
+    uint64_t coop_large_steps;   /* hard steps evaluated with candidate loads (in-core) */
+    uint64_t coop_large_attempts;
 } gw_stats;
 
 /* ------------------------------------------------------------------ basics */

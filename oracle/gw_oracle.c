@@ -328,6 +328,10 @@ int oracle_walk(const uint64_t *beg, const uint32_t *csr, uint32_t nverts, const
 {
     if (c->algo > ALG_SOSR || c->maxhops == 0) return -1;
     if (c->init_mode == INIT_PER_VERTEX && c->wps == 0) return -1;
+    /* every source must be a vertex */
+    if (c->init_mode == INIT_PER_VERTEX && (uint64_t)wid_begin + count > (uint64_t)nverts * c->wps) return -1;
+    if (c->init_mode == INIT_SINGLE_SOURCE && nverts <= (c->algo == ALG_SOSR ? 3u : 1u)) return -1;
+    if (nverts == 0) return -1;
     memset(stats, 0, sizeof(*stats));
     if (nthreads > 0) omp_set_num_threads(nthreads);
     const uint64_t stride = (uint64_t)c->maxhops + 1;

@@ -210,3 +210,70 @@ def test_c1_node2vec_sample_vs_oracle(gw, oracle):
     assert hs == int(H.sum(dtype=np.uint64))
     eng.close()
     dg.free()
+
+
+def hub_ring_graph(leaves):
+    """Vertex 0 joined to every leaf 1..leaves; leaf i also joined to its ring
+    neighbours.  A walker stepping leaf -> hub has prev degree 3 next to a hub
+    of degree `leaves`: the hard, position-decided cooperative steps, with runs
+    of N(prev) at every offset of N(hub)."""
+    V = leaves + 1
+    i = np.arange(1, V, dtype=np.int64)
+    nxt = np.where(i == leaves, 1, i + 1)
+    src = np.concatenate([np.zeros(leaves, np.int64), i, i, nxt])
+    dst = np.concatenate([i, np.zeros(leaves, np.int64), nxt, i])
+    order = np.lexsort((dst, src))
+    src, dst = src[order], dst[order]
+    beg = np.zeros(V + 1, dtype=np.uint64)
+    beg[1:] = np.cumsum(np.bincount(src, minlength=V))
+    return beg, dst.astype(np.uint32)
+
+
+HUB_CASES = [
+    # algo, leaves, p, q, alpha
+    (1, 60000, 0.5, 2.0, 0.2),     # SOPR: ~4000 trials per hub step
+    (2, 5000, 0.5, 2.0, 0.6),      # SOSR, smaller hub
+    (0, 60000, 0.05, 20.0, 0.2),   # Node2vec: only the run of prev accepts often
+    (0, 60000, 0.05, 0.5, 0.2),    # Node2vec: not-found bound above the min bound
+    (1, 1, 0.5, 2.0, 0.2),         # hub of degree 1
+]
+
+
+@pytest.mark.parametrize("case", HUB_CASES)
+def test_hub_steps_vs_oracle(gw, oracle, case):
+    algo, leaves, p, q, alpha = case
+    beg, csr = hub_ring_graph(leaves)
+    n = 3000
+    eng, st = run_engine(gw, beg, csr, algo, 9, wps=1, p=p, q=q, alpha=alpha, seed=99, init_mode=2, numwalks=n)
+    cfg = oracle_cfg(oracle, algo, 9, 1, p, q, alpha, seed=99, init_mode=2, numwalks=n)
+    ref = oracle.walk(beg, csr, cfg, 0, n, paths=True, nthreads=8)
+    P, L = eng.paths()
+    assert np.array_equal(L, ref["lens"])
+    assert np.array_equal(P, ref["paths"])
+    assert st["trials"] == ref["stats"]["trials"]
+    if leaves > 1000:
+        assert st["coop_small_steps"] > 0
+    eng.close()
+
+
+def test_c2_sopr_sample_vs_oracle(gw, oracle):
+    """Scale-24 symmetrised R-MAT, SOPR alpha 0.2, termination 0.15, length 20,
+    4 walkers per vertex (the in-core C2 workload): full GPU run, a strided
+    sample of walkers checked against the oracle."""
+    dg = gw.DeviceGraph(24, edgefactor=16, seed=1, symmetric=True)
+    beg, csr = dg.to_host()
+    V = dg.nverts
+    eng = gw.WalkEngine(algorithm=1, maxhops=20, alpha=0.2, term_prob=0.15, seed=42, walkpersource=4,
+                        record_paths=0)
+    eng.set_device_graph(dg.nverts, dg.nedges, dg.beg_ptr, dg.csr_ptr)
+    eng.init_walkers(1, 4, 42)
+    st = eng.run()
+    H = eng.hashes()
+    cfg = oracle_cfg(oracle, 1, 20, 4, alpha=0.2, term=0.15, seed=42)
+    for w0 in range(0, 4 * V - 512, 4 * V // 40):
+        r = oracle.walk(beg, csr, cfg, w0, 512, paths=False, nthreads=8)
+        assert np.array_equal(H[w0:w0 + 512], r["hashes"])
+    assert st["walkers"] == 4 * V
+    assert st["coop_small_steps"] > 0 and st["coop_large_steps"] > 0
+    eng.close()
+    dg.free()

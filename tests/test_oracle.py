@@ -92,6 +92,15 @@ def test_single_source_init(oracle):
     assert srcs == [1] * 5 + [3] * 5
 
 
+def test_walker_range_beyond_sources_is_rejected(oracle):
+    beg, csr = oracle.rmat_graph(8, 8, seed=1)
+    V = len(beg) - 1
+    cfg = oracle.make_cfg(algo=oracle.ALG_SOPR, maxhops=5, wps=2)
+    oracle.walk(beg, csr, cfg, 2 * V - 4, 4, paths=False)
+    with pytest.raises(ValueError):
+        oracle.walk(beg, csr, cfg, 2 * V - 4, 5, paths=False)
+
+
 def test_block_splitters(oracle):
     beg, csr = oracle.rmat_graph(12, 16, seed=1)
     vb, eb = oracle.split_equal_edge_mass(beg, 8)
