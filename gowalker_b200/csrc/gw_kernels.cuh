@@ -23,6 +23,20 @@ enum Counter : int {
     kCtrCount = 12
 };
 
+// Per-warp statistics a walk kernel keeps in shared memory and adds to the
+// Counter slots when it ends.
+enum WarpStat : int {
+    kWsSteps = 0,
+    kWsTrials,
+    kWsDone,
+    kWsHash,
+    kWsCoopSmall,
+    kWsCoopSmallAtt,
+    kWsCoopLarge,
+    kWsCoopLargeAtt,
+    kWsCount
+};
+
 // Error word bits set by kernels instead of trapping.
 enum ErrBit : uint32_t {
     kErrVertexRange = 1u,   // a neighbour id >= nverts

@@ -16,8 +16,6 @@
 #include <algorithm>
 #include <cstring>
 #include <vector>
-#include <iterator>
-#include <map>
 #include "gw_engine.cuh"
 #include "gw_ooc_kernels.cuh"
 #include "gw_mlp.cuh"
@@ -50,10 +48,11 @@ struct OocState {
     uint32_t *d_run_pre = nullptr, *d_run_off = nullptr, *d_nrun = nullptr;
     Decision *d_dec = nullptr, *h_dec = nullptr;
 
-    // zero-copy: device views of the host blocks, and what we registered
+    // zero-copy: device views of the host blocks, and the pinned copies made
+    // of pageable ones
     std::vector<const uint64_t *> map_beg;
     std::vector<const uint32_t *> map_csr;
-    std::map<uintptr_t, uintptr_t> reg;  // page ranges we registered: start -> end
+    std::vector<void *> staged;
     bool mapped = false;
 
     bool ready = false;
@@ -121,7 +120,7 @@ void gw_handle::ooc_release()
     if (o.h_blk_csr) cudaFreeHost((void *)o.h_blk_csr);
     if (o.h_cached) cudaFreeHost(o.h_cached);
     if (o.h_dec) cudaFreeHost(o.h_dec);
-    for (auto &r : o.reg) cudaHostUnregister((void *)r.first);
+    for (void *p : o.staged) cudaFreeHost(p);
     for (float *p : {o.d_params, o.d_train_ws, o.d_trace_x, o.d_trace_col, o.d_trace_y, o.d_feat_x, o.d_feat_col,
                      o.d_pred, o.d_emass, o.d_vfrac, o.d_prev_col, o.d_ema})
         cudaFree(p);
@@ -175,8 +174,8 @@ void gw_handle::ooc_invalidate()
     // host blocks changed: drop mappings so they are rebuilt on demand
     if (!ooc) return;
     cudaSetDevice(cfg.device);
-    for (auto &r : ooc->reg) cudaHostUnregister((void *)r.first);
-    ooc->reg.clear();
+    for (void *p : ooc->staged) cudaFreeHost(p);
+    ooc->staged.clear();
     ooc->mapped = false;
 }
 
@@ -249,58 +248,34 @@ static int ooc_walkers(gw_handle *h)
     return GW_OK;
 }
 
-// Make [p, p+bytes) readable by the device at address p.  Blocks handed to
-// gw_host_block are often slices of one array: neighbouring blocks share a
-// page (their offset ranges even share an entry), and a registration may not
-// overlap an earlier one, so only the pages no registration covers yet are
-// registered.  Memory that is already pinned (cudaHostAlloc, or registered by
-// the caller) is used as it is.  Needs a device that reads registered host
-// memory at its host address (checked by the caller).
-static int map_range(gw_handle *h, OocState &o, const void *p, uint64_t bytes)
+// Device-readable view of the host bytes [p, p+bytes): the caller's memory
+// itself when it is pinned and mapped (cudaHostAlloc, gw_host_alloc, or
+// registered mapped by the caller), otherwise a pinned mapped copy that the
+// handle owns.  The handle never registers the caller's pages: a
+// registration covers whole pages, and a later copy into another object that
+// shares such a page (a small array next to a block on the heap) would be
+// refused by the runtime.
+static int map_block(gw_handle *h, OocState &o, const void *p, uint64_t bytes, const void **view)
 {
+    *view = nullptr;
     if (!p || !bytes) return GW_OK;
     cudaPointerAttributes a0{}, a1{};
     const char *last = (const char *)p + bytes - 1;
-    if (cudaPointerGetAttributes(&a0, p) == cudaSuccess && a0.type == cudaMemoryTypeHost &&
+    if (cudaPointerGetAttributes(&a0, p) == cudaSuccess && a0.type == cudaMemoryTypeHost && a0.devicePointer &&
         cudaPointerGetAttributes(&a1, last) == cudaSuccess && a1.type == cudaMemoryTypeHost &&
-        a0.devicePointer == p) {
-        // both ends pinned, device address = host address: a block is one
-        // array, so one pinned allocation covers it
+        (const char *)a1.devicePointer == (const char *)a0.devicePointer + (bytes - 1)) {
+        *view = a0.devicePointer;  // one mapped allocation covers the block
         return GW_OK;
     }
     cudaGetLastError();
-    const uintptr_t page = 4096;
-    uintptr_t a = (uintptr_t)p & ~(page - 1);
-    const uintptr_t b = ((uintptr_t)p + bytes + page - 1) & ~(page - 1);
-    while (a < b) {
-        // skip pages inside one of our registrations
-        auto it = o.reg.upper_bound(a);
-        if (it != o.reg.begin()) {
-            auto pr = std::prev(it);
-            if (pr->second > a) {
-                a = pr->second;
-                continue;
-            }
-        }
-        uintptr_t end = b;
-        if (it != o.reg.end() && it->first < end) end = it->first;
-        // pages of the gap that somebody else already pinned are fine as they are
-        cudaPointerAttributes at{};
-        if (cudaPointerGetAttributes(&at, (const void *)a) == cudaSuccess && at.type == cudaMemoryTypeHost) {
-            a += page;
-            continue;
-        }
-        cudaGetLastError();
-        const cudaError_t e = cudaHostRegister((void *)a, end - a, cudaHostRegisterMapped | cudaHostRegisterReadOnly);
-        if (e == cudaErrorHostMemoryAlreadyRegistered) {
-            cudaGetLastError();  // pinned elsewhere in the range: take it page by page
-            a += page;
-            continue;
-        }
-        if (e != cudaSuccess) return h->cuda(e, "cudaHostRegister (zero-copy)");
-        o.reg[a] = end;
-        a = end;
-    }
+    void *stage = nullptr;
+    int st = h->cuda(cudaHostAlloc(&stage, bytes, cudaHostAllocMapped), "pinned staging of a host block (zero-copy)");
+    if (st) return st;
+    o.staged.push_back(stage);
+    memcpy(stage, p, bytes);
+    void *d = nullptr;
+    if ((st = h->cuda(cudaHostGetDevicePointer(&d, stage, 0), "cudaHostGetDevicePointer"))) return st;
+    *view = d;
     return GW_OK;
 }
 
@@ -309,20 +284,17 @@ static int ooc_map_host(gw_handle *h)
 {
     OocState &o = *h->ooc;
     if (o.mapped) return GW_OK;
-    int direct = 0;
-    cudaDeviceGetAttribute(&direct, cudaDevAttrCanUseHostPointerForRegisteredMem, h->cfg.device);
-    if (!direct)
-        return h->fail(GW_ERR_STATE, "zero-copy needs a device that reads registered host memory at its host address");
     o.map_beg.assign(o.nb, nullptr);
     o.map_csr.assign(o.nb, nullptr);
     for (uint32_t b = 0; b < o.nb; ++b) {
         const uint64_t nv = (uint64_t)h->vblocks[b + 1] - h->vblocks[b];
         const uint64_t ne = h->eblocks[b + 1] - h->eblocks[b];
+        const void *vb = nullptr, *vc = nullptr;
         int st;
-        if ((st = map_range(h, o, h->host_beg[b], (nv + 1) * 8))) return st;
-        if ((st = map_range(h, o, h->host_csr[b], ne * 4))) return st;
-        o.map_beg[b] = h->host_beg[b];
-        o.map_csr[b] = h->host_csr[b];
+        if ((st = map_block(h, o, h->host_beg[b], (nv + 1) * 8, &vb))) return st;
+        if ((st = map_block(h, o, h->host_csr[b], ne * 4, &vc))) return st;
+        o.map_beg[b] = (const uint64_t *)vb;
+        o.map_csr[b] = (const uint32_t *)vc;
     }
     o.mapped = true;
     return GW_OK;

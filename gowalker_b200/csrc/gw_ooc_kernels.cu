@@ -306,10 +306,13 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const OocStepArgs a)
 {
     __shared__ uint32_t s_vs[kMaxBlocks + 1];
     __shared__ uint32_t s_iv[kWalkThreads / 32][kCoopScratchWords];
+    __shared__ unsigned long long s_ws[kWalkThreads / 32][kWsCount];  // per-warp statistics
     for (uint32_t i = threadIdx.x; i <= a.nb; i += blockDim.x) s_vs[i] = a.vstart[i];
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (lane < kWsCount) s_ws[warp][lane] = 0;
     __syncthreads();
 
-    const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint32_t nrun = *a.nrun;
     const uint32_t total = a.run_pre[nrun];
@@ -319,20 +322,27 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const OocStepArgs a)
     bool exhausted = false;
     bool active = false;
 
-    uint32_t wid = 0, prev = 0, cur = 0, hop = 0, attempt = 0, pb = 0, cb = 0, deg = 0, pdeg = 0;
+    uint32_t wid = 0, prev = 0, cur = 0, hop = 0, hop0 = 0, attempt = 0, pb = 0, cb = 0, deg = 0, pdeg = 0;
     uint64_t idx = 0, head = 0, phead = 0, h = 0;
     const uint32_t *ccsr = nullptr, *pcsr = nullptr;
     U4 r{0, 0, 0, 0};
-    StepThr t{};
-    uint32_t *prow = nullptr;
-    unsigned long long n_steps = 0, n_trials = 0, n_done = 0, hsum = 0;
+    StepThr t{0.f, 0.f, 0.f};
+    uint32_t n_trials = 0;  // trials not yet added to s_ws
 
+    // Statistics of the walker leaving this lane (finished or parked): its
+    // steps in this launch are the hops it made since it was loaded.
+    auto flush = [&]() {
+        atomicAdd(&s_ws[warp][kWsSteps], (unsigned long long)(hop - hop0));
+        atomicAdd(&s_ws[warp][kWsTrials], (unsigned long long)n_trials);
+        n_trials = 0;
+    };
     auto finish = [&]() {
         a.hashes[wid] = h;
         a.lens[wid] = hop + 1;
         a.walkers[idx].prev_blk = kFinished;
-        hsum += h;
-        n_done++;
+        atomicAdd(&s_ws[warp][kWsHash], (unsigned long long)h);
+        atomicAdd(&s_ws[warp][kWsDone], 1ull);
+        flush();
         active = false;
     };
     // Enter a step at vertex cur (block cb), prev adjacency already set:
@@ -390,10 +400,10 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const OocStepArgs a)
                 prev = rec.prev;
                 cur = rec.cur;
                 hop = rec.hop;
+                hop0 = hop;
                 pb = rec.prev_blk;
                 cb = rec.cur_blk;
                 h = ((uint64_t)rec.hash_hi << 32) | rec.hash_lo;
-                if (PATHS) prow = a.paths + (uint64_t)wid * a.stride;
                 if (hop >= maxhops) {
                     finish();
                 } else {
@@ -419,10 +429,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const OocStepArgs a)
             const uint32_t *cc = shfl_ptr(ccsr, L), *pc = shfl_ptr(pcsr, L);
             uint32_t xs;
             const uint32_t astar = warp_first_accept<SOPR>(
-                a.c, shfl_thr(t, L), __shfl_sync(0xFFFFFFFFu, wid, L), __shfl_sync(0xFFFFFFFFu, hop, L), p0,
+                a.c, shfl_thr<SOPR>(t, L), __shfl_sync(0xFFFFFFFFu, wid, L), __shfl_sync(0xFFFFFFFFu, hop, L), p0,
                 kMaxAttempts, cc + hd, __shfl_sync(0xFFFFFFFFu, deg, L), __shfl_sync(0xFFFFFFFFu, prev, L),
-                __shfl_sync(0xFFFFFFFFu, cur, L), pc + ph, __shfl_sync(0xFFFFFFFFu, pdeg, L), s_iv[threadIdx.x >> 5],
-                &xs);
+                __shfl_sync(0xFFFFFFFFu, cur, L), pc + ph, __shfl_sync(0xFFFFFFFFu, pdeg, L), s_iv[warp], &xs);
             if (lane == (uint32_t)L) {
                 n_trials += astar - p0;
                 if (astar >= kMaxAttempts) {
@@ -437,14 +446,17 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const OocStepArgs a)
         if (!active) continue;
 
         const uint32_t pos = r.x % deg;
-        const float rv = rand_val(r.y, t.maxv);
+        const float rv = rand_val(r.y, thr_max<SOPR>(a.c, t));
         const uint32_t x = __ldg(ccsr + head + pos);
         n_trials++;
-        if (accept_candidate<SOPR>(t, rv, x, prev, cur, pcsr + phead, pdeg)) {
+        if (accept_candidate<SOPR>(a.c, t, rv, x, prev, cur, pcsr + phead, pdeg)) {
             hop++;
-            n_steps++;
             h = hash_step(h, x);
-            if (PATHS) prow[hop] = x;
+            if (PATHS) a.paths[(uint64_t)wid * a.stride + hop] = x;
+            if (n_trials & 0x80000000u) {  // a step adds < 2^27: no wrap
+                atomicAdd(&s_ws[warp][kWsTrials], (unsigned long long)n_trials);
+                n_trials = 0;
+            }
             prev = cur;
             pb = cb;
             phead = head;
@@ -470,6 +482,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const OocStepArgs a)
                     rec.hash_lo = (uint32_t)h;
                     rec.hash_hi = (uint32_t)(h >> 32);
                     a.walkers[idx] = rec;
+                    flush();
                     active = false;
                 } else {
                     cb = nbx;
@@ -485,15 +498,12 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const OocStepArgs a)
         }
     }
 
-    n_steps = warp_sum(n_steps);
-    n_trials = warp_sum(n_trials);
-    n_done = warp_sum(n_done);
-    hsum = warp_sum(hsum);
+    __syncwarp();
     if (lane == 0) {
-        atomicAdd(&a.ctr[kCtrSteps], n_steps);
-        atomicAdd(&a.ctr[kCtrTrials], n_trials);
-        atomicAdd(&a.ctr[kCtrDone], n_done);
-        atomicAdd(&a.ctr[kCtrHashSum], hsum);
+        atomicAdd(&a.ctr[kCtrSteps], s_ws[warp][kWsSteps]);
+        atomicAdd(&a.ctr[kCtrTrials], s_ws[warp][kWsTrials]);
+        atomicAdd(&a.ctr[kCtrDone], s_ws[warp][kWsDone]);
+        atomicAdd(&a.ctr[kCtrHashSum], s_ws[warp][kWsHash]);
     }
 }
 

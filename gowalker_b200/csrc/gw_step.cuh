@@ -13,7 +13,10 @@
 //             alpha/(float)prev_deg in fp32 (323-326); the x==prev compare is
 //             fp64 (341), the others fp32 (334, 368, 373).
 // Every rounding step is an explicit _rn intrinsic so no contraction or
-// fast-math flag can change a bit.
+// fast-math flag can change a bit.  The fp64 compare is carried out in fp32
+// without changing a verdict: for a float rv and a double T,
+// (double)rv < T  <=>  rv < RU(T), RU(T) the smallest float >= T (if T is a
+// float, RU(T) = T; otherwise every float below RU(T) is below T).
 #pragma once
 #include <cstdint>
 #include "gw_philox.cuh"
@@ -31,39 +34,58 @@ struct StepConsts {
     double one_m_alpha;        // 1.0 - (double)alpha
 };
 
-// Thresholds of one step (depend on deg / prev_deg for SOPR).
+// Per-step thresholds.  Node2vec's are run constants and live in
+// StepConsts; SOPR/SOSR's depend on deg and prev_deg and take three floats.
 struct StepThr {
-    float maxv, minv;
-    float t_prev;      // Node2vec: x == prev accepts below 1/p
-    float t_found;     // x in N(prev)
-    float t_notfound;  // otherwise
-    double t_prev_d;   // SOPR: x == prev accepts below (1-alpha)/deg in fp64
+    float inv_deg;  // (float)((1-alpha)/deg), divided in fp64
+    float sum;      // inv_deg + alpha/(float)prev_deg
+    float t_prev;   // RU((1-alpha)/deg): x == prev accepts iff rv < t_prev
 };
 
 template <bool SOPR>
 __device__ __forceinline__ StepThr step_thresholds(const StepConsts &c, uint64_t deg, uint64_t pdeg)
 {
-    StepThr t;
-    if constexpr (!SOPR) {
-        t.maxv = c.n2v_maxv;
-        t.minv = c.n2v_minv;
-        t.t_prev = c.inv_p;
-        t.t_found = 1.0f;
-        t.t_notfound = c.inv_q;
-        t.t_prev_d = 0.0;
-    } else {
+    StepThr t{0.f, 0.f, 0.f};
+    if constexpr (SOPR) {
         const double tp = __ddiv_rn(c.one_m_alpha, (double)deg);
-        const float inv_deg = __double2float_rn(tp);
+        t.inv_deg = __double2float_rn(tp);
         const float inv_prev = __fdiv_rn(c.alpha, __ull2float_rn((unsigned long long)pdeg));
-        const float sum = __fadd_rn(inv_deg, inv_prev);
-        t.maxv = (inv_deg < sum) ? sum : inv_deg;   // std::max(inv_deg, sum)
-        t.minv = (sum < inv_deg) ? sum : inv_deg;   // std::min(inv_deg, sum)
-        t.t_prev = 0.f;
-        t.t_found = sum;
-        t.t_notfound = inv_deg;
-        t.t_prev_d = tp;
+        t.sum = __fadd_rn(t.inv_deg, inv_prev);
+        t.t_prev = __double2float_ru(tp);
     }
     return t;
+}
+
+// The five thresholds of a trial (engine/engine.hpp:209-258, 334-375).
+template <bool SOPR>
+__device__ __forceinline__ float thr_max(const StepConsts &c, const StepThr &t)
+{
+    if constexpr (SOPR) return (t.inv_deg < t.sum) ? t.sum : t.inv_deg;  // std::max(inv_deg, sum)
+    else return c.n2v_maxv;
+}
+template <bool SOPR>
+__device__ __forceinline__ float thr_min(const StepConsts &c, const StepThr &t)
+{
+    if constexpr (SOPR) return (t.sum < t.inv_deg) ? t.sum : t.inv_deg;  // std::min(inv_deg, sum)
+    else return c.n2v_minv;
+}
+template <bool SOPR>
+__device__ __forceinline__ float thr_prev(const StepConsts &c, const StepThr &t)
+{
+    if constexpr (SOPR) return t.t_prev;
+    else return c.inv_p;
+}
+template <bool SOPR>
+__device__ __forceinline__ float thr_found(const StepConsts &c, const StepThr &t)
+{
+    if constexpr (SOPR) return t.sum;
+    else return 1.0f;
+}
+template <bool SOPR>
+__device__ __forceinline__ float thr_notfound(const StepConsts &c, const StepThr &t)
+{
+    if constexpr (SOPR) return t.inv_deg;
+    else return c.inv_q;
 }
 
 __device__ __forceinline__ U4 draw(const StepConsts &c, uint32_t wid, uint32_t hop, uint32_t attempt)
@@ -96,20 +118,17 @@ __device__ __forceinline__ bool search_sorted(const uint32_t *__restrict__ base,
 }
 
 // Acceptance of candidate x drawn with rand value rv (engine/engine.hpp:209-258,
-// 334-375).  `searched` gets the membership result when a search ran.
+// 334-375).
 template <bool SOPR>
-__device__ __forceinline__ bool accept_candidate(const StepThr &t, float rv, uint32_t x, uint32_t prev,
-                                                 uint32_t cur, const uint32_t *__restrict__ prev_adj,
+__device__ __forceinline__ bool accept_candidate(const StepConsts &c, const StepThr &t, float rv, uint32_t x,
+                                                 uint32_t prev, uint32_t cur, const uint32_t *__restrict__ prev_adj,
                                                  uint32_t pdeg)
 {
-    if (rv <= t.minv) return true;
-    if (x == prev) {
-        if constexpr (SOPR) return (double)rv < t.t_prev_d;
-        else return rv < t.t_prev;
-    }
+    if (rv <= thr_min<SOPR>(c, t)) return true;
+    if (x == prev) return rv < thr_prev<SOPR>(c, t);
     // x is drawn from N(cur); when prev == cur the search must succeed.
     const bool found = (prev == cur) ? true : search_sorted(prev_adj, pdeg, x);
-    return found ? (rv < t.t_found) : (rv < t.t_notfound);
+    return found ? (rv < thr_found<SOPR>(c, t)) : (rv < thr_notfound<SOPR>(c, t));
 }
 
 // A walker whose step has already rejected this many attempts is served by
@@ -129,15 +148,15 @@ __device__ __forceinline__ T *shfl_ptr(T *p, int src)
     return reinterpret_cast<T *>(shfl64(reinterpret_cast<uint64_t>(p), src));
 }
 
+template <bool SOPR>
 __device__ __forceinline__ StepThr shfl_thr(const StepThr &t, int src)
 {
-    StepThr o;
-    o.maxv = __shfl_sync(0xFFFFFFFFu, t.maxv, src);
-    o.minv = __shfl_sync(0xFFFFFFFFu, t.minv, src);
-    o.t_prev = __shfl_sync(0xFFFFFFFFu, t.t_prev, src);
-    o.t_found = __shfl_sync(0xFFFFFFFFu, t.t_found, src);
-    o.t_notfound = __shfl_sync(0xFFFFFFFFu, t.t_notfound, src);
-    o.t_prev_d = __shfl_sync(0xFFFFFFFFu, t.t_prev_d, src);
+    StepThr o{0.f, 0.f, 0.f};
+    if constexpr (SOPR) {
+        o.inv_deg = __shfl_sync(0xFFFFFFFFu, t.inv_deg, src);
+        o.sum = __shfl_sync(0xFFFFFFFFu, t.sum, src);
+        o.t_prev = __shfl_sync(0xFFFFFFFFu, t.t_prev, src);
+    }
     return o;
 }
 
@@ -236,13 +255,12 @@ __device__ __forceinline__ uint32_t warp_first_accept_runs(const StepConsts &c, 
     uint32_t kq;
     {
         const uint32_t which = lane & 3u;
+        const float maxv = thr_max<SOPR>(c, t);
+        const float bound = which == 0 ? thr_min<SOPR>(c, t) : which == 1 ? thr_prev<SOPR>(c, t)
+                                       : which == 2 ? thr_found<SOPR>(c, t) : thr_notfound<SOPR>(c, t);
         kq = rand_prefix([&](uint32_t k) {
-            const float rv = rand_val(k << 8, t.maxv);
-            bool prev_ok;
-            if constexpr (SOPR) prev_ok = (double)rv < t.t_prev_d;
-            else prev_ok = rv < t.t_prev;
-            return which == 0 ? (rv <= t.minv) : which == 1 ? prev_ok : which == 2 ? (rv < t.t_found)
-                                                                                    : (rv < t.t_notfound);
+            const float rv = rand_val(k << 8, maxv);
+            return which == 0 ? (rv <= bound) : (rv < bound);
         });
     }
     const uint32_t k_min = __shfl_sync(0xFFFFFFFFu, kq, 0), k_prev = __shfl_sync(0xFFFFFFFFu, kq, 1);
@@ -319,6 +337,7 @@ __device__ __forceinline__ uint32_t warp_first_accept(const StepConsts &c, const
         return warp_first_accept_runs<SOPR>(c, t, wid, hop, p0, limit, cand, deg, prev, prev_adj, pdeg, iv, x_out);
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t M = fastmod_magic(deg);
+    const float maxv = thr_max<SOPR>(c, t);
     for (uint32_t base = p0; base < limit; base += 32) {
         const uint32_t att = base + lane;
         bool acc = false;
@@ -326,9 +345,9 @@ __device__ __forceinline__ uint32_t warp_first_accept(const StepConsts &c, const
         if (att < limit) {
             const U4 r = draw(c, wid, hop, att);
             const uint32_t pos = fastmod(r.x, M, deg);
-            const float rv = rand_val(r.y, t.maxv);
+            const float rv = rand_val(r.y, maxv);
             x = __ldg(cand + pos);
-            acc = accept_candidate<SOPR>(t, rv, x, prev, cur, prev_adj, pdeg);
+            acc = accept_candidate<SOPR>(c, t, rv, x, prev, cur, prev_adj, pdeg);
         }
         const unsigned m = __ballot_sync(0xFFFFFFFFu, acc);
         if (m) {

@@ -24,8 +24,12 @@ template <bool SOPR, bool PATHS, bool COOP, int MINB>
 __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const IncoreArgs a)
 {
     __shared__ uint32_t s_iv[kWalkThreads / 32][kCoopScratchWords];  // per-warp scratch of warp_first_accept
+    __shared__ unsigned long long s_ws[kWalkThreads / 32][kWsCount];  // per-warp statistics
+    const uint32_t warp = threadIdx.x >> 5;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
+    if (lane < kWsCount) s_ws[warp][lane] = 0;
+    __syncwarp();
     const uint64_t *__restrict__ beg = a.beg;
     const uint32_t *__restrict__ csr = a.csr;
     const uint32_t maxhops = a.c.maxhops;
@@ -34,20 +38,27 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const Incore
     bool exhausted = false;          // warp-uniform
     bool active = false;
 
+    // Lane state.  Statistics live in s_ws and the path row is recomputed
+    // from wid, so the registers hold only what the next trial reads.
     uint32_t wid = 0, prev = 0, cur = 0, hop = 0, attempt = 0;
     uint32_t deg = 0, pdeg = 0;
     uint64_t head = 0, phead = 0, h = 0;
     U4 r{0, 0, 0, 0};
-    StepThr t{};
-    uint32_t *prow = nullptr;
-    unsigned long long n_steps = 0, n_trials = 0, n_done = 0, hsum = 0;
-    unsigned long long n_cs = 0, n_csa = 0, n_cl = 0, n_cla = 0;  // cooperative steps / attempts by path
+    StepThr t{0.f, 0.f, 0.f};
+    uint32_t n_trials = 0;  // trials not yet added to s_ws
 
+    auto flush_trials = [&]() {
+        atomicAdd(&s_ws[warp][kWsTrials], (unsigned long long)n_trials);
+        n_trials = 0;
+    };
+    // A walker's steps are its hops: every accepted trial moves it one hop.
     auto finish = [&]() {
         a.hashes[wid] = h;
         a.lens[wid] = hop + 1;
-        hsum += h;
-        n_done++;
+        atomicAdd(&s_ws[warp][kWsSteps], (unsigned long long)hop);
+        atomicAdd(&s_ws[warp][kWsDone], 1ull);
+        atomicAdd(&s_ws[warp][kWsHash], (unsigned long long)h);
+        flush_trials();
         active = false;
     };
 
@@ -75,10 +86,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const Incore
                 prev = cur = src;
                 hop = 0;
                 h = hash_init(src);
-                if (PATHS) {
-                    prow = a.paths + (uint64_t)wid * a.stride;
-                    prow[0] = src;
-                }
+                if (PATHS) a.paths[(uint64_t)wid * a.stride] = src;
                 if (src >= a.nverts) {
                     atomicOr(a.err, kErrSource);
                     finish();
@@ -104,8 +112,8 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const Incore
         if (!__any_sync(0xFFFFFFFFu, active)) break;
 
         // Walkers whose step keeps rejecting (a low-degree prev next to a hub
-        // under SOPR) are served one at a time by the whole warp, 32 attempts
-        // per round; the lane then re-takes the accepting attempt below.
+        // under SOPR) are served one at a time by the whole warp; the lane
+        // then re-takes the accepting attempt below.
         for (unsigned hm = COOP ? __ballot_sync(0xFFFFFFFFu, active && attempt > kHardAttempts) : 0u; hm;
              hm &= hm - 1) {
             const int L = __ffs(hm) - 1;
@@ -113,19 +121,15 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const Incore
             const uint64_t hd = shfl64(head, L), ph = shfl64(phead, L);
             uint32_t xs;
             const uint32_t astar = warp_first_accept<SOPR>(
-                a.c, shfl_thr(t, L), __shfl_sync(0xFFFFFFFFu, wid, L), __shfl_sync(0xFFFFFFFFu, hop, L), p0,
+                a.c, shfl_thr<SOPR>(t, L), __shfl_sync(0xFFFFFFFFu, wid, L), __shfl_sync(0xFFFFFFFFu, hop, L), p0,
                 kMaxAttempts, csr + hd, __shfl_sync(0xFFFFFFFFu, deg, L), __shfl_sync(0xFFFFFFFFu, prev, L),
-                __shfl_sync(0xFFFFFFFFu, cur, L), csr + ph, __shfl_sync(0xFFFFFFFFu, pdeg, L), s_iv[threadIdx.x >> 5],
-                &xs);
+                __shfl_sync(0xFFFFFFFFu, cur, L), csr + ph, __shfl_sync(0xFFFFFFFFu, pdeg, L), s_iv[warp], &xs);
             if (lane == (uint32_t)L) {
                 n_trials += astar - p0;
-                if (pdeg < 32 && prev != cur) {
-                    n_cs++;
-                    n_csa += astar - p0 + 1;
-                } else {
-                    n_cl++;
-                    n_cla += astar - p0 + 1;
-                }
+                const bool by_pos = pdeg < 32 && prev != cur;
+                atomicAdd(&s_ws[warp][by_pos ? kWsCoopSmall : kWsCoopLarge], 1ull);
+                atomicAdd(&s_ws[warp][by_pos ? kWsCoopSmallAtt : kWsCoopLargeAtt],
+                          (unsigned long long)(astar - p0 + 1));
                 if (astar >= kMaxAttempts) {
                     atomicOr(a.err, kErrTrials);
                     finish();
@@ -139,14 +143,14 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const Incore
 
         // One rejection-sampling trial.
         const uint32_t pos = r.x % deg;
-        const float rv = rand_val(r.y, t.maxv);
+        const float rv = rand_val(r.y, thr_max<SOPR>(a.c, t));
         const uint32_t x = __ldg(csr + head + pos);
         n_trials++;
-        if (accept_candidate<SOPR>(t, rv, x, prev, cur, csr + phead, pdeg)) {
+        if (accept_candidate<SOPR>(a.c, t, rv, x, prev, cur, csr + phead, pdeg)) {
             hop++;
-            n_steps++;
             h = hash_step(h, x);
-            if (PATHS) prow[hop] = x;
+            if (PATHS) a.paths[(uint64_t)wid * a.stride + hop] = x;
+            if (n_trials & 0x80000000u) flush_trials();  // a step adds < 2^27: no wrap
             prev = cur;
             phead = head;
             pdeg = deg;
@@ -185,24 +189,17 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const Incore
         }
     }
 
-    n_steps = warp_sum(n_steps);
-    n_trials = warp_sum(n_trials);
-    n_done = warp_sum(n_done);
-    hsum = warp_sum(hsum);
-    n_cs = warp_sum(n_cs);
-    n_csa = warp_sum(n_csa);
-    n_cl = warp_sum(n_cl);
-    n_cla = warp_sum(n_cla);
+    __syncwarp();
     if (lane == 0) {
-        atomicAdd(&a.ctr[kCtrSteps], n_steps);
-        atomicAdd(&a.ctr[kCtrTrials], n_trials);
-        atomicAdd(&a.ctr[kCtrDone], n_done);
-        atomicAdd(&a.ctr[kCtrHashSum], hsum);
+        atomicAdd(&a.ctr[kCtrSteps], s_ws[warp][kWsSteps]);
+        atomicAdd(&a.ctr[kCtrTrials], s_ws[warp][kWsTrials]);
+        atomicAdd(&a.ctr[kCtrDone], s_ws[warp][kWsDone]);
+        atomicAdd(&a.ctr[kCtrHashSum], s_ws[warp][kWsHash]);
         if (COOP) {
-            atomicAdd(&a.ctr[kCtrCoopSmall], n_cs);
-            atomicAdd(&a.ctr[kCtrCoopSmallAtt], n_csa);
-            atomicAdd(&a.ctr[kCtrCoopLarge], n_cl);
-            atomicAdd(&a.ctr[kCtrCoopLargeAtt], n_cla);
+            atomicAdd(&a.ctr[kCtrCoopSmall], s_ws[warp][kWsCoopSmall]);
+            atomicAdd(&a.ctr[kCtrCoopSmallAtt], s_ws[warp][kWsCoopSmallAtt]);
+            atomicAdd(&a.ctr[kCtrCoopLarge], s_ws[warp][kWsCoopLarge]);
+            atomicAdd(&a.ctr[kCtrCoopLargeAtt], s_ws[warp][kWsCoopLargeAtt]);
         }
     }
 }

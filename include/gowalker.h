@@ -15,8 +15,10 @@
  *     failure on a handle.
  *   - Plain pointers and sizes only.  Host buffers passed to gw_host_block are
  *     borrowed for the life of the handle (the reference keeps every block in
- *     pinned host memory, engine/engine.hpp:74-77); pin them (cudaHostAlloc or
- *     cudaHostRegister) for full copy bandwidth.
+ *     pinned host memory, engine/engine.hpp:74-77); pin them (gw_host_alloc,
+ *     cudaHostAlloc or cudaHostRegister) for full copy bandwidth.  The
+ *     zero-copy tail reads pinned, mapped blocks in place and stages pageable
+ *     ones into pinned memory of its own (it never registers caller pages).
  *   - One host thread per handle.  The handle owns its device memory and its
  *     CUDA streams.
  *   - Walks are bit-identical to the reference CPU step rule

@@ -1,6 +1,8 @@
 """GPU tests of the out-of-core path: device block cache, bucketing, block
 choice, zero-copy tail.  Walks must be bit-identical to the oracle whatever
 the cache size or schedule (counter-based draws)."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -92,3 +94,29 @@ def test_ooc_rejects_tiny_cache(gw, oracle):
     beg, csr = graph(oracle)
     with pytest.raises(gw.GwError):
         run_ooc(gw, beg, csr, 8, 1)
+
+
+def test_zero_copy_leaves_neighbouring_host_data_writable(gw, oracle):
+    """The zero-copy tail maps host blocks page by page.  Results copied back
+    into host memory that shares a page with a mapped block must still land."""
+    beg, csr = graph(oracle, scale=13, ef=12, sym=True, cap=7000, seed=3)
+    V = len(beg) - 1
+    arena = np.zeros(V + 1 + V, dtype=np.uint64)   # offsets, then the hash output in the same pages
+    arena[:V + 1] = beg
+    from gowalker_b200.preprocess import split_equal_edge_mass
+    vb, eb = split_equal_edge_mass(beg, 10)
+    maxv = int(np.diff(vb.astype(np.int64)).max())
+    maxe = int(np.diff(eb.astype(np.int64)).max())
+    slot = ((maxv + 2) & ~1) * 8 + ((max(maxe, 1) + 3) & ~3) * 4
+    eng = gw.WalkEngine(algorithm=1, maxhops=20, alpha=0.2, term_prob=0.15, seed=5, walkpersource=1,
+                        record_paths=0, cache_size=slot * 3, zero_copy=1, zero_threshold=400)
+    eng.set_host_graph(arena[:V + 1], csr, vb, eb)
+    eng.init_walkers(1, 1, 5)
+    st = eng.run()
+    assert st["zero_copy_steps"] > 0
+    out = arena[V + 1:]
+    eng._check(eng.L.gw_path_hashes(eng.h, 0, V, out.ctypes.data_as(ctypes.c_void_p)))
+    ref = oracle.walk(beg, csr, oracle.make_cfg(algo=1, maxhops=20, alpha=0.2, term_prob=0.15, seed=5), 0, V,
+                      paths=False)
+    assert np.array_equal(out, ref["hashes"])
+    eng.close()
