@@ -468,6 +468,7 @@ int gw_handle::run_incore(gw_stats *stats)
     a.csr = dev_csr;
     a.nverts = nverts;
     a.nwalkers = (uint32_t)nwalkers;
+    a.wid_stride = 1;
     a.paths = (cfg.record_paths == GW_PATHS_FULL) ? d_paths : nullptr;
     a.stride = cfg.maxhops + 1;
     a.lens = d_lens;
@@ -479,15 +480,25 @@ int gw_handle::run_incore(gw_stats *stats)
     const int combo = (sopr ? 4 : 0) | (a.paths ? 2 : 0) | (coop ? 1 : 0);
     int variant = tuned_variant[combo];
     if (cfg.blockpergrid == 0 && variant < 0) {
-        // Autotuner: time each register-cap variant on one slice of this
-        // run's walkers (their outputs are rewritten by the full run below)
-        // and keep the fastest for every later run of this kernel class.
-        const uint64_t ns = std::min<uint64_t>(nwalkers, std::max<uint64_t>((uint64_t)num_sms * 4096, nwalkers / 16));
+        // Autotuner: time each register-cap variant on this run's walkers
+        // (their outputs are rewritten by the full run below) and keep the
+        // fastest for every later run of this kernel class.  Runs of up to
+        // 2^22 walkers are timed whole: with few walkers per lane the tail of
+        // the last round decides, and a part of the run would misrank the
+        // variants.  Larger runs are timed on every 16th walker id, which
+        // keeps the run's mix of source degrees (R-MAT ids are not random in
+        // degree, so a contiguous range would not).  Variants run in a
+        // forward then a reverse pass and keep their best time, so none
+        // gains from the caches the previous one warmed.
+        const uint32_t stride = nwalkers > (1ull << 22) ? 16u : 1u;
         IncoreArgs c = a;
-        c.wid_base = (uint32_t)((nwalkers - ns) * 3 / 8);
-        c.nwalkers = (uint32_t)ns;
+        c.wid_base = 0;
+        c.wid_stride = stride;
+        c.nwalkers = (uint32_t)(nwalkers / stride);
         float best = 1e30f;
-        for (int v = 0; v < kIncoreVariants; ++v) {
+        for (int v = 0; v < kIncoreVariants; ++v) tuned_ms[combo][v] = 1e30f;
+        for (int i = 0; i < 2 * kIncoreVariants; ++i) {
+            const int v = i < kIncoreVariants ? i : 2 * kIncoreVariants - 1 - i;
             if ((st = cuda(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * kCtrCount, s), "memset"))) return st;
             if ((st = cuda(cudaEventRecord(ev_kernel0, s), "event"))) return st;
             if ((st = cuda(launch_walk_incore(c, sopr, coop, v, incore_grid(sopr, c.paths != nullptr, coop, v, num_sms), s),
@@ -497,7 +508,7 @@ int gw_handle::run_incore(gw_stats *stats)
             if ((st = cuda(cudaEventSynchronize(ev_kernel1), "tuning"))) return st;
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ev_kernel0, ev_kernel1);
-            tuned_ms[combo][v] = ms;
+            tuned_ms[combo][v] = std::min(tuned_ms[combo][v], ms);
             if (ms < best) {
                 best = ms;
                 variant = v;

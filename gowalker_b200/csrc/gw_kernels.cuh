@@ -68,8 +68,9 @@ struct IncoreArgs {
     const uint64_t *beg;       // nverts+1 global offsets
     const uint32_t *csr;       // nedges neighbour ids
     uint32_t nverts;
-    uint32_t nwalkers;         // walkers of this launch: ids wid_base .. wid_base+nwalkers-1
+    uint32_t nwalkers;         // walkers of this launch: ids wid_base + i * wid_stride, i < nwalkers
     uint32_t wid_base;
+    uint32_t wid_stride;       // 1 for a run; > 1 for the autotuner's sample
     uint32_t *paths;           // rows indexed by walker id, or null
     uint32_t stride;           // maxhops + 1
     uint32_t *lens;            // vertices per path
@@ -99,8 +100,8 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
 }
 
 // Grid size (CTAs) for a persistent walk kernel on this device.
-// `variant` selects the register cap (0: 3 CTAs/SM, 1: 4, 2: 6), see gw_walk.cu.
-constexpr int kIncoreVariants = 3;
+// `variant` selects the register cap (0: 4 CTAs/SM, 1: 5, 2: 6, 3: 8), see gw_walk.cu.
+constexpr int kIncoreVariants = 4;
 int incore_grid(bool sopr, bool paths, bool coop, int variant, int num_sms);
 cudaError_t launch_walk_incore(const IncoreArgs &a, bool sopr, bool coop, int variant, int grid, cudaStream_t s);
 

@@ -119,6 +119,7 @@ extern "C" int gw_walk_noalloc(const gw_config *cfg, const uint64_t *d_beg, cons
     a.csr = d_csr;
     a.nverts = nverts;
     a.nwalkers = (uint32_t)nwalkers;
+    a.wid_stride = 1;
     a.paths = (cfg->record_paths == GW_PATHS_FULL) ? d_paths : nullptr;
     a.stride = cfg->maxhops + 1;
     a.lens = d_lens;
@@ -127,7 +128,7 @@ extern "C" int gw_walk_noalloc(const gw_config *cfg, const uint64_t *d_beg, cons
     a.err = err;
     const bool sopr = cfg->algorithm != GW_NODE2VEC;
     const bool coop = needs_coop(cfg->algorithm, a.c);
-    const int variant = 1;  // 4 CTAs per SM; this entry point keeps no tuning state
+    const int variant = 1;  // 5 CTAs per SM; this entry point keeps no tuning state
     const int grid =
         cfg->blockpergrid ? (int)cfg->blockpergrid : incore_grid(sopr, a.paths != nullptr, coop, variant, num_sms);
     e = launch_walk_incore(a, sopr, coop, variant, grid, s);

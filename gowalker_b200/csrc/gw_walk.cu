@@ -20,11 +20,19 @@
 
 namespace gw {
 
+// Words of a lane's walker parked in shared memory while its warp serves hard
+// steps (kPkAstar receives the accepting attempt found for it).
+enum ParkWord : int {
+    kPkWid = 0, kPkPrev, kPkCur, kPkHop, kPkAttempt, kPkDeg, kPkPdeg, kPkHeadLo, kPkHeadHi, kPkPheadLo,
+    kPkPheadHi, kPkHashLo, kPkHashHi, kPkThr0, kPkThr1, kPkThr2, kPkRx, kPkRy, kPkTrials, kPkAstar, kPkCount
+};
+
 template <bool SOPR, bool PATHS, bool COOP, int MINB>
 __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const IncoreArgs a)
 {
     __shared__ uint32_t s_iv[kWalkThreads / 32][kCoopScratchWords];  // per-warp scratch of warp_first_accept
     __shared__ unsigned long long s_ws[kWalkThreads / 32][kWsCount];  // per-warp statistics
+    __shared__ uint32_t s_park[COOP ? kWalkThreads / 32 : 1][kPkCount][32];  // lane state during hard steps
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
@@ -81,7 +89,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const Incore
             const uint32_t avail = q_end - q_next;
             const uint32_t rank = __popc(need & lt_mask);
             if (!active && rank < avail) {
-                wid = a.wid_base + q_next + rank;
+                wid = a.wid_base + (q_next + rank) * a.wid_stride;
                 const uint32_t src = walker_source(a.init, wid);
                 prev = cur = src;
                 hop = 0;
@@ -113,30 +121,82 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const Incore
 
         // Walkers whose step keeps rejecting (a low-degree prev next to a hub
         // under SOPR) are served one at a time by the whole warp; the lane
-        // then re-takes the accepting attempt below.
-        for (unsigned hm = COOP ? __ballot_sync(0xFFFFFFFFu, active && attempt > kHardAttempts) : 0u; hm;
-             hm &= hm - 1) {
-            const int L = __ffs(hm) - 1;
-            const uint32_t p0 = __shfl_sync(0xFFFFFFFFu, attempt, L) - 1;
-            const uint64_t hd = shfl64(head, L), ph = shfl64(phead, L);
-            uint32_t xs;
-            const uint32_t astar = warp_first_accept<SOPR>(
-                a.c, shfl_thr<SOPR>(t, L), __shfl_sync(0xFFFFFFFFu, wid, L), __shfl_sync(0xFFFFFFFFu, hop, L), p0,
-                kMaxAttempts, csr + hd, __shfl_sync(0xFFFFFFFFu, deg, L), __shfl_sync(0xFFFFFFFFu, prev, L),
-                __shfl_sync(0xFFFFFFFFu, cur, L), csr + ph, __shfl_sync(0xFFFFFFFFu, pdeg, L), s_iv[warp], &xs);
-            if (lane == (uint32_t)L) {
-                n_trials += astar - p0;
-                const bool by_pos = pdeg < 32 && prev != cur;
-                atomicAdd(&s_ws[warp][by_pos ? kWsCoopSmall : kWsCoopLarge], 1ull);
-                atomicAdd(&s_ws[warp][by_pos ? kWsCoopSmallAtt : kWsCoopLargeAtt],
-                          (unsigned long long)(astar - p0 + 1));
-                if (astar >= kMaxAttempts) {
-                    atomicOr(a.err, kErrTrials);
-                    finish();
-                } else {
-                    r = draw(a.c, wid, hop, astar);
-                    attempt = astar + 1;
+        // then re-takes the accepting attempt below.  Meanwhile every lane's
+        // walker is parked in shared memory: the registers go to the attempt
+        // loop, and lane L's fields reach all lanes as broadcast loads.
+        if (COOP) {
+            const unsigned hm = __ballot_sync(0xFFFFFFFFu, active && attempt > kHardAttempts);
+            if (hm) {
+                uint32_t(*pk)[32] = s_park[COOP ? warp : 0];
+                pk[kPkWid][lane] = wid;
+                pk[kPkPrev][lane] = prev;
+                pk[kPkCur][lane] = cur;
+                pk[kPkHop][lane] = hop;
+                pk[kPkAttempt][lane] = attempt;
+                pk[kPkDeg][lane] = deg;
+                pk[kPkPdeg][lane] = pdeg;
+                pk[kPkHeadLo][lane] = (uint32_t)head;
+                pk[kPkHeadHi][lane] = (uint32_t)(head >> 32);
+                pk[kPkPheadLo][lane] = (uint32_t)phead;
+                pk[kPkPheadHi][lane] = (uint32_t)(phead >> 32);
+                pk[kPkHashLo][lane] = (uint32_t)h;
+                pk[kPkHashHi][lane] = (uint32_t)(h >> 32);
+                pk[kPkThr0][lane] = __float_as_uint(t.inv_deg);
+                pk[kPkThr1][lane] = __float_as_uint(t.sum);
+                pk[kPkThr2][lane] = __float_as_uint(t.t_prev);
+                pk[kPkRx][lane] = r.x;
+                pk[kPkRy][lane] = r.y;
+                pk[kPkTrials][lane] = n_trials;
+                __syncwarp();
+                for (unsigned m = hm; m; m &= m - 1) {
+                    const int L = __ffs(m) - 1;
+                    const uint32_t p0 = pk[kPkAttempt][L] - 1;
+                    const uint32_t Lprev = pk[kPkPrev][L], Lcur = pk[kPkCur][L], Lpdeg = pk[kPkPdeg][L];
+                    const uint64_t hd = ((uint64_t)pk[kPkHeadHi][L] << 32) | pk[kPkHeadLo][L];
+                    const uint64_t ph = ((uint64_t)pk[kPkPheadHi][L] << 32) | pk[kPkPheadLo][L];
+                    const StepThr tl{__uint_as_float(pk[kPkThr0][L]), __uint_as_float(pk[kPkThr1][L]),
+                                     __uint_as_float(pk[kPkThr2][L])};
+                    uint32_t xs;
+                    const uint32_t astar = warp_first_accept<SOPR>(a.c, tl, pk[kPkWid][L], pk[kPkHop][L], p0,
+                                                                   kMaxAttempts, csr + hd, pk[kPkDeg][L], Lprev, Lcur,
+                                                                   csr + ph, Lpdeg, s_iv[warp], &xs);
+                    if (lane == 0) {
+                        pk[kPkAstar][L] = astar;
+                        const bool by_pos = Lpdeg < 32 && Lprev != Lcur;
+                        atomicAdd(&s_ws[warp][by_pos ? kWsCoopSmall : kWsCoopLarge], 1ull);
+                        atomicAdd(&s_ws[warp][by_pos ? kWsCoopSmallAtt : kWsCoopLargeAtt],
+                                  (unsigned long long)(astar - p0 + 1));
+                    }
                 }
+                __syncwarp();
+                wid = pk[kPkWid][lane];
+                prev = pk[kPkPrev][lane];
+                cur = pk[kPkCur][lane];
+                hop = pk[kPkHop][lane];
+                attempt = pk[kPkAttempt][lane];
+                deg = pk[kPkDeg][lane];
+                pdeg = pk[kPkPdeg][lane];
+                head = ((uint64_t)pk[kPkHeadHi][lane] << 32) | pk[kPkHeadLo][lane];
+                phead = ((uint64_t)pk[kPkPheadHi][lane] << 32) | pk[kPkPheadLo][lane];
+                h = ((uint64_t)pk[kPkHashHi][lane] << 32) | pk[kPkHashLo][lane];
+                t.inv_deg = __uint_as_float(pk[kPkThr0][lane]);
+                t.sum = __uint_as_float(pk[kPkThr1][lane]);
+                t.t_prev = __uint_as_float(pk[kPkThr2][lane]);
+                r.x = pk[kPkRx][lane];
+                r.y = pk[kPkRy][lane];
+                n_trials = pk[kPkTrials][lane];
+                if ((hm >> lane) & 1u) {
+                    const uint32_t astar = pk[kPkAstar][lane];
+                    n_trials += astar - (attempt - 1);
+                    if (astar >= kMaxAttempts) {
+                        atomicOr(a.err, kErrTrials);
+                        finish();
+                    } else {
+                        r = draw(a.c, wid, hop, astar);
+                        attempt = astar + 1;
+                    }
+                }
+                __syncwarp();
             }
         }
         if (!active) continue;
@@ -230,12 +290,13 @@ cudaError_t launch_validate_csr(const uint64_t *beg, const uint32_t *csr, uint32
 }
 
 // Register-cap variants the autotuner chooses between: at 256 threads per CTA,
-// 3, 4 or 6 resident CTAs per SM (<= 85, 64, 40 registers per thread).
+// 4, 5, 6 or 8 resident CTAs per SM (<= 64, 51, 40, 32 registers per thread).
 template <int V>
 struct MinBlocks;
-template <> struct MinBlocks<0> { static constexpr int value = 3; };
-template <> struct MinBlocks<1> { static constexpr int value = 4; };
+template <> struct MinBlocks<0> { static constexpr int value = 4; };
+template <> struct MinBlocks<1> { static constexpr int value = 5; };
 template <> struct MinBlocks<2> { static constexpr int value = 6; };
+template <> struct MinBlocks<3> { static constexpr int value = 8; };
 
 template <bool SOPR, bool PATHS, bool COOP, int V>
 static int grid_for(int num_sms)
@@ -258,7 +319,8 @@ static int grid_v(int variant, int num_sms)
 {
     if (variant == 0) return grid_for<SOPR, PATHS, COOP, 0>(num_sms);
     if (variant == 1) return grid_for<SOPR, PATHS, COOP, 1>(num_sms);
-    return grid_for<SOPR, PATHS, COOP, 2>(num_sms);
+    if (variant == 2) return grid_for<SOPR, PATHS, COOP, 2>(num_sms);
+    return grid_for<SOPR, PATHS, COOP, 3>(num_sms);
 }
 
 template <bool SOPR, bool PATHS, bool COOP>
@@ -266,7 +328,8 @@ static void launch_v(const IncoreArgs &a, int variant, int grid, cudaStream_t s)
 {
     if (variant == 0) launch_one<SOPR, PATHS, COOP, 0>(a, grid, s);
     else if (variant == 1) launch_one<SOPR, PATHS, COOP, 1>(a, grid, s);
-    else launch_one<SOPR, PATHS, COOP, 2>(a, grid, s);
+    else if (variant == 2) launch_one<SOPR, PATHS, COOP, 2>(a, grid, s);
+    else launch_one<SOPR, PATHS, COOP, 3>(a, grid, s);
 }
 
 int incore_grid(bool sopr, bool paths, bool coop, int variant, int num_sms)
