@@ -54,6 +54,7 @@ void gw::consts_from_config(const gw_config &c, StepConsts &k)
     k.alpha = c.alpha;
     k.term_prob = c.term_prob;
     k.one_m_alpha = 1.0 - (double)c.alpha;
+    philox_schedule(k.key0, k.key1, k.rk0, k.rk1);
 }
 
 static bool config_ok(const gw_config &c, std::string &why)

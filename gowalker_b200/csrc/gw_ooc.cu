@@ -366,24 +366,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     if ((st = bucketize(nlive))) return st;
 
     OocStepArgs a{};
-    // step constants as for the in-core kernel
-    {
-        StepConsts &k = a.c;
-        k.maxhops = cfg.maxhops;
-        k.key0 = (uint32_t)cfg.seed;
-        k.key1 = (uint32_t)(cfg.seed >> 32);
-        const float inv_p = 1.0f / cfg.p;
-        const float inv_q = 1.0f / cfg.q;
-        const float mx_q1 = (inv_q < 1.0f) ? 1.0f : inv_q;
-        const float mn_q1 = (1.0f < inv_q) ? 1.0f : inv_q;
-        k.n2v_maxv = (inv_p < mx_q1) ? mx_q1 : inv_p;
-        k.n2v_minv = (mn_q1 < inv_p) ? mn_q1 : inv_p;
-        k.inv_p = inv_p;
-        k.inv_q = inv_q;
-        k.alpha = cfg.alpha;
-        k.term_prob = cfg.term_prob;
-        k.one_m_alpha = 1.0 - (double)cfg.alpha;
-    }
+    consts_from_config(cfg, a.c);  // step constants as for the in-core kernel
     a.blk_beg = o.d_blk_beg;
     a.blk_csr = o.d_blk_csr;
     a.vstart = o.d_vstart;

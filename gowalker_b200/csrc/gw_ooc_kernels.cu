@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(1024) k_schedule(const uint32_t *__restrict__ 
 }
 
 template <bool SOPR, bool PATHS, bool COOP>
-__global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const OocStepArgs a)
+__global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant__ OocStepArgs a)
 {
     __shared__ uint32_t s_vs[kMaxBlocks + 1];
     __shared__ uint32_t s_iv[kWalkThreads / 32][kCoopScratchWords];

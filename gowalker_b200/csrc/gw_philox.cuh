@@ -62,6 +62,37 @@ GW_HD U4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint3
     return U4{c0, c1, c2, c3};
 }
 
+// The same generator with the key schedule given: rk0[r], rk1[r] are the
+// keys of round r (k + r * W, mod 2^32), philox_schedule() computes them.
+GW_HD U4 philox4x32_10_sched(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, const uint32_t *rk0,
+                             const uint32_t *rk1)
+{
+#if defined(__CUDA_ARCH__)
+#pragma unroll
+#endif
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = kPhiloxM0 * c0;
+        const uint32_t hi0 = mulhi32(kPhiloxM0, c0);
+        const uint32_t lo1 = kPhiloxM1 * c2;
+        const uint32_t hi1 = mulhi32(kPhiloxM1, c2);
+        const uint32_t n0 = hi1 ^ c1 ^ rk0[r];
+        const uint32_t n2 = hi0 ^ c3 ^ rk1[r];
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+    }
+    return U4{c0, c1, c2, c3};
+}
+
+inline void philox_schedule(uint32_t k0, uint32_t k1, uint32_t *rk0, uint32_t *rk1)
+{
+    for (int r = 0; r < 10; ++r) {
+        rk0[r] = k0 + (uint32_t)r * kPhiloxW0;
+        rk1[r] = k1 + (uint32_t)r * kPhiloxW1;
+    }
+}
+
 // Exact a % d for 32-bit a and d >= 1 by direct computation (Lemire, Kaser and
 // Kurz, "Faster remainder by direct computation", 2019): with the 64-bit
 // fraction M = ceil(2^64 / d), a % d = high64((M * a mod 2^64) * d).  M costs one

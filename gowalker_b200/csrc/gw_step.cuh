@@ -32,6 +32,7 @@ struct StepConsts {
     float alpha;               // SOPR/SOSR
     float term_prob;           // 0 = no termination draw
     double one_m_alpha;        // 1.0 - (double)alpha
+    uint32_t rk0[10], rk1[10]; // Philox key schedule: round r uses key + r * Weyl constant
 };
 
 // Per-step thresholds.  Node2vec's are run constants and live in
@@ -88,9 +89,12 @@ __device__ __forceinline__ float thr_notfound(const StepConsts &c, const StepThr
     else return c.inv_q;
 }
 
+// The walk draw.  The key schedule comes precomputed in the kernel's
+// parameters, so each round is two wide multiplies and two three-way xors
+// with a constant operand.
 __device__ __forceinline__ U4 draw(const StepConsts &c, uint32_t wid, uint32_t hop, uint32_t attempt)
 {
-    return philox4x32_10(wid, hop, attempt, kTagWalk, c.key0, c.key1);
+    return philox4x32_10_sched(wid, hop, attempt, kTagWalk, c.rk0, c.rk1);
 }
 
 __device__ __forceinline__ float rand_val(uint32_t y, float maxv)
@@ -194,6 +198,36 @@ __device__ __forceinline__ uint32_t rand_prefix(Pred pred)
     return lo;
 }
 
+// Integer bounds of a step's four rand-value tests, found by the whole warp:
+// lanes 8w..8w+7 compute bound w (0: rv <= min, 1: rv < prev, 2: rv < found,
+// 3: rv < notfound) and lane 8w returns it.  Each group tests the eight k
+// around the estimate bound / maxv * 2^24, within two of the true bound when
+// maxv and the bound are normal floats (one rounding of k * 2^-24 * maxv moves
+// it by at most half an ulp, i.e. by at most one step of k); a group whose
+// window does not bracket the bound falls back to rand_prefix.
+template <bool SOPR>
+__device__ __forceinline__ uint32_t rand_bounds(const StepConsts &c, const StepThr &t)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t which = lane >> 3;
+    const float maxv = thr_max<SOPR>(c, t);
+    const float bound = which == 0 ? thr_min<SOPR>(c, t) : which == 1 ? thr_prev<SOPR>(c, t)
+                      : which == 2 ? thr_found<SOPR>(c, t) : thr_notfound<SOPR>(c, t);
+    auto pred = [&](uint32_t k) {
+        const float rv = rand_val(k << 8, maxv);
+        return which == 0 ? (rv <= bound) : (rv < bound);
+    };
+    const double est = __dmul_rn(__ddiv_rn((double)bound, (double)maxv), 16777216.0);
+    const bool est_ok = est >= 0.0 && est <= 16777216.0;  // false for NaN
+    const int64_t base = (est_ok ? (int64_t)est : 0) - 4;
+    const int64_t kc = base + (int64_t)(lane & 7u);
+    const bool q = kc < 0 ? true : (kc >= (1 << 24) ? false : pred((uint32_t)kc));
+    const unsigned g = (__ballot_sync(0xFFFFFFFFu, q) >> (lane & 24u)) & 0xFFu;
+    // a bracket: true at the first candidate, false at the last, ones then zeros
+    if (est_ok && (g & 1u) && !(g & 0x80u) && g == (1u << __popc(g)) - 1u) return (uint32_t)(base + __popc(g));
+    return rand_prefix(pred);
+}
+
 // Hard steps whose prev has fewer than 32 neighbours are decided without
 // touching the candidate: a trial's verdict depends on x = cand[pos] only
 // through "x == prev" and "x in N(prev)", i.e. through whether pos falls in
@@ -251,20 +285,10 @@ __device__ __forceinline__ uint32_t warp_first_accept_runs(const StepConsts &c, 
             atomicOr(bm + w, mask);
         }
     }
-    // integer bounds of the four rand-value tests, one per lane of a quad
-    uint32_t kq;
-    {
-        const uint32_t which = lane & 3u;
-        const float maxv = thr_max<SOPR>(c, t);
-        const float bound = which == 0 ? thr_min<SOPR>(c, t) : which == 1 ? thr_prev<SOPR>(c, t)
-                                       : which == 2 ? thr_found<SOPR>(c, t) : thr_notfound<SOPR>(c, t);
-        kq = rand_prefix([&](uint32_t k) {
-            const float rv = rand_val(k << 8, maxv);
-            return which == 0 ? (rv <= bound) : (rv < bound);
-        });
-    }
-    const uint32_t k_min = __shfl_sync(0xFFFFFFFFu, kq, 0), k_prev = __shfl_sync(0xFFFFFFFFu, kq, 1);
-    const uint32_t k_found = __shfl_sync(0xFFFFFFFFu, kq, 2), k_nf = __shfl_sync(0xFFFFFFFFu, kq, 3);
+    // integer bounds of the four rand-value tests
+    const uint32_t kq = rand_bounds<SOPR>(c, t);
+    const uint32_t k_min = __shfl_sync(0xFFFFFFFFu, kq, 0), k_prev = __shfl_sync(0xFFFFFFFFu, kq, 8);
+    const uint32_t k_found = __shfl_sync(0xFFFFFFFFu, kq, 16), k_nf = __shfl_sync(0xFFFFFFFFu, kq, 24);
     const uint32_t k_fast = max(k_min, k_nf);
     const uint32_t plo = __shfl_sync(0xFFFFFFFFu, lo, (int)pdeg), phi = __shfl_sync(0xFFFFFFFFu, hi, (int)pdeg);
     const uint32_t m_lo = (uint32_t)M, m_hi = (uint32_t)(M >> 32);

@@ -28,7 +28,7 @@ enum ParkWord : int {
 };
 
 template <bool SOPR, bool PATHS, bool COOP, int MINB>
-__global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const IncoreArgs a)
+__global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const __grid_constant__ IncoreArgs a)
 {
     __shared__ uint32_t s_iv[kWalkThreads / 32][kCoopScratchWords];  // per-warp scratch of warp_first_accept
     __shared__ unsigned long long s_ws[kWalkThreads / 32][kWsCount];  // per-warp statistics

@@ -1,4 +1,5 @@
-// Test-only: the engine's fastmod (gw_philox.cuh) against the % operator.
+// Test-only: the engine's fastmod (gw_philox.cuh) against the % operator, and
+// its scheduled-key Philox against the plain one.
 #include <cstdint>
 #include <cstdio>
 #include <initializer_list>
@@ -24,6 +25,16 @@ int main()
     for (uint32_t d : {0xFFFFFFFFu, 0x80000000u, 0x80000001u, 3u, 641u}) {
         const uint64_t M = gw::fastmod_magic(d);
         for (uint64_t a = 0; a <= 0xFFFFFFFFull; a += 65537) { if (gw::fastmod((uint32_t)a, M, d) != (uint32_t)a % d) { printf("FAIL %llu %u\n", (unsigned long long)a, d); return 1; } ++checked; }
+    }
+    for (int k = 0; k < 20000; ++k) {
+        const uint32_t k0 = (uint32_t)next(), k1 = (uint32_t)next();
+        uint32_t rk0[10], rk1[10];
+        gw::philox_schedule(k0, k1, rk0, rk1);
+        const uint32_t c0 = (uint32_t)next(), c1 = (uint32_t)next(), c2 = (uint32_t)next(), c3 = (uint32_t)next();
+        const gw::U4 a = gw::philox4x32_10(c0, c1, c2, c3, k0, k1);
+        const gw::U4 b = gw::philox4x32_10_sched(c0, c1, c2, c3, rk0, rk1);
+        if (a.x != b.x || a.y != b.y || a.z != b.z || a.w != b.w) { printf("FAIL philox schedule\n"); return 1; }
+        ++checked;
     }
     printf("ok %llu\n", (unsigned long long)checked);
     return 0;

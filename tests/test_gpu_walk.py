@@ -277,3 +277,51 @@ def test_c2_sopr_sample_vs_oracle(gw, oracle):
     assert st["coop_small_steps"] > 0 and st["coop_large_steps"] > 0
     eng.close()
     dg.free()
+
+
+def _ru32(x):
+    """Smallest float32 >= the float64 x."""
+    f = np.float32(x)
+    return f if float(f) >= x else np.nextafter(f, np.float32(np.inf))
+
+
+def test_windowed_rand_bounds_match_search(tmp_path):
+    """The cooperative step's integer rand bounds (an estimate checked on an
+    eight-wide window) equal the exhaustive binary search's."""
+    so = tmp_path / "rb.so"
+    subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-shared", "-Xcompiler", "-fPIC",
+                    "-I", os.path.join(ROOT, "gowalker_b200", "csrc"), "-o", str(so),
+                    os.path.join(ROOT, "tests", "cuda", "rand_bounds_check.cu")], check=True)
+    L = ctypes.CDLL(str(so))
+    rng = np.random.default_rng(7)
+    rows = []
+    # SOPR thresholds as the kernels form them, from (deg, prev_deg, alpha)
+    for _ in range(3000):
+        deg = int(rng.integers(1, 1 << int(rng.integers(1, 32))))
+        pdeg = int(rng.integers(1, 1 << int(rng.integers(1, 24))))
+        alpha = float(rng.choice([0.0, 1.0, float(np.float32(rng.random()))]))
+        tp = (1.0 - alpha) / deg
+        inv_deg = np.float32(tp)
+        s = np.float32(inv_deg + np.float32(np.float32(alpha) / np.float32(pdeg)))
+        rows.append((inv_deg, s, _ru32(tp), 0, 0))
+    sopr = np.array(rows, dtype=np.float32)
+    # Node2vec constants from (p, q), plus raw extremes
+    rows = []
+    for _ in range(3000):
+        p, q = (np.float32(2.0 ** rng.uniform(-20, 20)) for _ in range(2))
+        ip, iq = np.float32(1) / p, np.float32(1) / q
+        mx = max(ip, max(iq, np.float32(1)))
+        mn = min(ip, min(iq, np.float32(1)))
+        rows.append((mx, mn, ip, iq, 0))
+    for _ in range(1000):
+        mx = np.float32(2.0 ** rng.uniform(-140, 100))
+        rows.append((mx, np.float32(mx * rng.random()), np.float32(mx * rng.uniform(0, 2)),
+                     np.float32(mx * rng.random()), 0))
+    n2v = np.array(rows, dtype=np.float32)
+    for flag, thr in ((1, sopr), (0, n2v)):
+        n = len(thr)
+        fast = np.zeros(4 * n, dtype=np.uint32)
+        slow = np.zeros(4 * n, dtype=np.uint32)
+        assert L.check_bounds(flag, thr.ctypes.data_as(ctypes.c_void_p), n, fast.ctypes.data_as(ctypes.c_void_p),
+                              slow.ctypes.data_as(ctypes.c_void_p)) == 0
+        assert np.array_equal(fast, slow), np.nonzero(fast != slow)[0][:10]
