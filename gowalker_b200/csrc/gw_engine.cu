@@ -203,6 +203,10 @@ void gw_handle::release()
     cudaFree(d_hashes);
     cudaFree(d_ctr);
     cudaFree(d_err);
+    cudaFree(d_index);
+    d_index = nullptr;
+    index_cap = 0;
+    index_nlvl = 0;
     if (h_ctr) cudaFreeHost(h_ctr);
     ooc_release();
     if (ev_start) cudaEventDestroy(ev_start);
@@ -423,6 +427,41 @@ extern "C" int gw_num_walkers(gw_handle *h, uint64_t *n)
 
 // ------------------------------------------------------------------ ABI: run
 
+// Sample levels of the resident CSR (CsrIndex): level L holds csr[j * 32^L]
+// for every j, ceil(nedges / 32^L) words, about 3% of the CSR in all.  Built
+// once per graph, after validation.
+int gw_handle::build_index(cudaStream_t s)
+{
+    index_nlvl = 0;
+    uint64_t n[kIdxLevels], total = 0;
+    uint32_t nl = 0;
+    for (uint64_t m = nedges; nl < (uint32_t)kIdxLevels && m > 64; ++nl) {
+        m = (m + 31) / 32;
+        n[nl] = m;
+        total += m;
+    }
+    if (nl == 0) return GW_OK;
+    if (total > index_cap) {
+        cudaFree(d_index);
+        d_index = nullptr;
+        index_cap = 0;
+        int st;
+        if ((st = cuda(cudaMalloc(&d_index, total * sizeof(uint32_t)), "CSR sample levels"))) return st;
+        index_cap = total;
+    }
+    uint32_t *dst = d_index;
+    const uint32_t *src = dev_csr;
+    for (uint32_t L = 0; L < nl; ++L) {
+        int st;
+        if ((st = cuda(launch_sample_level(src, n[L], dst, num_sms, s), "CSR sample level"))) return st;
+        index_lvl[L] = dst;
+        src = dst;
+        dst += n[L];
+    }
+    index_nlvl = nl;
+    return GW_OK;
+}
+
 int gw_handle::run_incore(gw_stats *stats)
 {
     int st;
@@ -454,6 +493,7 @@ int gw_handle::run_incore(gw_stats *stats)
         if (ends[0] != 0 || ends[1] != nedges)
             return fail(GW_ERR_GRAPH, "graph offsets must run from 0 to nedges (%llu..%llu)",
                         (unsigned long long)ends[0], (unsigned long long)ends[1]);
+        if ((st = build_index(s))) return st;
         validated = true;
     }
     IncoreArgs a{};
@@ -466,7 +506,9 @@ int gw_handle::run_incore(gw_stats *stats)
     a.init.key0 = (uint32_t)cfg.seed;
     a.init.key1 = (uint32_t)(cfg.seed >> 32);
     a.beg = dev_beg;
-    a.csr = dev_csr;
+    a.ix.csr = dev_csr;
+    a.ix.nlvl = index_nlvl;
+    for (uint32_t L = 0; L < index_nlvl; ++L) a.ix.lvl[L] = index_lvl[L];
     a.nverts = nverts;
     a.nwalkers = (uint32_t)nwalkers;
     a.wid_stride = 1;

@@ -40,6 +40,11 @@ struct gw_handle {
     bool resident = false;
     bool device_graph = false;
     bool validated = false;
+    // sample levels of the resident CSR, rebuilt whenever it is validated
+    uint32_t *d_index = nullptr;
+    uint64_t index_cap = 0;
+    const uint32_t *index_lvl[gw::kIdxLevels] = {};
+    uint32_t index_nlvl = 0;
 
     // walker population
     uint64_t nwalkers = 0;
@@ -80,6 +85,7 @@ struct gw_handle {
     bool host_graph_complete() const;
     int upload_whole_graph(cudaStream_t s, uint64_t *h2d);
     int ensure_outputs();
+    int build_index(cudaStream_t s);
     int run_incore(gw_stats *stats);
     int run_ooc(uint32_t policy, gw_stats *stats);
     void ooc_release();

@@ -66,7 +66,7 @@ struct IncoreArgs {
     StepConsts c;
     WalkerInit init;
     const uint64_t *beg;       // nverts+1 global offsets
-    const uint32_t *csr;       // nedges neighbour ids
+    CsrIndex ix;               // nedges neighbour ids and their sample levels
     uint32_t nverts;
     uint32_t nwalkers;         // walkers of this launch: ids wid_base + i * wid_stride, i < nwalkers
     uint32_t wid_base;
@@ -113,6 +113,8 @@ inline bool needs_coop(uint32_t algo, const StepConsts &c)
 {
     return algo != 0u || c.n2v_maxv > 8.0f * c.n2v_minv;
 }
+// One sample level: dst[j] = src[32 * j] for j < n.
+cudaError_t launch_sample_level(const uint32_t *src, uint64_t n, uint32_t *dst, int num_sms, cudaStream_t s);
 cudaError_t launch_validate_csr(const uint64_t *beg, const uint32_t *csr, uint32_t nverts, uint64_t nedges,
                                 uint32_t *err, int num_sms, cudaStream_t s);
 

@@ -116,7 +116,7 @@ extern "C" int gw_walk_noalloc(const gw_config *cfg, const uint64_t *d_beg, cons
     a.init.key0 = (uint32_t)cfg->seed;
     a.init.key1 = (uint32_t)(cfg->seed >> 32);
     a.beg = d_beg;
-    a.csr = d_csr;
+    a.ix = CsrIndex{d_csr, {}, 0};  // no sample levels: this entry point allocates nothing
     a.nverts = nverts;
     a.nwalkers = (uint32_t)nwalkers;
     a.wid_stride = 1;

@@ -428,10 +428,11 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
             const uint64_t hd = shfl64(head, L), ph = shfl64(phead, L);
             const uint32_t *cc = shfl_ptr(ccsr, L), *pc = shfl_ptr(pcsr, L);
             uint32_t xs;
+            const CsrIndex cix{cc, {}, 0}, pix{pc, {}, 0};
             const uint32_t astar = warp_first_accept<SOPR>(
                 a.c, shfl_thr<SOPR>(t, L), __shfl_sync(0xFFFFFFFFu, wid, L), __shfl_sync(0xFFFFFFFFu, hop, L), p0,
-                kMaxAttempts, cc + hd, __shfl_sync(0xFFFFFFFFu, deg, L), __shfl_sync(0xFFFFFFFFu, prev, L),
-                __shfl_sync(0xFFFFFFFFu, cur, L), pc + ph, __shfl_sync(0xFFFFFFFFu, pdeg, L), s_iv[warp], &xs);
+                kMaxAttempts, cix, hd, __shfl_sync(0xFFFFFFFFu, deg, L), __shfl_sync(0xFFFFFFFFu, prev, L),
+                __shfl_sync(0xFFFFFFFFu, cur, L), pix, ph, __shfl_sync(0xFFFFFFFFu, pdeg, L), s_iv[warp], &xs);
             if (lane == (uint32_t)L) {
                 n_trials += astar - p0;
                 if (astar >= kMaxAttempts) {
@@ -449,7 +450,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
         const float rv = rand_val(r.y, thr_max<SOPR>(a.c, t));
         const uint32_t x = __ldg(ccsr + head + pos);
         n_trials++;
-        if (accept_candidate<SOPR>(a.c, t, rv, x, prev, cur, pcsr + phead, pdeg)) {
+        if (accept_candidate<SOPR>(a.c, t, rv, x, prev, cur, CsrIndex{pcsr, {}, 0}, phead, pdeg)) {
             hop++;
             h = hash_step(h, x);
             if (PATHS) a.paths[(uint64_t)wid * a.stride + hop] = x;

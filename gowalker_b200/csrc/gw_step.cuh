@@ -107,31 +107,71 @@ __device__ __forceinline__ bool terminates(const StepConsts &c, uint32_t z)
     return c.term_prob > 0.0f && __uint2float_rn(z >> 8) * 0x1p-24f < c.term_prob;
 }
 
-// Membership of x in the sorted run base[0, n): plain binary search.
-__device__ __forceinline__ bool search_sorted(const uint32_t *__restrict__ base, uint32_t n, uint32_t x)
+// Neighbour array of the graph (or of one block) with its sample levels:
+// lvl[L-1][j] = csr[j * 32^L].  Inside one vertex's sorted neighbours the
+// entries of level L are every 32^L-th neighbour (by global position), so a
+// search walks down the levels, each a binary search over at most 65
+// contiguous entries (one or two lines, then L1 hits), and ends in fewer than
+// 32 neighbours: about one new line per level where a plain binary search
+// takes a miss per halving.  nlvl = 0 is a plain binary search.
+constexpr int kIdxLevels = 6;
+struct CsrIndex {
+    const uint32_t *csr;
+    const uint32_t *lvl[kIdxLevels];
+    uint32_t nlvl;
+};
+
+// First position p in [lo, hi) with csr[p] >= y, or hi (csr[lo, hi) sorted,
+// hi - lo < 2^32).  Ranges of at most 64 go straight to the last binary
+// search; longer ones start at the highest level with more than two entries
+// inside (level L qualifies when hi - lo > 2 * 32^L).
+__device__ __forceinline__ uint64_t csr_lower_bound(const CsrIndex &ix, uint64_t lo, uint64_t hi, uint32_t y)
 {
-    int32_t lo = 0, hi = (int32_t)n - 1;
-    while (lo <= hi) {
-        const int32_t mid = lo + ((hi - lo) >> 1);
-        const uint32_t v = __ldg(base + mid);
-        if (v == x) return true;
-        if (v < x) lo = mid + 1;
-        else hi = mid - 1;
+    if (hi - lo > 64 && ix.nlvl != 0) {
+        int L = min((int)ix.nlvl, (62 - __clzll((long long)(hi - lo))) / 5);  // (floor(log2 n) - 1) / 5
+        for (; L >= 1; --L) {
+            const uint32_t sh = 5u * (uint32_t)L;
+            if (hi - lo <= (2ull << sh)) continue;
+            const uint32_t *__restrict__ g = ix.lvl[L - 1];
+            const uint64_t j0 = (lo + (1ull << sh) - 1) >> sh, j1 = (hi - 1) >> sh;
+            uint32_t a = 0, b = (uint32_t)(j1 - j0) + 1;  // first j in [j0, j1] with csr[j << sh] >= y
+            while (a < b) {
+                const uint32_t m = (a + b) >> 1;
+                if (__ldg(g + j0 + m) < y) a = m + 1;
+                else b = m;
+            }
+            if (a > 0) lo = ((j0 + a - 1) << sh) + 1;
+            if (j0 + a <= j1) hi = (j0 + a) << sh;
+        }
     }
-    return false;
+    const uint32_t *__restrict__ p = ix.csr + lo;
+    uint32_t a = 0, b = (uint32_t)(hi - lo);
+    while (a < b) {
+        const uint32_t m = (a + b) >> 1;
+        if (__ldg(p + m) < y) a = m + 1;
+        else b = m;
+    }
+    return lo + a;
+}
+
+// Membership of x in the sorted csr[lo, lo + n).
+__device__ __forceinline__ bool csr_contains(const CsrIndex &ix, uint64_t lo, uint32_t n, uint32_t x)
+{
+    const uint64_t p = csr_lower_bound(ix, lo, lo + n, x);
+    return p < lo + n && __ldg(ix.csr + p) == x;
 }
 
 // Acceptance of candidate x drawn with rand value rv (engine/engine.hpp:209-258,
-// 334-375).
+// 334-375); N(prev) is pix.csr[phead, phead + pdeg).
 template <bool SOPR>
 __device__ __forceinline__ bool accept_candidate(const StepConsts &c, const StepThr &t, float rv, uint32_t x,
-                                                 uint32_t prev, uint32_t cur, const uint32_t *__restrict__ prev_adj,
+                                                 uint32_t prev, uint32_t cur, const CsrIndex &pix, uint64_t phead,
                                                  uint32_t pdeg)
 {
     if (rv <= thr_min<SOPR>(c, t)) return true;
     if (x == prev) return rv < thr_prev<SOPR>(c, t);
     // x is drawn from N(cur); when prev == cur the search must succeed.
-    const bool found = (prev == cur) ? true : search_sorted(prev_adj, pdeg, x);
+    const bool found = (prev == cur) ? true : csr_contains(pix, phead, pdeg, x);
     return found ? (rv < thr_found<SOPR>(c, t)) : (rv < thr_notfound<SOPR>(c, t));
 }
 
@@ -162,18 +202,6 @@ __device__ __forceinline__ StepThr shfl_thr(const StepThr &t, int src)
         o.t_prev = __shfl_sync(0xFFFFFFFFu, t.t_prev, src);
     }
     return o;
-}
-
-// First index in the sorted run a[0, n) whose value is >= y.
-__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *__restrict__ a, uint32_t n, uint32_t y)
-{
-    uint32_t lo = 0, hi = n;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(a + mid) < y) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
 }
 
 // Per-warp shared scratch of a cooperative step, in 32-bit words: run starts
@@ -229,7 +257,7 @@ __device__ __forceinline__ uint32_t rand_bounds(const StepConsts &c, const StepT
 }
 
 // Hard steps whose prev has fewer than 32 neighbours are decided without
-// touching the candidate: a trial's verdict depends on x = cand[pos] only
+// touching the candidate: a trial's verdict depends on x = N(cur)[pos] only
 // through "x == prev" and "x in N(prev)", i.e. through whether pos falls in
 // the run of prev, or of some y in N(prev), inside the sorted N(cur).  Those
 // runs are located once per step (one lower-bound search per lane).
@@ -245,8 +273,8 @@ __device__ __forceinline__ uint32_t rand_bounds(const StepConsts &c, const StepT
 template <bool SOPR>
 __device__ __forceinline__ uint32_t warp_first_accept_runs(const StepConsts &c, const StepThr &t, uint32_t wid,
                                                            uint32_t hop, uint32_t p0, uint32_t limit,
-                                                           const uint32_t *__restrict__ cand, uint32_t deg,
-                                                           uint32_t prev, const uint32_t *__restrict__ prev_adj,
+                                                           const CsrIndex &cix, uint64_t head, uint32_t deg,
+                                                           uint32_t prev, const CsrIndex &pix, uint64_t phead,
                                                            uint32_t pdeg, uint32_t *iv, uint32_t *x_out)
 {
     const uint32_t lane = threadIdx.x & 31u;
@@ -256,10 +284,10 @@ __device__ __forceinline__ uint32_t warp_first_accept_runs(const StepConsts &c, 
     // lane k < pdeg: run of N(prev)[k]; lane pdeg: run of prev
     uint32_t lo = 0, hi = 0;
     if (lane <= pdeg) {
-        const uint32_t y = (lane < pdeg) ? __ldg(prev_adj + lane) : prev;
-        lo = lower_bound_u32(cand, deg, y);
+        const uint32_t y = (lane < pdeg) ? __ldg(pix.csr + phead + lane) : prev;
+        lo = (uint32_t)(csr_lower_bound(cix, head, head + deg, y) - head);
         hi = lo;
-        while (hi < deg && __ldg(cand + hi) == y) hi++;
+        while (hi < deg && __ldg(cix.csr + head + hi) == y) hi++;
     }
     if (lane < pdeg) {
         iv[lane] = lo;
@@ -334,7 +362,7 @@ __device__ __forceinline__ uint32_t warp_first_accept_runs(const StepConsts &c, 
             const bool first_half = m0 != 0;
             const int f = __ffs(first_half ? m0 : m1) - 1;
             const uint32_t xf = __shfl_sync(0xFFFFFFFFu, first_half ? x0 : x1, f);
-            *x_out = __ldg(cand + fastmod(xf, M, deg));
+            *x_out = __ldg(cix.csr + head + fastmod(xf, M, deg));
             __syncwarp();
             return base + (first_half ? 0u : 32u) + (uint32_t)f;
         }
@@ -352,13 +380,13 @@ __device__ __forceinline__ uint32_t warp_first_accept_runs(const StepConsts &c, 
 template <bool SOPR>
 __device__ __forceinline__ uint32_t warp_first_accept(const StepConsts &c, const StepThr &t, uint32_t wid,
                                                       uint32_t hop, uint32_t p0, uint32_t limit,
-                                                      const uint32_t *__restrict__ cand, uint32_t deg,
-                                                      uint32_t prev, uint32_t cur,
-                                                      const uint32_t *__restrict__ prev_adj, uint32_t pdeg,
-                                                      uint32_t *iv, uint32_t *x_out)
+                                                      const CsrIndex &cix, uint64_t head, uint32_t deg,
+                                                      uint32_t prev, uint32_t cur, const CsrIndex &pix,
+                                                      uint64_t phead, uint32_t pdeg, uint32_t *iv, uint32_t *x_out)
 {
     if (pdeg < 32 && prev != cur)
-        return warp_first_accept_runs<SOPR>(c, t, wid, hop, p0, limit, cand, deg, prev, prev_adj, pdeg, iv, x_out);
+        return warp_first_accept_runs<SOPR>(c, t, wid, hop, p0, limit, cix, head, deg, prev, pix, phead, pdeg, iv,
+                                            x_out);
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t M = fastmod_magic(deg);
     const float maxv = thr_max<SOPR>(c, t);
@@ -370,8 +398,10 @@ __device__ __forceinline__ uint32_t warp_first_accept(const StepConsts &c, const
             const U4 r = draw(c, wid, hop, att);
             const uint32_t pos = fastmod(r.x, M, deg);
             const float rv = rand_val(r.y, maxv);
-            x = __ldg(cand + pos);
-            acc = accept_candidate<SOPR>(c, t, rv, x, prev, cur, prev_adj, pdeg);
+            x = __ldg(cix.csr + head + pos);
+            // N(prev) serves every attempt of the step and stays in L1: a
+            // plain binary search beats the sample levels here.
+            acc = accept_candidate<SOPR>(c, t, rv, x, prev, cur, CsrIndex{pix.csr, {}, 0}, phead, pdeg);
         }
         const unsigned m = __ballot_sync(0xFFFFFFFFu, acc);
         if (m) {

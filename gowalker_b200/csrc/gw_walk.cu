@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const __grid
     if (lane < kWsCount) s_ws[warp][lane] = 0;
     __syncwarp();
     const uint64_t *__restrict__ beg = a.beg;
-    const uint32_t *__restrict__ csr = a.csr;
+    const uint32_t *__restrict__ csr = a.ix.csr;
     const uint32_t maxhops = a.c.maxhops;
 
     uint32_t q_next = 0, q_end = 0;  // warp-uniform claimed range
@@ -158,8 +158,8 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const __grid
                                      __uint_as_float(pk[kPkThr2][L])};
                     uint32_t xs;
                     const uint32_t astar = warp_first_accept<SOPR>(a.c, tl, pk[kPkWid][L], pk[kPkHop][L], p0,
-                                                                   kMaxAttempts, csr + hd, pk[kPkDeg][L], Lprev, Lcur,
-                                                                   csr + ph, Lpdeg, s_iv[warp], &xs);
+                                                                   kMaxAttempts, a.ix, hd, pk[kPkDeg][L], Lprev, Lcur,
+                                                                   a.ix, ph, Lpdeg, s_iv[warp], &xs);
                     if (lane == 0) {
                         pk[kPkAstar][L] = astar;
                         const bool by_pos = Lpdeg < 32 && Lprev != Lcur;
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const __grid
         const float rv = rand_val(r.y, thr_max<SOPR>(a.c, t));
         const uint32_t x = __ldg(csr + head + pos);
         n_trials++;
-        if (accept_candidate<SOPR>(a.c, t, rv, x, prev, cur, csr + phead, pdeg)) {
+        if (accept_candidate<SOPR>(a.c, t, rv, x, prev, cur, a.ix, phead, pdeg)) {
             hop++;
             h = hash_step(h, x);
             if (PATHS) a.paths[(uint64_t)wid * a.stride + hop] = x;
@@ -280,6 +280,18 @@ __global__ void k_validate_csr(const uint64_t *__restrict__ beg, const uint32_t 
     }
     for (uint64_t i = t0; i < nedges; i += stride) bad |= csr[i] >= nverts;
     if (__any_sync(0xFFFFFFFFu, bad) && (threadIdx.x & 31u) == 0) atomicOr(err, kErrVertexRange);
+}
+
+__global__ void k_sample_level(const uint32_t *__restrict__ src, uint64_t n, uint32_t *__restrict__ dst)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) dst[j] = src[32 * j];
+}
+
+cudaError_t launch_sample_level(const uint32_t *src, uint64_t n, uint32_t *dst, int num_sms, cudaStream_t s)
+{
+    k_sample_level<<<num_sms * 8, 256, 0, s>>>(src, n, dst);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_validate_csr(const uint64_t *beg, const uint32_t *csr, uint32_t nverts, uint64_t nedges,
