@@ -50,7 +50,8 @@ class GwConfig(ctypes.Structure):
         ("seed", ctypes.c_uint64),
         ("record_paths", ctypes.c_uint32),
         ("device", ctypes.c_int32),
-        ("reserved", ctypes.c_uint32 * 8),
+        ("strict_blocks", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 7),
     ]
 
 

@@ -41,7 +41,7 @@ enum WarpStat : int {
 enum ErrBit : uint32_t {
     kErrVertexRange = 1u,   // a neighbour id >= nverts
     kErrSource = 2u,        // a walker source >= nverts
-    kErrBlock = 4u,         // a vertex outside every block
+    kErrBlock = 4u,         // a vertex outside every block, or a block scheduled absent
     kErrTrials = 8u,        // a step exceeded kMaxAttempts rejection trials
 };
 

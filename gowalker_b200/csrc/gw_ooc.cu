@@ -44,7 +44,8 @@ struct OocState {
 
     WalkerRec *w_a = nullptr, *w_b = nullptr;
     uint64_t w_cap = 0;
-    uint32_t *d_counts = nullptr, *d_offsets = nullptr, *d_cursor = nullptr;
+    // 2 * nb^2 buckets (unflagged, then kNeedPrev); d_pairs: nb^2 per-pair totals
+    uint32_t *d_counts = nullptr, *d_offsets = nullptr, *d_cursor = nullptr, *d_pairs = nullptr;
     uint32_t *d_run_pre = nullptr, *d_run_off = nullptr, *d_nrun = nullptr;
     Decision *d_dec = nullptr, *h_dec = nullptr;
 
@@ -110,6 +111,7 @@ void gw_handle::ooc_release()
     cudaFree(o.w_a);
     cudaFree(o.w_b);
     cudaFree(o.d_counts);
+    cudaFree(o.d_pairs);
     cudaFree(o.d_offsets);
     cudaFree(o.d_cursor);
     cudaFree(o.d_run_pre);
@@ -212,7 +214,8 @@ static int ooc_setup(gw_handle *h)
     if ((st = h->cuda(cudaMalloc(&o.d_estart, (nb + 1) * sizeof(uint64_t)), "estart"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_cached, nb * sizeof(uint32_t)), "cached list"))) return st;
     if ((st = h->cuda(cudaMallocHost(&o.h_cached, nb * sizeof(uint32_t)), "cached list"))) return st;
-    const uint64_t nbk = (uint64_t)nb * nb;
+    const uint64_t nbk = 2ull * nb * nb;
+    if ((st = h->cuda(cudaMalloc(&o.d_pairs, nbk / 2 * sizeof(uint32_t)), "pair counts"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_counts, nbk * sizeof(uint32_t)), "bucket counts"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_offsets, (nbk + 1) * sizeof(uint32_t)), "bucket offsets"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_cursor, nbk * sizeof(uint32_t)), "bucket cursors"))) return st;
@@ -307,7 +310,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     if ((st = ooc_walkers(this))) return st;
     OocState &o = *ooc;
     const uint32_t nb = o.nb;
-    const uint64_t nbk = (uint64_t)nb * nb;
+    const uint64_t nbk = 2ull * nb * nb;  // buckets: unflagged pairs, then kNeedPrev pairs
     cudaStream_t s = s_compute;
     const bool sopr = cfg.algorithm != GW_NODE2VEC;
     const bool paths = cfg.record_paths == GW_PATHS_FULL;
@@ -359,7 +362,8 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if ((e = cuda(launch_scan(o.d_counts, (uint32_t)nbk, o.d_offsets, s), "scan"))) return e;
         if ((e = cuda(cudaMemsetAsync(o.d_cursor, 0, nbk * sizeof(uint32_t), s), "memset"))) return e;
         if ((e = cuda(launch_scatter(o.w_a, n, nb, o.d_offsets, o.d_cursor, o.w_b, num_sms, s), "scatter"))) return e;
-        launches += 3;
+        if ((e = cuda(launch_combine(o.d_counts, nb, o.d_pairs, num_sms, s), "pair counts"))) return e;
+        launches += 4;
         std::swap(o.w_a, o.w_b);  // w_a: bucket-sorted live walkers
         return GW_OK;
     };
@@ -383,6 +387,11 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     a.ctr = d_ctr;
     a.err = d_err;
     const bool coop = needs_coop(cfg.algorithm, a.c);
+    // Lazy mode: a walker steps with only its current block resident until a
+    // trial needs N(prev).  Node2vec thresholds do not depend on deg(prev);
+    // SOPR/SOSR's do, and hard steps serve N(prev) to the whole warp, so
+    // those run with both blocks as the reference does.
+    a.lazy = (!sopr && !coop && !cfg.strict_blocks) ? 1u : 0u;
     int grid = (int)cfg.blockpergrid;
     if (grid <= 0) grid = ooc_grid(sopr, paths, coop, num_sms);
 
@@ -391,7 +400,8 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     cudaEventCreate(&k1);
     auto step = [&]() -> int {
         int e;
-        if ((e = cuda(launch_runnable(o.d_counts, o.d_offsets, o.d_blk_beg, nb, o.d_run_pre, o.d_run_off, o.d_nrun, s),
+        if ((e = cuda(launch_runnable(o.d_counts, o.d_offsets, o.d_blk_beg, nb, a.lazy, o.d_run_pre, o.d_run_off,
+                                      o.d_nrun, s),
                       "runnable")))
             return e;
         if ((e = cuda(cudaMemsetAsync(d_ctr + kCtrCursor, 0, sizeof(unsigned long long), s), "memset"))) return e;
@@ -444,7 +454,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         const bool tracing = learned && !o.trained && trace_t < kTraceIters + kHorizon;
         if (learned_active || tracing) {
             FeatureArgs f{};
-            f.counts = o.d_counts;
+            f.counts = o.d_pairs;
             f.blk_beg = o.d_blk_beg;
             f.emass = o.d_emass;
             f.vfrac = o.d_vfrac;
@@ -477,7 +487,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             }
         }
         // ---- plain block choice on the device (decision, fallback and rescue), read back
-        if ((st = cuda(launch_schedule(o.d_counts, o.d_offsets, nb, o.d_cached, ncached, o.nslots, cfg.zero_threshold,
+        if ((st = cuda(launch_schedule(o.d_pairs, o.d_offsets + nbk, nb, o.d_cached, ncached, o.nslots, cfg.zero_threshold,
                                        nullptr, 0.f, o.d_dec, s),
                        "schedule")))
             break;
@@ -513,6 +523,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 plain_bytes += db;
             }
         }
+        // progress guard: a learned choice that moved no walker hands the
+        // next decision to the plain rule and its rescue, which always make
+        // some bucket runnable
+        const bool learned_stalled = last_phase == 1 && steps_now == phase_steps_mark;
         phase_steps_mark = steps_now;
         phase_bytes_mark = h2d;
         last_phase = -1;
@@ -535,7 +549,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if (nlive == 0) break;
 
         std::vector<std::pair<int, int>> todo;  // (block, cached position or -1)
-        if (learned_active && !reverted && o.h_choose[0] > 0) {
+        if (learned_active && !reverted && !learned_stalled && o.h_choose[0] > 0) {
             for (int k = 0; k < o.h_choose[0]; ++k) todo.emplace_back(o.h_choose[1 + 2 * k], o.h_choose[2 + 2 * k]);
             learned_iters++;
             last_phase = 1;
@@ -694,6 +708,6 @@ extern "C" int gw_bucket_counts(gw_handle *h, uint32_t *out)
     if (!h || !out) return GW_ERR_ARG;
     if (!h->ooc || !h->ooc->ready) return h->fail(GW_ERR_STATE, "no bucket counts: the out-of-core path has not run");
     cudaSetDevice(h->cfg.device);
-    const uint64_t nbk = (uint64_t)h->ooc->nb * h->ooc->nb;
-    return h->cuda(cudaMemcpy(out, h->ooc->d_counts, nbk * sizeof(uint32_t), cudaMemcpyDeviceToHost), "bucket counts");
+    const uint64_t npairs = (uint64_t)h->ooc->nb * h->ooc->nb;
+    return h->cuda(cudaMemcpy(out, h->ooc->d_pairs, npairs * sizeof(uint32_t), cudaMemcpyDeviceToHost), "bucket counts");
 }

@@ -61,7 +61,8 @@ __global__ void k_init_walkers(WalkerInit in, const uint32_t *__restrict__ vstar
 
 __device__ __forceinline__ uint32_t bucket_of(const WalkerRec &r, uint32_t nb)
 {
-    return r.prev_blk == kFinished ? kNoBucket : r.prev_blk * nb + r.cur_blk;
+    if (r.prev_blk == kFinished) return kNoBucket;
+    return ((r.cur_blk & kNeedPrev) ? nb * nb : 0u) + r.prev_blk * nb + (r.cur_blk & ~kNeedPrev);
 }
 
 __global__ void k_count(const WalkerRec *__restrict__ w, uint64_t n, uint32_t nb, uint32_t *__restrict__ counts)
@@ -153,19 +154,26 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const uint32_t *__restric
 __global__ void __launch_bounds__(kScanThreads) k_runnable(const uint32_t *__restrict__ counts,
                                                            const uint32_t *__restrict__ offsets,
                                                            const uint64_t *const *__restrict__ blk_beg, uint32_t nb,
-                                                           uint32_t *__restrict__ run_pre,
+                                                           uint32_t lazy, uint32_t *__restrict__ run_pre,
                                                            uint32_t *__restrict__ run_off, uint32_t *__restrict__ nrun)
 {
     __shared__ uint8_t s_res[kMaxBlocks];
     for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) s_res[i] = blk_beg[i] != nullptr;
     __syncthreads();
-    const uint32_t n = nb * nb;
+    const uint32_t nn = nb * nb, n = 2 * nn;
+    // unflagged walkers need their current block (and, unless lazy, the
+    // previous one); flagged walkers need both
+    auto runnable = [&](uint32_t b) {
+        const uint32_t pc = b < nn ? b : b - nn;
+        const bool cur_ok = s_res[pc % nb] != 0, prev_ok = s_res[pc / nb] != 0;
+        return cur_ok && (prev_ok || (lazy && b < nn));
+    };
     const uint32_t per = (n + kScanThreads - 1) / kScanThreads;
     const uint32_t lo = min(threadIdx.x * per, n), hi = min(lo + per, n);
     uint32_t cnt = 0, sum = 0;
     for (uint32_t b = lo; b < hi; ++b) {
         const uint32_t c = counts[b];
-        if (c && s_res[b / nb] && s_res[b % nb]) {
+        if (c && runnable(b)) {
             cnt++;
             sum += c;
         }
@@ -175,7 +183,7 @@ __global__ void __launch_bounds__(kScanThreads) k_runnable(const uint32_t *__res
     uint32_t run = cta_exclusive_scan(sum, &tot_sum);
     for (uint32_t b = lo; b < hi; ++b) {
         const uint32_t c = counts[b];
-        if (c && s_res[b / nb] && s_res[b % nb]) {
+        if (c && runnable(b)) {
             run_off[k] = offsets[b];
             run_pre[k] = run;
             run += c;
@@ -203,7 +211,7 @@ __global__ void __launch_bounds__(kScanThreads) k_runnable(const uint32_t *__res
 // run ends.  `pred` (optional) replaces the scores by predicted demand scaled
 // by pred_weight: the learned policy.
 __global__ void __launch_bounds__(1024) k_schedule(const uint32_t *__restrict__ counts,
-                                                   const uint32_t *__restrict__ offsets, uint32_t nb,
+                                                   const uint32_t *__restrict__ live, uint32_t nb,
                                                    const uint32_t *__restrict__ cached, uint32_t ncached,
                                                    uint32_t nslots, uint32_t zero_threshold,
                                                    const float *__restrict__ pred, float pred_weight,
@@ -269,7 +277,7 @@ __global__ void __launch_bounds__(1024) k_schedule(const uint32_t *__restrict__ 
         const uint64_t best = s_best >> 11;
         const int32_t bi = (int32_t)(2047u - (uint32_t)(s_best & 2047u));
         d.score = best;
-        d.live = offsets[nbk];
+        d.live = *live;
         if (s_best != 0 && best > 0 && best > zero_threshold) {
             d.action = full ? 2 : 1;
             d.block = bi;
@@ -284,7 +292,7 @@ __global__ void __launch_bounds__(1024) k_schedule(const uint32_t *__restrict__ 
         if (s_bucket) {
             const uint32_t b = 0x1FFFFFu - (uint32_t)(s_bucket & 0x1FFFFFu);
             const uint32_t p = b / nb, c = b % nb;
-            d.rescue_block = (int32_t)(s_cached[p] ? c : p);
+            d.rescue_block = (int32_t)(s_cached[c] ? p : c);  // the current block first: lazy walkers need only it
             if (full) {
                 unsigned long long mn = ~0ull;
                 for (uint32_t j = 0; j < ncached; ++j) {
@@ -402,17 +410,25 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
                 hop = rec.hop;
                 hop0 = hop;
                 pb = rec.prev_blk;
-                cb = rec.cur_blk;
+                cb = rec.cur_blk & ~kNeedPrev;
                 h = ((uint64_t)rec.hash_hi << 32) | rec.hash_lo;
+                const uint64_t *pbeg = hop < maxhops ? a.blk_beg[pb] : nullptr;
                 if (hop >= maxhops) {
                     finish();
+                } else if (pbeg == nullptr && !a.lazy) {
+                    atomicOr(a.err, kErrBlock);  // scheduled without its previous block
+                    finish();
                 } else {
-                    const uint64_t *pbeg = a.blk_beg[pb];
-                    pcsr = a.blk_csr[pb];
-                    const uint32_t poff = prev - s_vs[pb];
-                    const uint64_t p0 = __ldg(pbeg + poff), p1 = __ldg(pbeg + poff + 1);
-                    phead = p0 - a.estart[pb];
-                    pdeg = (uint32_t)(p1 - p0);
+                    pcsr = nullptr;  // lazy mode, previous block absent: N(prev) unknown
+                    phead = 0;
+                    pdeg = 0;
+                    if (pbeg != nullptr) {
+                        pcsr = a.blk_csr[pb];
+                        const uint32_t poff = prev - s_vs[pb];
+                        const uint64_t p0 = __ldg(pbeg + poff), p1 = __ldg(pbeg + poff + 1);
+                        phead = p0 - a.estart[pb];
+                        pdeg = (uint32_t)(p1 - p0);
+                    }
                     enter();
                 }
             }
@@ -450,7 +466,28 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
         const float rv = rand_val(r.y, thr_max<SOPR>(a.c, t));
         const uint32_t x = __ldg(ccsr + head + pos);
         n_trials++;
-        if (accept_candidate<SOPR>(a.c, t, rv, x, prev, cur, CsrIndex{pcsr, {}, 0}, phead, pdeg)) {
+        const int verdict = pcsr != nullptr
+                                ? (accept_candidate<SOPR>(a.c, t, rv, x, prev, cur, CsrIndex{pcsr, {}, 0}, phead, pdeg) ? 1 : 0)
+                                : accept_without_prev<SOPR>(a.c, t, rv, x, prev, cur);
+        if (verdict < 0) {
+            // Needs N(prev), whose block is absent: park the walker flagged in
+            // bucket (prev block, cur block).  The step restarts at attempt 0
+            // once both blocks are resident (the draws are counter-based), so
+            // its attempts so far are not counted.
+            WalkerRec rec;
+            rec.wid = wid;
+            rec.prev = prev;
+            rec.cur = cur;
+            rec.hop = hop;
+            rec.prev_blk = pb;
+            rec.cur_blk = cb | kNeedPrev;
+            rec.hash_lo = (uint32_t)h;
+            rec.hash_hi = (uint32_t)(h >> 32);
+            a.walkers[idx] = rec;
+            n_trials -= attempt;
+            flush();
+            active = false;
+        } else if (verdict > 0) {
             hop++;
             h = hash_step(h, x);
             if (PATHS) a.paths[(uint64_t)wid * a.stride + hop] = x;
@@ -669,18 +706,30 @@ cudaError_t launch_scatter(const WalkerRec *in, uint64_t n, uint32_t nb, const u
 }
 
 cudaError_t launch_runnable(const uint32_t *counts, const uint32_t *offsets, const uint64_t *const *blk_beg,
-                            uint32_t nb, uint32_t *run_pre, uint32_t *run_off, uint32_t *nrun, cudaStream_t s)
+                            uint32_t nb, uint32_t lazy, uint32_t *run_pre, uint32_t *run_off, uint32_t *nrun,
+                            cudaStream_t s)
 {
-    k_runnable<<<1, kScanThreads, 0, s>>>(counts, offsets, blk_beg, nb, run_pre, run_off, nrun);
+    k_runnable<<<1, kScanThreads, 0, s>>>(counts, offsets, blk_beg, nb, lazy, run_pre, run_off, nrun);
     return cudaGetLastError();
 }
 
-cudaError_t launch_schedule(const uint32_t *counts, const uint32_t *offsets, uint32_t nb, const uint32_t *cached,
+__global__ void k_combine(const uint32_t *__restrict__ counts, uint32_t nn, uint32_t *__restrict__ combined)
+{
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x)
+        combined[k] = counts[k] + counts[nn + k];
+}
+
+cudaError_t launch_combine(const uint32_t *counts, uint32_t nb, uint32_t *combined, int num_sms, cudaStream_t s)
+{
+    k_combine<<<num_sms, 256, 0, s>>>(counts, nb * nb, combined);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_schedule(const uint32_t *counts, const uint32_t *live, uint32_t nb, const uint32_t *cached,
                             uint32_t ncached, uint32_t nslots, uint32_t zero_threshold, const float *pred,
                             float pred_weight, Decision *out, cudaStream_t s)
 {
-    k_schedule<<<1, 1024, 0, s>>>(counts, offsets, nb, cached, ncached, nslots, zero_threshold, pred, pred_weight,
-                                  out);
+    k_schedule<<<1, 1024, 0, s>>>(counts, live, nb, cached, ncached, nslots, zero_threshold, pred, pred_weight, out);
     return cudaGetLastError();
 }
 

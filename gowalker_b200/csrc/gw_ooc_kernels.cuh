@@ -19,6 +19,9 @@ static_assert(sizeof(WalkerRec) == 32, "walker record is 32 bytes");
 
 constexpr uint32_t kFinished = 0xFFFFFFFFu;  // prev_blk of a finished walker
 constexpr uint32_t kMaxBlocks = 1024;        // block table kept in shared memory
+// cur_blk flag of a walker whose step needs N(prev) while prev's block is
+// absent (lazy mode); such walkers sit in the second half of the buckets.
+constexpr uint32_t kNeedPrev = 0x80000000u;
 
 struct OocStepArgs {
     StepConsts c;
@@ -27,6 +30,7 @@ struct OocStepArgs {
     const uint32_t *vstart;          // [nb+1]
     const uint64_t *estart;          // [nb+1]
     uint32_t nb, nverts;
+    uint32_t lazy;                   // 1: a walker runs with only its current block resident
     WalkerRec *walkers;              // bucket-sorted, updated in place
     const uint32_t *run_pre;         // [nrun+1] prefix of runnable bucket sizes
     const uint32_t *run_off;         // [nrun] first walker of each runnable bucket
@@ -57,9 +61,15 @@ cudaError_t launch_count(const WalkerRec *w, uint64_t n, uint32_t nb, uint32_t *
 cudaError_t launch_scan(const uint32_t *counts, uint32_t n, uint32_t *offsets, cudaStream_t s);
 cudaError_t launch_scatter(const WalkerRec *in, uint64_t n, uint32_t nb, const uint32_t *offsets,
                            uint32_t *cursor, WalkerRec *out, int num_sms, cudaStream_t s);
+// Buckets are 2 * nb^2: (prev_blk, cur_blk), then the same pairs for walkers
+// flagged kNeedPrev.
 cudaError_t launch_runnable(const uint32_t *counts, const uint32_t *offsets, const uint64_t *const *blk_beg,
-                            uint32_t nb, uint32_t *run_pre, uint32_t *run_off, uint32_t *nrun, cudaStream_t s);
-cudaError_t launch_schedule(const uint32_t *counts, const uint32_t *offsets, uint32_t nb, const uint32_t *cached,
+                            uint32_t nb, uint32_t lazy, uint32_t *run_pre, uint32_t *run_off, uint32_t *nrun,
+                            cudaStream_t s);
+// combined[k] = counts[k] + counts[nb^2 + k]: walkers per (prev, cur) block pair.
+cudaError_t launch_combine(const uint32_t *counts, uint32_t nb, uint32_t *combined, int num_sms, cudaStream_t s);
+// `counts` are the nb^2 per-pair totals; `live` points at the live-walker count.
+cudaError_t launch_schedule(const uint32_t *counts, const uint32_t *live, uint32_t nb, const uint32_t *cached,
                             uint32_t ncached, uint32_t nslots, uint32_t zero_threshold, const float *pred,
                             float pred_weight, Decision *out, cudaStream_t s);
 // ---- learned policy: per-block features, training targets, decisions

@@ -175,6 +175,21 @@ __device__ __forceinline__ bool accept_candidate(const StepConsts &c, const Step
     return found ? (rv < thr_found<SOPR>(c, t)) : (rv < thr_notfound<SOPR>(c, t));
 }
 
+// The same verdict without N(prev), for a walker whose previous block is not
+// resident: 1 accept, 0 reject, -1 when it depends on x in N(prev) (the
+// found and not-found thresholds disagree at rv).
+template <bool SOPR>
+__device__ __forceinline__ int accept_without_prev(const StepConsts &c, const StepThr &t, float rv, uint32_t x,
+                                                   uint32_t prev, uint32_t cur)
+{
+    if (rv <= thr_min<SOPR>(c, t)) return 1;
+    if (x == prev) return rv < thr_prev<SOPR>(c, t) ? 1 : 0;
+    const bool af = rv < thr_found<SOPR>(c, t);
+    if (prev == cur) return af ? 1 : 0;
+    const bool an = rv < thr_notfound<SOPR>(c, t);
+    return af == an ? (af ? 1 : 0) : -1;
+}
+
 // A walker whose step has already rejected this many attempts is served by
 // the whole warp (warp_first_accept).
 constexpr uint32_t kHardAttempts = 4;

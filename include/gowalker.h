@@ -92,7 +92,10 @@ typedef struct gw_config {
     uint64_t seed;            /* Philox key of the walk stream */
     uint32_t record_paths;    /* GW_PATHS_* */
     int32_t device;           /* CUDA device ordinal */
-    uint32_t reserved[8];
+    uint32_t strict_blocks;   /* out-of-core: 1 = a walker runs only when both its blocks are
+                                 resident (the reference's rule); 0 = Node2vec walkers also run
+                                 with only the current block until a trial needs N(prev) */
+    uint32_t reserved[7];
 } gw_config;
 
 /* Per-run counters. */

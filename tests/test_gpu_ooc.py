@@ -120,3 +120,35 @@ def test_zero_copy_leaves_neighbouring_host_data_writable(gw, oracle):
                       paths=False)
     assert np.array_equal(out, ref["hashes"])
     eng.close()
+
+
+@pytest.mark.parametrize("sym", [False, True])
+def test_lazy_previous_block_same_walks_fewer_loads(gw, oracle, sym):
+    """Node2vec walkers may step with only their current block resident until
+    a trial needs N(prev): identical walks and trial counts, fewer loads than
+    requiring both blocks."""
+    beg, csr = graph(oracle, scale=13, ef=12, sym=sym, cap=7000, seed=3)
+    V = len(beg) - 1
+    res = {}
+    for strict in (1, 0):
+        from gowalker_b200.preprocess import split_equal_edge_mass
+        vb, eb = split_equal_edge_mass(beg, 16)
+        maxv = int(np.diff(vb.astype(np.int64)).max())
+        maxe = int(np.diff(eb.astype(np.int64)).max())
+        slot = ((maxv + 2) & ~1) * 8 + ((max(maxe, 1) + 3) & ~3) * 4
+        eng = gw.WalkEngine(algorithm=0, maxhops=30, p=0.5, q=2.0, seed=5, walkpersource=1, record_paths=1,
+                            cache_size=slot * 4, strict_blocks=strict)
+        eng.set_host_graph(beg, csr, vb, eb)
+        eng.init_walkers(0, 1, 5)
+        st = eng.run()
+        P, L = eng.paths()
+        res[strict] = (P, L, eng.hashes(), st)
+        assert int(eng.bucket_counts().sum()) == 0
+        eng.close()
+    ref = oracle.walk(beg, csr, oracle.make_cfg(algo=0, maxhops=30, p=0.5, q=2.0, seed=5), 0, V, paths=True)
+    for strict in (1, 0):
+        P, L, H, st = res[strict]
+        assert np.array_equal(P, ref["paths"]) and np.array_equal(L, ref["lens"])
+        assert np.array_equal(H, ref["hashes"])
+        assert st["steps"] == ref["stats"]["steps"] and st["trials"] == ref["stats"]["trials"]
+    assert res[0][3]["block_loads"] < res[1][3]["block_loads"]
