@@ -240,7 +240,7 @@ def run_ooc_bench(args, wl):
     policy = gw.GW_POLICY_LEARNED if args.policy == "learned" else gw.GW_POLICY_PLAIN
     eng = gw.WalkEngine(algorithm=wl["algo"], maxhops=wl["maxhops"], p=wl["p"], q=wl["q"], alpha=wl["alpha"],
                         term_prob=wl["term"], seed=42, walkpersource=wl["wps"], record_paths=1 if args.paths else 0,
-                        cache_size=wl["cache"], zero_copy=0)
+                        cache_size=wl["cache"], zero_copy=0, strict_blocks=1 if args.strict_blocks else 0)
     eng.set_host_graph(beg_t, csr_t[: len(csr)], vb, eb)
     stream = torch.cuda.ExternalStream(eng.stream_handle())
     for _ in range(args.warmup):
@@ -271,7 +271,10 @@ def run_ooc_bench(args, wl):
     line = {"metric": "walk steps/sec", "value": value, "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32 gathers, fp32/fp64 accept compares", "data": "synthetic",
-            "config": {"workload": wl["name"], "policy": args.policy, "vertices": len(beg) - 1, "edges": len(csr),
+            "config": {"workload": wl["name"], "policy": args.policy,
+                       "residency": "both blocks (reference rule)" if args.strict_blocks else
+                                    "current block until N(prev) is needed",
+                       "vertices": len(beg) - 1, "edges": len(csr),
                        "blocks": wl["nblocks"], "cache_bytes": wl["cache"], "walkers": eng.num_walkers(),
                        "graph_in": "pinned host memory", "paths_recorded": bool(args.paths)},
             "gpu_launches": tot["launches"],
@@ -471,6 +474,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--policy", default="plain", choices=["plain", "learned"], help="block policy (out-of-core)")
+    ap.add_argument("--strict-blocks", action="store_true",
+                    help="out-of-core: run a walker only when both its blocks are resident (the reference's rule)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.config])
     if args.scale:
