@@ -26,16 +26,14 @@ namespace gw {
 struct OocState {
     uint32_t nb = 0;
     uint32_t nslots = 0;
-    uint64_t slot_beg_words = 0, slot_csr_words = 0;
-    uint64_t *slot_beg = nullptr;  // nslots * slot_beg_words
-    uint32_t *slot_csr = nullptr;  // nslots * slot_csr_words
+    uint64_t slot_csr_words = 0;
+    uint64_t *d_beg = nullptr;     // offsets of every vertex (global, nverts+1): resident for the whole run
+    uint32_t *slot_csr = nullptr;  // nslots * slot_csr_words: neighbour lists cached by block
     std::vector<int> slot_block;   // block held by each slot, -1 = free
     std::vector<int> block_slot;   // slot of each block, -1 = absent
     std::vector<uint32_t> cached;  // the scheduler's cached list (GOwalker_scheduler_t::buckets)
 
-    const uint64_t **h_blk_beg = nullptr;  // pinned mirrors of the block tables
-    const uint32_t **h_blk_csr = nullptr;
-    const uint64_t **d_blk_beg = nullptr;
+    const uint32_t **h_blk_csr = nullptr;  // pinned mirror of the block table (null = absent)
     const uint32_t **d_blk_csr = nullptr;
     uint32_t *d_vstart = nullptr;
     uint64_t *d_estart = nullptr;
@@ -49,9 +47,8 @@ struct OocState {
     uint32_t *d_run_pre = nullptr, *d_run_off = nullptr, *d_nrun = nullptr;
     Decision *d_dec = nullptr, *h_dec = nullptr;
 
-    // zero-copy: device views of the host blocks, and the pinned copies made
-    // of pageable ones
-    std::vector<const uint64_t *> map_beg;
+    // zero-copy: device views of the host blocks' neighbour lists, and the
+    // pinned copies made of pageable ones
     std::vector<const uint32_t *> map_csr;
     std::vector<void *> staged;
     bool mapped = false;
@@ -80,15 +77,25 @@ constexpr float kSwapMargin = 0.25f;
 constexpr uint32_t kTrainEpochs = 400;
 constexpr float kTrainLr = 3e-3f;
 
-__global__ void k_validate_block(const uint64_t *beg, const uint32_t *csr, uint32_t nv, uint64_t e0, uint64_t e1,
-                                 uint32_t nverts, uint32_t *err)
+// Offsets of every vertex: non-decreasing, and each block starts at its
+// first edge (so every vertex's edges lie inside its block's edges).
+__global__ void k_validate_offsets(const uint64_t *beg, uint32_t nverts, const uint32_t *vstart, const uint64_t *estart,
+                                   uint32_t nb, uint32_t *err)
 {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool bad = false;
-    if (t0 == 0) bad |= (beg[0] != e0) | (beg[nv] != e1);
-    for (uint64_t v = t0; v < nv; v += stride) bad |= beg[v] > beg[v + 1];
-    for (uint64_t i = t0; i < e1 - e0; i += stride) bad |= csr[i] >= nverts;
+    for (uint64_t v = t0; v < nverts; v += stride) bad |= beg[v] > beg[v + 1];
+    for (uint64_t b = t0; b <= nb; b += stride) bad |= beg[vstart[b]] != estart[b];
+    if (__any_sync(0xFFFFFFFFu, bad) && (threadIdx.x & 31u) == 0) atomicOr(err, kErrVertexRange);
+}
+
+// Neighbour ids of a block just copied into a slot.
+__global__ void k_validate_block(const uint32_t *csr, uint64_t ne, uint32_t nverts, uint32_t *err)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    bool bad = false;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += stride) bad |= csr[i] >= nverts;
     if (__any_sync(0xFFFFFFFFu, bad) && (threadIdx.x & 31u) == 0) atomicOr(err, kErrVertexRange);
 }
 
@@ -101,9 +108,8 @@ void gw_handle::ooc_release()
     if (!ooc) return;
     OocState &o = *ooc;
     cudaSetDevice(cfg.device);
-    cudaFree(o.slot_beg);
+    cudaFree(o.d_beg);
     cudaFree(o.slot_csr);
-    cudaFree((void *)o.d_blk_beg);
     cudaFree((void *)o.d_blk_csr);
     cudaFree(o.d_vstart);
     cudaFree(o.d_estart);
@@ -118,7 +124,6 @@ void gw_handle::ooc_release()
     cudaFree(o.d_run_off);
     cudaFree(o.d_nrun);
     cudaFree(o.d_dec);
-    if (o.h_blk_beg) cudaFreeHost((void *)o.h_blk_beg);
     if (o.h_blk_csr) cudaFreeHost((void *)o.h_blk_csr);
     if (o.h_cached) cudaFreeHost(o.h_cached);
     if (o.h_dec) cudaFreeHost(o.h_dec);
@@ -189,26 +194,29 @@ static int ooc_setup(gw_handle *h)
     OocState &o = *h->ooc;
     const uint32_t nb = h->nblocks;
     o.nb = nb;
-    uint64_t maxv = 0, maxe = 0;
-    for (uint32_t b = 0; b < nb; ++b) {
-        maxv = std::max<uint64_t>(maxv, (uint64_t)h->vblocks[b + 1] - h->vblocks[b]);
-        maxe = std::max<uint64_t>(maxe, h->eblocks[b + 1] - h->eblocks[b]);
-    }
-    // slots hold the largest block (gpu/memory.hpp:65-107 sizes them the same way)
-    o.slot_beg_words = (maxv + 1 + 1) & ~1ull;   // keep slots 16-byte aligned
-    o.slot_csr_words = (std::max<uint64_t>(maxe, 1) + 3) & ~3ull;
-    const uint64_t slot_bytes = o.slot_beg_words * 8 + o.slot_csr_words * 4;
-    uint64_t ns = h->cfg.cache_size / slot_bytes;
+    uint64_t maxe = 0;
+    for (uint32_t b = 0; b < nb; ++b) maxe = std::max<uint64_t>(maxe, h->eblocks[b + 1] - h->eblocks[b]);
+    // The cache budget holds the offsets of every vertex, resident for the
+    // whole run (8 bytes per vertex), and slots of the largest block's
+    // neighbour list.  The reference sizes one slot for the largest block's
+    // offsets plus neighbours (gpu/memory.hpp:65-107); equal-edge-mass blocks
+    // differ several-fold in vertex count, so that layout strands about a
+    // fifth of the budget, and here an absent block's offsets stay readable.
+    const uint64_t beg_bytes = ((uint64_t)h->nverts + 1) * 8;
+    o.slot_csr_words = (std::max<uint64_t>(maxe, 1) + 3) & ~3ull;  // keep slots 16-byte aligned
+    const uint64_t slot_bytes = o.slot_csr_words * 4;
+    uint64_t ns = h->cfg.cache_size > beg_bytes ? (h->cfg.cache_size - beg_bytes) / slot_bytes : 0;
     if (ns > nb) ns = nb;
-    if (ns < 2) return h->fail(GW_ERR_ARG, "cache of %llu bytes holds fewer than 2 blocks of %llu bytes",
-                               (unsigned long long)h->cfg.cache_size, (unsigned long long)slot_bytes);
+    if (ns < 2)
+        return h->fail(GW_ERR_ARG,
+                       "cache of %llu bytes holds the %llu bytes of vertex offsets and fewer than 2 blocks of %llu bytes",
+                       (unsigned long long)h->cfg.cache_size, (unsigned long long)beg_bytes,
+                       (unsigned long long)slot_bytes);
     o.nslots = (uint32_t)ns;
     int st;
-    if ((st = h->cuda(cudaMalloc(&o.slot_beg, o.nslots * o.slot_beg_words * 8), "slot offsets"))) return st;
+    if ((st = h->cuda(cudaMalloc(&o.d_beg, beg_bytes), "vertex offsets"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.slot_csr, o.nslots * o.slot_csr_words * 4), "slot neighbours"))) return st;
-    if ((st = h->cuda(cudaMalloc((void **)&o.d_blk_beg, nb * sizeof(void *)), "block table"))) return st;
     if ((st = h->cuda(cudaMalloc((void **)&o.d_blk_csr, nb * sizeof(void *)), "block table"))) return st;
-    if ((st = h->cuda(cudaMallocHost((void **)&o.h_blk_beg, nb * sizeof(void *)), "block table"))) return st;
     if ((st = h->cuda(cudaMallocHost((void **)&o.h_blk_csr, nb * sizeof(void *)), "block table"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_vstart, (nb + 1) * sizeof(uint32_t)), "vstart"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_estart, (nb + 1) * sizeof(uint64_t)), "estart"))) return st;
@@ -287,16 +295,12 @@ static int ooc_map_host(gw_handle *h)
 {
     OocState &o = *h->ooc;
     if (o.mapped) return GW_OK;
-    o.map_beg.assign(o.nb, nullptr);
     o.map_csr.assign(o.nb, nullptr);
     for (uint32_t b = 0; b < o.nb; ++b) {
-        const uint64_t nv = (uint64_t)h->vblocks[b + 1] - h->vblocks[b];
         const uint64_t ne = h->eblocks[b + 1] - h->eblocks[b];
-        const void *vb = nullptr, *vc = nullptr;
+        const void *vc = nullptr;
         int st;
-        if ((st = map_block(h, o, h->host_beg[b], (nv + 1) * 8, &vb))) return st;
         if ((st = map_block(h, o, h->host_csr[b], ne * 4, &vc))) return st;
-        o.map_beg[b] = (const uint64_t *)vb;
         o.map_csr[b] = (const uint32_t *)vc;
     }
     o.mapped = true;
@@ -323,21 +327,25 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     std::fill(o.slot_block.begin(), o.slot_block.end(), -1);
     std::fill(o.block_slot.begin(), o.block_slot.end(), -1);
     o.cached.clear();
-    for (uint32_t b = 0; b < nb; ++b) {
-        o.h_blk_beg[b] = nullptr;
-        o.h_blk_csr[b] = nullptr;
-    }
+    for (uint32_t b = 0; b < nb; ++b) o.h_blk_csr[b] = nullptr;
     auto push_tables = [&]() -> int {
-        int e;
-        if ((e = cuda(cudaMemcpyAsync((void *)o.d_blk_beg, o.h_blk_beg, nb * sizeof(void *), cudaMemcpyHostToDevice, s),
-                      "block table")))
-            return e;
         return cuda(cudaMemcpyAsync((void *)o.d_blk_csr, o.h_blk_csr, nb * sizeof(void *), cudaMemcpyHostToDevice, s),
                     "block table");
     };
     if ((st = push_tables())) return st;
     if ((st = cuda(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * kCtrCount, s), "memset"))) return st;
     if ((st = cuda(cudaMemsetAsync(d_err, 0, sizeof(uint32_t), s), "memset"))) return st;
+    // every block's offsets into the resident offset array (neighbouring
+    // blocks share their boundary entry), then one validation pass
+    for (uint32_t b = 0; b < nb; ++b) {
+        const uint64_t nv = (uint64_t)vblocks[b + 1] - vblocks[b];
+        if ((st = cuda(cudaMemcpyAsync(o.d_beg + vblocks[b], host_beg[b], (nv + 1) * 8, cudaMemcpyHostToDevice, s),
+                       "block offsets")))
+            return st;
+        h2d += (nv + 1) * 8;
+    }
+    k_validate_offsets<<<num_sms * 4, 256, 0, s>>>(o.d_beg, nverts, o.d_vstart, o.d_estart, nb, d_err);
+    launches++;
 
     WalkerInit in{};
     in.mode = cfg.init_mode;
@@ -371,7 +379,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
 
     OocStepArgs a{};
     consts_from_config(cfg, a.c);  // step constants as for the in-core kernel
-    a.blk_beg = o.d_blk_beg;
+    a.beg = o.d_beg;
     a.blk_csr = o.d_blk_csr;
     a.vstart = o.d_vstart;
     a.estart = o.d_estart;
@@ -400,7 +408,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     cudaEventCreate(&k1);
     auto step = [&]() -> int {
         int e;
-        if ((e = cuda(launch_runnable(o.d_counts, o.d_offsets, o.d_blk_beg, nb, a.lazy, o.d_run_pre, o.d_run_off,
+        if ((e = cuda(launch_runnable(o.d_counts, o.d_offsets, o.d_blk_csr, nb, a.lazy, o.d_run_pre, o.d_run_off,
                                       o.d_nrun, s),
                       "runnable")))
             return e;
@@ -455,7 +463,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if (learned_active || tracing) {
             FeatureArgs f{};
             f.counts = o.d_pairs;
-            f.blk_beg = o.d_blk_beg;
+            f.blk_csr = o.d_blk_csr;
             f.emass = o.d_emass;
             f.vfrac = o.d_vfrac;
             f.prev_col = o.d_prev_col;
@@ -470,7 +478,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             launches++;
             if (learned_active) {
                 if ((st = cuda(mlp_forward(o.d_params, o.d_feat_x, nb, o.d_pred, s), "predictor"))) break;
-                if ((st = cuda(launch_learned_choose(o.d_pred, nb, o.d_blk_beg, o.d_cached, ncached,
+                if ((st = cuda(launch_learned_choose(o.d_pred, nb, o.d_blk_csr, o.d_cached, ncached,
                                                      o.nslots, kMaxLoadsPerIter, kSwapMargin, o.d_choose, s),
                                "learned choice")))
                     break;
@@ -560,10 +568,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             // ---- zero-copy tail: every absent block read through mapped host memory
             if ((st = ooc_map_host(this))) break;
             for (uint32_t b = 0; b < nb; ++b)
-                if (o.block_slot[b] < 0) {
-                    o.h_blk_beg[b] = o.map_beg[b];
-                    o.h_blk_csr[b] = o.map_csr[b];
-                }
+                if (o.block_slot[b] < 0) o.h_blk_csr[b] = o.map_csr[b];
             if ((st = push_tables())) break;
             unsigned long long before[kCtrCount];
             memcpy(before, h_ctr, sizeof(before));
@@ -576,10 +581,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             zc_steps += h_ctr[kCtrSteps] - before[kCtrSteps];
             // restore the table to device slots only
             for (uint32_t b = 0; b < nb; ++b)
-                if (o.block_slot[b] < 0) {
-                    o.h_blk_beg[b] = nullptr;
-                    o.h_blk_csr[b] = nullptr;
-                }
+                if (o.block_slot[b] < 0) o.h_blk_csr[b] = nullptr;
             if ((st = push_tables())) break;
             if ((st = bucketize(nlive))) break;
             iters++;
@@ -601,7 +603,6 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 const uint32_t victim = o.cached[position];
                 slot = o.block_slot[victim];
                 o.block_slot[victim] = -1;
-                o.h_blk_beg[victim] = nullptr;
                 o.h_blk_csr[victim] = nullptr;
                 o.cached[position] = (uint32_t)load_block;
             } else {
@@ -617,23 +618,17 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 break;
             }
             const uint32_t b = (uint32_t)load_block;
-            const uint64_t nv = (uint64_t)vblocks[b + 1] - vblocks[b];
             const uint64_t ne = eblocks[b + 1] - eblocks[b];
-            uint64_t *sb = o.slot_beg + (uint64_t)slot * o.slot_beg_words;
             uint32_t *sc = o.slot_csr + (uint64_t)slot * o.slot_csr_words;
-            if ((st = cuda(cudaMemcpyAsync(sb, host_beg[b], (nv + 1) * 8, cudaMemcpyHostToDevice, s), "block offsets")))
-                break;
             if (ne &&
                 (st = cuda(cudaMemcpyAsync(sc, host_csr[b], ne * 4, cudaMemcpyHostToDevice, s), "block neighbours")))
                 break;
-            h2d += (nv + 1) * 8 + ne * 4;
+            h2d += ne * 4;
             loads++;
-            k_validate_block<<<num_sms * 4, 256, 0, s>>>(sb, sc, (uint32_t)nv, eblocks[b], eblocks[b + 1], nverts,
-                                                         d_err);
+            k_validate_block<<<num_sms * 4, 256, 0, s>>>(sc, ne, nverts, d_err);
             launches++;
             o.slot_block[slot] = (int)b;
             o.block_slot[b] = slot;
-            o.h_blk_beg[b] = sb;
             o.h_blk_csr[b] = sc;
         }
         if (st) break;

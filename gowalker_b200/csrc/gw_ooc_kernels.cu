@@ -153,12 +153,12 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const uint32_t *__restric
 
 __global__ void __launch_bounds__(kScanThreads) k_runnable(const uint32_t *__restrict__ counts,
                                                            const uint32_t *__restrict__ offsets,
-                                                           const uint64_t *const *__restrict__ blk_beg, uint32_t nb,
+                                                           const uint32_t *const *__restrict__ blk_csr, uint32_t nb,
                                                            uint32_t lazy, uint32_t *__restrict__ run_pre,
                                                            uint32_t *__restrict__ run_off, uint32_t *__restrict__ nrun)
 {
     __shared__ uint8_t s_res[kMaxBlocks];
-    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) s_res[i] = blk_beg[i] != nullptr;
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) s_res[i] = blk_csr[i] != nullptr;
     __syncthreads();
     const uint32_t nn = nb * nb, n = 2 * nn;
     // unflagged walkers need their current block (and, unless lazy, the
@@ -362,12 +362,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
             finish();
             return;
         }
-        const uint64_t *cbeg = a.blk_beg[cb];
         ccsr = a.blk_csr[cb];
-        const uint32_t off = cur - s_vs[cb];
-        const uint64_t e0 = a.estart[cb];
-        const uint64_t b0 = __ldg(cbeg + off), b1 = __ldg(cbeg + off + 1);
-        head = b0 - e0;
+        const uint64_t b0 = __ldg(a.beg + cur), b1 = __ldg(a.beg + cur + 1);
+        head = b0 - a.estart[cb];
         deg = (uint32_t)(b1 - b0);
         if (deg == 0) {
             finish();
@@ -412,23 +409,18 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
                 pb = rec.prev_blk;
                 cb = rec.cur_blk & ~kNeedPrev;
                 h = ((uint64_t)rec.hash_hi << 32) | rec.hash_lo;
-                const uint64_t *pbeg = hop < maxhops ? a.blk_beg[pb] : nullptr;
+                // lazy mode: the previous block may be absent (pcsr null); its
+                // offsets are resident, so deg(prev) is known either way
+                pcsr = hop < maxhops ? a.blk_csr[pb] : nullptr;
                 if (hop >= maxhops) {
                     finish();
-                } else if (pbeg == nullptr && !a.lazy) {
+                } else if (pcsr == nullptr && !a.lazy) {
                     atomicOr(a.err, kErrBlock);  // scheduled without its previous block
                     finish();
                 } else {
-                    pcsr = nullptr;  // lazy mode, previous block absent: N(prev) unknown
-                    phead = 0;
-                    pdeg = 0;
-                    if (pbeg != nullptr) {
-                        pcsr = a.blk_csr[pb];
-                        const uint32_t poff = prev - s_vs[pb];
-                        const uint64_t p0 = __ldg(pbeg + poff), p1 = __ldg(pbeg + poff + 1);
-                        phead = p0 - a.estart[pb];
-                        pdeg = (uint32_t)(p1 - p0);
-                    }
+                    const uint64_t p0 = __ldg(a.beg + prev), p1 = __ldg(a.beg + prev + 1);
+                    phead = p0 - a.estart[pb];
+                    pdeg = (uint32_t)(p1 - p0);
                     enter();
                 }
             }
@@ -508,7 +500,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
                 finish();
             } else {
                 const uint32_t nbx = (x >= s_vs[cb] && x < s_vs[cb + 1]) ? cb : block_of(s_vs, a.nb, x);
-                if (a.blk_beg[nbx] == nullptr) {
+                if (a.blk_csr[nbx] == nullptr) {
                     // next block absent: park the walker in bucket (cb, nbx)
                     WalkerRec rec;
                     rec.wid = wid;
@@ -557,7 +549,7 @@ __global__ void __launch_bounds__(1024) k_features(const FeatureArgs f)
 {
     __shared__ uint8_t s_res[kMaxBlocks];
     const uint32_t nb = f.nb;
-    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) s_res[i] = f.blk_beg[i] != nullptr;
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) s_res[i] = f.blk_csr[i] != nullptr;
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
         uint64_t col = 0, row = 0, cross = 0, ready = 0;
@@ -608,14 +600,14 @@ __global__ void k_targets(const float *col_hist, uint32_t T, uint32_t k, uint32_
 // One thread: fill free slots with the highest predicted uncached blocks, then
 // swap while the best uncached block's predicted demand beats the worst
 // resident one's by `margin` (log scale); blocks chosen this round stay.
-__global__ void k_learned_choose(const float *__restrict__ pred, uint32_t nb, const uint64_t *const *blk_beg,
+__global__ void k_learned_choose(const float *__restrict__ pred, uint32_t nb, const uint32_t *const *blk_csr,
                                  const uint32_t *__restrict__ cached, uint32_t ncached, uint32_t nslots,
                                  uint32_t lmax, float margin, int32_t *out)
 {
     __shared__ uint8_t s_state[kMaxBlocks];  // 0 absent, 1 resident, 2 chosen now, 3 evicted now
     __shared__ int32_t s_pos[kMaxBlocks];
     for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
-        s_state[i] = blk_beg[i] != nullptr ? 1 : 0;
+        s_state[i] = blk_csr[i] != nullptr ? 1 : 0;
         s_pos[i] = -1;
     }
     __syncthreads();
@@ -668,11 +660,11 @@ cudaError_t launch_targets(const float *col_hist, uint32_t T, uint32_t k, uint32
     return cudaGetLastError();
 }
 
-cudaError_t launch_learned_choose(const float *pred, uint32_t nb, const uint64_t *const *blk_beg,
+cudaError_t launch_learned_choose(const float *pred, uint32_t nb, const uint32_t *const *blk_csr,
                                   const uint32_t *cached, uint32_t ncached, uint32_t nslots, uint32_t lmax,
                                   float margin, int32_t *out, cudaStream_t s)
 {
-    k_learned_choose<<<1, 256, 0, s>>>(pred, nb, blk_beg, cached, ncached, nslots, lmax, margin, out);
+    k_learned_choose<<<1, 256, 0, s>>>(pred, nb, blk_csr, cached, ncached, nslots, lmax, margin, out);
     return cudaGetLastError();
 }
 
@@ -705,11 +697,11 @@ cudaError_t launch_scatter(const WalkerRec *in, uint64_t n, uint32_t nb, const u
     return cudaGetLastError();
 }
 
-cudaError_t launch_runnable(const uint32_t *counts, const uint32_t *offsets, const uint64_t *const *blk_beg,
+cudaError_t launch_runnable(const uint32_t *counts, const uint32_t *offsets, const uint32_t *const *blk_csr,
                             uint32_t nb, uint32_t lazy, uint32_t *run_pre, uint32_t *run_off, uint32_t *nrun,
                             cudaStream_t s)
 {
-    k_runnable<<<1, kScanThreads, 0, s>>>(counts, offsets, blk_beg, nb, lazy, run_pre, run_off, nrun);
+    k_runnable<<<1, kScanThreads, 0, s>>>(counts, offsets, blk_csr, nb, lazy, run_pre, run_off, nrun);
     return cudaGetLastError();
 }
 

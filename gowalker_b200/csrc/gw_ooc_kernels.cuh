@@ -25,8 +25,8 @@ constexpr uint32_t kNeedPrev = 0x80000000u;
 
 struct OocStepArgs {
     StepConsts c;
-    const uint64_t *const *blk_beg;  // [nb] block offsets (entry 0 = vertex vstart[b]); null = absent
-    const uint32_t *const *blk_csr;  // [nb] block neighbours, indexed from estart[b]
+    const uint64_t *beg;             // [nverts+1] offsets of every vertex (global edge ids), resident
+    const uint32_t *const *blk_csr;  // [nb] block neighbours, indexed from estart[b]; null = absent
     const uint32_t *vstart;          // [nb+1]
     const uint64_t *estart;          // [nb+1]
     uint32_t nb, nverts;
@@ -63,7 +63,7 @@ cudaError_t launch_scatter(const WalkerRec *in, uint64_t n, uint32_t nb, const u
                            uint32_t *cursor, WalkerRec *out, int num_sms, cudaStream_t s);
 // Buckets are 2 * nb^2: (prev_blk, cur_blk), then the same pairs for walkers
 // flagged kNeedPrev.
-cudaError_t launch_runnable(const uint32_t *counts, const uint32_t *offsets, const uint64_t *const *blk_beg,
+cudaError_t launch_runnable(const uint32_t *counts, const uint32_t *offsets, const uint32_t *const *blk_csr,
                             uint32_t nb, uint32_t lazy, uint32_t *run_pre, uint32_t *run_off, uint32_t *nrun,
                             cudaStream_t s);
 // combined[k] = counts[k] + counts[nb^2 + k]: walkers per (prev, cur) block pair.
@@ -76,7 +76,7 @@ cudaError_t launch_schedule(const uint32_t *counts, const uint32_t *live, uint32
 
 struct FeatureArgs {
     const uint32_t *counts;            // [nb*nb] bucket counts after the last bucketing
-    const uint64_t *const *blk_beg;    // residency (non-null = resident)
+    const uint32_t *const *blk_csr;    // residency (non-null = resident)
     const float *emass, *vfrac;        // edge / vertex share of each block, times nb
     float *prev_col, *ema_arr;         // per-block history, updated in place
     uint32_t nb, iter;
@@ -89,7 +89,7 @@ cudaError_t launch_features(const FeatureArgs &f, cudaStream_t s);
 cudaError_t launch_targets(const float *col_hist, uint32_t T, uint32_t k, uint32_t nb, float *y, cudaStream_t s);
 // Up to lmax (block, cached position or -1 for a free slot) pairs by
 // predicted demand; out[0] = count, then the pairs.
-cudaError_t launch_learned_choose(const float *pred, uint32_t nb, const uint64_t *const *blk_beg,
+cudaError_t launch_learned_choose(const float *pred, uint32_t nb, const uint32_t *const *blk_csr,
                                   const uint32_t *cached, uint32_t ncached, uint32_t nslots, uint32_t lmax,
                                   float margin, int32_t *out, cudaStream_t s);
 

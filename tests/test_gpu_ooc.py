@@ -15,14 +15,17 @@ def graph(oracle, scale=13, ef=8, sym=False, cap=6000, seed=21):
     return oracle.build_csr(cap, src[keep], dst[keep], symmetric=sym)
 
 
+def cache_for(beg, eb, slots):
+    """Cache bytes for the resident vertex offsets plus `slots` neighbour slots."""
+    maxe = int(np.diff(eb.astype(np.int64)).max())
+    return len(beg) * 8 + ((max(maxe, 1) + 3) & ~3) * 4 * slots
+
+
 def run_ooc(gw, beg, csr, nblocks, slots, algo=0, maxhops=20, wps=1, p=0.5, q=2.0, alpha=0.2, term=0.0, seed=5,
             zero_copy=0, zero_threshold=0, paths=1, policy=0):
     from gowalker_b200.preprocess import split_equal_edge_mass
     vb, eb = split_equal_edge_mass(beg, nblocks)
-    maxv = int(np.diff(vb.astype(np.int64)).max())
-    maxe = int(np.diff(eb.astype(np.int64)).max())
-    slot = ((maxv + 2) & ~1) * 8 + ((max(maxe, 1) + 3) & ~3) * 4
-    cache = slot * slots
+    cache = cache_for(beg, eb, slots)
     eng = gw.WalkEngine(algorithm=algo, maxhops=maxhops, p=p, q=q, alpha=alpha, term_prob=term, seed=seed,
                         walkpersource=wps, record_paths=paths, cache_size=cache, zero_copy=zero_copy,
                         zero_threshold=zero_threshold)
@@ -105,11 +108,8 @@ def test_zero_copy_leaves_neighbouring_host_data_writable(gw, oracle):
     arena[:V + 1] = beg
     from gowalker_b200.preprocess import split_equal_edge_mass
     vb, eb = split_equal_edge_mass(beg, 10)
-    maxv = int(np.diff(vb.astype(np.int64)).max())
-    maxe = int(np.diff(eb.astype(np.int64)).max())
-    slot = ((maxv + 2) & ~1) * 8 + ((max(maxe, 1) + 3) & ~3) * 4
     eng = gw.WalkEngine(algorithm=1, maxhops=20, alpha=0.2, term_prob=0.15, seed=5, walkpersource=1,
-                        record_paths=0, cache_size=slot * 3, zero_copy=1, zero_threshold=400)
+                        record_paths=0, cache_size=cache_for(beg, eb, 3), zero_copy=1, zero_threshold=400)
     eng.set_host_graph(arena[:V + 1], csr, vb, eb)
     eng.init_walkers(1, 1, 5)
     st = eng.run()
@@ -133,11 +133,8 @@ def test_lazy_previous_block_same_walks_fewer_loads(gw, oracle, sym):
     for strict in (1, 0):
         from gowalker_b200.preprocess import split_equal_edge_mass
         vb, eb = split_equal_edge_mass(beg, 16)
-        maxv = int(np.diff(vb.astype(np.int64)).max())
-        maxe = int(np.diff(eb.astype(np.int64)).max())
-        slot = ((maxv + 2) & ~1) * 8 + ((max(maxe, 1) + 3) & ~3) * 4
         eng = gw.WalkEngine(algorithm=0, maxhops=30, p=0.5, q=2.0, seed=5, walkpersource=1, record_paths=1,
-                            cache_size=slot * 4, strict_blocks=strict)
+                            cache_size=cache_for(beg, eb, 4), strict_blocks=strict)
         eng.set_host_graph(beg, csr, vb, eb)
         eng.init_walkers(0, 1, 5)
         st = eng.run()
