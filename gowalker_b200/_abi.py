@@ -51,7 +51,8 @@ class GwConfig(ctypes.Structure):
         ("record_paths", ctypes.c_uint32),
         ("device", ctypes.c_int32),
         ("strict_blocks", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 7),
+        ("prefetch", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 6),
     ]
 
 

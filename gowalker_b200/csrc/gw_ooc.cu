@@ -445,10 +445,55 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     double pred_err_sum = 0.0;
     uint32_t pred_err_n = 0;
     std::vector<float> prev_pred;
+    // Prefetch: each decision is taken one iteration ahead and its block is
+    // copied on the copy stream into a staging slot while the current step
+    // kernel runs; it becomes resident at the start of the next iteration.
+    // One slot is the staging slot, so nslots - 1 blocks are resident.
+    const bool prefetch = cfg.prefetch != 0;
+    const uint32_t capacity = prefetch ? o.nslots - 1 : o.nslots;
+    int staged_block = -1, staged_pos = -1, staging_slot = prefetch ? 0 : -1;
+    if (prefetch && o.nslots < 3) {
+        cudaEventDestroy(k0);
+        cudaEventDestroy(k1);
+        return fail(GW_ERR_ARG, "prefetch needs a cache of at least 3 blocks (has %u)", o.nslots);
+    }
+    cudaEvent_t staged_ev = nullptr;
+    if (prefetch) cudaEventCreateWithFlags(&staged_ev, cudaEventDisableTiming);
     while (!done) {
         if (++iters > kMaxIters) {
             st = fail(GW_ERR_STATE, "out-of-core run exceeded %u scheduler iterations", kMaxIters);
             break;
+        }
+        if (staged_block >= 0) {
+            // ---- the block copied during the last step becomes resident
+            if ((st = cuda(cudaStreamWaitEvent(s, staged_ev, 0), "staged copy"))) break;
+            int freed = -1;
+            if (staged_pos >= 0) {
+                const uint32_t victim = o.cached[staged_pos];
+                freed = o.block_slot[victim];
+                o.slot_block[freed] = -1;
+                o.block_slot[victim] = -1;
+                o.h_blk_csr[victim] = nullptr;
+                o.cached[staged_pos] = (uint32_t)staged_block;
+            } else {
+                o.cached.push_back((uint32_t)staged_block);
+            }
+            const uint32_t b = (uint32_t)staged_block;
+            uint32_t *sc = o.slot_csr + (uint64_t)staging_slot * o.slot_csr_words;
+            k_validate_block<<<num_sms * 4, 256, 0, s>>>(sc, eblocks[b + 1] - eblocks[b], nverts, d_err);
+            launches++;
+            o.slot_block[staging_slot] = (int)b;
+            o.block_slot[b] = staging_slot;
+            o.h_blk_csr[b] = sc;
+            staging_slot = freed;
+            if (staging_slot < 0)
+                for (uint32_t k = 0; k < o.nslots; ++k)
+                    if (o.slot_block[k] < 0) {
+                        staging_slot = (int)k;
+                        break;
+                    }
+            staged_block = -1;
+            if ((st = push_tables())) break;
         }
         const uint32_t ncached = (uint32_t)o.cached.size();
         for (uint32_t j = 0; j < ncached; ++j) o.h_cached[j] = o.cached[j];
@@ -478,8 +523,8 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             launches++;
             if (learned_active) {
                 if ((st = cuda(mlp_forward(o.d_params, o.d_feat_x, nb, o.d_pred, s), "predictor"))) break;
-                if ((st = cuda(launch_learned_choose(o.d_pred, nb, o.d_blk_csr, o.d_cached, ncached,
-                                                     o.nslots, kMaxLoadsPerIter, kSwapMargin, o.d_choose, s),
+                if ((st = cuda(launch_learned_choose(o.d_pred, nb, o.d_blk_csr, o.d_cached, ncached, capacity,
+                                                     prefetch ? 1u : kMaxLoadsPerIter, kSwapMargin, o.d_choose, s),
                                "learned choice")))
                     break;
                 launches += 2;
@@ -495,7 +540,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             }
         }
         // ---- plain block choice on the device (decision, fallback and rescue), read back
-        if ((st = cuda(launch_schedule(o.d_pairs, o.d_offsets + nbk, nb, o.d_cached, ncached, o.nslots, cfg.zero_threshold,
+        if ((st = cuda(launch_schedule(o.d_pairs, o.d_offsets + nbk, nb, o.d_cached, ncached, capacity, cfg.zero_threshold,
                                        nullptr, 0.f, o.d_dec, s),
                        "schedule")))
             break;
@@ -526,7 +571,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             if (last_phase == 1) {
                 learned_steps += ds;
                 learned_bytes += db;
-            } else if (o.cached.size() >= o.nslots) {
+            } else if (o.cached.size() >= capacity) {
                 plain_steps += ds;
                 plain_bytes += db;
             }
@@ -564,7 +609,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         } else if (d.action == 1 || d.action == 2) {
             todo.emplace_back(d.block, d.action == 2 ? d.position : -1);
             last_phase = 0;
-        } else if (cfg.zero_copy) {
+        } else if (cfg.zero_copy && !prefetch) {
             // ---- zero-copy tail: every absent block read through mapped host memory
             if ((st = ooc_map_host(this))) break;
             for (uint32_t b = 0; b < nb; ++b)
@@ -587,14 +632,34 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             iters++;
             done = true;
             break;
-        } else if (d.rescue_block >= 0 && (o.cached.size() < o.nslots || d.rescue_position >= 0)) {
-            todo.emplace_back(d.rescue_block, (o.cached.size() >= o.nslots) ? d.rescue_position : -1);
+        } else if (d.rescue_block >= 0 && (o.cached.size() < capacity || d.rescue_position >= 0)) {
+            todo.emplace_back(d.rescue_block, (o.cached.size() >= capacity) ? d.rescue_position : -1);
             last_phase = 0;
+        } else if (prefetch) {
+            // decided before this iteration's step: every live walker's
+            // blocks are resident, so the step runs them; nothing to stage
         } else {
             st = fail(GW_ERR_STATE, "no block can make progress (%u live walkers)", (unsigned)nlive);
             break;
         }
 
+        if (prefetch && !todo.empty()) {
+            // ---- copy the chosen block into the staging slot on the copy
+            // stream; it overlaps this iteration's step (everything on the
+            // compute stream has finished: the decision read-back synced it)
+            const uint32_t b = (uint32_t)todo.front().first;
+            const uint64_t ne = eblocks[b + 1] - eblocks[b];
+            uint32_t *sc = o.slot_csr + (uint64_t)staging_slot * o.slot_csr_words;
+            if (ne &&
+                (st = cuda(cudaMemcpyAsync(sc, host_csr[b], ne * 4, cudaMemcpyHostToDevice, s_copy), "block neighbours")))
+                break;
+            if ((st = cuda(cudaEventRecord(staged_ev, s_copy), "event"))) break;
+            h2d += ne * 4;
+            loads++;
+            staged_block = (int)b;
+            staged_pos = todo.front().second;
+            todo.clear();
+        }
         // ---- load the chosen blocks into slots
         for (const auto &ld : todo) {
             const int load_block = ld.first, position = ld.second;
@@ -666,6 +731,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             st = cuda(cudaStreamSynchronize(s), "run");
     } else {
         cudaStreamSynchronize(s);
+    }
+    if (staged_ev) {
+        cudaStreamSynchronize(s_copy);  // a staged copy may still be in flight
+        cudaEventDestroy(staged_ev);
     }
     cudaEventDestroy(k0);
     cudaEventDestroy(k1);

@@ -95,7 +95,10 @@ typedef struct gw_config {
     uint32_t strict_blocks;   /* out-of-core: 1 = a walker runs only when both its blocks are
                                  resident (the reference's rule); 0 = Node2vec walkers also run
                                  with only the current block until a trial needs N(prev) */
-    uint32_t reserved[7];
+    uint32_t prefetch;        /* out-of-core: 1 = take each block choice one iteration ahead and
+                                 copy the block on the copy stream while the step kernel runs
+                                 (one cache slot stages the copy) */
+    uint32_t reserved[6];
 } gw_config;
 
 /* Per-run counters. */

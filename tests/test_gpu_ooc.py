@@ -149,3 +149,25 @@ def test_lazy_previous_block_same_walks_fewer_loads(gw, oracle, sym):
         assert np.array_equal(H, ref["hashes"])
         assert st["steps"] == ref["stats"]["steps"] and st["trials"] == ref["stats"]["trials"]
     assert res[0][3]["block_loads"] < res[1][3]["block_loads"]
+
+
+@pytest.mark.parametrize("algo,policy", [(0, 0), (1, 0), (0, 1)])
+def test_prefetch_same_walks(gw, oracle, algo, policy):
+    """Block choices taken one iteration ahead, copies overlapped with the
+    step kernel in a staging slot: the walks stay those of the oracle."""
+    beg, csr = graph(oracle, scale=13, ef=12, sym=algo == 1, cap=7000, seed=3)
+    V = len(beg) - 1
+    from gowalker_b200.preprocess import split_equal_edge_mass
+    vb, eb = split_equal_edge_mass(beg, 12)
+    eng = gw.WalkEngine(algorithm=algo, maxhops=25, p=0.5, q=2.0, alpha=0.2, term_prob=0.15 if algo else 0.0,
+                        seed=11, walkpersource=1, record_paths=1, cache_size=cache_for(beg, eb, 4), prefetch=1)
+    eng.set_host_graph(beg, csr, vb, eb)
+    eng.init_walkers(algo, 1, 11)
+    st = eng.run(policy)
+    P, L = eng.paths()
+    ref = oracle.walk(beg, csr, oracle.make_cfg(algo=algo, maxhops=25, p=0.5, q=2.0, alpha=0.2,
+                                                term_prob=0.15 if algo else 0.0, seed=11), 0, V, paths=True)
+    assert np.array_equal(P, ref["paths"]) and np.array_equal(L, ref["lens"])
+    assert st["steps"] == ref["stats"]["steps"] and st["trials"] == ref["stats"]["trials"]
+    assert st["block_loads"] > 0 and int(eng.bucket_counts().sum()) == 0
+    eng.close()
