@@ -328,6 +328,29 @@ def ref_scenario(base: str, algo: int, p: float, q: float, alpha: float, maxhops
     return nb, [ref_walk(L, *s) for s in starts]
 
 
+def ref_single_steps(base: str, algo: int, p: float, q: float, alpha: float, seed: int, starts,
+                     unmodified: bool = False):
+    """One reference step per start tuple (wid, prev, cur, hop, prev_blk,
+    cur_blk) on a dataset whose current block holds every neighbour of cur:
+    the reference's cross-block loop (engine/engine.hpp:173-274) then stops
+    after one step and re-buckets the walker, whose new vertex is returned
+    (-1 when it was not re-bucketed).  Run in a fresh process ('spawn')."""
+    L = ref_lib(unmodified)
+    if L is None:
+        raise FileNotFoundError("oracle/_ref harness not built")
+    L.ref_open(base.encode(), algo, p, q, alpha, 1 << 20, 1, 64)
+    L.ref_set_seed(seed)
+    tr = np.zeros((4, 4), dtype=np.uint32)
+    n, pushed = ctypes.c_uint64(0), ctypes.c_int(0)
+    state = np.zeros(5, dtype=np.uint32)
+    out = np.full(len(starts), -1, dtype=np.int64)
+    for i, s in enumerate(starts):
+        L.ref_walk(*s, _p(tr, ctypes.c_uint32), 4, ctypes.byref(n), ctypes.byref(pushed), _p(state, ctypes.c_uint32))
+        if pushed.value:
+            out[i] = int(state[1])
+    return out
+
+
 def harness_graph(beg: np.ndarray, csr: np.ndarray):
     """Graph G' for driving the reference's cross-block loop from a walk's
     first step: vertex V+v is a copy of v's adjacency (nothing points to it),

@@ -191,3 +191,55 @@ def test_mlp_oracle_gradient_by_finite_differences():
         pp[idx] -= 2e-6
         lm, _ = M.loss_and_grad(pp, x, t)
         assert abs((lp - lm) / 2e-6 - g[idx]) < 1e-5 * max(1.0, abs(g[idx]))
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_step_unmod.so")),
+                    reason="reference harness not built (needs the GOWalker sources)")
+@pytest.mark.parametrize("algo", [0, 1])
+def test_transition_law_chi_square(oracle, tmp_path, algo):
+    """Transition frequencies out of one (prev, cur) state against the analytic
+    second-order law (engine/engine.hpp:209-258, 334-375): the oracle (the
+    engine's stream) and the reference's own CPU step fed the Philox stream
+    follow it; the unmodified reference does not.  That outcome is recorded,
+    not fixed: its RandNum::inlineRandPair (util/util.hpp:291-301) builds
+    rand_val by reading the low 32 bits of a 64-bit integer as a float."""
+    from scipy.stats import chisquare
+    V = 200
+    src, dst = oracle.rmat_edges(8, 0, 8 << 8, seed=3)
+    keep = (src < V) & (dst < V)
+    beg, csr = oracle.build_csr(V, src[keep], dst[keep], symmetric=True)
+    # vertices 0..V-1 in block 0; V+v, a copy of v's adjacency that nothing
+    # points to, in block 1: a walker at (V+p, c) takes one step inside block 0
+    beg2, csr2, _, _ = oracle.harness_graph(beg, csr)
+    E = int(beg[-1])
+    base = str(tmp_path / "g")
+    oracle.write_dataset(base, beg2, csr2)
+    oracle.write_blocks(base, 1, np.array([0, V, 2 * V], dtype=np.uint32), np.array([0, E, 2 * E], dtype=np.uint64))
+    deg = np.diff(beg.astype(np.int64))
+    c = int(np.argsort(deg)[-3])
+    nc = csr[beg[c]:beg[c + 1]]
+    p = int(max(nc, key=lambda y: len(np.intersect1d(nc, csr[beg[y]:beg[y + 1]]))))
+    found = np.isin(nc, csr[beg[p]:beg[p + 1]])
+    assert 0 < found.sum() < len(nc)
+    if algo == 0:  # Node2vec p=0.5, q=2: weight 1 in N(prev), 1/q outside (x == V+p never occurs)
+        w = np.where(found, 1.0, 0.5)
+    else:          # SOPR alpha 0.2: (1-alpha)/deg(cur) + alpha/deg(prev) in N(prev)
+        w = 0.8 / deg[c] + np.where(found, 0.2 / deg[p], 0.0)
+    prob = w / w.sum()
+    n = 30000
+    starts = [(i, V + p, c, 0, 1, 0) for i in range(n)]
+
+    def pvalue(nxt):
+        assert np.all(nxt >= 0)
+        counts = np.array([np.sum(nxt == x) for x in nc])
+        return chisquare(counts, prob * counts.sum()).pvalue
+
+    res = {}
+    for unmod in (False, True):
+        with mp.get_context("spawn").Pool(1) as pool:
+            res[unmod] = pool.apply(oracle.ref_single_steps, (base, algo, 0.5, 2.0, 0.2, 12345, starts, unmod))
+    cfg = oracle.make_cfg(algo=algo, maxhops=1, p=0.5, q=2.0, alpha=0.2, seed=777)
+    ours = np.array([oracle.walk_traced(beg2, csr2, cfg, i, V + p, c, 0, cap=16)[1][0] for i in range(n)])
+    assert pvalue(ours) > 1e-3
+    assert pvalue(res[False]) > 1e-3
+    assert pvalue(res[True]) < 1e-4
