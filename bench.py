@@ -241,7 +241,7 @@ def run_ooc_bench(args, wl):
     eng = gw.WalkEngine(algorithm=wl["algo"], maxhops=wl["maxhops"], p=wl["p"], q=wl["q"], alpha=wl["alpha"],
                         term_prob=wl["term"], seed=42, walkpersource=wl["wps"], record_paths=1 if args.paths else 0,
                         cache_size=wl["cache"], zero_copy=0, strict_blocks=1 if args.strict_blocks else 0,
-                        prefetch=1 if args.prefetch else 0)
+                        prefetch=1 if args.prefetch else 0, compress_blocks=1 if args.compress else 0)
     eng.set_host_graph(beg_t, csr_t[: len(csr)], vb, eb)
     stream = torch.cuda.ExternalStream(eng.stream_handle())
     for _ in range(args.warmup):
@@ -276,6 +276,7 @@ def run_ooc_bench(args, wl):
                        "residency": "both blocks (reference rule)" if args.strict_blocks else
                                     "current block until N(prev) is needed",
                        "prefetch": bool(args.prefetch),
+                       "compressed_blocks": bool(args.compress),
                        "vertices": len(beg) - 1, "edges": len(csr),
                        "blocks": wl["nblocks"], "cache_bytes": wl["cache"], "walkers": eng.num_walkers(),
                        "graph_in": "pinned host memory", "paths_recorded": bool(args.paths)},
@@ -476,6 +477,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--policy", default="plain", choices=["plain", "learned"], help="block policy (out-of-core)")
+    ap.add_argument("--compress", action="store_true",
+                    help="out-of-core: copy compressed neighbour lists and decode them on the device")
     ap.add_argument("--prefetch", action="store_true",
                     help="out-of-core: choose blocks one iteration ahead and overlap their copies with the step")
     ap.add_argument("--strict-blocks", action="store_true",

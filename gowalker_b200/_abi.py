@@ -52,7 +52,8 @@ class GwConfig(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("strict_blocks", ctypes.c_uint32),
         ("prefetch", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 6),
+        ("compress_blocks", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 5),
     ]
 
 

@@ -1,0 +1,51 @@
+// Compressed neighbour lists of out-of-core blocks (internal to libgowalker.so).
+//
+// A block's neighbour ids cross the host link once per load, so the engine
+// keeps a compressed copy of every block in pinned host memory and decodes it
+// on the device into the block's cache slot.  Layout of one block's buffer:
+//
+//   u32 voff[nv + 1]      byte offset of each vertex's chunks in the payload
+//   (pad to 16 bytes)
+//   payload               per vertex, ceil(deg / 32) chunks of up to 32 ids:
+//                           u8  w       bit width of the chunk's deltas
+//                           u32 first   first id (little endian, unaligned)
+//                           (k-1) deltas, zigzag-coded, packed LSB first at w bits
+//   8 bytes of padding    so a decoder may read up to 5 bytes past a field
+//
+// Deltas are id[i] - id[i-1] modulo 2^32, zigzag-coded, so any neighbour order
+// (sorted or not, duplicates included) round-trips exactly; sorted lists give
+// small deltas.  The offsets of every vertex are resident on the device, so
+// the decoder knows each vertex's degree and output position without them
+// crossing the link again.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+
+namespace gw {
+
+constexpr uint32_t kChunkIds = 32;
+
+struct CompressedBlock {
+    uint8_t *host = nullptr;   // pinned (cudaHostAlloc), owned by the handle
+    uint64_t bytes = 0;        // whole buffer: offsets, payload, padding
+    uint64_t payload_off = 0;  // start of the payload in the buffer
+    uint64_t payload_bytes = 0;
+};
+
+// Encode block [beg[0], beg[nv]) (global edge ids; csr indexed from beg[0]).
+// Checks that the offsets are non-decreasing and start and end at e0 / e1.
+// Returns false with `why` set when they are not or the payload would exceed
+// 2^32 bytes.  Uses up to `threads` host threads.
+bool compress_block(const uint64_t *beg, const uint32_t *csr, uint32_t nv, uint64_t e0, uint64_t e1,
+                    unsigned threads, CompressedBlock &out, std::string &why);
+
+// Decode a block copied to the device at `src` (the layout above) into `out`
+// (neighbour slot, indexed from e0).  beg: resident offsets of every vertex,
+// v0: the block's first vertex.  Any offset or payload read outside the
+// buffer sets kErrBlock in *err and skips the vertex.
+cudaError_t launch_decode_block(const uint8_t *src, uint64_t payload_off, uint64_t payload_bytes, uint32_t nv,
+                                const uint64_t *beg, uint32_t v0, uint64_t e0, uint64_t ne, uint32_t *out,
+                                uint32_t *err, int num_sms, cudaStream_t s);
+
+}  // namespace gw

@@ -350,7 +350,7 @@ extern "C" int gw_host_block(gw_handle *h, uint32_t blk, const uint64_t *beg, co
     h->host_beg[blk] = beg;
     h->host_csr[blk] = csr;
     h->resident = false;
-    h->ooc_invalidate();
+    h->ooc_invalidate(true);
     return GW_OK;
 }
 
@@ -377,7 +377,7 @@ extern "C" int gw_cache_reset(gw_handle *h)
     if (!h) return GW_ERR_ARG;
     if (h->device_graph) return GW_OK;
     h->resident = false;
-    h->ooc_invalidate();
+    h->ooc_invalidate(false);
     return GW_OK;
 }
 

@@ -89,5 +89,5 @@ struct gw_handle {
     int run_incore(gw_stats *stats);
     int run_ooc(uint32_t policy, gw_stats *stats);
     void ooc_release();
-    void ooc_invalidate();
+    void ooc_invalidate(bool blocks_changed);
 };

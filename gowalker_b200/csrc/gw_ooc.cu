@@ -19,7 +19,9 @@
 #include "gw_engine.cuh"
 #include "gw_ooc_kernels.cuh"
 #include "gw_mlp.cuh"
+#include "gw_compress.cuh"
 #include <cmath>
+#include <thread>
 
 namespace gw {
 
@@ -52,6 +54,12 @@ struct OocState {
     std::vector<const uint32_t *> map_csr;
     std::vector<void *> staged;
     bool mapped = false;
+
+    // compressed neighbour lists (compress_blocks): pinned host copies of
+    // every block, and the device buffer a load lands in before decoding
+    bool compressed = false;
+    std::vector<CompressedBlock> cblk;
+    uint8_t *d_cstage = nullptr;
 
     bool ready = false;
 
@@ -128,6 +136,9 @@ void gw_handle::ooc_release()
     if (o.h_cached) cudaFreeHost(o.h_cached);
     if (o.h_dec) cudaFreeHost(o.h_dec);
     for (void *p : o.staged) cudaFreeHost(p);
+    for (auto &c : o.cblk)
+        if (c.host) cudaFreeHost(c.host);
+    cudaFree(o.d_cstage);
     for (float *p : {o.d_params, o.d_train_ws, o.d_trace_x, o.d_trace_col, o.d_trace_y, o.d_feat_x, o.d_feat_col,
                      o.d_pred, o.d_emass, o.d_vfrac, o.d_prev_col, o.d_ema})
         cudaFree(p);
@@ -176,10 +187,16 @@ static int learned_setup(gw_handle *h)
     return GW_OK;
 }
 
-void gw_handle::ooc_invalidate()
+void gw_handle::ooc_invalidate(bool blocks_changed)
 {
-    // host blocks changed: drop mappings so they are rebuilt on demand
+    // drop mappings so they are rebuilt on demand; compressed copies are
+    // derived from the host blocks and the slot count from their size, so a
+    // change of block data tears the out-of-core state down
     if (!ooc) return;
+    if (blocks_changed && ooc->compressed) {
+        ooc_release();
+        return;
+    }
     cudaSetDevice(cfg.device);
     for (void *p : ooc->staged) cudaFreeHost(p);
     ooc->staged.clear();
@@ -188,6 +205,9 @@ void gw_handle::ooc_invalidate()
 
 static int ooc_setup(gw_handle *h)
 {
+    // a mode change of the block copies rebuilds the state; so does a set-up
+    // that failed half-way
+    if (h->ooc && (!h->ooc->ready || h->ooc->compressed != (h->cfg.compress_blocks != 0))) h->ooc_release();
     if (h->ooc && h->ooc->ready) return GW_OK;
     if (h->nblocks > kMaxBlocks) return h->fail(GW_ERR_ARG, "at most %u blocks (got %u)", kMaxBlocks, h->nblocks);
     if (!h->ooc) h->ooc = new OocState();
@@ -202,18 +222,39 @@ static int ooc_setup(gw_handle *h)
     // offsets plus neighbours (gpu/memory.hpp:65-107); equal-edge-mass blocks
     // differ several-fold in vertex count, so that layout strands about a
     // fifth of the budget, and here an absent block's offsets stay readable.
-    const uint64_t beg_bytes = ((uint64_t)h->nverts + 1) * 8;
+    uint64_t beg_bytes = ((uint64_t)h->nverts + 1) * 8;
     o.slot_csr_words = (std::max<uint64_t>(maxe, 1) + 3) & ~3ull;  // keep slots 16-byte aligned
     const uint64_t slot_bytes = o.slot_csr_words * 4;
+    // Compressed blocks: encode every block once (host threads), and keep a
+    // device buffer of the largest compressed block inside the cache budget.
+    uint64_t cstage = 0;
+    o.compressed = h->cfg.compress_blocks != 0;
+    if (o.compressed) {
+        for (uint32_t b = 0; b < nb; ++b)
+            if (!h->host_beg[b] || (!h->host_csr[b] && h->eblocks[b + 1] > h->eblocks[b]))
+                return h->fail(GW_ERR_STATE, "block %u has no host data to compress", b);
+        const unsigned threads = std::max(1u, std::thread::hardware_concurrency());
+        o.cblk.assign(nb, CompressedBlock{});
+        for (uint32_t b = 0; b < nb; ++b) {
+            std::string why;
+            if (!compress_block(h->host_beg[b], h->host_csr[b], h->vblocks[b + 1] - h->vblocks[b], h->eblocks[b],
+                                h->eblocks[b + 1], threads, o.cblk[b], why))
+                return h->fail(GW_ERR_GRAPH, "block %u: %s", b, why.c_str());
+            cstage = std::max<uint64_t>(cstage, (o.cblk[b].bytes + 255) & ~255ull);
+        }
+        beg_bytes += cstage;
+    }
     uint64_t ns = h->cfg.cache_size > beg_bytes ? (h->cfg.cache_size - beg_bytes) / slot_bytes : 0;
     if (ns > nb) ns = nb;
     if (ns < 2)
         return h->fail(GW_ERR_ARG,
-                       "cache of %llu bytes holds the %llu bytes of vertex offsets and fewer than 2 blocks of %llu bytes",
+                       "cache of %llu bytes holds the %llu bytes of vertex offsets%s and fewer than 2 blocks of %llu bytes",
                        (unsigned long long)h->cfg.cache_size, (unsigned long long)beg_bytes,
-                       (unsigned long long)slot_bytes);
+                       o.compressed ? " and the compressed-block buffer" : "", (unsigned long long)slot_bytes);
     o.nslots = (uint32_t)ns;
     int st;
+    if (cstage && (st = h->cuda(cudaMalloc(&o.d_cstage, cstage), "compressed-block buffer"))) return st;
+    beg_bytes = ((uint64_t)h->nverts + 1) * 8;
     if ((st = h->cuda(cudaMalloc(&o.d_beg, beg_bytes), "vertex offsets"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.slot_csr, o.nslots * o.slot_csr_words * 4), "slot neighbours"))) return st;
     if ((st = h->cuda(cudaMalloc((void **)&o.d_blk_csr, nb * sizeof(void *)), "block table"))) return st;
@@ -333,6 +374,25 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                     "block table");
     };
     if ((st = push_tables())) return st;
+    // A block's neighbour list into slot memory `sc` on stream `cs`: a plain
+    // copy, or the compressed copy into the staging buffer and a decode.
+    auto copy_block = [&](uint32_t b, uint32_t *sc, cudaStream_t cs, uint64_t *bytes) -> int {
+        const uint64_t ne = eblocks[b + 1] - eblocks[b];
+        if (!o.compressed) {
+            *bytes = ne * 4;
+            if (!ne) return GW_OK;
+            return cuda(cudaMemcpyAsync(sc, host_csr[b], ne * 4, cudaMemcpyHostToDevice, cs), "block neighbours");
+        }
+        const CompressedBlock &cb = o.cblk[b];
+        *bytes = cb.bytes;
+        int e;
+        if ((e = cuda(cudaMemcpyAsync(o.d_cstage, cb.host, cb.bytes, cudaMemcpyHostToDevice, cs), "compressed block")))
+            return e;
+        launches++;
+        return cuda(launch_decode_block(o.d_cstage, cb.payload_off, cb.payload_bytes, vblocks[b + 1] - vblocks[b],
+                                        o.d_beg, vblocks[b], eblocks[b], ne, sc, d_err, num_sms, cs),
+                    "block decode");
+    };
     if ((st = cuda(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * kCtrCount, s), "memset"))) return st;
     if ((st = cuda(cudaMemsetAsync(d_err, 0, sizeof(uint32_t), s), "memset"))) return st;
     // every block's offsets into the resident offset array (neighbouring
@@ -648,13 +708,11 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             // stream; it overlaps this iteration's step (everything on the
             // compute stream has finished: the decision read-back synced it)
             const uint32_t b = (uint32_t)todo.front().first;
-            const uint64_t ne = eblocks[b + 1] - eblocks[b];
             uint32_t *sc = o.slot_csr + (uint64_t)staging_slot * o.slot_csr_words;
-            if (ne &&
-                (st = cuda(cudaMemcpyAsync(sc, host_csr[b], ne * 4, cudaMemcpyHostToDevice, s_copy), "block neighbours")))
-                break;
+            uint64_t bytes = 0;
+            if ((st = copy_block(b, sc, s_copy, &bytes))) break;
             if ((st = cuda(cudaEventRecord(staged_ev, s_copy), "event"))) break;
-            h2d += ne * 4;
+            h2d += bytes;
             loads++;
             staged_block = (int)b;
             staged_pos = todo.front().second;
@@ -685,10 +743,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             const uint32_t b = (uint32_t)load_block;
             const uint64_t ne = eblocks[b + 1] - eblocks[b];
             uint32_t *sc = o.slot_csr + (uint64_t)slot * o.slot_csr_words;
-            if (ne &&
-                (st = cuda(cudaMemcpyAsync(sc, host_csr[b], ne * 4, cudaMemcpyHostToDevice, s), "block neighbours")))
-                break;
-            h2d += ne * 4;
+            uint64_t bytes = 0;
+            if ((st = copy_block(b, sc, s, &bytes))) break;
+            h2d += bytes;
             loads++;
             k_validate_block<<<num_sms * 4, 256, 0, s>>>(sc, ne, nverts, d_err);
             launches++;

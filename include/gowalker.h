@@ -98,7 +98,10 @@ typedef struct gw_config {
     uint32_t prefetch;        /* out-of-core: 1 = take each block choice one iteration ahead and
                                  copy the block on the copy stream while the step kernel runs
                                  (one cache slot stages the copy) */
-    uint32_t reserved[6];
+    uint32_t compress_blocks; /* out-of-core: 1 = keep a compressed copy of every block's neighbour
+                                 lists in pinned host memory (chunks of 32 ids, bit-packed deltas),
+                                 copy that and decode it on the device: fewer host-link bytes */
+    uint32_t reserved[5];
 } gw_config;
 
 /* Per-run counters. */

@@ -171,3 +171,71 @@ def test_prefetch_same_walks(gw, oracle, algo, policy):
     assert st["steps"] == ref["stats"]["steps"] and st["trials"] == ref["stats"]["trials"]
     assert st["block_loads"] > 0 and int(eng.bucket_counts().sum()) == 0
     eng.close()
+
+
+@pytest.mark.parametrize("algo,prefetch", [(0, 0), (0, 1), (1, 0), (2, 1)])
+def test_compressed_blocks_same_walks(gw, oracle, algo, prefetch):
+    """Blocks copied as compressed neighbour lists and decoded on the device:
+    the walks are the oracle's and fewer bytes cross the host link."""
+    beg, csr = graph(oracle, scale=13, ef=12, sym=algo != 0, cap=7000, seed=3)
+    V = len(beg) - 1
+    from gowalker_b200.preprocess import split_equal_edge_mass
+    vb, eb = split_equal_edge_mass(beg, 12)
+    term = 0.15 if algo else 0.0
+    out = {}
+    for comp in (0, 1):
+        eng = gw.WalkEngine(algorithm=algo, maxhops=25, p=0.5, q=2.0, alpha=0.2, term_prob=term, seed=11,
+                            walkpersource=1, record_paths=1, cache_size=cache_for(beg, eb, 6),
+                            prefetch=prefetch, compress_blocks=comp)
+        eng.set_host_graph(beg, csr, vb, eb)
+        eng.init_walkers(algo, 1, 11)
+        st = eng.run()
+        P, L = eng.paths()
+        out[comp] = (P, L, st)
+        assert st["block_loads"] > 0 and int(eng.bucket_counts().sum()) == 0
+        eng.close()
+    ref = oracle.walk(beg, csr, oracle.make_cfg(algo=algo, maxhops=25, p=0.5, q=2.0, alpha=0.2, term_prob=term,
+                                                seed=11), 0, V, paths=True)
+    for comp in (0, 1):
+        P, L, st = out[comp]
+        assert np.array_equal(P, ref["paths"]) and np.array_equal(L, ref["lens"])
+        assert st["steps"] == ref["stats"]["steps"] and st["trials"] == ref["stats"]["trials"]
+    per_load = [out[c][2]["h2d_bytes"] / max(out[c][2]["block_loads"], 1) for c in (0, 1)]
+    assert per_load[1] < 0.8 * per_load[0]
+
+
+def test_compressed_blocks_unsorted_duplicates(gw, oracle):
+    """Exact round trip whatever the neighbour order: every adjacency list
+    shuffled (negative deltas) with duplicate edges (zero deltas); compressed
+    and plain block copies give bit-identical walks."""
+    beg, csr = graph(oracle, scale=13, ef=12, sym=False, cap=7000, seed=5)
+    rng = np.random.default_rng(3)
+    V = len(beg) - 1
+    deg = np.diff(beg.astype(np.int64))
+    lists = []
+    for v in range(V):
+        a = csr[int(beg[v]):int(beg[v + 1])].copy()
+        if len(a) and v % 3 == 0:
+            a = np.concatenate([a, a[: 1 + len(a) // 4]])  # duplicates
+        rng.shuffle(a)
+        lists.append(a)
+    deg = np.array([len(a) for a in lists])
+    beg2 = np.zeros(V + 1, dtype=np.uint64)
+    beg2[1:] = np.cumsum(deg)
+    csr2 = np.concatenate(lists).astype(np.uint32)
+    assert (deg > 32).sum() > 10 and (deg == 0).sum() > 0
+    from gowalker_b200.preprocess import split_equal_edge_mass
+    vb, eb = split_equal_edge_mass(beg2, 10)
+    hs = {}
+    for comp in (0, 1):
+        eng = gw.WalkEngine(algorithm=0, maxhops=30, p=0.5, q=2.0, seed=21, walkpersource=2, record_paths=1,
+                            cache_size=cache_for(beg2, eb, 5), compress_blocks=comp)
+        eng.set_host_graph(beg2, csr2, vb, eb)
+        eng.init_walkers(0, 2, 21)
+        st = eng.run()
+        P, L = eng.paths()
+        assert st["block_loads"] > 0
+        hs[comp] = (P, L, eng.hashes(), st["steps"], st["trials"])
+        eng.close()
+    for a, b in zip(hs[0], hs[1]):
+        assert np.array_equal(np.asarray(a), np.asarray(b))
