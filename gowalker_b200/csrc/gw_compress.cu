@@ -21,15 +21,21 @@ static inline uint32_t chunk_width(const uint32_t *ids, uint32_t k)
     return bit_length(m);
 }
 
-static uint64_t vertex_bytes(const uint32_t *ids, uint64_t d)
+// Bytes of a vertex's chunks; with `group` non-null, also the byte offset
+// (from the vertex's first chunk) of every 32nd chunk.
+static uint64_t vertex_bytes(const uint32_t *ids, uint64_t d, uint64_t *group)
 {
-    uint64_t s = 0;
-    for (uint64_t j = 0; j < d; j += kChunkIds) {
+    uint64_t s = 0, c = 0;
+    for (uint64_t j = 0; j < d; j += kChunkIds, ++c) {
+        if (group && c % kChunkIds == 0) group[c / kChunkIds] = s;
         const uint32_t k = (uint32_t)std::min<uint64_t>(kChunkIds, d - j);
         s += 5 + ((uint64_t)(k - 1) * chunk_width(ids + j, k) + 7) / 8;
     }
     return s;
 }
+
+static inline uint64_t nchunks(uint64_t d) { return (d + kChunkIds - 1) / kChunkIds; }
+static inline uint64_t ngroups(uint64_t d) { return nchunks(d) > kChunkIds ? (nchunks(d) + kChunkIds - 1) / kChunkIds : 0; }
 
 static void encode_vertex(const uint32_t *ids, uint64_t d, uint8_t *p)
 {
@@ -75,22 +81,30 @@ bool compress_block(const uint64_t *beg, const uint32_t *csr, uint32_t nv, uint6
         cut[t] = (uint32_t)(std::lower_bound(beg, beg + nv, target) - beg);
         cut[t] = std::max(cut[t], cut[t - 1]);
     }
-    std::vector<uint64_t> off(nv + 1, 0);
+    std::vector<uint64_t> off(nv + 1, 0), gstart(nv + 1, 0);
+    for (uint32_t v = 0; v < nv; ++v) gstart[v + 1] = gstart[v] + ngroups(beg[v + 1] - beg[v]);
+    const uint64_t nsplit = gstart[nv];
+    std::vector<uint64_t> gofs(nsplit);  // byte offset of each group, from its vertex's first chunk
     auto run = [&](auto &&fn) {
         std::vector<std::thread> pool;
         for (unsigned t = 0; t < threads; ++t) pool.emplace_back(fn, cut[t], cut[t + 1]);
         for (auto &th : pool) th.join();
     };
     run([&](uint32_t a, uint32_t b) {
-        for (uint32_t v = a; v < b; ++v) off[v + 1] = vertex_bytes(csr + (beg[v] - e0), beg[v + 1] - beg[v]);
+        for (uint32_t v = a; v < b; ++v) {
+            const uint64_t d = beg[v + 1] - beg[v];
+            off[v + 1] = vertex_bytes(csr + (beg[v] - e0), d, ngroups(d) ? gofs.data() + gstart[v] : nullptr);
+        }
     });
     for (uint32_t v = 0; v < nv; ++v) off[v + 1] += off[v];
     const uint64_t payload = off[nv];
-    if (payload >= (1ull << 32)) {
+    if (payload >= (1ull << 32) || nsplit >= (1ull << 30)) {
         why = "block too large to compress (payload of 4 GB or more)";
         return false;
     }
-    out.payload_off = ((uint64_t)(nv + 1) * 4 + 15) & ~15ull;
+    out.split_off = ((uint64_t)(nv + 1) * 4 + 15) & ~15ull;
+    out.nsplit = (uint32_t)nsplit;
+    out.payload_off = (out.split_off + nsplit * 12 + 15) & ~15ull;
     out.payload_bytes = payload;
     out.bytes = (out.payload_off + payload + 8 + 15) & ~15ull;
     if (cudaHostAlloc((void **)&out.host, out.bytes, cudaHostAllocDefault) != cudaSuccess) {
@@ -103,6 +117,13 @@ bool compress_block(const uint64_t *beg, const uint32_t *csr, uint32_t nv, uint6
     memset(out.host + out.payload_off + payload, 0, out.bytes - out.payload_off - payload);
     uint32_t *voff = (uint32_t *)out.host;
     for (uint32_t v = 0; v <= nv; ++v) voff[v] = (uint32_t)off[v];
+    uint32_t *split = (uint32_t *)(out.host + out.split_off);
+    for (uint32_t v = 0; v < nv; ++v)
+        for (uint64_t g = gstart[v]; g < gstart[v + 1]; ++g) {
+            split[3 * g] = v;
+            split[3 * g + 1] = (uint32_t)((g - gstart[v]) * kChunkIds);
+            split[3 * g + 2] = (uint32_t)(off[v] + gofs[g]);
+        }
     uint8_t *pay = out.host + out.payload_off;
     run([&](uint32_t a, uint32_t b) {
         for (uint32_t v = a; v < b; ++v) encode_vertex(csr + (beg[v] - e0), beg[v + 1] - beg[v], pay + off[v]);
@@ -110,29 +131,53 @@ bool compress_block(const uint64_t *beg, const uint32_t *csr, uint32_t nv, uint6
     return true;
 }
 
-// One warp per vertex: lane i of a chunk extracts delta i (lane 0 the first
-// id), a warp prefix sum (mod 2^32) rebuilds the ids.
-__global__ void k_decode_block(const uint8_t *__restrict__ src, uint64_t payload_off, uint64_t payload_bytes,
-                               uint32_t nv, const uint64_t *__restrict__ beg, uint32_t v0, uint64_t e0, uint64_t ne,
+// Warp tasks: task t < nv decodes vertex t if it has at most 32 chunks;
+// task nv + g decodes split group g (32 chunks of a larger vertex).  Within a
+// chunk, lane i extracts delta i (lane 0 the first id) and a warp prefix sum
+// (mod 2^32) rebuilds the ids.
+__global__ void k_decode_block(const uint8_t *__restrict__ src, uint64_t split_off, uint32_t nsplit,
+                               uint64_t payload_off, uint64_t payload_bytes, uint32_t nv,
+                               const uint64_t *__restrict__ beg, uint32_t v0, uint64_t e0, uint64_t ne,
                                uint32_t *__restrict__ out, uint32_t *err)
 {
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const uint32_t *voff = reinterpret_cast<const uint32_t *>(src);
+    const uint32_t *split = reinterpret_cast<const uint32_t *>(src + split_off);
     const uint8_t *pay = src + payload_off;
-    for (uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < nv; v += nwarps) {
+    const uint64_t ntasks = (uint64_t)nv + nsplit;
+    for (uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntasks; t += nwarps) {
+        uint32_t v, c0;
+        uint64_t pos;
+        if (t < nv) {
+            v = (uint32_t)t;
+            c0 = 0;
+            pos = __ldg(voff + v);
+        } else {
+            const uint64_t g = t - nv;
+            v = __ldg(split + 3 * g);
+            c0 = __ldg(split + 3 * g + 1);
+            pos = __ldg(split + 3 * g + 2);
+            if (v >= nv) {
+                if (lane == 0) atomicOr(err, kErrBlock);
+                continue;
+            }
+        }
         const uint64_t b0 = __ldg(beg + v0 + v), b1 = __ldg(beg + v0 + v + 1);
         bool bad = b1 < b0 || b0 < e0 || b1 - e0 > ne;
         const uint64_t d = bad ? 0 : b1 - b0;
-        uint64_t pos = __ldg(voff + v);
-        for (uint64_t j = 0; j < d; j += kChunkIds) {
+        const uint64_t nch = (d + kChunkIds - 1) / kChunkIds;
+        if (t < nv && nch > kChunkIds) continue;  // decoded by its split groups
+        const uint64_t c1 = min(nch, (uint64_t)c0 + kChunkIds);
+        for (uint64_t c = c0; c < c1; ++c) {
+            const uint64_t j = c * kChunkIds;
             const uint32_t k = (uint32_t)min((uint64_t)kChunkIds, d - j);
             if (pos + 5 > payload_bytes) {
                 bad = true;
                 break;
             }
-            const uint8_t *c = pay + pos;
-            const uint32_t w = c[0];
+            const uint8_t *ch = pay + pos;
+            const uint32_t w = ch[0];
             const uint64_t packed = ((uint64_t)(k - 1) * w + 7) >> 3;
             if (w > 32 || pos + 5 + packed > payload_bytes) {
                 bad = true;
@@ -140,10 +185,10 @@ __global__ void k_decode_block(const uint8_t *__restrict__ src, uint64_t payload
             }
             uint32_t x = 0;
             if (lane == 0) {
-                x = (uint32_t)c[1] | ((uint32_t)c[2] << 8) | ((uint32_t)c[3] << 16) | ((uint32_t)c[4] << 24);
+                x = (uint32_t)ch[1] | ((uint32_t)ch[2] << 8) | ((uint32_t)ch[3] << 16) | ((uint32_t)ch[4] << 24);
             } else if (lane < k && w != 0) {
                 const uint32_t bp = (lane - 1) * w;
-                const uint8_t *q = c + 5 + (bp >> 3);  // up to 4 bytes past the field: the buffer is padded
+                const uint8_t *q = ch + 5 + (bp >> 3);  // up to 4 bytes past the field: the buffer is padded
                 const uint64_t acc = (uint64_t)q[0] | ((uint64_t)q[1] << 8) | ((uint64_t)q[2] << 16) |
                                      ((uint64_t)q[3] << 24) | ((uint64_t)q[4] << 32);
                 const uint64_t mask = (w == 32) ? 0xFFFFFFFFull : ((1ull << w) - 1);
@@ -162,12 +207,13 @@ __global__ void k_decode_block(const uint8_t *__restrict__ src, uint64_t payload
     }
 }
 
-cudaError_t launch_decode_block(const uint8_t *src, uint64_t payload_off, uint64_t payload_bytes, uint32_t nv,
-                                const uint64_t *beg, uint32_t v0, uint64_t e0, uint64_t ne, uint32_t *out,
-                                uint32_t *err, int num_sms, cudaStream_t s)
+cudaError_t launch_decode_block(const uint8_t *src, const CompressedBlock &cb, uint32_t nv, const uint64_t *beg,
+                                uint32_t v0, uint64_t e0, uint64_t ne, uint32_t *out, uint32_t *err, int num_sms,
+                                cudaStream_t s)
 {
     if (nv == 0) return cudaSuccess;
-    k_decode_block<<<num_sms * 8, 256, 0, s>>>(src, payload_off, payload_bytes, nv, beg, v0, e0, ne, out, err);
+    k_decode_block<<<num_sms * 8, 256, 0, s>>>(src, cb.split_off, cb.nsplit, cb.payload_off, cb.payload_bytes, nv, beg,
+                                               v0, e0, ne, out, err);
     return cudaGetLastError();
 }
 

@@ -6,6 +6,11 @@
 //
 //   u32 voff[nv + 1]      byte offset of each vertex's chunks in the payload
 //   (pad to 16 bytes)
+//   u32 split[3 * nsplit] for every vertex with more than 32 chunks, one
+//                         entry (vertex, first chunk, byte offset) per group
+//                         of 32 chunks, so no decoder task walks more than
+//                         32 chunks in sequence (hub vertices have 10^5+)
+//   (pad to 16 bytes)
 //   payload               per vertex, ceil(deg / 32) chunks of up to 32 ids:
 //                           u8  w       bit width of the chunk's deltas
 //                           u32 first   first id (little endian, unaligned)
@@ -29,6 +34,8 @@ constexpr uint32_t kChunkIds = 32;
 struct CompressedBlock {
     uint8_t *host = nullptr;   // pinned (cudaHostAlloc), owned by the handle
     uint64_t bytes = 0;        // whole buffer: offsets, payload, padding
+    uint64_t split_off = 0;    // start of the split entries in the buffer
+    uint32_t nsplit = 0;
     uint64_t payload_off = 0;  // start of the payload in the buffer
     uint64_t payload_bytes = 0;
 };
@@ -44,8 +51,8 @@ bool compress_block(const uint64_t *beg, const uint32_t *csr, uint32_t nv, uint6
 // (neighbour slot, indexed from e0).  beg: resident offsets of every vertex,
 // v0: the block's first vertex.  Any offset or payload read outside the
 // buffer sets kErrBlock in *err and skips the vertex.
-cudaError_t launch_decode_block(const uint8_t *src, uint64_t payload_off, uint64_t payload_bytes, uint32_t nv,
-                                const uint64_t *beg, uint32_t v0, uint64_t e0, uint64_t ne, uint32_t *out,
-                                uint32_t *err, int num_sms, cudaStream_t s);
+cudaError_t launch_decode_block(const uint8_t *src, const CompressedBlock &cb, uint32_t nv, const uint64_t *beg,
+                                uint32_t v0, uint64_t e0, uint64_t ne, uint32_t *out, uint32_t *err, int num_sms,
+                                cudaStream_t s);
 
 }  // namespace gw

@@ -35,8 +35,15 @@ struct OocState {
     std::vector<int> block_slot;   // slot of each block, -1 = absent
     std::vector<uint32_t> cached;  // the scheduler's cached list (GOwalker_scheduler_t::buckets)
 
-    const uint32_t **h_blk_csr = nullptr;  // pinned mirror of the block table (null = absent)
-    const uint32_t **d_blk_csr = nullptr;
+    const uint32_t **h_blk_csr = nullptr;  // host block table (null = absent)
+    const uint32_t **d_blk_csr = nullptr;  // the table the step kernels read
+    // pinned copies of the table, alternating per push (a push may still be
+    // in flight when the host edits the table for the next iteration), and
+    // the table as the decision stream reads it
+    const uint32_t **h_blk_pin[2] = {nullptr, nullptr};
+    const uint32_t **d_blk_csr2 = nullptr;
+    uint32_t pin_next = 0;
+    unsigned long long *d_snap = nullptr;  // counters and error word after the last re-bucketing
     uint32_t *d_vstart = nullptr;
     uint64_t *d_estart = nullptr;
     uint32_t *h_cached = nullptr;  // pinned
@@ -59,7 +66,8 @@ struct OocState {
     // every block, and the device buffer a load lands in before decoding
     bool compressed = false;
     std::vector<CompressedBlock> cblk;
-    uint8_t *d_cstage = nullptr;
+    uint8_t *d_cstage[2] = {nullptr, nullptr};  // prefetch uploads alternate: one may wait for its decode
+    uint32_t nstage = 0;
 
     bool ready = false;
 
@@ -138,7 +146,12 @@ void gw_handle::ooc_release()
     for (void *p : o.staged) cudaFreeHost(p);
     for (auto &c : o.cblk)
         if (c.host) cudaFreeHost(c.host);
-    cudaFree(o.d_cstage);
+    cudaFree(o.d_cstage[0]);
+    cudaFree(o.d_cstage[1]);
+    cudaFree((void *)o.d_blk_csr2);
+    cudaFree(o.d_snap);
+    for (auto *p : o.h_blk_pin)
+        if (p) cudaFreeHost((void *)p);
     for (float *p : {o.d_params, o.d_train_ws, o.d_trace_x, o.d_trace_col, o.d_trace_y, o.d_feat_x, o.d_feat_col,
                      o.d_pred, o.d_emass, o.d_vfrac, o.d_prev_col, o.d_ema})
         cudaFree(p);
@@ -207,7 +220,9 @@ static int ooc_setup(gw_handle *h)
 {
     // a mode change of the block copies rebuilds the state; so does a set-up
     // that failed half-way
-    if (h->ooc && (!h->ooc->ready || h->ooc->compressed != (h->cfg.compress_blocks != 0))) h->ooc_release();
+    if (h->ooc && (!h->ooc->ready || h->ooc->compressed != (h->cfg.compress_blocks != 0) ||
+                   (h->ooc->compressed && h->ooc->nstage != (h->cfg.prefetch ? 2u : 1u))))
+        h->ooc_release();
     if (h->ooc && h->ooc->ready) return GW_OK;
     if (h->nblocks > kMaxBlocks) return h->fail(GW_ERR_ARG, "at most %u blocks (got %u)", kMaxBlocks, h->nblocks);
     if (!h->ooc) h->ooc = new OocState();
@@ -242,7 +257,8 @@ static int ooc_setup(gw_handle *h)
                 return h->fail(GW_ERR_GRAPH, "block %u: %s", b, why.c_str());
             cstage = std::max<uint64_t>(cstage, (o.cblk[b].bytes + 255) & ~255ull);
         }
-        beg_bytes += cstage;
+        o.nstage = h->cfg.prefetch ? 2u : 1u;
+        beg_bytes += cstage * o.nstage;
     }
     uint64_t ns = h->cfg.cache_size > beg_bytes ? (h->cfg.cache_size - beg_bytes) / slot_bytes : 0;
     if (ns > nb) ns = nb;
@@ -253,12 +269,18 @@ static int ooc_setup(gw_handle *h)
                        o.compressed ? " and the compressed-block buffer" : "", (unsigned long long)slot_bytes);
     o.nslots = (uint32_t)ns;
     int st;
-    if (cstage && (st = h->cuda(cudaMalloc(&o.d_cstage, cstage), "compressed-block buffer"))) return st;
+    for (uint32_t i = 0; cstage && i < o.nstage; ++i)
+        if ((st = h->cuda(cudaMalloc(&o.d_cstage[i], cstage), "compressed-block buffer"))) return st;
     beg_bytes = ((uint64_t)h->nverts + 1) * 8;
     if ((st = h->cuda(cudaMalloc(&o.d_beg, beg_bytes), "vertex offsets"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.slot_csr, o.nslots * o.slot_csr_words * 4), "slot neighbours"))) return st;
     if ((st = h->cuda(cudaMalloc((void **)&o.d_blk_csr, nb * sizeof(void *)), "block table"))) return st;
     if ((st = h->cuda(cudaMallocHost((void **)&o.h_blk_csr, nb * sizeof(void *)), "block table"))) return st;
+    for (auto &p : o.h_blk_pin)
+        if ((st = h->cuda(cudaMallocHost((void **)&p, nb * sizeof(void *)), "block table"))) return st;
+    if ((st = h->cuda(cudaMalloc((void **)&o.d_blk_csr2, nb * sizeof(void *)), "block table"))) return st;
+    if ((st = h->cuda(cudaMalloc(&o.d_snap, sizeof(unsigned long long) * (kCtrCount + 1)), "counter snapshot")))
+        return st;
     if ((st = h->cuda(cudaMalloc(&o.d_vstart, (nb + 1) * sizeof(uint32_t)), "vstart"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_estart, (nb + 1) * sizeof(uint64_t)), "estart"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_cached, nb * sizeof(uint32_t)), "cached list"))) return st;
@@ -369,14 +391,23 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     std::fill(o.block_slot.begin(), o.block_slot.end(), -1);
     o.cached.clear();
     for (uint32_t b = 0; b < nb; ++b) o.h_blk_csr[b] = nullptr;
+    const uint32_t **pin_last = o.h_blk_pin[0];
     auto push_tables = [&]() -> int {
-        return cuda(cudaMemcpyAsync((void *)o.d_blk_csr, o.h_blk_csr, nb * sizeof(void *), cudaMemcpyHostToDevice, s),
+        pin_last = o.h_blk_pin[o.pin_next];
+        o.pin_next ^= 1u;
+        memcpy((void *)pin_last, o.h_blk_csr, nb * sizeof(void *));
+        return cuda(cudaMemcpyAsync((void *)o.d_blk_csr, pin_last, nb * sizeof(void *), cudaMemcpyHostToDevice, s),
                     "block table");
     };
     if ((st = push_tables())) return st;
-    // A block's neighbour list into slot memory `sc` on stream `cs`: a plain
-    // copy, or the compressed copy into the staging buffer and a decode.
-    auto copy_block = [&](uint32_t b, uint32_t *sc, cudaStream_t cs, uint64_t *bytes) -> int {
+    // A block's neighbour list towards slot memory `sc` on stream `cs`: a
+    // plain copy into the slot, or the compressed copy into the staging
+    // buffer `stage`; decode_block then expands a compressed one into the
+    // slot.  A prefetched block is uploaded on the copy stream and decoded on
+    // the compute stream when it is installed; the two staging buffers
+    // alternate, and an upload is issued only after the decision that waited
+    // for the re-bucketing following the decode that last read its buffer.
+    auto upload_block = [&](uint32_t b, uint32_t *sc, cudaStream_t cs, uint32_t stage, uint64_t *bytes) -> int {
         const uint64_t ne = eblocks[b + 1] - eblocks[b];
         if (!o.compressed) {
             *bytes = ne * 4;
@@ -385,12 +416,13 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         }
         const CompressedBlock &cb = o.cblk[b];
         *bytes = cb.bytes;
-        int e;
-        if ((e = cuda(cudaMemcpyAsync(o.d_cstage, cb.host, cb.bytes, cudaMemcpyHostToDevice, cs), "compressed block")))
-            return e;
+        return cuda(cudaMemcpyAsync(o.d_cstage[stage], cb.host, cb.bytes, cudaMemcpyHostToDevice, cs), "compressed block");
+    };
+    auto decode_block = [&](uint32_t b, uint32_t *sc, cudaStream_t cs, uint32_t stage) -> int {
+        if (!o.compressed) return GW_OK;
         launches++;
-        return cuda(launch_decode_block(o.d_cstage, cb.payload_off, cb.payload_bytes, vblocks[b + 1] - vblocks[b],
-                                        o.d_beg, vblocks[b], eblocks[b], ne, sc, d_err, num_sms, cs),
+        return cuda(launch_decode_block(o.d_cstage[stage], o.cblk[b], vblocks[b + 1] - vblocks[b], o.d_beg, vblocks[b],
+                                        eblocks[b], eblocks[b + 1] - eblocks[b], sc, d_err, num_sms, cs),
                     "block decode");
     };
     if ((st = cuda(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * kCtrCount, s), "memset"))) return st;
@@ -422,6 +454,8 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         return st;
     launches++;
     uint64_t nlive = nwalkers;  // records in w_a (unsorted)
+    cudaEvent_t ev_buck = nullptr;  // the last re-bucketing (and counter snapshot) is done
+    if ((st = cuda(cudaEventCreateWithFlags(&ev_buck, cudaEventDisableTiming), "event"))) return st;
 
     auto bucketize = [&](uint64_t n) -> int {
         int e;
@@ -433,7 +467,13 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if ((e = cuda(launch_combine(o.d_counts, nb, o.d_pairs, num_sms, s), "pair counts"))) return e;
         launches += 4;
         std::swap(o.w_a, o.w_b);  // w_a: bucket-sorted live walkers
-        return GW_OK;
+        // what the next decision reads: counters and error word as of now
+        if ((e = cuda(cudaMemcpyAsync(o.d_snap, d_ctr, sizeof(unsigned long long) * kCtrCount, cudaMemcpyDeviceToDevice,
+                                      s), "counter snapshot")) ||
+            (e = cuda(cudaMemcpyAsync(o.d_snap + kCtrCount, d_err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s),
+                      "error snapshot")))
+            return e;
+        return cuda(cudaEventRecord(ev_buck, s), "event");
     };
     if ((st = bucketize(nlive))) return st;
 
@@ -519,6 +559,12 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     }
     cudaEvent_t staged_ev = nullptr;
     if (prefetch) cudaEventCreateWithFlags(&staged_ev, cudaEventDisableTiming);
+    // Decisions run on their own stream when prefetching: they read the
+    // counts of the last re-bucketing (ev_buck) and never wait for a copy,
+    // so the next block's upload queues right behind the one in flight.
+    cudaStream_t ds = s;
+    if (prefetch) cudaStreamCreateWithFlags(&ds, cudaStreamNonBlocking);
+    uint32_t upload_stage = 0, staged_stage = 0;
     while (!done) {
         if (++iters > kMaxIters) {
             st = fail(GW_ERR_STATE, "out-of-core run exceeded %u scheduler iterations", kMaxIters);
@@ -540,6 +586,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             }
             const uint32_t b = (uint32_t)staged_block;
             uint32_t *sc = o.slot_csr + (uint64_t)staging_slot * o.slot_csr_words;
+            // a compressed block is expanded here, on the compute stream, so
+            // the next block's copy overlaps this decode as well as the step
+            if ((st = decode_block(b, sc, s, staged_stage))) break;
             k_validate_block<<<num_sms * 4, 256, 0, s>>>(sc, eblocks[b + 1] - eblocks[b], nverts, d_err);
             launches++;
             o.slot_block[staging_slot] = (int)b;
@@ -557,9 +606,13 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         }
         const uint32_t ncached = (uint32_t)o.cached.size();
         for (uint32_t j = 0; j < ncached; ++j) o.h_cached[j] = o.cached[j];
+        if ((st = cuda(cudaStreamWaitEvent(ds, ev_buck, 0), "decision wait"))) break;
         if (ncached &&
-            (st = cuda(cudaMemcpyAsync(o.d_cached, o.h_cached, ncached * sizeof(uint32_t), cudaMemcpyHostToDevice, s),
+            (st = cuda(cudaMemcpyAsync(o.d_cached, o.h_cached, ncached * sizeof(uint32_t), cudaMemcpyHostToDevice, ds),
                        "cached list")))
+            break;
+        if ((st = cuda(cudaMemcpyAsync((void *)o.d_blk_csr2, pin_last, nb * sizeof(void *), cudaMemcpyHostToDevice, ds),
+                       "block table")))
             break;
         // ---- learned policy: features (traces while training), prediction, choice
         const bool learned = policy == GW_POLICY_LEARNED;
@@ -568,7 +621,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if (learned_active || tracing) {
             FeatureArgs f{};
             f.counts = o.d_pairs;
-            f.blk_csr = o.d_blk_csr;
+            f.blk_csr = o.d_blk_csr2;
             f.emass = o.d_emass;
             f.vfrac = o.d_vfrac;
             f.prev_col = o.d_prev_col;
@@ -579,41 +632,38 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             f.inv_live = nlive ? 1.f / (float)nlive : 0.f;
             f.x = tracing ? o.d_trace_x + (uint64_t)std::min(trace_t, kTraceIters - 1) * nb * kMlpIn : o.d_feat_x;
             f.col = tracing ? o.d_trace_col + (uint64_t)trace_t * nb : o.d_feat_col;
-            if ((st = cuda(launch_features(f, s), "features"))) break;
+            if ((st = cuda(launch_features(f, ds), "features"))) break;
             launches++;
             if (learned_active) {
-                if ((st = cuda(mlp_forward(o.d_params, o.d_feat_x, nb, o.d_pred, s), "predictor"))) break;
-                if ((st = cuda(launch_learned_choose(o.d_pred, nb, o.d_blk_csr, o.d_cached, ncached, capacity,
-                                                     prefetch ? 1u : kMaxLoadsPerIter, kSwapMargin, o.d_choose, s),
+                if ((st = cuda(mlp_forward(o.d_params, o.d_feat_x, nb, o.d_pred, ds), "predictor"))) break;
+                if ((st = cuda(launch_learned_choose(o.d_pred, nb, o.d_blk_csr2, o.d_cached, ncached, capacity,
+                                                     prefetch ? 1u : kMaxLoadsPerIter, kSwapMargin, o.d_choose, ds),
                                "learned choice")))
                     break;
                 launches += 2;
                 if ((st = cuda(cudaMemcpyAsync(o.h_choose, o.d_choose, sizeof(int32_t) * (2 * kMaxLoadsPerIter + 1),
-                                               cudaMemcpyDeviceToHost, s), "choice")))
+                                               cudaMemcpyDeviceToHost, ds), "choice")))
                     break;
-                if ((st = cuda(cudaMemcpyAsync(o.h_pred, o.d_pred, sizeof(float) * nb, cudaMemcpyDeviceToHost, s),
+                if ((st = cuda(cudaMemcpyAsync(o.h_pred, o.d_pred, sizeof(float) * nb, cudaMemcpyDeviceToHost, ds),
                                "predictions")))
                     break;
-                if ((st = cuda(cudaMemcpyAsync(o.h_col, o.d_feat_col, sizeof(float) * nb, cudaMemcpyDeviceToHost, s),
+                if ((st = cuda(cudaMemcpyAsync(o.h_col, o.d_feat_col, sizeof(float) * nb, cudaMemcpyDeviceToHost, ds),
                                "demand")))
                     break;
             }
         }
         // ---- plain block choice on the device (decision, fallback and rescue), read back
         if ((st = cuda(launch_schedule(o.d_pairs, o.d_offsets + nbk, nb, o.d_cached, ncached, capacity, cfg.zero_threshold,
-                                       nullptr, 0.f, o.d_dec, s),
+                                       nullptr, 0.f, o.d_dec, ds),
                        "schedule")))
             break;
         launches++;
-        if ((st = cuda(cudaMemcpyAsync(o.h_dec, o.d_dec, sizeof(Decision), cudaMemcpyDeviceToHost, s), "decision")))
+        if ((st = cuda(cudaMemcpyAsync(o.h_dec, o.d_dec, sizeof(Decision), cudaMemcpyDeviceToHost, ds), "decision")))
             break;
-        if ((st = cuda(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(unsigned long long) * kCtrCount, cudaMemcpyDeviceToHost, s),
-                       "counters")))
+        if ((st = cuda(cudaMemcpyAsync(h_ctr, o.d_snap, sizeof(unsigned long long) * (kCtrCount + 1),
+                                       cudaMemcpyDeviceToHost, ds), "counters")))
             break;
-        if ((st = cuda(cudaMemcpyAsync(h_ctr + kCtrCount, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
-                       "error word")))
-            break;
-        if ((st = cuda(cudaStreamSynchronize(s), "schedule sync"))) break;
+        if ((st = cuda(cudaStreamSynchronize(ds), "schedule sync"))) break;
         if (iters > 1) {
             float ms = 0.f;
             if (cudaEventElapsedTime(&ms, k0, k1) == cudaSuccess) kernel_ms += ms;
@@ -710,7 +760,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             const uint32_t b = (uint32_t)todo.front().first;
             uint32_t *sc = o.slot_csr + (uint64_t)staging_slot * o.slot_csr_words;
             uint64_t bytes = 0;
-            if ((st = copy_block(b, sc, s_copy, &bytes))) break;
+            upload_stage ^= o.nstage == 2 ? 1u : 0u;
+            staged_stage = upload_stage;
+            if ((st = upload_block(b, sc, s_copy, upload_stage, &bytes))) break;
             if ((st = cuda(cudaEventRecord(staged_ev, s_copy), "event"))) break;
             h2d += bytes;
             loads++;
@@ -744,7 +796,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             const uint64_t ne = eblocks[b + 1] - eblocks[b];
             uint32_t *sc = o.slot_csr + (uint64_t)slot * o.slot_csr_words;
             uint64_t bytes = 0;
-            if ((st = copy_block(b, sc, s, &bytes))) break;
+            if ((st = upload_block(b, sc, s, 0, &bytes)) || (st = decode_block(b, sc, s, 0))) break;
             h2d += bytes;
             loads++;
             k_validate_block<<<num_sms * 4, 256, 0, s>>>(sc, ne, nverts, d_err);
@@ -764,14 +816,15 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if (tracing) {
             trace_t++;
             if (trace_t == kTraceIters + kHorizon) {
-                if ((st = cuda(launch_targets(o.d_trace_col, kTraceIters, kHorizon, nb, o.d_trace_y, s), "targets")))
+                if ((st = cuda(cudaStreamWaitEvent(ds, ev_buck, 0), "training wait"))) break;
+                if ((st = cuda(launch_targets(o.d_trace_col, kTraceIters, kHorizon, nb, o.d_trace_y, ds), "targets")))
                     break;
                 if ((st = cuda(mlp_train(o.d_params, o.d_trace_x, o.d_trace_y, kTraceIters * nb, kTrainEpochs,
-                                         kTrainLr, 0x6C6561726E6564ull, o.d_train_ws, nullptr, s),
+                                         kTrainLr, 0x6C6561726E6564ull, o.d_train_ws, nullptr, ds),
                                "predictor training")))
                     break;
                 const float *loss_dev = o.d_train_ws + (uint64_t)kMlpGradCtas * (kMlpParams + 1) + 3 * kMlpParams;
-                if ((st = cuda(cudaMemcpyAsync(&o.train_loss, loss_dev, sizeof(float), cudaMemcpyDeviceToHost, s),
+                if ((st = cuda(cudaMemcpyAsync(&o.train_loss, loss_dev, sizeof(float), cudaMemcpyDeviceToHost, ds),
                                "loss")))
                     break;
                 launches += 2 + 3 * kTrainEpochs;
@@ -793,6 +846,11 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         cudaStreamSynchronize(s_copy);  // a staged copy may still be in flight
         cudaEventDestroy(staged_ev);
     }
+    if (ds != s) {
+        cudaStreamSynchronize(ds);
+        cudaStreamDestroy(ds);
+    }
+    cudaEventDestroy(ev_buck);
     cudaEventDestroy(k0);
     cudaEventDestroy(k1);
     if (st) return st;

@@ -215,6 +215,8 @@ def test_compressed_blocks_unsorted_duplicates(gw, oracle):
     lists = []
     for v in range(V):
         a = csr[int(beg[v]):int(beg[v + 1])].copy()
+        if v == 0:  # a hub: decoded in groups of 32 chunks by several warps
+            a = np.concatenate([a, np.arange(1, V, dtype=np.uint32)])
         if len(a) and v % 3 == 0:
             a = np.concatenate([a, a[: 1 + len(a) // 4]])  # duplicates
         rng.shuffle(a)
@@ -223,7 +225,7 @@ def test_compressed_blocks_unsorted_duplicates(gw, oracle):
     beg2 = np.zeros(V + 1, dtype=np.uint64)
     beg2[1:] = np.cumsum(deg)
     csr2 = np.concatenate(lists).astype(np.uint32)
-    assert (deg > 32).sum() > 10 and (deg == 0).sum() > 0
+    assert (deg > 32).sum() > 10 and (deg == 0).sum() > 0 and deg.max() > 4 * 1024
     from gowalker_b200.preprocess import split_equal_edge_mass
     vb, eb = split_equal_edge_mass(beg2, 10)
     hs = {}
