@@ -49,7 +49,10 @@ struct OocState {
     uint32_t *h_cached = nullptr;  // pinned
     uint32_t *d_cached = nullptr;
 
-    WalkerRec *w_a = nullptr, *w_b = nullptr;
+    WalkerRec *w_rec = nullptr;                    // records, never moved
+    uint32_t *w_ord[2] = {nullptr, nullptr};       // record index per sorted position (current, next)
+    uint32_t *w_key[2] = {nullptr, nullptr};       // bucket per sorted position
+    uint32_t w_cur = 0;
     uint64_t w_cap = 0;
     // 2 * nb^2 buckets (unflagged, then kNeedPrev); d_pairs: nb^2 per-pair totals
     uint32_t *d_counts = nullptr, *d_offsets = nullptr, *d_cursor = nullptr, *d_pairs = nullptr;
@@ -130,8 +133,11 @@ void gw_handle::ooc_release()
     cudaFree(o.d_vstart);
     cudaFree(o.d_estart);
     cudaFree(o.d_cached);
-    cudaFree(o.w_a);
-    cudaFree(o.w_b);
+    cudaFree(o.w_rec);
+    for (int i = 0; i < 2; ++i) {
+        cudaFree(o.w_ord[i]);
+        cudaFree(o.w_key[i]);
+    }
     cudaFree(o.d_counts);
     cudaFree(o.d_pairs);
     cudaFree(o.d_offsets);
@@ -311,12 +317,19 @@ static int ooc_walkers(gw_handle *h)
 {
     OocState &o = *h->ooc;
     if (h->nwalkers > o.w_cap) {
-        cudaFree(o.w_a);
-        cudaFree(o.w_b);
-        o.w_a = o.w_b = nullptr;
+        cudaFree(o.w_rec);
+        o.w_rec = nullptr;
+        for (int i = 0; i < 2; ++i) {
+            cudaFree(o.w_ord[i]);
+            cudaFree(o.w_key[i]);
+            o.w_ord[i] = o.w_key[i] = nullptr;
+        }
         int st;
-        if ((st = h->cuda(cudaMalloc(&o.w_a, h->nwalkers * sizeof(WalkerRec)), "walker records"))) return st;
-        if ((st = h->cuda(cudaMalloc(&o.w_b, h->nwalkers * sizeof(WalkerRec)), "walker records"))) return st;
+        if ((st = h->cuda(cudaMalloc(&o.w_rec, h->nwalkers * sizeof(WalkerRec)), "walker records"))) return st;
+        for (int i = 0; i < 2; ++i) {
+            if ((st = h->cuda(cudaMalloc(&o.w_ord[i], h->nwalkers * sizeof(uint32_t)), "walker order"))) return st;
+            if ((st = h->cuda(cudaMalloc(&o.w_key[i], h->nwalkers * sizeof(uint32_t)), "walker buckets"))) return st;
+        }
         o.w_cap = h->nwalkers;
     }
     return GW_OK;
@@ -448,7 +461,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     in.key0 = (uint32_t)cfg.seed;
     in.key1 = (uint32_t)(cfg.seed >> 32);
     const uint32_t stride = cfg.maxhops + 1;
-    if ((st = cuda(launch_init_walkers(in, o.d_vstart, nb, nwalkers, o.w_a, paths ? d_paths : nullptr, stride, num_sms,
+    o.w_cur = 0;
+    if ((st = cuda(launch_init_walkers(in, o.d_vstart, nb, nwalkers, o.w_rec, o.w_ord[0], o.w_key[0], paths ? d_paths : nullptr,
+                                       stride, num_sms,
                                        s),
                    "init walkers")))
         return st;
@@ -460,13 +475,17 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     auto bucketize = [&](uint64_t n) -> int {
         int e;
         if ((e = cuda(cudaMemsetAsync(o.d_counts, 0, nbk * sizeof(uint32_t), s), "memset"))) return e;
-        if ((e = cuda(launch_count(o.w_a, n, nb, o.d_counts, num_sms, s), "count"))) return e;
+        const uint32_t c = o.w_cur;
+        if ((e = cuda(launch_count(o.w_key[c], n, o.d_counts, num_sms, s), "count"))) return e;
         if ((e = cuda(launch_scan(o.d_counts, (uint32_t)nbk, o.d_offsets, s), "scan"))) return e;
         if ((e = cuda(cudaMemsetAsync(o.d_cursor, 0, nbk * sizeof(uint32_t), s), "memset"))) return e;
-        if ((e = cuda(launch_scatter(o.w_a, n, nb, o.d_offsets, o.d_cursor, o.w_b, num_sms, s), "scatter"))) return e;
+        if ((e = cuda(launch_scatter(o.w_key[c], o.w_ord[c], n, o.d_offsets, o.d_cursor, o.w_key[c ^ 1], o.w_ord[c ^ 1],
+                                     num_sms, s),
+                      "scatter")))
+            return e;
         if ((e = cuda(launch_combine(o.d_counts, nb, o.d_pairs, num_sms, s), "pair counts"))) return e;
         launches += 4;
-        std::swap(o.w_a, o.w_b);  // w_a: bucket-sorted live walkers
+        o.w_cur ^= 1u;  // the sorted index of the live walkers
         // what the next decision reads: counters and error word as of now
         if ((e = cuda(cudaMemcpyAsync(o.d_snap, d_ctr, sizeof(unsigned long long) * kCtrCount, cudaMemcpyDeviceToDevice,
                                       s), "counter snapshot")) ||
@@ -513,7 +532,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                       "runnable")))
             return e;
         if ((e = cuda(cudaMemsetAsync(d_ctr + kCtrCursor, 0, sizeof(unsigned long long), s), "memset"))) return e;
-        a.walkers = o.w_a;
+        a.recs = o.w_rec;
+        a.order = o.w_ord[o.w_cur];
+        a.keys = o.w_key[o.w_cur];
         if ((e = cuda(cudaEventRecord(k0, s), "event"))) return e;
         if ((e = cuda(launch_walk_ooc(a, sopr, coop, grid, s), "walk kernel"))) return e;
         if ((e = cuda(cudaEventRecord(k1, s), "event"))) return e;

@@ -19,7 +19,6 @@
 
 namespace gw {
 
-constexpr uint32_t kNoBucket = 0xFFFFFFFFu;
 
 __device__ __forceinline__ uint32_t block_of(const uint32_t *vs, uint32_t nb, uint32_t v)
 {
@@ -33,8 +32,15 @@ __device__ __forceinline__ uint32_t block_of(const uint32_t *vs, uint32_t nb, ui
     return lo;
 }
 
+__device__ __forceinline__ uint32_t bucket_of(const WalkerRec &r, uint32_t nb)
+{
+    if (r.prev_blk == kFinished) return kNoBucket;
+    return ((r.cur_blk & kNeedPrev) ? nb * nb : 0u) + r.prev_blk * nb + (r.cur_blk & ~kNeedPrev);
+}
+
 __global__ void k_init_walkers(WalkerInit in, const uint32_t *__restrict__ vstart, uint32_t nb, uint64_t n,
-                               WalkerRec *__restrict__ out, uint32_t *__restrict__ paths, uint32_t stride)
+                               WalkerRec *__restrict__ out, uint32_t *__restrict__ order, uint32_t *__restrict__ keys,
+                               uint32_t *__restrict__ paths, uint32_t stride)
 {
     __shared__ uint32_t s_vs[kMaxBlocks + 1];
     for (uint32_t i = threadIdx.x; i <= nb; i += blockDim.x) s_vs[i] = vstart[i];
@@ -55,42 +61,37 @@ __global__ void k_init_walkers(WalkerInit in, const uint32_t *__restrict__ vstar
         r.hash_lo = (uint32_t)h;
         r.hash_hi = (uint32_t)(h >> 32);
         out[i] = r;
+        order[i] = (uint32_t)i;
+        keys[i] = bucket_of(r, nb);
         if (paths) paths[(uint64_t)wid * stride] = src;
     }
 }
 
-__device__ __forceinline__ uint32_t bucket_of(const WalkerRec &r, uint32_t nb)
-{
-    if (r.prev_blk == kFinished) return kNoBucket;
-    return ((r.cur_blk & kNeedPrev) ? nb * nb : 0u) + r.prev_blk * nb + (r.cur_blk & ~kNeedPrev);
-}
-
-__global__ void k_count(const WalkerRec *__restrict__ w, uint64_t n, uint32_t nb, uint32_t *__restrict__ counts)
+__global__ void k_count(const uint32_t *__restrict__ keys, uint64_t n, uint32_t *__restrict__ counts)
 {
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t base = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull; base < n; base += step) {
         const uint64_t i = base + lane;
-        const uint32_t b = (i < n) ? bucket_of(w[i], nb) : kNoBucket;
+        const uint32_t b = (i < n) ? keys[i] : kNoBucket;
         const unsigned grp = __match_any_sync(0xFFFFFFFFu, b);
         if (b != kNoBucket && lane == (uint32_t)(__ffs(grp) - 1)) atomicAdd(&counts[b], (uint32_t)__popc(grp));
     }
 }
 
-__global__ void k_scatter(const WalkerRec *__restrict__ in, uint64_t n, uint32_t nb,
+__global__ void k_scatter(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ order_in, uint64_t n,
                           const uint32_t *__restrict__ offsets, uint32_t *__restrict__ cursor,
-                          WalkerRec *__restrict__ out)
+                          uint32_t *__restrict__ keys_out, uint32_t *__restrict__ order_out)
 {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt = (1u << lane) - 1u;
     const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t base = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull; base < n; base += step) {
         const uint64_t i = base + lane;
-        WalkerRec r{};
-        uint32_t b = kNoBucket;
+        uint32_t r = 0, b = kNoBucket;
         if (i < n) {
-            r = in[i];
-            b = bucket_of(r, nb);
+            b = keys_in[i];
+            r = order_in[i];
         }
         const unsigned grp = __match_any_sync(0xFFFFFFFFu, b);
         if (b != kNoBucket) {
@@ -98,7 +99,8 @@ __global__ void k_scatter(const WalkerRec *__restrict__ in, uint64_t n, uint32_t
             uint32_t pos = 0;
             if (lane == leader) pos = atomicAdd(&cursor[b], (uint32_t)__popc(grp));
             pos = __shfl_sync(grp, pos, leader) + (uint32_t)__popc(grp & lt);
-            out[offsets[b] + pos] = r;
+            keys_out[offsets[b] + pos] = b;
+            order_out[offsets[b] + pos] = r;
         }
     }
 }
@@ -347,7 +349,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
     auto finish = [&]() {
         a.hashes[wid] = h;
         a.lens[wid] = hop + 1;
-        a.walkers[idx].prev_blk = kFinished;
+        a.keys[idx] = kNoBucket;
         atomicAdd(&s_ws[warp][kWsHash], (unsigned long long)h);
         atomicAdd(&s_ws[warp][kWsDone], 1ull);
         flush();
@@ -400,7 +402,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
                     else hi = mid;
                 }
                 idx = (uint64_t)__ldg(a.run_off + lo) + (g - __ldg(a.run_pre + lo));
-                const WalkerRec rec = a.walkers[idx];
+                const WalkerRec rec = a.recs[__ldg(a.order + idx)];
                 wid = rec.wid;
                 prev = rec.prev;
                 cur = rec.cur;
@@ -475,7 +477,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
             rec.cur_blk = cb | kNeedPrev;
             rec.hash_lo = (uint32_t)h;
             rec.hash_hi = (uint32_t)(h >> 32);
-            a.walkers[idx] = rec;
+            a.recs[__ldg(a.order + idx)] = rec;
+            a.keys[idx] = bucket_of(rec, a.nb);
             n_trials -= attempt;
             flush();
             active = false;
@@ -511,7 +514,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
                     rec.cur_blk = nbx;
                     rec.hash_lo = (uint32_t)h;
                     rec.hash_hi = (uint32_t)(h >> 32);
-                    a.walkers[idx] = rec;
+                    a.recs[__ldg(a.order + idx)] = rec;
+                    a.keys[idx] = bucket_of(rec, a.nb);
                     flush();
                     active = false;
                 } else {
@@ -671,16 +675,16 @@ cudaError_t launch_learned_choose(const float *pred, uint32_t nb, const uint32_t
 // ------------------------------------------------------------------ launchers
 
 cudaError_t launch_init_walkers(const WalkerInit &in, const uint32_t *vstart, uint32_t nb, uint64_t n,
-                                WalkerRec *out, uint32_t *paths, uint32_t stride, int num_sms, cudaStream_t s)
+                                WalkerRec *recs, uint32_t *order, uint32_t *keys, uint32_t *paths, uint32_t stride,
+                                int num_sms, cudaStream_t s)
 {
-    k_init_walkers<<<num_sms * 8, 256, 0, s>>>(in, vstart, nb, n, out, paths, stride);
+    k_init_walkers<<<num_sms * 8, 256, 0, s>>>(in, vstart, nb, n, recs, order, keys, paths, stride);
     return cudaGetLastError();
 }
 
-cudaError_t launch_count(const WalkerRec *w, uint64_t n, uint32_t nb, uint32_t *counts, int num_sms,
-                         cudaStream_t s)
+cudaError_t launch_count(const uint32_t *keys, uint64_t n, uint32_t *counts, int num_sms, cudaStream_t s)
 {
-    k_count<<<num_sms * 8, 256, 0, s>>>(w, n, nb, counts);
+    k_count<<<num_sms * 8, 256, 0, s>>>(keys, n, counts);
     return cudaGetLastError();
 }
 
@@ -690,10 +694,10 @@ cudaError_t launch_scan(const uint32_t *counts, uint32_t n, uint32_t *offsets, c
     return cudaGetLastError();
 }
 
-cudaError_t launch_scatter(const WalkerRec *in, uint64_t n, uint32_t nb, const uint32_t *offsets,
-                           uint32_t *cursor, WalkerRec *out, int num_sms, cudaStream_t s)
+cudaError_t launch_scatter(const uint32_t *keys_in, const uint32_t *order_in, uint64_t n, const uint32_t *offsets,
+                           uint32_t *cursor, uint32_t *keys_out, uint32_t *order_out, int num_sms, cudaStream_t s)
 {
-    k_scatter<<<num_sms * 8, 256, 0, s>>>(in, n, nb, offsets, cursor, out);
+    k_scatter<<<num_sms * 8, 256, 0, s>>>(keys_in, order_in, n, offsets, cursor, keys_out, order_out);
     return cudaGetLastError();
 }
 

@@ -18,6 +18,7 @@ struct __align__(16) WalkerRec {
 static_assert(sizeof(WalkerRec) == 32, "walker record is 32 bytes");
 
 constexpr uint32_t kFinished = 0xFFFFFFFFu;  // prev_blk of a finished walker
+constexpr uint32_t kNoBucket = 0xFFFFFFFFu;  // bucket key of a finished walker
 constexpr uint32_t kMaxBlocks = 1024;        // block table kept in shared memory
 // cur_blk flag of a walker whose step needs N(prev) while prev's block is
 // absent (lazy mode); such walkers sit in the second half of the buckets.
@@ -31,7 +32,9 @@ struct OocStepArgs {
     const uint64_t *estart;          // [nb+1]
     uint32_t nb, nverts;
     uint32_t lazy;                   // 1: a walker runs with only its current block resident
-    WalkerRec *walkers;              // bucket-sorted, updated in place
+    WalkerRec *recs;                 // one record per walker, never moved
+    const uint32_t *order;           // record of each bucket-sorted position
+    uint32_t *keys;                  // bucket of each sorted position; kNoBucket once finished
     const uint32_t *run_pre;         // [nrun+1] prefix of runnable bucket sizes
     const uint32_t *run_off;         // [nrun] first walker of each runnable bucket
     const uint32_t *nrun;            // runnable bucket count (device)
@@ -54,13 +57,16 @@ struct Decision {
     uint64_t score;
 };
 
+// Walkers are sorted by bucket through an index: records stay where
+// k_init_walkers puts them; `order` and `keys` (record index and bucket of
+// each sorted position) are what bucketing moves, 8 bytes per walker.
 cudaError_t launch_init_walkers(const WalkerInit &in, const uint32_t *vstart, uint32_t nb, uint64_t n,
-                                WalkerRec *out, uint32_t *paths, uint32_t stride, int num_sms, cudaStream_t s);
-cudaError_t launch_count(const WalkerRec *w, uint64_t n, uint32_t nb, uint32_t *counts, int num_sms,
-                         cudaStream_t s);
+                                WalkerRec *recs, uint32_t *order, uint32_t *keys, uint32_t *paths, uint32_t stride,
+                                int num_sms, cudaStream_t s);
+cudaError_t launch_count(const uint32_t *keys, uint64_t n, uint32_t *counts, int num_sms, cudaStream_t s);
 cudaError_t launch_scan(const uint32_t *counts, uint32_t n, uint32_t *offsets, cudaStream_t s);
-cudaError_t launch_scatter(const WalkerRec *in, uint64_t n, uint32_t nb, const uint32_t *offsets,
-                           uint32_t *cursor, WalkerRec *out, int num_sms, cudaStream_t s);
+cudaError_t launch_scatter(const uint32_t *keys_in, const uint32_t *order_in, uint64_t n, const uint32_t *offsets,
+                           uint32_t *cursor, uint32_t *keys_out, uint32_t *order_out, int num_sms, cudaStream_t s);
 // Buckets are 2 * nb^2: (prev_blk, cur_blk), then the same pairs for walkers
 // flagged kNeedPrev.
 cudaError_t launch_runnable(const uint32_t *counts, const uint32_t *offsets, const uint32_t *const *blk_csr,
