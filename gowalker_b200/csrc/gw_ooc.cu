@@ -54,6 +54,7 @@ struct OocState {
     uint32_t *w_key[2] = {nullptr, nullptr};       // bucket per sorted position
     uint32_t w_cur = 0;
     uint64_t w_cap = 0;
+    uint32_t *d_n = nullptr, *h_n = nullptr;  // sorted positions (device; pinned host word to set it)
     // 2 * nb^2 buckets (unflagged, then kNeedPrev); d_pairs: nb^2 per-pair totals
     uint32_t *d_counts = nullptr, *d_offsets = nullptr, *d_cursor = nullptr, *d_pairs = nullptr;
     uint32_t *d_run_pre = nullptr, *d_run_off = nullptr, *d_nrun = nullptr;
@@ -138,6 +139,8 @@ void gw_handle::ooc_release()
         cudaFree(o.w_ord[i]);
         cudaFree(o.w_key[i]);
     }
+    cudaFree(o.d_n);
+    if (o.h_n) cudaFreeHost(o.h_n);
     cudaFree(o.d_counts);
     cudaFree(o.d_pairs);
     cudaFree(o.d_offsets);
@@ -287,6 +290,8 @@ static int ooc_setup(gw_handle *h)
     if ((st = h->cuda(cudaMalloc((void **)&o.d_blk_csr2, nb * sizeof(void *)), "block table"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_snap, sizeof(unsigned long long) * (kCtrCount + 1)), "counter snapshot")))
         return st;
+    if ((st = h->cuda(cudaMalloc(&o.d_n, sizeof(uint32_t)), "walker count"))) return st;
+    if ((st = h->cuda(cudaMallocHost(&o.h_n, sizeof(uint32_t)), "walker count"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_vstart, (nb + 1) * sizeof(uint32_t)), "vstart"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_estart, (nb + 1) * sizeof(uint64_t)), "estart"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_cached, nb * sizeof(uint32_t)), "cached list"))) return st;
@@ -472,28 +477,56 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     cudaEvent_t ev_buck = nullptr;  // the last re-bucketing (and counter snapshot) is done
     if ((st = cuda(cudaEventCreateWithFlags(&ev_buck, cudaEventDisableTiming), "event"))) return st;
 
-    auto bucketize = [&](uint64_t n) -> int {
+    // Re-bucketing: count, scan and scatter the sorted index from buffer c to
+    // c^1, per-pair totals, the new walker count into d_n, and the counter
+    // snapshot the next decision reads.  The sequence is captured once per
+    // run and buffer parity as a CUDA graph and replayed every iteration.
+    auto bucketize_ops = [&](uint32_t c) -> int {
         int e;
         if ((e = cuda(cudaMemsetAsync(o.d_counts, 0, nbk * sizeof(uint32_t), s), "memset"))) return e;
-        const uint32_t c = o.w_cur;
-        if ((e = cuda(launch_count(o.w_key[c], n, o.d_counts, num_sms, s), "count"))) return e;
+        if ((e = cuda(launch_count(o.w_key[c], o.d_n, o.d_counts, num_sms, s), "count"))) return e;
         if ((e = cuda(launch_scan(o.d_counts, (uint32_t)nbk, o.d_offsets, s), "scan"))) return e;
         if ((e = cuda(cudaMemsetAsync(o.d_cursor, 0, nbk * sizeof(uint32_t), s), "memset"))) return e;
-        if ((e = cuda(launch_scatter(o.w_key[c], o.w_ord[c], n, o.d_offsets, o.d_cursor, o.w_key[c ^ 1], o.w_ord[c ^ 1],
-                                     num_sms, s),
+        if ((e = cuda(launch_scatter(o.w_key[c], o.w_ord[c], o.d_n, o.d_offsets, o.d_cursor, o.w_key[c ^ 1],
+                                     o.w_ord[c ^ 1], num_sms, s),
                       "scatter")))
             return e;
         if ((e = cuda(launch_combine(o.d_counts, nb, o.d_pairs, num_sms, s), "pair counts"))) return e;
+        if ((e = cuda(cudaMemcpyAsync(o.d_n, o.d_offsets + nbk, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s),
+                      "walker count")))
+            return e;
+        if ((e = cuda(cudaMemcpyAsync(o.d_snap, d_ctr, sizeof(unsigned long long) * kCtrCount, cudaMemcpyDeviceToDevice,
+                                      s), "counter snapshot")))
+            return e;
+        return cuda(cudaMemcpyAsync(o.d_snap + kCtrCount, d_err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s),
+                    "error snapshot");
+    };
+    cudaGraphExec_t bgraph[2] = {nullptr, nullptr};
+    auto bucketize = [&](uint64_t) -> int {
+        const uint32_t c = o.w_cur;
+        int e;
+        if (!bgraph[c]) {
+            cudaGraph_t g = nullptr;
+            if ((e = cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture"))) return e;
+            const int eo = bucketize_ops(c);
+            const cudaError_t ec = cudaStreamEndCapture(s, &g);
+            if (eo) {
+                if (g) cudaGraphDestroy(g);
+                return eo;
+            }
+            if ((e = cuda(ec, "capture"))) return e;
+            e = cuda(cudaGraphInstantiate(&bgraph[c], g, 0), "graph instantiate");
+            cudaGraphDestroy(g);
+            if (e) return e;
+        }
+        if ((e = cuda(cudaGraphLaunch(bgraph[c], s), "bucketing graph"))) return e;
         launches += 4;
         o.w_cur ^= 1u;  // the sorted index of the live walkers
-        // what the next decision reads: counters and error word as of now
-        if ((e = cuda(cudaMemcpyAsync(o.d_snap, d_ctr, sizeof(unsigned long long) * kCtrCount, cudaMemcpyDeviceToDevice,
-                                      s), "counter snapshot")) ||
-            (e = cuda(cudaMemcpyAsync(o.d_snap + kCtrCount, d_err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s),
-                      "error snapshot")))
-            return e;
         return cuda(cudaEventRecord(ev_buck, s), "event");
     };
+    *o.h_n = (uint32_t)nwalkers;
+    if ((st = cuda(cudaMemcpyAsync(o.d_n, o.h_n, sizeof(uint32_t), cudaMemcpyHostToDevice, s), "walker count")))
+        return st;
     if ((st = bucketize(nlive))) return st;
 
     OocStepArgs a{};
@@ -871,6 +904,8 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         cudaStreamSynchronize(ds);
         cudaStreamDestroy(ds);
     }
+    for (auto &g : bgraph)
+        if (g) cudaGraphExecDestroy(g);
     cudaEventDestroy(ev_buck);
     cudaEventDestroy(k0);
     cudaEventDestroy(k1);

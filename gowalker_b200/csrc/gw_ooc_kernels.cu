@@ -67,8 +67,9 @@ __global__ void k_init_walkers(WalkerInit in, const uint32_t *__restrict__ vstar
     }
 }
 
-__global__ void k_count(const uint32_t *__restrict__ keys, uint64_t n, uint32_t *__restrict__ counts)
+__global__ void k_count(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ n_ptr, uint32_t *__restrict__ counts)
 {
+    const uint64_t n = *n_ptr;
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t base = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull; base < n; base += step) {
@@ -79,10 +80,12 @@ __global__ void k_count(const uint32_t *__restrict__ keys, uint64_t n, uint32_t 
     }
 }
 
-__global__ void k_scatter(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ order_in, uint64_t n,
-                          const uint32_t *__restrict__ offsets, uint32_t *__restrict__ cursor,
-                          uint32_t *__restrict__ keys_out, uint32_t *__restrict__ order_out)
+__global__ void k_scatter(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ order_in,
+                          const uint32_t *__restrict__ n_ptr, const uint32_t *__restrict__ offsets,
+                          uint32_t *__restrict__ cursor, uint32_t *__restrict__ keys_out,
+                          uint32_t *__restrict__ order_out)
 {
+    const uint64_t n = *n_ptr;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt = (1u << lane) - 1u;
     const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
@@ -682,7 +685,7 @@ cudaError_t launch_init_walkers(const WalkerInit &in, const uint32_t *vstart, ui
     return cudaGetLastError();
 }
 
-cudaError_t launch_count(const uint32_t *keys, uint64_t n, uint32_t *counts, int num_sms, cudaStream_t s)
+cudaError_t launch_count(const uint32_t *keys, const uint32_t *n, uint32_t *counts, int num_sms, cudaStream_t s)
 {
     k_count<<<num_sms * 8, 256, 0, s>>>(keys, n, counts);
     return cudaGetLastError();
@@ -694,7 +697,7 @@ cudaError_t launch_scan(const uint32_t *counts, uint32_t n, uint32_t *offsets, c
     return cudaGetLastError();
 }
 
-cudaError_t launch_scatter(const uint32_t *keys_in, const uint32_t *order_in, uint64_t n, const uint32_t *offsets,
+cudaError_t launch_scatter(const uint32_t *keys_in, const uint32_t *order_in, const uint32_t *n, const uint32_t *offsets,
                            uint32_t *cursor, uint32_t *keys_out, uint32_t *order_out, int num_sms, cudaStream_t s)
 {
     k_scatter<<<num_sms * 8, 256, 0, s>>>(keys_in, order_in, n, offsets, cursor, keys_out, order_out);

@@ -63,9 +63,11 @@ struct Decision {
 cudaError_t launch_init_walkers(const WalkerInit &in, const uint32_t *vstart, uint32_t nb, uint64_t n,
                                 WalkerRec *recs, uint32_t *order, uint32_t *keys, uint32_t *paths, uint32_t stride,
                                 int num_sms, cudaStream_t s);
-cudaError_t launch_count(const uint32_t *keys, uint64_t n, uint32_t *counts, int num_sms, cudaStream_t s);
+// `n` points at the number of sorted positions (a device word, so the
+// bucketing sequence can be captured once and replayed).
+cudaError_t launch_count(const uint32_t *keys, const uint32_t *n, uint32_t *counts, int num_sms, cudaStream_t s);
 cudaError_t launch_scan(const uint32_t *counts, uint32_t n, uint32_t *offsets, cudaStream_t s);
-cudaError_t launch_scatter(const uint32_t *keys_in, const uint32_t *order_in, uint64_t n, const uint32_t *offsets,
+cudaError_t launch_scatter(const uint32_t *keys_in, const uint32_t *order_in, const uint32_t *n, const uint32_t *offsets,
                            uint32_t *cursor, uint32_t *keys_out, uint32_t *order_out, int num_sms, cudaStream_t s);
 // Buckets are 2 * nb^2: (prev_blk, cur_blk), then the same pairs for walkers
 // flagged kNeedPrev.
