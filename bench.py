@@ -47,6 +47,9 @@ WORKLOADS = {
                     "rejecting ids >= 41.6M, thinned to 1.47B edges, 64 equal-edge-mass blocks, 1.5 GB device cache",
                scale=26, nverts=41_600_000, target=1_470_000_000, nsamples=2_600_000_000, ef=0, algo=0, maxhops=80,
                wps=1, p=0.5, q=2.0, alpha=0.2, term=0.0, nblocks=64, cache=1_500_000_000, ooc=True),
+    "prep": dict(name="edge list -> CSR on the device (gw_edges_csr): R-MAT scale 24 ef 16 sample list "
+                      "(268,435,456 u32 pairs, (a,b,c,d) = (0.57,0.19,0.19,0.05)), symmetrised, deduplicated, sorted",
+                 scale=24, ef=16, prep=True),
 }
 L2_BYTES = 126 * 1024 * 1024
 
@@ -224,6 +227,32 @@ def run_reference_arm(args, wl):
     return 0
 
 
+def run_prep_reference(args, wl):
+    """The converter restatement (numpy, one thread) on a bounded prefix of
+    the same sample list, per step."""
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    n = wl["ef"] << wl["scale"]
+    V = 1 << wl["scale"]
+    src, dst = rmat_edges_torch(wl["scale"], n, 1)
+    src, dst = src.cpu().numpy().view(np.uint32), dst.cpu().numpy().view(np.uint32)
+    for _ in range(args.warmup):
+        prep_cpu_baseline(src, dst, V, 0.5)
+    vals = [prep_cpu_baseline(src, dst, V, args.ref_seconds) for _ in range(args.steps)]
+    v = sum(x["value"] for x in vals) / len(vals)
+    line = {"impl": "reference", "metric": "edge-list samples converted/sec", "value": v, "unit": "samples/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * args.ref_seconds, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32 ids, u64 keys", "data": "synthetic",
+            "config": {"workload": wl["name"]},
+            "cpu_baseline": dict(vals[-1], value=v),
+            "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 PCIE_GEN5_X16_GBS = 64.0  # nominal host-link peak per direction
 
 
@@ -305,6 +334,133 @@ def run_ooc_bench(args, wl):
     print(json.dumps(line), flush=True)
     eng.close()
     return 0
+
+
+def rmat_edges_torch(scale, n, seed, abc=(0.57, 0.19, 0.19)):
+    """Seeded R-MAT sample list generated on the device with torch's RNG:
+    `scale` quadrant choices per sample (a: (0,0), b: (0,1), c: (1,0),
+    d: (1,1)).  Returns int32 device tensors (ids < 2^scale)."""
+    import torch
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    a, b, c = abc
+    src = torch.zeros(n, dtype=torch.int32, device="cuda")
+    dst = torch.zeros(n, dtype=torch.int32, device="cuda")
+    for _ in range(scale):
+        u = torch.rand(n, device="cuda", generator=g)
+        src.mul_(2).add_((u >= a + b).to(torch.int32))
+        dst.mul_(2).add_((((u >= a) & (u < a + b)) | (u >= a + b + c)).to(torch.int32))
+        del u
+    return src, dst
+
+
+def run_prep_bench(args, wl):
+    """gw_edges_csr on the workload's sample list: value with the list resident
+    in HBM; e2e from pinned host arrays to the CSR back in pinned host memory."""
+    import ctypes
+    import torch
+    import gowalker_b200 as gw
+    torch.cuda.set_device(0)
+    L = gw.load()
+    n = wl["ef"] << wl["scale"]
+    V = 1 << wl["scale"]
+    flags = gw.GW_EDGES_SYMMETRIC | gw.GW_EDGES_SORT | gw.GW_EDGES_DEDUP
+    src, dst = rmat_edges_torch(wl["scale"], n, 1)
+    h_src = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    h_dst = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    h_src.copy_(src)
+    h_dst.copy_(dst)
+    torch.cuda.synchronize()
+
+    def convert(ps, pd):
+        db, dc, ne, nv = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_uint64(), ctypes.c_uint32()
+        st = L.gw_edges_csr(ctypes.c_void_p(ps), ctypes.c_void_p(pd), n, V, flags, ctypes.byref(db),
+                            ctypes.byref(dc), ctypes.byref(ne), ctypes.byref(nv))
+        if st != 0:
+            raise gw.GwError(st, "gw_edges_csr failed")
+        return db.value, dc.value, int(ne.value)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    for _ in range(args.warmup):
+        db, dc, ne = convert(src.data_ptr(), dst.data_ptr())
+        L.gw_device_free(ctypes.c_void_p(db))
+        L.gw_device_free(ctypes.c_void_p(dc))
+    clocks = ClockSampler(0)
+    clocks.start()
+    dev_ms = []
+    for _ in range(args.steps):
+        ms, (db, dc, ne) = timed(lambda: convert(src.data_ptr(), dst.data_ptr()))
+        dev_ms.append(ms)
+        L.gw_device_free(ctypes.c_void_p(db))
+        L.gw_device_free(ctypes.c_void_p(dc))
+    h_beg = torch.empty(V + 1, dtype=torch.int64, pin_memory=True)
+    h_csr = torch.empty(ne, dtype=torch.int32, pin_memory=True)
+
+    def e2e_step():
+        db, dc, ne2 = convert(h_src.data_ptr(), h_dst.data_ptr())
+        L.gw_memcpy(ctypes.c_void_p(h_beg.data_ptr()), ctypes.c_void_p(db), (V + 1) * 8)
+        L.gw_memcpy(ctypes.c_void_p(h_csr.data_ptr()), ctypes.c_void_p(dc), ne2 * 4)
+        L.gw_device_free(ctypes.c_void_p(db))
+        L.gw_device_free(ctypes.c_void_p(dc))
+        return ne2
+
+    e2e_ms = []
+    for _ in range(args.steps):
+        ms, ne2 = timed(e2e_step)
+        assert ne2 == ne
+        e2e_ms.append(ms)
+    clk = clocks.stop()
+    ms = sum(dev_ms) / len(dev_ms)
+    ems = sum(e2e_ms) / len(e2e_ms)
+    # Least traffic a conversion can have: read the pairs once (8 B per
+    # sample), write the offsets and the kept neighbour ids once.
+    min_bytes = 8 * n + 8 * (V + 1) + 4 * ne
+    peaks, peak_kind = measured_peaks()
+    hbm = peaks["hbm_gbs"]
+    achieved = min_bytes / (ms / 1e3) / 1e9
+    line = {"metric": "edge-list samples converted/sec", "value": n / (ms / 1e3), "unit": "samples/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 ids, u64 keys", "data": "synthetic",
+            "config": {"workload": wl["name"], "vertices": V, "samples": n, "edges_out": ne,
+                       "l2": "inputs larger than L2 (2 GB of pairs)"},
+            "gpu_launches": 2,
+            "library_launches": "CUB radix sort (8-bit digits over 32 + bit_length(V) key bits), unique, scan",
+            "e2e": {"value": n / (ems / 1e3), "unit": "samples/s", "h2d_bytes_per_step": 8 * n,
+                    "d2h_bytes_per_step": 8 * (V + 1) + 4 * ne},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None, "peak_source": peak_kind,
+                         "note": "achieved counts the least I/O of a conversion (pairs in, CSR out); the radix "
+                                 "sort's digit passes read and write every key again"}}
+    if clk:
+        line["clocks"] = clk
+    if args.cpu_seconds > 0:
+        line["cpu_baseline"] = prep_cpu_baseline(h_src.numpy().view(np.uint32), h_dst.numpy().view(np.uint32), V,
+                                                 args.cpu_seconds)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def prep_cpu_baseline(src, dst, V, target_s):
+    """The oracle's converter (numpy, one thread) on a prefix of the sample
+    list sized to take about target_s seconds."""
+    from oracle import oracle as O
+    k = 1 << 18
+    t0 = time.time()
+    O.convert_edges(src[:k], dst[:k], V, symmetric=True, dedup=True)
+    dt = max(time.time() - t0, 1e-3)
+    k = int(min(len(src), max(k, k * target_s / dt)))
+    t0 = time.time()
+    O.convert_edges(src[:k], dst[:k], V, symmetric=True, dedup=True)
+    dt = time.time() - t0
+    return {"value": k / dt, "unit": "samples/s", "cores": 1, "kind": "port",
+            "sample": "first %d of the samples, symmetrised + deduplicated + sorted" % k}
 
 
 def run_ours(args, wl):
@@ -500,7 +656,11 @@ def main():
     if args.warmup < 3:
         log("note: fewer than 3 warm-up steps")
     if args.impl == "reference":
+        if wl.get("prep"):
+            return run_prep_reference(args, wl)
         return run_reference_arm(args, wl)
+    if wl.get("prep"):
+        return run_prep_bench(args, wl)
     if wl.get("ooc"):
         return run_ooc_bench(args, wl)
     return run_ours(args, wl)

@@ -8,10 +8,16 @@
 //
 // Pipeline: sample kernel -> u64 keys (src<<32|dst, invalid = ~0) ->
 // radix sort (CUB) -> unique (CUB) -> optional even thinning to an exact edge
-// count -> offsets kernel + neighbour extraction.
+// count -> offsets + neighbour extraction (csr_from_sorted).
+//
+// The same key pipeline turns a caller's edge list into a CSR
+// (gw_edges_csr), and gw_split_blocks computes block split points from the
+// offsets on the device.
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
+#include <algorithm>
 #include <cstdint>
 #include "gw_philox.cuh"
 #include "../../include/gowalker.h"
@@ -60,16 +66,219 @@ __global__ void k_thin(const uint64_t *in, uint64_t U, uint64_t k, uint64_t *out
     }
 }
 
-// beg[v] = first index whose source >= v; csr[i] = low word of key i.
-__global__ void k_offsets(const uint64_t *keys, uint64_t n, uint32_t nverts, uint64_t *beg, uint32_t *csr)
+// Degrees from the runs of a source-sorted key list: the first key of a run
+// adds -i and the last adds i+1 to cnt[src] (mod 2^64), so cnt[v] ends as the
+// run length; two uncontended atomics per vertex whatever the gaps between
+// sources.  csr[i] = low word of key i.
+__global__ void k_runs(const uint64_t *__restrict__ keys, uint64_t n, unsigned long long *cnt,
+                       uint32_t *__restrict__ csr)
 {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += stride) {
-        const int64_t s_here = (i < n) ? (int64_t)(keys[i] >> 32) : (int64_t)nverts;
-        const int64_t s_prev = (i > 0) ? (int64_t)(keys[i - 1] >> 32) : -1;
-        for (int64_t v = s_prev + 1; v <= s_here; ++v) beg[v] = i;
-        if (i < n) csr[i] = (uint32_t)keys[i];
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint64_t k = keys[i];
+        const uint32_t s = (uint32_t)(k >> 32);
+        if (i == 0 || (uint32_t)(keys[i - 1] >> 32) != s) atomicAdd(cnt + s, 0ull - (unsigned long long)i);
+        if (i + 1 == n || (uint32_t)(keys[i + 1] >> 32) != s) atomicAdd(cnt + s, (unsigned long long)(i + 1));
+        csr[i] = (uint32_t)k;
     }
+}
+
+// Edge list -> keys at fixed positions (edge i at i, or at 2i and 2i+1 when
+// symmetric) so a stable sort by source keeps input order.  Self loops and
+// out-of-range ids become the marker ~0, which sorts after every kept key for
+// any sort that covers bit 32 + bit_length(nverts) - 1 (no kept source reaches
+// 2^b - 1).  Per-thread maximum id and kept count are folded with one atomic
+// per warp at the end.
+__global__ void k_edge_keys(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst, uint64_t n,
+                            uint64_t first, uint32_t lim, int symmetric, uint64_t *__restrict__ keys,
+                            unsigned int *max_id, unsigned long long *nkept, unsigned int *range_err)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    uint32_t mx = 0, bad = 0;
+    uint64_t kept = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t s = __ldg(src + i), d = __ldg(dst + i);
+        const bool in_range = s < lim && d < lim;
+        const bool ok = in_range && s != d;
+        bad |= in_range ? 0u : 1u;
+        if (ok) {
+            mx = max(mx, max(s, d));
+            ++kept;
+        }
+        const uint64_t j = first + i;
+        if (symmetric) {
+            keys[2 * j] = ok ? (((uint64_t)s << 32) | d) : ~0ull;
+            keys[2 * j + 1] = ok ? (((uint64_t)d << 32) | s) : ~0ull;
+        } else {
+            keys[j] = ok ? (((uint64_t)s << 32) | d) : ~0ull;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+        bad |= __shfl_xor_sync(0xFFFFFFFFu, bad, o);
+        kept += __shfl_xor_sync(0xFFFFFFFFu, kept, o);
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        if (kept) {
+            atomicMax(max_id, mx);
+            atomicAdd(nkept, (unsigned long long)kept);
+        }
+        if (bad) atomicOr(range_err, 1u);
+    }
+}
+
+// First index in [lo, hi) with beg[idx] > t (hi if none), found by one warp
+// with 32 probes per round.  Every lane returns the same value.
+__device__ uint64_t warp_upper_bound(const uint64_t *beg, uint64_t lo, uint64_t hi, uint64_t t)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    while (hi - lo > 32) {
+        const uint64_t len = hi - lo;
+        const uint64_t q = lo + len * (lane + 1) / 33;  // strictly increasing, all < hi
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, beg[q] > t);
+        const uint64_t qprev = __shfl_up_sync(0xFFFFFFFFu, q, 1);
+        if (m == 0) {
+            lo = __shfl_sync(0xFFFFFFFFu, q, 31) + 1;
+        } else {
+            const int f = __ffs(m) - 1;
+            const uint64_t qf = __shfl_sync(0xFFFFFFFFu, q, f);
+            const uint64_t qb = __shfl_sync(0xFFFFFFFFu, qprev, f);
+            hi = qf;
+            lo = f == 0 ? lo : qb + 1;
+        }
+    }
+    const uint64_t q = lo + lane;
+    const unsigned m = __ballot_sync(0xFFFFFFFFu, q < hi && beg[q] > t);
+    return m ? lo + (uint64_t)(__ffs(m) - 1) : hi;
+}
+
+// The reference splitter (preprocess/split.hpp:15-87) over nv = nverts + 1
+// offsets, one warp.  The reference checks every v in order; here each
+// round finds the next v that meets either rule by search: the edge rule
+// first holds at the first v with beg[v] > rd_edges + max_nedges, the vertex
+// rule at max(v, cur_pos + max_nverts); the edge rule wins a tie, as in the
+// reference's if / else-if.  Writes at most cap+1 split points, counts all.
+__global__ void k_split_reference(const uint64_t *beg, uint64_t nv, uint64_t max_nedges, uint64_t max_nverts,
+                                  uint32_t cap, uint32_t *vb, uint64_t *eb, uint32_t *count)
+{
+    if (threadIdx.x >= 32) return;
+    const uint32_t lane = threadIdx.x;
+    uint64_t cur_pos = 0, rd_edges = 0, v = 0, nb = 0;
+    if (lane == 0) {
+        vb[0] = 0;
+        eb[0] = 0;
+    }
+    while (v < nv) {
+        const uint64_t ve = warp_upper_bound(beg, v, nv, rd_edges + max_nedges);
+        const uint64_t vv = max(v, cur_pos + max_nverts);
+        if (ve >= nv && vv >= nv) break;
+        uint64_t cut;
+        if (vv < ve) {
+            cut = vv;
+            v = vv + 1;
+        } else {
+            cut = ve - 1;
+            v = ve + 1;
+        }
+        cur_pos = cut;
+        rd_edges = beg[cut];
+        ++nb;
+        if (lane == 0 && nb <= cap) {
+            vb[nb] = (uint32_t)cut;
+            eb[nb] = rd_edges;
+        }
+    }
+    ++nb;
+    if (lane == 0) {
+        if (nb <= cap) {
+            vb[nb] = (uint32_t)(nv - 1);
+            eb[nb] = beg[nv - 1];
+        }
+        *count = (uint32_t)min(nb, (uint64_t)0xFFFFFFFFu);
+    }
+}
+
+// Equal-edge-mass split: thread k < nblocks-1 finds the first vertex
+// v < V with beg[v] >= floor((k+1)*E/nblocks) (V if none), clipped to
+// [1, V-1]; thread 0 then makes the cut list non-decreasing.
+__global__ void k_split_equal(const uint64_t *beg, uint32_t V, uint32_t nblocks, uint32_t *vb, uint64_t *eb)
+{
+    const uint64_t E = beg[V];
+    const uint32_t hi_clip = V > 1 ? V - 1 : 1;
+    for (uint32_t k = threadIdx.x; k + 1 < nblocks; k += blockDim.x) {
+        const uint64_t t = (uint64_t)((unsigned __int128)(k + 1) * E / nblocks);
+        uint64_t lo = 0, hi = V;  // lower bound over beg[0, V)
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (beg[mid] < t) lo = mid + 1;
+            else hi = mid;
+        }
+        vb[k + 1] = (uint32_t)(lo < 1 ? 1 : (lo > hi_clip ? hi_clip : lo));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        vb[0] = 0;
+        vb[nblocks] = V;
+        uint32_t run = 0;
+        for (uint32_t k = 0; k <= nblocks; ++k) {
+            run = max(run, vb[k]);
+            vb[k] = run;
+            eb[k] = beg[run];
+        }
+    }
+}
+
+// offsets + neighbour ids from n sorted keys (sources < nverts).  Allocates
+// *beg_out and *csr_out; s is synchronised before return.
+static cudaError_t csr_from_sorted(const uint64_t *keys, uint64_t n, uint32_t nverts, cudaStream_t s,
+                                   uint64_t **beg_out, uint32_t **csr_out)
+{
+    unsigned long long *cnt = nullptr;
+    uint64_t *beg = nullptr;
+    uint32_t *csr = nullptr;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0;
+    const uint64_t nb = (uint64_t)nverts + 1;
+    cudaError_t e;
+    do {
+        if ((e = cudaMalloc(&cnt, nb * sizeof(uint64_t))) != cudaSuccess) break;
+        if ((e = cudaMalloc(&beg, nb * sizeof(uint64_t))) != cudaSuccess) break;
+        if ((e = cudaMalloc(&csr, (n ? n : 1) * sizeof(uint32_t))) != cudaSuccess) break;
+        if ((e = cudaMemsetAsync(cnt, 0, nb * sizeof(uint64_t), s)) != cudaSuccess) break;
+        if (n) {
+            k_runs<<<148 * 16, 256, 0, s>>>(keys, n, cnt, csr);
+            if ((e = cudaGetLastError()) != cudaSuccess) break;
+        }
+        if ((e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, (const uint64_t *)cnt, beg, nb, s)) != cudaSuccess)
+            break;
+        if ((e = cudaMalloc(&tmp, tmp_bytes)) != cudaSuccess) break;
+        if ((e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, (const uint64_t *)cnt, beg, nb, s)) != cudaSuccess)
+            break;
+        e = cudaStreamSynchronize(s);
+    } while (0);
+    cudaFree(cnt);
+    cudaFree(tmp);
+    if (e != cudaSuccess) {
+        cudaFree(beg);
+        cudaFree(csr);
+        return e;
+    }
+    *beg_out = beg;
+    *csr_out = csr;
+    return cudaSuccess;
+}
+
+static inline uint32_t bit_length32(uint32_t x) { return x ? 32u - (uint32_t)__builtin_clz(x) : 0u; }
+
+static bool device_accessible(const void *p)
+{
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
 }  // namespace gw
@@ -132,11 +341,7 @@ extern "C" int gw_rmat_csr(uint32_t scale, uint32_t nverts, uint64_t nsamples, c
             U = target_edges;
         }
     }
-    GEN_CHECK(cudaMalloc(&beg, ((uint64_t)nverts + 1) * sizeof(uint64_t)));
-    GEN_CHECK(cudaMalloc(&csr, (U ? U : 1) * sizeof(uint32_t)));
-    k_offsets<<<blocks, threads, 0, s>>>(keys, U, nverts, beg, csr);
-    GEN_CHECK(cudaGetLastError());
-    GEN_CHECK(cudaStreamSynchronize(s));
+    GEN_CHECK(csr_from_sorted(keys, U, nverts, s, &beg, &csr));
     *d_beg = beg;
     *d_csr = csr;
     *nedges = U;
@@ -149,6 +354,163 @@ done:
     cudaFree(d_nsel);
     cudaFree(beg);
     cudaFree(csr);
+    return rc;
+}
+
+extern "C" int gw_edges_csr(const uint32_t *src, const uint32_t *dst, uint64_t n, uint32_t nverts, uint32_t flags,
+                            uint64_t **d_beg, uint32_t **d_csr, uint64_t *nedges, uint32_t *nverts_out)
+{
+    if (!d_beg || !d_csr || !nedges || (n && (!src || !dst))) return GW_ERR_ARG;
+    if (flags & ~(GW_EDGES_SYMMETRIC | GW_EDGES_SORT | GW_EDGES_DEDUP)) return GW_ERR_ARG;
+    const bool symmetric = flags & GW_EDGES_SYMMETRIC;
+    const bool dedup = flags & GW_EDGES_DEDUP;
+    const bool sorted = dedup || (flags & GW_EDGES_SORT);
+    if (n > (symmetric ? (1ull << 62) : (1ull << 63)) / sizeof(uint64_t)) return GW_ERR_ARG;
+    const uint64_t m = n * (symmetric ? 2 : 1);
+    int rc = GW_OK;
+    cudaStream_t s = 0;
+    uint64_t *keys = nullptr, *alt = nullptr, *beg = nullptr;
+    uint32_t *csr = nullptr, *stage = nullptr;
+    unsigned int *d_max = nullptr, *d_err = nullptr;
+    unsigned long long *d_kept = nullptr;
+    int64_t *d_nsel = nullptr;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0, tb2 = 0;
+    unsigned int h_max = 0, h_err = 0;
+    unsigned long long h_kept = 0;
+    uint64_t U = 0;
+    uint32_t V = nverts, bits = 0;
+    const uint32_t lim = nverts ? nverts : 0xFFFFFFFFu;
+    const int blocks = 148 * 16, threads = 256;
+    // Host inputs are staged in chunks; device (or managed) inputs are read in place.
+    const bool in_place = n == 0 || (device_accessible(src) && device_accessible(dst));
+    const uint64_t chunk = in_place ? (n ? n : 1) : std::min<uint64_t>(n, 1ull << 26);
+
+    GEN_CHECK(cudaMalloc(&keys, (m ? m : 1) * sizeof(uint64_t)));
+    GEN_CHECK(cudaMalloc(&alt, (m ? m : 1) * sizeof(uint64_t)));
+    GEN_CHECK(cudaMalloc(&d_max, 2 * sizeof(unsigned int)));
+    GEN_CHECK(cudaMalloc(&d_kept, sizeof(unsigned long long)));
+    GEN_CHECK(cudaMalloc(&d_nsel, sizeof(int64_t)));
+    d_err = d_max + 1;
+    GEN_CHECK(cudaMemsetAsync(d_max, 0, 2 * sizeof(unsigned int), s));
+    GEN_CHECK(cudaMemsetAsync(d_kept, 0, sizeof(unsigned long long), s));
+    if (!in_place) GEN_CHECK(cudaMalloc(&stage, 2 * chunk * sizeof(uint32_t)));
+    for (uint64_t i0 = 0; i0 < n; i0 += chunk) {
+        const uint64_t k = std::min(chunk, n - i0);
+        const uint32_t *ps = src + i0, *pd = dst + i0;
+        if (!in_place) {
+            GEN_CHECK(cudaMemcpyAsync(stage, src + i0, k * sizeof(uint32_t), cudaMemcpyDefault, s));
+            GEN_CHECK(cudaMemcpyAsync(stage + chunk, dst + i0, k * sizeof(uint32_t), cudaMemcpyDefault, s));
+            ps = stage;
+            pd = stage + chunk;
+        }
+        k_edge_keys<<<blocks, threads, 0, s>>>(ps, pd, k, i0, lim, symmetric ? 1 : 0, keys, d_max, d_kept, d_err);
+        GEN_CHECK(cudaGetLastError());
+    }
+    GEN_CHECK(cudaMemcpyAsync(&h_max, d_max, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    GEN_CHECK(cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    GEN_CHECK(cudaMemcpyAsync(&h_kept, d_kept, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    GEN_CHECK(cudaStreamSynchronize(s));
+    if (h_err) {
+        rc = GW_ERR_ARG;
+        goto done;
+    }
+    if (!nverts) V = h_kept ? h_max + 1 : 0;
+    U = h_kept * (symmetric ? 2 : 1);
+    bits = bit_length32(V);
+    if (U) {
+        // Kept sources are < V <= 2^bits - 1, the marker's source digit, so a
+        // sort covering bits [32, 32+bits) leaves the m - U markers last.
+        const int b0 = sorted ? 0 : 32, b1 = 32 + (int)bits;
+        GEN_CHECK(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, keys, alt, m, b0, b1, s));
+        if (dedup) {
+            GEN_CHECK(cub::DeviceSelect::Unique(nullptr, tb2, alt, keys, d_nsel, (int64_t)U, s));
+            tmp_bytes = std::max(tmp_bytes, tb2);
+        }
+        GEN_CHECK(cudaMalloc(&tmp, tmp_bytes));
+        GEN_CHECK(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, keys, alt, m, b0, b1, s));
+        std::swap(keys, alt);
+        if (dedup) {
+            int64_t nsel = 0;
+            GEN_CHECK(cub::DeviceSelect::Unique(tmp, tmp_bytes, keys, alt, d_nsel, (int64_t)U, s));
+            GEN_CHECK(cudaMemcpyAsync(&nsel, d_nsel, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+            GEN_CHECK(cudaStreamSynchronize(s));
+            std::swap(keys, alt);
+            U = (uint64_t)nsel;
+        }
+    }
+    GEN_CHECK(csr_from_sorted(keys, U, V, s, &beg, &csr));
+    *d_beg = beg;
+    *d_csr = csr;
+    *nedges = U;
+    if (nverts_out) *nverts_out = V;
+    beg = nullptr;
+    csr = nullptr;
+done:
+    cudaFree(keys);
+    cudaFree(alt);
+    cudaFree(stage);
+    cudaFree(tmp);
+    cudaFree(d_max);
+    cudaFree(d_kept);
+    cudaFree(d_nsel);
+    cudaFree(beg);
+    cudaFree(csr);
+    return rc;
+}
+
+extern "C" int gw_split_blocks(const uint64_t *beg, uint32_t nverts, uint32_t mode, uint64_t param,
+                               uint32_t *vblocks, uint64_t *eblocks, uint32_t cap, uint32_t *nblocks)
+{
+    if (!beg || !vblocks || !eblocks || !nblocks || cap == 0xFFFFFFFFu) return GW_ERR_ARG;
+    if (mode != GW_SPLIT_REFERENCE && mode != GW_SPLIT_EQUAL_EDGES) return GW_ERR_ARG;
+    if (mode == GW_SPLIT_EQUAL_EDGES && (param < 1 || param > nverts)) return GW_ERR_ARG;
+    int rc = GW_OK;
+    cudaStream_t s = 0;
+    const uint64_t nv = (uint64_t)nverts + 1;
+    const uint64_t *d_beg = beg;
+    uint64_t *own = nullptr, *d_eb = nullptr;
+    uint32_t *d_vb = nullptr, *d_count = nullptr;
+    uint64_t b0 = 0;
+    uint32_t count = 0;
+    const uint64_t slots = mode == GW_SPLIT_EQUAL_EDGES ? param + 1 : (uint64_t)cap + 1;
+    if (!device_accessible(beg)) {
+        GEN_CHECK(cudaMalloc(&own, nv * sizeof(uint64_t)));
+        GEN_CHECK(cudaMemcpy(own, beg, nv * sizeof(uint64_t), cudaMemcpyDefault));
+        d_beg = own;
+    }
+    GEN_CHECK(cudaMemcpy(&b0, d_beg, sizeof(uint64_t), cudaMemcpyDefault));
+    if (b0 != 0) {
+        rc = GW_ERR_ARG;
+        goto done;
+    }
+    GEN_CHECK(cudaMalloc(&d_vb, slots * sizeof(uint32_t)));
+    GEN_CHECK(cudaMalloc(&d_eb, slots * sizeof(uint64_t)));
+    GEN_CHECK(cudaMalloc(&d_count, sizeof(uint32_t)));
+    if (mode == GW_SPLIT_REFERENCE) {
+        k_split_reference<<<1, 32, 0, s>>>(d_beg, nv, param / sizeof(uint32_t), param / sizeof(uint64_t), cap, d_vb,
+                                           d_eb, d_count);
+        GEN_CHECK(cudaGetLastError());
+        GEN_CHECK(cudaMemcpyAsync(&count, d_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        GEN_CHECK(cudaStreamSynchronize(s));
+    } else {
+        count = (uint32_t)param;
+        k_split_equal<<<1, 1024, 0, s>>>(d_beg, nverts, count, d_vb, d_eb);
+        GEN_CHECK(cudaGetLastError());
+        GEN_CHECK(cudaStreamSynchronize(s));
+    }
+    *nblocks = count;
+    if (count > cap) {
+        rc = GW_ERR_ARG;
+        goto done;
+    }
+    GEN_CHECK(cudaMemcpy(vblocks, d_vb, ((uint64_t)count + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    GEN_CHECK(cudaMemcpy(eblocks, d_eb, ((uint64_t)count + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+done:
+    cudaFree(own);
+    cudaFree(d_vb);
+    cudaFree(d_eb);
+    cudaFree(d_count);
     return rc;
 }
 

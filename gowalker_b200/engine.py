@@ -167,12 +167,14 @@ class WalkEngine:
 
 
 class DeviceGraph:
-    """CSR built on the device by gw_rmat_csr; frees itself."""
+    """CSR built on the device (gw_rmat_csr, or gw_edges_csr through
+    ``from_edges``); frees itself."""
 
     def __init__(self, scale, nverts=None, nsamples=None, edgefactor=16, abc=(0.57, 0.19, 0.19), seed=1,
                  symmetric=True, target_edges=0):
         L = _abi.load()
         self.L = L
+        self.beg_ptr = self.csr_ptr = None
         nverts = (1 << scale) if nverts is None else nverts
         nsamples = (edgefactor << scale) if nsamples is None else nsamples
         a, b, c = abc
@@ -185,6 +187,47 @@ class DeviceGraph:
             raise GwError(st, "gw_rmat_csr failed")
         self.nverts, self.nedges = nverts, int(ne.value)
         self.beg_ptr, self.csr_ptr = db.value, dc.value
+
+    @classmethod
+    def from_edges(cls, src, dst, nverts=0, symmetric=False, sort=True, dedup=False):
+        """CSR of the edge list (src[i], dst[i]) built on the device by
+        gw_edges_csr (the reference converter plus its neighbour sort,
+        preprocess/graph_converter.hpp:286-449, preprocess/precompute.hpp:42-133).
+        src / dst: u32 numpy arrays (host) or objects with ``data_ptr()``
+        (device tensors of 4-byte ints).  nverts 0 takes the largest id + 1."""
+        L = _abi.load()
+        self = cls.__new__(cls)
+        self.L = L
+        self.beg_ptr = self.csr_ptr = None
+        keep = []
+
+        def ptr(a):
+            if hasattr(a, "data_ptr"):
+                if a.element_size() != 4 or not a.is_contiguous():
+                    raise ValueError("edge arrays must be contiguous 4-byte integers")
+                return a.data_ptr(), a.numel()
+            a = np.ascontiguousarray(a, dtype=np.uint32)
+            keep.append(a)
+            return a.ctypes.data, a.size
+
+        ps, n = ptr(src)
+        pd, nd = ptr(dst)
+        if n != nd:
+            raise ValueError("src and dst differ in length")
+        flags = ((_abi.GW_EDGES_SYMMETRIC if symmetric else 0) | (_abi.GW_EDGES_SORT if sort else 0) |
+                 (_abi.GW_EDGES_DEDUP if dedup else 0))
+        db, dc, ne, nv = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_uint64(), ctypes.c_uint32()
+        st = L.gw_edges_csr(ctypes.c_void_p(ps), ctypes.c_void_p(pd), n, nverts, flags, ctypes.byref(db),
+                            ctypes.byref(dc), ctypes.byref(ne), ctypes.byref(nv))
+        if st != 0:
+            raise GwError(st, "gw_edges_csr failed")
+        self.nverts, self.nedges = int(nv.value), int(ne.value)
+        self.beg_ptr, self.csr_ptr = db.value, dc.value
+        return self
+
+    def split(self, mode=_abi.GW_SPLIT_REFERENCE, param=1024 << 20, cap=1 << 16):
+        """Block split points (vblocks u32, eblocks u64) from the resident offsets."""
+        return split_blocks_device(ctypes.c_void_p(self.beg_ptr), self.nverts, mode, param, cap)
 
     def to_host(self, pinned=False):
         """Copy to host numpy arrays (or pinned torch tensors)."""
@@ -216,3 +259,24 @@ class DeviceGraph:
             self.free()
         except Exception:
             pass
+
+
+def split_blocks_device(beg, nverts, mode=_abi.GW_SPLIT_REFERENCE, param=1024 << 20, cap=1 << 16):
+    """gw_split_blocks: the reference splitter (param = block size in bytes,
+    preprocess/split.hpp:15-87) or equal edge mass (param = block count), run
+    on the device over offsets in host (numpy) or device memory (a pointer)."""
+    L = _abi.load()
+    if isinstance(beg, np.ndarray):
+        beg = np.ascontiguousarray(beg, dtype=np.uint64)
+        p = ctypes.c_void_p(beg.ctypes.data)
+    else:
+        p = beg
+    vb = np.zeros(cap + 1, dtype=np.uint32)
+    eb = np.zeros(cap + 1, dtype=np.uint64)
+    nb = ctypes.c_uint32()
+    st = L.gw_split_blocks(p, nverts, mode, param, ctypes.c_void_p(vb.ctypes.data), ctypes.c_void_p(eb.ctypes.data),
+                           cap, ctypes.byref(nb))
+    if st != 0:
+        raise GwError(st, "gw_split_blocks failed (%d blocks)" % nb.value)
+    k = int(nb.value)
+    return vb[: k + 1].copy(), eb[: k + 1].copy()

@@ -115,7 +115,7 @@ def split_equal_edge_mass(beg: np.ndarray, nblocks: int):
     E = int(beg[-1])
     if nblocks < 1 or nblocks > V:
         raise ValueError("need 1 <= nblocks <= nvertices")
-    targets = (np.arange(1, nblocks, dtype=np.float64) * E / nblocks).astype(np.uint64)
+    targets = np.array([k * E // nblocks for k in range(1, nblocks)], dtype=np.uint64)
     cuts = np.searchsorted(beg[:-1], targets, side="left").astype(np.int64)
     cuts = np.maximum.accumulate(np.clip(cuts, 1, max(V - 1, 1)))
     vb = np.concatenate([[0], cuts, [V]]).astype(np.int64)

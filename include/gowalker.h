@@ -221,6 +221,45 @@ int gw_bucket_counts(gw_handle *h, uint32_t *out);
 int gw_rmat_csr(uint32_t scale, uint32_t nverts, uint64_t nsamples, const uint32_t thr[3], uint64_t seed,
                 int symmetric, uint64_t target_edges, uint64_t **d_beg, uint32_t **d_csr, uint64_t *nedges);
 
+/* Edge list -> CSR on the device, in place of the reference's text-to-CSR
+ * pass (graph_converter::convert, preprocess/graph_converter.hpp:286-449) and
+ * its optional neighbour sort (sort_vertex_neighbors,
+ * preprocess/precompute.hpp:42-133).  Edge i is (src[i], dst[i]); both
+ * arrays may be host or device memory.  Self loops are dropped
+ * (graph_converter.hpp:362-363).  Flags:
+ *   GW_EDGES_SYMMETRIC  edge i also yields (dst[i], src[i]), right after it;
+ *   GW_EDGES_SORT       each vertex's neighbours ascending (the `sorted` flag);
+ *                       without it a vertex keeps its edges in input order,
+ *                       which for a source-sorted list is the converter's CSR;
+ *   GW_EDGES_DEDUP      repeated (src, dst) pairs kept once (implies SORT).
+ * nverts 0 takes the largest id of a kept edge + 1 (the converter's
+ * max_vert + 1); otherwise an id >= nverts fails with GW_ERR_ARG, as does an
+ * id of 2^32-1 (no u32 vertex count covers it).  Allocates *d_beg (nverts+1
+ * u64) and *d_csr (max(nedges,1) u32) on the current device; free them with
+ * gw_device_free. */
+#define GW_EDGES_SYMMETRIC 1u
+#define GW_EDGES_SORT 2u
+#define GW_EDGES_DEDUP 4u
+int gw_edges_csr(const uint32_t *src, const uint32_t *dst, uint64_t n, uint32_t nverts, uint32_t flags,
+                 uint64_t **d_beg, uint32_t **d_csr, uint64_t *nedges, uint32_t *nverts_out);
+
+/* Block split points over CSR offsets beg[0..nverts] (host or device
+ * memory), computed on the device.
+ *   GW_SPLIT_REFERENCE   param = block size in bytes: the reference splitter
+ *                        (split_blocks, preprocess/split.hpp:15-87), which cuts
+ *                        when a block's edges pass param/4 (one vertex back) or
+ *                        its vertices reach param/8;
+ *   GW_SPLIT_EQUAL_EDGES param = block count: block k ends at the first vertex
+ *                        whose offset reaches floor(k*E/param), at least one
+ *                        vertex per block.
+ * Writes nblocks+1 entries to vblocks (u32) and eblocks (u64), host memory
+ * with room for cap+1 each; *nblocks gets the block count.  When it exceeds
+ * cap nothing is written and the call fails with GW_ERR_ARG. */
+#define GW_SPLIT_REFERENCE 0u
+#define GW_SPLIT_EQUAL_EDGES 1u
+int gw_split_blocks(const uint64_t *beg, uint32_t nverts, uint32_t mode, uint64_t param, uint32_t *vblocks,
+                    uint64_t *eblocks, uint32_t cap, uint32_t *nblocks);
+
 int gw_device_free(void *p);
 
 /* Pinned host memory for graph blocks and walker batches, in place of the

@@ -9,7 +9,9 @@ Contents:
     counter-based R-MAT sampler and the Node2vec / SOPR / SOSR whole-walk
     restatement of engine/engine.hpp:158-404;
   * a numpy CSR builder (drop self loops, optional symmetrisation, dedup,
-    sorted adjacency) for the synthetic R-MAT graphs;
+    sorted adjacency) for the synthetic R-MAT graphs, the edge-list converter
+    restatement (convert_edges) and a line-by-line one of the reference's
+    streaming converter (convert_stream) that pins it;
   * writers for the reference's on-disk format: ``<base>.beg`` (u64, V+1),
     ``<base>.csr`` (u32, E), ``<base>.meta`` (packed u32 nvertices, u64 nedges,
     u32 min_vert; preprocess/graph_converter.hpp finalize()), and the block
@@ -156,6 +158,76 @@ def build_csr(nverts: int, src: np.ndarray, dst: np.ndarray, symmetric: bool = T
     return beg, csr
 
 
+def convert_edges(src, dst, nverts: int = 0, symmetric: bool = False, sort: bool = False, dedup: bool = False):
+    """Edge list -> (beg, csr, nverts): the reference's converter
+    (graph_converter::convert, preprocess/graph_converter.hpp:286-449) with
+    its optional neighbour sort (sort_vertex_neighbors,
+    preprocess/precompute.hpp:42-133), generalised to lists that are not
+    source-sorted.  Self loops are dropped (graph_converter.hpp:362-363).
+    Without ``sort`` a vertex keeps its edges in input order (a stable sort
+    by source); ``symmetric`` puts (dst, src) right after each edge; ``dedup``
+    keeps one copy of each (src, dst) and implies ``sort``.  nverts 0 means
+    the largest kept id + 1.  Raises ValueError on an id >= nverts (or
+    2^32-1, when nverts is 0)."""
+    src = np.asarray(src, dtype=np.uint64)
+    dst = np.asarray(dst, dtype=np.uint64)
+    lim = nverts if nverts else 0xFFFFFFFF
+    if len(src) and (int(src.max()) >= lim or int(dst.max()) >= lim):
+        raise ValueError("vertex id out of range")
+    keep = src != dst
+    src, dst = src[keep], dst[keep]
+    if symmetric:
+        src, dst = np.stack([src, dst], 1).reshape(-1), np.stack([dst, src], 1).reshape(-1)
+    if not nverts:
+        nverts = int(max(src.max(), dst.max())) + 1 if len(src) else 0
+    keys = (src << np.uint64(32)) | dst
+    if dedup:
+        keys = np.unique(keys)
+    elif sort:
+        keys = np.sort(keys, kind="stable")
+    else:
+        keys = keys[np.argsort(keys >> np.uint64(32), kind="stable")]
+    s = (keys >> np.uint64(32)).astype(np.int64)
+    beg = np.zeros(nverts + 1, dtype=np.uint64)
+    beg[1:] = np.cumsum(np.bincount(s, minlength=nverts)).astype(np.uint64)
+    return beg, (keys & np.uint64(0xFFFFFFFF)).astype(np.uint32), nverts
+
+
+def convert_stream(edges, sort: bool = False):
+    """Line-by-line restatement of the converter's streaming loop for a
+    source-sorted list (graph_converter.hpp:167-216 convert, 220-226
+    dealfirstline, 257-263 finalize), pure Python for small inputs: pins
+    convert_edges.  Returns (beg, csr, nverts) with nverts = max_vert + 1."""
+    beg, csr = [0], []
+    adj, curr, max_vert, first = [], 0, 0, True
+    for frm, to in edges:
+        if first:
+            if frm != 0:
+                beg.extend([0] * frm)  # sync_zeros(from)
+                curr = frm
+            first = False
+        if frm == to:
+            continue
+        max_vert = max(max_vert, frm, to)
+        if frm == curr:
+            adj.append(to)
+        elif frm < curr:
+            raise ValueError("edge list is not source-sorted")
+        else:
+            csr.extend(adj)
+            beg.append(len(csr))
+            beg.extend([len(csr)] * (frm - curr - 1))
+            curr, adj = frm, [to]
+    csr.extend(adj)
+    beg.append(len(csr))
+    if max_vert > curr:
+        beg.extend([len(csr)] * (max_vert - curr))
+    if sort:
+        for v in range(len(beg) - 1):
+            csr[beg[v]:beg[v + 1]] = sorted(csr[beg[v]:beg[v + 1]])
+    return np.array(beg, dtype=np.uint64), np.array(csr, dtype=np.uint32), len(beg) - 1
+
+
 def rmat_graph(scale: int, edgefactor: int = 16, seed: int = 1, abc=RMAT_ABC, symmetric: bool = True):
     """Synthetic R-MAT graph: (edgefactor << scale) counter-based samples."""
     n = edgefactor << scale
@@ -272,7 +344,7 @@ def split_equal_edge_mass(beg: np.ndarray, nblocks: int):
     first vertex whose offset reaches b*E/nblocks."""
     V = len(beg) - 1
     E = int(beg[-1])
-    targets = (np.arange(1, nblocks, dtype=np.float64) * E / nblocks).astype(np.uint64)
+    targets = np.array([k * E // nblocks for k in range(1, nblocks)], dtype=np.uint64)
     cuts = np.searchsorted(beg[:-1], targets, side="left").astype(np.int64)
     cuts = np.maximum.accumulate(np.clip(cuts, 1, max(V - 1, 1)))
     vb = np.concatenate([[0], cuts, [V]]).astype(np.int64)

@@ -243,3 +243,51 @@ def test_transition_law_chi_square(oracle, tmp_path, algo):
     assert pvalue(ours) > 1e-3
     assert pvalue(res[False]) > 1e-3
     assert pvalue(res[True]) < 1e-4
+
+
+@pytest.mark.parametrize("sort", [False, True])
+@pytest.mark.parametrize("case", range(6))
+def test_convert_edges_pinned_by_streaming_converter(oracle, sort, case):
+    """The vectorised converter restatement equals a line-by-line replay of
+    the reference's streaming converter (graph_converter.hpp:167-263) on
+    source-sorted lists with self loops, repeats, gaps, a first source > 0
+    and a largest id that only appears as a destination."""
+    rng = np.random.default_rng(100 + case)
+    nv = [5, 17, 64, 300, 1000, 40][case]
+    n = [8, 40, 500, 3000, 2000, 200][case]
+    src = np.sort(rng.integers(case % 3, nv - 1, n)).astype(np.uint32)
+    dst = rng.integers(0, nv, n).astype(np.uint32)
+    loops = rng.random(n) < 0.1
+    dst[loops] = src[loops]
+    rep = rng.random(n) < 0.2  # repeat the previous edge
+    rep[0] = False
+    for i in np.nonzero(rep)[0]:
+        if src[i] == src[i - 1]:
+            dst[i] = dst[i - 1]
+    dst[-1] = nv - 1 if src[-1] != nv - 1 else 0  # largest id as a destination only
+    edges = list(zip(src.tolist(), dst.tolist()))
+    b1, c1, n1 = oracle.convert_stream(edges, sort=sort)
+    b2, c2, n2 = oracle.convert_edges(src, dst, 0, symmetric=False, sort=sort)
+    assert n1 == n2
+    assert np.array_equal(b1, b2) and np.array_equal(c1, c2)
+    if sort:
+        oracle.check_csr(b2, c2)
+
+
+def test_convert_edges_dedup_symmetric_is_build_csr(oracle):
+    rng = np.random.default_rng(7)
+    src = rng.integers(0, 500, 20000).astype(np.uint32)
+    dst = rng.integers(0, 500, 20000).astype(np.uint32)
+    b1, c1 = oracle.build_csr(500, src, dst, symmetric=True)
+    b2, c2, nv = oracle.convert_edges(src, dst, 500, symmetric=True, dedup=True)
+    assert nv == 500 and np.array_equal(b1, b2) and np.array_equal(c1, c2)
+    with pytest.raises(ValueError):
+        oracle.convert_edges(src, dst, 499)
+
+
+def test_split_equal_edge_mass_integer_targets(oracle):
+    """The equal-edge-mass cut targets are floor(k*E/nblocks) in integers."""
+    beg = np.array([0, 3, 3, 10, 11, 20, 20, 21], dtype=np.uint64)
+    vb, eb = oracle.split_equal_edge_mass(beg, 3)
+    # targets 7 and 14: first offsets >= them are beg[3]=10 and beg[5]=20
+    assert vb.tolist() == [0, 3, 5, 7] and eb.tolist() == [0, 10, 20, 21]
