@@ -431,7 +431,8 @@ def run_prep_bench(args, wl):
             "config": {"workload": wl["name"], "vertices": V, "samples": n, "edges_out": ne,
                        "l2": "inputs larger than L2 (2 GB of pairs)"},
             "gpu_launches": 2,
-            "library_launches": "CUB radix sort (8-bit digits over 32 + bit_length(V) key bits), unique, scan",
+            "library_launches": "CUB radix sort (8-bit digits over the 2 x bit_length(V-1) bits of the packed "
+                                "(src, dst) key), unique, scan",
             "e2e": {"value": n / (ems / 1e3), "unit": "samples/s", "h2d_bytes_per_step": 8 * n,
                     "d2h_bytes_per_step": 8 * (V + 1) + 4 * ne},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",

@@ -18,7 +18,10 @@
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
 #include <algorithm>
+#include <chrono>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include "gw_philox.cuh"
 #include "../../include/gowalker.h"
 
@@ -66,51 +69,114 @@ __global__ void k_thin(const uint64_t *in, uint64_t U, uint64_t k, uint64_t *out
     }
 }
 
-// Degrees from the runs of a source-sorted key list: the first key of a run
-// adds -i and the last adds i+1 to cnt[src] (mod 2^64), so cnt[v] ends as the
-// run length; two uncontended atomics per vertex whatever the gaps between
-// sources.  csr[i] = low word of key i.
-__global__ void k_runs(const uint64_t *__restrict__ keys, uint64_t n, unsigned long long *cnt,
+// Degrees from the runs of a source-sorted key list (key = src << sh | dst):
+// the first key of a run adds -i and the last adds i+1 to cnt[src] (mod 2^64),
+// so cnt[v] ends as the run length; two uncontended atomics per vertex
+// whatever the gaps between sources.  csr[i] = dst of key i.
+__global__ void k_runs(const uint64_t *__restrict__ keys, uint64_t n, uint32_t sh, unsigned long long *cnt,
                        uint32_t *__restrict__ csr)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t mask = (1ull << sh) - 1;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint64_t k = keys[i];
+        const uint64_t s = k >> sh;
+        if (i == 0 || (keys[i - 1] >> sh) != s) atomicAdd(cnt + s, 0ull - (unsigned long long)i);
+        if (i + 1 == n || (keys[i + 1] >> sh) != s) atomicAdd(cnt + s, (unsigned long long)(i + 1));
+        csr[i] = (uint32_t)(k & mask);
+    }
+}
+
+// key = src << 32 | dst  ->  src << sh | dst (dst < 2^sh), in place.
+__global__ void k_repack(uint64_t *keys, uint64_t n, uint32_t sh)
 {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint64_t k = keys[i];
-        const uint32_t s = (uint32_t)(k >> 32);
-        if (i == 0 || (uint32_t)(keys[i - 1] >> 32) != s) atomicAdd(cnt + s, 0ull - (unsigned long long)i);
-        if (i + 1 == n || (uint32_t)(keys[i + 1] >> 32) != s) atomicAdd(cnt + s, (unsigned long long)(i + 1));
-        csr[i] = (uint32_t)k;
+        keys[i] = ((k >> 32) << sh) | (k & 0xFFFFFFFFull);
     }
 }
 
-// Edge list -> keys at fixed positions (edge i at i, or at 2i and 2i+1 when
-// symmetric) so a stable sort by source keeps input order.  Self loops and
-// out-of-range ids become the marker ~0, which sorts after every kept key for
-// any sort that covers bit 32 + bit_length(nverts) - 1 (no kept source reaches
-// 2^b - 1).  Per-thread maximum id and kept count are folded with one atomic
-// per warp at the end.
-__global__ void k_edge_keys(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst, uint64_t n,
-                            uint64_t first, uint32_t lim, int symmetric, uint64_t *__restrict__ keys,
-                            unsigned int *max_id, unsigned long long *nkept, unsigned int *range_err)
+constexpr int kKeyThreads = 256, kKeyItems = 4;
+
+// Edge list -> sort keys src << sh | dst (edge i and, when symmetric, its
+// reverse).  Self loops and out-of-range ids are dropped.
+//   COMPACT  kept keys go to a dense prefix of `keys` (a block claims its
+//            range with one atomic per 1024 edges; order inside is arbitrary,
+//            which a sort over the whole key makes irrelevant).
+//   !COMPACT edge i at position i (2i and 2i+1 when symmetric), dropped ones
+//            as the marker ~0, so a stable sort by source keeps input order;
+//            with sh = 32 the marker sorts after every kept key for any sort
+//            covering bit 32 + bit_length(nverts) - 1 (no kept source
+//            reaches 2^b - 1).
+// Per-thread maximum id and kept count are folded with one atomic per warp.
+template <bool COMPACT>
+__global__ void __launch_bounds__(kKeyThreads)
+    k_edge_keys(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst, uint64_t n, uint64_t first,
+                uint32_t lim, uint32_t sh, int symmetric, uint64_t *__restrict__ keys,
+                unsigned long long *cursor, unsigned int *max_id, unsigned long long *nkept,
+                unsigned int *range_err)
 {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    __shared__ unsigned int s_cnt;
+    __shared__ unsigned long long s_base;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t per = symmetric ? 2 : 1;
+    const uint64_t span = (uint64_t)kKeyThreads * kKeyItems;
     uint32_t mx = 0, bad = 0;
     uint64_t kept = 0;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint32_t s = __ldg(src + i), d = __ldg(dst + i);
-        const bool in_range = s < lim && d < lim;
-        const bool ok = in_range && s != d;
-        bad |= in_range ? 0u : 1u;
-        if (ok) {
-            mx = max(mx, max(s, d));
-            ++kept;
+    for (uint64_t b0 = (uint64_t)blockIdx.x * span; b0 < n; b0 += (uint64_t)gridDim.x * span) {
+        uint32_t sv[kKeyItems], dv[kKeyItems];
+        bool ok[kKeyItems];
+        uint32_t c = 0;
+#pragma unroll
+        for (int k = 0; k < kKeyItems; ++k) {
+            const uint64_t i = b0 + (uint64_t)k * kKeyThreads + threadIdx.x;
+            sv[k] = dv[k] = 0;
+            ok[k] = false;
+            if (i < n) {
+                sv[k] = __ldg(src + i);
+                dv[k] = __ldg(dst + i);
+                const bool in_range = sv[k] < lim && dv[k] < lim;
+                ok[k] = in_range && sv[k] != dv[k];
+                bad |= in_range ? 0u : 1u;
+                if (ok[k]) mx = max(mx, max(sv[k], dv[k]));
+            }
+            c += ok[k] ? 1u : 0u;
         }
-        const uint64_t j = first + i;
-        if (symmetric) {
-            keys[2 * j] = ok ? (((uint64_t)s << 32) | d) : ~0ull;
-            keys[2 * j + 1] = ok ? (((uint64_t)d << 32) | s) : ~0ull;
+        kept += c;
+        if (COMPACT) {
+            if (threadIdx.x == 0) s_cnt = 0;
+            __syncthreads();
+            uint32_t x = c;  // inclusive warp scan of the per-thread counts
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+                if (lane >= (uint32_t)o) x += y;
+            }
+            uint32_t wbase = 0;
+            if (lane == 31) wbase = atomicAdd(&s_cnt, x);
+            wbase = __shfl_sync(0xFFFFFFFFu, wbase, 31);
+            __syncthreads();
+            if (threadIdx.x == 0) s_base = atomicAdd(cursor, (unsigned long long)s_cnt * per);
+            __syncthreads();
+            uint64_t pos = s_base + (uint64_t)(wbase + x - c) * per;
+#pragma unroll
+            for (int k = 0; k < kKeyItems; ++k) {
+                if (!ok[k]) continue;
+                keys[pos] = ((uint64_t)sv[k] << sh) | dv[k];
+                if (symmetric) keys[pos + 1] = ((uint64_t)dv[k] << sh) | sv[k];
+                pos += per;
+            }
+            __syncthreads();  // s_cnt / s_base are reused by the next round
         } else {
-            keys[j] = ok ? (((uint64_t)s << 32) | d) : ~0ull;
+#pragma unroll
+            for (int k = 0; k < kKeyItems; ++k) {
+                const uint64_t i = b0 + (uint64_t)k * kKeyThreads + threadIdx.x;
+                if (i >= n) continue;
+                const uint64_t j = (first + i) * per;
+                keys[j] = ok[k] ? (((uint64_t)sv[k] << sh) | dv[k]) : ~0ull;
+                if (symmetric) keys[j + 1] = ok[k] ? (((uint64_t)dv[k] << sh) | sv[k]) : ~0ull;
+            }
         }
     }
 #pragma unroll
@@ -119,7 +185,7 @@ __global__ void k_edge_keys(const uint32_t *__restrict__ src, const uint32_t *__
         bad |= __shfl_xor_sync(0xFFFFFFFFu, bad, o);
         kept += __shfl_xor_sync(0xFFFFFFFFu, kept, o);
     }
-    if ((threadIdx.x & 31u) == 0) {
+    if (lane == 0) {
         if (kept) {
             atomicMax(max_id, mx);
             atomicAdd(nkept, (unsigned long long)kept);
@@ -229,9 +295,9 @@ __global__ void k_split_equal(const uint64_t *beg, uint32_t V, uint32_t nblocks,
     }
 }
 
-// offsets + neighbour ids from n sorted keys (sources < nverts).  Allocates
-// *beg_out and *csr_out; s is synchronised before return.
-static cudaError_t csr_from_sorted(const uint64_t *keys, uint64_t n, uint32_t nverts, cudaStream_t s,
+// offsets + neighbour ids from n sorted keys src << sh | dst (sources <
+// nverts).  Allocates *beg_out and *csr_out; s is synchronised before return.
+static cudaError_t csr_from_sorted(const uint64_t *keys, uint64_t n, uint32_t sh, uint32_t nverts, cudaStream_t s,
                                    uint64_t **beg_out, uint32_t **csr_out)
 {
     unsigned long long *cnt = nullptr;
@@ -247,7 +313,7 @@ static cudaError_t csr_from_sorted(const uint64_t *keys, uint64_t n, uint32_t nv
         if ((e = cudaMalloc(&csr, (n ? n : 1) * sizeof(uint32_t))) != cudaSuccess) break;
         if ((e = cudaMemsetAsync(cnt, 0, nb * sizeof(uint64_t), s)) != cudaSuccess) break;
         if (n) {
-            k_runs<<<148 * 16, 256, 0, s>>>(keys, n, cnt, csr);
+            k_runs<<<148 * 16, 256, 0, s>>>(keys, n, sh, cnt, csr);
             if ((e = cudaGetLastError()) != cudaSuccess) break;
         }
         if ((e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, (const uint64_t *)cnt, beg, nb, s)) != cudaSuccess)
@@ -280,6 +346,29 @@ static bool device_accessible(const void *p)
     }
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
+
+// Phase times of a conversion on stderr when GOWALKER_TRACE is set (each mark
+// synchronises the stream, so tracing slows the call down).
+struct PhaseTrace {
+    bool on;
+    cudaStream_t s;
+    std::chrono::steady_clock::time_point t0;
+    explicit PhaseTrace(cudaStream_t st) : s(st)
+    {
+        const char *e = getenv("GOWALKER_TRACE");
+        on = e && *e && *e != '0';
+        t0 = std::chrono::steady_clock::now();
+    }
+    void mark(const char *what)
+    {
+        if (!on) return;
+        cudaStreamSynchronize(s);
+        const auto t = std::chrono::steady_clock::now();
+        fprintf(stderr, "[gowalker] gw_edges_csr %-10s %9.3f ms\n", what,
+                std::chrono::duration<double, std::milli>(t - t0).count());
+        t0 = t;
+    }
+};
 
 }  // namespace gw
 
@@ -341,7 +430,7 @@ extern "C" int gw_rmat_csr(uint32_t scale, uint32_t nverts, uint64_t nsamples, c
             U = target_edges;
         }
     }
-    GEN_CHECK(csr_from_sorted(keys, U, nverts, s, &beg, &csr));
+    GEN_CHECK(csr_from_sorted(keys, U, 32, nverts, s, &beg, &csr));
     *d_beg = beg;
     *d_csr = csr;
     *nedges = U;
@@ -369,32 +458,38 @@ extern "C" int gw_edges_csr(const uint32_t *src, const uint32_t *dst, uint64_t n
     const uint64_t m = n * (symmetric ? 2 : 1);
     int rc = GW_OK;
     cudaStream_t s = 0;
+    PhaseTrace trace(s);
     uint64_t *keys = nullptr, *alt = nullptr, *beg = nullptr;
     uint32_t *csr = nullptr, *stage = nullptr;
     unsigned int *d_max = nullptr, *d_err = nullptr;
-    unsigned long long *d_kept = nullptr;
+    unsigned long long *d_cnt = nullptr;  // [0] kept edges, [1] compaction cursor
     int64_t *d_nsel = nullptr;
     void *tmp = nullptr;
     size_t tmp_bytes = 0, tb2 = 0;
     unsigned int h_max = 0, h_err = 0;
     unsigned long long h_kept = 0;
     uint64_t U = 0;
-    uint32_t V = nverts, bits = 0;
+    uint32_t V = nverts, sh = 32;
     const uint32_t lim = nverts ? nverts : 0xFFFFFFFFu;
-    const int blocks = 148 * 16, threads = 256;
+    const int threads = kKeyThreads;
+    int blocks = 148 * 8;
     // Host inputs are staged in chunks; device (or managed) inputs are read in place.
     const bool in_place = n == 0 || (device_accessible(src) && device_accessible(dst));
     const uint64_t chunk = in_place ? (n ? n : 1) : std::min<uint64_t>(n, 1ull << 26);
+    // Sorted output: compacted keys, packed as src << bit_length(nverts-1) | dst
+    // when nverts is given (otherwise repacked once the largest id is known).
+    if (sorted && nverts) sh = bit_length32(nverts - 1);
 
     GEN_CHECK(cudaMalloc(&keys, (m ? m : 1) * sizeof(uint64_t)));
     GEN_CHECK(cudaMalloc(&alt, (m ? m : 1) * sizeof(uint64_t)));
     GEN_CHECK(cudaMalloc(&d_max, 2 * sizeof(unsigned int)));
-    GEN_CHECK(cudaMalloc(&d_kept, sizeof(unsigned long long)));
+    GEN_CHECK(cudaMalloc(&d_cnt, 2 * sizeof(unsigned long long)));
     GEN_CHECK(cudaMalloc(&d_nsel, sizeof(int64_t)));
     d_err = d_max + 1;
     GEN_CHECK(cudaMemsetAsync(d_max, 0, 2 * sizeof(unsigned int), s));
-    GEN_CHECK(cudaMemsetAsync(d_kept, 0, sizeof(unsigned long long), s));
+    GEN_CHECK(cudaMemsetAsync(d_cnt, 0, 2 * sizeof(unsigned long long), s));
     if (!in_place) GEN_CHECK(cudaMalloc(&stage, 2 * chunk * sizeof(uint32_t)));
+    trace.mark("alloc");
     for (uint64_t i0 = 0; i0 < n; i0 += chunk) {
         const uint64_t k = std::min(chunk, n - i0);
         const uint32_t *ps = src + i0, *pd = dst + i0;
@@ -404,32 +499,56 @@ extern "C" int gw_edges_csr(const uint32_t *src, const uint32_t *dst, uint64_t n
             ps = stage;
             pd = stage + chunk;
         }
-        k_edge_keys<<<blocks, threads, 0, s>>>(ps, pd, k, i0, lim, symmetric ? 1 : 0, keys, d_max, d_kept, d_err);
+        const uint64_t need = (k + (uint64_t)kKeyThreads * kKeyItems - 1) / ((uint64_t)kKeyThreads * kKeyItems);
+        blocks = (int)std::min<uint64_t>(need ? need : 1, 148 * 8);
+        if (sorted)
+            k_edge_keys<true><<<blocks, threads, 0, s>>>(ps, pd, k, i0, lim, sh, symmetric ? 1 : 0, keys, d_cnt + 1,
+                                                         d_max, d_cnt, d_err);
+        else
+            k_edge_keys<false><<<blocks, threads, 0, s>>>(ps, pd, k, i0, lim, sh, symmetric ? 1 : 0, keys, d_cnt + 1,
+                                                          d_max, d_cnt, d_err);
         GEN_CHECK(cudaGetLastError());
     }
     GEN_CHECK(cudaMemcpyAsync(&h_max, d_max, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
     GEN_CHECK(cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-    GEN_CHECK(cudaMemcpyAsync(&h_kept, d_kept, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    GEN_CHECK(cudaMemcpyAsync(&h_kept, d_cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     GEN_CHECK(cudaStreamSynchronize(s));
+    trace.mark("keys");
     if (h_err) {
         rc = GW_ERR_ARG;
         goto done;
     }
     if (!nverts) V = h_kept ? h_max + 1 : 0;
     U = h_kept * (symmetric ? 2 : 1);
-    bits = bit_length32(V);
     if (U) {
-        // Kept sources are < V <= 2^bits - 1, the marker's source digit, so a
-        // sort covering bits [32, 32+bits) leaves the m - U markers last.
-        const int b0 = sorted ? 0 : 32, b1 = 32 + (int)bits;
-        GEN_CHECK(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, keys, alt, m, b0, b1, s));
+        int b0, b1;
+        if (sorted) {
+            // compacted: U keys, no markers; sort the packed source and destination bits
+            const uint32_t bv = bit_length32(V - 1);
+            if (sh != bv) {
+                k_repack<<<148 * 8, 256, 0, s>>>(keys, U, bv);
+                GEN_CHECK(cudaGetLastError());
+                sh = bv;
+            }
+            b0 = 0;
+            b1 = (int)(sh + bv);
+        } else {
+            // fixed positions: sort m keys by source only; markers end up last
+            b0 = 32;
+            b1 = 32 + (int)bit_length32(V);
+        }
+        const uint64_t nsort = sorted ? U : m;
+        cub::DoubleBuffer<uint64_t> db(keys, alt);
+        GEN_CHECK(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, nsort, b0, b1, s));
         if (dedup) {
-            GEN_CHECK(cub::DeviceSelect::Unique(nullptr, tb2, alt, keys, d_nsel, (int64_t)U, s));
+            GEN_CHECK(cub::DeviceSelect::Unique(nullptr, tb2, keys, alt, d_nsel, (int64_t)U, s));
             tmp_bytes = std::max(tmp_bytes, tb2);
         }
         GEN_CHECK(cudaMalloc(&tmp, tmp_bytes));
-        GEN_CHECK(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, keys, alt, m, b0, b1, s));
-        std::swap(keys, alt);
+        GEN_CHECK(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, db, nsort, b0, b1, s));
+        keys = db.Current();
+        alt = db.Alternate();
+        trace.mark("sort");
         if (dedup) {
             int64_t nsel = 0;
             GEN_CHECK(cub::DeviceSelect::Unique(tmp, tmp_bytes, keys, alt, d_nsel, (int64_t)U, s));
@@ -437,9 +556,11 @@ extern "C" int gw_edges_csr(const uint32_t *src, const uint32_t *dst, uint64_t n
             GEN_CHECK(cudaStreamSynchronize(s));
             std::swap(keys, alt);
             U = (uint64_t)nsel;
+            trace.mark("unique");
         }
     }
-    GEN_CHECK(csr_from_sorted(keys, U, V, s, &beg, &csr));
+    GEN_CHECK(csr_from_sorted(keys, U, sh, V, s, &beg, &csr));
+    trace.mark("csr");
     *d_beg = beg;
     *d_csr = csr;
     *nedges = U;
@@ -452,10 +573,11 @@ done:
     cudaFree(stage);
     cudaFree(tmp);
     cudaFree(d_max);
-    cudaFree(d_kept);
+    cudaFree(d_cnt);
     cudaFree(d_nsel);
     cudaFree(beg);
     cudaFree(csr);
+    trace.mark("free");
     return rc;
 }
 
