@@ -47,6 +47,11 @@ WORKLOADS = {
                     "rejecting ids >= 41.6M, thinned to 1.47B edges, 64 equal-edge-mass blocks, 1.5 GB device cache",
                scale=26, nverts=41_600_000, target=1_470_000_000, nsamples=2_600_000_000, ef=0, algo=0, maxhops=80,
                wps=1, p=0.5, q=2.0, alpha=0.2, term=0.0, nblocks=64, cache=1_500_000_000, ooc=True),
+    "c3s": dict(name="C3 at 1/16 size (profiling case): out-of-core Node2vec p=0.5 q=2 length 80, 1 walker/vertex, "
+                     "directed R-MAT scale 22 rejecting ids >= 2.6M, thinned to 91.875M edges, 64 equal-edge-mass "
+                     "blocks, 93.75 MB device cache",
+                scale=22, nverts=2_600_000, target=91_875_000, nsamples=162_500_000, ef=0, algo=0, maxhops=80,
+                wps=1, p=0.5, q=2.0, alpha=0.2, term=0.0, nblocks=64, cache=93_750_000, ooc=True),
     "prep": dict(name="edge list -> CSR on the device (gw_edges_csr): R-MAT scale 24 ef 16 sample list "
                       "(268,435,456 u32 pairs, (a,b,c,d) = (0.57,0.19,0.19,0.05)), symmetrised, deduplicated, sorted",
                  scale=24, ef=16, prep=True),
