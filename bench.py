@@ -271,7 +271,7 @@ def run_ooc_bench(args, wl):
     dg.free()
     from gowalker_b200.preprocess import split_equal_edge_mass
     vb, eb = split_equal_edge_mass(beg, wl["nblocks"])
-    policy = gw.GW_POLICY_LEARNED if args.policy == "learned" else gw.GW_POLICY_PLAIN
+    policy = {"plain": gw.GW_POLICY_PLAIN, "learned": gw.GW_POLICY_LEARNED, "sa": gw.GW_POLICY_SA}[args.policy]
     eng = gw.WalkEngine(algorithm=wl["algo"], maxhops=wl["maxhops"], p=wl["p"], q=wl["q"], alpha=wl["alpha"],
                         term_prob=wl["term"], seed=42, walkpersource=wl["wps"], record_paths=1 if args.paths else 0,
                         cache_size=wl["cache"], zero_copy=0, strict_blocks=1 if args.strict_blocks else 0,
@@ -647,7 +647,8 @@ def main():
     ap.add_argument("--paths", type=int, default=1, help="record full paths (1) or hashes only (0)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
-    ap.add_argument("--policy", default="plain", choices=["plain", "learned"], help="block policy (out-of-core)")
+    ap.add_argument("--policy", default="plain", choices=["plain", "learned", "sa"],
+                    help="block policy (out-of-core): GOWalker's rule, the learned predictor, SOWalker's annealing")
     ap.add_argument("--compress", action="store_true",
                     help="out-of-core: copy compressed neighbour lists and decode them on the device")
     ap.add_argument("--prefetch", action="store_true",

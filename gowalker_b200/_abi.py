@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libgowalker.so")
 GW_OK = 0
 GW_NODE2VEC, GW_SOPR, GW_SOSR = 0, 1, 2
 GW_INIT_PER_VERTEX, GW_INIT_SINGLE_SOURCE, GW_INIT_RANDOM = 0, 1, 2
-GW_POLICY_PLAIN, GW_POLICY_LEARNED = 0, 1
+GW_POLICY_PLAIN, GW_POLICY_LEARNED, GW_POLICY_SA = 0, 1, 2
 GW_PATHS_NONE, GW_PATHS_FULL = 0, 1
 GW_EDGES_SYMMETRIC, GW_EDGES_SORT, GW_EDGES_DEDUP = 1, 2, 4
 GW_SPLIT_REFERENCE, GW_SPLIT_EQUAL_EDGES = 0, 1
@@ -24,7 +24,7 @@ EXPORTS = (
     "gw_version", "gw_status_string", "gw_config_default", "gw_create", "gw_destroy", "gw_last_error",
     "gw_set_config", "gw_stream", "gw_set_graph_meta", "gw_host_block", "gw_device_graph", "gw_cache_reset",
     "gw_init_walkers", "gw_run", "gw_num_walkers", "gw_get_paths", "gw_path_hashes", "gw_checksum",
-    "gw_bucket_counts", "gw_rmat_csr", "gw_edges_csr", "gw_split_blocks", "gw_device_free", "gw_memcpy", "gw_walk_noalloc",
+    "gw_bucket_counts", "gw_rmat_csr", "gw_edges_csr", "gw_split_blocks", "gw_sa_choose_blocks", "gw_device_free", "gw_memcpy", "gw_walk_noalloc",
     "gw_mlp_forward", "gw_mlp_grad", "gw_mlp_train", "gw_host_alloc", "gw_host_free",
 )
 GW_MLP_INPUTS = 16
@@ -128,6 +128,7 @@ def load():
         "gw_rmat_csr": ([u32, u32, u64, u32p, u64, i32, u64, ctypes.POINTER(vp), ctypes.POINTER(vp), u64p], i32),
         "gw_edges_csr": ([vp, vp, u64, u32, u32, ctypes.POINTER(vp), ctypes.POINTER(vp), u64p, u32p], i32),
         "gw_split_blocks": ([vp, u32, u32, u64, vp, vp, u32, u32p], i32),
+        "gw_sa_choose_blocks": ([vp, u32, vp, u32, u32, u64, u32, vp], i32),
         "gw_device_free": ([vp], i32),
         "gw_memcpy": ([vp, vp, u64], i32),
         "gw_walk_noalloc": ([ctypes.POINTER(GwConfig), vp, vp, u32, u64, u64, vp, vp, vp, vp,

@@ -606,7 +606,7 @@ int gw_handle::run_incore(gw_stats *stats)
 extern "C" int gw_run(gw_handle *h, uint32_t policy, gw_stats *stats)
 {
     if (!h) return GW_ERR_ARG;
-    if (policy > GW_POLICY_LEARNED) return h->fail(GW_ERR_ARG, "unknown policy %u", policy);
+    if (policy > GW_POLICY_SA) return h->fail(GW_ERR_ARG, "unknown policy %u", policy);
     if (h->nblocks == 0) return h->fail(GW_ERR_STATE, "no graph");
     if (!h->walkers_ready) return h->fail(GW_ERR_STATE, "call gw_init_walkers first");
     cudaSetDevice(h->cfg.device);

@@ -59,6 +59,7 @@ struct OocState {
     uint32_t *d_counts = nullptr, *d_offsets = nullptr, *d_cursor = nullptr, *d_pairs = nullptr;
     uint32_t *d_run_pre = nullptr, *d_run_off = nullptr, *d_nrun = nullptr;
     Decision *d_dec = nullptr, *h_dec = nullptr;
+    SaState *d_sa = nullptr;  // annealing policy: the held block set
 
     // zero-copy: device views of the host blocks' neighbour lists, and the
     // pinned copies made of pageable ones
@@ -149,6 +150,7 @@ void gw_handle::ooc_release()
     cudaFree(o.d_run_off);
     cudaFree(o.d_nrun);
     cudaFree(o.d_dec);
+    cudaFree(o.d_sa);
     if (o.h_blk_csr) cudaFreeHost((void *)o.h_blk_csr);
     if (o.h_cached) cudaFreeHost(o.h_cached);
     if (o.h_dec) cudaFreeHost(o.h_dec);
@@ -305,6 +307,7 @@ static int ooc_setup(gw_handle *h)
     if ((st = h->cuda(cudaMalloc(&o.d_run_off, nbk * sizeof(uint32_t)), "runnable offsets"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_nrun, sizeof(uint32_t)), "runnable count"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_dec, sizeof(Decision)), "decision"))) return st;
+    if ((st = h->cuda(cudaMalloc(&o.d_sa, sizeof(SaState)), "annealing state"))) return st;
     if ((st = h->cuda(cudaMallocHost(&o.h_dec, sizeof(Decision)), "decision"))) return st;
     if ((st = h->cuda(cudaMemcpy(o.d_vstart, h->vblocks.data(), (nb + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice),
                       "vstart")))
@@ -591,6 +594,11 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             return st;
         }
     }
+    if (policy == GW_POLICY_SA && (st = cuda(cudaMemsetAsync(o.d_sa, 0, sizeof(SaState), s), "memset"))) {
+        cudaEventDestroy(k0);
+        cudaEventDestroy(k1);
+        return st;
+    }
     uint32_t trace_t = 0, learned_iters = 0;
     bool reverted = false, have_prev_pred = false;
     uint64_t learned_steps = 0, learned_bytes = 0, plain_steps = 0, plain_bytes = 0;
@@ -712,6 +720,13 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                        "schedule")))
             break;
         launches++;
+        if (policy == GW_POLICY_SA) {
+            if ((st = cuda(launch_sa_choose(o.d_pairs, nb, o.d_cached, ncached, capacity, cfg.seed, false, o.d_sa,
+                                            o.d_dec, ds),
+                           "annealed block choice")))
+                break;
+            launches++;
+        }
         if ((st = cuda(cudaMemcpyAsync(o.h_dec, o.d_dec, sizeof(Decision), cudaMemcpyDeviceToHost, ds), "decision")))
             break;
         if ((st = cuda(cudaMemcpyAsync(h_ctr, o.d_snap, sizeof(unsigned long long) * (kCtrCount + 1),

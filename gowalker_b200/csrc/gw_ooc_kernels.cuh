@@ -80,6 +80,18 @@ cudaError_t launch_combine(const uint32_t *counts, uint32_t nb, uint32_t *combin
 cudaError_t launch_schedule(const uint32_t *counts, const uint32_t *live, uint32_t nb, const uint32_t *cached,
                             uint32_t ncached, uint32_t nslots, uint32_t zero_threshold, const float *pred,
                             float pred_weight, Decision *out, cudaStream_t s);
+// ---- SOWalker annealing policy (gw_sa.cu): the block set held across
+// iterations until all of it is resident
+struct SaState {
+    uint32_t k;      // size of the held set, 0 = none
+    uint32_t calls;  // annealing calls so far (the draws' second counter word)
+    uint32_t set[kMaxBlocks];
+};
+// Anneals a new set when forced, when none is held or when the held one is
+// all resident; then (unless forced) points `dec` at the set's first absent
+// block.  counts: nb^2 walkers per (prev, cur) block pair.
+cudaError_t launch_sa_choose(const uint32_t *counts, uint32_t nb, const uint32_t *cached, uint32_t ncached,
+                             uint32_t k, uint64_t seed, bool force, SaState *st, Decision *dec, cudaStream_t s);
 // ---- learned policy: per-block features, training targets, decisions
 
 struct FeatureArgs {

@@ -280,3 +280,20 @@ def split_blocks_device(beg, nverts, mode=_abi.GW_SPLIT_REFERENCE, param=1024 <<
         raise GwError(st, "gw_split_blocks failed (%d blocks)" % nb.value)
     k = int(nb.value)
     return vb[: k + 1].copy(), eb[: k + 1].copy()
+
+
+def sa_choose_blocks(counts, cached, k, seed=42, call=0):
+    """gw_sa_choose_blocks: SOWalker's annealed block set (engine/schedule.hpp:455-593)
+    computed on the device from the nb x nb (prev, cur) walker counts, the
+    resident blocks and the slot count k."""
+    L = _abi.load()
+    counts = np.ascontiguousarray(counts, dtype=np.uint32)
+    nb = counts.shape[0]
+    cached = np.ascontiguousarray(cached, dtype=np.uint32)
+    out = np.zeros(max(min(k, nb), 1), dtype=np.uint32)
+    st = L.gw_sa_choose_blocks(ctypes.c_void_p(counts.ctypes.data), nb,
+                               ctypes.c_void_p(cached.ctypes.data if cached.size else 0), cached.size, k, seed, call,
+                               ctypes.c_void_p(out.ctypes.data))
+    if st != 0:
+        raise GwError(st, "gw_sa_choose_blocks failed")
+    return out[: min(k, nb)]

@@ -497,7 +497,8 @@ static void print_help()
            "- length:        the number of steps of each walk\n"
            "- p, q:          node2vec parameters; alpha: SOPR/SOSR parameter\n"
            "- zero:          finish stragglers through mapped host memory (zero_threshold per block size)\n"
-           "- gpu cpu walkaware GOWalker SOWalker: scheduler flags (the plain GOWalker rule runs on the device)\n"
+           "- GOWalker / SOWalker: block choice by the GOWalker rule or by SOWalker's annealed block set\n"
+           "  (both on the device); gpu cpu walkaware: accepted, no effect\n"
            "- learned:       block choice by the trained demand predictor (plain rule as fallback)\n"
            "- termination F: stop each walk with probability F per step (SOPR/SOSR workloads)\n"
            "- seed N, device N, keepblocks, persource, paths FILE, pathsbin FILE\n"
@@ -592,10 +593,11 @@ int walk_app_main(int argc, const char **argv, AlgorithmType algo)
             printf("Please select one walker from GOWalker and SOWalker!\n");
             return 0;
         }
-        if (SOWalker) fprintf(stderr, "note: the SOWalker annealing scheduler is not built; using the GOWalker rule\n");
         graph_block blocks(&conf);
         graph_driver driver(&conf, m);
-        GOwalker_scheduler_t sched(m, ex.learned);
+        GOwalker_scheduler_t go_sched(m, ex.learned);
+        SOwalker_scheduler_t so_sched(m);
+        scheduler &sched = (SOWalker && !GOWalker) ? static_cast<scheduler &>(so_sched) : go_sched;
         graph_walk walk(conf, driver, blocks);
         const bid_t nmblocks = (bid_t)std::max<size_t>(1, conf.cache_size / conf.blocksize);
         graph_cache cache(blocks.nblocks, blocksize);

@@ -192,6 +192,12 @@ private:
     bool learned_;
 };
 
+class SOwalker_scheduler_t : public scheduler {  // engine/schedule.hpp:369-621 (annealing on the device)
+public:
+    explicit SOwalker_scheduler_t(metrics &m) : scheduler(m) {}
+    uint32_t policy() const override { return GW_POLICY_SA; }
+};
+
 // ---------------------------------------------------------------- engine
 class graph_engine {  // engine/engine.hpp:34-639
 public:

@@ -65,6 +65,8 @@ extern "C" {
 #define GW_POLICY_PLAIN 0u   /* GOwalker_scheduler_t::max_choose_blocks
                                 (engine/schedule.hpp:70-138) on the device */
 #define GW_POLICY_LEARNED 1u /* MLP demand predictor, plain policy as fallback */
+#define GW_POLICY_SA 2u      /* SOwalker_scheduler_t::choose_blocks (engine/schedule.hpp:455-593):
+                                an annealed block set, loaded block by block */
 
 /* path recording */
 #define GW_PATHS_NONE 0u   /* per-walker hash and length only */
@@ -242,6 +244,16 @@ int gw_rmat_csr(uint32_t scale, uint32_t nverts, uint64_t nsamples, const uint32
 #define GW_EDGES_DEDUP 4u
 int gw_edges_csr(const uint32_t *src, const uint32_t *dst, uint64_t n, uint32_t nverts, uint32_t flags,
                  uint64_t **d_beg, uint32_t **d_csr, uint64_t *nedges, uint32_t *nverts_out);
+
+/* SOWalker's annealing block choice (SOwalker_scheduler_t::choose_blocks,
+ * engine/schedule.hpp:455-593) on the device, exactly as GW_POLICY_SA runs
+ * it: counts = nblocks*nblocks walkers per (prev, cur) block pair, cached =
+ * the ncached resident blocks, k = cache slots; the annealing draws are
+ * Philox4x32-10 (round, call, 0, 'SANN') under `seed` (the reference uses
+ * std::rand).  Host memory in and out; writes the min(k, nblocks) chosen
+ * blocks to out.  nblocks <= 1024. */
+int gw_sa_choose_blocks(const uint32_t *counts, uint32_t nblocks, const uint32_t *cached, uint32_t ncached,
+                        uint32_t k, uint64_t seed, uint32_t call, uint32_t *out);
 
 /* Block split points over CSR offsets beg[0..nverts] (host or device
  * memory), computed on the device.

@@ -25,6 +25,7 @@ Contents:
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import subprocess
 
@@ -352,6 +353,91 @@ def split_equal_edge_mass(beg: np.ndarray, nblocks: int):
     vb = vb.astype(np.uint32)
     eb = beg[vb.astype(np.int64)].astype(np.uint64)
     return vb, eb
+
+
+# ------------------------------------------------------------------ SOWalker annealing block choice
+
+TAG_SA = 0x53414E4E  # 'SANN'
+
+
+def sa_exp_nonpos(x: float) -> float:
+    """exp(x), x <= 0, by the fixed steps the device uses (every operation an
+    IEEE double rounded to nearest): Cody-Waite reduction x = n ln2 + r with
+    ln2 = 45426 * 2^-16 + 1.4286068203094172e-06, Taylor series of exp(r) to
+    r^13/13! by Horner, then 2^n.  Bit-identical to the device's version."""
+    if not (x > -700.0):
+        return 0.0
+    if x >= 0.0:
+        return 1.0
+    nd = float(round(x * 1.4426950408889634))
+    r = (x - nd * 0.693145751953125) - nd * 1.4286068203094172e-06
+    q = 1.0
+    for k in range(13, 0, -1):
+        q = 1.0 + (r * q) / k
+    return math.ldexp(q, int(nd))
+
+
+def sa_choose_blocks(counts, cached, k: int, seed: int, call: int):
+    """Restatement of SOwalker_scheduler_t::choose_blocks
+    (engine/schedule.hpp:455-593): rank blocks by walkers whose current block
+    they are (ties by id), take the first k-1 and the best partner for the
+    k-th (schedule.hpp:488-500), then anneal one-for-one swaps (523-583):
+    score = walkers inside the set // blocks of the set not resident (0 when
+    all are), accept better, or worse-but-positive with probability
+    exp((y_tmp - y_can)/T) in float, T = 100 x 0.998^i while > 0.001, at most
+    C(nb, k) rounds.  Round i of call c draws Philox(i, c, 0, 'SANN') under
+    seed where the reference calls std::rand."""
+    bw = [[int(v) for v in row] for row in np.asarray(counts, dtype=np.uint64)]
+    nb = len(bw)
+    k = min(k, nb)
+    isc = [0] * nb
+    for b in cached:
+        isc[int(b)] = 1
+    pw = [sum(bw[p][c] for p in range(nb)) for c in range(nb)]
+    idx = sorted(range(nb), key=lambda b: (-pw[b], b))
+    if 0 < k < nb:
+        best, bi = 0, None
+        for pi in range(k - 1, nb):
+            p = idx[pi]
+            w = sum(bw[p][idx[ci]] + bw[idx[ci]][p] for ci in range(k - 1))
+            if w > best:
+                best, bi = w, pi
+        if bi is not None:
+            idx[k - 1], idx[bi] = idx[bi], idx[k - 1]
+    cand = idx[:k]
+    if 0 < k < nb:
+        f32 = np.float32
+        score = sum(bw[p][c] for p in cand for c in cand)
+        comm = sum(isc[b] for b in cand)
+
+        def y(sc, cm):
+            return f32(sc // (k - cm)) if cm < k else f32(0.0)
+
+        ycan = y(score, comm)
+        maxiter = min(math.comb(nb, k), 1 << 20)
+        T = f32(100.0)
+        key = [seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF]
+        it = 0
+        while it < maxiter and T > f32(0.001):
+            r = [int(v) for v in philox([it, call, 0, TAG_SA], key)]
+            pos = k + r[0] % (nb - k)
+            tp = r[1] % k
+            out, inn = cand[tp], idx[pos]
+            a = sum(bw[out][x] + bw[x][out] for x in cand)
+            b = sum(bw[inn][x] + bw[x][inn] for j, x in enumerate(cand) if j != tp)
+            score2 = score - (a - bw[out][out]) + (b + bw[inn][inn])
+            comm2 = comm - isc[out] + isc[inn]
+            y2 = y(score2, comm2)
+            acc = bool(y2 > ycan)
+            if not acc and y2 > 0:
+                d = f32(f32(y2 - ycan) / T)
+                acc = r[2] * 2.0 ** -32 < sa_exp_nonpos(float(d))
+            if acc:
+                cand[tp], idx[pos] = inn, out
+                score, comm, ycan = score2, comm2, y2
+            T = f32(T * f32(0.998))
+            it += 1
+    return np.array(cand, dtype=np.uint32)
 
 
 # ------------------------------------------------------------------ reference harness

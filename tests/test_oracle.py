@@ -291,3 +291,24 @@ def test_split_equal_edge_mass_integer_targets(oracle):
     vb, eb = oracle.split_equal_edge_mass(beg, 3)
     # targets 7 and 14: first offsets >= them are beg[3]=10 and beg[5]=20
     assert vb.tolist() == [0, 3, 5, 7] and eb.tolist() == [0, 10, 20, 21]
+
+
+def test_sa_exp_accuracy(oracle):
+    """The fixed-step exp the annealing acceptance uses is within 1 ulp-ish of
+    libm over the range it sees."""
+    import math
+    for x in -np.logspace(-9, 2.84, 3000):
+        e = math.exp(float(x))
+        assert abs(oracle.sa_exp_nonpos(float(x)) - e) <= 4e-16 * e
+    assert oracle.sa_exp_nonpos(-800.0) == 0.0 and oracle.sa_exp_nonpos(0.0) == 1.0
+
+
+def test_sa_choice_properties(oracle):
+    rng = np.random.default_rng(4)
+    c = rng.integers(0, 100, (20, 20)).astype(np.uint32)
+    c[3, 3] = c[7, 3] = 100000
+    s = oracle.sa_choose_blocks(c, [], 6, 1, 0)
+    assert len(set(s.tolist())) == 6 and s.max() < 20
+    assert 3 in s  # the block the hot walkers wait for
+    assert np.array_equal(s, oracle.sa_choose_blocks(c, [], 6, 1, 0))
+    assert sorted(oracle.sa_choose_blocks(c, [], 25, 1, 0).tolist()) == list(range(20))
