@@ -37,12 +37,18 @@ namespace gw {
 constexpr uint32_t kTagSa = 0x53414E4Eu;  // 'SANN'
 constexpr uint32_t kSaSmemMaxNb = 200;     // counts staged in shared memory up to 200 blocks (160 KB)
 constexpr uint32_t kSaMaxRounds = 1u << 20;
+constexpr uint32_t kSaDraws = 1024;        // annealing draws made per CTA pass
+
+// 1/k rounded to nearest (each a correctly rounded quotient), k = 1..13.
+__constant__ double kInv[14] = {0.0,       1.0 / 1,  1.0 / 2,  1.0 / 3,  1.0 / 4,  1.0 / 5,  1.0 / 6,
+                                1.0 / 7,   1.0 / 8,  1.0 / 9,  1.0 / 10, 1.0 / 11, 1.0 / 12, 1.0 / 13};
 
 // exp(x) for x <= 0 in IEEE double with every operation rounded to nearest
 // (no contraction), so any IEEE implementation of the same steps gives the
 // same bits.  Cody-Waite reduction x = n ln2 + r, ln2 split as 45426 * 2^-16
 // (exact products n * hi for |n| < 2^36) plus the remainder, then the Taylor
-// series of exp(r), |r| <= ln2/2, to r^13/13! by Horner; x <= -700 gives 0.
+// series of exp(r), |r| <= ln2/2, to r^13/13! by Horner (q = 1 + r q / k with
+// the division as a product by 1/k); x <= -700 gives 0.
 __device__ double sa_exp_nonpos(double x)
 {
     if (!(x > -700.0)) return 0.0;
@@ -52,13 +58,13 @@ __device__ double sa_exp_nonpos(double x)
     const double lo = 1.4286068203094172e-06;
     const double r = __dsub_rn(__dsub_rn(x, __dmul_rn(nd, hi)), __dmul_rn(nd, lo));
     double q = 1.0;
-    for (int k = 13; k >= 1; --k) q = __dadd_rn(1.0, __ddiv_rn(__dmul_rn(r, q), (double)k));
+    for (int k = 13; k >= 1; --k) q = __dadd_rn(1.0, __dmul_rn(__dmul_rn(r, q), kInv[k]));
     return ldexp(q, (int)nd);
 }
 
-__device__ __forceinline__ float sa_score(unsigned long long score, uint32_t comm, uint32_t k)
+__device__ __forceinline__ float sa_score(uint32_t score, uint32_t comm, uint32_t k)
 {
-    return comm < k ? __ull2float_rn(score / (unsigned long long)(k - comm)) : 0.f;
+    return comm < k ? __uint2float_rn(score / (k - comm)) : 0.f;
 }
 
 // One CTA of 1024 threads.  force: anneal regardless of the held set and
@@ -71,8 +77,11 @@ __global__ void __launch_bounds__(1024)
     __shared__ uint8_t s_isc[kMaxBlocks];
     __shared__ uint32_t s_idx[kMaxBlocks], s_cand[kMaxBlocks];
     __shared__ unsigned long long s_pw[kMaxBlocks];
+    __shared__ unsigned long long s_link[kMaxBlocks];
+    __shared__ uint16_t s_pos[kSaDraws], s_tp[kSaDraws];
+    __shared__ uint32_t s_rz[kSaDraws];
     __shared__ unsigned long long s_best, s_score;
-    __shared__ int s_need;
+    __shared__ int s_need, s_done;
     const uint32_t tid = threadIdx.x, lane = tid & 31u;
     const bool staged = nb <= kSaSmemMaxNb;
     const uint32_t *bw = staged ? s_bw : counts;
@@ -141,55 +150,77 @@ __global__ void __launch_bounds__(1024)
             if (v) atomicAdd(&s_score, (unsigned long long)v);
         }
         __syncthreads();
-        // 4. annealing, warp 0
-        if (tid < 32 && k > 0 && k < nb) {
+        // 4. annealing.  link[x] = walkers between block x and the set (both
+        // directions), kept current on every accepted swap, makes a round
+        // O(1); the rounds' draws are made 1024 at a time by the whole CTA,
+        // the rounds themselves run in warp 0 (every lane the same state).
+        if (k > 0 && k < nb) {
+            for (uint32_t x = tid; x < nb; x += blockDim.x) {
+                unsigned long long w = 0;
+                for (uint32_t j = 0; j < k; ++j) {
+                    const uint32_t c = s_cand[j];
+                    w += (unsigned long long)bw[x * nb + c] + bw[c * nb + x];
+                }
+                s_link[x] = w;
+            }
+            if (tid == 0) s_done = 0;
             const uint32_t call = st->calls;
-            unsigned long long score = s_score;
-            uint32_t comm = 0;
-            for (uint32_t j = 0; j < k; ++j) comm += s_isc[s_cand[j]];
-            float ycan = sa_score(score, comm, k);
             // C(nb, k), saturated: the temperature ends the loop after ~5,760 rounds anyway
             const uint32_t kk = min(k, nb - k);
             unsigned long long maxiter = 1;
             for (uint32_t i = 0; i < kk && maxiter <= kSaMaxRounds; ++i) maxiter = maxiter * (nb - i) / (i + 1);
             if (maxiter > kSaMaxRounds) maxiter = kSaMaxRounds;
+            uint32_t score = (uint32_t)s_score;  // walkers inside the set: at most all live walkers (< 2^32)
+            uint32_t comm = 0;
+            for (uint32_t j = 0; j < k; ++j) comm += s_isc[s_cand[j]];
+            float ycan = sa_score(score, comm, k);
             float T = 100.0f;
-            for (uint32_t it = 0; it < maxiter && T > 0.001f; ++it) {
-                const U4 r = philox4x32_10(it, call, 0u, kTagSa, key0, key1);
-                const uint32_t pos = k + r.x % (nb - k);
-                const uint32_t tp = r.y % k;
-                const uint32_t out = s_cand[tp], in = s_idx[pos];
-                unsigned long long a = 0, b = 0;
-                for (uint32_t j = lane; j < k; j += 32) {
-                    const uint32_t x = s_cand[j];
-                    a += (unsigned long long)bw[out * nb + x] + bw[x * nb + out];
-                    if (j != tp) b += (unsigned long long)bw[in * nb + x] + bw[x * nb + in];
+            uint32_t it = 0;
+            __syncthreads();
+            for (uint32_t base = 0; !s_done; base += kSaDraws) {
+                const uint32_t ri = base + tid;
+                if (tid < kSaDraws && ri < maxiter) {
+                    const U4 r = philox4x32_10(ri, call, 0u, kTagSa, key0, key1);
+                    s_pos[tid] = (uint16_t)(k + r.x % (nb - k));
+                    s_tp[tid] = (uint16_t)(r.y % k);
+                    s_rz[tid] = r.z;
                 }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
-                    b += __shfl_xor_sync(0xFFFFFFFFu, b, o);
-                }
-                const unsigned long long score2 = score - (a - bw[out * nb + out]) + (b + bw[in * nb + in]);
-                const uint32_t comm2 = comm - s_isc[out] + s_isc[in];
-                const float y2 = sa_score(score2, comm2, k);
-                bool acc = y2 > ycan;
-                if (!acc && y2 > 0.f) {
-                    const double pr = sa_exp_nonpos((double)__fdiv_rn(__fsub_rn(y2, ycan), T));
-                    acc = (double)r.z * 0x1p-32 < pr;
-                }
-                if (acc) {
-                    __syncwarp();
-                    if (lane == 0) {
-                        s_cand[tp] = in;
-                        s_idx[pos] = out;
+                __syncthreads();
+                if (tid < 32) {
+                    for (uint32_t j = 0; j < kSaDraws && it < maxiter && T > 0.001f; ++j, ++it) {
+                        const uint32_t pos = s_pos[j], tp = s_tp[j];
+                        const uint32_t out = s_cand[tp], in = s_idx[pos];
+                        const uint32_t b_oo = bw[out * nb + out], b_ii = bw[in * nb + in];
+                        const uint32_t b_io = bw[in * nb + out], b_oi = bw[out * nb + in];
+                        // set minus out's links plus in's links to the set without out
+                        const uint32_t score2 = (uint32_t)((unsigned long long)score - (s_link[out] - b_oo) +
+                                                           (s_link[in] - b_io - b_oi + b_ii));
+                        const uint32_t comm2 = comm - s_isc[out] + s_isc[in];
+                        const float y2 = sa_score(score2, comm2, k);
+                        bool acc = y2 > ycan;
+                        if (!acc && y2 > 0.f) {
+                            const double pr = sa_exp_nonpos((double)__fdiv_rn(__fsub_rn(y2, ycan), T));
+                            acc = (double)s_rz[j] * 0x1p-32 < pr;
+                        }
+                        if (acc) {
+                            for (uint32_t x = lane; x < nb; x += 32)
+                                s_link[x] += ((unsigned long long)bw[x * nb + in] + bw[in * nb + x]) -
+                                             ((unsigned long long)bw[x * nb + out] + bw[out * nb + x]);
+                            __syncwarp();
+                            if (lane == 0) {
+                                s_cand[tp] = in;
+                                s_idx[pos] = out;
+                            }
+                            __syncwarp();
+                            score = score2;
+                            comm = comm2;
+                            ycan = y2;
+                        }
+                        T = __fmul_rn(T, 0.998f);
                     }
-                    __syncwarp();
-                    score = score2;
-                    comm = comm2;
-                    ycan = y2;
+                    if (tid == 0) s_done = !(it < maxiter && T > 0.001f);
                 }
-                T = __fmul_rn(T, 0.998f);
+                __syncthreads();
             }
         }
         __syncthreads();

@@ -364,7 +364,8 @@ def sa_exp_nonpos(x: float) -> float:
     """exp(x), x <= 0, by the fixed steps the device uses (every operation an
     IEEE double rounded to nearest): Cody-Waite reduction x = n ln2 + r with
     ln2 = 45426 * 2^-16 + 1.4286068203094172e-06, Taylor series of exp(r) to
-    r^13/13! by Horner, then 2^n.  Bit-identical to the device's version."""
+    r^13/13! by Horner (q = 1 + (r q)(1/k)), then 2^n.  Bit-identical to the
+    device's version."""
     if not (x > -700.0):
         return 0.0
     if x >= 0.0:
@@ -373,7 +374,7 @@ def sa_exp_nonpos(x: float) -> float:
     r = (x - nd * 0.693145751953125) - nd * 1.4286068203094172e-06
     q = 1.0
     for k in range(13, 0, -1):
-        q = 1.0 + (r * q) / k
+        q = 1.0 + (r * q) * (1.0 / k)
     return math.ldexp(q, int(nd))
 
 
