@@ -12,7 +12,8 @@
 //      set: score = walkers inside the set / blocks of the set not yet
 //      resident (integer division, as the reference's wid_t / size_t); a
 //      better score is taken, a worse positive one with probability
-//      exp((y_tmp - y_can) / T); T from 100 by x0.998 while above 0.001, at
+//      exp((y_tmp - y_can) / T) -- here when (y_tmp - y_can) / T > ln(u) for
+//      the round's uniform draw u; T from 100 by x0.998 while above 0.001, at
 //      most C(nblocks, k) rounds (schedule.hpp:523-583).
 // The reference draws with std::rand seeded by the clock; here round i of
 // annealing call c draws Philox4x32-10 (i, c, 0, 'SANN') under the walk seed,
@@ -39,27 +40,34 @@ constexpr uint32_t kSaSmemMaxNb = 200;     // counts staged in shared memory up 
 constexpr uint32_t kSaMaxRounds = 1u << 20;
 constexpr uint32_t kSaDraws = 1024;        // annealing draws made per CTA pass
 
-// 1/k rounded to nearest (each a correctly rounded quotient), k = 1..13.
-__constant__ double kInv[14] = {0.0,       1.0 / 1,  1.0 / 2,  1.0 / 3,  1.0 / 4,  1.0 / 5,  1.0 / 6,
-                                1.0 / 7,   1.0 / 8,  1.0 / 9,  1.0 / 10, 1.0 / 11, 1.0 / 12, 1.0 / 13};
+// 1/(2j+1) rounded to nearest (each a correctly rounded quotient), j = 0..11.
+__constant__ double kInvOdd[12] = {1.0 / 1,  1.0 / 3,  1.0 / 5,  1.0 / 7,  1.0 / 9,  1.0 / 11,
+                                   1.0 / 13, 1.0 / 15, 1.0 / 17, 1.0 / 19, 1.0 / 21, 1.0 / 23};
 
-// exp(x) for x <= 0 in IEEE double with every operation rounded to nearest
-// (no contraction), so any IEEE implementation of the same steps gives the
-// same bits.  Cody-Waite reduction x = n ln2 + r, ln2 split as 45426 * 2^-16
-// (exact products n * hi for |n| < 2^36) plus the remainder, then the Taylor
-// series of exp(r), |r| <= ln2/2, to r^13/13! by Horner (q = 1 + r q / k with
-// the division as a product by 1/k); x <= -700 gives 0.
-__device__ double sa_exp_nonpos(double x)
+// ln(z * 2^-32) for a 32-bit draw z, in IEEE double with every operation
+// rounded to nearest (no contraction), so any IEEE implementation of the same
+// steps gives the same bits: u = m 2^e with m in [sqrt(1/2), sqrt(2)),
+// ln u = e ln2 + 2 atanh(s), s = (m-1)/(m+1), the atanh series to s^23/23
+// by Horner in s^2 (|s| < 0.172: truncation below 1e-19).  z = 0 gives -inf.
+// Acceptance "d > ln(u)" is the reference's "u < exp(d)", with the
+// transcendental moved off the annealing chain into the parallel draw pass.
+__device__ double sa_log_draw(uint32_t z)
 {
-    if (!(x > -700.0)) return 0.0;
-    if (x >= 0.0) return 1.0;
-    const double nd = rint(__dmul_rn(x, 1.4426950408889634));
-    const double hi = 0.693145751953125;
-    const double lo = 1.4286068203094172e-06;
-    const double r = __dsub_rn(__dsub_rn(x, __dmul_rn(nd, hi)), __dmul_rn(nd, lo));
-    double q = 1.0;
-    for (int k = 13; k >= 1; --k) q = __dadd_rn(1.0, __dmul_rn(__dmul_rn(r, q), kInv[k]));
-    return ldexp(q, (int)nd);
+    if (z == 0) return -__longlong_as_double(0x7FF0000000000000ll);
+    int e = 31 - __clz(z);             // z = 2^e * (1.f), e in [0, 31]
+    double m = (double)z * ldexp(1.0, -e);  // exact: [1, 2)
+    if (m >= 1.4142135623730951) {
+        m = __dmul_rn(m, 0.5);  // exact
+        e += 1;
+    }
+    const double s = __ddiv_rn(__dsub_rn(m, 1.0), __dadd_rn(m, 1.0));
+    const double s2 = __dmul_rn(s, s);
+    double q = kInvOdd[11];
+    for (int j = 10; j >= 0; --j) q = __dadd_rn(kInvOdd[j], __dmul_rn(s2, q));
+    const double lnm = __dmul_rn(__dmul_rn(2.0, s), q);
+    const double ex = (double)(e - 32);
+    // ln2 split as 45426 * 2^-16 (exact products) plus the remainder
+    return __dadd_rn(__dadd_rn(__dmul_rn(ex, 0.693145751953125), __dmul_rn(ex, 1.4286068203094172e-06)), lnm);
 }
 
 __device__ __forceinline__ float sa_score(uint32_t score, uint32_t comm, uint32_t k)
@@ -79,7 +87,7 @@ __global__ void __launch_bounds__(1024)
     __shared__ unsigned long long s_pw[kMaxBlocks];
     __shared__ unsigned long long s_link[kMaxBlocks];
     __shared__ uint16_t s_pos[kSaDraws], s_tp[kSaDraws];
-    __shared__ uint32_t s_rz[kSaDraws];
+    __shared__ double s_lnu[kSaDraws];
     __shared__ unsigned long long s_best, s_score;
     __shared__ int s_need, s_done;
     const uint32_t tid = threadIdx.x, lane = tid & 31u;
@@ -183,7 +191,7 @@ __global__ void __launch_bounds__(1024)
                     const U4 r = philox4x32_10(ri, call, 0u, kTagSa, key0, key1);
                     s_pos[tid] = (uint16_t)(k + r.x % (nb - k));
                     s_tp[tid] = (uint16_t)(r.y % k);
-                    s_rz[tid] = r.z;
+                    s_lnu[tid] = sa_log_draw(r.z);
                 }
                 __syncthreads();
                 if (tid < 32) {
@@ -198,10 +206,7 @@ __global__ void __launch_bounds__(1024)
                         const uint32_t comm2 = comm - s_isc[out] + s_isc[in];
                         const float y2 = sa_score(score2, comm2, k);
                         bool acc = y2 > ycan;
-                        if (!acc && y2 > 0.f) {
-                            const double pr = sa_exp_nonpos((double)__fdiv_rn(__fsub_rn(y2, ycan), T));
-                            acc = (double)s_rz[j] * 0x1p-32 < pr;
-                        }
+                        if (!acc && y2 > 0.f) acc = (double)__fdiv_rn(__fsub_rn(y2, ycan), T) > s_lnu[j];
                         if (acc) {
                             for (uint32_t x = lane; x < nb; x += 32)
                                 s_link[x] += ((unsigned long long)bw[x * nb + in] + bw[in * nb + x]) -

@@ -360,22 +360,28 @@ def split_equal_edge_mass(beg: np.ndarray, nblocks: int):
 TAG_SA = 0x53414E4E  # 'SANN'
 
 
-def sa_exp_nonpos(x: float) -> float:
-    """exp(x), x <= 0, by the fixed steps the device uses (every operation an
-    IEEE double rounded to nearest): Cody-Waite reduction x = n ln2 + r with
-    ln2 = 45426 * 2^-16 + 1.4286068203094172e-06, Taylor series of exp(r) to
-    r^13/13! by Horner (q = 1 + (r q)(1/k)), then 2^n.  Bit-identical to the
-    device's version."""
-    if not (x > -700.0):
-        return 0.0
-    if x >= 0.0:
-        return 1.0
-    nd = float(round(x * 1.4426950408889634))
-    r = (x - nd * 0.693145751953125) - nd * 1.4286068203094172e-06
-    q = 1.0
-    for k in range(13, 0, -1):
-        q = 1.0 + (r * q) * (1.0 / k)
-    return math.ldexp(q, int(nd))
+def sa_log_draw(z: int) -> float:
+    """ln(z * 2^-32) by the fixed steps the device uses (every operation an
+    IEEE double rounded to nearest): z = 2^e * m, m in [sqrt(1/2), sqrt(2)),
+    ln = e ln2 + 2 atanh((m-1)/(m+1)), the atanh series to s^23/23 by Horner
+    in s^2, ln2 = 45426 * 2^-16 + 1.4286068203094172e-06.  z = 0 gives -inf.
+    Bit-identical to the device's version."""
+    if z == 0:
+        return -math.inf
+    e = z.bit_length() - 1
+    m = float(z) * math.ldexp(1.0, -e)
+    if m >= 1.4142135623730951:
+        m = m * 0.5
+        e += 1
+    s = (m - 1.0) / (m + 1.0)
+    s2 = s * s
+    inv = [1.0 / (2 * j + 1) for j in range(12)]
+    q = inv[11]
+    for j in range(10, -1, -1):
+        q = inv[j] + s2 * q
+    lnm = (2.0 * s) * q
+    ex = float(e - 32)
+    return (ex * 0.693145751953125 + ex * 1.4286068203094172e-06) + lnm
 
 
 def sa_choose_blocks(counts, cached, k: int, seed: int, call: int):
@@ -385,7 +391,8 @@ def sa_choose_blocks(counts, cached, k: int, seed: int, call: int):
     k-th (schedule.hpp:488-500), then anneal one-for-one swaps (523-583):
     score = walkers inside the set // blocks of the set not resident (0 when
     all are), accept better, or worse-but-positive with probability
-    exp((y_tmp - y_can)/T) in float, T = 100 x 0.998^i while > 0.001, at most
+    exp((y_tmp - y_can)/T) -- as (y_tmp - y_can)/T > ln(u) for the round's
+    uniform u (sa_log_draw) -- in float, T = 100 x 0.998^i while > 0.001, at most
     C(nb, k) rounds.  Round i of call c draws Philox(i, c, 0, 'SANN') under
     seed where the reference calls std::rand."""
     bw = [[int(v) for v in row] for row in np.asarray(counts, dtype=np.uint64)]
@@ -432,7 +439,7 @@ def sa_choose_blocks(counts, cached, k: int, seed: int, call: int):
             acc = bool(y2 > ycan)
             if not acc and y2 > 0:
                 d = f32(f32(y2 - ycan) / T)
-                acc = r[2] * 2.0 ** -32 < sa_exp_nonpos(float(d))
+                acc = float(d) > sa_log_draw(r[2])
             if acc:
                 cand[tp], idx[pos] = inn, out
                 score, comm, ycan = score2, comm2, y2

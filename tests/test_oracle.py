@@ -293,14 +293,17 @@ def test_split_equal_edge_mass_integer_targets(oracle):
     assert vb.tolist() == [0, 3, 5, 7] and eb.tolist() == [0, 10, 20, 21]
 
 
-def test_sa_exp_accuracy(oracle):
-    """The fixed-step exp the annealing acceptance uses is within 1 ulp-ish of
-    libm over the range it sees."""
+def test_sa_log_accuracy(oracle):
+    """The fixed-step log of a 32-bit draw the annealing acceptance uses is
+    within a few ulp of libm."""
     import math
-    for x in -np.logspace(-9, 2.84, 3000):
-        e = math.exp(float(x))
-        assert abs(oracle.sa_exp_nonpos(float(x)) - e) <= 4e-16 * e
-    assert oracle.sa_exp_nonpos(-800.0) == 0.0 and oracle.sa_exp_nonpos(0.0) == 1.0
+    rng = np.random.default_rng(2)
+    for z in list(rng.integers(1, 1 << 32, 3000)) + [1, 2, 3, 0xFFFFFFFF, 1 << 31, 0xB504F333]:
+        z = int(z)
+        want = math.log(z * 2.0 ** -32)
+        got = oracle.sa_log_draw(z)
+        assert abs(got - want) <= 4e-16 * max(abs(want), 1e-300) + 1e-300, z
+    assert oracle.sa_log_draw(0) == -math.inf and oracle.sa_log_draw((1 << 32) - 1) < 0
 
 
 def test_sa_choice_properties(oracle):
