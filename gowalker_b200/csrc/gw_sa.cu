@@ -88,6 +88,8 @@ __global__ void __launch_bounds__(1024)
     __shared__ unsigned long long s_link[kMaxBlocks];
     __shared__ uint16_t s_pos[kSaDraws], s_tp[kSaDraws];
     __shared__ double s_lnu[kSaDraws];
+    __shared__ float s_temp[kSaDraws];
+    __shared__ float s_tnext;
     __shared__ unsigned long long s_best, s_score;
     __shared__ int s_need, s_done;
     const uint32_t tid = threadIdx.x, lane = tid & 31u;
@@ -160,8 +162,12 @@ __global__ void __launch_bounds__(1024)
         __syncthreads();
         // 4. annealing.  link[x] = walkers between block x and the set (both
         // directions), kept current on every accepted swap, makes a round
-        // O(1); the rounds' draws are made 1024 at a time by the whole CTA,
-        // the rounds themselves run in warp 0 (every lane the same state).
+        // O(1).  The rounds' draws, their ln(u) and the temperature sequence
+        // are made 1024 rounds at a time by the whole CTA; warp 0 then runs
+        // the rounds 32 at a time speculatively: every lane evaluates one
+        // round against the current set, the first accepting round is
+        // applied and the rounds after it are evaluated again -- exactly the
+        // sequential chain, since a rejected round changes nothing.
         if (k > 0 && k < nb) {
             for (uint32_t x = tid; x < nb; x += blockDim.x) {
                 unsigned long long w = 0;
@@ -171,7 +177,10 @@ __global__ void __launch_bounds__(1024)
                 }
                 s_link[x] = w;
             }
-            if (tid == 0) s_done = 0;
+            if (tid == 0) {
+                s_done = 0;
+                s_tnext = 100.0f;
+            }
             const uint32_t call = st->calls;
             // C(nb, k), saturated: the temperature ends the loop after ~5,760 rounds anyway
             const uint32_t kk = min(k, nb - k);
@@ -182,8 +191,6 @@ __global__ void __launch_bounds__(1024)
             uint32_t comm = 0;
             for (uint32_t j = 0; j < k; ++j) comm += s_isc[s_cand[j]];
             float ycan = sa_score(score, comm, k);
-            float T = 100.0f;
-            uint32_t it = 0;
             __syncthreads();
             for (uint32_t base = 0; !s_done; base += kSaDraws) {
                 const uint32_t ri = base + tid;
@@ -193,37 +200,69 @@ __global__ void __launch_bounds__(1024)
                     s_tp[tid] = (uint16_t)(r.y % k);
                     s_lnu[tid] = sa_log_draw(r.z);
                 }
-                __syncthreads();
-                if (tid < 32) {
-                    for (uint32_t j = 0; j < kSaDraws && it < maxiter && T > 0.001f; ++j, ++it) {
-                        const uint32_t pos = s_pos[j], tp = s_tp[j];
-                        const uint32_t out = s_cand[tp], in = s_idx[pos];
-                        const uint32_t b_oo = bw[out * nb + out], b_ii = bw[in * nb + in];
-                        const uint32_t b_io = bw[in * nb + out], b_oi = bw[out * nb + in];
-                        // set minus out's links plus in's links to the set without out
-                        const uint32_t score2 = (uint32_t)((unsigned long long)score - (s_link[out] - b_oo) +
-                                                           (s_link[in] - b_io - b_oi + b_ii));
-                        const uint32_t comm2 = comm - s_isc[out] + s_isc[in];
-                        const float y2 = sa_score(score2, comm2, k);
-                        bool acc = y2 > ycan;
-                        if (!acc && y2 > 0.f) acc = (double)__fdiv_rn(__fsub_rn(y2, ycan), T) > s_lnu[j];
-                        if (acc) {
-                            for (uint32_t x = lane; x < nb; x += 32)
-                                s_link[x] += ((unsigned long long)bw[x * nb + in] + bw[in * nb + x]) -
-                                             ((unsigned long long)bw[x * nb + out] + bw[out * nb + x]);
-                            __syncwarp();
-                            if (lane == 0) {
-                                s_cand[tp] = in;
-                                s_idx[pos] = out;
-                            }
-                            __syncwarp();
-                            score = score2;
-                            comm = comm2;
-                            ycan = y2;
-                        }
+                if (tid == 0) {
+                    float T = s_tnext;
+                    for (uint32_t j = 0; j < kSaDraws; ++j) {
+                        s_temp[j] = T;
                         T = __fmul_rn(T, 0.998f);
                     }
-                    if (tid == 0) s_done = !(it < maxiter && T > 0.001f);
+                    s_tnext = T;
+                }
+                __syncthreads();
+                if (tid < 32) {
+                    uint32_t j = 0;
+                    bool finished = false;
+                    while (j < kSaDraws) {
+                        const uint32_t jl = j + lane;
+                        const bool valid = jl < kSaDraws && base + jl < maxiter && s_temp[jl] > 0.001f;
+                        const unsigned vmask = __ballot_sync(0xFFFFFFFFu, valid);
+                        if (vmask == 0) {
+                            finished = true;
+                            break;
+                        }
+                        uint32_t pos = 0, tp = 0, out = 0, in = 0, score2 = 0, comm2 = 0;
+                        float y2 = 0.f;
+                        bool acc = false;
+                        if (valid) {
+                            pos = s_pos[jl];
+                            tp = s_tp[jl];
+                            out = s_cand[tp];
+                            in = s_idx[pos];
+                            const uint32_t b_oo = bw[out * nb + out], b_ii = bw[in * nb + in];
+                            const uint32_t b_io = bw[in * nb + out], b_oi = bw[out * nb + in];
+                            // the set minus out's links, plus in's links to the set without out
+                            score2 = (uint32_t)((unsigned long long)score - (s_link[out] - b_oo) +
+                                                (s_link[in] - b_io - b_oi + b_ii));
+                            comm2 = comm - s_isc[out] + s_isc[in];
+                            y2 = sa_score(score2, comm2, k);
+                            acc = y2 > ycan ||
+                                  (y2 > 0.f && (double)__fdiv_rn(__fsub_rn(y2, ycan), s_temp[jl]) > s_lnu[jl]);
+                        }
+                        const unsigned amask = __ballot_sync(0xFFFFFFFFu, acc);
+                        if (amask == 0) {
+                            j += (uint32_t)__popc(vmask);
+                            continue;
+                        }
+                        const int f = __ffs(amask) - 1;
+                        pos = __shfl_sync(0xFFFFFFFFu, pos, f);
+                        tp = __shfl_sync(0xFFFFFFFFu, tp, f);
+                        out = __shfl_sync(0xFFFFFFFFu, out, f);
+                        in = __shfl_sync(0xFFFFFFFFu, in, f);
+                        score = __shfl_sync(0xFFFFFFFFu, score2, f);
+                        comm = __shfl_sync(0xFFFFFFFFu, comm2, f);
+                        ycan = __shfl_sync(0xFFFFFFFFu, y2, f);
+                        for (uint32_t x = lane; x < nb; x += 32)
+                            s_link[x] += ((unsigned long long)bw[x * nb + in] + bw[in * nb + x]) -
+                                         ((unsigned long long)bw[x * nb + out] + bw[out * nb + x]);
+                        __syncwarp();
+                        if (lane == 0) {
+                            s_cand[tp] = in;
+                            s_idx[pos] = out;
+                        }
+                        __syncwarp();
+                        j += (uint32_t)f + 1;
+                    }
+                    if (lane == 0 && finished) s_done = 1;
                 }
                 __syncthreads();
             }
