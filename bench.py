@@ -322,7 +322,7 @@ def run_ooc_bench(args, wl):
             "iterations_per_run": tot["iterations"] / args.steps,
             "learned": {"iterations_per_run": tot["learned_iterations"] / args.steps,
                         "reverted_runs": tot["policy_reverted"], "train_loss": last.get("train_loss"),
-                        "pred_error": last.get("pred_error")},
+                        "pred_error": last.get("pred_error"), "persist_error": last.get("persist_error")},
             "trials_per_step": tot["trials"] / max(tot["steps"], 1),
             "roofline": {"bound": "host-link", "achieved": link, "peak": PCIE_GEN5_X16_GBS, "unit": "GB/s",
                          "frac": link / PCIE_GEN5_X16_GBS, "traffic": None,

@@ -77,7 +77,8 @@ class GwStats(ctypes.Structure):
         ("train_loss", ctypes.c_float),
         ("pred_error", ctypes.c_float),
         ("kernel_variant", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 3),
+        ("persist_error", ctypes.c_float),
+        ("reserved", ctypes.c_uint32 * 2),
         ("coop_small_steps", ctypes.c_uint64),
         ("coop_small_attempts", ctypes.c_uint64),
         ("coop_large_steps", ctypes.c_uint64),

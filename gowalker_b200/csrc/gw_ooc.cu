@@ -21,6 +21,7 @@
 #include "gw_mlp.cuh"
 #include "gw_compress.cuh"
 #include <cmath>
+#include <deque>
 #include <thread>
 
 namespace gw {
@@ -600,13 +601,13 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         return st;
     }
     uint32_t trace_t = 0, learned_iters = 0;
-    bool reverted = false, have_prev_pred = false;
+    bool reverted = false;
     uint64_t learned_steps = 0, learned_bytes = 0, plain_steps = 0, plain_bytes = 0;
     uint64_t phase_steps_mark = 0, phase_bytes_mark = 0;
     int last_phase = -1;
-    double pred_err_sum = 0.0;
+    double pred_err_sum = 0.0, persist_err_sum = 0.0;
     uint32_t pred_err_n = 0;
-    std::vector<float> prev_pred;
+    std::deque<std::vector<float>> hist_pred, hist_col;  // predictions / demand awaiting their horizon
     // Prefetch: each decision is taken one iteration ahead and its block is
     // copied on the copy stream into a staging slot while the current step
     // kernel runs; it becomes resident at the start of the next iteration.
@@ -679,8 +680,11 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         // ---- learned policy: features (traces while training), prediction, choice
         const bool learned = policy == GW_POLICY_LEARNED;
         const bool learned_active = learned && o.trained && !reverted;
+        // once trained the predictor keeps predicting (its error is measured)
+        // even after its judge has handed the choice back to the plain rule
+        const bool predicting = learned && o.trained;
         const bool tracing = learned && !o.trained && trace_t < kTraceIters + kHorizon;
-        if (learned_active || tracing) {
+        if (predicting || tracing) {
             FeatureArgs f{};
             f.counts = o.d_pairs;
             f.blk_csr = o.d_blk_csr2;
@@ -696,16 +700,21 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             f.col = tracing ? o.d_trace_col + (uint64_t)trace_t * nb : o.d_feat_col;
             if ((st = cuda(launch_features(f, ds), "features"))) break;
             launches++;
-            if (learned_active) {
+            if (predicting) {
                 if ((st = cuda(mlp_forward(o.d_params, o.d_feat_x, nb, o.d_pred, ds), "predictor"))) break;
+                launches++;
+            }
+            if (learned_active) {
                 if ((st = cuda(launch_learned_choose(o.d_pred, nb, o.d_blk_csr2, o.d_cached, ncached, capacity,
                                                      prefetch ? 1u : kMaxLoadsPerIter, kSwapMargin, o.d_choose, ds),
                                "learned choice")))
                     break;
-                launches += 2;
+                launches++;
                 if ((st = cuda(cudaMemcpyAsync(o.h_choose, o.d_choose, sizeof(int32_t) * (2 * kMaxLoadsPerIter + 1),
                                                cudaMemcpyDeviceToHost, ds), "choice")))
                     break;
+            }
+            if (predicting) {
                 if ((st = cuda(cudaMemcpyAsync(o.h_pred, o.d_pred, sizeof(float) * nb, cudaMemcpyDeviceToHost, ds),
                                "predictions")))
                     break;
@@ -762,16 +771,31 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         phase_steps_mark = steps_now;
         phase_bytes_mark = h2d;
         last_phase = -1;
-        if (learned_active) {
-            // observed demand vs the previous iteration's prediction
-            if (have_prev_pred) {
-                double e = 0.0;
-                for (uint32_t i = 0; i < nb; ++i) e += std::fabs(prev_pred[i] - std::log1p((double)o.h_col[i]));
-                pred_err_sum += e / nb;
+        if (predicting) {
+            // Each prediction is scored once the kHorizon iterations it
+            // forecasts have been observed, against the training target
+            // log1p(mean demand over them), beside the forecast without the
+            // network: the demand of the iteration it was made in, carried
+            // forward (what the plain rule assumes).
+            hist_pred.emplace_back(o.h_pred, o.h_pred + nb);
+            hist_col.emplace_back(o.h_col, o.h_col + nb);
+            if (hist_col.size() > kHorizon) {
+                double ep = 0.0, eq = 0.0;
+                for (uint32_t i = 0; i < nb; ++i) {
+                    double m = 0.0;
+                    for (uint32_t t = 1; t <= kHorizon; ++t) m += hist_col[t][i];
+                    const double target = std::log1p(m / kHorizon);
+                    ep += std::fabs((double)hist_pred[0][i] - target);
+                    eq += std::fabs(std::log1p((double)hist_col[0][i]) - target);
+                }
+                pred_err_sum += ep / nb;
+                persist_err_sum += eq / nb;
                 pred_err_n++;
+                hist_pred.pop_front();
+                hist_col.pop_front();
             }
-            prev_pred.assign(o.h_pred, o.h_pred + nb);
-            have_prev_pred = true;
+        }
+        if (learned_active) {
             if (learned_iters >= 16 && plain_steps > 0 && learned_steps > 0 &&
                 (double)learned_bytes / (double)learned_steps > (double)plain_bytes / (double)plain_steps) {
                 reverted = true;  // the judge: learned moves more bytes per step than the plain rule
@@ -944,6 +968,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         stats->policy_reverted = reverted ? 1u : 0u;
         stats->train_loss = (policy == GW_POLICY_LEARNED) ? o.train_loss : 0.f;
         stats->pred_error = pred_err_n ? (float)(pred_err_sum / pred_err_n) : 0.f;
+        stats->persist_error = pred_err_n ? (float)(persist_err_sum / pred_err_n) : 0.f;
     }
     const uint32_t errw = (uint32_t)h_ctr[kCtrCount];
     if (errw) return fail(GW_ERR_DEVICE, "kernel error word 0x%x", errw);

@@ -122,9 +122,12 @@ typedef struct gw_stats {
     uint32_t learned_iterations; /* iterations decided by the predictor */
     uint32_t policy_reverted;    /* 1 when the judge sent the run back to the plain policy */
     float train_loss;            /* predictor training loss (mean squared, log1p scale) */
-    float pred_error;            /* mean |predicted - observed| demand, log1p scale */
+    float pred_error;            /* learned: mean |prediction - realised target| per block, the target
+                                    log1p(mean demand over the next 3 iterations) */
     uint32_t kernel_variant;     /* register-cap variant the autotuner picked (in-core) */
-    uint32_t reserved[3];
+    float persist_error;         /* learned: the same error of the forecast without the network
+                                    (this iteration's demand carried forward) */
+    uint32_t reserved[2];
     uint64_t coop_small_steps;   /* hard steps decided from candidate positions (in-core) */
     uint64_t coop_small_attempts;
     uint64_t coop_large_steps;   /* hard steps evaluated with candidate loads (in-core) */
