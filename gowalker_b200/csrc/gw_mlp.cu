@@ -147,9 +147,11 @@ __global__ void k_mlp_init(float *P, uint32_t k0, uint32_t k1)
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= kMlpParams) return;
     float scale = 0.f;
+    // hidden layers uniform in +-sqrt(6 / fan_in); the output layer starts at
+    // zero, so an untrained network outputs 0 (the residual forecast: "no
+    // change") and training moves it only where the data says so
     if (p < kOffB1) scale = 0.6123724f;              // sqrt(6 / 16)
     else if (p >= kOffW2 && p < kOffB2) scale = 0.30618622f;  // sqrt(6 / 64)
-    else if (p >= kOffW3 && p < kOffB3) scale = 0.30618622f;
     const U4 r = philox4x32_10((uint32_t)p, 0x4D4C5031u, 0u, 0u, k0, k1);
     const float u = __uint2float_rn(r.x >> 8) * 0x1p-24f;
     P[p] = (2.f * u - 1.f) * scale;

@@ -82,7 +82,7 @@ struct OocState {
     float train_loss = 0.f;
     float *d_params = nullptr, *d_train_ws = nullptr;
     float *d_trace_x = nullptr, *d_trace_col = nullptr, *d_trace_y = nullptr;
-    float *d_feat_x = nullptr, *d_feat_col = nullptr, *d_pred = nullptr;
+    float *d_train_x = nullptr, *d_pred = nullptr;
     float *d_emass = nullptr, *d_vfrac = nullptr, *d_prev_col = nullptr, *d_ema = nullptr;
     int32_t *d_choose = nullptr, *h_choose = nullptr;
     float *h_pred = nullptr, *h_col = nullptr;
@@ -92,8 +92,11 @@ struct OocState {
 // the targets) train the predictor; it then loads up to 4 blocks per
 // iteration, swapping a resident block out only for one whose predicted demand
 // is higher by `kSwapMargin` (log1p scale).
-constexpr uint32_t kTraceIters = 20;
+constexpr uint32_t kTraceIters = 20;  // training samples: the last 20 iterations whose horizon is observed
 constexpr uint32_t kHorizon = 3;
+constexpr uint32_t kTraceRing = kTraceIters + kHorizon;
+constexpr uint32_t kRetrain = 16;        // retrain (warm) every 16 iterations on the sliding window
+constexpr uint32_t kRetrainEpochs = 100;
 constexpr uint32_t kMaxLoadsPerIter = 4;
 constexpr float kSwapMargin = 0.25f;
 constexpr uint32_t kTrainEpochs = 400;
@@ -164,7 +167,7 @@ void gw_handle::ooc_release()
     cudaFree(o.d_snap);
     for (auto *p : o.h_blk_pin)
         if (p) cudaFreeHost((void *)p);
-    for (float *p : {o.d_params, o.d_train_ws, o.d_trace_x, o.d_trace_col, o.d_trace_y, o.d_feat_x, o.d_feat_col,
+    for (float *p : {o.d_params, o.d_train_ws, o.d_trace_x, o.d_trace_col, o.d_trace_y, o.d_train_x,
                      o.d_pred, o.d_emass, o.d_vfrac, o.d_prev_col, o.d_ema})
         cudaFree(p);
     cudaFree(o.d_choose);
@@ -185,11 +188,10 @@ static int learned_setup(gw_handle *h)
     if ((st = dalloc(&o.d_params, kMlpParams, "predictor weights"))) return st;
     if ((st = dalloc(&o.d_train_ws, (uint64_t)kMlpGradCtas * (kMlpParams + 1) + 3 * kMlpParams + 1, "training state")))
         return st;
-    if ((st = dalloc(&o.d_trace_x, (uint64_t)kTraceIters * nb * kMlpIn, "traces"))) return st;
-    if ((st = dalloc(&o.d_trace_col, (uint64_t)(kTraceIters + kHorizon) * nb, "traces"))) return st;
+    if ((st = dalloc(&o.d_trace_x, (uint64_t)kTraceRing * nb * kMlpIn, "traces"))) return st;
+    if ((st = dalloc(&o.d_trace_col, (uint64_t)kTraceRing * nb, "traces"))) return st;
     if ((st = dalloc(&o.d_trace_y, (uint64_t)kTraceIters * nb, "targets"))) return st;
-    if ((st = dalloc(&o.d_feat_x, (uint64_t)nb * kMlpIn, "features"))) return st;
-    if ((st = dalloc(&o.d_feat_col, nb, "demand"))) return st;
+    if ((st = dalloc(&o.d_train_x, (uint64_t)kTraceIters * nb * kMlpIn, "training set"))) return st;
     if ((st = dalloc(&o.d_pred, nb, "predictions"))) return st;
     if ((st = dalloc(&o.d_emass, nb, "edge shares"))) return st;
     if ((st = dalloc(&o.d_vfrac, nb, "vertex shares"))) return st;
@@ -683,8 +685,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         // once trained the predictor keeps predicting (its error is measured)
         // even after its judge has handed the choice back to the plain rule
         const bool predicting = learned && o.trained;
-        const bool tracing = learned && !o.trained && trace_t < kTraceIters + kHorizon;
-        if (predicting || tracing) {
+        const bool tracing = learned;  // features and demand go to the trace ring every iteration
+        float *ring_x = o.d_trace_x + (uint64_t)(trace_t % kTraceRing) * nb * kMlpIn;
+        float *ring_col = o.d_trace_col + (uint64_t)(trace_t % kTraceRing) * nb;
+        if (tracing) {
             FeatureArgs f{};
             f.counts = o.d_pairs;
             f.blk_csr = o.d_blk_csr2;
@@ -696,13 +700,14 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             f.iter = iters;
             f.live_frac = (float)nlive / (float)nwalkers;
             f.inv_live = nlive ? 1.f / (float)nlive : 0.f;
-            f.x = tracing ? o.d_trace_x + (uint64_t)std::min(trace_t, kTraceIters - 1) * nb * kMlpIn : o.d_feat_x;
-            f.col = tracing ? o.d_trace_col + (uint64_t)trace_t * nb : o.d_feat_col;
+            f.x = ring_x;
+            f.col = ring_col;
             if ((st = cuda(launch_features(f, ds), "features"))) break;
             launches++;
             if (predicting) {
-                if ((st = cuda(mlp_forward(o.d_params, o.d_feat_x, nb, o.d_pred, ds), "predictor"))) break;
-                launches++;
+                if ((st = cuda(mlp_forward(o.d_params, ring_x, nb, o.d_pred, ds), "predictor"))) break;
+                if ((st = cuda(launch_add_level(o.d_pred, ring_x, nb, ds), "predictor"))) break;
+                launches += 2;
             }
             if (learned_active) {
                 if ((st = cuda(launch_learned_choose(o.d_pred, nb, o.d_blk_csr2, o.d_cached, ncached, capacity,
@@ -718,7 +723,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 if ((st = cuda(cudaMemcpyAsync(o.h_pred, o.d_pred, sizeof(float) * nb, cudaMemcpyDeviceToHost, ds),
                                "predictions")))
                     break;
-                if ((st = cuda(cudaMemcpyAsync(o.h_col, o.d_feat_col, sizeof(float) * nb, cudaMemcpyDeviceToHost, ds),
+                if ((st = cuda(cudaMemcpyAsync(o.h_col, ring_col, sizeof(float) * nb, cudaMemcpyDeviceToHost, ds),
                                "demand")))
                     break;
             }
@@ -905,22 +910,28 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if ((st = step())) break;
         if ((st = bucketize(nlive))) break;
 
-        // ---- predictor training after kTraceIters + kHorizon traced iterations
+        // ---- predictor training: once kTraceRing iterations are traced, and
+        // again (warm, fewer epochs) every kRetrain iterations on the sliding
+        // window of the last kTraceIters iterations whose horizon is observed
         if (tracing) {
             trace_t++;
-            if (trace_t == kTraceIters + kHorizon) {
+            if (trace_t >= kTraceRing && (trace_t - kTraceRing) % kRetrain == 0) {
                 if ((st = cuda(cudaStreamWaitEvent(ds, ev_buck, 0), "training wait"))) break;
-                if ((st = cuda(launch_targets(o.d_trace_col, kTraceIters, kHorizon, nb, o.d_trace_y, ds), "targets")))
+                if ((st = cuda(launch_gather_train(o.d_trace_x, o.d_trace_col, trace_t - kTraceRing, kTraceRing,
+                                                   kTraceIters, kHorizon, nb, o.d_train_x, o.d_trace_y, ds),
+                               "training set")))
                     break;
-                if ((st = cuda(mlp_train(o.d_params, o.d_trace_x, o.d_trace_y, kTraceIters * nb, kTrainEpochs,
-                                         kTrainLr, 0x6C6561726E6564ull, o.d_train_ws, nullptr, ds),
+                const bool first = !o.trained;
+                if ((st = cuda(mlp_train(o.d_params, o.d_train_x, o.d_trace_y, kTraceIters * nb,
+                                         first ? kTrainEpochs : kRetrainEpochs, kTrainLr,
+                                         first ? 0x6C6561726E6564ull : 0ull, o.d_train_ws, nullptr, ds),
                                "predictor training")))
                     break;
                 const float *loss_dev = o.d_train_ws + (uint64_t)kMlpGradCtas * (kMlpParams + 1) + 3 * kMlpParams;
                 if ((st = cuda(cudaMemcpyAsync(&o.train_loss, loss_dev, sizeof(float), cudaMemcpyDeviceToHost, ds),
                                "loss")))
                     break;
-                launches += 2 + 3 * kTrainEpochs;
+                launches += 1 + 3 * (first ? kTrainEpochs : kRetrainEpochs);
                 o.trained = true;
             }
         }

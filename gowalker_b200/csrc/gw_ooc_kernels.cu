@@ -585,7 +585,7 @@ __global__ void __launch_bounds__(1024) k_features(const FeatureArgs f)
         x[8] = log1pf(ema);
         x[9] = log1pf(arr);
         x[10] = f.live_frac;
-        x[11] = fminf((float)f.iter, 256.f) * (1.f / 256.f);
+        x[11] = 0.f;  // (the iteration count: left out, it only grows past what training saw)
         x[12] = colf * f.inv_live * (float)nb;
         x[13] = log1pf((float)(row + col - diag));
         x[14] = log1pf((float)(row - diag));
@@ -594,14 +594,31 @@ __global__ void __launch_bounds__(1024) k_features(const FeatureArgs f)
     }
 }
 
-__global__ void k_targets(const float *col_hist, uint32_t T, uint32_t k, uint32_t nb, float *y)
+// Training set from the trace ring (ring slots of kMlpIn features and of
+// demand per block; iteration t lives in slot t % ring): samples t0 .. t0+T-1
+// gathered in order, with targets y = log1p(mean demand over the next k
+// iterations) - x[0] (x[0] = log1p of the demand then), so the network
+// learns the change of log demand and an untrained one forecasts no change.
+__global__ void k_gather_train(const float *ring_x, const float *ring_col, uint32_t t0, uint32_t ring, uint32_t T,
+                               uint32_t k, uint32_t nb, float *train_x, float *y)
 {
     const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= T * nb) return;
-    const uint32_t t = idx / nb, i = idx % nb;
+    const uint32_t j = idx / nb, i = idx % nb;
+    const uint32_t t = t0 + j;
+    const float *xs = ring_x + ((uint64_t)(t % ring) * nb + i) * 16;
+    float *xd = train_x + (uint64_t)idx * 16;
+    for (int f = 0; f < 16; ++f) xd[f] = xs[f];
     float s = 0.f;
-    for (uint32_t d = 1; d <= k; ++d) s += col_hist[(uint64_t)(t + d) * nb + i];
-    y[idx] = log1pf(s / (float)k);
+    for (uint32_t d = 1; d <= k; ++d) s += ring_col[(uint64_t)((t + d) % ring) * nb + i];
+    y[idx] = log1pf(s / (float)k) - xs[0];
+}
+
+// pred[i] += x[i][0]: the residual forecast back to log demand.
+__global__ void k_add_level(float *pred, const float *x, uint32_t nb)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nb) pred[i] += x[(uint64_t)i * 16];
 }
 
 // One thread: fill free slots with the highest predicted uncached blocks, then
@@ -660,10 +677,17 @@ cudaError_t launch_features(const FeatureArgs &f, cudaStream_t s)
     return cudaGetLastError();
 }
 
-cudaError_t launch_targets(const float *col_hist, uint32_t T, uint32_t k, uint32_t nb, float *y, cudaStream_t s)
+cudaError_t launch_gather_train(const float *ring_x, const float *ring_col, uint32_t t0, uint32_t ring, uint32_t T,
+                                uint32_t k, uint32_t nb, float *train_x, float *y, cudaStream_t s)
 {
     const uint32_t n = T * nb;
-    k_targets<<<(n + 255) / 256, 256, 0, s>>>(col_hist, T, k, nb, y);
+    k_gather_train<<<(n + 255) / 256, 256, 0, s>>>(ring_x, ring_col, t0, ring, T, k, nb, train_x, y);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_add_level(float *pred, const float *x, uint32_t nb, cudaStream_t s)
+{
+    k_add_level<<<(nb + 255) / 256, 256, 0, s>>>(pred, x, nb);
     return cudaGetLastError();
 }
 

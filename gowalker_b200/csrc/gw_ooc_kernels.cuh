@@ -105,8 +105,13 @@ struct FeatureArgs {
     float *col;                        // [nb] walkers waiting with cur block = i (demand) out
 };
 cudaError_t launch_features(const FeatureArgs &f, cudaStream_t s);
-// y[t][i] = log1p(mean over t' in (t, t+k] of col_hist[t'][i]) for t < T
-cudaError_t launch_targets(const float *col_hist, uint32_t T, uint32_t k, uint32_t nb, float *y, cudaStream_t s);
+// Samples t0 .. t0+T-1 from the trace ring (iteration t in slot t % ring) into
+// train_x, with y[j][i] = log1p(mean demand over t+1 .. t+k) - x[t][i][0]: the
+// network forecasts the change of log demand
+cudaError_t launch_gather_train(const float *ring_x, const float *ring_col, uint32_t t0, uint32_t ring, uint32_t T,
+                                uint32_t k, uint32_t nb, float *train_x, float *y, cudaStream_t s);
+// pred[i] += x[i][0]
+cudaError_t launch_add_level(float *pred, const float *x, uint32_t nb, cudaStream_t s);
 // Up to lmax (block, cached position or -1 for a free slot) pairs by
 // predicted demand; out[0] = count, then the pairs.
 cudaError_t launch_learned_choose(const float *pred, uint32_t nb, const uint32_t *const *blk_csr,
