@@ -52,6 +52,17 @@ WORKLOADS = {
                      "blocks, 93.75 MB device cache",
                 scale=22, nverts=2_600_000, target=91_875_000, nsamples=162_500_000, ef=0, algo=0, maxhops=80,
                 wps=1, p=0.5, q=2.0, alpha=0.2, term=0.0, nblocks=64, cache=93_750_000, ooc=True),
+    "c4": dict(name="C4: out-of-core SOPR/SOSR transition rule (alpha 0.2, termination 0.15, max length 20), 2 walkers "
+                    "per vertex, undirected R-MAT scale 26 rejecting ids >= 65.6M, symmetrised and thinned to 3.6B "
+                    "directed edges, 128 equal-edge-mass blocks, 4 GB device cache",
+               scale=26, nverts=65_600_000, target=3_600_000_000, nsamples=2_100_000_000, ef=0, algo=1, maxhops=20,
+               wps=2, p=0.5, q=2.0, alpha=0.2, term=0.15, nblocks=128, cache=4_000_000_000, ooc=True, sym=True),
+    "c5": dict(name="C5: out-of-core Node2vec p=0.5 q=2 length 80, 1 walker/vertex, web-shaped graph: 133.6M vertices, "
+                    "5.5B directed edges, 80% of edges within +-65,536 of the source id, R-MAT (scale 28) sources and "
+                    "remaining edges, 256 equal-edge-mass blocks, 8 GB device cache",
+               scale=28, nverts=133_600_000, target=5_500_000_000, nsamples=8_300_000_000, ef=0, algo=0, maxhops=80,
+               wps=1, p=0.5, q=2.0, alpha=0.2, term=0.0, nblocks=256, cache=8_000_000_000, ooc=True, web=True,
+               local_permille=800, window=65536),
     "prep": dict(name="edge list -> CSR on the device (gw_edges_csr): R-MAT scale 24 ef 16 sample list "
                       "(268,435,456 u32 pairs, (a,b,c,d) = (0.57,0.19,0.19,0.05)), symmetrised, deduplicated, sorted",
                  scale=24, ef=16, prep=True),
@@ -139,10 +150,16 @@ def build_graph(gw, wl):
         nsamples = wl["nsamples"]
         for _ in range(4):
             try:
-                dg = gw.DeviceGraph(wl["scale"], nverts=wl["nverts"], nsamples=nsamples, seed=1, symmetric=False,
-                                    target_edges=wl["target"])
+                if wl.get("web"):
+                    dg = gw.DeviceGraph.web(wl["scale"], wl["nverts"], nsamples, local_permille=wl["local_permille"],
+                                            window=wl["window"], seed=1, target_edges=wl["target"])
+                else:
+                    dg = gw.DeviceGraph(wl["scale"], nverts=wl["nverts"], nsamples=nsamples, seed=1,
+                                        symmetric=bool(wl.get("sym")), target_edges=wl["target"])
                 break
-            except gw.GwError:
+            except gw.GwError as exc:
+                if exc.status != -1:
+                    raise
                 nsamples = int(nsamples * 1.2)  # too few unique edges: sample more
         else:
             raise RuntimeError("could not reach the target edge count")

@@ -6,9 +6,11 @@
 // (seed, sample index), so the graph is identical whichever device, chunking
 // or thread count builds it, and identical to the oracle's CPU build.
 //
-// Pipeline: sample kernel -> u64 keys (src<<32|dst, invalid = ~0) ->
-// radix sort (CUB) -> unique (CUB) -> optional even thinning to an exact edge
-// count -> offsets + neighbour extraction (csr_from_sorted).
+// Pipeline (sampled_csr): count the kept samples, write their packed keys
+// (src << bit_length(V-1) | dst) compacted, radix sort (CUB) -> unique (CUB)
+// -> optional even thinning to an exact edge count -> offsets + neighbour
+// extraction (csr_from_sorted).  Samplers: R-MAT (gw_rmat_csr) and the
+// web-shaped locality-ordered graph (gw_web_csr).
 //
 // The same key pipeline turns a caller's edge list into a CSR
 // (gw_edges_csr), and gw_split_blocks computes block split points from the
@@ -27,33 +29,117 @@
 
 namespace gw {
 
-__global__ void k_rmat_keys(uint32_t scale, uint32_t nverts, uint64_t nsamples, uint32_t t0, uint32_t t1,
-                            uint32_t t2, uint32_t k0, uint32_t k1, int symmetric, uint64_t *keys)
+constexpr uint32_t kTagWeb = 0x57454230u;  // 'WEB0'
+
+// R-MAT sample e: `scale` quadrant choices, level l from lane (l & 3) of
+// Philox(e_lo, e_hi, l >> 2, 'RMAT') against the u32 thresholds a, a+b, a+b+c.
+__device__ __forceinline__ void rmat_sample(uint64_t e, uint32_t scale, uint32_t t0, uint32_t t1, uint32_t t2,
+                                            uint32_t k0, uint32_t k1, uint32_t &s, uint32_t &d)
 {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nsamples; e += stride) {
-        uint32_t s = 0, d = 0;
-        U4 r{0, 0, 0, 0};
-        for (uint32_t l = 0; l < scale; ++l) {
-            if ((l & 3u) == 0) r = philox4x32_10((uint32_t)e, (uint32_t)(e >> 32), l >> 2, kTagRmat, k0, k1);
-            const uint32_t lanes[4] = {r.x, r.y, r.z, r.w};
-            const uint32_t u = lanes[l & 3u];
-            uint32_t sb, db;
-            if (u < t0) { sb = 0; db = 0; }
-            else if (u < t1) { sb = 0; db = 1; }
-            else if (u < t2) { sb = 1; db = 0; }
-            else { sb = 1; db = 1; }
-            s = (s << 1) | sb;
-            d = (d << 1) | db;
+    s = d = 0;
+    U4 r{0, 0, 0, 0};
+    for (uint32_t l = 0; l < scale; ++l) {
+        if ((l & 3u) == 0) r = philox4x32_10((uint32_t)e, (uint32_t)(e >> 32), l >> 2, kTagRmat, k0, k1);
+        const uint32_t lanes[4] = {r.x, r.y, r.z, r.w};
+        const uint32_t u = lanes[l & 3u];
+        uint32_t sb, db;
+        if (u < t0) { sb = 0; db = 0; }
+        else if (u < t1) { sb = 0; db = 1; }
+        else if (u < t2) { sb = 1; db = 0; }
+        else { sb = 1; db = 1; }
+        s = (s << 1) | sb;
+        d = (d << 1) | db;
+    }
+}
+
+struct RmatSampler {
+    uint32_t scale, nverts, t0, t1, t2, k0, k1;
+    __device__ bool operator()(uint64_t e, uint32_t &s, uint32_t &d) const
+    {
+        rmat_sample(e, scale, t0, t1, t2, k0, k1, s, d);
+        return s < nverts && d < nverts && s != d;
+    }
+};
+
+// Web-shaped sample e (locality-ordered ids): Philox(e_lo, e_hi, 0, 'WEB0')
+// lane x decides local (x % 1000 < local_permille) or not.  Both take the
+// R-MAT sample's source (hubs and out-degree skew from R-MAT's source
+// marginal); a local edge goes to src + o with o uniform over
+// [-window, -1] u [1, window] (lane y), clipped to [0, nverts); the rest keep
+// the R-MAT destination.
+struct WebSampler {
+    uint32_t scale, nverts, t0, t1, t2, k0, k1, local_permille, window;
+    __device__ bool operator()(uint64_t e, uint32_t &s, uint32_t &d) const
+    {
+        rmat_sample(e, scale, t0, t1, t2, k0, k1, s, d);
+        const U4 r = philox4x32_10((uint32_t)e, (uint32_t)(e >> 32), 0u, kTagWeb, k0, k1);
+        if (r.x % 1000u < local_permille) {
+            int64_t o = (int64_t)(r.y % (2u * window)) - (int64_t)window;
+            if (o >= 0) o += 1;
+            int64_t t = (int64_t)s + o;
+            t = t < 0 ? 0 : (t >= (int64_t)nverts ? (int64_t)nverts - 1 : t);
+            d = (uint32_t)t;
         }
-        const bool ok = s < nverts && d < nverts && s != d;
-        const uint64_t kf = ok ? (((uint64_t)s << 32) | d) : ~0ull;
-        if (symmetric) {
-            keys[2 * e] = kf;
-            keys[2 * e + 1] = ok ? (((uint64_t)d << 32) | s) : ~0ull;
-        } else {
-            keys[e] = kf;
+        return s < nverts && d < nverts && s != d;
+    }
+};
+
+// Sampled edges -> packed keys src << sh | dst of the kept samples (and their
+// reverses when symmetric), compacted: a block claims its output range with
+// one atomic per 1024 samples.  COUNT: only count the kept keys.
+template <class Sampler, bool COUNT>
+__global__ void __launch_bounds__(256)
+    k_sample_keys(Sampler smp, uint64_t nsamples, uint32_t sh, int symmetric, uint64_t *__restrict__ keys,
+                  unsigned long long *cursor)
+{
+    __shared__ unsigned int s_cnt;
+    __shared__ unsigned long long s_base;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t per = symmetric ? 2 : 1;
+    const uint64_t span = 256ull * 4;
+    unsigned long long total = 0;
+    for (uint64_t b0 = (uint64_t)blockIdx.x * span; b0 < nsamples; b0 += (uint64_t)gridDim.x * span) {
+        uint32_t sv[4], dv[4];
+        bool ok[4];
+        uint32_t c = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint64_t e = b0 + (uint64_t)k * 256 + threadIdx.x;
+            ok[k] = e < nsamples && smp(e, sv[k], dv[k]);
+            c += ok[k] ? 1u : 0u;
         }
+        if (COUNT) {
+            total += c;
+            continue;
+        }
+        if (threadIdx.x == 0) s_cnt = 0;
+        __syncthreads();
+        uint32_t x = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= (uint32_t)o) x += y;
+        }
+        uint32_t wbase = 0;
+        if (lane == 31) wbase = atomicAdd(&s_cnt, x);
+        wbase = __shfl_sync(0xFFFFFFFFu, wbase, 31);
+        __syncthreads();
+        if (threadIdx.x == 0) s_base = atomicAdd(cursor, (unsigned long long)s_cnt * per);
+        __syncthreads();
+        uint64_t pos = s_base + (uint64_t)(wbase + x - c) * per;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (!ok[k]) continue;
+            keys[pos] = ((uint64_t)sv[k] << sh) | dv[k];
+            if (symmetric) keys[pos + 1] = ((uint64_t)dv[k] << sh) | sv[k];
+            pos += per;
+        }
+        __syncthreads();
+    }
+    if (COUNT) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xFFFFFFFFu, total, o);
+        if (lane == 0 && total) atomicAdd(cursor, total * per);
     }
 }
 
@@ -370,6 +456,95 @@ struct PhaseTrace {
     }
 };
 
+// Sampled edge list -> CSR: count the kept keys, write them compacted and
+// packed (src << bit_length(nverts-1) | dst), radix-sort, drop repeats, thin
+// evenly to target_edges when given, then offsets and neighbour ids.
+template <class Sampler>
+static int sampled_csr(const Sampler &smp, uint64_t nsamples, uint32_t nverts, bool symmetric, uint64_t target_edges,
+                       uint64_t **d_beg, uint32_t **d_csr, uint64_t *nedges)
+{
+    cudaStream_t s = 0;
+    const uint32_t sh = bit_length32(nverts - 1);
+    const int blocks = 148 * 8;
+    uint64_t *keys = nullptr, *alt = nullptr, *beg = nullptr;
+    uint32_t *csr = nullptr;
+    unsigned long long *d_cur = nullptr, h_cur = 0;
+    int64_t *d_nsel = nullptr, nsel = 0;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0, tb2 = 0;
+    uint64_t U = 0;
+    int rc = GW_OK;
+    cudaError_t e = cudaSuccess;
+#define SC_CHECK(x)                       \
+    do {                                  \
+        if ((e = (x)) != cudaSuccess) {   \
+            rc = GW_ERR_CUDA;             \
+            goto out;                     \
+        }                                 \
+    } while (0)
+    SC_CHECK(cudaMalloc(&d_cur, sizeof(unsigned long long)));
+    SC_CHECK(cudaMalloc(&d_nsel, sizeof(int64_t)));
+    SC_CHECK(cudaMemsetAsync(d_cur, 0, sizeof(unsigned long long), s));
+    k_sample_keys<Sampler, true><<<blocks, 256, 0, s>>>(smp, nsamples, sh, symmetric ? 1 : 0, nullptr, d_cur);
+    SC_CHECK(cudaGetLastError());
+    SC_CHECK(cudaMemcpyAsync(&h_cur, d_cur, sizeof(h_cur), cudaMemcpyDeviceToHost, s));
+    SC_CHECK(cudaStreamSynchronize(s));
+    U = h_cur;
+    SC_CHECK(cudaMalloc(&keys, (U ? U : 1) * sizeof(uint64_t)));
+    SC_CHECK(cudaMalloc(&alt, (U ? U : 1) * sizeof(uint64_t)));
+    SC_CHECK(cudaMemsetAsync(d_cur, 0, sizeof(unsigned long long), s));
+    k_sample_keys<Sampler, false><<<blocks, 256, 0, s>>>(smp, nsamples, sh, symmetric ? 1 : 0, keys, d_cur);
+    SC_CHECK(cudaGetLastError());
+    if (U) {
+        cub::DoubleBuffer<uint64_t> db(keys, alt);
+        const int b1 = (int)(2 * sh);
+        SC_CHECK(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, U, 0, b1, s));
+        SC_CHECK(cub::DeviceSelect::Unique(nullptr, tb2, keys, alt, d_nsel, (int64_t)U, s));
+        tmp_bytes = std::max(tmp_bytes, tb2);
+        SC_CHECK(cudaMalloc(&tmp, tmp_bytes));
+        SC_CHECK(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, db, U, 0, b1, s));
+        keys = db.Current();
+        alt = db.Alternate();
+        SC_CHECK(cub::DeviceSelect::Unique(tmp, tmp_bytes, keys, alt, d_nsel, (int64_t)U, s));
+        SC_CHECK(cudaMemcpyAsync(&nsel, d_nsel, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        SC_CHECK(cudaStreamSynchronize(s));
+        std::swap(keys, alt);
+        U = (uint64_t)nsel;
+    }
+    if (target_edges > 0) {
+        if (U < target_edges) {
+            rc = GW_ERR_ARG;  // too few unique edges: sample more
+            goto out;
+        }
+        if (U > target_edges) {
+            k_thin<<<blocks * 2, 256, 0, s>>>(keys, U, U - target_edges, alt);
+            SC_CHECK(cudaGetLastError());
+            std::swap(keys, alt);
+            U = target_edges;
+        }
+    }
+    SC_CHECK(csr_from_sorted(keys, U, sh, nverts, s, &beg, &csr));
+    *d_beg = beg;
+    *d_csr = csr;
+    *nedges = U;
+    beg = nullptr;
+    csr = nullptr;
+out:
+#undef SC_CHECK
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (e == cudaErrorMemoryAllocation) rc = GW_ERR_NOMEM;
+    }
+    cudaFree(keys);
+    cudaFree(alt);
+    cudaFree(tmp);
+    cudaFree(d_cur);
+    cudaFree(d_nsel);
+    cudaFree(beg);
+    cudaFree(csr);
+    return rc;
+}
+
 }  // namespace gw
 
 using namespace gw;
@@ -386,64 +561,20 @@ extern "C" int gw_rmat_csr(uint32_t scale, uint32_t nverts, uint64_t nsamples, c
 {
     if (!thr || !d_beg || !d_csr || !nedges || scale == 0 || scale > 32 || nverts == 0) return GW_ERR_ARG;
     if (scale < 32 && (uint64_t)nverts > (1ull << scale)) return GW_ERR_ARG;
-    int rc = GW_OK;
-    const uint64_t nkeys = nsamples * (symmetric ? 2 : 1);
-    uint64_t *keys = nullptr, *alt = nullptr, *beg = nullptr;
-    uint32_t *csr = nullptr;
-    void *tmp = nullptr;
-    int64_t *d_nsel = nullptr;
-    size_t tmp_bytes = 0, tb2 = 0;
-    int64_t nsel = 0;
-    uint64_t U = 0;
-    const int threads = 256;
-    const int blocks = 148 * 16;
-    cudaStream_t s = 0;
+    const RmatSampler smp{scale, nverts, thr[0], thr[1], thr[2], (uint32_t)seed, (uint32_t)(seed >> 32)};
+    return sampled_csr(smp, nsamples, nverts, symmetric != 0, target_edges, d_beg, d_csr, nedges);
+}
 
-    GEN_CHECK(cudaMalloc(&keys, nkeys * sizeof(uint64_t)));
-    GEN_CHECK(cudaMalloc(&alt, nkeys * sizeof(uint64_t)));
-    GEN_CHECK(cudaMalloc(&d_nsel, sizeof(int64_t)));
-    k_rmat_keys<<<blocks, threads, 0, s>>>(scale, nverts, nsamples, thr[0], thr[1], thr[2], (uint32_t)seed,
-                                           (uint32_t)(seed >> 32), symmetric, keys);
-    GEN_CHECK(cudaGetLastError());
-    GEN_CHECK(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, keys, alt, nkeys, 0, 64, s));
-    GEN_CHECK(cub::DeviceSelect::Unique(nullptr, tb2, alt, keys, d_nsel, (int64_t)nkeys, s));
-    if (tb2 > tmp_bytes) tmp_bytes = tb2;
-    GEN_CHECK(cudaMalloc(&tmp, tmp_bytes));
-    GEN_CHECK(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, keys, alt, nkeys, 0, 64, s));
-    GEN_CHECK(cub::DeviceSelect::Unique(tmp, tmp_bytes, alt, keys, d_nsel, (int64_t)nkeys, s));
-    GEN_CHECK(cudaMemcpyAsync(&nsel, d_nsel, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    GEN_CHECK(cudaStreamSynchronize(s));
-    U = (uint64_t)nsel;
-    if (U > 0) {
-        uint64_t last = 0;
-        GEN_CHECK(cudaMemcpy(&last, keys + (U - 1), sizeof(uint64_t), cudaMemcpyDeviceToHost));
-        if (last == ~0ull) U -= 1;  // the invalid-sample marker sorts last
-    }
-    if (target_edges > 0) {
-        if (U < target_edges) { rc = GW_ERR_ARG; goto done; }
-        if (U > target_edges) {
-            k_thin<<<blocks, threads, 0, s>>>(keys, U, U - target_edges, alt);
-            GEN_CHECK(cudaGetLastError());
-            uint64_t *t = keys;
-            keys = alt;
-            alt = t;
-            U = target_edges;
-        }
-    }
-    GEN_CHECK(csr_from_sorted(keys, U, 32, nverts, s, &beg, &csr));
-    *d_beg = beg;
-    *d_csr = csr;
-    *nedges = U;
-    beg = nullptr;
-    csr = nullptr;
-done:
-    cudaFree(keys);
-    cudaFree(alt);
-    cudaFree(tmp);
-    cudaFree(d_nsel);
-    cudaFree(beg);
-    cudaFree(csr);
-    return rc;
+extern "C" int gw_web_csr(uint32_t scale, uint32_t nverts, uint64_t nsamples, const uint32_t thr[3],
+                          uint32_t local_permille, uint32_t window, uint64_t seed, uint64_t target_edges,
+                          uint64_t **d_beg, uint32_t **d_csr, uint64_t *nedges)
+{
+    if (!thr || !d_beg || !d_csr || !nedges || scale == 0 || scale > 32 || nverts == 0) return GW_ERR_ARG;
+    if (scale < 32 && (uint64_t)nverts > (1ull << scale)) return GW_ERR_ARG;
+    if (local_permille > 1000 || window == 0 || window > (1u << 30)) return GW_ERR_ARG;
+    const WebSampler smp{scale, nverts, thr[0], thr[1], thr[2], (uint32_t)seed, (uint32_t)(seed >> 32),
+                         local_permille, window};
+    return sampled_csr(smp, nsamples, nverts, false, target_edges, d_beg, d_csr, nedges);
 }
 
 extern "C" int gw_edges_csr(const uint32_t *src, const uint32_t *dst, uint64_t n, uint32_t nverts, uint32_t flags,

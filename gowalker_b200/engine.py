@@ -189,6 +189,26 @@ class DeviceGraph:
         self.beg_ptr, self.csr_ptr = db.value, dc.value
 
     @classmethod
+    def web(cls, scale, nverts, nsamples, local_permille=800, window=65536, abc=(0.57, 0.19, 0.19), seed=1,
+            target_edges=0):
+        """Web-shaped locality-ordered graph built on the device by gw_web_csr."""
+        L = _abi.load()
+        self = cls.__new__(cls)
+        self.L = L
+        self.beg_ptr = self.csr_ptr = None
+        a, b, c = abc
+        thr = [int(a * 4294967296.0), int((a + b) * 4294967296.0), int((a + b + c) * 4294967296.0)]
+        thr = (ctypes.c_uint32 * 3)(*[min(t, 0xFFFFFFFF) for t in thr])
+        db, dc, ne = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_uint64()
+        st = L.gw_web_csr(scale, nverts, nsamples, thr, local_permille, window, seed, target_edges,
+                          ctypes.byref(db), ctypes.byref(dc), ctypes.byref(ne))
+        if st != 0:
+            raise GwError(st, "gw_web_csr failed")
+        self.nverts, self.nedges = nverts, int(ne.value)
+        self.beg_ptr, self.csr_ptr = db.value, dc.value
+        return self
+
+    @classmethod
     def from_edges(cls, src, dst, nverts=0, symmetric=False, sort=True, dedup=False):
         """CSR of the edge list (src[i], dst[i]) built on the device by
         gw_edges_csr (the reference converter plus its neighbour sort,

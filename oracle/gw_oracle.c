@@ -124,6 +124,36 @@ void oracle_rmat_edges(uint32_t scale, uint64_t first, uint64_t count, const uin
         rmat_one(scale, first + (uint64_t)i, thr, seed, &src[i], &dst[i]);
 }
 
+#define WEB_TAG 0x57454230u /* 'WEB0' */
+
+/* Web-shaped sample e (locality-ordered ids), the device's WebSampler
+ * restated: the R-MAT sample's source; Philox(e_lo, e_hi, 0, 'WEB0') lane 0
+ * decides local (lane0 % 1000 < local_permille), and a local edge goes to
+ * src + o, o uniform over [-window, -1] u [1, window] from lane 1, clipped to
+ * [0, nverts).  Raw samples: the caller drops ids >= nverts and self loops. */
+void oracle_web_edges(uint32_t scale, uint32_t nverts, uint64_t first, uint64_t count, const uint32_t thr[3],
+                      uint32_t local_permille, uint32_t window, uint64_t seed, uint32_t *src, uint32_t *dst,
+                      int nthreads)
+{
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)count; ++i) {
+        const uint64_t e = first + (uint64_t)i;
+        uint32_t s, d, r[4];
+        rmat_one(scale, e, thr, seed, &s, &d);
+        draw4(seed, (uint32_t)e, (uint32_t)(e >> 32), 0u, WEB_TAG, r);
+        if (r[0] % 1000u < local_permille) {
+            int64_t o = (int64_t)(r[1] % (2u * window)) - (int64_t)window;
+            if (o >= 0) o += 1;
+            int64_t t = (int64_t)s + o;
+            t = t < 0 ? 0 : (t >= (int64_t)nverts ? (int64_t)nverts - 1 : t);
+            d = (uint32_t)t;
+        }
+        src[i] = s;
+        dst[i] = d;
+    }
+}
+
 /* ---------------------------------------------------------------- walks */
 
 typedef struct {

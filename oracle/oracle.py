@@ -93,6 +93,8 @@ def lib():
         L.oracle_philox4x32_10.argtypes = [u32p, u32p, u32p]
         L.oracle_rmat_edges.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, u32p,
                                         ctypes.c_uint64, u32p, u32p, ctypes.c_int]
+        L.oracle_web_edges.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, u32p,
+                                       ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.c_int]
         L.oracle_walk.argtypes = [u64p, u32p, ctypes.c_uint32, ctypes.POINTER(Cfg), ctypes.c_uint32,
                                   ctypes.c_uint32, u32p, u32p, u64p, u32p, ctypes.POINTER(Stats),
                                   ctypes.c_int]
@@ -140,6 +142,32 @@ def rmat_edges(scale: int, first: int, count: int, seed: int = 1, abc=RMAT_ABC, 
     lib().oracle_rmat_edges(scale, first, count, _p(thr, ctypes.c_uint32), seed,
                             _p(src, ctypes.c_uint32), _p(dst, ctypes.c_uint32), nthreads)
     return src, dst
+
+
+def web_edges(scale: int, nverts: int, first: int, count: int, local_permille: int = 800, window: int = 65536,
+              seed: int = 1, abc=RMAT_ABC, nthreads: int = 0):
+    """Raw web-shaped samples (gw_oracle.c oracle_web_edges): R-MAT sources,
+    80% of edges to a destination within +-window of the source."""
+    thr = rmat_thresholds(*abc)
+    src = np.empty(count, dtype=np.uint32)
+    dst = np.empty(count, dtype=np.uint32)
+    lib().oracle_web_edges(scale, nverts, first, count, _p(thr, ctypes.c_uint32), local_permille, window, seed,
+                           _p(src, ctypes.c_uint32), _p(dst, ctypes.c_uint32), nthreads)
+    return src, dst
+
+
+def thin_sorted(beg: np.ndarray, csr: np.ndarray, target: int):
+    """Keep `target` of the U sorted unique edges: edge i goes when
+    floor((i+1)k/U) > floor(ik/U), k = U - target (the device's k_thin)."""
+    U = len(csr)
+    k = U - target
+    if U >= (1 << 20):
+        raise ValueError("thin_sorted is for small cases")
+    keep = np.array([(ii + 1) * k // U == ii * k // U for ii in range(U)], dtype=bool)
+    src = np.repeat(np.arange(len(beg) - 1, dtype=np.int64), np.diff(beg.astype(np.int64)))[keep]
+    nb = np.zeros(len(beg), dtype=np.uint64)
+    nb[1:] = np.cumsum(np.bincount(src, minlength=len(beg) - 1)).astype(np.uint64)
+    return nb, csr[keep]
 
 
 def build_csr(nverts: int, src: np.ndarray, dst: np.ndarray, symmetric: bool = True):
