@@ -158,4 +158,7 @@ def test_generator_thinning_matches_oracle(gw, oracle, maker):
     b2, c2 = oracle.thin_sorted(b0, c0, target)
     assert np.array_equal(b1, b2) and np.array_equal(c1, c2)
     with pytest.raises(gw.GwError):
-        gw.DeviceGraph(scale, nverts=V, nsamples=n, seed=3, symmetric=False, target_edges=len(c0) + 1)
+        if maker == "rmat":
+            gw.DeviceGraph(scale, nverts=V, nsamples=n, seed=3, symmetric=False, target_edges=len(c0) + 1)
+        else:
+            gw.DeviceGraph.web(scale, V, n, window=100, seed=3, target_edges=len(c0) + 1)
