@@ -58,11 +58,12 @@ WORKLOADS = {
                scale=26, nverts=65_600_000, target=3_600_000_000, nsamples=2_100_000_000, ef=0, algo=1, maxhops=20,
                wps=2, p=0.5, q=2.0, alpha=0.2, term=0.15, nblocks=128, cache=4_000_000_000, ooc=True, sym=True),
     "c5": dict(name="C5: out-of-core Node2vec p=0.5 q=2 length 80, 1 walker/vertex, web-shaped graph: 133.6M vertices, "
-                    "5.5B directed edges, 80% of edges within +-65,536 of the source id, R-MAT (scale 28) sources and "
-                    "remaining edges, 256 equal-edge-mass blocks, 8 GB device cache",
-               scale=28, nverts=133_600_000, target=5_500_000_000, nsamples=8_300_000_000, ef=0, algo=0, maxhops=80,
+                    "5.5B directed edges, out-degree power law P(D>=d)=(d/6.8)^-1.1 (exponent 2.1, cap 65,536), 80% "
+                    "of edges within +-65,536 of the source id, the rest to R-MAT (scale 28) destinations, 256 "
+                    "equal-edge-mass blocks, 8 GB device cache",
+               scale=28, nverts=133_600_000, target=5_500_000_000, nsamples=0, ef=0, algo=0, maxhops=80,
                wps=1, p=0.5, q=2.0, alpha=0.2, term=0.0, nblocks=256, cache=8_000_000_000, ooc=True, web=True,
-               local_permille=800, window=65536),
+               dmin=6.8, tail=1.1, max_degree=65536, local_permille=800, window=65536),
     "prep": dict(name="edge list -> CSR on the device (gw_edges_csr): R-MAT scale 24 ef 16 sample list "
                       "(268,435,456 u32 pairs, (a,b,c,d) = (0.57,0.19,0.19,0.05)), symmetrised, deduplicated, sorted",
                  scale=24, ef=16, prep=True),
@@ -151,7 +152,8 @@ def build_graph(gw, wl):
         for _ in range(4):
             try:
                 if wl.get("web"):
-                    dg = gw.DeviceGraph.web(wl["scale"], wl["nverts"], nsamples, local_permille=wl["local_permille"],
+                    dg = gw.DeviceGraph.web(wl["scale"], wl["nverts"], dmin=wl["dmin"], tail=wl["tail"],
+                                            max_degree=wl["max_degree"], local_permille=wl["local_permille"],
                                             window=wl["window"], seed=1, target_edges=wl["target"])
                 else:
                     dg = gw.DeviceGraph(wl["scale"], nverts=wl["nverts"], nsamples=nsamples, seed=1,
@@ -161,6 +163,7 @@ def build_graph(gw, wl):
                 if exc.status != -1:
                     raise
                 nsamples = int(nsamples * 1.2)  # too few unique edges: sample more
+                wl["dmin"] = wl.get("dmin", 1.0) * 1.1
         else:
             raise RuntimeError("could not reach the target edge count")
         log("graph: V=%d E=%d from %d samples, built on device in %.1fs" % (dg.nverts, dg.nedges, nsamples,

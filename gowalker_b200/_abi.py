@@ -127,7 +127,8 @@ def load():
         "gw_checksum": ([vp, u64p, u64p], i32),
         "gw_bucket_counts": ([vp, vp], i32),
         "gw_rmat_csr": ([u32, u32, u64, u32p, u64, i32, u64, ctypes.POINTER(vp), ctypes.POINTER(vp), u64p], i32),
-        "gw_web_csr": ([u32, u32, u64, u32p, u32, u32, u64, u64, ctypes.POINTER(vp), ctypes.POINTER(vp), u64p], i32),
+        "gw_web_csr": ([u32, u32, u32p, ctypes.c_double, ctypes.c_double, u32, u32, u32, u64, u64,
+                        ctypes.POINTER(vp), ctypes.POINTER(vp), u64p], i32),
         "gw_edges_csr": ([vp, vp, u64, u32, u32, ctypes.POINTER(vp), ctypes.POINTER(vp), u64p, u32p], i32),
         "gw_split_blocks": ([vp, u32, u32, u64, vp, vp, u32, u32p], i32),
         "gw_sa_choose_blocks": ([vp, u32, vp, u32, u32, u64, u32, vp], i32),

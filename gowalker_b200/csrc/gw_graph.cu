@@ -9,8 +9,9 @@
 // Pipeline (sampled_csr): count the kept samples, write their packed keys
 // (src << bit_length(V-1) | dst) compacted, radix sort (CUB) -> unique (CUB)
 // -> optional even thinning to an exact edge count -> offsets + neighbour
-// extraction (csr_from_sorted).  Samplers: R-MAT (gw_rmat_csr) and the
-// web-shaped locality-ordered graph (gw_web_csr).
+// extraction (csr_from_sorted).  The web-shaped locality-ordered graph
+// (gw_web_csr) draws a power-law degree per vertex, scans the degrees and
+// writes each vertex's edges in place before the same sort.
 //
 // The same key pipeline turns a caller's edge list into a CSR
 // (gw_edges_csr), and gw_split_blocks computes block split points from the
@@ -24,6 +25,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include "gw_fixedmath.cuh"
 #include "gw_philox.cuh"
 #include "../../include/gowalker.h"
 
@@ -61,28 +63,78 @@ struct RmatSampler {
     }
 };
 
-// Web-shaped sample e (locality-ordered ids): Philox(e_lo, e_hi, 0, 'WEB0')
-// lane x decides local (x % 1000 < local_permille) or not.  Both take the
-// R-MAT sample's source (hubs and out-degree skew from R-MAT's source
-// marginal); a local edge goes to src + o with o uniform over
-// [-window, -1] u [1, window] (lane y), clipped to [0, nverts); the rest keep
-// the R-MAT destination.
-struct WebSampler {
-    uint32_t scale, nverts, t0, t1, t2, k0, k1, local_permille, window;
-    __device__ bool operator()(uint64_t e, uint32_t &s, uint32_t &d) const
-    {
-        rmat_sample(e, scale, t0, t1, t2, k0, k1, s, d);
-        const U4 r = philox4x32_10((uint32_t)e, (uint32_t)(e >> 32), 0u, kTagWeb, k0, k1);
-        if (r.x % 1000u < local_permille) {
-            int64_t o = (int64_t)(r.y % (2u * window)) - (int64_t)window;
-            if (o >= 0) o += 1;
-            int64_t t = (int64_t)s + o;
-            t = t < 0 ? 0 : (t >= (int64_t)nverts ? (int64_t)nverts - 1 : t);
-            d = (uint32_t)t;
-        }
-        return s < nverts && d < nverts && s != d;
-    }
+// Web-shaped graph (locality-ordered ids).  Vertex v's out-degree is
+// floor(dmin / u^(1/tail)) capped at max_degree, u = Philox(v, 0, 0, 'WDEG')
+// lane x / 2^32 (x = 0 read as 1): a power law P(D >= d) = (d/dmin)^-tail,
+// every vertex at least floor(dmin) edges, computed with the fixed-step log
+// and exp so the oracle reproduces it.  Edge j of v draws Philox(j, v, 0,
+// 'WEB0'): lane x % 1000 < local_permille makes it local, to v + o with o
+// uniform over [-window, -1] u [1, window] (lane y), clipped to [0, nverts);
+// otherwise its destination follows R-MAT's destination marginal over
+// `scale` levels (bit 1 for quadrants b and d; level l from lane l & 3 of
+// Philox(j, v, 1 + l/4, 'WEB0')), rejected when >= nverts.
+constexpr uint32_t kTagWebDeg = 0x57444547u;  // 'WDEG'
+
+struct WebParams {
+    uint32_t nverts, scale, t0, t1, t2, k0, k1, local_permille, window, max_degree;
+    double dmin, tail;
 };
+
+__device__ __forceinline__ uint32_t web_degree(const WebParams &p, uint32_t v)
+{
+    const U4 r = philox4x32_10(v, 0u, 0u, kTagWebDeg, p.k0, p.k1);
+    const uint32_t z = r.x ? r.x : 1u;
+    const double pw = fm_exp_nonpos(__ddiv_rn(fm_log_u32(z), p.tail));  // u^(1/tail), in (0, 1]
+    const double d = __ddiv_rn(p.dmin, pw);
+    return d >= (double)p.max_degree ? p.max_degree : (uint32_t)d;
+}
+
+// false when the edge is dropped (self loop after clipping, or a remote
+// destination >= nverts)
+__device__ __forceinline__ bool web_edge(const WebParams &p, uint32_t v, uint32_t j, uint32_t &dst)
+{
+    const U4 r = philox4x32_10(j, v, 0u, kTagWeb, p.k0, p.k1);
+    if (r.x % 1000u < p.local_permille) {
+        int64_t o = (int64_t)(r.y % (2u * p.window)) - (int64_t)p.window;
+        if (o >= 0) o += 1;
+        int64_t t = (int64_t)v + o;
+        t = t < 0 ? 0 : (t >= (int64_t)p.nverts ? (int64_t)p.nverts - 1 : t);
+        dst = (uint32_t)t;
+    } else {
+        uint32_t d = 0;
+        U4 q{0, 0, 0, 0};
+        for (uint32_t l = 0; l < p.scale; ++l) {
+            if ((l & 3u) == 0) q = philox4x32_10(j, v, 1u + (l >> 2), kTagWeb, p.k0, p.k1);
+            const uint32_t lanes[4] = {q.x, q.y, q.z, q.w};
+            const uint32_t u = lanes[l & 3u];
+            d = (d << 1) | (((u >= p.t0 && u < p.t1) || u >= p.t2) ? 1u : 0u);
+        }
+        dst = d;
+    }
+    return dst < p.nverts && dst != v;
+}
+
+__global__ void k_web_degrees(WebParams p, unsigned long long *deg)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v <= p.nverts; v += stride)
+        deg[v] = v < p.nverts ? web_degree(p, (uint32_t)v) : 0ull;
+}
+
+// Thread per vertex: edge j of v at estart[v] + j, key v << sh | dst, or the
+// marker ~0 for a dropped edge (it sorts after every kept key).
+__global__ void k_web_edges(WebParams p, const unsigned long long *__restrict__ estart, uint32_t sh,
+                            uint64_t *__restrict__ keys)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < p.nverts; v += stride) {
+        const uint64_t e0 = estart[v], n = estart[v + 1] - e0;
+        for (uint32_t j = 0; j < n; ++j) {
+            uint32_t d;
+            keys[e0 + j] = web_edge(p, (uint32_t)v, j, d) ? ((v << sh) | d) : ~0ull;
+        }
+    }
+}
 
 // Sampled edges -> packed keys src << sh | dst of the kept samples (and their
 // reverses when symmetric), compacted: a block claims its output range with
@@ -565,16 +617,106 @@ extern "C" int gw_rmat_csr(uint32_t scale, uint32_t nverts, uint64_t nsamples, c
     return sampled_csr(smp, nsamples, nverts, symmetric != 0, target_edges, d_beg, d_csr, nedges);
 }
 
-extern "C" int gw_web_csr(uint32_t scale, uint32_t nverts, uint64_t nsamples, const uint32_t thr[3],
-                          uint32_t local_permille, uint32_t window, uint64_t seed, uint64_t target_edges,
-                          uint64_t **d_beg, uint32_t **d_csr, uint64_t *nedges)
+extern "C" int gw_web_csr(uint32_t scale, uint32_t nverts, const uint32_t thr[3], double dmin, double tail,
+                          uint32_t max_degree, uint32_t local_permille, uint32_t window, uint64_t seed,
+                          uint64_t target_edges, uint64_t **d_beg, uint32_t **d_csr, uint64_t *nedges)
 {
-    if (!thr || !d_beg || !d_csr || !nedges || scale == 0 || scale > 32 || nverts == 0) return GW_ERR_ARG;
-    if (scale < 32 && (uint64_t)nverts > (1ull << scale)) return GW_ERR_ARG;
-    if (local_permille > 1000 || window == 0 || window > (1u << 30)) return GW_ERR_ARG;
-    const WebSampler smp{scale, nverts, thr[0], thr[1], thr[2], (uint32_t)seed, (uint32_t)(seed >> 32),
-                         local_permille, window};
-    return sampled_csr(smp, nsamples, nverts, false, target_edges, d_beg, d_csr, nedges);
+    if (!thr || !d_beg || !d_csr || !nedges || scale == 0 || scale > 32 || nverts < 2) return GW_ERR_ARG;
+    if (local_permille > 1000 || window == 0 || window > (1u << 30) || max_degree == 0) return GW_ERR_ARG;
+    if (!(dmin >= 1.0 && dmin <= 1e9) || !(tail >= 0.05 && tail <= 100.0)) return GW_ERR_ARG;
+    const WebParams p{nverts, scale, thr[0], thr[1], thr[2], (uint32_t)seed, (uint32_t)(seed >> 32),
+                      local_permille, window, max_degree, dmin, tail};
+    cudaStream_t s = 0;
+    const uint64_t nb = (uint64_t)nverts + 1;
+    const uint32_t sh = bit_length32(nverts - 1), bsrc = bit_length32(nverts);
+    unsigned long long *deg = nullptr, *estart = nullptr;
+    uint64_t *keys = nullptr, *alt = nullptr, *beg = nullptr;
+    uint32_t *csr = nullptr;
+    int64_t *d_nsel = nullptr, nsel = 0;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0, tb2 = 0;
+    uint64_t M = 0, U = 0;
+    int rc = GW_OK;
+    cudaError_t e = cudaSuccess;
+#define WB_CHECK(x)                       \
+    do {                                  \
+        if ((e = (x)) != cudaSuccess) {   \
+            rc = GW_ERR_CUDA;             \
+            goto out;                     \
+        }                                 \
+    } while (0)
+    WB_CHECK(cudaMalloc(&deg, nb * sizeof(unsigned long long)));
+    WB_CHECK(cudaMalloc(&estart, nb * sizeof(unsigned long long)));
+    WB_CHECK(cudaMalloc(&d_nsel, sizeof(int64_t)));
+    k_web_degrees<<<148 * 8, 256, 0, s>>>(p, deg);
+    WB_CHECK(cudaGetLastError());
+    WB_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, deg, estart, nb, s));
+    WB_CHECK(cudaMalloc(&tmp, tmp_bytes));
+    WB_CHECK(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, deg, estart, nb, s));
+    WB_CHECK(cudaMemcpyAsync(&M, estart + nverts, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    WB_CHECK(cudaStreamSynchronize(s));
+    cudaFree(tmp);
+    tmp = nullptr;
+    cudaFree(deg);
+    deg = nullptr;
+    WB_CHECK(cudaMalloc(&keys, (M ? M : 1) * sizeof(uint64_t)));
+    WB_CHECK(cudaMalloc(&alt, (M ? M : 1) * sizeof(uint64_t)));
+    k_web_edges<<<148 * 16, 128, 0, s>>>(p, estart, sh, keys);
+    WB_CHECK(cudaGetLastError());
+    if (M) {
+        cub::DoubleBuffer<uint64_t> db(keys, alt);
+        const int b1 = (int)(sh + bsrc);  // the marker's bits there are all ones: it sorts last
+        WB_CHECK(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, M, 0, b1, s));
+        WB_CHECK(cub::DeviceSelect::Unique(nullptr, tb2, keys, alt, d_nsel, (int64_t)M, s));
+        tmp_bytes = std::max(tmp_bytes, tb2);
+        WB_CHECK(cudaMalloc(&tmp, tmp_bytes));
+        WB_CHECK(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, db, M, 0, b1, s));
+        keys = db.Current();
+        alt = db.Alternate();
+        WB_CHECK(cub::DeviceSelect::Unique(tmp, tmp_bytes, keys, alt, d_nsel, (int64_t)M, s));
+        WB_CHECK(cudaMemcpyAsync(&nsel, d_nsel, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        WB_CHECK(cudaStreamSynchronize(s));
+        std::swap(keys, alt);
+        U = (uint64_t)nsel;
+        if (U) {
+            uint64_t last = 0;
+            WB_CHECK(cudaMemcpy(&last, keys + (U - 1), sizeof(uint64_t), cudaMemcpyDeviceToHost));
+            if (last == ~0ull) U -= 1;
+        }
+    }
+    if (target_edges > 0) {
+        if (U < target_edges) {
+            rc = GW_ERR_ARG;
+            goto out;
+        }
+        if (U > target_edges) {
+            k_thin<<<148 * 16, 256, 0, s>>>(keys, U, U - target_edges, alt);
+            WB_CHECK(cudaGetLastError());
+            std::swap(keys, alt);
+            U = target_edges;
+        }
+    }
+    WB_CHECK(csr_from_sorted(keys, U, sh, nverts, s, &beg, &csr));
+    *d_beg = beg;
+    *d_csr = csr;
+    *nedges = U;
+    beg = nullptr;
+    csr = nullptr;
+out:
+#undef WB_CHECK
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (e == cudaErrorMemoryAllocation) rc = GW_ERR_NOMEM;
+    }
+    cudaFree(deg);
+    cudaFree(estart);
+    cudaFree(keys);
+    cudaFree(alt);
+    cudaFree(tmp);
+    cudaFree(d_nsel);
+    cudaFree(beg);
+    cudaFree(csr);
+    return rc;
 }
 
 extern "C" int gw_edges_csr(const uint32_t *src, const uint32_t *dst, uint64_t n, uint32_t nverts, uint32_t flags,

@@ -29,6 +29,7 @@
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
+#include "gw_fixedmath.cuh"
 #include "gw_ooc_kernels.cuh"
 #include "gw_philox.cuh"
 #include "../../include/gowalker.h"
@@ -40,35 +41,11 @@ constexpr uint32_t kSaSmemMaxNb = 200;     // counts staged in shared memory up 
 constexpr uint32_t kSaMaxRounds = 1u << 20;
 constexpr uint32_t kSaDraws = 1024;        // annealing draws made per CTA pass
 
-// 1/(2j+1) rounded to nearest (each a correctly rounded quotient), j = 0..11.
-__constant__ double kInvOdd[12] = {1.0 / 1,  1.0 / 3,  1.0 / 5,  1.0 / 7,  1.0 / 9,  1.0 / 11,
-                                   1.0 / 13, 1.0 / 15, 1.0 / 17, 1.0 / 19, 1.0 / 21, 1.0 / 23};
-
-// ln(z * 2^-32) for a 32-bit draw z, in IEEE double with every operation
-// rounded to nearest (no contraction), so any IEEE implementation of the same
-// steps gives the same bits: u = m 2^e with m in [sqrt(1/2), sqrt(2)),
-// ln u = e ln2 + 2 atanh(s), s = (m-1)/(m+1), the atanh series to s^23/23
-// by Horner in s^2 (|s| < 0.172: truncation below 1e-19).  z = 0 gives -inf.
-// Acceptance "d > ln(u)" is the reference's "u < exp(d)", with the
-// transcendental moved off the annealing chain into the parallel draw pass.
-__device__ double sa_log_draw(uint32_t z)
-{
-    if (z == 0) return -__longlong_as_double(0x7FF0000000000000ll);
-    int e = 31 - __clz(z);             // z = 2^e * (1.f), e in [0, 31]
-    double m = (double)z * ldexp(1.0, -e);  // exact: [1, 2)
-    if (m >= 1.4142135623730951) {
-        m = __dmul_rn(m, 0.5);  // exact
-        e += 1;
-    }
-    const double s = __ddiv_rn(__dsub_rn(m, 1.0), __dadd_rn(m, 1.0));
-    const double s2 = __dmul_rn(s, s);
-    double q = kInvOdd[11];
-    for (int j = 10; j >= 0; --j) q = __dadd_rn(kInvOdd[j], __dmul_rn(s2, q));
-    const double lnm = __dmul_rn(__dmul_rn(2.0, s), q);
-    const double ex = (double)(e - 32);
-    // ln2 split as 45426 * 2^-16 (exact products) plus the remainder
-    return __dadd_rn(__dadd_rn(__dmul_rn(ex, 0.693145751953125), __dmul_rn(ex, 1.4286068203094172e-06)), lnm);
-}
+// ln(u) of a round's 32-bit draw by the fixed steps of fm_log_u32 (the
+// oracle restates them): acceptance "d > ln(u)" is the reference's
+// "u < exp(d)", with the transcendental moved off the annealing chain into
+// the parallel draw pass.
+__device__ __forceinline__ double sa_log_draw(uint32_t z) { return fm_log_u32(z); }
 
 __device__ __forceinline__ float sa_score(uint32_t score, uint32_t comm, uint32_t k)
 {

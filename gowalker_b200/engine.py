@@ -189,9 +189,11 @@ class DeviceGraph:
         self.beg_ptr, self.csr_ptr = db.value, dc.value
 
     @classmethod
-    def web(cls, scale, nverts, nsamples, local_permille=800, window=65536, abc=(0.57, 0.19, 0.19), seed=1,
-            target_edges=0):
-        """Web-shaped locality-ordered graph built on the device by gw_web_csr."""
+    def web(cls, scale, nverts, dmin=6.0, tail=1.1, max_degree=65536, local_permille=800, window=65536,
+            abc=(0.57, 0.19, 0.19), seed=1, target_edges=0):
+        """Web-shaped locality-ordered graph built on the device by gw_web_csr:
+        power-law out-degrees (P(D >= d) = (d/dmin)^-tail), local edges within
+        +-window of the source, the rest to R-MAT-distributed destinations."""
         L = _abi.load()
         self = cls.__new__(cls)
         self.L = L
@@ -200,7 +202,7 @@ class DeviceGraph:
         thr = [int(a * 4294967296.0), int((a + b) * 4294967296.0), int((a + b + c) * 4294967296.0)]
         thr = (ctypes.c_uint32 * 3)(*[min(t, 0xFFFFFFFF) for t in thr])
         db, dc, ne = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_uint64()
-        st = L.gw_web_csr(scale, nverts, nsamples, thr, local_permille, window, seed, target_edges,
+        st = L.gw_web_csr(scale, nverts, thr, dmin, tail, max_degree, local_permille, window, seed, target_edges,
                           ctypes.byref(db), ctypes.byref(dc), ctypes.byref(ne))
         if st != 0:
             raise GwError(st, "gw_web_csr failed")

@@ -276,17 +276,21 @@ int gw_split_blocks(const uint64_t *beg, uint32_t nverts, uint32_t mode, uint64_
                     uint64_t *eblocks, uint32_t cap, uint32_t *nblocks);
 
 /* Web-shaped synthetic graph on the device (locality-ordered ids, the
- * full-pipeline workload's stand-in): sample e takes the R-MAT sample e's
- * source (scale / thr as gw_rmat_csr); with probability local_permille/1000
- * (Philox(e, 0, 'WEB0') lane 0 % 1000) its destination is src + o, o uniform
- * over [-window, -1] u [1, window], clipped to [0, nverts); otherwise the
- * R-MAT destination.  Ids >= nverts are rejected, self loops dropped,
- * duplicates removed, adjacency sorted, then thinned evenly to target_edges
- * when non-zero (GW_ERR_ARG if fewer unique edges).  Directed.  Outputs as
+ * full-pipeline workload's stand-in), directed.  Vertex v's out-degree is
+ * floor(dmin / u^(1/tail)) capped at max_degree, u from Philox(v, 0, 0,
+ * 'WDEG') -- a power law P(D >= d) = (d/dmin)^-tail (density exponent
+ * 1 + tail), at least floor(dmin) per vertex.  Edge j of v: with probability
+ * local_permille/1000 (Philox(j, v, 0, 'WEB0') lane 0 % 1000) it goes to
+ * v + o, o uniform over [-window, -1] u [1, window], clipped to [0, nverts);
+ * otherwise to a destination drawn from R-MAT's destination marginal over
+ * `scale` levels (thr as gw_rmat_csr), rejected when >= nverts.  Self loops
+ * and repeats dropped, adjacency sorted, then thinned evenly to target_edges
+ * when non-zero (GW_ERR_ARG if fewer edges).  The power and log use fixed
+ * IEEE-double steps so a CPU restatement reproduces the graph.  Outputs as
  * gw_rmat_csr. */
-int gw_web_csr(uint32_t scale, uint32_t nverts, uint64_t nsamples, const uint32_t thr[3], uint32_t local_permille,
-               uint32_t window, uint64_t seed, uint64_t target_edges, uint64_t **d_beg, uint32_t **d_csr,
-               uint64_t *nedges);
+int gw_web_csr(uint32_t scale, uint32_t nverts, const uint32_t thr[3], double dmin, double tail, uint32_t max_degree,
+               uint32_t local_permille, uint32_t window, uint64_t seed, uint64_t target_edges, uint64_t **d_beg,
+               uint32_t **d_csr, uint64_t *nedges);
 
 int gw_device_free(void *p);
 

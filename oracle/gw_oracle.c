@@ -42,6 +42,7 @@
  * distinct sectors touched by the binary search of each trial.  These give the
  * algorithmic bytes per step used for the roofline.
  */
+#include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -124,33 +125,91 @@ void oracle_rmat_edges(uint32_t scale, uint64_t first, uint64_t count, const uin
         rmat_one(scale, first + (uint64_t)i, thr, seed, &src[i], &dst[i]);
 }
 
-#define WEB_TAG 0x57454230u /* 'WEB0' */
+#define WEB_TAG 0x57454230u  /* 'WEB0' */
+#define WDEG_TAG 0x57444547u /* 'WDEG' */
 
-/* Web-shaped sample e (locality-ordered ids), the device's WebSampler
- * restated: the R-MAT sample's source; Philox(e_lo, e_hi, 0, 'WEB0') lane 0
- * decides local (lane0 % 1000 < local_permille), and a local edge goes to
- * src + o, o uniform over [-window, -1] u [1, window] from lane 1, clipped to
- * [0, nverts).  Raw samples: the caller drops ids >= nverts and self loops. */
-void oracle_web_edges(uint32_t scale, uint32_t nverts, uint64_t first, uint64_t count, const uint32_t thr[3],
-                      uint32_t local_permille, uint32_t window, uint64_t seed, uint32_t *src, uint32_t *dst,
-                      int nthreads)
+/* Fixed-step ln(z * 2^-32) and exp(x <= 0) in IEEE double, the device's
+ * fm_log_u32 / fm_exp_nonpos step for step (this file builds with
+ * -ffp-contract=off, so every operation rounds to nearest on its own). */
+static double fm_log_u32(uint32_t z)
 {
-    if (nthreads > 0) omp_set_num_threads(nthreads);
+    if (z == 0) return -INFINITY;
+    int e = 31 - __builtin_clz(z);
+    double m = (double)z * ldexp(1.0, -e);
+    if (m >= 1.4142135623730951) {
+        m = m * 0.5;
+        e += 1;
+    }
+    const double s = (m - 1.0) / (m + 1.0);
+    const double s2 = s * s;
+    double q = 1.0 / 23;
+    for (int j = 10; j >= 0; --j) q = 1.0 / (2 * j + 1) + s2 * q;
+    const double lnm = (2.0 * s) * q;
+    const double ex = (double)(e - 32);
+    return (ex * 0.693145751953125 + ex * 1.4286068203094172e-06) + lnm;
+}
+
+static double fm_exp_nonpos(double x)
+{
+    if (!(x > -700.0)) return 0.0;
+    if (x >= 0.0) return 1.0;
+    const double nd = nearbyint(x * 1.4426950408889634);
+    const double r = (x - nd * 0.693145751953125) - nd * 1.4286068203094172e-06;
+    double q = 1.0;
+    for (int k = 13; k >= 1; --k) q = 1.0 + (r * q) * (1.0 / k);
+    return ldexp(q, (int)nd);
+}
+
+/* Web-shaped graph (gw_web_csr restated).  Out-degree of v:
+ * floor(dmin / u^(1/tail)) capped at max_degree, u = Philox(v, 0, 0, 'WDEG')
+ * lane 0 / 2^32 (0 read as 1). */
+void oracle_web_degrees(uint32_t nverts, double dmin, double tail, uint32_t max_degree, uint64_t seed,
+                        uint64_t *deg)
+{
 #pragma omp parallel for schedule(static)
-    for (int64_t i = 0; i < (int64_t)count; ++i) {
-        const uint64_t e = first + (uint64_t)i;
-        uint32_t s, d, r[4];
-        rmat_one(scale, e, thr, seed, &s, &d);
-        draw4(seed, (uint32_t)e, (uint32_t)(e >> 32), 0u, WEB_TAG, r);
-        if (r[0] % 1000u < local_permille) {
-            int64_t o = (int64_t)(r[1] % (2u * window)) - (int64_t)window;
-            if (o >= 0) o += 1;
-            int64_t t = (int64_t)s + o;
-            t = t < 0 ? 0 : (t >= (int64_t)nverts ? (int64_t)nverts - 1 : t);
-            d = (uint32_t)t;
+    for (int64_t v = 0; v < (int64_t)nverts; ++v) {
+        uint32_t r[4];
+        draw4(seed, (uint32_t)v, 0u, 0u, WDEG_TAG, r);
+        const uint32_t z = r[0] ? r[0] : 1u;
+        const double pw = fm_exp_nonpos(fm_log_u32(z) / tail);
+        const double d = dmin / pw;
+        deg[v] = d >= (double)max_degree ? max_degree : (uint64_t)d;
+    }
+}
+
+/* Edge j of v at estart[v] + j: Philox(j, v, 0, 'WEB0') lane 0 % 1000 <
+ * local_permille makes it local (v + o, o uniform over [-window, -1] u
+ * [1, window] from lane 1, clipped); otherwise the destination takes `scale`
+ * bits from R-MAT's destination marginal (quadrants b, d; level l from lane
+ * l & 3 of Philox(j, v, 1 + l/4, 'WEB0')).  dst = 0xFFFFFFFF marks a dropped
+ * edge (self loop or destination >= nverts). */
+void oracle_web_edges(uint32_t scale, uint32_t nverts, const uint32_t thr[3], uint32_t local_permille,
+                      uint32_t window, uint64_t seed, const uint64_t *estart, uint32_t *src, uint32_t *dst)
+{
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t v = 0; v < (int64_t)nverts; ++v) {
+        for (uint64_t j = 0; j < estart[v + 1] - estart[v]; ++j) {
+            uint32_t r[4], d;
+            draw4(seed, (uint32_t)j, (uint32_t)v, 0u, WEB_TAG, r);
+            if (r[0] % 1000u < local_permille) {
+                int64_t o = (int64_t)(r[1] % (2u * window)) - (int64_t)window;
+                if (o >= 0) o += 1;
+                int64_t t = v + o;
+                t = t < 0 ? 0 : (t >= (int64_t)nverts ? (int64_t)nverts - 1 : t);
+                d = (uint32_t)t;
+            } else {
+                uint32_t q[4] = {0, 0, 0, 0};
+                d = 0;
+                for (uint32_t l = 0; l < scale; ++l) {
+                    if ((l & 3u) == 0) draw4(seed, (uint32_t)j, (uint32_t)v, 1u + (l >> 2), WEB_TAG, q);
+                    const uint32_t u = q[l & 3u];
+                    d = (d << 1) | (((u >= thr[0] && u < thr[1]) || u >= thr[2]) ? 1u : 0u);
+                }
+            }
+            const uint64_t e = estart[v] + j;
+            src[e] = (uint32_t)v;
+            dst[e] = (d < nverts && d != (uint32_t)v) ? d : 0xFFFFFFFFu;
         }
-        src[i] = s;
-        dst[i] = d;
     }
 }
 

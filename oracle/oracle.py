@@ -93,8 +93,10 @@ def lib():
         L.oracle_philox4x32_10.argtypes = [u32p, u32p, u32p]
         L.oracle_rmat_edges.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, u32p,
                                         ctypes.c_uint64, u32p, u32p, ctypes.c_int]
-        L.oracle_web_edges.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, u32p,
-                                       ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.c_int]
+        L.oracle_web_degrees.argtypes = [ctypes.c_uint32, ctypes.c_double, ctypes.c_double, ctypes.c_uint32,
+                                         ctypes.c_uint64, u64p]
+        L.oracle_web_edges.argtypes = [ctypes.c_uint32, ctypes.c_uint32, u32p, ctypes.c_uint32, ctypes.c_uint32,
+                                       ctypes.c_uint64, u64p, u32p, u32p]
         L.oracle_walk.argtypes = [u64p, u32p, ctypes.c_uint32, ctypes.POINTER(Cfg), ctypes.c_uint32,
                                   ctypes.c_uint32, u32p, u32p, u64p, u32p, ctypes.POINTER(Stats),
                                   ctypes.c_int]
@@ -144,16 +146,29 @@ def rmat_edges(scale: int, first: int, count: int, seed: int = 1, abc=RMAT_ABC, 
     return src, dst
 
 
-def web_edges(scale: int, nverts: int, first: int, count: int, local_permille: int = 800, window: int = 65536,
-              seed: int = 1, abc=RMAT_ABC, nthreads: int = 0):
-    """Raw web-shaped samples (gw_oracle.c oracle_web_edges): R-MAT sources,
-    80% of edges to a destination within +-window of the source."""
+def web_degrees(nverts: int, dmin: float = 6.0, tail: float = 1.1, max_degree: int = 65536, seed: int = 1):
+    """Out-degree draws of the web-shaped graph (gw_oracle.c oracle_web_degrees)."""
+    deg = np.empty(nverts, dtype=np.uint64)
+    lib().oracle_web_degrees(nverts, dmin, tail, max_degree, seed, _p(deg, ctypes.c_uint64))
+    return deg
+
+
+def web_graph(scale: int, nverts: int, dmin: float = 6.0, tail: float = 1.1, max_degree: int = 65536,
+              local_permille: int = 800, window: int = 65536, seed: int = 1, abc=RMAT_ABC):
+    """The web-shaped graph's CSR before thinning (gw_web_csr restated):
+    power-law degrees, each vertex's edges drawn in place, dropped ones
+    removed, repeats removed, adjacency sorted."""
+    deg = web_degrees(nverts, dmin, tail, max_degree, seed)
+    estart = np.zeros(nverts + 1, dtype=np.uint64)
+    estart[1:] = np.cumsum(deg)
+    m = int(estart[-1])
+    src = np.empty(m, dtype=np.uint32)
+    dst = np.empty(m, dtype=np.uint32)
     thr = rmat_thresholds(*abc)
-    src = np.empty(count, dtype=np.uint32)
-    dst = np.empty(count, dtype=np.uint32)
-    lib().oracle_web_edges(scale, nverts, first, count, _p(thr, ctypes.c_uint32), local_permille, window, seed,
-                           _p(src, ctypes.c_uint32), _p(dst, ctypes.c_uint32), nthreads)
-    return src, dst
+    lib().oracle_web_edges(scale, nverts, _p(thr, ctypes.c_uint32), local_permille, window, seed,
+                           _p(estart, ctypes.c_uint64), _p(src, ctypes.c_uint32), _p(dst, ctypes.c_uint32))
+    keep = dst != 0xFFFFFFFF
+    return build_csr(nverts, src[keep], dst[keep], symmetric=False)
 
 
 def thin_sorted(beg: np.ndarray, csr: np.ndarray, target: int):

@@ -124,17 +124,17 @@ def test_split_equal_edges_matches_restatement(gw, oracle, nblocks):
         assert np.array_equal(vb, rv) and np.array_equal(eb, re_)
 
 
-@pytest.mark.parametrize("window,local", [(64, 800), (4096, 500), (3, 1000)])
-def test_web_graph_matches_oracle(gw, oracle, window, local):
-    """The web-shaped generator (R-MAT sources, local destinations) against
-    the oracle's restatement of its sampler."""
-    scale, V, n = 14, 12000, 300000
-    g = gw.DeviceGraph.web(scale, V, n, local_permille=local, window=window, seed=7)
+@pytest.mark.parametrize("window,local,dmin", [(64, 800, 6.0), (4096, 500, 3.5), (3, 1000, 2.0)])
+def test_web_graph_matches_oracle(gw, oracle, window, local, dmin):
+    """The web-shaped generator (power-law out-degrees drawn with the
+    fixed-step log/exp, local and R-MAT-distributed destinations) against the
+    oracle's restatement."""
+    scale, V = 14, 12000
+    g = gw.DeviceGraph.web(scale, V, dmin=dmin, local_permille=local, window=window, seed=7)
     b1, c1 = g.to_host()
-    s, d = oracle.web_edges(scale, V, 0, n, local, window, seed=7)
-    keep = (s < V) & (d < V)
-    b2, c2 = oracle.build_csr(V, s[keep], d[keep], symmetric=False)
+    b2, c2 = oracle.web_graph(scale, V, dmin=dmin, local_permille=local, window=window, seed=7)
     assert np.array_equal(b1, b2) and np.array_equal(c1, c2)
+    assert np.diff(b1.astype(np.int64)).min() >= 1  # every vertex keeps an out-edge
 
 
 @pytest.mark.parametrize("maker", ["rmat", "web"])
@@ -143,17 +143,17 @@ def test_generator_thinning_matches_oracle(gw, oracle, maker):
     if maker == "rmat":
         full = gw.DeviceGraph(scale, nverts=V, nsamples=n, seed=3, symmetric=False)
         s, d = oracle.rmat_edges(scale, 0, n, 3)
+        keep = (s < V) & (d < V)
+        b0, c0 = oracle.build_csr(V, s[keep], d[keep], symmetric=False)
     else:
-        full = gw.DeviceGraph.web(scale, V, n, window=100, seed=3)
-        s, d = oracle.web_edges(scale, V, 0, n, 800, 100, seed=3)
-    keep = (s < V) & (d < V)
-    b0, c0 = oracle.build_csr(V, s[keep], d[keep], symmetric=False)
+        full = gw.DeviceGraph.web(scale, V, window=100, seed=3)
+        b0, c0 = oracle.web_graph(scale, V, window=100, seed=3)
     assert full.nedges == len(c0)
     target = len(c0) - len(c0) // 7
     if maker == "rmat":
         thin = gw.DeviceGraph(scale, nverts=V, nsamples=n, seed=3, symmetric=False, target_edges=target)
     else:
-        thin = gw.DeviceGraph.web(scale, V, n, window=100, seed=3, target_edges=target)
+        thin = gw.DeviceGraph.web(scale, V, window=100, seed=3, target_edges=target)
     b1, c1 = thin.to_host()
     b2, c2 = oracle.thin_sorted(b0, c0, target)
     assert np.array_equal(b1, b2) and np.array_equal(c1, c2)
@@ -161,4 +161,4 @@ def test_generator_thinning_matches_oracle(gw, oracle, maker):
         if maker == "rmat":
             gw.DeviceGraph(scale, nverts=V, nsamples=n, seed=3, symmetric=False, target_edges=len(c0) + 1)
         else:
-            gw.DeviceGraph.web(scale, V, n, window=100, seed=3, target_edges=len(c0) + 1)
+            gw.DeviceGraph.web(scale, V, window=100, seed=3, target_edges=len(c0) + 1)

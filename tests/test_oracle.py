@@ -315,3 +315,13 @@ def test_sa_choice_properties(oracle):
     assert 3 in s  # the block the hot walkers wait for
     assert np.array_equal(s, oracle.sa_choose_blocks(c, [], 6, 1, 0))
     assert sorted(oracle.sa_choose_blocks(c, [], 25, 1, 0).tolist()) == list(range(20))
+
+
+def test_web_degrees_power_law(oracle):
+    """Out-degrees of the web-shaped graph: at least floor(dmin), a power-law
+    tail P(D >= d) ~ d^-1.1 (density exponent 2.1), capped."""
+    deg = oracle.web_degrees(200000, 6.0, 1.1, 65536, 1).astype(np.float64)
+    assert deg.min() == 6 and deg.max() <= 65536
+    for a, b in [(20, 200), (50, 2000)]:
+        slope = np.log((deg >= b).mean() / (deg >= a).mean()) / np.log(b / a)
+        assert abs(slope + 1.1) < 0.05, slope
