@@ -23,6 +23,7 @@ GW_SPLIT_REFERENCE, GW_SPLIT_EQUAL_EDGES = 0, 1
 EXPORTS = (
     "gw_version", "gw_status_string", "gw_config_default", "gw_create", "gw_destroy", "gw_last_error",
     "gw_set_config", "gw_stream", "gw_set_graph_meta", "gw_host_block", "gw_device_graph", "gw_cache_reset",
+    "gw_host_weights", "gw_device_weights",
     "gw_init_walkers", "gw_run", "gw_num_walkers", "gw_get_paths", "gw_path_hashes", "gw_checksum",
     "gw_bucket_counts", "gw_rmat_csr", "gw_web_csr", "gw_edges_csr", "gw_split_blocks", "gw_sa_choose_blocks", "gw_device_free", "gw_memcpy", "gw_walk_noalloc",
     "gw_mlp_forward", "gw_mlp_grad", "gw_mlp_train", "gw_host_alloc", "gw_host_free",
@@ -119,6 +120,8 @@ def load():
         "gw_host_block": ([vp, u32, vp, vp], i32),
         "gw_device_graph": ([vp, vp, vp], i32),
         "gw_cache_reset": ([vp], i32),
+        "gw_host_weights": ([vp, u32, vp], i32),
+        "gw_device_weights": ([vp, vp], i32),
         "gw_init_walkers": ([vp, u32, u32, u64], i32),
         "gw_run": ([vp, u32, ctypes.POINTER(GwStats)], i32),
         "gw_num_walkers": ([vp, u64p], i32),

@@ -198,6 +198,11 @@ void gw_handle::release()
     if (s_copy) cudaStreamSynchronize(s_copy);
     cudaFree(own_beg);
     cudaFree(own_csr);
+    cudaFree(own_w);
+    cudaFree(d_alias);
+    own_w = nullptr;
+    d_alias = nullptr;
+    alias_ready = false;
     cudaFree(d_paths);
     cudaFree(d_lens);
     cudaFree(d_hashes);
@@ -224,7 +229,8 @@ void gw_handle::release()
 
 uint64_t gw_handle::graph_bytes() const
 {
-    return ((uint64_t)nverts + 1) * sizeof(uint64_t) + nedges * sizeof(uint32_t);
+    return ((uint64_t)nverts + 1) * sizeof(uint64_t) + nedges * sizeof(uint32_t) +
+           (weighted ? nedges * (sizeof(float) + sizeof(gw::AliasEntry)) : 0);
 }
 
 bool gw_handle::host_graph_complete() const
@@ -264,6 +270,20 @@ int gw_handle::upload_whole_graph(cudaStream_t s, uint64_t *h2d)
                 return st;
             bytes += ne * sizeof(uint32_t);
         }
+    }
+    if (weighted && !device_graph) {
+        if (!own_w && (st = cuda(cudaMalloc(&own_w, (nedges ? nedges : 1) * sizeof(float)), "edge weights")))
+            return st;
+        for (uint32_t b = 0; b < nblocks; ++b) {
+            const uint64_t ne = eblocks[b + 1] - eblocks[b];
+            if (!ne) continue;
+            if ((st = cuda(cudaMemcpyAsync(own_w + eblocks[b], host_w[b], ne * sizeof(float), cudaMemcpyHostToDevice,
+                                           s), "block weights H2D")))
+                return st;
+            bytes += ne * sizeof(float);
+        }
+        dev_w = own_w;
+        alias_ready = false;
     }
     dev_beg = own_beg;
     dev_csr = own_csr;
@@ -326,6 +346,12 @@ extern "C" int gw_set_graph_meta(gw_handle *h, uint32_t nverts, uint64_t nedges,
     h->eblocks.assign(eblocks, eblocks + nblocks + 1);
     h->host_beg.assign(nblocks, nullptr);
     h->host_csr.assign(nblocks, nullptr);
+    h->host_w.assign(nblocks, nullptr);
+    h->weighted = false;
+    h->dev_w = nullptr;
+    cudaFree(h->own_w);
+    h->own_w = nullptr;
+    h->alias_ready = false;
     h->dev_beg = nullptr;
     h->dev_csr = nullptr;
     h->resident = false;
@@ -369,6 +395,41 @@ extern "C" int gw_device_graph(gw_handle *h, const uint64_t *d_beg, const uint32
     h->resident = true;
     h->device_graph = true;
     h->validated = false;
+    h->alias_ready = false;
+    return GW_OK;
+}
+
+extern "C" int gw_host_weights(gw_handle *h, uint32_t blk, const float *w)
+{
+    if (!h) return GW_ERR_ARG;
+    if (blk >= h->nblocks) return h->fail(GW_ERR_ARG, "block %u out of range (%u blocks)", blk, h->nblocks);
+    if (h->device_graph) return h->fail(GW_ERR_STATE, "the graph is on the device: use gw_device_weights");
+    if (!w && h->eblocks[blk + 1] > h->eblocks[blk]) return h->fail(GW_ERR_ARG, "block %u weights missing", blk);
+    h->host_w[blk] = w;
+    bool all = true;
+    for (uint32_t b = 0; b < h->nblocks; ++b) all &= h->host_w[b] != nullptr || h->eblocks[b + 1] == h->eblocks[b];
+    h->weighted = all;
+    h->resident = false;  // the next in-core run uploads the weights with the graph
+    h->alias_ready = false;
+    h->ooc_invalidate(false);
+    return GW_OK;
+}
+
+extern "C" int gw_device_weights(gw_handle *h, const float *d_w)
+{
+    if (!h) return GW_ERR_ARG;
+    if (!h->device_graph) return h->fail(GW_ERR_STATE, "gw_device_weights needs a device graph (gw_device_graph)");
+    if (!d_w && h->nedges) {
+        h->weighted = false;
+        h->dev_w = nullptr;
+        return GW_OK;
+    }
+    cudaSetDevice(h->cfg.device);
+    cudaFree(h->own_w);
+    h->own_w = nullptr;
+    h->dev_w = d_w;
+    h->weighted = true;
+    h->alias_ready = false;
     return GW_OK;
 }
 
@@ -462,6 +523,36 @@ int gw_handle::build_index(cudaStream_t s)
     return GW_OK;
 }
 
+// Alias tables of every vertex from the resident weights: 8 bytes per edge
+// kept, 16 bytes per edge of scratch for the construction.
+int gw_handle::build_alias(cudaStream_t s)
+{
+    int st;
+    if (!d_alias && (st = cuda(cudaMalloc(&d_alias, (nedges ? nedges : 1) * sizeof(AliasEntry)), "alias tables")))
+        return st;
+    double *pd = nullptr;
+    uint32_t *q = nullptr;
+    if ((st = cuda(cudaMalloc(&pd, (nedges ? nedges : 1) * sizeof(double)), "alias scratch"))) return st;
+    if ((st = cuda(cudaMalloc(&q, 2 * (nedges ? nedges : 1) * sizeof(uint32_t)), "alias scratch"))) {
+        cudaFree(pd);
+        return st;
+    }
+    st = cuda(cudaMemsetAsync(d_err, 0, sizeof(uint32_t), s), "memset");
+    if (!st) st = cuda(launch_build_alias(dev_beg, dev_w, nverts, pd, q, q + nedges, d_alias, d_err, num_sms, s),
+                       "alias build");
+    if (!st) st = cuda(cudaMemcpyAsync(h_ctr + kCtrCount, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "D2H");
+    if (!st) st = cuda(cudaStreamSynchronize(s), "alias build");
+    cudaFree(pd);
+    cudaFree(q);
+    if (st) return st;
+    if ((uint32_t)h_ctr[kCtrCount] != 0) {
+        h_ctr[kCtrCount] = 0;
+        return fail(GW_ERR_GRAPH, "edge weights must be positive finite numbers");
+    }
+    alias_ready = true;
+    return GW_OK;
+}
+
 int gw_handle::run_incore(gw_stats *stats)
 {
     int st;
@@ -496,6 +587,11 @@ int gw_handle::run_incore(gw_stats *stats)
         if ((st = build_index(s))) return st;
         validated = true;
     }
+    if (weighted) {
+        if (cfg.algorithm != GW_NODE2VEC)
+            return fail(GW_ERR_ARG, "weighted walks are Node2vec walks (algorithm %u given)", cfg.algorithm);
+        if (!alias_ready && (st = build_alias(s))) return st;
+    }
     IncoreArgs a{};
     consts_from_config(cfg, a.c);
     a.init.mode = cfg.init_mode;
@@ -522,7 +618,7 @@ int gw_handle::run_incore(gw_stats *stats)
     const bool coop = needs_coop(cfg.algorithm, a.c);
     const int combo = (sopr ? 4 : 0) | (a.paths ? 2 : 0) | (coop ? 1 : 0);
     int variant = tuned_variant[combo];
-    if (cfg.blockpergrid == 0 && variant < 0) {
+    if (cfg.blockpergrid == 0 && variant < 0 && !weighted) {
         // Autotuner: time each register-cap variant on this run's walkers
         // (their outputs are rewritten by the full run below) and keep the
         // fastest for every later run of this kernel class.  Runs of up to
@@ -565,7 +661,11 @@ int gw_handle::run_incore(gw_stats *stats)
     int grid = (int)cfg.blockpergrid;
     if (grid <= 0) grid = incore_grid(sopr, a.paths != nullptr, coop, variant, num_sms);
     if ((st = cuda(cudaEventRecord(ev_kernel0, s), "event"))) return st;
-    if ((st = cuda(launch_walk_incore(a, sopr, coop, variant, grid, s), "walk kernel launch"))) return st;
+    if (weighted) {
+        if ((st = cuda(launch_walk_weighted(a, d_alias, num_sms, s), "weighted walk kernel launch"))) return st;
+    } else if ((st = cuda(launch_walk_incore(a, sopr, coop, variant, grid, s), "walk kernel launch"))) {
+        return st;
+    }
     if ((st = cuda(cudaEventRecord(ev_kernel1, s), "event"))) return st;
     if ((st = cuda(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(unsigned long long) * kCtrCount, cudaMemcpyDeviceToHost, s),
                    "counters D2H")))
@@ -620,6 +720,9 @@ extern "C" int gw_run(gw_handle *h, uint32_t policy, gw_stats *stats)
     }
     if (!h->host_graph_complete())
         return h->fail(GW_ERR_STATE, "graph blocks missing: call gw_host_block for every block");
+    if (h->weighted)
+        return h->fail(GW_ERR_ARG, "weighted walks run in-core: the cache (%llu bytes) must hold the whole graph",
+                       (unsigned long long)h->cfg.cache_size);
     return h->run_ooc(policy, stats);
 }
 

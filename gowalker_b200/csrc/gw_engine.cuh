@@ -6,6 +6,7 @@
 #include <string>
 #include <vector>
 #include "gw_kernels.cuh"
+#include "gw_weighted.cuh"
 #include "../../include/gowalker.h"
 
 namespace gw {
@@ -45,6 +46,14 @@ struct gw_handle {
     uint64_t index_cap = 0;
     const uint32_t *index_lvl[gw::kIdxLevels] = {};
     uint32_t index_nlvl = 0;
+
+    // edge weights (weighted Node2vec, in-core): per host block, or resident
+    std::vector<const float *> host_w;
+    const float *dev_w = nullptr;
+    float *own_w = nullptr;
+    bool weighted = false;
+    gw::AliasEntry *d_alias = nullptr;  // alias tables, rebuilt when the graph or weights change
+    bool alias_ready = false;
 
     // walker population
     uint64_t nwalkers = 0;
@@ -86,6 +95,7 @@ struct gw_handle {
     int upload_whole_graph(cudaStream_t s, uint64_t *h2d);
     int ensure_outputs();
     int build_index(cudaStream_t s);
+    int build_alias(cudaStream_t s);
     int run_incore(gw_stats *stats);
     int run_ooc(uint32_t policy, gw_stats *stats);
     void ooc_release();

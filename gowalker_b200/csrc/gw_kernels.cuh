@@ -43,6 +43,7 @@ enum ErrBit : uint32_t {
     kErrSource = 2u,        // a walker source >= nverts
     kErrBlock = 4u,         // a vertex outside every block, or a block scheduled absent
     kErrTrials = 8u,        // a step exceeded kMaxAttempts rejection trials
+    kErrWeight = 16u,       // an edge weight that is not a positive finite number
 };
 
 // Rejection trials allowed for one step before the walker is stopped with

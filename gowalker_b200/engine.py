@@ -115,6 +115,20 @@ class WalkEngine:
             self._check(self.L.gw_host_block(self.h, b, _ptr(bv), _ptr(bc)))
         self._keep += [beg, csr]
 
+    def set_host_weights(self, w):
+        """Edge weights (float32 per edge, aligned with the CSR) for weighted
+        Node2vec, split like the graph's blocks; borrowed like the graph."""
+        w = np.ascontiguousarray(w, dtype=np.float32) if not hasattr(w, "data_ptr") else w
+        for b in range(len(self.vblocks) - 1):
+            e0, e1 = int(self.eblocks[b]), int(self.eblocks[b + 1])
+            bw = w[e0:e1]
+            self._keep.append(bw)
+            self._check(self.L.gw_host_weights(self.h, b, _ptr(bw) if e1 > e0 else ctypes.c_void_p(0)))
+        self._keep.append(w)
+
+    def set_device_weights(self, d_w_ptr):
+        self._check(self.L.gw_device_weights(self.h, ctypes.c_void_p(d_w_ptr)))
+
     def set_device_graph(self, nverts, nedges, d_beg_ptr, d_csr_ptr):
         self.set_graph_meta(nverts, nedges, [0, nverts], [0, nedges])
         self._check(self.L.gw_device_graph(self.h, ctypes.c_void_p(d_beg_ptr), ctypes.c_void_p(d_csr_ptr)))

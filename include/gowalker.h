@@ -179,6 +179,20 @@ int gw_host_block(gw_handle *h, uint32_t blk, const uint64_t *beg, const uint32_
  * nedges), borrowed.  The engine then runs in-core without host copies. */
 int gw_device_graph(gw_handle *h, const uint64_t *d_beg, const uint32_t *d_csr);
 
+/* Edge weights (real_t, one per edge as in the reference's <base>.wht,
+ * util/util.hpp:136-138), for weighted Node2vec: a step draws its candidate
+ * in proportion to the weight of cur -> x (Walker's alias table per vertex,
+ * built on the device) and accepts it by the unweighted rule.  The reference
+ * loads weights (engine/cache.hpp:71, gpu/memory.hpp:134-137) but never
+ * samples with them.  gw_host_weights borrows block blk's weights like
+ * gw_host_block (every block with edges needs them before walks are
+ * weighted); gw_device_weights gives the weights of a gw_device_graph graph
+ * (NULL: unweighted again).  Weighted walks are Node2vec walks and run
+ * in-core; a weight that is not positive and finite fails the run with
+ * GW_ERR_GRAPH. */
+int gw_host_weights(gw_handle *h, uint32_t blk, const float *w);
+int gw_device_weights(gw_handle *h, const float *d_w);
+
 /* Drop every cached block so the next run copies the graph from the host
  * blocks again. */
 int gw_cache_reset(gw_handle *h);

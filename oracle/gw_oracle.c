@@ -292,8 +292,8 @@ static inline int search_sorted(const uint32_t *csr, uint64_t lo, uint64_t hi, u
 /* One walk from an explicit state.  Returns the number of real moves.
  * path (may be NULL) receives the vertices visited after `cur`.
  * trace (may be NULL, capacity trace_cap) receives every trial. */
-static uint32_t walk_from(const uint64_t *beg, const uint32_t *csr, const oracle_cfg *c,
-                          uint32_t wid, uint32_t *pprev, uint32_t *pcur, uint32_t *phop,
+static uint32_t walk_from(const uint64_t *beg, const uint32_t *csr, const float *aprob, const uint32_t *aalias,
+                          const oracle_cfg *c, uint32_t wid, uint32_t *pprev, uint32_t *pcur, uint32_t *phop,
                           uint64_t *phash, uint32_t *path, oracle_stats *st,
                           oracle_trial *trace, uint64_t trace_cap, uint64_t *ntrace,
                           uint64_t *trial_counter)
@@ -371,7 +371,14 @@ static uint32_t walk_from(const uint64_t *beg, const uint32_t *csr, const oracle
                 t->rv_bits = f2u(rv);
             }
             if (ntrace) (*ntrace)++;
-            x = csr[head + pos];
+            if (aprob) {
+                /* weighted: alias column pos, kept when coin < prob, else its alias */
+                const float coin = (float)(r[3] >> 8) * 0x1p-24f;
+                const uint64_t col = coin < aprob[head + pos] ? pos : aalias[head + pos];
+                x = csr[head + col];
+            } else {
+                x = csr[head + pos];
+            }
             if (rv <= minv) break;
             if (x == prev) {
                 int acc = (c->algo == ALG_NODE2VEC) ? (rv < t_prev_f) : ((double)rv < t_prev_d);
@@ -411,9 +418,9 @@ uint64_t oracle_hash_init(uint32_t source)
  *   lens:   count u32 (vertices recorded) or NULL
  *   hashes: count u64 (FNV-1a over the path's 32-bit vertices) or NULL
  *   finals: count x 3 u32 (prev, cur, hop) after the walk, or NULL */
-int oracle_walk(const uint64_t *beg, const uint32_t *csr, uint32_t nverts, const oracle_cfg *c,
-                uint32_t wid_begin, uint32_t count, uint32_t *paths, uint32_t *lens,
-                uint64_t *hashes, uint32_t *finals, oracle_stats *stats, int nthreads)
+static int walk_many(const uint64_t *beg, const uint32_t *csr, const float *aprob, const uint32_t *aalias,
+                     uint32_t nverts, const oracle_cfg *c, uint32_t wid_begin, uint32_t count, uint32_t *paths,
+                     uint32_t *lens, uint64_t *hashes, uint32_t *finals, oracle_stats *stats, int nthreads)
 {
     if (c->algo > ALG_SOSR || c->maxhops == 0) return -1;
     if (c->init_mode == INIT_PER_VERTEX && c->wps == 0) return -1;
@@ -437,8 +444,8 @@ int oracle_walk(const uint64_t *beg, const uint32_t *csr, uint32_t nverts, const
             uint64_t tc = 0;
             uint32_t *path = paths ? paths + (uint64_t)i * stride : NULL;
             if (path) path[0] = src;
-            uint32_t moves = walk_from(beg, csr, c, wid, &prev, &cur, &hop, &h, path ? path + 1 : NULL,
-                                       &st, NULL, 0, NULL, &tc);
+            uint32_t moves = walk_from(beg, csr, aprob, aalias, c, wid, &prev, &cur, &hop, &h,
+                                       path ? path + 1 : NULL, &st, NULL, 0, NULL, &tc);
             if (lens) lens[i] = moves + 1;
             if (hashes) hashes[i] = h;
             if (finals) {
@@ -461,6 +468,85 @@ int oracle_walk(const uint64_t *beg, const uint32_t *csr, uint32_t nverts, const
     return 0;
 }
 
+int oracle_walk(const uint64_t *beg, const uint32_t *csr, uint32_t nverts, const oracle_cfg *c,
+                uint32_t wid_begin, uint32_t count, uint32_t *paths, uint32_t *lens,
+                uint64_t *hashes, uint32_t *finals, oracle_stats *stats, int nthreads)
+{
+    return walk_many(beg, csr, NULL, NULL, nverts, c, wid_begin, count, paths, lens, hashes, finals, stats,
+                     nthreads);
+}
+
+/* Weighted Node2vec (the device's gw_weighted.cu): candidates by the alias
+ * tables of oracle_build_alias, acceptance by the unweighted rule. */
+int oracle_walk_weighted(const uint64_t *beg, const uint32_t *csr, const float *aprob, const uint32_t *aalias,
+                         uint32_t nverts, const oracle_cfg *c, uint32_t wid_begin, uint32_t count, uint32_t *paths,
+                         uint32_t *lens, uint64_t *hashes, uint32_t *finals, oracle_stats *stats, int nthreads)
+{
+    if (c->algo != ALG_NODE2VEC) return -1;
+    return walk_many(beg, csr, aprob, aalias, nverts, c, wid_begin, count, paths, lens, hashes, finals, stats,
+                     nthreads);
+}
+
+/* Walker's alias tables by Vose's method, per vertex (the device's
+ * k_build_alias step for step): weights summed in double in index order,
+ * p_i = w_i * deg / sum, small (p < 1) and large queues in index order; the
+ * next small s takes the front large l (prob[s] = (float)p_s, alias[s] = l,
+ * p_l = (p_l + p_s) - 1, l to the back of the small queue when below 1);
+ * leftovers get probability 1.  Returns -1 on a weight that is not positive
+ * and finite. */
+int oracle_build_alias(const uint64_t *beg, const float *w, uint32_t nverts, float *prob, uint32_t *alias)
+{
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 1024) reduction(| : bad)
+    for (int64_t v = 0; v < (int64_t)nverts; ++v) {
+        const uint64_t h = beg[v], d = beg[v + 1] - h;
+        if (d == 0) continue;
+        double sum = 0.0;
+        int b = 0;
+        for (uint64_t i = 0; i < d; ++i) {
+            const float wi = w[h + i];
+            b |= !(wi > 0.f && wi < INFINITY);
+            sum = sum + (double)wi;
+        }
+        if (b) {
+            bad = 1;
+            continue;
+        }
+        double *p = malloc(d * sizeof(double));
+        uint32_t *small = malloc(d * sizeof(uint32_t)), *large = malloc(d * sizeof(uint32_t));
+        uint64_t ns = 0, nl = 0, hs = 0, hl = 0;
+        for (uint64_t i = 0; i < d; ++i) {
+            p[i] = ((double)w[h + i] * (double)d) / sum;
+            if (p[i] < 1.0) small[ns++] = (uint32_t)i;
+            else large[nl++] = (uint32_t)i;
+        }
+        while (hs < ns && hl < nl) {
+            const uint32_t s = small[hs++], l = large[hl];
+            prob[h + s] = (float)p[s];
+            alias[h + s] = l;
+            p[l] = (p[l] + p[s]) - 1.0;
+            if (p[l] < 1.0) {
+                ++hl;
+                small[ns++] = l;
+            }
+        }
+        while (hl < nl) {
+            const uint32_t l = large[hl++];
+            prob[h + l] = 1.0f;
+            alias[h + l] = l;
+        }
+        while (hs < ns) {
+            const uint32_t s = small[hs++];
+            prob[h + s] = 1.0f;
+            alias[h + s] = s;
+        }
+        free(p);
+        free(small);
+        free(large);
+    }
+    return bad ? -1 : 0;
+}
+
 /* Single walker from an explicit state (prev, cur, hop) with a trial trace,
  * for the differential test against the reference's sidewalkupdate.
  * Returns the number of moves; *ntrace receives the number of trials. */
@@ -473,7 +559,7 @@ uint32_t oracle_walk_traced(const uint64_t *beg, const uint32_t *csr, const orac
     memset(&st, 0, sizeof(st));
     uint64_t h = 0, tc = 0;
     *ntrace = 0;
-    uint32_t moves = walk_from(beg, csr, c, wid, &prev, &cur, &hop, &h, path, &st, trace, trace_cap,
+    uint32_t moves = walk_from(beg, csr, NULL, NULL, c, wid, &prev, &cur, &hop, &h, path, &st, trace, trace_cap,
                                ntrace, &tc);
     if (final3) {
         final3[0] = prev;

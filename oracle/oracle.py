@@ -101,6 +101,13 @@ def lib():
                                   ctypes.c_uint32, u32p, u32p, u64p, u32p, ctypes.POINTER(Stats),
                                   ctypes.c_int]
         L.oracle_walk.restype = ctypes.c_int
+        f32p = ctypes.POINTER(ctypes.c_float)
+        L.oracle_walk_weighted.argtypes = [u64p, u32p, f32p, u32p, ctypes.c_uint32, ctypes.POINTER(Cfg),
+                                           ctypes.c_uint32, ctypes.c_uint32, u32p, u32p, u64p, u32p,
+                                           ctypes.POINTER(Stats), ctypes.c_int]
+        L.oracle_walk_weighted.restype = ctypes.c_int
+        L.oracle_build_alias.argtypes = [u64p, f32p, ctypes.c_uint32, f32p, u32p]
+        L.oracle_build_alias.restype = ctypes.c_int
         L.oracle_walk_traced.argtypes = [u64p, u32p, ctypes.POINTER(Cfg), ctypes.c_uint32,
                                          ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, u32p,
                                          u32p, ctypes.c_uint64, u64p, u32p]
@@ -292,10 +299,25 @@ def make_cfg(algo=ALG_NODE2VEC, maxhops=80, p=2.0, q=0.5, alpha=0.2, term_prob=0
     return Cfg(algo, maxhops, p, q, alpha, term_prob, seed, keying, init_mode, wps, numwalks)
 
 
+def build_alias(beg, w):
+    """Walker's alias tables of every vertex's out-edge weights
+    (gw_oracle.c oracle_build_alias): (prob float32, alias u32 local index)."""
+    beg = np.ascontiguousarray(beg, dtype=np.uint64)
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    prob = np.zeros(len(w), dtype=np.float32)
+    alias = np.zeros(len(w), dtype=np.uint32)
+    rc = lib().oracle_build_alias(_p(beg, ctypes.c_uint64), _p(w, ctypes.c_float), len(beg) - 1,
+                                  _p(prob, ctypes.c_float), _p(alias, ctypes.c_uint32))
+    if rc != 0:
+        raise ValueError("edge weights must be positive finite numbers")
+    return prob, alias
+
+
 def walk(beg, csr, cfg: Cfg, wid_begin: int, count: int, paths: bool = True, finals: bool = False,
-         nthreads: int = 0):
+         nthreads: int = 0, alias=None):
     """Walk walkers [wid_begin, wid_begin+count).  Returns a dict with
-    paths (count x maxhops+1, zero padded), lens, hashes, finals, stats."""
+    paths (count x maxhops+1, zero padded), lens, hashes, finals, stats.
+    alias = (prob, alias) from build_alias: weighted Node2vec."""
     nverts = len(beg) - 1
     stride = cfg.maxhops + 1
     P = np.zeros((count, stride), dtype=np.uint32) if paths else None
@@ -303,9 +325,16 @@ def walk(beg, csr, cfg: Cfg, wid_begin: int, count: int, paths: bool = True, fin
     H = np.zeros(count, dtype=np.uint64)
     F = np.zeros((count, 3), dtype=np.uint32) if finals else None
     st = Stats()
-    rc = lib().oracle_walk(_p(beg, ctypes.c_uint64), _p(csr, ctypes.c_uint32), nverts, ctypes.byref(cfg),
-                           wid_begin, count, _p(P, ctypes.c_uint32), _p(L, ctypes.c_uint32),
-                           _p(H, ctypes.c_uint64), _p(F, ctypes.c_uint32), ctypes.byref(st), nthreads)
+    if alias is not None:
+        rc = lib().oracle_walk_weighted(_p(beg, ctypes.c_uint64), _p(csr, ctypes.c_uint32),
+                                        _p(alias[0], ctypes.c_float), _p(alias[1], ctypes.c_uint32), nverts,
+                                        ctypes.byref(cfg), wid_begin, count, _p(P, ctypes.c_uint32),
+                                        _p(L, ctypes.c_uint32), _p(H, ctypes.c_uint64), _p(F, ctypes.c_uint32),
+                                        ctypes.byref(st), nthreads)
+    else:
+        rc = lib().oracle_walk(_p(beg, ctypes.c_uint64), _p(csr, ctypes.c_uint32), nverts, ctypes.byref(cfg),
+                               wid_begin, count, _p(P, ctypes.c_uint32), _p(L, ctypes.c_uint32),
+                               _p(H, ctypes.c_uint64), _p(F, ctypes.c_uint32), ctypes.byref(st), nthreads)
     if rc != 0:
         raise ValueError("oracle_walk rejected the configuration")
     return {"paths": P, "lens": L, "hashes": H, "finals": F, "stats": st.as_dict()}

@@ -325,3 +325,70 @@ def test_web_degrees_power_law(oracle):
     for a, b in [(20, 200), (50, 2000)]:
         slope = np.log((deg >= b).mean() / (deg >= a).mean()) / np.log(b / a)
         assert abs(slope + 1.1) < 0.05, slope
+
+
+def test_alias_tables_reproduce_weights(oracle):
+    beg, csr = oracle.rmat_graph(10)
+    rng = np.random.default_rng(1)
+    w = rng.lognormal(0.0, 1.5, len(csr)).astype(np.float32)
+    prob, alias = oracle.build_alias(beg, w)
+    V = len(beg) - 1
+    for v in rng.choice(V, 200, replace=False):
+        h, d = int(beg[v]), int(beg[v + 1] - beg[v])
+        if d == 0:
+            continue
+        got = np.zeros(d)
+        np.add.at(got, np.arange(d), prob[h:h + d])
+        np.add.at(got, alias[h:h + d].astype(np.int64), 1.0 - prob[h:h + d].astype(np.float64))
+        want = w[h:h + d].astype(np.float64) / w[h:h + d].astype(np.float64).sum() * d
+        assert np.abs(got - want).max() < 1e-5 * max(1.0, want.max())
+    with pytest.raises(ValueError):
+        bad = w.copy()
+        bad[5] = 0.0
+        oracle.build_alias(beg, bad)
+
+
+def test_weighted_oracle_equal_weights_is_unweighted(oracle):
+    beg, csr = oracle.rmat_graph(11)
+    cfg = oracle.make_cfg(algo=0, maxhops=15, p=2.0, q=0.5, seed=9)
+    al = oracle.build_alias(beg, np.full(len(csr), 3.5, np.float32))
+    a = oracle.walk(beg, csr, cfg, 0, 2048, alias=al)
+    b = oracle.walk(beg, csr, cfg, 0, 2048)
+    assert np.array_equal(a["paths"], b["paths"]) and np.array_equal(a["hashes"], b["hashes"])
+
+
+def test_weighted_node2vec_transition_law_chi_square(oracle):
+    """Second-order transitions of the weighted oracle follow
+    P(x | prev, cur) ~ w(cur, x) * (1/p if x == prev, 1 if x in N(prev), 1/q else)."""
+    import math
+    rng = np.random.default_rng(4)
+    V = 40
+    src = rng.integers(0, V, 600)
+    dst = rng.integers(0, V, 600)
+    beg, csr = oracle.build_csr(V, src, dst, symmetric=True)
+    w = rng.uniform(0.2, 4.0, len(csr)).astype(np.float32)
+    p, q = 2.0, 0.5
+    cfg = oracle.make_cfg(algo=0, maxhops=4, p=p, q=q, seed=17, wps=4000)
+    nz = np.nonzero(np.diff(beg.astype(np.int64)))[0]
+    r = oracle.walk(beg, csr, cfg, 0, V * 4000, alias=oracle.build_alias(beg, w))
+    P, L = r["paths"], r["lens"]
+    counts = {}
+    for row, n in zip(P, L):
+        for t in range(2, n):
+            key = (int(row[t - 2]), int(row[t - 1]))
+            counts.setdefault(key, {}).setdefault(int(row[t]), 0)
+            counts[key][int(row[t])] += 1
+    tested = 0
+    for (a, b), obs in sorted(counts.items(), key=lambda kv: -sum(kv[1].values()))[:25]:
+        nb = csr[beg[b]:beg[b + 1]]
+        wb = w[beg[b]:beg[b + 1]].astype(np.float64)
+        na = set(csr[beg[a]:beg[a + 1]].tolist())
+        bias = np.array([1 / p if x == a else (1.0 if x in na else 1 / q) for x in nb])
+        pr = wb * bias / (wb * bias).sum()
+        n = sum(obs.values())
+        chi = sum((obs.get(int(x), 0) - n * px) ** 2 / (n * px) for x, px in zip(nb, pr))
+        dof = len(nb) - 1
+        # chi-square upper tail bound: mean dof, sd sqrt(2 dof); 5 sd is far beyond chance
+        assert chi < dof + 5 * math.sqrt(2 * dof) + 10, ((a, b), chi, dof)
+        tested += 1
+    assert tested == 25 and len(nz) == V
