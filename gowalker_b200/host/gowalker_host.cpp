@@ -300,6 +300,7 @@ graph_cache::~graph_cache()
     for (auto &c : cache_blocks) {
         gw_host_free(c.beg_pos);
         gw_host_free(c.csr);
+        gw_host_free(c.weights);
     }
 }
 
@@ -309,12 +310,17 @@ graph_driver::graph_driver(graph_config *conf, metrics &m) : _m(m)
     edgedesc = open((conf->base_name + ".csr").c_str(), O_RDONLY);
     _weighted = conf->is_weighted;
     if (vertdesc < 0 || edgedesc < 0) throw std::runtime_error("cannot open " + conf->base_name + ".beg/.csr");
+    if (_weighted) {  // util/util.hpp:136-138
+        whtdesc = open((conf->base_name + ".wht").c_str(), O_RDONLY);
+        if (whtdesc < 0) throw std::runtime_error("weighted: cannot open " + conf->base_name + ".wht");
+    }
 }
 
 graph_driver::~graph_driver()
 {
     if (vertdesc >= 0) close(vertdesc);
     if (edgedesc >= 0) close(edgedesc);
+    if (whtdesc >= 0) close(whtdesc);
 }
 
 void graph_driver::load_block_info_all(graph_cache &cache, graph_block *gb, bid_t ci, bid_t bi, size_t)
@@ -330,6 +336,11 @@ void graph_driver::load_block_info_all(graph_cache &cache, graph_block *gb, bid_
         if (gw_host_alloc(b.nedges * sizeof(vid_t), &p) != GW_OK) throw std::runtime_error("pinned allocation");
         c.csr = (vid_t *)p;
         read_range(edgedesc, c.csr, b.nedges * sizeof(vid_t), (off_t)b.start_edge * sizeof(vid_t));
+        if (_weighted) {
+            if (gw_host_alloc(b.nedges * sizeof(real_t), &p) != GW_OK) throw std::runtime_error("pinned allocation");
+            c.weights = (real_t *)p;
+            read_range(whtdesc, c.weights, b.nedges * sizeof(real_t), (off_t)b.start_edge * sizeof(real_t));
+        }
     }
 }
 
@@ -377,6 +388,9 @@ graph_engine::graph_engine(graph_cache &_cache, graph_walk &manager, graph_drive
     for (bid_t b = 0; b < cache->ncblock; ++b) {
         driver->load_block_info_all(*cache, gb, b, b, conf->blocksize);
         if (check(gw_host_block(h_, b, cache->cache_blocks[b].beg_pos, cache->cache_blocks[b].csr), "gw_host_block"))
+            return;
+        if (driver->_weighted && gb->eblocks[b + 1] > gb->eblocks[b] &&
+            check(gw_host_weights(h_, b, cache->cache_blocks[b].weights), "gw_host_weights"))
             return;
     }
 }
@@ -487,7 +501,8 @@ void graph_engine::epilogue()
 static void print_help()
 {
     printf("- dataset:       the dataset path (<base>.beg/.csr/.meta in GOWalker's format)\n"
-           "- weighted:      whether the dataset is weighted (weights are not used by the walk)\n"
+           "- weighted:      read <base>.wht (one float per edge): Node2vec draws each step in proportion to the\n"
+           "                 edge weights (in-core); the reference loads weights but never samples with them\n"
            "- sorted:        whether the vertex neighbors are sorted (required)\n"
            "- skip:          use the preprocessed files as they are\n"
            "- blocksize:     the size (MB) of each block\n"

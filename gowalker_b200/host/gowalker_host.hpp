@@ -135,6 +135,7 @@ struct cache_block {  // engine/cache.hpp:63-121: pinned host copy of one block
     block_t *block = nullptr;
     eid_t *beg_pos = nullptr;
     vid_t *csr = nullptr;
+    real_t *weights = nullptr;  // with `weighted`: <base>.wht, one real_t per edge
 };
 
 class graph_cache {  // engine/cache.hpp:195-223
@@ -154,7 +155,7 @@ public:
     ~graph_driver();
     void load_block_info_all(graph_cache &cache, graph_block *global_blocks, bid_t cache_index, bid_t block_index,
                              size_t blocksize);
-    int vertdesc = -1, edgedesc = -1;
+    int vertdesc = -1, edgedesc = -1, whtdesc = -1;
     bool _weighted = false;
     metrics &_m;
 };

@@ -3,6 +3,7 @@
 Files (written and read exactly as the reference does):
   <base>.beg   u64 x (V+1) absolute CSR offsets
   <base>.csr   u32 x E     neighbour ids, sorted per vertex
+  <base>.wht   f32 x E     edge weights (weighted datasets only)
   <base>.meta  16 packed bytes: u32 nvertices, u64 nedges, u32 min_vert
                (preprocess/graph_converter.hpp finalize(), util/io.hpp:29-42)
   <dir>/sowalker_<MB>/<name>_<MB>MB.vert.blocks  u32 x (nblocks+1)
@@ -33,6 +34,12 @@ def write_dataset(base: str, beg: np.ndarray, csr: np.ndarray, min_vert: int = 0
     meta = (np.uint32(len(beg) - 1).tobytes() + np.uint64(len(csr)).tobytes() + np.uint32(min_vert).tobytes())
     with open(base + ".meta", "wb") as f:
         f.write(meta)
+
+
+def write_weights(base: str, w: np.ndarray) -> None:
+    """<base>.wht: one float32 (real_t) per edge, aligned with <base>.csr
+    (util/util.hpp:136-138)."""
+    np.asarray(w, dtype=np.float32).tofile(base + ".wht")
 
 
 def read_meta(base: str):

@@ -111,3 +111,25 @@ def test_app_walks_match_oracle(apps, dataset, oracle, tmp_path, app, algo, extr
         assert lines[w].split() == [str(x) for x in ref["paths"][w, :L]], w
     metrics = open(os.path.join(os.path.dirname(base), "randgraph_metrics.txt")).read()
     assert ".0_Total_time=" in metrics and ".1_GPUTime=" in metrics and ".steps=" in metrics
+
+
+@pytest.mark.gpu
+def test_weighted_node2vec_app_matches_oracle(apps, dataset, oracle, tmp_path):
+    """`weighted` reads <base>.wht and the walks follow the weights."""
+    from gowalker_b200 import preprocess as P
+    base, beg, csr = dataset
+    wbase = str(tmp_path / "gw")
+    P.write_dataset(wbase, beg, csr)
+    w = np.random.default_rng(6).lognormal(0.0, 1.0, len(csr)).astype(np.float32)
+    P.write_weights(wbase, w)
+    pfile = tmp_path / "paths.txt"
+    run(apps, "Node2vec", wbase + ".txt", "skip", "weighted", "seed", 3, "paths", pfile, "GOWalker", "p", 2,
+        "q", 0.5, "length", 15)
+    V = len(beg) - 1
+    ref = oracle.walk(beg, csr, oracle.make_cfg(algo=0, maxhops=15, seed=3, p=2.0, q=0.5), 0, V, paths=True,
+                      alias=oracle.build_alias(beg, w))
+    lines = open(pfile).read().splitlines()
+    assert len(lines) == V
+    for i in range(0, V, max(1, V // 300)):
+        L = int(ref["lens"][i])
+        assert lines[i].split() == [str(x) for x in ref["paths"][i, :L]], i
