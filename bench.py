@@ -43,6 +43,9 @@ WORKLOADS = {
                scale=24, ef=16, algo=1, maxhops=20, wps=4, p=0.5, q=2.0, alpha=0.2, term=0.15),
     "c1": dict(name="C1: Node2vec p=2 q=0.5 length 80, 1 walker/vertex, R-MAT scale 20 ef 16 symmetrised, in-core",
                scale=20, ef=16, algo=0, maxhops=80, wps=1, p=2.0, q=0.5, alpha=0.2, term=0.0),
+    "c1w": dict(name="C1 weighted: Node2vec p=2 q=0.5 length 80, 1 walker/vertex, R-MAT scale 20 ef 16 symmetrised, "
+                     "edge weights lognormal(0, 1) (torch generator seed 1), in-core",
+                scale=20, ef=16, algo=0, maxhops=80, wps=1, p=2.0, q=0.5, alpha=0.2, term=0.0, weighted=True),
     "c3": dict(name="C3: out-of-core Node2vec p=0.5 q=2 length 80, 1 walker/vertex, directed R-MAT scale 26 "
                     "rejecting ids >= 41.6M, thinned to 1.47B edges, 64 equal-edge-mass blocks, 1.5 GB device cache",
                scale=26, nverts=41_600_000, target=1_470_000_000, nsamples=2_600_000_000, ef=0, algo=0, maxhops=80,
@@ -181,7 +184,7 @@ def host_graph(dg):
     return beg_t, csr_t, beg, csr
 
 
-def oracle_sample(O, beg, csr, wl, seed, target_s, nchunks=32, threads=0):
+def oracle_sample(O, beg, csr, wl, seed, target_s, nchunks=32, threads=0, alias=None):
     """Time the oracle on an evenly spread sample of the workload's walkers,
     sized to take about target_s seconds.  Returns (steps, seconds, stats,
     walkers, description)."""
@@ -191,7 +194,7 @@ def oracle_sample(O, beg, csr, wl, seed, target_s, nchunks=32, threads=0):
                      term_prob=wl["term"], seed=seed, wps=wl["wps"])
     # calibration
     t0 = time.time()
-    r = O.walk(beg, csr, cfg, nwalk // 3, 20000, paths=False, nthreads=threads)
+    r = O.walk(beg, csr, cfg, nwalk // 3, 20000, paths=False, nthreads=threads, alias=alias)
     dt = max(time.time() - t0, 1e-3)
     per_walker = dt / 20000
     count = int(max(nchunks * 64, min(nwalk, target_s / per_walker)))
@@ -200,7 +203,7 @@ def oracle_sample(O, beg, csr, wl, seed, target_s, nchunks=32, threads=0):
     tot = {k: 0 for k in r["stats"]}
     t0 = time.time()
     for s in starts:
-        rr = O.walk(beg, csr, cfg, s, chunk, paths=False, nthreads=threads)
+        rr = O.walk(beg, csr, cfg, s, chunk, paths=False, nthreads=threads, alias=alias)
         for k, v in rr["stats"].items():
             tot[k] += v
     secs = time.time() - t0
@@ -208,11 +211,12 @@ def oracle_sample(O, beg, csr, wl, seed, target_s, nchunks=32, threads=0):
     return tot["steps"], secs, tot, chunk * nchunks, desc
 
 
-def algorithmic_bytes(stats, walkers, paths):
+def algorithmic_bytes(stats, walkers, paths, weighted=False):
     """Bytes the walk must move: 32-B sectors for (beg[cur], beg[cur+1]), one csr
     sector per trial, the distinct sectors of each trial's search of N(prev),
-    plus the per-walker outputs (hash 8 B, length 4 B, path entries 4 B)."""
-    b = 32 * (stats["off_sectors"] + stats["trials"] + stats["search_sectors"])
+    plus the per-walker outputs (hash 8 B, length 4 B, path entries 4 B).
+    Weighted walks read one more sector per trial (the alias-table entry)."""
+    b = 32 * (stats["off_sectors"] + stats["trials"] * (2 if weighted else 1) + stats["search_sectors"])
     b += 12 * walkers
     if paths:
         b += 4 * (stats["steps"] + walkers)
@@ -230,14 +234,21 @@ def run_reference_arm(args, wl):
         return 0
     dg = build_graph(gw, wl)
     _, _, beg, csr = host_graph(dg)[:4]
+    alias = None
+    if wl.get("weighted"):
+        import torch
+        g = torch.Generator(device="cuda")
+        g.manual_seed(1)
+        w = torch.empty(dg.nedges, dtype=torch.float32, device="cuda").log_normal_(0.0, 1.0, generator=g)
+        alias = O.build_alias(beg, w.cpu().numpy())
     dg.free()
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
-        oracle_sample(O, beg, csr, wl, 42, 0.5, threads=threads)
+        oracle_sample(O, beg, csr, wl, 42, 0.5, threads=threads, alias=alias)
     steps = secs = 0.0
     desc = ""
     for _ in range(args.steps):
-        s, t, _, _, desc = oracle_sample(O, beg, csr, wl, 42, args.ref_seconds, threads=threads)
+        s, t, _, _, desc = oracle_sample(O, beg, csr, wl, 42, args.ref_seconds, threads=threads, alias=alias)
         steps += s
         secs += t
     v = steps / secs
@@ -514,6 +525,12 @@ def run_ours(args, wl):
     eng = gw.WalkEngine(**cfgkw)
     eng.set_device_graph(dg.nverts, dg.nedges, dg.beg_ptr, dg.csr_ptr)
     stream = torch.cuda.ExternalStream(eng.stream_handle(), device=local)
+    d_w = None
+    if wl.get("weighted"):
+        g = torch.Generator(device="cuda")
+        g.manual_seed(1)
+        d_w = torch.empty(dg.nedges, dtype=torch.float32, device="cuda").log_normal_(0.0, 1.0, generator=g)
+        eng.set_device_weights(d_w.data_ptr())
 
     def barrier():
         if dist is not None:
@@ -557,6 +574,11 @@ def run_ours(args, wl):
     beg_t, csr_t, beg, csr = host_graph(dg)
     eng2 = gw.WalkEngine(**cfgkw)
     eng2.set_host_graph(beg_t, csr_t[: dg.nedges])
+    h_w = None
+    if d_w is not None:
+        h_w = torch.empty(dg.nedges, dtype=torch.float32, pin_memory=True)
+        h_w.copy_(d_w)
+        eng2.set_host_weights(h_w)
     stream2 = torch.cuda.ExternalStream(eng2.stream_handle(), device=local)
     for _ in range(max(1, args.warmup)):
         eng2.cache_reset()
@@ -622,9 +644,10 @@ def run_ours(args, wl):
         from oracle import oracle as O
         O.lib()
         threads = os.cpu_count() or 1
+        alias = O.build_alias(beg, h_w.numpy()) if h_w is not None else None
         s_steps, s_secs, s_stats, s_walk, s_desc = oracle_sample(O, beg, csr, wl, seed, args.cpu_seconds,
-                                                                 threads=threads)
-        bpstep = algorithmic_bytes(s_stats, s_walk, paths) / max(s_steps, 1)
+                                                                 threads=threads, alias=alias)
+        bpstep = algorithmic_bytes(s_stats, s_walk, paths, weighted=alias is not None) / max(s_steps, 1)
         kernel_s = kernel_ms / 1000.0 / args.steps
         steps_per_launch = steps / args.steps
         achieved = bpstep * steps_per_launch / kernel_s / 1e9
@@ -634,7 +657,7 @@ def run_ours(args, wl):
                             "traffic": (dram_ps * steps_per_launch) if dram_ps else None,
                             "peak_source": peak_kind,
                             "algorithmic_bytes_per_step": bpstep, "kernel_ms_per_launch": kernel_ms / args.steps,
-                            "kernel": "k_walk_incore"}
+                            "kernel": "k_walk_weighted" if h_w is not None else "k_walk_incore"}
         if dram_ps:
             line["roofline"]["dram_bytes_per_step"] = dram_ps
             line["roofline"]["dram_frac"] = dram_ps * steps_per_launch / kernel_s / 1e9 / peaks["hbm_gbs"]
