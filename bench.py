@@ -317,7 +317,8 @@ def run_ooc_bench(args, wl):
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    tot = {"steps": 0, "h2d_bytes": 0, "kernel_ms": 0.0, "block_loads": 0, "iterations": 0, "launches": 0,
+    tot = {"steps": 0, "h2d_bytes": 0, "kernel_ms": 0.0, "bucket_ms": 0.0, "block_loads": 0, "iterations": 0,
+           "launches": 0,
            "d2h_bytes": 0, "trials": 0, "learned_iterations": 0, "policy_reverted": 0}
     last = {}
     for _ in range(args.steps):
@@ -357,7 +358,8 @@ def run_ooc_bench(args, wl):
             "trials_per_step": tot["trials"] / max(tot["steps"], 1),
             "roofline": {"bound": "host-link", "achieved": link, "peak": PCIE_GEN5_X16_GBS, "unit": "GB/s",
                          "frac": link / PCIE_GEN5_X16_GBS, "traffic": None,
-                         "kernel_ms_per_run": tot["kernel_ms"] / args.steps},
+                         "kernel_ms_per_run": tot["kernel_ms"] / args.steps,
+                         "bucket_ms_per_run": tot["bucket_ms"] / args.steps},
             "checksum": {"path_hash_sum": hs}}
     if clk:
         line["clocks"] = clk

@@ -79,7 +79,8 @@ class GwStats(ctypes.Structure):
         ("pred_error", ctypes.c_float),
         ("kernel_variant", ctypes.c_uint32),
         ("persist_error", ctypes.c_float),
-        ("reserved", ctypes.c_uint32 * 2),
+        ("bucket_ms", ctypes.c_float),
+        ("reserved", ctypes.c_uint32 * 1),
         ("coop_small_steps", ctypes.c_uint64),
         ("coop_small_attempts", ctypes.c_uint64),
         ("coop_large_steps", ctypes.c_uint64),

@@ -407,7 +407,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     const bool paths = cfg.record_paths == GW_PATHS_FULL;
     uint64_t h2d = 0, loads = 0, zc_steps = 0;
     uint32_t iters = 0, launches = 0;
-    float kernel_ms = 0.f;
+    float kernel_ms = 0.f, bucket_ms = 0.f;
+    cudaEvent_t bk0 = nullptr, bk1 = nullptr;  // around the last re-bucketing
+    if ((st = cuda(cudaEventCreate(&bk0), "event")) || (st = cuda(cudaEventCreate(&bk1), "event"))) return st;
+    bool bk_pending = false;
 
     if ((st = cuda(cudaEventRecord(ev_start, s), "event"))) return st;
     // cold cache
@@ -525,7 +528,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             cudaGraphDestroy(g);
             if (e) return e;
         }
+        if ((e = cuda(cudaEventRecord(bk0, s), "event"))) return e;
         if ((e = cuda(cudaGraphLaunch(bgraph[c], s), "bucketing graph"))) return e;
+        if ((e = cuda(cudaEventRecord(bk1, s), "event"))) return e;
+        bk_pending = true;
         launches += 4;
         o.w_cur ^= 1u;  // the sorted index of the live walkers
         return cuda(cudaEventRecord(ev_buck, s), "event");
@@ -751,6 +757,11 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             float ms = 0.f;
             if (cudaEventElapsedTime(&ms, k0, k1) == cudaSuccess) kernel_ms += ms;
         }
+        if (bk_pending) {  // the decision waited for that re-bucketing
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, bk0, bk1) == cudaSuccess) bucket_ms += ms;
+            bk_pending = false;
+        }
         if ((uint32_t)h_ctr[kCtrCount] != 0) {
             st = fail(GW_ERR_GRAPH, "block data failed validation or a kernel reported 0x%x",
                       (uint32_t)h_ctr[kCtrCount]);
@@ -957,6 +968,8 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     for (auto &g : bgraph)
         if (g) cudaGraphExecDestroy(g);
     cudaEventDestroy(ev_buck);
+    cudaEventDestroy(bk0);
+    cudaEventDestroy(bk1);
     cudaEventDestroy(k0);
     cudaEventDestroy(k1);
     if (st) return st;
@@ -974,6 +987,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         stats->iterations = iters;
         stats->launches = launches;
         stats->kernel_ms = kernel_ms;
+        stats->bucket_ms = bucket_ms;
         cudaEventElapsedTime(&stats->total_ms, ev_start, ev_stop);
         stats->learned_iterations = learned_iters;
         stats->policy_reverted = reverted ? 1u : 0u;

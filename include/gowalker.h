@@ -127,7 +127,8 @@ typedef struct gw_stats {
     uint32_t kernel_variant;     /* register-cap variant the autotuner picked (in-core) */
     float persist_error;         /* learned: the same error of the forecast without the network
                                     (this iteration's demand carried forward) */
-    uint32_t reserved[2];
+    float bucket_ms;             /* out-of-core: time re-bucketing walkers (CUDA events) */
+    uint32_t reserved[1];
     uint64_t coop_small_steps;   /* hard steps decided from candidate positions (in-core) */
     uint64_t coop_small_attempts;
     uint64_t coop_large_steps;   /* hard steps evaluated with candidate loads (in-core) */
