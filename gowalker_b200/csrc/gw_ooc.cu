@@ -20,7 +20,10 @@
 #include "gw_ooc_kernels.cuh"
 #include "gw_mlp.cuh"
 #include "gw_compress.cuh"
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <deque>
 #include <thread>
 
@@ -408,6 +411,23 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     uint64_t h2d = 0, loads = 0, zc_steps = 0;
     uint32_t iters = 0, launches = 0;
     float kernel_ms = 0.f, bucket_ms = 0.f;
+    // GOWALKER_TRACE: per-run phase totals on stderr (install = wait for the
+    // staged copy + decode + validation on the compute stream; decision =
+    // host time blocked on the decision stream; copy = prefetch uploads)
+    const char *trace_env = getenv("GOWALKER_TRACE");
+    const bool trace = trace_env && *trace_env && *trace_env != '0';
+    cudaEvent_t tin0 = nullptr, tin1 = nullptr, tcp[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    bool tcp_live[2] = {false, false};
+    uint32_t tcp_next = 0;
+    double t_install = 0.0, t_copy = 0.0, t_decision = 0.0;
+    if (trace) {
+        cudaEventCreate(&tin0);
+        cudaEventCreate(&tin1);
+        for (auto &pr : tcp) {
+            cudaEventCreate(&pr[0]);
+            cudaEventCreate(&pr[1]);
+        }
+    }
     cudaEvent_t bk0 = nullptr, bk1 = nullptr;  // around the last re-bucketing
     if ((st = cuda(cudaEventCreate(&bk0), "event")) || (st = cuda(cudaEventCreate(&bk1), "event"))) return st;
     bool bk_pending = false;
@@ -643,6 +663,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         }
         if (staged_block >= 0) {
             // ---- the block copied during the last step becomes resident
+            if (trace) cudaEventRecord(tin0, s);
             if ((st = cuda(cudaStreamWaitEvent(s, staged_ev, 0), "staged copy"))) break;
             int freed = -1;
             if (staged_pos >= 0) {
@@ -674,6 +695,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                     }
             staged_block = -1;
             if ((st = push_tables())) break;
+            if (trace) cudaEventRecord(tin1, s);
         }
         const uint32_t ncached = (uint32_t)o.cached.size();
         for (uint32_t j = 0; j < ncached; ++j) o.h_cached[j] = o.cached[j];
@@ -752,7 +774,20 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if ((st = cuda(cudaMemcpyAsync(h_ctr, o.d_snap, sizeof(unsigned long long) * (kCtrCount + 1),
                                        cudaMemcpyDeviceToHost, ds), "counters")))
             break;
+        const auto tw0 = std::chrono::steady_clock::now();
         if ((st = cuda(cudaStreamSynchronize(ds), "schedule sync"))) break;
+        if (trace) {
+            t_decision += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw0).count();
+            float ms = 0.f;
+            if (cudaEventQuery(tin1) == cudaSuccess && cudaEventElapsedTime(&ms, tin0, tin1) == cudaSuccess)
+                t_install += ms;
+            for (int k = 0; k < 2; ++k)
+                if (tcp_live[k] && cudaEventQuery(tcp[k][1]) == cudaSuccess &&
+                    cudaEventElapsedTime(&ms, tcp[k][0], tcp[k][1]) == cudaSuccess) {
+                    t_copy += ms;
+                    tcp_live[k] = false;
+                }
+        }
         if (iters > 1) {
             float ms = 0.f;
             if (cudaEventElapsedTime(&ms, k0, k1) == cudaSuccess) kernel_ms += ms;
@@ -871,7 +906,20 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             uint64_t bytes = 0;
             upload_stage ^= o.nstage == 2 ? 1u : 0u;
             staged_stage = upload_stage;
+            if (trace) {
+                if (tcp_live[tcp_next]) {  // still unread: wait for it
+                    cudaEventSynchronize(tcp[tcp_next][1]);
+                    float ms = 0.f;
+                    if (cudaEventElapsedTime(&ms, tcp[tcp_next][0], tcp[tcp_next][1]) == cudaSuccess) t_copy += ms;
+                }
+                cudaEventRecord(tcp[tcp_next][0], s_copy);
+            }
             if ((st = upload_block(b, sc, s_copy, upload_stage, &bytes))) break;
+            if (trace) {
+                cudaEventRecord(tcp[tcp_next][1], s_copy);
+                tcp_live[tcp_next] = true;
+                tcp_next ^= 1u;
+            }
             if ((st = cuda(cudaEventRecord(staged_ev, s_copy), "event"))) break;
             h2d += bytes;
             loads++;
@@ -970,6 +1018,14 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     cudaEventDestroy(ev_buck);
     cudaEventDestroy(bk0);
     cudaEventDestroy(bk1);
+    if (trace) {
+        cudaEventDestroy(tin0);
+        cudaEventDestroy(tin1);
+        for (auto &pr : tcp) {
+            cudaEventDestroy(pr[0]);
+            cudaEventDestroy(pr[1]);
+        }
+    }
     cudaEventDestroy(k0);
     cudaEventDestroy(k1);
     if (st) return st;
@@ -989,6 +1045,11 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         stats->kernel_ms = kernel_ms;
         stats->bucket_ms = bucket_ms;
         cudaEventElapsedTime(&stats->total_ms, ev_start, ev_stop);
+        if (trace)
+            fprintf(stderr,
+                    "[gowalker] out-of-core run: %u iterations, %.1f ms total, step %.1f, re-bucketing %.1f, "
+                    "install %.1f, prefetch copies %.1f (copy stream), host blocked on decisions %.1f ms\n",
+                    iters, stats->total_ms, kernel_ms, bucket_ms, t_install, t_copy, t_decision);
         stats->learned_iterations = learned_iters;
         stats->policy_reverted = reverted ? 1u : 0u;
         stats->train_loss = (policy == GW_POLICY_LEARNED) ? o.train_loss : 0.f;
