@@ -417,7 +417,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     const char *trace_env = getenv("GOWALKER_TRACE");
     const bool trace = trace_env && *trace_env && *trace_env != '0';
     cudaEvent_t tin0 = nullptr, tin1 = nullptr, tcp[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-    bool tcp_live[2] = {false, false};
+    bool tcp_live[2] = {false, false}, tin_live = false;
     uint32_t tcp_next = 0;
     double t_install = 0.0, t_copy = 0.0, t_decision = 0.0;
     if (trace) {
@@ -695,7 +695,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                     }
             staged_block = -1;
             if ((st = push_tables())) break;
-            if (trace) cudaEventRecord(tin1, s);
+            if (trace) {
+                cudaEventRecord(tin1, s);
+                tin_live = true;
+            }
         }
         const uint32_t ncached = (uint32_t)o.cached.size();
         for (uint32_t j = 0; j < ncached; ++j) o.h_cached[j] = o.cached[j];
@@ -779,14 +782,17 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if (trace) {
             t_decision += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw0).count();
             float ms = 0.f;
-            if (cudaEventQuery(tin1) == cudaSuccess && cudaEventElapsedTime(&ms, tin0, tin1) == cudaSuccess)
+            if (tin_live && cudaEventQuery(tin1) == cudaSuccess && cudaEventElapsedTime(&ms, tin0, tin1) == cudaSuccess) {
                 t_install += ms;
+                tin_live = false;
+            }
             for (int k = 0; k < 2; ++k)
                 if (tcp_live[k] && cudaEventQuery(tcp[k][1]) == cudaSuccess &&
                     cudaEventElapsedTime(&ms, tcp[k][0], tcp[k][1]) == cudaSuccess) {
                     t_copy += ms;
                     tcp_live[k] = false;
                 }
+            cudaGetLastError();  // a query of work still in flight is not an error of the run
         }
         if (iters > 1) {
             float ms = 0.f;
@@ -911,6 +917,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                     cudaEventSynchronize(tcp[tcp_next][1]);
                     float ms = 0.f;
                     if (cudaEventElapsedTime(&ms, tcp[tcp_next][0], tcp[tcp_next][1]) == cudaSuccess) t_copy += ms;
+                    tcp_live[tcp_next] = false;
                 }
                 cudaEventRecord(tcp[tcp_next][0], s_copy);
             }
