@@ -67,6 +67,11 @@ WORKLOADS = {
                scale=28, nverts=133_600_000, target=5_500_000_000, nsamples=0, ef=0, algo=0, maxhops=80,
                wps=1, p=0.5, q=2.0, alpha=0.2, term=0.0, nblocks=256, cache=8_000_000_000, ooc=True, web=True,
                dmin=6.8, tail=1.1, max_degree=65536, local_permille=800, window=65536),
+    "c5s": dict(name="C5 at 1/16 size (profiling case): out-of-core Node2vec p=0.5 q=2 length 80, 1 walker/vertex, "
+                     "web-shaped graph, 8.35M vertices, 343.75M edges, 256 equal-edge-mass blocks, 500 MB device cache",
+                scale=24, nverts=8_350_000, target=343_750_000, nsamples=0, ef=0, algo=0, maxhops=80, wps=1, p=0.5,
+                q=2.0, alpha=0.2, term=0.0, nblocks=256, cache=500_000_000, ooc=True, web=True, dmin=6.8, tail=1.1,
+                max_degree=65536, local_permille=800, window=65536),
     "prep": dict(name="edge list -> CSR on the device (gw_edges_csr): R-MAT scale 24 ef 16 sample list "
                       "(268,435,456 u32 pairs, (a,b,c,d) = (0.57,0.19,0.19,0.05)), symmetrised, deduplicated, sorted",
                  scale=24, ef=16, prep=True),

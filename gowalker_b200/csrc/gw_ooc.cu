@@ -417,10 +417,17 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     const char *trace_env = getenv("GOWALKER_TRACE");
     const bool trace = trace_env && *trace_env && *trace_env != '0';
     cudaEvent_t tin0 = nullptr, tin1 = nullptr, tcp[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    cudaEvent_t td0 = nullptr, td1 = nullptr, tr0 = nullptr, tr1 = nullptr;
+    bool tr_live = false;
+    double t_sched = 0.0, t_runnable = 0.0;
     bool tcp_live[2] = {false, false}, tin_live = false;
     uint32_t tcp_next = 0;
     double t_install = 0.0, t_copy = 0.0, t_decision = 0.0;
     if (trace) {
+        cudaEventCreate(&td0);
+        cudaEventCreate(&td1);
+        cudaEventCreate(&tr0);
+        cudaEventCreate(&tr1);
         cudaEventCreate(&tin0);
         cudaEventCreate(&tin1);
         for (auto &pr : tcp) {
@@ -592,10 +599,15 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     cudaEventCreate(&k1);
     auto step = [&]() -> int {
         int e;
+        if (trace) cudaEventRecord(tr0, s);
         if ((e = cuda(launch_runnable(o.d_counts, o.d_offsets, o.d_blk_csr, nb, a.lazy, o.d_run_pre, o.d_run_off,
                                       o.d_nrun, s),
                       "runnable")))
             return e;
+        if (trace) {
+            cudaEventRecord(tr1, s);
+            tr_live = true;
+        }
         if ((e = cuda(cudaMemsetAsync(d_ctr + kCtrCursor, 0, sizeof(unsigned long long), s), "memset"))) return e;
         a.recs = o.w_rec;
         a.order = o.w_ord[o.w_cur];
@@ -760,6 +772,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             }
         }
         // ---- plain block choice on the device (decision, fallback and rescue), read back
+        if (trace) cudaEventRecord(td0, ds);
         if ((st = cuda(launch_schedule(o.d_pairs, o.d_offsets + nbk, nb, o.d_cached, ncached, capacity, cfg.zero_threshold,
                                        nullptr, 0.f, o.d_dec, ds),
                        "schedule")))
@@ -777,11 +790,17 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if ((st = cuda(cudaMemcpyAsync(h_ctr, o.d_snap, sizeof(unsigned long long) * (kCtrCount + 1),
                                        cudaMemcpyDeviceToHost, ds), "counters")))
             break;
+        if (trace) cudaEventRecord(td1, ds);
         const auto tw0 = std::chrono::steady_clock::now();
         if ((st = cuda(cudaStreamSynchronize(ds), "schedule sync"))) break;
         if (trace) {
             t_decision += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw0).count();
             float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, td0, td1) == cudaSuccess) t_sched += ms;
+            if (tr_live && cudaEventElapsedTime(&ms, tr0, tr1) == cudaSuccess) {
+                t_runnable += ms;
+                tr_live = false;
+            }
             if (tin_live && cudaEventQuery(tin1) == cudaSuccess && cudaEventElapsedTime(&ms, tin0, tin1) == cudaSuccess) {
                 t_install += ms;
                 tin_live = false;
@@ -1026,6 +1045,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     cudaEventDestroy(bk0);
     cudaEventDestroy(bk1);
     if (trace) {
+        cudaEventDestroy(td0);
+        cudaEventDestroy(td1);
+        cudaEventDestroy(tr0);
+        cudaEventDestroy(tr1);
         cudaEventDestroy(tin0);
         cudaEventDestroy(tin1);
         for (auto &pr : tcp) {
@@ -1055,8 +1078,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if (trace)
             fprintf(stderr,
                     "[gowalker] out-of-core run: %u iterations, %.1f ms total, step %.1f, re-bucketing %.1f, "
-                    "install %.1f, prefetch copies %.1f (copy stream), host blocked on decisions %.1f ms\n",
-                    iters, stats->total_ms, kernel_ms, bucket_ms, t_install, t_copy, t_decision);
+                    "install %.1f, prefetch copies %.1f (copy stream), host blocked on decisions %.1f ms "
+                    "(decision kernels and read-back %.1f), runnable-bucket pass %.1f ms\n",
+                    iters, stats->total_ms, kernel_ms, bucket_ms, t_install, t_copy, t_decision, t_sched, t_runnable);
         stats->learned_iterations = learned_iters;
         stats->policy_reverted = reverted ? 1u : 0u;
         stats->train_loss = (policy == GW_POLICY_LEARNED) ? o.train_loss : 0.f;
