@@ -5,7 +5,7 @@
 //  k_count         walkers per (prev block, cur block) bucket, warp-aggregated
 //                  atomics (one atomic per distinct bucket per warp instead of
 //                  one per walker, gpu/gpuwalk.hpp:179)
-//  k_scan          exclusive scan of the nblocks^2 bucket counts in one CTA
+//  k_scan          exclusive scan of the bucket counts in one CTA (coalesced warp segments)
 //                  (the reference scans them on one thread, gpu/gpuwalk.hpp:321-338)
 //  k_scatter       walkers into bucket order, finished walkers dropped
 //                  (gpu/gpuwalk.hpp:340-360 + the spill of engine/walk.hpp:484-525)
@@ -111,49 +111,65 @@ __global__ void k_scatter(const uint32_t *__restrict__ keys_in, const uint32_t *
 // One-CTA scans over at most 2^20 entries (nblocks <= 1024).
 constexpr int kScanThreads = 1024;
 
-__device__ __forceinline__ uint32_t cta_exclusive_scan(uint32_t v, uint32_t *total)
+
+// Warp w of the CTA owns entries [w * seg, (w + 1) * seg) and walks them 32
+// at a time, so every load and store of a round is one coalesced line; the
+// warps' totals are scanned once through shared memory.
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, uint32_t lane)
 {
-    __shared__ uint32_t s_w[32];
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    uint32_t x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
         if (lane >= (uint32_t)o) x += y;
     }
-    if (lane == 31) s_w[warp] = x;
+    return x;
+}
+
+__device__ __forceinline__ uint32_t warp_sum(uint32_t x)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xFFFFFFFFu, x, o);
+    return x;
+}
+
+// Exclusive scan of the warps' totals: warp w gets the sum of warps < w.
+__device__ __forceinline__ uint32_t cta_warp_base(uint32_t wtotal, uint32_t *total)
+{
+    __shared__ uint32_t s_t[32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (lane == 0) s_t[warp] = wtotal;
     __syncthreads();
     if (warp == 0) {
-        uint32_t w = (lane < (blockDim.x >> 5)) ? s_w[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
-            if (lane >= (uint32_t)o) w += y;
-        }
-        s_w[lane] = w;
+        const uint32_t v = lane < (blockDim.x >> 5) ? s_t[lane] : 0u;
+        const uint32_t inc = warp_incl_scan(v, lane);
+        s_t[lane] = inc - v;
+        if (lane == 31 && total) *total = inc;
     }
     __syncthreads();
-    const uint32_t before = (warp > 0 ? s_w[warp - 1] : 0) + x - v;
-    if (total) *total = s_w[(blockDim.x >> 5) - 1];
+    const uint32_t b = s_t[warp];
     __syncthreads();
-    return before;
+    return b;
 }
 
 __global__ void __launch_bounds__(kScanThreads) k_scan(const uint32_t *__restrict__ in, uint32_t n,
                                                        uint32_t *__restrict__ out)
 {
-    const uint32_t per = (n + kScanThreads - 1) / kScanThreads;
-    const uint32_t lo = min(threadIdx.x * per, n), hi = min(lo + per, n);
-    uint32_t sum = 0;
-    for (uint32_t i = lo; i < hi; ++i) sum += in[i];
-    uint32_t total = 0;
-    uint32_t run = cta_exclusive_scan(sum, &total);
-    for (uint32_t i = lo; i < hi; ++i) {
-        const uint32_t c = in[i];
-        out[i] = run;
-        run += c;
+    __shared__ uint32_t s_total;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t seg = ((n + nw - 1) / nw + 31u) & ~31u;
+    const uint32_t lo = min(warp * seg, n), hi = min(lo + seg, n);
+    uint32_t part = 0;
+    for (uint32_t i = lo + lane; i < hi; i += 32) part += in[i];
+    uint32_t base = cta_warp_base(warp_sum(part), &s_total);
+    for (uint32_t i0 = lo; i0 < hi; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const uint32_t v = i < hi ? in[i] : 0u;
+        const uint32_t inc = warp_incl_scan(v, lane);
+        if (i < hi) out[i] = base + inc - v;
+        base += __shfl_sync(0xFFFFFFFFu, inc, 31);
     }
-    if (threadIdx.x == 0) out[n] = total;
+    __syncthreads();
+    if (threadIdx.x == 0) out[n] = s_total;
 }
 
 __global__ void __launch_bounds__(kScanThreads) k_runnable(const uint32_t *__restrict__ counts,
@@ -163,6 +179,7 @@ __global__ void __launch_bounds__(kScanThreads) k_runnable(const uint32_t *__res
                                                            uint32_t *__restrict__ run_off, uint32_t *__restrict__ nrun)
 {
     __shared__ uint8_t s_res[kMaxBlocks];
+    __shared__ uint32_t s_cnt, s_sum;
     for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) s_res[i] = blk_csr[i] != nullptr;
     __syncthreads();
     const uint32_t nn = nb * nb, n = 2 * nn;
@@ -173,31 +190,39 @@ __global__ void __launch_bounds__(kScanThreads) k_runnable(const uint32_t *__res
         const bool cur_ok = s_res[pc % nb] != 0, prev_ok = s_res[pc / nb] != 0;
         return cur_ok && (prev_ok || (lazy && b < nn));
     };
-    const uint32_t per = (n + kScanThreads - 1) / kScanThreads;
-    const uint32_t lo = min(threadIdx.x * per, n), hi = min(lo + per, n);
-    uint32_t cnt = 0, sum = 0;
-    for (uint32_t b = lo; b < hi; ++b) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t seg = ((n + nw - 1) / nw + 31u) & ~31u;
+    const uint32_t lo = min(warp * seg, n), hi = min(lo + seg, n);
+    uint32_t pc = 0, ps = 0;
+    for (uint32_t b = lo + lane; b < hi; b += 32) {
         const uint32_t c = counts[b];
         if (c && runnable(b)) {
-            cnt++;
-            sum += c;
+            pc++;
+            ps += c;
         }
     }
-    uint32_t tot_cnt = 0, tot_sum = 0;
-    uint32_t k = cta_exclusive_scan(cnt, &tot_cnt);
-    uint32_t run = cta_exclusive_scan(sum, &tot_sum);
-    for (uint32_t b = lo; b < hi; ++b) {
-        const uint32_t c = counts[b];
-        if (c && runnable(b)) {
+    uint32_t kb = cta_warp_base(warp_sum(pc), &s_cnt);
+    uint32_t sb = cta_warp_base(warp_sum(ps), &s_sum);
+    for (uint32_t b0 = lo; b0 < hi; b0 += 32) {
+        const uint32_t b = b0 + lane;
+        const uint32_t c = b < hi ? counts[b] : 0u;
+        const bool f = c && runnable(b);
+        const unsigned fm = __ballot_sync(0xFFFFFFFFu, f);
+        const uint32_t v = f ? c : 0u;
+        const uint32_t inc = warp_incl_scan(v, lane);
+        if (f) {
+            const uint32_t k = kb + (uint32_t)__popc(fm & lt);
             run_off[k] = offsets[b];
-            run_pre[k] = run;
-            run += c;
-            k++;
+            run_pre[k] = sb + inc - v;
         }
+        kb += (uint32_t)__popc(fm);
+        sb += __shfl_sync(0xFFFFFFFFu, inc, 31);
     }
+    __syncthreads();
     if (threadIdx.x == 0) {
-        *nrun = tot_cnt;
-        run_pre[tot_cnt] = tot_sum;
+        *nrun = s_cnt;
+        run_pre[s_cnt] = s_sum;
     }
 }
 
