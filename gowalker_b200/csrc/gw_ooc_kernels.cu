@@ -159,8 +159,10 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const uint32_t *__restric
     const uint32_t seg = ((n + nw - 1) / nw + 31u) & ~31u;
     const uint32_t lo = min(warp * seg, n), hi = min(lo + seg, n);
     uint32_t part = 0;
+#pragma unroll 4
     for (uint32_t i = lo + lane; i < hi; i += 32) part += in[i];
     uint32_t base = cta_warp_base(warp_sum(part), &s_total);
+#pragma unroll 4
     for (uint32_t i0 = lo; i0 < hi; i0 += 32) {
         const uint32_t i = i0 + lane;
         const uint32_t v = i < hi ? in[i] : 0u;
@@ -195,6 +197,7 @@ __global__ void __launch_bounds__(kScanThreads) k_runnable(const uint32_t *__res
     const uint32_t seg = ((n + nw - 1) / nw + 31u) & ~31u;
     const uint32_t lo = min(warp * seg, n), hi = min(lo + seg, n);
     uint32_t pc = 0, ps = 0;
+#pragma unroll 4
     for (uint32_t b = lo + lane; b < hi; b += 32) {
         const uint32_t c = counts[b];
         if (c && runnable(b)) {
@@ -204,6 +207,7 @@ __global__ void __launch_bounds__(kScanThreads) k_runnable(const uint32_t *__res
     }
     uint32_t kb = cta_warp_base(warp_sum(pc), &s_cnt);
     uint32_t sb = cta_warp_base(warp_sum(ps), &s_sum);
+#pragma unroll 4
     for (uint32_t b0 = lo; b0 < hi; b0 += 32) {
         const uint32_t b = b0 + lane;
         const uint32_t c = b < hi ? counts[b] : 0u;
@@ -264,35 +268,50 @@ __global__ void __launch_bounds__(1024) k_schedule(const uint32_t *__restrict__ 
     }
     __syncthreads();
     const bool full = ncached >= nslots;
-    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
-        uint64_t incident = 0;  // walkers in buckets touching i (row + column, diagonal once)
-        for (uint32_t c = 0; c < nb; ++c) incident += (uint64_t)counts[i * nb + c] + (c != i ? counts[c * nb + i] : 0u);
-        s_inc[i] = incident;
-        if (s_cached[i]) continue;
-        uint64_t score = 0;
+    // one warp per block i: lanes split the row / column and the cached list
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (uint32_t i = warp; i < nb; i += nw) {
+        unsigned long long incident = 0;  // walkers in buckets touching i (row + column, diagonal once)
+        for (uint32_t c = lane; c < nb; c += 32)
+            incident += (unsigned long long)counts[i * nb + c] + (c != i ? counts[c * nb + i] : 0u);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) incident += __shfl_xor_sync(0xFFFFFFFFu, incident, o);
+        if (lane == 0) s_inc[i] = incident;
+        if (s_cached[i]) continue;  // warp-uniform
+        unsigned long long score = 0;
         uint32_t pos = 0;
         if (!full) {
-            for (uint32_t j = 0; j < ncached; ++j) {
+            for (uint32_t j = lane; j < ncached; j += 32) {
                 const uint32_t c = s_list[j];
-                score += (uint64_t)counts[i * nb + c] + counts[c * nb + i];
+                score += (unsigned long long)counts[i * nb + c] + counts[c * nb + i];
             }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) score += __shfl_xor_sync(0xFFFFFFFFu, score, o);
             score += counts[i * nb + i];
         } else {
-            uint64_t all = 0, mn = 0xFFFFFFFFull;
-            for (uint32_t j = 0; j < ncached; ++j) {
+            // all minus the smallest link; the first position on ties
+            unsigned long long all = 0, key = ~0ull;  // (value << 32) | position
+            for (uint32_t j = lane; j < ncached; j += 32) {
                 const uint32_t c = s_list[j];
-                const uint64_t v = (uint64_t)counts[i * nb + c] + counts[c * nb + i];
+                const unsigned long long v = (unsigned long long)counts[i * nb + c] + counts[c * nb + i];
                 all += v;
-                if (v < mn) {
-                    mn = v;
-                    pos = j;
-                }
+                const unsigned long long kv = (v << 32) | j;
+                key = kv < key ? kv : key;
             }
-            score = all - mn;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                all += __shfl_xor_sync(0xFFFFFFFFu, all, o);
+                const unsigned long long ko = __shfl_xor_sync(0xFFFFFFFFu, key, o);
+                key = ko < key ? ko : key;
+            }
+            score = all - (key >> 32);
+            pos = (uint32_t)key;
         }
         if (pred) score = (uint64_t)fmaxf(0.f, pred_weight * pred[i]) + (score > 0 ? 1 : 0);
-        s_pos[i] = pos;
-        atomicMax(&s_best, (score << 11) | (2047u - i));
+        if (lane == 0) {
+            s_pos[i] = pos;
+            atomicMax(&s_best, (score << 11) | (2047u - i));
+        }
     }
     // fullest bucket with an absent block
     const uint32_t nbk = nb * nb;
