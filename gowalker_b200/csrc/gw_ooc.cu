@@ -397,6 +397,54 @@ static int ooc_map_host(gw_handle *h)
     return GW_OK;
 }
 
+// Two alternating event pairs around a recurring piece of stream work: a
+// pair is read back only when it comes round again (its work finished an
+// iteration ago) or when the run drains it, so timing never stalls the host.
+struct EvRing {
+    cudaEvent_t e[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    bool pend[2] = {false, false};
+    uint32_t p = 0;
+    void create()
+    {
+        for (auto &x : e) {
+            cudaEventCreate(&x[0]);
+            cudaEventCreate(&x[1]);
+        }
+    }
+    void destroy()
+    {
+        for (auto &x : e) {
+            if (x[0]) cudaEventDestroy(x[0]);
+            if (x[1]) cudaEventDestroy(x[1]);
+            x[0] = x[1] = nullptr;
+        }
+    }
+    void collect(uint32_t k, float &acc)
+    {
+        float ms = 0.f;
+        if (pend[k] && cudaEventSynchronize(e[k][1]) == cudaSuccess && cudaEventElapsedTime(&ms, e[k][0], e[k][1]) == cudaSuccess)
+            acc += ms;
+        pend[k] = false;
+    }
+    cudaError_t begin(cudaStream_t st, float &acc)
+    {
+        collect(p, acc);
+        return cudaEventRecord(e[p][0], st);
+    }
+    cudaError_t end(cudaStream_t st)
+    {
+        const cudaError_t r = cudaEventRecord(e[p][1], st);
+        pend[p] = true;
+        p ^= 1u;
+        return r;
+    }
+    void drain(float &acc)
+    {
+        collect(0, acc);
+        collect(1, acc);
+    }
+};
+
 int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
 {
     int st;
@@ -417,8 +465,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     const char *trace_env = getenv("GOWALKER_TRACE");
     const bool trace = trace_env && *trace_env && *trace_env != '0';
     cudaEvent_t tin0 = nullptr, tin1 = nullptr, tcp[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-    cudaEvent_t td0 = nullptr, td1 = nullptr, tr0 = nullptr, tr1 = nullptr;
-    bool tr_live = false;
+    cudaEvent_t td0 = nullptr, td1 = nullptr;
     double t_sched = 0.0, t_runnable = 0.0;
     bool tcp_live[2] = {false, false}, tin_live = false;
     uint32_t tcp_next = 0;
@@ -426,8 +473,6 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     if (trace) {
         cudaEventCreate(&td0);
         cudaEventCreate(&td1);
-        cudaEventCreate(&tr0);
-        cudaEventCreate(&tr1);
         cudaEventCreate(&tin0);
         cudaEventCreate(&tin1);
         for (auto &pr : tcp) {
@@ -435,9 +480,11 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             cudaEventCreate(&pr[1]);
         }
     }
-    cudaEvent_t bk0 = nullptr, bk1 = nullptr;  // around the last re-bucketing
-    if ((st = cuda(cudaEventCreate(&bk0), "event")) || (st = cuda(cudaEventCreate(&bk1), "event"))) return st;
-    bool bk_pending = false;
+    EvRing bring, kring, rring;  // re-bucketing, step kernel, runnable pass (trace)
+    bring.create();
+    kring.create();
+    if (trace) rring.create();
+    float t_runnable_f = 0.f;
 
     if ((st = cuda(cudaEventRecord(ev_start, s), "event"))) return st;
     // cold cache
@@ -512,6 +559,8 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     uint64_t nlive = nwalkers;  // records in w_a (unsorted)
     cudaEvent_t ev_buck = nullptr;  // the last re-bucketing (and counter snapshot) is done
     if ((st = cuda(cudaEventCreateWithFlags(&ev_buck, cudaEventDisableTiming), "event"))) return st;
+    cudaEvent_t ev_dec = nullptr;  // this iteration's decision has read the counts
+    if ((st = cuda(cudaEventCreateWithFlags(&ev_dec, cudaEventDisableTiming), "event"))) return st;
 
     // Re-bucketing: count, scan and scatter the sorted index from buffer c to
     // c^1, per-pair totals, the new walker count into d_n, and the counter
@@ -555,10 +604,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             cudaGraphDestroy(g);
             if (e) return e;
         }
-        if ((e = cuda(cudaEventRecord(bk0, s), "event"))) return e;
+        if ((e = cuda(bring.begin(s, bucket_ms), "event"))) return e;
         if ((e = cuda(cudaGraphLaunch(bgraph[c], s), "bucketing graph"))) return e;
-        if ((e = cuda(cudaEventRecord(bk1, s), "event"))) return e;
-        bk_pending = true;
+        if ((e = cuda(bring.end(s), "event"))) return e;
         launches += 4;
         o.w_cur ^= 1u;  // the sorted index of the live walkers
         return cuda(cudaEventRecord(ev_buck, s), "event");
@@ -594,27 +642,21 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     int grid = (int)cfg.blockpergrid;
     if (grid <= 0) grid = ooc_grid(sopr, paths, coop, num_sms);
 
-    cudaEvent_t k0 = nullptr, k1 = nullptr;
-    cudaEventCreate(&k0);
-    cudaEventCreate(&k1);
     auto step = [&]() -> int {
         int e;
-        if (trace) cudaEventRecord(tr0, s);
+        if (trace) rring.begin(s, t_runnable_f);
         if ((e = cuda(launch_runnable(o.d_counts, o.d_offsets, o.d_blk_csr, nb, a.lazy, o.d_run_pre, o.d_run_off,
                                       o.d_nrun, s),
                       "runnable")))
             return e;
-        if (trace) {
-            cudaEventRecord(tr1, s);
-            tr_live = true;
-        }
+        if (trace) rring.end(s);
         if ((e = cuda(cudaMemsetAsync(d_ctr + kCtrCursor, 0, sizeof(unsigned long long), s), "memset"))) return e;
         a.recs = o.w_rec;
         a.order = o.w_ord[o.w_cur];
         a.keys = o.w_key[o.w_cur];
-        if ((e = cuda(cudaEventRecord(k0, s), "event"))) return e;
+        if ((e = cuda(kring.begin(s, kernel_ms), "event"))) return e;
         if ((e = cuda(launch_walk_ooc(a, sopr, coop, grid, s), "walk kernel"))) return e;
-        if ((e = cuda(cudaEventRecord(k1, s), "event"))) return e;
+        if ((e = cuda(kring.end(s), "event"))) return e;
         launches += 2;
         return GW_OK;
     };
@@ -623,21 +665,24 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     bool done = false;
     // learned-policy state of this run
     if (policy == GW_POLICY_LEARNED && (st = learned_setup(this))) {
-        cudaEventDestroy(k0);
-        cudaEventDestroy(k1);
+        kring.destroy();
+        bring.destroy();
+        rring.destroy();
         return st;
     }
     if (policy == GW_POLICY_LEARNED) {
         if ((st = cuda(cudaMemsetAsync(o.d_prev_col, 0, sizeof(float) * nb, s), "memset")) ||
             (st = cuda(cudaMemsetAsync(o.d_ema, 0, sizeof(float) * nb, s), "memset"))) {
-            cudaEventDestroy(k0);
-            cudaEventDestroy(k1);
+            kring.destroy();
+            bring.destroy();
+            rring.destroy();
             return st;
         }
     }
     if (policy == GW_POLICY_SA && (st = cuda(cudaMemsetAsync(o.d_sa, 0, sizeof(SaState), s), "memset"))) {
-        cudaEventDestroy(k0);
-        cudaEventDestroy(k1);
+        kring.destroy();
+        bring.destroy();
+        rring.destroy();
         return st;
     }
     uint32_t trace_t = 0, learned_iters = 0;
@@ -656,8 +701,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     const uint32_t capacity = prefetch ? o.nslots - 1 : o.nslots;
     int staged_block = -1, staged_pos = -1, staging_slot = prefetch ? 0 : -1;
     if (prefetch && o.nslots < 3) {
-        cudaEventDestroy(k0);
-        cudaEventDestroy(k1);
+        kring.destroy();
+        bring.destroy();
+        rring.destroy();
         return fail(GW_ERR_ARG, "prefetch needs a cache of at least 3 blocks (has %u)", o.nslots);
     }
     cudaEvent_t staged_ev = nullptr;
@@ -791,16 +837,25 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                                        cudaMemcpyDeviceToHost, ds), "counters")))
             break;
         if (trace) cudaEventRecord(td1, ds);
+        // With prefetch the decision picks the block of the next iteration,
+        // so this iteration's step needs nothing from it: walk now, while the
+        // decision runs on its own stream, and re-bucket once the decision
+        // has read the counts that the re-bucketing rewrites.
+        bool stepped = false;
+        if (prefetch) {
+            if ((st = cuda(cudaEventRecord(ev_dec, ds), "event"))) break;
+            if ((st = step())) break;
+            if ((st = cuda(cudaStreamWaitEvent(s, ev_dec, 0), "decision wait"))) break;
+            if ((st = bucketize(nlive))) break;
+            stepped = true;
+        }
         const auto tw0 = std::chrono::steady_clock::now();
         if ((st = cuda(cudaStreamSynchronize(ds), "schedule sync"))) break;
         if (trace) {
             t_decision += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw0).count();
             float ms = 0.f;
             if (cudaEventElapsedTime(&ms, td0, td1) == cudaSuccess) t_sched += ms;
-            if (tr_live && cudaEventElapsedTime(&ms, tr0, tr1) == cudaSuccess) {
-                t_runnable += ms;
-                tr_live = false;
-            }
+
             if (tin_live && cudaEventQuery(tin1) == cudaSuccess && cudaEventElapsedTime(&ms, tin0, tin1) == cudaSuccess) {
                 t_install += ms;
                 tin_live = false;
@@ -812,15 +867,6 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                     tcp_live[k] = false;
                 }
             cudaGetLastError();  // a query of work still in flight is not an error of the run
-        }
-        if (iters > 1) {
-            float ms = 0.f;
-            if (cudaEventElapsedTime(&ms, k0, k1) == cudaSuccess) kernel_ms += ms;
-        }
-        if (bk_pending) {  // the decision waited for that re-bucketing
-            float ms = 0.f;
-            if (cudaEventElapsedTime(&ms, bk0, bk1) == cudaSuccess) bucket_ms += ms;
-            bk_pending = false;
         }
         if ((uint32_t)h_ctr[kCtrCount] != 0) {
             st = fail(GW_ERR_GRAPH, "block data failed validation or a kernel reported 0x%x",
@@ -900,8 +946,6 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             if ((st = cuda(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(before), cudaMemcpyDeviceToHost, s), "counters")))
                 break;
             if ((st = cuda(cudaStreamSynchronize(s), "zero-copy"))) break;
-            float ms = 0.f;
-            if (cudaEventElapsedTime(&ms, k0, k1) == cudaSuccess) kernel_ms += ms;
             zc_steps += h_ctr[kCtrSteps] - before[kCtrSteps];
             // restore the table to device slots only
             for (uint32_t b = 0; b < nb; ++b)
@@ -989,11 +1033,13 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             o.h_blk_csr[b] = sc;
         }
         if (st) break;
-        if ((st = push_tables())) break;
 
         // ---- walk every runnable bucket, then re-bucket
-        if ((st = step())) break;
-        if ((st = bucketize(nlive))) break;
+        if (!stepped) {
+            if ((st = push_tables())) break;
+            if ((st = step())) break;
+            if ((st = bucketize(nlive))) break;
+        }
 
         // ---- predictor training: once kTraceRing iterations are traced, and
         // again (warm, fewer epochs) every kRetrain iterations on the sliding
@@ -1042,13 +1088,18 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     for (auto &g : bgraph)
         if (g) cudaGraphExecDestroy(g);
     cudaEventDestroy(ev_buck);
-    cudaEventDestroy(bk0);
-    cudaEventDestroy(bk1);
+    cudaEventDestroy(ev_dec);
+    kring.drain(kernel_ms);
+    bring.drain(bucket_ms);
+    if (trace) rring.drain(t_runnable_f);
+    t_runnable += t_runnable_f;
+    kring.destroy();
+    bring.destroy();
+    rring.destroy();
+    cudaGetLastError();
     if (trace) {
         cudaEventDestroy(td0);
         cudaEventDestroy(td1);
-        cudaEventDestroy(tr0);
-        cudaEventDestroy(tr1);
         cudaEventDestroy(tin0);
         cudaEventDestroy(tin1);
         for (auto &pr : tcp) {
@@ -1056,8 +1107,6 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             cudaEventDestroy(pr[1]);
         }
     }
-    cudaEventDestroy(k0);
-    cudaEventDestroy(k1);
     if (st) return st;
     last_hash_sum = h_ctr[kCtrHashSum];
     last_steps = h_ctr[kCtrSteps];
