@@ -640,7 +640,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     // those run with both blocks as the reference does.
     a.lazy = (!sopr && !coop && !cfg.strict_blocks) ? 1u : 0u;
     int grid = (int)cfg.blockpergrid;
-    if (grid <= 0) grid = ooc_grid(sopr, paths, coop, num_sms);
+    // With prefetch the decision kernels (one CTA each) run beside the step
+    // kernel: the step leaves one SM free for them, so the next block's copy
+    // starts while the step runs instead of after it.
+    if (grid <= 0) grid = ooc_grid(sopr, paths, coop, cfg.prefetch && num_sms > 8 ? num_sms - 1 : num_sms);
 
     auto step = [&]() -> int {
         int e;
