@@ -50,8 +50,8 @@ struct OocState {
     unsigned long long *d_snap = nullptr;  // counters and error word after the last re-bucketing
     uint32_t *d_vstart = nullptr;
     uint64_t *d_estart = nullptr;
-    uint32_t *h_cached = nullptr;  // pinned
-    uint32_t *d_cached = nullptr;
+    uint32_t *h_cached = nullptr;  // pinned and mapped: the decision kernels read it in place
+    uint32_t *d_cached = nullptr;  // h_cached's device alias
 
     WalkerRec *w_rec = nullptr;                    // records, never moved
     uint32_t *w_ord[2] = {nullptr, nullptr};       // record index per sorted position (current, next)
@@ -141,7 +141,6 @@ void gw_handle::ooc_release()
     cudaFree((void *)o.d_blk_csr);
     cudaFree(o.d_vstart);
     cudaFree(o.d_estart);
-    cudaFree(o.d_cached);
     cudaFree(o.w_rec);
     for (int i = 0; i < 2; ++i) {
         cudaFree(o.w_ord[i]);
@@ -302,8 +301,9 @@ static int ooc_setup(gw_handle *h)
     if ((st = h->cuda(cudaMallocHost(&o.h_n, sizeof(uint32_t)), "walker count"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_vstart, (nb + 1) * sizeof(uint32_t)), "vstart"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_estart, (nb + 1) * sizeof(uint64_t)), "estart"))) return st;
-    if ((st = h->cuda(cudaMalloc(&o.d_cached, nb * sizeof(uint32_t)), "cached list"))) return st;
-    if ((st = h->cuda(cudaMallocHost(&o.h_cached, nb * sizeof(uint32_t)), "cached list"))) return st;
+    if ((st = h->cuda(cudaHostAlloc((void **)&o.h_cached, nb * sizeof(uint32_t), cudaHostAllocMapped), "cached list")))
+        return st;
+    if ((st = h->cuda(cudaHostGetDevicePointer((void **)&o.d_cached, o.h_cached, 0), "cached list"))) return st;
     const uint64_t nbk = 2ull * nb * nb;
     if ((st = h->cuda(cudaMalloc(&o.d_pairs, nbk / 2 * sizeof(uint32_t)), "pair counts"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_counts, nbk * sizeof(uint32_t)), "bucket counts"))) return st;
@@ -764,11 +764,13 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         const uint32_t ncached = (uint32_t)o.cached.size();
         for (uint32_t j = 0; j < ncached; ++j) o.h_cached[j] = o.cached[j];
         if ((st = cuda(cudaStreamWaitEvent(ds, ev_buck, 0), "decision wait"))) break;
-        if (ncached &&
-            (st = cuda(cudaMemcpyAsync(o.d_cached, o.h_cached, ncached * sizeof(uint32_t), cudaMemcpyHostToDevice, ds),
-                       "cached list")))
-            break;
-        if ((st = cuda(cudaMemcpyAsync((void *)o.d_blk_csr2, pin_last, nb * sizeof(void *), cudaMemcpyHostToDevice, ds),
+        // The cached list is read in place from mapped host memory (the last
+        // decision on ds has finished, so nothing reads it while it changes):
+        // no host-to-device copy in the decision's path, where it would queue
+        // behind the block copy in flight.  Only the learned policy needs the
+        // block table on the decision stream.
+        if (policy == GW_POLICY_LEARNED &&
+            (st = cuda(cudaMemcpyAsync((void *)o.d_blk_csr2, pin_last, nb * sizeof(void *), cudaMemcpyHostToDevice, ds),
                        "block table")))
             break;
         // ---- learned policy: features (traces while training), prediction, choice
