@@ -62,7 +62,7 @@ struct OocState {
     // 2 * nb^2 buckets (unflagged, then kNeedPrev); d_pairs: nb^2 per-pair totals
     uint32_t *d_counts = nullptr, *d_offsets = nullptr, *d_cursor = nullptr, *d_pairs = nullptr;
     uint32_t *d_run_pre = nullptr, *d_run_off = nullptr, *d_nrun = nullptr;
-    Decision *d_dec = nullptr, *h_dec = nullptr;
+    Decision *d_dec = nullptr, *h_dec = nullptr;  // pinned, mapped: the decision kernels write it in place
     SaState *d_sa = nullptr;  // annealing policy: the held block set
 
     // zero-copy: device views of the host blocks' neighbour lists, and the
@@ -155,7 +155,6 @@ void gw_handle::ooc_release()
     cudaFree(o.d_run_pre);
     cudaFree(o.d_run_off);
     cudaFree(o.d_nrun);
-    cudaFree(o.d_dec);
     cudaFree(o.d_sa);
     if (o.h_blk_csr) cudaFreeHost((void *)o.h_blk_csr);
     if (o.h_cached) cudaFreeHost(o.h_cached);
@@ -312,9 +311,10 @@ static int ooc_setup(gw_handle *h)
     if ((st = h->cuda(cudaMalloc(&o.d_run_pre, (nbk + 1) * sizeof(uint32_t)), "runnable prefix"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_run_off, nbk * sizeof(uint32_t)), "runnable offsets"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_nrun, sizeof(uint32_t)), "runnable count"))) return st;
-    if ((st = h->cuda(cudaMalloc(&o.d_dec, sizeof(Decision)), "decision"))) return st;
+
     if ((st = h->cuda(cudaMalloc(&o.d_sa, sizeof(SaState)), "annealing state"))) return st;
-    if ((st = h->cuda(cudaMallocHost(&o.h_dec, sizeof(Decision)), "decision"))) return st;
+    if ((st = h->cuda(cudaHostAlloc((void **)&o.h_dec, sizeof(Decision), cudaHostAllocMapped), "decision"))) return st;
+    if ((st = h->cuda(cudaHostGetDevicePointer((void **)&o.d_dec, o.h_dec, 0), "decision"))) return st;
     if ((st = h->cuda(cudaMemcpy(o.d_vstart, h->vblocks.data(), (nb + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice),
                       "vstart")))
         return st;
@@ -836,8 +836,6 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 break;
             launches++;
         }
-        if ((st = cuda(cudaMemcpyAsync(o.h_dec, o.d_dec, sizeof(Decision), cudaMemcpyDeviceToHost, ds), "decision")))
-            break;
         if ((st = cuda(cudaMemcpyAsync(h_ctr, o.d_snap, sizeof(unsigned long long) * (kCtrCount + 1),
                                        cudaMemcpyDeviceToHost, ds), "counters")))
             break;

@@ -355,6 +355,7 @@ __global__ void __launch_bounds__(1024) k_schedule(const uint32_t *__restrict__ 
             }
         }
         *out = d;
+        __threadfence_system();  // `out` may be mapped host memory
     }
 }
 

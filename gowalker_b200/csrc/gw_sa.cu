@@ -279,6 +279,7 @@ __global__ void __launch_bounds__(1024)
         d.position = pos;
     }
     *dec = d;
+    __threadfence_system();  // `dec` may be mapped host memory
 }
 
 cudaError_t launch_sa_choose(const uint32_t *counts, uint32_t nb, const uint32_t *cached, uint32_t ncached,
