@@ -47,7 +47,9 @@ struct OocState {
     const uint32_t **h_blk_pin[2] = {nullptr, nullptr};
     const uint32_t **d_blk_csr2 = nullptr;
     uint32_t pin_next = 0;
-    unsigned long long *d_snap = nullptr;  // counters and error word after the last re-bucketing
+    // counters and error word after a re-bucketing, one per bucketing
+    // parity, pinned and mapped: the re-bucketing writes them in place
+    unsigned long long *h_snap[2] = {nullptr, nullptr}, *dm_snap[2] = {nullptr, nullptr};
     uint32_t *d_vstart = nullptr;
     uint64_t *d_estart = nullptr;
     uint32_t *h_cached = nullptr;  // pinned and mapped: the decision kernels read it in place
@@ -165,7 +167,9 @@ void gw_handle::ooc_release()
     cudaFree(o.d_cstage[0]);
     cudaFree(o.d_cstage[1]);
     cudaFree((void *)o.d_blk_csr2);
-    cudaFree(o.d_snap);
+    for (auto &p : o.h_snap)
+        if (p) cudaFreeHost(p);
+    o.h_snap[0] = o.h_snap[1] = o.dm_snap[0] = o.dm_snap[1] = nullptr;
     for (auto *p : o.h_blk_pin)
         if (p) cudaFreeHost((void *)p);
     for (float *p : {o.d_params, o.d_train_ws, o.d_trace_x, o.d_trace_col, o.d_trace_y, o.d_train_x,
@@ -294,8 +298,13 @@ static int ooc_setup(gw_handle *h)
     for (auto &p : o.h_blk_pin)
         if ((st = h->cuda(cudaMallocHost((void **)&p, nb * sizeof(void *)), "block table"))) return st;
     if ((st = h->cuda(cudaMalloc((void **)&o.d_blk_csr2, nb * sizeof(void *)), "block table"))) return st;
-    if ((st = h->cuda(cudaMalloc(&o.d_snap, sizeof(unsigned long long) * (kCtrCount + 1)), "counter snapshot")))
-        return st;
+    for (int k = 0; k < 2; ++k) {
+        if ((st = h->cuda(cudaHostAlloc((void **)&o.h_snap[k], sizeof(unsigned long long) * (kCtrCount + 1),
+                                        cudaHostAllocMapped), "counter snapshot")))
+            return st;
+        if ((st = h->cuda(cudaHostGetDevicePointer((void **)&o.dm_snap[k], o.h_snap[k], 0), "counter snapshot")))
+            return st;
+    }
     if ((st = h->cuda(cudaMalloc(&o.d_n, sizeof(uint32_t)), "walker count"))) return st;
     if ((st = h->cuda(cudaMallocHost(&o.h_n, sizeof(uint32_t)), "walker count"))) return st;
     if ((st = h->cuda(cudaMalloc(&o.d_vstart, (nb + 1) * sizeof(uint32_t)), "vstart"))) return st;
@@ -580,12 +589,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if ((e = cuda(cudaMemcpyAsync(o.d_n, o.d_offsets + nbk, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s),
                       "walker count")))
             return e;
-        if ((e = cuda(cudaMemcpyAsync(o.d_snap, d_ctr, sizeof(unsigned long long) * kCtrCount, cudaMemcpyDeviceToDevice,
-                                      s), "counter snapshot")))
-            return e;
-        return cuda(cudaMemcpyAsync(o.d_snap + kCtrCount, d_err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s),
-                    "error snapshot");
+        return cuda(launch_snapshot(d_ctr, d_err, o.dm_snap[c], s), "counter snapshot");
     };
+    uint32_t snap_last = 0;  // snapshot parity of the last re-bucketing
     cudaGraphExec_t bgraph[2] = {nullptr, nullptr};
     auto bucketize = [&](uint64_t) -> int {
         const uint32_t c = o.w_cur;
@@ -604,6 +610,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             cudaGraphDestroy(g);
             if (e) return e;
         }
+        snap_last = c;
         if ((e = cuda(bring.begin(s, bucket_ms), "event"))) return e;
         if ((e = cuda(cudaGraphLaunch(bgraph[c], s), "bucketing graph"))) return e;
         if ((e = cuda(bring.end(s), "event"))) return e;
@@ -836,9 +843,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 break;
             launches++;
         }
-        if ((st = cuda(cudaMemcpyAsync(h_ctr, o.d_snap, sizeof(unsigned long long) * (kCtrCount + 1),
-                                       cudaMemcpyDeviceToHost, ds), "counters")))
-            break;
+        // the snapshot this decision reads: the last re-bucketing's (the
+        // next one, issued below with prefetch, writes the other parity)
+        const uint32_t snap_read = snap_last;
         if (trace) cudaEventRecord(td1, ds);
         // With prefetch the decision picks the block of the next iteration,
         // so this iteration's step needs nothing from it: walk now, while the
@@ -854,6 +861,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         }
         const auto tw0 = std::chrono::steady_clock::now();
         if ((st = cuda(cudaStreamSynchronize(ds), "schedule sync"))) break;
+        memcpy(h_ctr, o.h_snap[snap_read], sizeof(unsigned long long) * (kCtrCount + 1));
         if (trace) {
             t_decision += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw0).count();
             float ms = 0.f;

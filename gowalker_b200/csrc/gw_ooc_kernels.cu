@@ -787,6 +787,23 @@ __global__ void k_combine(const uint32_t *__restrict__ counts, uint32_t nn, uint
         combined[k] = counts[k] + counts[nn + k];
 }
 
+// Counters and error word into out (mapped host memory): one thread each.
+__global__ void k_snapshot(const unsigned long long *__restrict__ ctr, const uint32_t *__restrict__ err,
+                           unsigned long long *out)
+{
+    const uint32_t i = threadIdx.x;
+    if (i < kCtrCount) out[i] = ctr[i];
+    else if (i == kCtrCount) out[i] = *err;
+    __threadfence_system();
+}
+
+cudaError_t launch_snapshot(const unsigned long long *ctr, const uint32_t *err, unsigned long long *out,
+                            cudaStream_t s)
+{
+    k_snapshot<<<1, 32, 0, s>>>(ctr, err, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_combine(const uint32_t *counts, uint32_t nb, uint32_t *combined, int num_sms, cudaStream_t s)
 {
     k_combine<<<num_sms, 256, 0, s>>>(counts, nb * nb, combined);

@@ -74,6 +74,9 @@ cudaError_t launch_scatter(const uint32_t *keys_in, const uint32_t *order_in, co
 cudaError_t launch_runnable(const uint32_t *counts, const uint32_t *offsets, const uint32_t *const *blk_csr,
                             uint32_t nb, uint32_t lazy, uint32_t *run_pre, uint32_t *run_off, uint32_t *nrun,
                             cudaStream_t s);
+// Counters (kCtrCount) and the error word into out[0 .. kCtrCount] (mapped host memory).
+cudaError_t launch_snapshot(const unsigned long long *ctr, const uint32_t *err, unsigned long long *out,
+                            cudaStream_t s);
 // combined[k] = counts[k] + counts[nb^2 + k]: walkers per (prev, cur) block pair.
 cudaError_t launch_combine(const uint32_t *counts, uint32_t nb, uint32_t *combined, int num_sms, cudaStream_t s);
 // `counts` are the nb^2 per-pair totals; `live` points at the live-walker count.
