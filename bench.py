@@ -664,7 +664,7 @@ def run_ours(args, wl):
                             "traffic": (dram_ps * steps_per_launch) if dram_ps else None,
                             "peak_source": peak_kind,
                             "algorithmic_bytes_per_step": bpstep, "kernel_ms_per_launch": kernel_ms / args.steps,
-                            "kernel": "k_walk_weighted" if h_w is not None else "k_walk_incore"}
+                            "kernel": "k_walk_incore (weighted)" if h_w is not None else "k_walk_incore"}
         if dram_ps:
             line["roofline"]["dram_bytes_per_step"] = dram_ps
             line["roofline"]["dram_frac"] = dram_ps * steps_per_launch / kernel_s / 1e9 / peaks["hbm_gbs"]

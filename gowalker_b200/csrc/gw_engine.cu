@@ -615,10 +615,18 @@ int gw_handle::run_incore(gw_stats *stats)
     a.ctr = d_ctr;
     a.err = d_err;
     const bool sopr = cfg.algorithm != GW_NODE2VEC;
-    const bool coop = needs_coop(cfg.algorithm, a.c);
-    const int combo = (sopr ? 4 : 0) | (a.paths ? 2 : 0) | (coop ? 1 : 0);
+    const bool coop = !weighted && needs_coop(cfg.algorithm, a.c);
+    a.alias = weighted ? reinterpret_cast<const uint2 *>(d_alias) : nullptr;
+    // kernel class for the autotuner: (sopr, paths, coop), weighted Node2vec apart
+    const int combo = weighted ? 8 | (a.paths ? 2 : 0) : (sopr ? 4 : 0) | (a.paths ? 2 : 0) | (coop ? 1 : 0);
+    auto grid_of = [&](int v, bool paths_on) {
+        return weighted ? incore_grid_weighted(paths_on, v, num_sms) : incore_grid(sopr, paths_on, coop, v, num_sms);
+    };
+    auto launch = [&](const IncoreArgs &x, int v, int g) {
+        return weighted ? launch_walk_incore_weighted(x, v, g, s) : launch_walk_incore(x, sopr, coop, v, g, s);
+    };
     int variant = tuned_variant[combo];
-    if (cfg.blockpergrid == 0 && variant < 0 && !weighted) {
+    if (cfg.blockpergrid == 0 && variant < 0) {
         // Autotuner: time each register-cap variant on this run's walkers
         // (their outputs are rewritten by the full run below) and keep the
         // fastest for every later run of this kernel class.  Runs of up to
@@ -640,8 +648,7 @@ int gw_handle::run_incore(gw_stats *stats)
             const int v = i < kIncoreVariants ? i : 2 * kIncoreVariants - 1 - i;
             if ((st = cuda(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * kCtrCount, s), "memset"))) return st;
             if ((st = cuda(cudaEventRecord(ev_kernel0, s), "event"))) return st;
-            if ((st = cuda(launch_walk_incore(c, sopr, coop, v, incore_grid(sopr, c.paths != nullptr, coop, v, num_sms), s),
-                           "walk kernel launch (tuning)")))
+            if ((st = cuda(launch(c, v, grid_of(v, c.paths != nullptr)), "walk kernel launch (tuning)")))
                 return st;
             if ((st = cuda(cudaEventRecord(ev_kernel1, s), "event"))) return st;
             if ((st = cuda(cudaEventSynchronize(ev_kernel1), "tuning"))) return st;
@@ -659,13 +666,9 @@ int gw_handle::run_incore(gw_stats *stats)
     last_variant = variant;
     if ((st = cuda(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * kCtrCount, s), "memset"))) return st;
     int grid = (int)cfg.blockpergrid;
-    if (grid <= 0) grid = incore_grid(sopr, a.paths != nullptr, coop, variant, num_sms);
+    if (grid <= 0) grid = grid_of(variant, a.paths != nullptr);
     if ((st = cuda(cudaEventRecord(ev_kernel0, s), "event"))) return st;
-    if (weighted) {
-        if ((st = cuda(launch_walk_weighted(a, d_alias, num_sms, s), "weighted walk kernel launch"))) return st;
-    } else if ((st = cuda(launch_walk_incore(a, sopr, coop, variant, grid, s), "walk kernel launch"))) {
-        return st;
-    }
+    if ((st = cuda(launch(a, variant, grid), "walk kernel launch"))) return st;
     if ((st = cuda(cudaEventRecord(ev_kernel1, s), "event"))) return st;
     if ((st = cuda(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(unsigned long long) * kCtrCount, cudaMemcpyDeviceToHost, s),
                    "counters D2H")))

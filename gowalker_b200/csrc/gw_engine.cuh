@@ -79,8 +79,8 @@ struct gw_handle {
 
     // autotuner: best register-cap variant per in-core kernel class
     // (sopr, paths, coop) and the measured times of each variant
-    int tuned_variant[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
-    float tuned_ms[8][gw::kIncoreVariants] = {};
+    int tuned_variant[16] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
+    float tuned_ms[16][gw::kIncoreVariants] = {};
     int last_variant = -1;
 
     // out-of-core state (gw_ooc.cu)

@@ -78,6 +78,7 @@ struct IncoreArgs {
     uint64_t *hashes;          // FNV-1a per path
     unsigned long long *ctr;   // Counter slots
     uint32_t *err;             // ErrBit word
+    const uint2 *alias;        // weighted Node2vec: {prob bits, alias column} per edge; null when unweighted
 };
 
 // Source vertex of walker `wid` (engine/walk.hpp:32-49 per-vertex ids
@@ -105,6 +106,9 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
 constexpr int kIncoreVariants = 4;
 int incore_grid(bool sopr, bool paths, bool coop, int variant, int num_sms);
 cudaError_t launch_walk_incore(const IncoreArgs &a, bool sopr, bool coop, int variant, int grid, cudaStream_t s);
+// Weighted Node2vec through the same kernel (candidates from a.alias).
+int incore_grid_weighted(bool paths, int variant, int num_sms);
+cudaError_t launch_walk_incore_weighted(const IncoreArgs &a, int variant, int grid, cudaStream_t s);
 
 // Whether a run needs the warp-cooperative path for hard steps: always for
 // SOPR/SOSR (acceptance ~ deg(prev)/deg(cur) next to hubs); for Node2vec

@@ -27,7 +27,10 @@ enum ParkWord : int {
     kPkPheadHi, kPkHashLo, kPkHashHi, kPkThr0, kPkThr1, kPkThr2, kPkRx, kPkRy, kPkTrials, kPkAstar, kPkCount
 };
 
-template <bool SOPR, bool PATHS, bool COOP, int MINB>
+// W: weighted Node2vec -- the trial's candidate is alias column r.x % deg,
+// kept when float(r.w >> 8) * 2^-24 < its probability, else its alias (the
+// alias tables of gw_weighted.cu); everything else is the unweighted step.
+template <bool SOPR, bool PATHS, bool COOP, int MINB, bool W = false>
 __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const __grid_constant__ IncoreArgs a)
 {
     __shared__ uint32_t s_iv[kWalkThreads / 32][kCoopScratchWords];  // per-warp scratch of warp_first_accept
@@ -204,7 +207,12 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const __grid
         // One rejection-sampling trial.
         const uint32_t pos = r.x % deg;
         const float rv = rand_val(r.y, thr_max<SOPR>(a.c, t));
-        const uint32_t x = __ldg(csr + head + pos);
+        uint32_t col = pos;
+        if constexpr (W) {
+            const uint2 e = __ldg(a.alias + head + pos);
+            if (!(__uint2float_rn(r.w >> 8) * 0x1p-24f < __uint_as_float(e.x))) col = e.y;
+        }
+        const uint32_t x = __ldg(csr + head + col);
         n_trials++;
         if (accept_candidate<SOPR>(a.c, t, rv, x, prev, cur, a.ix, phead, pdeg)) {
             hop++;
@@ -310,38 +318,51 @@ template <> struct MinBlocks<1> { static constexpr int value = 5; };
 template <> struct MinBlocks<2> { static constexpr int value = 6; };
 template <> struct MinBlocks<3> { static constexpr int value = 8; };
 
-template <bool SOPR, bool PATHS, bool COOP, int V>
+template <bool SOPR, bool PATHS, bool COOP, int V, bool W = false>
 static int grid_for(int num_sms)
 {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_incore<SOPR, PATHS, COOP, MinBlocks<V>::value>,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_incore<SOPR, PATHS, COOP, MinBlocks<V>::value, W>,
                                                   kWalkThreads, 0);
     if (per_sm < 1) per_sm = 1;
     return per_sm * num_sms;
 }
 
-template <bool SOPR, bool PATHS, bool COOP, int V>
+template <bool SOPR, bool PATHS, bool COOP, int V, bool W = false>
 static void launch_one(const IncoreArgs &a, int grid, cudaStream_t s)
 {
-    k_walk_incore<SOPR, PATHS, COOP, MinBlocks<V>::value><<<grid, kWalkThreads, 0, s>>>(a);
+    k_walk_incore<SOPR, PATHS, COOP, MinBlocks<V>::value, W><<<grid, kWalkThreads, 0, s>>>(a);
 }
 
-template <bool SOPR, bool PATHS, bool COOP>
+template <bool SOPR, bool PATHS, bool COOP, bool W = false>
 static int grid_v(int variant, int num_sms)
 {
-    if (variant == 0) return grid_for<SOPR, PATHS, COOP, 0>(num_sms);
-    if (variant == 1) return grid_for<SOPR, PATHS, COOP, 1>(num_sms);
-    if (variant == 2) return grid_for<SOPR, PATHS, COOP, 2>(num_sms);
-    return grid_for<SOPR, PATHS, COOP, 3>(num_sms);
+    if (variant == 0) return grid_for<SOPR, PATHS, COOP, 0, W>(num_sms);
+    if (variant == 1) return grid_for<SOPR, PATHS, COOP, 1, W>(num_sms);
+    if (variant == 2) return grid_for<SOPR, PATHS, COOP, 2, W>(num_sms);
+    return grid_for<SOPR, PATHS, COOP, 3, W>(num_sms);
 }
 
-template <bool SOPR, bool PATHS, bool COOP>
+template <bool SOPR, bool PATHS, bool COOP, bool W = false>
 static void launch_v(const IncoreArgs &a, int variant, int grid, cudaStream_t s)
 {
-    if (variant == 0) launch_one<SOPR, PATHS, COOP, 0>(a, grid, s);
-    else if (variant == 1) launch_one<SOPR, PATHS, COOP, 1>(a, grid, s);
-    else if (variant == 2) launch_one<SOPR, PATHS, COOP, 2>(a, grid, s);
-    else launch_one<SOPR, PATHS, COOP, 3>(a, grid, s);
+    if (variant == 0) launch_one<SOPR, PATHS, COOP, 0, W>(a, grid, s);
+    else if (variant == 1) launch_one<SOPR, PATHS, COOP, 1, W>(a, grid, s);
+    else if (variant == 2) launch_one<SOPR, PATHS, COOP, 2, W>(a, grid, s);
+    else launch_one<SOPR, PATHS, COOP, 3, W>(a, grid, s);
+}
+
+int incore_grid_weighted(bool paths, int variant, int num_sms)
+{
+    return paths ? grid_v<false, true, false, true>(variant, num_sms) : grid_v<false, false, false, true>(variant, num_sms);
+}
+
+cudaError_t launch_walk_incore_weighted(const IncoreArgs &a, int variant, int grid, cudaStream_t s)
+{
+    if (!a.alias) return cudaErrorInvalidValue;
+    if (a.paths) launch_v<false, true, false, true>(a, variant, grid, s);
+    else launch_v<false, false, false, true>(a, variant, grid, s);
+    return cudaGetLastError();
 }
 
 int incore_grid(bool sopr, bool paths, bool coop, int variant, int num_sms)

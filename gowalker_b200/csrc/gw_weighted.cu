@@ -1,4 +1,4 @@
-// Weighted Node2vec walks, in-core (GW has no counterpart: the reference loads
+// Weighted Node2vec walks, in-core (the reference has no counterpart: it loads
 // edge weights, engine/cache.hpp:71, gpu/memory.hpp:134-137, and never samples
 // with them).
 //
@@ -12,6 +12,8 @@
 // float(lane w >> 8) * 2^-24; the trial takes column i when coin < prob[i],
 // its alias otherwise.  Lanes y (rand value) and z (termination) keep their
 // meaning, so a graph whose weights are all equal walks exactly as unweighted.
+// The walk itself is the in-core kernel (gw_walk.cu) with its W flag; this
+// file builds the alias tables.
 //
 // Alias tables (Vose's method, per vertex, one thread each): the weights are
 // summed in double in index order, scaled to p_i = w_i * deg / sum, split
@@ -24,7 +26,6 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "gw_kernels.cuh"
-#include "gw_step.cuh"
 #include "gw_weighted.cuh"
 
 namespace gw {
@@ -77,87 +78,6 @@ __global__ void k_build_alias(const uint64_t *__restrict__ beg, const float *__r
     }
 }
 
-// One walker per thread, grid-stride over the walker ids; the oracle's step
-// loop (oracle/gw_oracle.c walk_from) with the alias draw.
-template <bool PATHS>
-__global__ void __launch_bounds__(256) k_walk_weighted(const __grid_constant__ IncoreArgs a,
-                                                       const AliasEntry *__restrict__ al)
-{
-    const uint64_t *__restrict__ beg = a.beg;
-    const uint32_t *__restrict__ csr = a.ix.csr;
-    const uint32_t maxhops = a.c.maxhops;
-    const StepThr t{0.f, 0.f, 0.f};
-    const float maxv = a.c.n2v_maxv;
-    unsigned long long steps = 0, trials = 0, done = 0, hsum = 0;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.nwalkers; i += stride) {
-        const uint32_t wid = a.wid_base + (uint32_t)i * a.wid_stride;
-        const uint32_t src = walker_source(a.init, wid);
-        uint32_t prev = src, cur = src, hop = 0, moves = 0;
-        uint64_t h = hash_init(src);
-        if (PATHS) a.paths[(uint64_t)wid * a.stride] = src;
-        if (src >= a.nverts) {
-            atomicOr(a.err, kErrSource);
-            hop = maxhops;
-        }
-        while (hop < maxhops) {
-            if (hop > 0 && a.c.term_prob > 0.f && terminates(a.c, draw(a.c, wid, hop, 0).z)) break;
-            const uint64_t head = __ldg(beg + cur), deg = __ldg(beg + cur + 1) - head;
-            if (deg == 0) break;  // dead end (engine/engine.hpp:196-199)
-            const uint64_t phead = __ldg(beg + prev);
-            const uint32_t pdeg = (uint32_t)(__ldg(beg + prev + 1) - phead);
-            uint32_t attempt = 0, x = 0;
-            bool ok = false;
-            while (attempt < kMaxAttempts) {
-                const U4 r = draw(a.c, wid, hop, attempt);
-                ++attempt;
-                const uint64_t pos = (uint64_t)r.x % deg;
-                const uint2 e = __ldg(reinterpret_cast<const uint2 *>(al + head + pos));
-                const float coin = __uint2float_rn(r.w >> 8) * 0x1p-24f;
-                const uint64_t col = coin < __uint_as_float(e.x) ? pos : (uint64_t)e.y;
-                x = __ldg(csr + head + col);
-                if (accept_candidate<false>(a.c, t, rand_val(r.y, maxv), x, prev, cur, a.ix, phead, pdeg)) {
-                    ok = true;
-                    break;
-                }
-            }
-            trials += attempt;
-            if (!ok) {
-                atomicOr(a.err, kErrTrials);
-                break;
-            }
-            if (x >= a.nverts) {
-                atomicOr(a.err, kErrVertexRange);
-                break;
-            }
-            prev = cur;
-            cur = x;
-            ++hop;
-            ++moves;
-            h = hash_step(h, x);
-            if (PATHS) a.paths[(uint64_t)wid * a.stride + moves] = x;
-        }
-        a.hashes[wid] = h;
-        a.lens[wid] = moves + 1;
-        steps += moves;
-        done += 1;
-        hsum += h;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        steps += __shfl_xor_sync(0xFFFFFFFFu, steps, o);
-        trials += __shfl_xor_sync(0xFFFFFFFFu, trials, o);
-        done += __shfl_xor_sync(0xFFFFFFFFu, done, o);
-        hsum += __shfl_xor_sync(0xFFFFFFFFu, hsum, o);
-    }
-    if ((threadIdx.x & 31u) == 0 && done) {
-        atomicAdd(&a.ctr[kCtrSteps], steps);
-        atomicAdd(&a.ctr[kCtrTrials], trials);
-        atomicAdd(&a.ctr[kCtrDone], done);
-        atomicAdd(&a.ctr[kCtrHashSum], hsum);
-    }
-}
-
 cudaError_t launch_build_alias(const uint64_t *beg, const float *w, uint32_t nverts, double *pd, uint32_t *qs,
                                uint32_t *ql, AliasEntry *out, uint32_t *err, int num_sms, cudaStream_t s)
 {
@@ -165,12 +85,5 @@ cudaError_t launch_build_alias(const uint64_t *beg, const float *w, uint32_t nve
     return cudaGetLastError();
 }
 
-cudaError_t launch_walk_weighted(const IncoreArgs &a, const AliasEntry *al, int num_sms, cudaStream_t s)
-{
-    const int grid = num_sms * 8;
-    if (a.paths) k_walk_weighted<true><<<grid, 256, 0, s>>>(a, al);
-    else k_walk_weighted<false><<<grid, 256, 0, s>>>(a, al);
-    return cudaGetLastError();
-}
 
 }  // namespace gw

@@ -19,6 +19,5 @@ static_assert(sizeof(AliasEntry) == 8, "one 8-byte load per trial");
 // positive and finite sets kErrWeight (that vertex gets a uniform table).
 cudaError_t launch_build_alias(const uint64_t *beg, const float *w, uint32_t nverts, double *pd, uint32_t *qs,
                                uint32_t *ql, AliasEntry *out, uint32_t *err, int num_sms, cudaStream_t s);
-cudaError_t launch_walk_weighted(const IncoreArgs &a, const AliasEntry *al, int num_sms, cudaStream_t s);
 
 }  // namespace gw
