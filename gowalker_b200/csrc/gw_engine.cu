@@ -739,16 +739,30 @@ extern "C" int gw_get_paths(gw_handle *h, uint64_t first, uint64_t n, uint32_t *
     if (first + n > h->nwalkers) return h->fail(GW_ERR_ARG, "walker range out of bounds");
     cudaSetDevice(h->cfg.device);
     int st;
+    std::vector<uint32_t> own_lens;
+    uint32_t *L = lens;
+    if (!L && out && n) {  // the lengths are needed to zero the rows' tails
+        own_lens.resize(n);
+        L = own_lens.data();
+    }
+    if (L && n) {
+        if ((st = h->cuda(cudaMemcpy(L, h->d_lens + first, n * sizeof(uint32_t), cudaMemcpyDeviceToHost),
+                          "lengths D2H")))
+            return st;
+    }
     if (out && n) {
         if ((st = h->cuda(cudaMemcpy(out, h->d_paths + first * h->path_stride,
                                      n * h->path_stride * sizeof(uint32_t), cudaMemcpyDeviceToHost),
                           "paths D2H")))
             return st;
-    }
-    if (lens && n) {
-        if ((st = h->cuda(cudaMemcpy(lens, h->d_lens + first, n * sizeof(uint32_t), cudaMemcpyDeviceToHost),
-                          "lengths D2H")))
-            return st;
+        // The kernels write a row only up to the walk's length; the rest of
+        // the device row holds whatever the buffer held before, so the
+        // padding is made here.
+        const uint64_t stride = h->path_stride;
+        for (uint64_t i = 0; i < n; ++i) {
+            const uint64_t len = L[i] < stride ? L[i] : stride;
+            std::fill(out + i * stride + len, out + (i + 1) * stride, 0u);
+        }
     }
     return GW_OK;
 }

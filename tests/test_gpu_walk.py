@@ -325,3 +325,23 @@ def test_windowed_rand_bounds_match_search(tmp_path):
         assert L.check_bounds(flag, thr.ctypes.data_as(ctypes.c_void_p), n, fast.ctypes.data_as(ctypes.c_void_p),
                               slow.ctypes.data_as(ctypes.c_void_p)) == 0
         assert np.array_equal(fast, slow), np.nonzero(fast != slow)[0][:10]
+
+
+def test_path_rows_zero_padded_after_longer_walks(gw, oracle):
+    """gw_get_paths pads each row past the walk's length with zeros, also when
+    the device rows still hold an earlier, longer run's vertices."""
+    beg, csr = oracle.rmat_graph(11)
+    V = len(beg) - 1
+    eng = gw.WalkEngine(algorithm=1, maxhops=20, alpha=0.2, term_prob=0.0, seed=4, walkpersource=1, record_paths=1,
+                        cache_size=1 << 34)
+    eng.set_host_graph(beg, csr)
+    eng.init_walkers(1, 1, 4)
+    eng.run()
+    eng.set_config(term_prob=0.3)
+    eng.init_walkers(1, 1, 4)
+    eng.run()
+    P, L = eng.paths()
+    ref = oracle.walk(beg, csr, oracle.make_cfg(algo=1, maxhops=20, alpha=0.2, term_prob=0.3, seed=4), 0, V)
+    assert (L < 21).any()
+    assert np.array_equal(L, ref["lens"]) and np.array_equal(P, ref["paths"])
+    eng.close()
