@@ -15,7 +15,8 @@
 // The walk itself is the in-core kernel (gw_walk.cu) with its W flag; this
 // file builds the alias tables.
 //
-// Alias tables (Vose's method, per vertex, one thread each): the weights are
+// Alias tables (Vose's method, per vertex: one thread each, a CTA for each
+// vertex above 256 neighbours): the weights are
 // summed in double in index order, scaled to p_i = w_i * deg / sum, split
 // into a queue of p < 1 and a queue of p >= 1 in index order; repeatedly the
 // next small s takes the front large l as its alias (prob[s] = (float)p_s)
@@ -30,6 +31,39 @@
 
 namespace gw {
 
+constexpr uint64_t kHubDeg = 256;            // vertices above this degree get a CTA each
+constexpr uint64_t kHubSmemEntries = 20480;  // their probabilities in shared memory up to this degree (160 KB)
+
+// Vose's loop for one vertex whose probabilities p[0, d) are scaled; the
+// queues hold indices in the order they are pushed.  p and the queues may be
+// shared or global memory.
+__device__ void vose_loop(uint64_t d, double *p, uint32_t *small, uint32_t *large, AliasEntry *out)
+{
+    uint64_t ns = 0, nl = 0, hs = 0, hl = 0;
+    for (uint64_t i = 0; i < d; ++i) {
+        if (p[i] < 1.0) small[ns++] = (uint32_t)i;
+        else large[nl++] = (uint32_t)i;
+    }
+    while (hs < ns && hl < nl) {
+        const uint32_t sidx = small[hs++], lidx = large[hl];
+        out[sidx] = AliasEntry{__double2float_rn(p[sidx]), lidx};
+        p[lidx] = __dsub_rn(__dadd_rn(p[lidx], p[sidx]), 1.0);
+        if (p[lidx] < 1.0) {
+            ++hl;
+            small[ns++] = lidx;
+        }
+    }
+    while (hl < nl) {
+        const uint32_t lidx = large[hl++];
+        out[lidx] = AliasEntry{1.f, lidx};
+    }
+    while (hs < ns) {
+        const uint32_t sidx = small[hs++];
+        out[sidx] = AliasEntry{1.f, sidx};
+    }
+}
+
+// Vertices of degree at most kHubDeg: one thread each.
 __global__ void k_build_alias(const uint64_t *__restrict__ beg, const float *__restrict__ w, uint32_t nverts,
                               double *__restrict__ pd, uint32_t *__restrict__ qs, uint32_t *__restrict__ ql,
                               AliasEntry *__restrict__ out, uint32_t *err)
@@ -37,7 +71,7 @@ __global__ void k_build_alias(const uint64_t *__restrict__ beg, const float *__r
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nverts; v += stride) {
         const uint64_t h = beg[v], d = beg[v + 1] - h;
-        if (d == 0) continue;
+        if (d == 0 || d > kHubDeg) continue;
         double sum = 0.0;
         bool bad = false;
         for (uint64_t i = 0; i < d; ++i) {
@@ -50,31 +84,52 @@ __global__ void k_build_alias(const uint64_t *__restrict__ beg, const float *__r
             for (uint64_t i = 0; i < d; ++i) out[h + i] = AliasEntry{1.f, (uint32_t)i};
             continue;
         }
-        double *p = pd + h;
-        uint32_t *small = qs + h, *large = ql + h;
-        uint64_t ns = 0, nl = 0, hs = 0, hl = 0;
-        for (uint64_t i = 0; i < d; ++i) {
-            p[i] = __ddiv_rn(__dmul_rn((double)w[h + i], (double)d), sum);
-            if (p[i] < 1.0) small[ns++] = (uint32_t)i;
-            else large[nl++] = (uint32_t)i;
-        }
-        while (hs < ns && hl < nl) {
-            const uint32_t sidx = small[hs++], lidx = large[hl];
-            out[h + sidx] = AliasEntry{__double2float_rn(p[sidx]), lidx};
-            p[lidx] = __dsub_rn(__dadd_rn(p[lidx], p[sidx]), 1.0);
-            if (p[lidx] < 1.0) {
-                ++hl;
-                small[ns++] = lidx;
+        for (uint64_t i = 0; i < d; ++i) pd[h + i] = __ddiv_rn(__dmul_rn((double)w[h + i], (double)d), sum);
+        vose_loop(d, pd + h, qs + h, ql + h, out + h);
+    }
+}
+
+// Vertices of degree above kHubDeg: one CTA each.  The sum stays one
+// sequential chain of double additions in index order (thread 0) and the
+// loop stays Vose's serial loop, so the tables equal the small-vertex path's;
+// the CTA scales the probabilities in parallel and the loop runs on
+// shared-memory probabilities (up to kHubSmemEntries), where a serial chain
+// of dependent accesses costs far less than in global memory.
+__global__ void __launch_bounds__(128)
+    k_build_alias_hubs(const uint64_t *__restrict__ beg, const float *__restrict__ w, uint32_t nverts,
+                       double *__restrict__ pd, uint32_t *__restrict__ qs, uint32_t *__restrict__ ql,
+                       AliasEntry *__restrict__ out, uint32_t *err)
+{
+    extern __shared__ double s_p[];
+    __shared__ double s_sum;
+    __shared__ int s_bad;
+    for (uint64_t v = blockIdx.x; v < nverts; v += gridDim.x) {
+        const uint64_t h = beg[v], d = beg[v + 1] - h;
+        if (d <= kHubDeg) continue;  // uniform over the CTA
+        if (threadIdx.x == 0) {
+            double sum = 0.0;
+            bool bad = false;
+            for (uint64_t i = 0; i < d; ++i) {
+                const float wi = w[h + i];
+                bad |= !(wi > 0.f && wi < __int_as_float(0x7F800000));
+                sum = __dadd_rn(sum, (double)wi);
             }
+            s_sum = sum;
+            s_bad = bad ? 1 : 0;
         }
-        while (hl < nl) {
-            const uint32_t lidx = large[hl++];
-            out[h + lidx] = AliasEntry{1.f, lidx};
+        __syncthreads();
+        if (s_bad) {
+            if (threadIdx.x == 0) atomicOr(err, kErrWeight);
+            for (uint64_t i = threadIdx.x; i < d; i += blockDim.x) out[h + i] = AliasEntry{1.f, (uint32_t)i};
+        } else {
+            double *p = d <= kHubSmemEntries ? s_p : pd + h;
+            const double sum = s_sum;
+            for (uint64_t i = threadIdx.x; i < d; i += blockDim.x)
+                p[i] = __ddiv_rn(__dmul_rn((double)w[h + i], (double)d), sum);
+            __syncthreads();
+            if (threadIdx.x == 0) vose_loop(d, p, qs + h, ql + h, out + h);
         }
-        while (hs < ns) {
-            const uint32_t sidx = small[hs++];
-            out[h + sidx] = AliasEntry{1.f, sidx};
-        }
+        __syncthreads();
     }
 }
 
@@ -82,6 +137,13 @@ cudaError_t launch_build_alias(const uint64_t *beg, const float *w, uint32_t nve
                                uint32_t *ql, AliasEntry *out, uint32_t *err, int num_sms, cudaStream_t s)
 {
     k_build_alias<<<num_sms * 8, 128, 0, s>>>(beg, w, nverts, pd, qs, ql, out, err);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const size_t smem = kHubSmemEntries * sizeof(double);
+    if ((e = cudaFuncSetAttribute(k_build_alias_hubs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+        cudaSuccess)
+        return e;
+    k_build_alias_hubs<<<num_sms * 2, 128, smem, s>>>(beg, w, nverts, pd, qs, ql, out, err);
     return cudaGetLastError();
 }
 
