@@ -507,6 +507,26 @@ def prep_cpu_baseline(src, dst, V, target_s):
             "sample": "first %d of the samples, symmetrised + deduplicated + sorted" % k}
 
 
+def rank_seed(rank):
+    """Walk seed of a rank: every rank walks its own replica of the workload
+    (walkers are independent), so the per-GPU work stays fixed as N grows."""
+    return 42 + rank
+
+
+def reduce_rank_times(dist, ms, ms2, steps, e2e_steps, device):
+    """Whole-job figures from every rank's own: the slowest rank's times (max)
+    and all ranks' steps (sum), so value = all steps / the max time.  Every
+    rank must call it (two all-reduces, in the same order everywhere)."""
+    if dist is None:
+        return ms, ms2, float(steps), float(e2e_steps)
+    import torch
+    tmax = torch.tensor([ms, ms2], dtype=torch.float64, device=device)
+    tsum = torch.tensor([float(steps), float(e2e_steps)], dtype=torch.float64, device=device)
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return float(tmax[0]), float(tmax[1]), float(tsum[0]), float(tsum[1])
+
+
 def run_ours(args, wl):
     import torch
     import gowalker_b200 as gw
@@ -522,7 +542,7 @@ def run_ours(args, wl):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     torch.cuda.set_device(local)
-    seed = 42 + rank
+    seed = rank_seed(rank)
     paths = 1 if args.paths else 0
 
     dg = build_graph(gw, wl)
@@ -612,16 +632,7 @@ def run_ours(args, wl):
         log("warning: e2e checksum differs from the device-resident run")
 
     # max over ranks
-    t = torch.tensor([ms, ms2, float(steps), float(e2e_steps)], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        tmax = t.clone()
-        dist.all_reduce(tmax[:2], op=dist.ReduceOp.MAX)
-        tsum = t.clone()
-        dist.all_reduce(tsum[2:], op=dist.ReduceOp.SUM)
-        ms, ms2 = float(tmax[0]), float(tmax[1])
-        steps_all, e2e_all = float(tsum[2]), float(tsum[3])
-    else:
-        steps_all, e2e_all = float(steps), float(e2e_steps)
+    ms, ms2, steps_all, e2e_all = reduce_rank_times(dist, ms, ms2, steps, e2e_steps, "cuda")
 
     if rank == 0:
         peaks, peak_kind = measured_peaks()
