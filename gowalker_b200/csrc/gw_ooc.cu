@@ -87,7 +87,7 @@ struct OocState {
     float train_loss = 0.f;
     float *d_params = nullptr, *d_train_ws = nullptr;
     float *d_trace_x = nullptr, *d_trace_col = nullptr, *d_trace_y = nullptr;
-    float *d_train_x = nullptr, *d_pred = nullptr;
+    float *d_train_x = nullptr, *d_pred = nullptr, *d_pred_res = nullptr;  // forecast log demand, its change
     float *d_emass = nullptr, *d_vfrac = nullptr, *d_prev_col = nullptr, *d_ema = nullptr;
     int32_t *d_choose = nullptr, *h_choose = nullptr;
     float *h_pred = nullptr, *h_col = nullptr;
@@ -172,7 +172,7 @@ void gw_handle::ooc_release()
     o.h_snap[0] = o.h_snap[1] = o.dm_snap[0] = o.dm_snap[1] = nullptr;
     for (auto *p : o.h_blk_pin)
         if (p) cudaFreeHost((void *)p);
-    for (float *p : {o.d_params, o.d_train_ws, o.d_trace_x, o.d_trace_col, o.d_trace_y, o.d_train_x,
+    for (float *p : {o.d_params, o.d_pred_res, o.d_train_ws, o.d_trace_x, o.d_trace_col, o.d_trace_y, o.d_train_x,
                      o.d_pred, o.d_emass, o.d_vfrac, o.d_prev_col, o.d_ema})
         cudaFree(p);
     cudaFree(o.d_choose);
@@ -198,6 +198,7 @@ static int learned_setup(gw_handle *h)
     if ((st = dalloc(&o.d_trace_y, (uint64_t)kTraceIters * nb, "targets"))) return st;
     if ((st = dalloc(&o.d_train_x, (uint64_t)kTraceIters * nb * kMlpIn, "training set"))) return st;
     if ((st = dalloc(&o.d_pred, nb, "predictions"))) return st;
+    if ((st = dalloc(&o.d_pred_res, nb, "predictions"))) return st;
     if ((st = dalloc(&o.d_emass, nb, "edge shares"))) return st;
     if ((st = dalloc(&o.d_vfrac, nb, "vertex shares"))) return st;
     if ((st = dalloc(&o.d_prev_col, nb, "history"))) return st;
@@ -696,6 +697,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         return st;
     }
     uint32_t trace_t = 0, learned_iters = 0;
+    bool stall_next = false;  // a learned choice moved no walker: the next decision is the plain rule's
     bool reverted = false;
     uint64_t learned_steps = 0, learned_bytes = 0, plain_steps = 0, plain_bytes = 0;
     uint64_t phase_steps_mark = 0, phase_bytes_mark = 0;
@@ -806,19 +808,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             if ((st = cuda(launch_features(f, ds), "features"))) break;
             launches++;
             if (predicting) {
-                if ((st = cuda(mlp_forward(o.d_params, ring_x, nb, o.d_pred, ds), "predictor"))) break;
-                if ((st = cuda(launch_add_level(o.d_pred, ring_x, nb, ds), "predictor"))) break;
+                if ((st = cuda(mlp_forward(o.d_params, ring_x, nb, o.d_pred_res, ds), "predictor"))) break;
+                if ((st = cuda(launch_add_level(o.d_pred_res, ring_x, o.d_pred, nb, ds), "predictor"))) break;
                 launches += 2;
-            }
-            if (learned_active) {
-                if ((st = cuda(launch_learned_choose(o.d_pred, nb, o.d_blk_csr2, o.d_cached, ncached, capacity,
-                                                     prefetch ? 1u : kMaxLoadsPerIter, kSwapMargin, o.d_choose, ds),
-                               "learned choice")))
-                    break;
-                launches++;
-                if ((st = cuda(cudaMemcpyAsync(o.h_choose, o.d_choose, sizeof(int32_t) * (2 * kMaxLoadsPerIter + 1),
-                                               cudaMemcpyDeviceToHost, ds), "choice")))
-                    break;
             }
             if (predicting) {
                 if ((st = cuda(cudaMemcpyAsync(o.h_pred, o.d_pred, sizeof(float) * nb, cudaMemcpyDeviceToHost, ds),
@@ -831,8 +823,11 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         }
         // ---- plain block choice on the device (decision, fallback and rescue), read back
         if (trace) cudaEventRecord(td0, ds);
+        // learned: the plain rule's scores, each block's scaled by the
+        // network's forecast growth of its demand
+        const bool learned_decides = learned_active && !stall_next;
         if ((st = cuda(launch_schedule(o.d_pairs, o.d_offsets + nbk, nb, o.d_cached, ncached, capacity, cfg.zero_threshold,
-                                       nullptr, 0.f, o.d_dec, ds),
+                                       learned_decides ? o.d_pred_res : nullptr, 1.f, o.d_dec, ds),
                        "schedule")))
             break;
         launches++;
@@ -901,6 +896,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         // next decision to the plain rule and its rescue, which always make
         // some bucket runnable
         const bool learned_stalled = last_phase == 1 && steps_now == phase_steps_mark;
+        stall_next = learned_stalled;
         phase_steps_mark = steps_now;
         phase_bytes_mark = h2d;
         last_phase = -1;
@@ -938,13 +934,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if (nlive == 0) break;
 
         std::vector<std::pair<int, int>> todo;  // (block, cached position or -1)
-        if (learned_active && !reverted && !learned_stalled && o.h_choose[0] > 0) {
-            for (int k = 0; k < o.h_choose[0]; ++k) todo.emplace_back(o.h_choose[1 + 2 * k], o.h_choose[2 + 2 * k]);
-            learned_iters++;
-            last_phase = 1;
-        } else if (d.action == 1 || d.action == 2) {
+        if (d.action == 1 || d.action == 2) {
             todo.emplace_back(d.block, d.action == 2 ? d.position : -1);
-            last_phase = 0;
+            last_phase = learned_decides ? 1 : 0;
+            if (learned_decides) learned_iters++;
         } else if (cfg.zero_copy && !prefetch) {
             // ---- zero-copy tail: every absent block read through mapped host memory
             if ((st = ooc_map_host(this))) break;

@@ -307,7 +307,8 @@ __global__ void __launch_bounds__(1024) k_schedule(const uint32_t *__restrict__ 
             score = all - (key >> 32);
             pos = (uint32_t)key;
         }
-        if (pred) score = (uint64_t)fmaxf(0.f, pred_weight * pred[i]) + (score > 0 ? 1 : 0);
+        // learned: scale by the forecast growth of block i's demand, e^pred
+        if (pred) score = (unsigned long long)((double)score * exp((double)fminf(fmaxf(pred_weight * pred[i], -4.f), 4.f)));
         if (lane == 0) {
             s_pos[i] = pos;
             atomicMax(&s_best, (score << 11) | (2047u - i));
@@ -659,11 +660,11 @@ __global__ void k_gather_train(const float *ring_x, const float *ring_col, uint3
     y[idx] = log1pf(s / (float)k) - xs[0];
 }
 
-// pred[i] += x[i][0]: the residual forecast back to log demand.
-__global__ void k_add_level(float *pred, const float *x, uint32_t nb)
+// level[i] = res[i] + x[i][0]: the forecast change back to log demand.
+__global__ void k_add_level(const float *res, const float *x, float *level, uint32_t nb)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nb) pred[i] += x[(uint64_t)i * 16];
+    if (i < nb) level[i] = res[i] + x[(uint64_t)i * 16];
 }
 
 // One thread: fill free slots with the highest predicted uncached blocks, then
@@ -730,9 +731,9 @@ cudaError_t launch_gather_train(const float *ring_x, const float *ring_col, uint
     return cudaGetLastError();
 }
 
-cudaError_t launch_add_level(float *pred, const float *x, uint32_t nb, cudaStream_t s)
+cudaError_t launch_add_level(const float *res, const float *x, float *level, uint32_t nb, cudaStream_t s)
 {
-    k_add_level<<<(nb + 255) / 256, 256, 0, s>>>(pred, x, nb);
+    k_add_level<<<(nb + 255) / 256, 256, 0, s>>>(res, x, level, nb);
     return cudaGetLastError();
 }
 

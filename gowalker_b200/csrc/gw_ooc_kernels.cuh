@@ -113,8 +113,8 @@ cudaError_t launch_features(const FeatureArgs &f, cudaStream_t s);
 // network forecasts the change of log demand
 cudaError_t launch_gather_train(const float *ring_x, const float *ring_col, uint32_t t0, uint32_t ring, uint32_t T,
                                 uint32_t k, uint32_t nb, float *train_x, float *y, cudaStream_t s);
-// pred[i] += x[i][0]
-cudaError_t launch_add_level(float *pred, const float *x, uint32_t nb, cudaStream_t s);
+// level[i] = res[i] + x[i][0]
+cudaError_t launch_add_level(const float *res, const float *x, float *level, uint32_t nb, cudaStream_t s);
 // Up to lmax (block, cached position or -1 for a free slot) pairs by
 // predicted demand; out[0] = count, then the pairs.
 cudaError_t launch_learned_choose(const float *pred, uint32_t nb, const uint32_t *const *blk_csr,
