@@ -89,21 +89,17 @@ struct OocState {
     float *d_trace_x = nullptr, *d_trace_col = nullptr, *d_trace_y = nullptr;
     float *d_train_x = nullptr, *d_pred = nullptr, *d_pred_res = nullptr;  // forecast log demand, its change
     float *d_emass = nullptr, *d_vfrac = nullptr, *d_prev_col = nullptr, *d_ema = nullptr;
-    int32_t *d_choose = nullptr, *h_choose = nullptr;
     float *h_pred = nullptr, *h_col = nullptr;
 };
 
 // Learned policy constants: traces of 20 plain iterations (+3 of horizon for
-// the targets) train the predictor; it then loads up to 4 blocks per
-// iteration, swapping a resident block out only for one whose predicted demand
-// is higher by `kSwapMargin` (log1p scale).
+// the targets) train the predictor; its forecast change of each block's log
+// demand then scales GOWalker's block scores (e^change, clipped to e^+-4).
 constexpr uint32_t kTraceIters = 20;  // training samples: the last 20 iterations whose horizon is observed
 constexpr uint32_t kHorizon = 3;
 constexpr uint32_t kTraceRing = kTraceIters + kHorizon;
 constexpr uint32_t kRetrain = 16;        // retrain (warm) every 16 iterations on the sliding window
 constexpr uint32_t kRetrainEpochs = 100;
-constexpr uint32_t kMaxLoadsPerIter = 4;
-constexpr float kSwapMargin = 0.25f;
 constexpr uint32_t kTrainEpochs = 400;
 constexpr float kTrainLr = 3e-3f;
 
@@ -175,8 +171,6 @@ void gw_handle::ooc_release()
     for (float *p : {o.d_params, o.d_pred_res, o.d_train_ws, o.d_trace_x, o.d_trace_col, o.d_trace_y, o.d_train_x,
                      o.d_pred, o.d_emass, o.d_vfrac, o.d_prev_col, o.d_ema})
         cudaFree(p);
-    cudaFree(o.d_choose);
-    if (o.h_choose) cudaFreeHost(o.h_choose);
     if (o.h_pred) cudaFreeHost(o.h_pred);
     if (o.h_col) cudaFreeHost(o.h_col);
     delete ooc;
@@ -203,8 +197,6 @@ static int learned_setup(gw_handle *h)
     if ((st = dalloc(&o.d_vfrac, nb, "vertex shares"))) return st;
     if ((st = dalloc(&o.d_prev_col, nb, "history"))) return st;
     if ((st = dalloc(&o.d_ema, nb, "history"))) return st;
-    if ((st = h->cuda(cudaMalloc(&o.d_choose, sizeof(int32_t) * (2 * kMaxLoadsPerIter + 1)), "choice"))) return st;
-    if ((st = h->cuda(cudaMallocHost(&o.h_choose, sizeof(int32_t) * (2 * kMaxLoadsPerIter + 1)), "choice"))) return st;
     if ((st = h->cuda(cudaMallocHost(&o.h_pred, sizeof(float) * nb), "predictions"))) return st;
     if ((st = h->cuda(cudaMallocHost(&o.h_col, sizeof(float) * nb), "demand"))) return st;
     std::vector<float> em(nb), vf(nb);

@@ -667,55 +667,6 @@ __global__ void k_add_level(const float *res, const float *x, float *level, uint
     if (i < nb) level[i] = res[i] + x[(uint64_t)i * 16];
 }
 
-// One thread: fill free slots with the highest predicted uncached blocks, then
-// swap while the best uncached block's predicted demand beats the worst
-// resident one's by `margin` (log scale); blocks chosen this round stay.
-__global__ void k_learned_choose(const float *__restrict__ pred, uint32_t nb, const uint32_t *const *blk_csr,
-                                 const uint32_t *__restrict__ cached, uint32_t ncached, uint32_t nslots,
-                                 uint32_t lmax, float margin, int32_t *out)
-{
-    __shared__ uint8_t s_state[kMaxBlocks];  // 0 absent, 1 resident, 2 chosen now, 3 evicted now
-    __shared__ int32_t s_pos[kMaxBlocks];
-    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
-        s_state[i] = blk_csr[i] != nullptr ? 1 : 0;
-        s_pos[i] = -1;
-    }
-    __syncthreads();
-    for (uint32_t j = threadIdx.x; j < ncached; j += blockDim.x) s_pos[cached[j]] = (int32_t)j;
-    __syncthreads();
-    if (threadIdx.x != 0) return;
-    uint32_t n = 0, used = ncached;
-    while (n < lmax) {
-        int bi = -1;
-        float bp = -1e30f;
-        for (uint32_t i = 0; i < nb; ++i)
-            if (s_state[i] == 0 && pred[i] > bp) {
-                bp = pred[i];
-                bi = (int)i;
-            }
-        if (bi < 0 || bp <= 0.05f) break;  // nothing worth a copy
-        int32_t pos = -1;
-        if (used >= nslots) {
-            int wj = -1;
-            float wp = 1e30f;
-            for (uint32_t i = 0; i < nb; ++i)
-                if (s_state[i] == 1 && s_pos[i] >= 0 && pred[i] < wp) {
-                    wp = pred[i];
-                    wj = (int)i;
-                }
-            if (wj < 0 || bp <= wp + margin) break;
-            pos = s_pos[wj];
-            s_state[wj] = 3;
-        } else {
-            used++;
-        }
-        s_state[bi] = 2;
-        out[1 + 2 * n] = bi;
-        out[2 + 2 * n] = pos;
-        n++;
-    }
-    out[0] = (int32_t)n;
-}
 
 cudaError_t launch_features(const FeatureArgs &f, cudaStream_t s)
 {
@@ -737,13 +688,6 @@ cudaError_t launch_add_level(const float *res, const float *x, float *level, uin
     return cudaGetLastError();
 }
 
-cudaError_t launch_learned_choose(const float *pred, uint32_t nb, const uint32_t *const *blk_csr,
-                                  const uint32_t *cached, uint32_t ncached, uint32_t nslots, uint32_t lmax,
-                                  float margin, int32_t *out, cudaStream_t s)
-{
-    k_learned_choose<<<1, 256, 0, s>>>(pred, nb, blk_csr, cached, ncached, nslots, lmax, margin, out);
-    return cudaGetLastError();
-}
 
 // ------------------------------------------------------------------ launchers
 

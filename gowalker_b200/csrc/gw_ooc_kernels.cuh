@@ -115,11 +115,6 @@ cudaError_t launch_gather_train(const float *ring_x, const float *ring_col, uint
                                 uint32_t k, uint32_t nb, float *train_x, float *y, cudaStream_t s);
 // level[i] = res[i] + x[i][0]
 cudaError_t launch_add_level(const float *res, const float *x, float *level, uint32_t nb, cudaStream_t s);
-// Up to lmax (block, cached position or -1 for a free slot) pairs by
-// predicted demand; out[0] = count, then the pairs.
-cudaError_t launch_learned_choose(const float *pred, uint32_t nb, const uint32_t *const *blk_csr,
-                                  const uint32_t *cached, uint32_t ncached, uint32_t nslots, uint32_t lmax,
-                                  float margin, int32_t *out, cudaStream_t s);
 
 int ooc_grid(bool sopr, bool paths, bool coop, int num_sms);
 cudaError_t launch_walk_ooc(const OocStepArgs &a, bool sopr, bool coop, int grid, cudaStream_t s);
