@@ -44,8 +44,8 @@ struct OocState {
     // pinned copies of the table, alternating per push (a push may still be
     // in flight when the host edits the table for the next iteration), and
     // the table as the decision stream reads it
-    const uint32_t **h_blk_pin[2] = {nullptr, nullptr};
-    const uint32_t **d_blk_csr2 = nullptr;
+    const uint32_t **h_blk_pin[2] = {nullptr, nullptr};   // pinned and mapped
+    const uint32_t **dm_blk_pin[2] = {nullptr, nullptr};  // their device aliases
     uint32_t pin_next = 0;
     // counters and error word after a re-bucketing, one per bucketing
     // parity, pinned and mapped: the re-bucketing writes them in place
@@ -162,7 +162,6 @@ void gw_handle::ooc_release()
         if (c.host) cudaFreeHost(c.host);
     cudaFree(o.d_cstage[0]);
     cudaFree(o.d_cstage[1]);
-    cudaFree((void *)o.d_blk_csr2);
     for (auto &p : o.h_snap)
         if (p) cudaFreeHost(p);
     o.h_snap[0] = o.h_snap[1] = o.dm_snap[0] = o.dm_snap[1] = nullptr;
@@ -288,9 +287,14 @@ static int ooc_setup(gw_handle *h)
     if ((st = h->cuda(cudaMalloc(&o.slot_csr, o.nslots * o.slot_csr_words * 4), "slot neighbours"))) return st;
     if ((st = h->cuda(cudaMalloc((void **)&o.d_blk_csr, nb * sizeof(void *)), "block table"))) return st;
     if ((st = h->cuda(cudaMallocHost((void **)&o.h_blk_csr, nb * sizeof(void *)), "block table"))) return st;
-    for (auto &p : o.h_blk_pin)
-        if ((st = h->cuda(cudaMallocHost((void **)&p, nb * sizeof(void *)), "block table"))) return st;
-    if ((st = h->cuda(cudaMalloc((void **)&o.d_blk_csr2, nb * sizeof(void *)), "block table"))) return st;
+    for (int k = 0; k < 2; ++k) {
+        if ((st = h->cuda(cudaHostAlloc((void **)&o.h_blk_pin[k], nb * sizeof(void *), cudaHostAllocMapped),
+                          "block table")))
+            return st;
+        if ((st = h->cuda(cudaHostGetDevicePointer((void **)&o.dm_blk_pin[k], (void *)o.h_blk_pin[k], 0),
+                          "block table")))
+            return st;
+    }
     for (int k = 0; k < 2; ++k) {
         if ((st = h->cuda(cudaHostAlloc((void **)&o.h_snap[k], sizeof(unsigned long long) * (kCtrCount + 1),
                                         cudaHostAllocMapped), "counter snapshot")))
@@ -495,8 +499,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     o.cached.clear();
     for (uint32_t b = 0; b < nb; ++b) o.h_blk_csr[b] = nullptr;
     const uint32_t **pin_last = o.h_blk_pin[0];
+    uint32_t pin_last_idx = 0;
     auto push_tables = [&]() -> int {
         pin_last = o.h_blk_pin[o.pin_next];
+        pin_last_idx = o.pin_next;
         o.pin_next ^= 1u;
         memcpy((void *)pin_last, o.h_blk_csr, nb * sizeof(void *));
         return cuda(cudaMemcpyAsync((void *)o.d_blk_csr, pin_last, nb * sizeof(void *), cudaMemcpyHostToDevice, s),
@@ -765,15 +771,11 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         const uint32_t ncached = (uint32_t)o.cached.size();
         for (uint32_t j = 0; j < ncached; ++j) o.h_cached[j] = o.cached[j];
         if ((st = cuda(cudaStreamWaitEvent(ds, ev_buck, 0), "decision wait"))) break;
-        // The cached list is read in place from mapped host memory (the last
-        // decision on ds has finished, so nothing reads it while it changes):
-        // no host-to-device copy in the decision's path, where it would queue
-        // behind the block copy in flight.  Only the learned policy needs the
-        // block table on the decision stream.
-        if (policy == GW_POLICY_LEARNED &&
-            (st = cuda(cudaMemcpyAsync((void *)o.d_blk_csr2, pin_last, nb * sizeof(void *), cudaMemcpyHostToDevice, ds),
-                       "block table")))
-            break;
+        // The cached list and (for the learned features) the block table are
+        // read in place from mapped host memory -- the last decision on ds
+        // has finished, and the table's ring slot is not rewritten before this
+        // one does -- so the decision's path has no host-to-device copy to
+        // queue behind the block copy in flight.
         // ---- learned policy: features (traces while training), prediction, choice
         const bool learned = policy == GW_POLICY_LEARNED;
         const bool learned_active = learned && o.trained && !reverted;
@@ -786,7 +788,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if (tracing) {
             FeatureArgs f{};
             f.counts = o.d_pairs;
-            f.blk_csr = o.d_blk_csr2;
+            f.blk_csr = o.dm_blk_pin[pin_last_idx];
             f.emass = o.d_emass;
             f.vfrac = o.d_vfrac;
             f.prev_col = o.d_prev_col;
