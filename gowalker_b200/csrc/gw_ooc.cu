@@ -84,7 +84,7 @@ struct OocState {
 
     // learned policy (gw_mlp.cu kernels): model, training traces, features
     bool learned_ready = false, trained = false;
-    float train_loss = 0.f;
+    float *h_loss = nullptr;  // pinned: the last training's loss, read back without blocking the host
     float *d_params = nullptr, *d_train_ws = nullptr;
     float *d_trace_x = nullptr, *d_trace_col = nullptr, *d_trace_y = nullptr;
     float *d_train_x = nullptr, *d_pred = nullptr, *d_pred_res = nullptr;  // forecast log demand, its change
@@ -167,6 +167,8 @@ void gw_handle::ooc_release()
     o.h_snap[0] = o.h_snap[1] = o.dm_snap[0] = o.dm_snap[1] = nullptr;
     for (auto *p : o.h_blk_pin)
         if (p) cudaFreeHost((void *)p);
+    if (o.h_loss) cudaFreeHost(o.h_loss);
+    o.h_loss = nullptr;
     for (float *p : {o.d_params, o.d_pred_res, o.d_train_ws, o.d_trace_x, o.d_trace_col, o.d_trace_y, o.d_train_x,
                      o.d_pred, o.d_emass, o.d_vfrac, o.d_prev_col, o.d_ema})
         cudaFree(p);
@@ -184,6 +186,8 @@ static int learned_setup(gw_handle *h)
     int st;
     auto dalloc = [&](float **p, uint64_t n, const char *what) { return h->cuda(cudaMalloc(p, n * sizeof(float)), what); };
     if ((st = dalloc(&o.d_params, kMlpParams, "predictor weights"))) return st;
+    if ((st = h->cuda(cudaMallocHost((void **)&o.h_loss, sizeof(float)), "training loss"))) return st;
+    *o.h_loss = 0.f;
     if ((st = dalloc(&o.d_train_ws, (uint64_t)kMlpGradCtas * (kMlpParams + 1) + 3 * kMlpParams + 1, "training state")))
         return st;
     if ((st = dalloc(&o.d_trace_x, (uint64_t)kTraceRing * nb * kMlpIn, "traces"))) return st;
@@ -1057,7 +1061,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                                "predictor training")))
                     break;
                 const float *loss_dev = o.d_train_ws + (uint64_t)kMlpGradCtas * (kMlpParams + 1) + 3 * kMlpParams;
-                if ((st = cuda(cudaMemcpyAsync(&o.train_loss, loss_dev, sizeof(float), cudaMemcpyDeviceToHost, ds),
+                if ((st = cuda(cudaMemcpyAsync(o.h_loss, loss_dev, sizeof(float), cudaMemcpyDeviceToHost, ds),
                                "loss")))
                     break;
                 launches += 1 + 3 * (first ? kTrainEpochs : kRetrainEpochs);
@@ -1130,7 +1134,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                     iters, stats->total_ms, kernel_ms, bucket_ms, t_install, t_copy, t_decision, t_sched, t_runnable);
         stats->learned_iterations = learned_iters;
         stats->policy_reverted = reverted ? 1u : 0u;
-        stats->train_loss = (policy == GW_POLICY_LEARNED) ? o.train_loss : 0.f;
+        stats->train_loss = (policy == GW_POLICY_LEARNED && o.h_loss) ? *o.h_loss : 0.f;
         stats->pred_error = pred_err_n ? (float)(pred_err_sum / pred_err_n) : 0.f;
         stats->persist_error = pred_err_n ? (float)(persist_err_sum / pred_err_n) : 0.f;
     }
