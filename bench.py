@@ -294,88 +294,215 @@ def run_prep_reference(args, wl):
     return 0
 
 
-PCIE_GEN5_X16_GBS = 64.0  # nominal host-link peak per direction
+PCIE_GEN5_X16_GBS = 64.0  # nominal host-link peak per direction, for context
+
+
+def cpu_model():
+    """Host CPU model name (for the CPU baseline's record)."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def measure_h2d_peak(device, nbytes=1 << 30, reps=4):
+    """Host-link peak of this box: the best of `reps` pinned host -> device
+    copies of `nbytes`, timed with CUDA events (GB/s)."""
+    import torch
+    h = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d = torch.empty(nbytes, dtype=torch.uint8, device=device)
+    best = 0.0
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        d.copy_(h, non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        best = max(best, nbytes / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    del h, d
+    torch.cuda.empty_cache()
+    return best
+
+
+def rank_shard(rank, world, n):
+    """Walker ids [first, first+count) of rank `rank`: the population split
+    into `world` contiguous id ranges (the reference's ids, engine/walk.hpp:
+    32-49), sizes differing by at most one."""
+    q, r = divmod(n, world)
+    first = rank * q + min(rank, r)
+    return first, q + (1 if rank < r else 0)
+
+
+def combine_hash_sums(dist, local, device):
+    """Sum (mod 2^64) of the ranks' path-hash sums: with walker-id shards it
+    equals the checksum of the whole population walked in one process.  Every
+    rank must call it."""
+    if dist is None:
+        return int(local) & 0xFFFFFFFFFFFFFFFF
+    import torch
+    world = dist.get_world_size()
+    v = torch.tensor([int(local) & 0xFFFFFFFF, int(local) >> 32], dtype=torch.int64, device=device)
+    out = [torch.zeros_like(v) for _ in range(world)]
+    dist.all_gather(out, v)
+    return sum(int(t[0]) | (int(t[1]) << 32) for t in out) & 0xFFFFFFFFFFFFFFFF
+
+
+def init_dist():
+    """torch.distributed over NCCL when launched by torchrun (RANK/WORLD_SIZE
+    in the environment), with a short timeout; returns (dist or None, rank,
+    world, local)."""
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world <= 1:
+        return None, rank, world, local
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return dist, rank, world, local
+
+
+POLICIES = {"plain": 0, "learned": 1, "sa": 2}
 
 
 def run_ooc_bench(args, wl):
-    """Out-of-core workload: blocks in pinned host memory, device cache capped."""
+    """Out-of-core workload: blocks in pinned host memory, device cache capped.
+    Default: the plain and the learned block policy, run after one another K
+    times each on the same engine; value = the learned arm's steps/s."""
     import torch
     import gowalker_b200 as gw
-    torch.cuda.set_device(0)
+    dist, rank, world, local = init_dist()
+    dev = torch.device("cuda", local)
+    peak_h2d = measure_h2d_peak(dev)
     dg = build_graph(gw, wl)
     beg_t, csr_t, beg, csr = host_graph(dg)
     dg.free()
     from gowalker_b200.preprocess import split_equal_edge_mass
     vb, eb = split_equal_edge_mass(beg, wl["nblocks"])
-    policy = {"plain": gw.GW_POLICY_PLAIN, "learned": gw.GW_POLICY_LEARNED, "sa": gw.GW_POLICY_SA}[args.policy]
+    arms = ["plain", "learned"] if args.policy == "pair" else [args.policy]
+    V = len(beg) - 1
+    first, count = rank_shard(rank, world, V * wl["wps"])
     eng = gw.WalkEngine(algorithm=wl["algo"], maxhops=wl["maxhops"], p=wl["p"], q=wl["q"], alpha=wl["alpha"],
-                        term_prob=wl["term"], seed=42, walkpersource=wl["wps"], record_paths=1 if args.paths else 0,
+                        term_prob=wl["term"], seed=42, walkpersource=wl["wps"], record_paths=0,
                         cache_size=wl["cache"], zero_copy=0, strict_blocks=1 if args.strict_blocks else 0,
-                        prefetch=1 if args.prefetch else 0, compress_blocks=1 if args.compress else 0)
+                        prefetch=0 if args.no_prefetch else 1, compress_blocks=0 if args.no_compress else 1,
+                        device=local)
     eng.set_host_graph(beg_t, csr_t[: len(csr)], vb, eb)
-    stream = torch.cuda.ExternalStream(eng.stream_handle())
+    stream = torch.cuda.ExternalStream(eng.stream_handle(), device=local)
+    h_hash = np.zeros(count, dtype=np.uint64)
+    L = gw.load()
+    import ctypes
+
+    def one(arm, timed=None):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record(stream)
+        eng.init_walkers(wl["algo"], wl["wps"], 42, first=first, count=count)
+        st = eng.run(POLICIES[arm])
+        ev[1].record(stream)
+        # the run's result back in host memory: every walker's path hash
+        eng._check(L.gw_path_hashes(eng.h, 0, count, ctypes.c_void_p(h_hash.ctypes.data)))
+        ev[2].record(stream)
+        if timed is not None:
+            timed.append((ev, st, int(h_hash.sum(dtype=np.uint64))))
+        return st
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
     for _ in range(args.warmup):
-        eng.init_walkers(wl["algo"], wl["wps"], 42)
-        eng.run(policy)
-    torch.cuda.synchronize()
-    clocks = ClockSampler(0)
+        for arm in arms:
+            one(arm)
+    barrier()
+    clocks = ClockSampler(local)
     clocks.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    tot = {"steps": 0, "h2d_bytes": 0, "kernel_ms": 0.0, "bucket_ms": 0.0, "block_loads": 0, "iterations": 0,
-           "launches": 0,
-           "d2h_bytes": 0, "trials": 0, "learned_iterations": 0, "policy_reverted": 0}
-    last = {}
+    rec = {arm: [] for arm in arms}
     for _ in range(args.steps):
-        eng.init_walkers(wl["algo"], wl["wps"], 42)
-        st = eng.run(policy)
-        for k in tot:
-            tot[k] += st[k]
-        last = st
-    hs, _ = eng.checksum()
-    e1.record(stream)
-    torch.cuda.synchronize()
+        for arm in arms:
+            one(arm, rec[arm])
+    barrier()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    value = tot["steps"] / (ms / 1000.0)
-    h2d_step = tot["h2d_bytes"] / args.steps
-    link = h2d_step / (ms / 1000.0 / args.steps) / 1e9
-    line = {"metric": "walk steps/sec", "value": value, "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int32 gathers, fp32/fp64 accept compares", "data": "synthetic",
-            "config": {"workload": wl["name"], "policy": args.policy,
-                       "residency": "both blocks (reference rule)" if args.strict_blocks else
-                                    "current block until N(prev) is needed",
-                       "prefetch": bool(args.prefetch),
-                       "compressed_blocks": bool(args.compress),
-                       "vertices": len(beg) - 1, "edges": len(csr),
-                       "blocks": wl["nblocks"], "cache_bytes": wl["cache"], "walkers": eng.num_walkers(),
-                       "graph_in": "pinned host memory", "paths_recorded": bool(args.paths)},
-            "gpu_launches": tot["launches"],
-            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": int(h2d_step),
-                    "d2h_bytes_per_step": int(tot["d2h_bytes"] / args.steps)},
-            "h2d_bytes_per_walk_step": tot["h2d_bytes"] / max(tot["steps"], 1),
-            "block_loads_per_run": tot["block_loads"] / args.steps,
-            "iterations_per_run": tot["iterations"] / args.steps,
-            "learned": {"iterations_per_run": tot["learned_iterations"] / args.steps,
-                        "reverted_runs": tot["policy_reverted"], "train_loss": last.get("train_loss"),
-                        "pred_error": last.get("pred_error"), "persist_error": last.get("persist_error")},
-            "trials_per_step": tot["trials"] / max(tot["steps"], 1),
-            "roofline": {"bound": "host-link", "achieved": link, "peak": PCIE_GEN5_X16_GBS, "unit": "GB/s",
-                         "frac": link / PCIE_GEN5_X16_GBS, "traffic": None,
-                         "kernel_ms_per_run": tot["kernel_ms"] / args.steps,
-                         "bucket_ms_per_run": tot["bucket_ms"] / args.steps},
-            "checksum": {"path_hash_sum": hs}}
-    if clk:
-        line["clocks"] = clk
-    if args.cpu_seconds > 0:
-        from oracle import oracle as O
-        threads = os.cpu_count() or 1
-        s_steps, s_secs, _, _, s_desc = oracle_sample(O, beg, csr, wl, 42, args.cpu_seconds, threads=threads)
-        line["cpu_baseline"] = {"value": s_steps / s_secs, "unit": "steps/s", "cores": threads, "kind": "port",
-                                "sample": s_desc}
-    print(json.dumps(line), flush=True)
+    res = {}
+    for arm in arms:
+        run_ms = sum(ev[0].elapsed_time(ev[1]) for ev, _, _ in rec[arm])
+        e2e_ms = sum(ev[0].elapsed_time(ev[2]) for ev, _, _ in rec[arm])
+        sts = [st for _, st, _ in rec[arm]]
+        steps = sum(st["steps"] for st in sts)
+        h2d = sum(st["h2d_bytes"] for st in sts)
+        run_ms, e2e_ms, steps_all, h2d_all = reduce_rank_times(dist, run_ms, e2e_ms, steps, h2d, "cuda")
+        hsum = combine_hash_sums(dist, rec[arm][-1][2], dev)
+        res[arm] = dict(
+            value=steps_all / (run_ms / 1e3), e2e=steps_all / (e2e_ms / 1e3), ms_per_run=run_ms / args.steps,
+            h2d_bytes_per_run=h2d_all / args.steps, h2d_bytes_per_walk_step=h2d_all / max(steps_all, 1),
+            steps_per_run=steps_all / args.steps, block_loads_per_run=sum(s["block_loads"] for s in sts) / args.steps,
+            iterations_per_run=sum(s["iterations"] for s in sts) / args.steps,
+            launches=sum(s["launches"] for s in sts), path_hash_sum=str(hsum),
+            kernel_ms_per_run=sum(s["kernel_ms"] for s in sts) / args.steps,
+            bucket_ms_per_run=sum(s["bucket_ms"] for s in sts) / args.steps,
+            learned_iterations_per_run=sum(s["learned_iterations"] for s in sts) / args.steps,
+            reverted_runs=sum(s["policy_reverted"] for s in sts))
+        if arm == "learned":
+            res[arm]["pred_error"] = sts[-1]["pred_error"]
+            res[arm]["persist_error"] = sts[-1]["persist_error"]
+            res[arm]["train_loss"] = sts[-1]["train_loss"]
+    head = "learned" if "learned" in res else arms[0]
+    r = res[head]
+    if rank == 0:
+        link = r["h2d_bytes_per_run"] / (r["ms_per_run"] / 1e3) / 1e9
+        line = {"metric": "walk steps/sec on 1 B200, learned vs plain schedule (bit-exact); H2D bytes/step"
+                          if args.policy == "pair" else "walk steps/sec",
+                "value": r["value"], "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["ms_per_run"], "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "int32 gathers, fp32/fp64 accept compares",
+                "data": "synthetic",
+                "config": {"workload": wl["name"], "arms": arms, "headline_arm": head,
+                           "residency": "both blocks (reference rule)" if args.strict_blocks else
+                                        "current block until N(prev) is needed",
+                           "prefetch": not args.no_prefetch, "compressed_blocks": not args.no_compress,
+                           "vertices": V, "edges": len(csr), "blocks": wl["nblocks"], "cache_bytes": wl["cache"],
+                           "walkers": V * wl["wps"], "graph_in": "pinned host memory",
+                           "l2": "every run copies the graph's blocks from the host into a 1.5 GB-class device "
+                                 "cache far larger than L2; no flush",
+                           "parallelism": "walker-id shards, one per rank" if world > 1 else "1 GPU",
+                           "walk_seed": 42, "generator_seed": 1},
+                "gpu_launches": sum(res[a]["launches"] for a in arms),
+                "e2e": {"value": r["e2e"], "unit": "steps/s", "h2d_bytes_per_step": int(r["h2d_bytes_per_run"]),
+                        "d2h_bytes_per_step": 8 * V * wl["wps"],
+                        "note": "per step: one full run through the C ABI from pinned host blocks (cold device "
+                                "cache), then every walker's 64-bit path hash read back to host memory"},
+                "h2d_bytes_per_walk_step": r["h2d_bytes_per_walk_step"],
+                "arms": res,
+                "roofline": {"bound": "host-link", "achieved": link, "peak": peak_h2d, "unit": "GB/s",
+                             "frac": link / peak_h2d, "traffic": None,
+                             "peak_source": "measured: best pinned 1 GiB host-to-device copy in this run",
+                             "nominal_pcie_gen5_x16": PCIE_GEN5_X16_GBS,
+                             "kernel": "block copies (cudaMemcpyAsync of compressed blocks) overlapped with "
+                                       "k_walk_ooc"},
+                "walks_identical_across_arms": len({res[a]["path_hash_sum"] for a in arms}) == 1}
+        if "plain" in res and "learned" in res:
+            line["learned_over_plain"] = {
+                "steps_per_s": res["learned"]["value"] / res["plain"]["value"],
+                "h2d_bytes_per_step": res["learned"]["h2d_bytes_per_walk_step"] / res["plain"]["h2d_bytes_per_walk_step"],
+                "target": "steps/s >= 1.3, H2D bytes/step <= 0.75"}
+        if clk:
+            line["clocks"] = clk
+        if args.cpu_seconds > 0:
+            from oracle import oracle as O
+            threads = os.cpu_count() or 1
+            s_steps, s_secs, _, _, s_desc = oracle_sample(O, beg, csr, wl, 42, args.cpu_seconds, threads=threads)
+            line["cpu_baseline"] = {"value": s_steps / s_secs, "unit": "steps/s", "cores": threads, "kind": "port",
+                                    "cpu_model": cpu_model(), "sample": s_desc}
+        print(json.dumps(line), flush=True)
     eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 
@@ -708,12 +835,14 @@ def main():
     ap.add_argument("--paths", type=int, default=1, help="record full paths (1) or hashes only (0)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
-    ap.add_argument("--policy", default="plain", choices=["plain", "learned", "sa"],
-                    help="block policy (out-of-core): GOWalker's rule, the learned predictor, SOWalker's annealing")
-    ap.add_argument("--compress", action="store_true",
-                    help="out-of-core: copy compressed neighbour lists and decode them on the device")
-    ap.add_argument("--prefetch", action="store_true",
-                    help="out-of-core: choose blocks one iteration ahead and overlap their copies with the step")
+    ap.add_argument("--policy", default="pair", choices=["pair", "plain", "learned", "sa"],
+                    help="block policy (out-of-core): both GOWalker's rule and the learned predictor (pair), or "
+                         "one of GOWalker's rule, the learned predictor, SOWalker's annealing")
+    ap.add_argument("--no-compress", action="store_true",
+                    help="out-of-core: copy plain neighbour lists (default: compressed, decoded on the device)")
+    ap.add_argument("--no-prefetch", action="store_true",
+                    help="out-of-core: take each block choice in its own iteration (default: one iteration "
+                         "ahead, the copy overlapped with the step)")
     ap.add_argument("--strict-blocks", action="store_true",
                     help="out-of-core: run a walker only when both its blocks are resident (the reference's rule)")
     args = ap.parse_args()

@@ -9,11 +9,12 @@ from ._abi import (GW_EDGES_DEDUP, GW_EDGES_SORT, GW_EDGES_SYMMETRIC, GW_SPLIT_E
                    GW_INIT_PER_VERTEX, GW_INIT_RANDOM, GW_INIT_SINGLE_SOURCE, GW_NODE2VEC, GW_PATHS_FULL,
                    GW_PATHS_NONE, GW_POLICY_LEARNED, GW_POLICY_PLAIN, GW_POLICY_SA, GW_SOPR, GW_SOSR, GwConfig, GwError,
                    GwStats, LIB_PATH, load)
-from .engine import DeviceGraph, WalkEngine, default_config, sa_choose_blocks, split_blocks_device
+from .engine import (DeviceGraph, WalkEngine, default_config, plain_choose_block, sa_choose_blocks,
+                     split_blocks_device)
 
 __all__ = [
     "GW_NODE2VEC", "GW_SOPR", "GW_SOSR", "GW_INIT_PER_VERTEX", "GW_INIT_SINGLE_SOURCE", "GW_INIT_RANDOM",
-    "GW_POLICY_PLAIN", "GW_POLICY_LEARNED", "GW_POLICY_SA", "sa_choose_blocks", "GW_PATHS_NONE", "GW_PATHS_FULL", "GwConfig", "GwStats",
+    "GW_POLICY_PLAIN", "GW_POLICY_LEARNED", "GW_POLICY_SA", "sa_choose_blocks", "plain_choose_block", "GW_PATHS_NONE", "GW_PATHS_FULL", "GwConfig", "GwStats",
     "GwError", "WalkEngine", "DeviceGraph", "default_config", "load", "LIB_PATH", "split_blocks_device",
     "GW_EDGES_SYMMETRIC", "GW_EDGES_SORT", "GW_EDGES_DEDUP", "GW_SPLIT_REFERENCE", "GW_SPLIT_EQUAL_EDGES",
 ]

@@ -24,8 +24,9 @@ EXPORTS = (
     "gw_version", "gw_status_string", "gw_config_default", "gw_create", "gw_destroy", "gw_last_error",
     "gw_set_config", "gw_stream", "gw_set_graph_meta", "gw_host_block", "gw_device_graph", "gw_cache_reset",
     "gw_host_weights", "gw_device_weights",
-    "gw_init_walkers", "gw_run", "gw_num_walkers", "gw_get_paths", "gw_path_hashes", "gw_checksum",
-    "gw_bucket_counts", "gw_rmat_csr", "gw_web_csr", "gw_edges_csr", "gw_split_blocks", "gw_sa_choose_blocks", "gw_device_free", "gw_memcpy", "gw_walk_noalloc",
+    "gw_init_walkers", "gw_init_walker_range", "gw_run", "gw_num_walkers", "gw_get_paths", "gw_path_hashes", "gw_checksum",
+    "gw_bucket_counts", "gw_rmat_csr", "gw_web_csr", "gw_edges_csr", "gw_split_blocks", "gw_sa_choose_blocks",
+    "gw_plain_choose_block", "gw_device_free", "gw_memcpy", "gw_walk_noalloc", "gw_philox_rate",
     "gw_mlp_forward", "gw_mlp_grad", "gw_mlp_train", "gw_host_alloc", "gw_host_free",
 )
 GW_MLP_INPUTS = 16
@@ -124,6 +125,7 @@ def load():
         "gw_host_weights": ([vp, u32, vp], i32),
         "gw_device_weights": ([vp, vp], i32),
         "gw_init_walkers": ([vp, u32, u32, u64], i32),
+        "gw_init_walker_range": ([vp, u32, u32, u64, u64, u64], i32),
         "gw_run": ([vp, u32, ctypes.POINTER(GwStats)], i32),
         "gw_num_walkers": ([vp, u64p], i32),
         "gw_get_paths": ([vp, u64, u64, vp, vp], i32),
@@ -136,7 +138,9 @@ def load():
         "gw_edges_csr": ([vp, vp, u64, u32, u32, ctypes.POINTER(vp), ctypes.POINTER(vp), u64p, u32p], i32),
         "gw_split_blocks": ([vp, u32, u32, u64, vp, vp, u32, u32p], i32),
         "gw_sa_choose_blocks": ([vp, u32, vp, u32, u32, u64, u32, vp], i32),
+        "gw_plain_choose_block": ([vp, u32, vp, u32, u32, u32, vp], i32),
         "gw_device_free": ([vp], i32),
+        "gw_philox_rate": ([i32, u32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_float)], i32),
         "gw_memcpy": ([vp, vp, u64], i32),
         "gw_walk_noalloc": ([ctypes.POINTER(GwConfig), vp, vp, u32, u64, u64, vp, vp, vp, vp,
                              ctypes.POINTER(GwStats)], i32),

@@ -446,6 +446,12 @@ extern "C" int gw_cache_reset(gw_handle *h)
 
 extern "C" int gw_init_walkers(gw_handle *h, uint32_t algo, uint32_t wps, uint64_t seed)
 {
+    return gw_init_walker_range(h, algo, wps, seed, 0, ~0ull);
+}
+
+extern "C" int gw_init_walker_range(gw_handle *h, uint32_t algo, uint32_t wps, uint64_t seed, uint64_t first,
+                                    uint64_t count)
+{
     if (!h) return GW_ERR_ARG;
     if (h->nblocks == 0) return h->fail(GW_ERR_STATE, "set the graph meta first");
     if (algo > GW_SOSR) return h->fail(GW_ERR_ARG, "unknown algorithm %u", algo);
@@ -469,8 +475,13 @@ extern "C" int gw_init_walkers(gw_handle *h, uint32_t algo, uint32_t wps, uint64
     }
     if (n > 0xFFFFFFFFull) return h->fail(GW_ERR_ARG, "walker ids are 32-bit (wid_t); %llu walkers", (unsigned long long)n);
     if (n == 0) return h->fail(GW_ERR_ARG, "no walkers");
+    if (first < n && count == ~0ull) count = n - first;  // to the end of the population
+    if (first >= n || count == 0 || count > n - first)
+        return h->fail(GW_ERR_ARG, "walker range [%llu, +%llu) outside the %llu walkers", (unsigned long long)first,
+                       (unsigned long long)count, (unsigned long long)n);
     cudaSetDevice(h->cfg.device);
-    h->nwalkers = n;
+    h->nwalkers = count;
+    h->wid_first = (uint32_t)first;
     h->numwalks_eff = (uint32_t)n;
     int st = h->ensure_outputs();
     if (st) return st;
@@ -607,7 +618,9 @@ int gw_handle::run_incore(gw_stats *stats)
     for (uint32_t L = 0; L < index_nlvl; ++L) a.ix.lvl[L] = index_lvl[L];
     a.nverts = nverts;
     a.nwalkers = (uint32_t)nwalkers;
+    a.wid_base = wid_first;
     a.wid_stride = 1;
+    a.out_base = wid_first;
     a.paths = (cfg.record_paths == GW_PATHS_FULL) ? d_paths : nullptr;
     a.stride = cfg.maxhops + 1;
     a.lens = d_lens;
@@ -639,7 +652,7 @@ int gw_handle::run_incore(gw_stats *stats)
         // gains from the caches the previous one warmed.
         const uint32_t stride = nwalkers > (1ull << 22) ? 16u : 1u;
         IncoreArgs c = a;
-        c.wid_base = 0;
+        c.wid_base = wid_first;
         c.wid_stride = stride;
         c.nwalkers = (uint32_t)(nwalkers / stride);
         float best = 1e30f;

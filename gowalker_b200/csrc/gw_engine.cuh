@@ -56,8 +56,9 @@ struct gw_handle {
     bool alias_ready = false;
 
     // walker population
-    uint64_t nwalkers = 0;
-    uint32_t numwalks_eff = 0;
+    uint64_t nwalkers = 0;      // walkers of the population: ids wid_first .. wid_first + nwalkers - 1
+    uint32_t wid_first = 0;     // first walker id (a shard of the whole population)
+    uint32_t numwalks_eff = 0;  // walkers of the whole population (SOSR's single-source split uses it)
     bool walkers_ready = false;
     bool ooc_walkers_stale = true;
 

@@ -72,6 +72,7 @@ struct IncoreArgs {
     uint32_t nwalkers;         // walkers of this launch: ids wid_base + i * wid_stride, i < nwalkers
     uint32_t wid_base;
     uint32_t wid_stride;       // 1 for a run; > 1 for the autotuner's sample
+    uint32_t out_base;         // first walker id of the population: outputs are indexed by wid - out_base
     uint32_t *paths;           // rows indexed by walker id, or null
     uint32_t stride;           // maxhops + 1
     uint32_t *lens;            // vertices per path

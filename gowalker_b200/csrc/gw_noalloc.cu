@@ -29,7 +29,33 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
-void *g_scratch_addr[kMaxDevices];  // device address of g_noalloc_scratch, looked up once per device
+// Device address of g_noalloc_scratch per device, and the CUDA context it was
+// looked up in: a cudaDeviceReset in the host process ends that context and
+// the module is loaded again (at a new address, maybe) in the next one, so an
+// address is reused only while the device's context is the same.
+void *g_scratch_addr[kMaxDevices];
+void *g_scratch_ctx[kMaxDevices];
+typedef int (*CtxGetCurrentFn)(void **);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+
+// The current context of the calling thread (the device's primary context
+// once the runtime has used that device), from the driver entry point the
+// runtime hands out, so the library links no driver library of its own.
+void *current_context()
+{
+    if (!g_ctx_get_current) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        g_ctx_get_current = (CtxGetCurrentFn)fn;
+    }
+    void *ctx = nullptr;
+    return g_ctx_get_current(&ctx) == 0 ? ctx : nullptr;
+}
 
 // The array's name is a host-side stand-in in host code; its device address
 // comes from cudaGetSymbolAddress, with the device current.
@@ -37,17 +63,37 @@ int scratch_address(int device, void **out)
 {
     if (device < 0 || device >= kMaxDevices) return GW_ERR_ARG;
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[device]) {
+    void *ctx = current_context();
+    if (!g_scratch_addr[device] || !ctx || ctx != g_scratch_ctx[device]) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
             cudaGetLastError();
             return GW_ERR_CUDA;
         }
         g_scratch_addr[device] = p;
+        g_scratch_ctx[device] = current_context();
     }
     *out = g_scratch_addr[device];
     return GW_OK;
 }
+
+// Restores the calling thread's current device on every return path: the
+// callers this entry point serves (plugins, pool-owning hosts) keep their own
+// device selection.
+struct DeviceGuard {
+    int saved = -1;
+    DeviceGuard()
+    {
+        if (cudaGetDevice(&saved) != cudaSuccess) {
+            cudaGetLastError();
+            saved = -1;
+        }
+    }
+    ~DeviceGuard()
+    {
+        if (saved >= 0) cudaSetDevice(saved);
+    }
+};
 
 }  // namespace
 
@@ -75,6 +121,7 @@ extern "C" int gw_walk_noalloc(const gw_config *cfg, const uint64_t *d_beg, cons
     // walker ids are 32-bit (wid_t): larger populations are refused
     if (implied != nwalkers || nwalkers == 0 || nwalkers > 0xFFFFFFFFull) return GW_ERR_ARG;
 
+    DeviceGuard keep_device;
     if (cudaSetDevice(cfg->device) != cudaSuccess) {
         cudaGetLastError();
         return GW_ERR_CUDA;
@@ -95,6 +142,10 @@ extern "C" int gw_walk_noalloc(const gw_config *cfg, const uint64_t *d_beg, cons
     unsigned long long host_ctr[kCtrCount + 1];
     uint64_t ends[2] = {1, 0};
     cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(unsigned long long) * kScratchWords, s);
+    // path rows end with zeros past each walk's length, as gw_get_paths
+    // returns them (the kernel writes only the visited entries)
+    if (e == cudaSuccess && cfg->record_paths == GW_PATHS_FULL)
+        e = cudaMemsetAsync(d_paths, 0, nwalkers * ((uint64_t)cfg->maxhops + 1) * sizeof(uint32_t), s);
     if (e == cudaSuccess) e = launch_validate_csr(d_beg, d_csr, nverts, nedges, err, num_sms, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(host_ctr, ctr, sizeof(host_ctr), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&ends[0], d_beg, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);

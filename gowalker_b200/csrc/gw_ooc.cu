@@ -86,6 +86,15 @@ struct OocState {
     bool learned_ready = false, trained = false;
     float *h_loss = nullptr;  // pinned: the last training's loss, read back without blocking the host
     float *d_params = nullptr, *d_train_ws = nullptr;
+    // Training runs on a stream of its own into a second copy of the weights
+    // (d_params_train), from a snapshot of the trace window; the decisions
+    // keep using d_params until a training has finished, when its weights are
+    // copied over.  No decision ever waits for a training.
+    float *d_params_train = nullptr;
+    cudaStream_t ts = nullptr;
+    cudaEvent_t ev_gathered = nullptr, ev_trained = nullptr;
+    cudaGraphExec_t retrain_graph = nullptr;  // kRetrainEpochs of warm training + the loss read-back
+    bool train_inflight = false;
     float *d_trace_x = nullptr, *d_trace_col = nullptr, *d_trace_y = nullptr;
     float *d_train_x = nullptr, *d_pred = nullptr, *d_pred_res = nullptr;  // forecast log demand, its change
     float *d_emass = nullptr, *d_vfrac = nullptr, *d_prev_col = nullptr, *d_ema = nullptr;
@@ -169,7 +178,14 @@ void gw_handle::ooc_release()
         if (p) cudaFreeHost((void *)p);
     if (o.h_loss) cudaFreeHost(o.h_loss);
     o.h_loss = nullptr;
-    for (float *p : {o.d_params, o.d_pred_res, o.d_train_ws, o.d_trace_x, o.d_trace_col, o.d_trace_y, o.d_train_x,
+    if (o.ts) {
+        cudaStreamSynchronize(o.ts);
+        cudaStreamDestroy(o.ts);
+    }
+    if (o.ev_gathered) cudaEventDestroy(o.ev_gathered);
+    if (o.ev_trained) cudaEventDestroy(o.ev_trained);
+    if (o.retrain_graph) cudaGraphExecDestroy(o.retrain_graph);
+    for (float *p : {o.d_params, o.d_params_train, o.d_pred_res, o.d_train_ws, o.d_trace_x, o.d_trace_col, o.d_trace_y, o.d_train_x,
                      o.d_pred, o.d_emass, o.d_vfrac, o.d_prev_col, o.d_ema})
         cudaFree(p);
     if (o.h_pred) cudaFreeHost(o.h_pred);
@@ -186,6 +202,10 @@ static int learned_setup(gw_handle *h)
     int st;
     auto dalloc = [&](float **p, uint64_t n, const char *what) { return h->cuda(cudaMalloc(p, n * sizeof(float)), what); };
     if ((st = dalloc(&o.d_params, kMlpParams, "predictor weights"))) return st;
+    if ((st = dalloc(&o.d_params_train, kMlpParams, "predictor weights"))) return st;
+    if ((st = h->cuda(cudaStreamCreateWithFlags(&o.ts, cudaStreamNonBlocking), "training stream"))) return st;
+    if ((st = h->cuda(cudaEventCreateWithFlags(&o.ev_gathered, cudaEventDisableTiming), "event"))) return st;
+    if ((st = h->cuda(cudaEventCreateWithFlags(&o.ev_trained, cudaEventDisableTiming), "event"))) return st;
     if ((st = h->cuda(cudaMallocHost((void **)&o.h_loss, sizeof(float)), "training loss"))) return st;
     *o.h_loss = 0.f;
     if ((st = dalloc(&o.d_train_ws, (uint64_t)kMlpGradCtas * (kMlpParams + 1) + 3 * kMlpParams + 1, "training state")))
@@ -562,9 +582,8 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     in.key1 = (uint32_t)(cfg.seed >> 32);
     const uint32_t stride = cfg.maxhops + 1;
     o.w_cur = 0;
-    if ((st = cuda(launch_init_walkers(in, o.d_vstart, nb, nwalkers, o.w_rec, o.w_ord[0], o.w_key[0], paths ? d_paths : nullptr,
-                                       stride, num_sms,
-                                       s),
+    if ((st = cuda(launch_init_walkers(in, o.d_vstart, nb, wid_first, nwalkers, o.w_rec, o.w_ord[0], o.w_key[0],
+                                       paths ? d_paths : nullptr, stride, num_sms, s),
                    "init walkers")))
         return st;
     launches++;
@@ -639,6 +658,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     a.nrun = o.d_nrun;
     a.paths = paths ? d_paths : nullptr;
     a.stride = stride;
+    a.out_base = wid_first;
     a.lens = d_lens;
     a.hashes = d_hashes;
     a.ctr = d_ctr;
@@ -698,7 +718,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         rring.destroy();
         return st;
     }
-    uint32_t trace_t = 0, learned_iters = 0;
+    uint32_t trace_t = 0, learned_iters = 0, next_train = 0;
+    const float *loss_dev = o.d_train_ws ? o.d_train_ws + (uint64_t)kMlpGradCtas * (kMlpParams + 1) + 3 * kMlpParams
+                                         : nullptr;
     bool stall_next = false;  // a learned choice moved no walker: the next decision is the plain rule's
     bool reverted = false;
     uint64_t learned_steps = 0, learned_bytes = 0, plain_steps = 0, plain_bytes = 0;
@@ -782,6 +804,24 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         // queue behind the block copy in flight.
         // ---- learned policy: features (traces while training), prediction, choice
         const bool learned = policy == GW_POLICY_LEARNED;
+        // a training that has finished (host-side query: never a wait) hands
+        // its weights to the decisions from this iteration on
+        if (learned && o.train_inflight) {
+            const cudaError_t q = cudaEventQuery(o.ev_trained);
+            if (q == cudaSuccess) {
+                if ((st = cuda(cudaMemcpyAsync(o.d_params, o.d_params_train, sizeof(float) * kMlpParams,
+                                               cudaMemcpyDeviceToDevice, ds),
+                               "predictor weights")))
+                    break;
+                o.train_inflight = false;
+                o.trained = true;
+            } else if (q != cudaErrorNotReady) {
+                st = cuda(q, "predictor training");
+                break;
+            } else {
+                cudaGetLastError();
+            }
+        }
         const bool learned_active = learned && o.trained && !reverted;
         // once trained the predictor keeps predicting (its error is measured)
         // even after its judge has handed the choice back to the plain rule
@@ -1045,27 +1085,54 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
 
         // ---- predictor training: once kTraceRing iterations are traced, and
         // again (warm, fewer epochs) every kRetrain iterations on the sliding
-        // window of the last kTraceIters iterations whose horizon is observed
+        // window of the last kTraceIters iterations whose horizon is observed.
+        // The window is copied out of the trace ring on the decision stream;
+        // the training runs on its own stream and is adopted when done.
         if (tracing) {
             trace_t++;
-            if (trace_t >= kTraceRing && (trace_t - kTraceRing) % kRetrain == 0) {
-                if ((st = cuda(cudaStreamWaitEvent(ds, ev_buck, 0), "training wait"))) break;
+            if (trace_t >= kTraceRing && trace_t >= next_train && !o.train_inflight) {
                 if ((st = cuda(launch_gather_train(o.d_trace_x, o.d_trace_col, trace_t - kTraceRing, kTraceRing,
                                                    kTraceIters, kHorizon, nb, o.d_train_x, o.d_trace_y, ds),
                                "training set")))
                     break;
-                const bool first = !o.trained;
-                if ((st = cuda(mlp_train(o.d_params, o.d_train_x, o.d_trace_y, kTraceIters * nb,
-                                         first ? kTrainEpochs : kRetrainEpochs, kTrainLr,
-                                         first ? 0x6C6561726E6564ull : 0ull, o.d_train_ws, nullptr, ds),
-                               "predictor training")))
+                if ((st = cuda(cudaEventRecord(o.ev_gathered, ds), "event")) ||
+                    (st = cuda(cudaStreamWaitEvent(o.ts, o.ev_gathered, 0), "training wait")))
                     break;
-                const float *loss_dev = o.d_train_ws + (uint64_t)kMlpGradCtas * (kMlpParams + 1) + 3 * kMlpParams;
-                if ((st = cuda(cudaMemcpyAsync(o.h_loss, loss_dev, sizeof(float), cudaMemcpyDeviceToHost, ds),
-                               "loss")))
-                    break;
-                launches += 1 + 3 * (first ? kTrainEpochs : kRetrainEpochs);
-                o.trained = true;
+                launches++;
+                if (!o.trained) {
+                    // first training: from a fresh initialisation, on the stream
+                    if ((st = cuda(mlp_train(o.d_params_train, o.d_train_x, o.d_trace_y, kTraceIters * nb,
+                                             kTrainEpochs, kTrainLr, 0x6C6561726E6564ull, o.d_train_ws, nullptr, o.ts),
+                                   "predictor training")) ||
+                        (st = cuda(cudaMemcpyAsync(o.h_loss, loss_dev, sizeof(float), cudaMemcpyDeviceToHost, o.ts),
+                                   "loss")))
+                        break;
+                    launches += 1 + 3 * kTrainEpochs;
+                } else {
+                    // warm retraining of the weights in use: one graph launch
+                    if (!o.retrain_graph) {
+                        cudaGraph_t g = nullptr;
+                        if ((st = cuda(cudaStreamBeginCapture(o.ts, cudaStreamCaptureModeThreadLocal), "capture")))
+                            break;
+                        cudaError_t e1 = mlp_train(o.d_params_train, o.d_train_x, o.d_trace_y, kTraceIters * nb,
+                                                   kRetrainEpochs, kTrainLr, 0ull, o.d_train_ws, nullptr, o.ts);
+                        if (e1 == cudaSuccess)
+                            e1 = cudaMemcpyAsync(o.h_loss, loss_dev, sizeof(float), cudaMemcpyDeviceToHost, o.ts);
+                        const cudaError_t e2 = cudaStreamEndCapture(o.ts, &g);
+                        if ((st = cuda(e1 != cudaSuccess ? e1 : e2, "training capture"))) {
+                            if (g) cudaGraphDestroy(g);
+                            break;
+                        }
+                        st = cuda(cudaGraphInstantiate(&o.retrain_graph, g, 0), "graph instantiate");
+                        cudaGraphDestroy(g);
+                        if (st) break;
+                    }
+                    if ((st = cuda(cudaGraphLaunch(o.retrain_graph, o.ts), "predictor training"))) break;
+                    launches += 3 * kRetrainEpochs;
+                }
+                if ((st = cuda(cudaEventRecord(o.ev_trained, o.ts), "event"))) break;
+                o.train_inflight = true;
+                next_train = trace_t + kRetrain;
             }
         }
     }
@@ -1087,6 +1154,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         cudaStreamSynchronize(ds);
         cudaStreamDestroy(ds);
     }
+    // a training still in flight finishes here; its weights are adopted by
+    // the next run's first decision
+    if (o.ts) cudaStreamSynchronize(o.ts);
     for (auto &g : bgraph)
         if (g) cudaGraphExecDestroy(g);
     cudaEventDestroy(ev_buck);
@@ -1153,4 +1223,48 @@ extern "C" int gw_bucket_counts(gw_handle *h, uint32_t *out)
     cudaSetDevice(h->cfg.device);
     const uint64_t npairs = (uint64_t)h->ooc->nb * h->ooc->nb;
     return h->cuda(cudaMemcpy(out, h->ooc->d_pairs, npairs * sizeof(uint32_t), cudaMemcpyDeviceToHost), "bucket counts");
+}
+
+extern "C" int gw_plain_choose_block(const uint32_t *counts, uint32_t nblocks, const uint32_t *cached,
+                                     uint32_t ncached, uint32_t nslots, uint32_t zero_threshold, int32_t *out)
+{
+    if (!counts || !out || (ncached && !cached) || nblocks == 0 || nblocks > kMaxBlocks || ncached > nblocks ||
+        nslots == 0)
+        return GW_ERR_ARG;
+    std::vector<uint8_t> seen(nblocks, 0);
+    for (uint32_t j = 0; j < ncached; ++j) {
+        if (cached[j] >= nblocks || seen[cached[j]]) return GW_ERR_ARG;
+        seen[cached[j]] = 1;
+    }
+    const uint64_t nn = (uint64_t)nblocks * nblocks;
+    uint32_t *d_counts = nullptr, *d_cached = nullptr, *d_live = nullptr;
+    Decision *d_dec = nullptr;
+    Decision h{};
+    int rc = GW_OK;
+    do {
+        if (cudaMalloc(&d_counts, nn * sizeof(uint32_t)) != cudaSuccess ||
+            cudaMalloc(&d_cached, (ncached ? ncached : 1) * sizeof(uint32_t)) != cudaSuccess ||
+            cudaMalloc(&d_live, sizeof(uint32_t)) != cudaSuccess || cudaMalloc(&d_dec, sizeof(Decision)) != cudaSuccess) {
+            rc = GW_ERR_NOMEM;
+            break;
+        }
+        if (cudaMemcpy(d_counts, counts, nn * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+            (ncached && cudaMemcpy(d_cached, cached, ncached * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess) ||
+            cudaMemset(d_live, 0, sizeof(uint32_t)) != cudaSuccess ||
+            launch_schedule(d_counts, d_live, nblocks, d_cached, ncached, nslots, zero_threshold, nullptr, 1.f, d_dec,
+                            0) != cudaSuccess ||
+            cudaMemcpy(&h, d_dec, sizeof(Decision), cudaMemcpyDeviceToHost) != cudaSuccess) {
+            rc = GW_ERR_CUDA;
+            break;
+        }
+        out[0] = h.action;
+        out[1] = h.block;
+        out[2] = h.position;
+    } while (0);
+    if (rc != GW_OK) cudaGetLastError();
+    cudaFree(d_counts);
+    cudaFree(d_cached);
+    cudaFree(d_live);
+    cudaFree(d_dec);
+    return rc;
 }

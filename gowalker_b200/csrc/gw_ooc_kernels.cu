@@ -38,16 +38,16 @@ __device__ __forceinline__ uint32_t bucket_of(const WalkerRec &r, uint32_t nb)
     return ((r.cur_blk & kNeedPrev) ? nb * nb : 0u) + r.prev_blk * nb + (r.cur_blk & ~kNeedPrev);
 }
 
-__global__ void k_init_walkers(WalkerInit in, const uint32_t *__restrict__ vstart, uint32_t nb, uint64_t n,
-                               WalkerRec *__restrict__ out, uint32_t *__restrict__ order, uint32_t *__restrict__ keys,
-                               uint32_t *__restrict__ paths, uint32_t stride)
+__global__ void k_init_walkers(WalkerInit in, const uint32_t *__restrict__ vstart, uint32_t nb, uint32_t wid0,
+                               uint64_t n, WalkerRec *__restrict__ out, uint32_t *__restrict__ order,
+                               uint32_t *__restrict__ keys, uint32_t *__restrict__ paths, uint32_t stride)
 {
     __shared__ uint32_t s_vs[kMaxBlocks + 1];
     for (uint32_t i = threadIdx.x; i <= nb; i += blockDim.x) s_vs[i] = vstart[i];
     __syncthreads();
     const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += step) {
-        const uint32_t wid = (uint32_t)i;
+        const uint32_t wid = wid0 + (uint32_t)i;
         const uint32_t src = walker_source(in, wid);
         const uint32_t b = block_of(s_vs, nb, src);
         const uint64_t h = hash_init(src);
@@ -63,7 +63,7 @@ __global__ void k_init_walkers(WalkerInit in, const uint32_t *__restrict__ vstar
         out[i] = r;
         order[i] = (uint32_t)i;
         keys[i] = bucket_of(r, nb);
-        if (paths) paths[(uint64_t)wid * stride] = src;
+        if (paths) paths[i * stride] = src;
     }
 }
 
@@ -396,8 +396,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
         n_trials = 0;
     };
     auto finish = [&]() {
-        a.hashes[wid] = h;
-        a.lens[wid] = hop + 1;
+        a.hashes[wid - a.out_base] = h;
+        a.lens[wid - a.out_base] = hop + 1;
         a.keys[idx] = kNoBucket;
         atomicAdd(&s_ws[warp][kWsHash], (unsigned long long)h);
         atomicAdd(&s_ws[warp][kWsDone], 1ull);
@@ -534,7 +534,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
         } else if (verdict > 0) {
             hop++;
             h = hash_step(h, x);
-            if (PATHS) a.paths[(uint64_t)wid * a.stride + hop] = x;
+            if (PATHS) a.paths[(uint64_t)(wid - a.out_base) * a.stride + hop] = x;
             if (n_trials & 0x80000000u) {  // a step adds < 2^27: no wrap
                 atomicAdd(&s_ws[warp][kWsTrials], (unsigned long long)n_trials);
                 n_trials = 0;
@@ -691,11 +691,11 @@ cudaError_t launch_add_level(const float *res, const float *x, float *level, uin
 
 // ------------------------------------------------------------------ launchers
 
-cudaError_t launch_init_walkers(const WalkerInit &in, const uint32_t *vstart, uint32_t nb, uint64_t n,
+cudaError_t launch_init_walkers(const WalkerInit &in, const uint32_t *vstart, uint32_t nb, uint32_t wid0, uint64_t n,
                                 WalkerRec *recs, uint32_t *order, uint32_t *keys, uint32_t *paths, uint32_t stride,
                                 int num_sms, cudaStream_t s)
 {
-    k_init_walkers<<<num_sms * 8, 256, 0, s>>>(in, vstart, nb, n, recs, order, keys, paths, stride);
+    k_init_walkers<<<num_sms * 8, 256, 0, s>>>(in, vstart, nb, wid0, n, recs, order, keys, paths, stride);
     return cudaGetLastError();
 }
 

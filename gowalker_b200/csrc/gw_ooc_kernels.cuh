@@ -40,6 +40,7 @@ struct OocStepArgs {
     const uint32_t *nrun;            // runnable bucket count (device)
     uint32_t *paths;                 // or null
     uint32_t stride;
+    uint32_t out_base;               // first walker id of the population: outputs at wid - out_base
     uint32_t *lens;
     uint64_t *hashes;
     unsigned long long *ctr;
@@ -60,7 +61,7 @@ struct Decision {
 // Walkers are sorted by bucket through an index: records stay where
 // k_init_walkers puts them; `order` and `keys` (record index and bucket of
 // each sorted position) are what bucketing moves, 8 bytes per walker.
-cudaError_t launch_init_walkers(const WalkerInit &in, const uint32_t *vstart, uint32_t nb, uint64_t n,
+cudaError_t launch_init_walkers(const WalkerInit &in, const uint32_t *vstart, uint32_t nb, uint32_t wid0, uint64_t n,
                                 WalkerRec *recs, uint32_t *order, uint32_t *keys, uint32_t *paths, uint32_t stride,
                                 int num_sms, cudaStream_t s);
 // `n` points at the number of sorted positions (a device word, so the

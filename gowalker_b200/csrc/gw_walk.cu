@@ -64,8 +64,8 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const __grid
     };
     // A walker's steps are its hops: every accepted trial moves it one hop.
     auto finish = [&]() {
-        a.hashes[wid] = h;
-        a.lens[wid] = hop + 1;
+        a.hashes[wid - a.out_base] = h;
+        a.lens[wid - a.out_base] = hop + 1;
         atomicAdd(&s_ws[warp][kWsSteps], (unsigned long long)hop);
         atomicAdd(&s_ws[warp][kWsDone], 1ull);
         atomicAdd(&s_ws[warp][kWsHash], (unsigned long long)h);
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const __grid
                 prev = cur = src;
                 hop = 0;
                 h = hash_init(src);
-                if (PATHS) a.paths[(uint64_t)wid * a.stride] = src;
+                if (PATHS) a.paths[(uint64_t)(wid - a.out_base) * a.stride] = src;
                 if (src >= a.nverts) {
                     atomicOr(a.err, kErrSource);
                     finish();
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const __grid
         if (accept_candidate<SOPR>(a.c, t, rv, x, prev, cur, a.ix, phead, pdeg)) {
             hop++;
             h = hash_step(h, x);
-            if (PATHS) a.paths[(uint64_t)wid * a.stride + hop] = x;
+            if (PATHS) a.paths[(uint64_t)(wid - a.out_base) * a.stride + hop] = x;
             if (n_trials & 0x80000000u) flush_trials();  // a step adds < 2^27: no wrap
             prev = cur;
             phead = head;

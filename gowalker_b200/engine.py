@@ -137,12 +137,18 @@ class WalkEngine:
         self._check(self.L.gw_cache_reset(self.h))
 
     # -- walks
-    def init_walkers(self, algo=None, walkpersource=None, seed=None):
+    def init_walkers(self, algo=None, walkpersource=None, seed=None, first=0, count=None):
+        """The whole walker population, or the shard of walker ids
+        [first, first+count) of it (gw_init_walker_range)."""
         algo = self.cfg.algorithm if algo is None else algo
         wps = self.cfg.walkpersource if walkpersource is None else walkpersource
         seed = self.cfg.seed if seed is None else seed
         self.cfg.algorithm, self.cfg.walkpersource, self.cfg.seed = algo, wps, seed
-        self._check(self.L.gw_init_walkers(self.h, algo, wps, seed))
+        if first == 0 and count is None:
+            self._check(self.L.gw_init_walkers(self.h, algo, wps, seed))
+        else:
+            self._check(self.L.gw_init_walker_range(self.h, algo, wps, seed, first,
+                                                    0xFFFFFFFFFFFFFFFF if count is None else count))
 
     def run(self, policy=_abi.GW_POLICY_PLAIN) -> dict:
         st = GwStats()
@@ -333,3 +339,21 @@ def sa_choose_blocks(counts, cached, k, seed=42, call=0):
     if st != 0:
         raise GwError(st, "gw_sa_choose_blocks failed")
     return out[: min(k, nb)]
+
+
+def plain_choose_block(counts, cached, nslots, zero_threshold=0):
+    """gw_plain_choose_block: GOWalker's block choice (max_choose_blocks,
+    engine/schedule.hpp:70-138) as the device takes it, from the nb x nb
+    (prev, cur) walker counts, the scheduler's cached list and the slot count.
+    Returns (action, block, position)."""
+    L = _abi.load()
+    counts = np.ascontiguousarray(counts, dtype=np.uint32)
+    nb = counts.shape[0]
+    cached = np.ascontiguousarray(cached, dtype=np.uint32)
+    out = np.zeros(3, dtype=np.int32)
+    st = L.gw_plain_choose_block(ctypes.c_void_p(counts.ctypes.data), nb,
+                                 ctypes.c_void_p(cached.ctypes.data if cached.size else 0), cached.size, nslots,
+                                 zero_threshold, ctypes.c_void_p(out.ctypes.data))
+    if st != 0:
+        raise GwError(st, "gw_plain_choose_block failed")
+    return int(out[0]), int(out[1]), int(out[2])

@@ -204,6 +204,17 @@ int gw_cache_reset(gw_handle *h);
  * walker population; walkers are generated on the device. */
 int gw_init_walkers(gw_handle *h, uint32_t algo, uint32_t walkpersource, uint64_t seed);
 
+/* One shard of that population: the walkers with ids [first, first+count)
+ * of the population gw_init_walkers would set (ids as the reference assigns
+ * them, engine/walk.hpp:32-49: v*walkpersource + i per vertex).  A walk
+ * depends only on its id and the seed, so shards of one population walked on
+ * different devices (or one after another) together give exactly the walks
+ * of the whole population.  Per-walker results (gw_get_paths,
+ * gw_path_hashes) are then indexed from the shard's first walker: row 0 is
+ * walker `first`.  gw_init_walkers is the shard [0, all). */
+int gw_init_walker_range(gw_handle *h, uint32_t algo, uint32_t walkpersource, uint64_t seed, uint64_t first,
+                         uint64_t count);
+
 /* Runs every walker to the end.  Replaces graph_engine::pipe_run
  * (engine/engine.hpp:517-638) with its pipeline / zero_gpujob launches
  * (406-515): the plain or learned block policy, device bucketing, and the
@@ -213,7 +224,8 @@ int gw_run(gw_handle *h, uint32_t policy, gw_stats *stats);
 /* Walker count of the current population. */
 int gw_num_walkers(gw_handle *h, uint64_t *n);
 
-/* Paths of walkers [first, first+n): out = n rows of maxhops+1 u32 (zero
+/* Paths of walkers [first, first+n) of the population (row 0 = its first
+ * walker; see gw_init_walker_range): out = n rows of maxhops+1 u32 (zero
  * padded), lens = vertices per row.  Needs record_paths = GW_PATHS_FULL. */
 int gw_get_paths(gw_handle *h, uint64_t first, uint64_t n, uint32_t *out, uint32_t *lens);
 
@@ -272,6 +284,21 @@ int gw_edges_csr(const uint32_t *src, const uint32_t *dst, uint64_t n, uint32_t 
  * blocks to out.  nblocks <= 1024. */
 int gw_sa_choose_blocks(const uint32_t *counts, uint32_t nblocks, const uint32_t *cached, uint32_t ncached,
                         uint32_t k, uint64_t seed, uint32_t call, uint32_t *out);
+
+/* GOWalker's block choice, GOwalker_scheduler_t::max_choose_blocks
+ * (engine/schedule.hpp:70-138), on the device, exactly as GW_POLICY_PLAIN
+ * takes it each iteration: counts = nblocks*nblocks walkers per (prev block,
+ * cur block) pair; cached = the scheduler's list of the ncached resident
+ * blocks in order (its `buckets`, distinct); nslots = cache slots
+ * (graph_cache::ncblock).  out[0] = action: 0 when no block scores above 0
+ * and zero_threshold (the reference returns false), 1 when block out[1] is
+ * appended to the list (out[2] = ncached), 2 when out[1] replaces the block
+ * at list position out[2].  Among equal best scores the lowest block id
+ * wins (the reference's std::sort leaves that order open; its insertion sort
+ * for at most 16 uncached blocks gives the same).  Host memory in and out;
+ * nblocks <= 1024. */
+int gw_plain_choose_block(const uint32_t *counts, uint32_t nblocks, const uint32_t *cached, uint32_t ncached,
+                          uint32_t nslots, uint32_t zero_threshold, int32_t *out);
 
 /* Block split points over CSR offsets beg[0..nverts] (host or device
  * memory), computed on the device.
@@ -354,8 +381,9 @@ int gw_mlp_train(float *d_params, const float *d_x, const float *d_t, uint32_t n
  * device) over a CSR already on the device (d_beg: nverts+1 u64 offsets,
  * d_csr: nedges u32 ids, sorted per vertex), writing the caller's buffers:
  * d_hashes (nwalkers u64), d_lens (nwalkers u32) and, when record_paths is
- * GW_PATHS_FULL, d_paths (nwalkers rows of maxhops+1 u32).  The walks are the
- * ones gw_run produces for the same configuration, bit for bit.
+ * GW_PATHS_FULL, d_paths (nwalkers rows of maxhops+1 u32, zero past each
+ * walk's length, as gw_get_paths returns them).  The walks are the ones
+ * gw_run produces for the same configuration, bit for bit.
  *
  * Allocates nothing: no cudaMalloc, no cudaFree, no allocating library call.
  * Its only other memory is a 256-byte array in the library (the run's work
@@ -367,7 +395,9 @@ int gw_mlp_train(float *d_params, const float *d_x, const float *d_t, uint32_t n
  * device.
  *
  * The first call on a device looks up the array's device address with that
- * device current; make that first call before any stream capture.  The call
+ * device current (again after the device's context changes, e.g. after a
+ * cudaDeviceReset); make that first call before any stream capture.  The
+ * calling thread's current device is the same on return as before.  The call
  * runs on `stream` (a cudaStream_t, 0 for the default stream) and returns
  * after the walk has finished; it first checks the CSR (GW_ERR_GRAPH if
  * offsets are not monotone or an id is out of range).  Every call shares the
@@ -376,6 +406,15 @@ int gw_mlp_train(float *d_params, const float *d_x, const float *d_t, uint32_t n
 int gw_walk_noalloc(const gw_config *cfg, const uint64_t *d_beg, const uint32_t *d_csr, uint32_t nverts,
                     uint64_t nedges, uint64_t nwalkers, uint64_t *d_hashes, uint32_t *d_lens, uint32_t *d_paths,
                     void *stream, gw_stats *stats);
+
+/* Issue rate of the walk's random draws on `device`: every thread evaluates
+ * the step kernels' keyed Philox4x32-10 (per_thread evaluations, nothing
+ * else), timed with CUDA events, best of three launches after a warm-up one.
+ * *evals_per_s is the bound on rejection trials per second of any kernel
+ * that draws once per trial; *ms (may be NULL) the best launch time.  No
+ * counterpart in the reference (a measurement for the roofline of
+ * trial-bound walks). */
+int gw_philox_rate(int device, uint32_t per_thread, double *evals_per_s, float *ms);
 
 /* Plain copy between any two host / device pointers (cudaMemcpyDefault),
  * synchronous: lets callers without their own CUDA runtime move the buffers

@@ -296,7 +296,7 @@ static uint32_t walk_from(const uint64_t *beg, const uint32_t *csr, const float 
                           const oracle_cfg *c, uint32_t wid, uint32_t *pprev, uint32_t *pcur, uint32_t *phop,
                           uint64_t *phash, uint32_t *path, oracle_stats *st,
                           oracle_trial *trace, uint64_t trace_cap, uint64_t *ntrace,
-                          uint64_t *trial_counter)
+                          uint64_t *trial_counter, uint8_t *needprev)
 {
     uint32_t prev = *pprev, cur = *pcur, hop = *phop;
     uint64_t h = *phash;
@@ -353,6 +353,7 @@ static uint32_t walk_from(const uint64_t *beg, const uint32_t *csr, const float 
         }
 
         uint32_t attempt = 0, x;
+        uint8_t np = 0; /* some trial of this step is decided only by x in N(prev) */
         for (;;) {
             if (c->keying == KEY_HOP_ATTEMPT)
                 draw4(c->seed, wid, hop, attempt, 0, r);
@@ -386,6 +387,7 @@ static uint32_t walk_from(const uint64_t *beg, const uint32_t *csr, const float 
                 continue;
             }
             int found;
+            if (prev != cur && ((rv < t_found) != (rv < t_notfound))) np = 1;
             if (prev == cur)
                 found = 1; /* x is drawn from N(cur) = N(prev): the search must succeed */
             else
@@ -398,6 +400,7 @@ static uint32_t walk_from(const uint64_t *beg, const uint32_t *csr, const float 
         hop++;
         h = (h ^ (uint64_t)x) * FNV_PRIME;
         if (path) path[moves] = x;
+        if (needprev) needprev[moves] = np;
         moves++;
         st->steps++;
     }
@@ -419,13 +422,18 @@ uint64_t oracle_hash_init(uint32_t source)
  *   hashes: count u64 (FNV-1a over the path's 32-bit vertices) or NULL
  *   finals: count x 3 u32 (prev, cur, hop) after the walk, or NULL */
 static int walk_many(const uint64_t *beg, const uint32_t *csr, const float *aprob, const uint32_t *aalias,
-                     uint32_t nverts, const oracle_cfg *c, uint32_t wid_begin, uint32_t count, uint32_t *paths,
-                     uint32_t *lens, uint64_t *hashes, uint32_t *finals, oracle_stats *stats, int nthreads)
+                     uint32_t nverts, const oracle_cfg *c, uint32_t wid_begin, const uint32_t *ids, uint32_t count,
+                     uint32_t *paths, uint32_t *lens, uint64_t *hashes, uint32_t *finals, oracle_stats *stats,
+                     int nthreads)
 {
     if (c->algo > ALG_SOSR || c->maxhops == 0) return -1;
     if (c->init_mode == INIT_PER_VERTEX && c->wps == 0) return -1;
     /* every source must be a vertex */
-    if (c->init_mode == INIT_PER_VERTEX && (uint64_t)wid_begin + count > (uint64_t)nverts * c->wps) return -1;
+    if (c->init_mode == INIT_PER_VERTEX && !ids && (uint64_t)wid_begin + count > (uint64_t)nverts * c->wps)
+        return -1;
+    if (c->init_mode == INIT_PER_VERTEX && ids)
+        for (uint32_t i = 0; i < count; ++i)
+            if ((uint64_t)ids[i] >= (uint64_t)nverts * c->wps) return -1;
     if (c->init_mode == INIT_SINGLE_SOURCE && nverts <= (c->algo == ALG_SOSR ? 3u : 1u)) return -1;
     if (nverts == 0) return -1;
     memset(stats, 0, sizeof(*stats));
@@ -437,7 +445,7 @@ static int walk_many(const uint64_t *beg, const uint32_t *csr, const float *apro
         memset(&st, 0, sizeof(st));
 #pragma omp for schedule(dynamic, 1024)
         for (int64_t i = 0; i < (int64_t)count; ++i) {
-            uint32_t wid = wid_begin + (uint32_t)i;
+            uint32_t wid = ids ? ids[i] : wid_begin + (uint32_t)i;
             uint32_t src = oracle_walker_source(c, nverts, wid);
             uint32_t prev = src, cur = src, hop = 0;
             uint64_t h = oracle_hash_init(src);
@@ -445,7 +453,7 @@ static int walk_many(const uint64_t *beg, const uint32_t *csr, const float *apro
             uint32_t *path = paths ? paths + (uint64_t)i * stride : NULL;
             if (path) path[0] = src;
             uint32_t moves = walk_from(beg, csr, aprob, aalias, c, wid, &prev, &cur, &hop, &h,
-                                       path ? path + 1 : NULL, &st, NULL, 0, NULL, &tc);
+                                       path ? path + 1 : NULL, &st, NULL, 0, NULL, &tc, NULL);
             if (lens) lens[i] = moves + 1;
             if (hashes) hashes[i] = h;
             if (finals) {
@@ -472,8 +480,17 @@ int oracle_walk(const uint64_t *beg, const uint32_t *csr, uint32_t nverts, const
                 uint32_t wid_begin, uint32_t count, uint32_t *paths, uint32_t *lens,
                 uint64_t *hashes, uint32_t *finals, oracle_stats *stats, int nthreads)
 {
-    return walk_many(beg, csr, NULL, NULL, nverts, c, wid_begin, count, paths, lens, hashes, finals, stats,
+    return walk_many(beg, csr, NULL, NULL, nverts, c, wid_begin, NULL, count, paths, lens, hashes, finals, stats,
                      nthreads);
+}
+
+/* The walkers whose ids are listed (any order, repeats allowed): row i of
+ * the outputs is walker ids[i]. */
+int oracle_walk_ids(const uint64_t *beg, const uint32_t *csr, uint32_t nverts, const oracle_cfg *c,
+                    const uint32_t *ids, uint32_t count, uint32_t *paths, uint32_t *lens, uint64_t *hashes,
+                    oracle_stats *stats, int nthreads)
+{
+    return walk_many(beg, csr, NULL, NULL, nverts, c, 0, ids, count, paths, lens, hashes, NULL, stats, nthreads);
 }
 
 /* Weighted Node2vec (the device's gw_weighted.cu): candidates by the alias
@@ -483,7 +500,7 @@ int oracle_walk_weighted(const uint64_t *beg, const uint32_t *csr, const float *
                          uint32_t *lens, uint64_t *hashes, uint32_t *finals, oracle_stats *stats, int nthreads)
 {
     if (c->algo != ALG_NODE2VEC) return -1;
-    return walk_many(beg, csr, aprob, aalias, nverts, c, wid_begin, count, paths, lens, hashes, finals, stats,
+    return walk_many(beg, csr, aprob, aalias, nverts, c, wid_begin, NULL, count, paths, lens, hashes, finals, stats,
                      nthreads);
 }
 
@@ -560,11 +577,309 @@ uint32_t oracle_walk_traced(const uint64_t *beg, const uint32_t *csr, const orac
     uint64_t h = 0, tc = 0;
     *ntrace = 0;
     uint32_t moves = walk_from(beg, csr, NULL, NULL, c, wid, &prev, &cur, &hop, &h, path, &st, trace, trace_cap,
-                               ntrace, &tc);
+                               ntrace, &tc, NULL);
     if (final3) {
         final3[0] = prev;
         final3[1] = cur;
         final3[2] = hop;
     }
     return moves;
+}
+
+
+/* ------------------------------------------------------------------ out-of-core schedule emulation
+ *
+ * A walk does not depend on the block schedule, so the blocks each walker
+ * will need, in order, are fixed in advance.  oracle_walk_reqs writes them
+ * per walker as u16 entries, one per "enter" (the engine's step set-up at the
+ * walker's current vertex):
+ *   bits 0-13  block of the current vertex
+ *   bit 14     terminal: the walk ends at this enter (dead end, or the
+ *              termination draw) -- it still needs the block resident
+ *   bit 15     the step taken from here has a trial decided only by whether
+ *              the candidate is in N(prev) (the lazy residency rule then
+ *              needs the previous block resident too)
+ * A walk that reaches maxhops has no terminal entry.  reqs is count x
+ * (maxhops+1) u16, nent[i] the entries of walker wid_begin+i. */
+int oracle_walk_reqs(const uint64_t *beg, const uint32_t *csr, uint32_t nverts, const oracle_cfg *c,
+                     const uint32_t *vstart, uint32_t nb, uint32_t wid_begin, uint32_t count, uint16_t *reqs,
+                     uint32_t *nent, int nthreads)
+{
+    if (c->algo > ALG_SOSR || c->maxhops == 0 || nb == 0 || nb > 1024 || nverts == 0) return -1;
+    if (c->init_mode == INIT_PER_VERTEX && (c->wps == 0 || (uint64_t)wid_begin + count > (uint64_t)nverts * c->wps))
+        return -1;
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    const uint64_t stride = (uint64_t)c->maxhops + 1;
+    int bad = 0;
+#pragma omp parallel reduction(| : bad)
+    {
+        oracle_stats st;
+        memset(&st, 0, sizeof(st));
+        uint32_t *path = (uint32_t *)malloc(sizeof(uint32_t) * c->maxhops);
+        uint8_t *np = (uint8_t *)malloc(c->maxhops);
+#pragma omp for schedule(dynamic, 1024)
+        for (int64_t i = 0; i < (int64_t)count; ++i) {
+            const uint32_t wid = wid_begin + (uint32_t)i;
+            const uint32_t src = oracle_walker_source(c, nverts, wid);
+            uint32_t prev = src, cur = src, hop = 0;
+            uint64_t h = oracle_hash_init(src), tc = 0;
+            const uint32_t moves = walk_from(beg, csr, NULL, NULL, c, wid, &prev, &cur, &hop, &h, path, &st, NULL, 0,
+                                             NULL, &tc, np);
+            uint16_t *r = reqs + (uint64_t)i * stride;
+            for (uint32_t e = 0; e <= moves && e < c->maxhops; ++e) {
+                const uint32_t v = e ? path[e - 1] : src;
+                /* block of v: the last block starting at or before it */
+                uint32_t lo = 0, hi = nb;
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (vstart[mid] <= v) lo = mid;
+                    else hi = mid;
+                }
+                if (v >= vstart[nb]) bad = 1;
+                uint16_t ent = (uint16_t)lo;
+                if (e < moves) {
+                    if (np[e]) ent |= 0x8000u;
+                } else {
+                    ent |= 0x4000u; /* moves < maxhops: the walk ends at this enter */
+                }
+                r[e] = ent;
+            }
+            nent[i] = moves + (moves < c->maxhops ? 1u : 0u);
+        }
+        free(path);
+        free(np);
+    }
+    return bad ? -1 : 0;
+}
+
+typedef struct {
+    uint64_t iterations, loads, steps, parks, rescues;
+    uint64_t finished;
+} oracle_sched_stats;
+
+/* Plain block choice, GOwalker_scheduler_t::max_choose_blocks
+ * (engine/schedule.hpp:70-138), with the engine's rescue when nothing
+ * qualifies: *action 1 append, 2 replace cached[*pos], 0 none (then *rblk /
+ * *rpos give the rescue: the fullest bucket with an absent block, its current
+ * block first, evicting the cached block with the fewest incident walkers
+ * outside that bucket).  Ties: lowest block id, first position. */
+static void plain_choice(const uint64_t *pairs, uint32_t nb, const uint32_t *cached, uint32_t ncached,
+                         uint32_t nslots, uint64_t zero_threshold, int *action, int *blk, int *pos, int *rblk,
+                         int *rpos)
+{
+    uint8_t isc[1024];
+    memset(isc, 0, nb);
+    for (uint32_t j = 0; j < ncached; ++j) isc[cached[j]] = 1;
+    const int full = ncached >= nslots;
+    int64_t best = -1;
+    int bi = -1, bp = -1;
+    for (uint32_t i = 0; i < nb; ++i) {
+        if (isc[i]) continue;
+        uint64_t score = 0;
+        int p = (int)ncached;
+        if (!full) {
+            for (uint32_t j = 0; j < ncached; ++j) score += pairs[(uint64_t)i * nb + cached[j]] + pairs[(uint64_t)cached[j] * nb + i];
+            score += pairs[(uint64_t)i * nb + i];
+        } else {
+            uint64_t all = 0, mn = 0xFFFFFFFFull;
+            p = 0;
+            for (uint32_t j = 0; j < ncached; ++j) {
+                const uint64_t v = pairs[(uint64_t)i * nb + cached[j]] + pairs[(uint64_t)cached[j] * nb + i];
+                all += v;
+                if (v < mn) {
+                    mn = v;
+                    p = (int)j;
+                }
+            }
+            score = all - mn;
+        }
+        if ((int64_t)score > best) {
+            best = (int64_t)score;
+            bi = (int)i;
+            bp = p;
+        }
+    }
+    if (bi >= 0 && best > 0 && (uint64_t)best > zero_threshold) {
+        *action = full ? 2 : 1;
+        *blk = bi;
+        *pos = bp;
+    } else {
+        *action = 0;
+        *blk = *pos = -1;
+    }
+    *rblk = *rpos = -1;
+    uint64_t bc = 0;
+    int64_t bb = -1;
+    for (uint64_t b = 0; b < (uint64_t)nb * nb; ++b)
+        if (pairs[b] > bc && !(isc[b / nb] && isc[b % nb])) {
+            bc = pairs[b];
+            bb = (int64_t)b;
+        }
+    if (bb >= 0) {
+        const uint32_t p = (uint32_t)(bb / nb), cc = (uint32_t)(bb % nb);
+        *rblk = (int)(isc[cc] ? p : cc);
+        if (full) {
+            uint64_t mn = ~0ull;
+            for (uint32_t j = 0; j < ncached; ++j) {
+                const uint32_t b2 = cached[j];
+                if (b2 == p || b2 == cc) continue;
+                uint64_t inc = 0;
+                for (uint32_t k = 0; k < nb; ++k)
+                    inc += pairs[(uint64_t)b2 * nb + k] + (k != b2 ? pairs[(uint64_t)k * nb + b2] : 0);
+                if (inc < mn) {
+                    mn = inc;
+                    *rpos = (int)j;
+                }
+            }
+        }
+    }
+}
+
+/* The out-of-core engine's block schedule replayed on the CPU from the
+ * walkers' requirement entries (oracle_walk_reqs): per iteration, the block
+ * staged in the last iteration becomes resident, the plain choice is taken
+ * from the bucket counts of the last re-bucketing (prefetch: the decision
+ * picks the next iteration's block), every runnable walker advances while
+ * its blocks are resident, and the walkers are re-bucketed by (prev block,
+ * cur block, needs-prev flag).  `lazy` is the engine's residency rule (0:
+ * both blocks, the reference's).  nslots = cache slots; with prefetch one of
+ * them stages the next block.  log (optional, 3 x iterations cap): per
+ * iteration the loaded block, the cached position it replaced (-1 append)
+ * and the steps taken.  Returns the iteration count or -1. */
+int64_t oracle_sched_replay(const uint16_t *reqs, const uint32_t *nent, uint32_t count, uint32_t stride, uint32_t nb,
+                            uint32_t nslots, int prefetch, int lazy, uint64_t zero_threshold, int32_t *log,
+                            uint64_t log_cap, oracle_sched_stats *out)
+{
+    if (nb == 0 || nb > 1024 || nslots < (prefetch ? 3u : 2u)) return -1;
+    memset(out, 0, sizeof(*out));
+    const uint64_t nn = (uint64_t)nb * nb;
+    uint32_t *e = (uint32_t *)calloc(count, sizeof(uint32_t));      /* next entry of each walker */
+    uint8_t *flag = (uint8_t *)calloc(count, 1);                     /* parked needing its prev block */
+    uint64_t *cnt = (uint64_t *)calloc(2 * nn, sizeof(uint64_t));   /* bucket counts */
+    uint64_t *pairs = (uint64_t *)calloc(nn, sizeof(uint64_t));
+    uint32_t *live = (uint32_t *)malloc(sizeof(uint32_t) * (count ? count : 1));
+    uint8_t res[1024];
+    uint32_t cached[1024], ncached = 0;
+    memset(res, 0, sizeof(res));
+    uint32_t nlive = 0;
+    for (uint32_t w = 0; w < count; ++w)
+        if (nent[w]) live[nlive++] = w;
+        else out->finished++;
+    const uint32_t capacity = prefetch ? nslots - 1 : nslots;
+    int staged = -1, staged_pos = -1;
+    int64_t it = 0;
+#define BLK(w, k) ((uint32_t)(reqs[(uint64_t)(w) * stride + (k)] & 0x3FFFu))
+    /* bucket counts of the live walkers (the re-bucketing) */
+#define REBUCKET()                                                                 \
+    do {                                                                            \
+        memset(cnt, 0, sizeof(uint64_t) * 2 * nn);                                  \
+        for (uint32_t k = 0; k < nlive; ++k) {                                      \
+            const uint32_t w = live[k];                                             \
+            const uint32_t cb = BLK(w, e[w]), pb = e[w] ? BLK(w, e[w] - 1) : cb;     \
+            cnt[(flag[w] ? nn : 0) + (uint64_t)pb * nb + cb]++;                     \
+        }                                                                           \
+        for (uint64_t b = 0; b < nn; ++b) pairs[b] = cnt[b] + cnt[nn + b];          \
+    } while (0)
+    REBUCKET();
+    for (;;) {
+        if (++it > (1 << 22)) {
+            it = -1;
+            break;
+        }
+        if (prefetch && staged >= 0) {
+            if (staged_pos >= 0) {
+                res[cached[staged_pos]] = 0;
+                cached[staged_pos] = (uint32_t)staged;
+            } else {
+                cached[ncached++] = (uint32_t)staged;
+            }
+            res[staged] = 1;
+            staged = -1;
+        }
+        int action, blk, pos, rblk, rpos;
+        plain_choice(pairs, nb, cached, ncached, capacity, zero_threshold, &action, &blk, &pos, &rblk, &rpos);
+        const uint32_t live_at_decision = nlive;
+        int load = -1, lpos = -1;
+        if (action) {
+            load = blk;
+            lpos = action == 2 ? pos : -1;
+        } else if (rblk >= 0 && (ncached < capacity || rpos >= 0)) {
+            load = rblk;
+            lpos = ncached >= capacity ? rpos : -1;
+            out->rescues++;
+        }
+        if (!prefetch && live_at_decision == 0) break;
+        if (!prefetch && load >= 0) {
+            /* loaded before this iteration's step */
+            if (lpos >= 0) {
+                res[cached[lpos]] = 0;
+                cached[lpos] = (uint32_t)load;
+            } else {
+                cached[ncached++] = (uint32_t)load;
+            }
+            res[load] = 1;
+        }
+        /* the step: every walker of a runnable bucket advances while it can */
+        uint64_t steps_before = out->steps;
+        uint32_t k2 = 0;
+        for (uint32_t k = 0; k < nlive; ++k) {
+            const uint32_t w = live[k];
+            uint32_t ew = e[w];
+            const uint32_t cb0 = BLK(w, ew), pb0 = ew ? BLK(w, ew - 1) : cb0;
+            const int runnable = res[cb0] && (res[pb0] || (lazy && !flag[w]));
+            int done = 0;
+            if (runnable) {
+                flag[w] = 0;
+                for (;;) {
+                    const uint16_t ent = reqs[(uint64_t)w * stride + ew];
+                    const uint32_t cb = ent & 0x3FFFu, pb = ew ? BLK(w, ew - 1) : cb;
+                    if (ent & 0x4000u) {
+                        done = 1;
+                        break;
+                    }
+                    if (!res[pb] && (!lazy || (ent & 0x8000u))) {
+                        flag[w] = 1; /* parked: needs N(prev) */
+                        out->parks++;
+                        break;
+                    }
+                    (void)cb;
+                    ew++;
+                    out->steps++;
+                    if (ew >= nent[w]) {
+                        done = 1;
+                        break;
+                    }
+                    if (!res[BLK(w, ew)]) {
+                        out->parks++;
+                        break;
+                    }
+                }
+                e[w] = ew;
+            }
+            if (done) out->finished++;
+            else live[k2++] = w;
+        }
+        nlive = k2;
+        if (log && (uint64_t)(it - 1) < log_cap) {
+            log[3 * (it - 1) + 0] = load;
+            log[3 * (it - 1) + 1] = lpos;
+            log[3 * (it - 1) + 2] = (int32_t)(out->steps - steps_before);
+        }
+        if (load >= 0) out->loads++;
+        if (prefetch) {
+            if (live_at_decision == 0) break;
+            staged = load;
+            staged_pos = lpos;
+        }
+        REBUCKET();
+    }
+#undef REBUCKET
+#undef BLK
+    out->iterations = it > 0 ? (uint64_t)it : 0;
+    free(e);
+    free(flag);
+    free(cnt);
+    free(pairs);
+    free(live);
+    return it;
 }

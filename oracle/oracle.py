@@ -72,6 +72,13 @@ class Stats(ctypes.Structure):
         return {name: int(getattr(self, name)) for name, _ in self._fields_}
 
 
+class SchedStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("iterations", "loads", "steps", "parks", "rescues", "finished")]
+
+    def as_dict(self):
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
 _LIB = None
 
 
@@ -102,6 +109,18 @@ def lib():
                                   ctypes.c_int]
         L.oracle_walk.restype = ctypes.c_int
         f32p = ctypes.POINTER(ctypes.c_float)
+        L.oracle_walk_ids.argtypes = [u64p, u32p, ctypes.c_uint32, ctypes.POINTER(Cfg), u32p, ctypes.c_uint32,
+                                      u32p, u32p, u64p, ctypes.POINTER(Stats), ctypes.c_int]
+        L.oracle_walk_ids.restype = ctypes.c_int
+        L.oracle_walk_reqs.argtypes = [u64p, u32p, ctypes.c_uint32, ctypes.POINTER(Cfg), u32p, ctypes.c_uint32,
+                                       ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint16), u32p,
+                                       ctypes.c_int]
+        L.oracle_walk_reqs.restype = ctypes.c_int
+        L.oracle_sched_replay.argtypes = [ctypes.POINTER(ctypes.c_uint16), u32p, ctypes.c_uint32, ctypes.c_uint32,
+                                          ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32), ctypes.c_uint64,
+                                          ctypes.POINTER(SchedStats)]
+        L.oracle_sched_replay.restype = ctypes.c_int64
         L.oracle_walk_weighted.argtypes = [u64p, u32p, f32p, u32p, ctypes.c_uint32, ctypes.POINTER(Cfg),
                                            ctypes.c_uint32, ctypes.c_uint32, u32p, u32p, u64p, u32p,
                                            ctypes.POINTER(Stats), ctypes.c_int]
@@ -340,6 +359,60 @@ def walk(beg, csr, cfg: Cfg, wid_begin: int, count: int, paths: bool = True, fin
     return {"paths": P, "lens": L, "hashes": H, "finals": F, "stats": st.as_dict()}
 
 
+def walk_ids(beg, csr, cfg: Cfg, ids, paths: bool = False, nthreads: int = 0):
+    """Walk the listed walkers (u32 ids, any order): row i is walker ids[i].
+    Returns a dict with paths (or None), lens, hashes, stats."""
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    n = ids.size
+    P = np.zeros((n, cfg.maxhops + 1), dtype=np.uint32) if paths else None
+    L = np.zeros(n, dtype=np.uint32)
+    H = np.zeros(n, dtype=np.uint64)
+    st = Stats()
+    rc = lib().oracle_walk_ids(_p(beg, ctypes.c_uint64), _p(csr, ctypes.c_uint32), len(beg) - 1, ctypes.byref(cfg),
+                               _p(ids, ctypes.c_uint32), n, _p(P, ctypes.c_uint32), _p(L, ctypes.c_uint32),
+                               _p(H, ctypes.c_uint64), ctypes.byref(st), nthreads)
+    if rc != 0:
+        raise ValueError("oracle_walk_ids rejected the configuration")
+    return {"paths": P, "lens": L, "hashes": H, "stats": st.as_dict()}
+
+
+def walk_requirements(beg, csr, cfg: Cfg, vstart, wid_begin: int, count: int, nthreads: int = 0):
+    """The blocks walkers [wid_begin, wid_begin+count) will need, in order
+    (gw_oracle.c oracle_walk_reqs): count x (maxhops+1) u16 entries (block,
+    bit 14 terminal, bit 15 needs the previous block under the lazy rule) and
+    the entry count of each walker."""
+    vstart = np.ascontiguousarray(vstart, dtype=np.uint32)
+    stride = cfg.maxhops + 1
+    reqs = np.zeros((count, stride), dtype=np.uint16)
+    nent = np.zeros(count, dtype=np.uint32)
+    rc = lib().oracle_walk_reqs(_p(beg, ctypes.c_uint64), _p(csr, ctypes.c_uint32), len(beg) - 1, ctypes.byref(cfg),
+                                _p(vstart, ctypes.c_uint32), len(vstart) - 1, wid_begin, count,
+                                reqs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), _p(nent, ctypes.c_uint32),
+                                nthreads)
+    if rc != 0:
+        raise ValueError("oracle_walk_reqs rejected the configuration")
+    return reqs, nent
+
+
+def sched_replay(reqs, nent, nb: int, nslots: int, prefetch: bool = True, lazy: bool = True,
+                 zero_threshold: int = 0, log: bool = False):
+    """The out-of-core engine's plain block schedule replayed on the CPU
+    (gw_oracle.c oracle_sched_replay).  Returns (stats dict, per-iteration log
+    of (loaded block, replaced position, steps) or None)."""
+    reqs = np.ascontiguousarray(reqs, dtype=np.uint16)
+    nent = np.ascontiguousarray(nent, dtype=np.uint32)
+    cap = 1 << 22 if log else 0
+    lg = np.zeros((cap, 3), dtype=np.int32) if log else None
+    st = SchedStats()
+    it = lib().oracle_sched_replay(reqs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), _p(nent, ctypes.c_uint32),
+                                   len(nent), reqs.shape[1], nb, nslots, int(prefetch), int(lazy), zero_threshold,
+                                   lg.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) if log else None, cap,
+                                   ctypes.byref(st))
+    if it < 0:
+        raise ValueError("schedule replay failed (bad arguments or no progress)")
+    return st.as_dict(), (lg[:it].copy() if log else None)
+
+
 def walk_traced(beg, csr, cfg: Cfg, wid: int, prev: int, cur: int, hop: int, cap: int = 1 << 16):
     path = np.zeros(cfg.maxhops + 1, dtype=np.uint32)
     trace = np.zeros((cap, 4), dtype=np.uint32)
@@ -425,6 +498,59 @@ def split_equal_edge_mass(beg: np.ndarray, nblocks: int):
     vb = vb.astype(np.uint32)
     eb = beg[vb.astype(np.int64)].astype(np.uint64)
     return vb, eb
+
+
+# ------------------------------------------------------------------ GOWalker block choice
+
+def max_choose_blocks(counts, cached, nslots: int, zero_threshold: int = 0):
+    """Restatement of GOwalker_scheduler_t::max_choose_blocks
+    (engine/schedule.hpp:70-138).  counts: nb x nb walkers per (prev block,
+    cur block); cached: the scheduler's list of resident blocks in order (its
+    `buckets`); nslots: cache slots (graph_cache::ncblock).
+
+    Cache not full (len(cached) < nslots, 108-131): every uncached block i
+    scores sum over cached c of counts[i,c] + counts[c,i], plus counts[i,i];
+    the best is appended.  Full (83-107): s_j = counts[i,c_j] + counts[c_j,i],
+    the score is sum_j s_j - min_j s_j, and i replaces the cached block of the
+    first smallest s_j (strict `<` from 0xffffffff, 95-98).  A block is taken
+    only if its score is > 0 and > zero_threshold (101, 124).  The reference
+    orders scores with std::sort (not stable); among equal best scores this
+    takes the lowest block id, which is libstdc++'s order when at most 16
+    blocks are uncached (its insertion sort keeps the ascending order in which
+    pre_cached is built, 79-84).
+
+    Returns (action, block, position): (0, -1, -1) when nothing qualifies (the
+    reference returns false), (1, i, len(cached)) when i is appended,
+    (2, i, j) when i replaces cached[j]."""
+    c = np.asarray(counts, dtype=np.uint64)
+    nb = c.shape[0]
+    c = c.reshape(nb, nb)
+    cached = [int(x) for x in cached]
+    isc = np.zeros(nb, dtype=bool)
+    isc[cached] = True
+    pre = [i for i in range(nb) if not isc[i]]
+    if not pre:
+        return (0, -1, -1)
+    cl = np.array(cached, dtype=np.int64)
+    best_i, best_s, best_pos = -1, -1, -1
+    full = len(cached) >= nslots
+    for i in pre:
+        links = (c[i, cl] + c[cl, i]) if len(cl) else np.zeros(0, dtype=np.uint64)
+        if full:
+            mn, idx = 0xFFFFFFFF, 0
+            for j, v in enumerate(links):
+                if int(v) < mn:
+                    mn, idx = int(v), j
+            score = int(links.sum()) - mn
+            pos = idx
+        else:
+            score = int(links.sum()) + int(c[i, i])
+            pos = len(cached)
+        if score > best_s:  # first (lowest id) of equal scores
+            best_i, best_s, best_pos = i, score, pos
+    if best_s > 0 and best_s > zero_threshold:
+        return (2 if full else 1, best_i, best_pos)
+    return (0, -1, -1)
 
 
 # ------------------------------------------------------------------ SOWalker annealing block choice
@@ -540,6 +666,34 @@ def ref_lib(unmodified: bool = False):
     L.ref_get_block.argtypes = [ctypes.c_uint32]
     L.ref_get_block.restype = ctypes.c_uint32
     return L
+
+
+def ref_choose_blocks(base: str, cases):
+    """Open the reference harness on the dataset at `base` (its block count is
+    the scheduler's nblocks) and run the reference's own
+    GOwalker_scheduler_t::max_choose_blocks once per case (counts, cached,
+    nslots, zero_threshold).  Returns one (chose, list after) per case.  Run in
+    a fresh process ('spawn'): the harness keeps global state."""
+    L = ref_lib()
+    if L is None:
+        raise FileNotFoundError("oracle/_ref harness not built")
+    u32p = ctypes.POINTER(ctypes.c_uint32)
+    L.ref_max_choose_blocks.argtypes = [u32p, u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, u32p, u32p]
+    L.ref_max_choose_blocks.restype = ctypes.c_int
+    nb = L.ref_open(base.encode(), ALG_NODE2VEC, 0.5, 2.0, 0.2, 80, 1, 1)
+    out = []
+    for counts, cached, nslots, zt in cases:
+        c = np.ascontiguousarray(counts, dtype=np.uint32).reshape(-1)
+        assert c.size == nb * nb
+        cl = np.ascontiguousarray(cached, dtype=np.uint32)
+        lst = np.zeros(nb + 1, dtype=np.uint32)
+        n = ctypes.c_uint32(0)
+        r = L.ref_max_choose_blocks(_p(c, ctypes.c_uint32), _p(cl, ctypes.c_uint32) if cl.size else None, cl.size,
+                                    nslots, zt, _p(lst, ctypes.c_uint32), ctypes.byref(n))
+        if r < 0:
+            raise RuntimeError("reference harness refused the case")
+        out.append((bool(r), lst[: n.value].copy()))
+    return out
 
 
 def ref_walk(L, wid, prev, cur, hop, prev_blk, cur_blk, cap=1 << 16):

@@ -224,3 +224,30 @@ extern "C" uint32_t ref_get_block(uint32_t v)
 {
     return g_ref ? g_ref->blocks->get_block(v) : 0xFFFFFFFFu;
 }
+
+/* GOwalker_scheduler_t::max_choose_blocks (engine/schedule.hpp:70-138), the
+ * reference's own code, on given bucket counts: counts = nb*nb walkers per
+ * (prev block, cur block) pair, nb = the opened dataset's block count;
+ * cached = the scheduler's list (its `buckets`) in order; nslots = the device
+ * cache's slot count (graph_cache::ncblock).  Returns 1 when the reference
+ * chose a block; out_list receives its list afterwards (*out_n entries, room
+ * for nb).  The counts are cleared again before returning. */
+extern "C" int ref_max_choose_blocks(const uint32_t *counts, const uint32_t *cached, uint32_t ncached,
+                                     uint32_t nslots, uint32_t zero_threshold, uint32_t *out_list,
+                                     uint32_t *out_n)
+{
+    RefState *s = g_ref;
+    if (!s || nslots == 0) return -1;
+    graph_walk *w = s->walk;
+    const bid_t nb = w->nblocks;
+    for (bid_t b = 0; b < nb * nb; ++b) w->block_walks[b].num = counts[b];
+    GOwalker_scheduler_t *g = static_cast<GOwalker_scheduler_t *>(s->sched);
+    g->buckets.assign(cached, cached + ncached);
+    graph_cache slots(nslots, s->conf.blocksize);
+    s->conf.zero_threshold = zero_threshold;
+    const bool chose = g->max_choose_blocks(s->conf, slots, *s->driver, *w, nullptr, nullptr, *s->g_cache, *s->m);
+    *out_n = (uint32_t)g->buckets.size();
+    for (size_t j = 0; j < g->buckets.size(); ++j) out_list[j] = g->buckets[j];
+    for (bid_t b = 0; b < nb * nb; ++b) w->block_walks[b].num = 0;
+    return chose ? 1 : 0;
+}

@@ -279,3 +279,32 @@ def test_trained_predictor_beats_carrying_demand_forward(gw, oracle, case):
     e0.run(gw.GW_POLICY_PLAIN)
     assert e0.checksum() == hs
     e0.close()
+
+
+@pytest.mark.parametrize("algo,prefetch,strict,slots", [(0, 0, 0, 5), (0, 1, 0, 6), (0, 0, 1, 5), (0, 1, 1, 6),
+                                                         (1, 1, 0, 6), (1, 0, 0, 4)])
+def test_block_schedule_matches_cpu_replay(gw, oracle, algo, prefetch, strict, slots):
+    """The engine's whole plain block schedule -- GOWalker's choice each
+    iteration (engine/schedule.hpp:70-138), the rescue when nothing
+    qualifies, the residency rule, prefetch one iteration ahead -- replayed on
+    the CPU from the walkers' block requirements (the oracle's walks), gives
+    the same number of iterations and block loads, and the same steps, as the
+    GPU run."""
+    from gowalker_b200.preprocess import split_equal_edge_mass
+    beg, csr = graph(oracle, scale=14, ef=8, cap=12000, seed=31)
+    nb = 16
+    vb, eb = split_equal_edge_mass(beg, nb)
+    term = 0.15 if algo else 0.0
+    eng = gw.WalkEngine(algorithm=algo, maxhops=30, p=0.5, q=2.0, alpha=0.2, term_prob=term, seed=9, walkpersource=1,
+                        record_paths=0, cache_size=cache_for(beg, eb, slots), zero_copy=0, zero_threshold=0,
+                        prefetch=prefetch, strict_blocks=strict)
+    eng.set_host_graph(beg, csr, vb, eb)
+    eng.init_walkers(algo, 1, 9)
+    st = eng.run(gw.GW_POLICY_PLAIN)
+    eng.close()
+    cfg = oracle.make_cfg(algo=algo, maxhops=30, p=0.5, q=2.0, alpha=0.2, term_prob=term, seed=9)
+    reqs, nent = oracle.walk_requirements(beg, csr, cfg, vb, 0, len(beg) - 1)
+    lazy = algo == 0 and not strict
+    rs, _ = oracle.sched_replay(reqs, nent, nb, slots, prefetch=bool(prefetch), lazy=lazy)
+    assert (st["iterations"], st["block_loads"], st["steps"]) == (rs["iterations"], rs["loads"], rs["steps"])
+    assert rs["loads"] > 2 * nb

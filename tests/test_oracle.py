@@ -392,3 +392,33 @@ def test_weighted_node2vec_transition_law_chi_square(oracle):
         assert chi < dof + 5 * math.sqrt(2 * dof) + 10, ((a, b), chi, dof)
         tested += 1
     assert tested == 25 and len(nz) == V
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_step.so")),
+                    reason="reference harness not built (needs the GOWalker sources)")
+@pytest.mark.parametrize("nb", [6, 20, 64])
+def test_max_choose_blocks_matches_reference(oracle, tmp_path, nb):
+    """The oracle's restatement of GOWalker's block choice takes the decision
+    the reference's own GOwalker_scheduler_t::max_choose_blocks
+    (engine/schedule.hpp:70-138, compiled from its sources) takes, on random
+    and adversarial bucket-count matrices: not-full and full caches, zero
+    threshold at and below the best score, all-zero counts, equal scores
+    among at most 16 uncached blocks, shared smallest links."""
+    import schedule_cases as SC
+    # one vertex per block: the scheduler's nblocks is nb
+    beg = np.arange(nb + 1, dtype=np.uint64)
+    csr = ((np.arange(nb) + 1) % nb).astype(np.uint32)
+    base = str(tmp_path / "g")
+    oracle.write_dataset(base, beg, csr)
+    oracle.write_blocks(base, 1, np.arange(nb + 1, dtype=np.uint32), beg.copy())
+    cases = SC.cases(nb, seed=nb)
+    assert len(cases) >= 30
+    with mp.get_context("spawn").Pool(1) as pool:
+        res = pool.apply(oracle.ref_choose_blocks, (base, cases))
+    acts = set()
+    for (counts, cached, nslots, zt), (chose, after) in zip(cases, res):
+        want = SC.ref_to_decision(cached, chose, after)
+        got = oracle.max_choose_blocks(counts, cached, nslots, zt)
+        assert got == want, (cached, nslots, zt)
+        acts.add(got[0])
+    assert acts == {0, 1, 2}

@@ -12,12 +12,12 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _noalloc(gw, cfg, dg, nwalkers, paths):
+def _noalloc(gw, cfg, dg, nwalkers, paths, fill=0):
     import torch
     L = gw.load()
-    hashes = torch.zeros(nwalkers, dtype=torch.int64, device="cuda")
-    lens = torch.zeros(nwalkers, dtype=torch.int32, device="cuda")
-    prows = torch.zeros((nwalkers, cfg.maxhops + 1), dtype=torch.int32, device="cuda") if paths else None
+    hashes = torch.full((nwalkers,), fill, dtype=torch.int64, device="cuda")
+    lens = torch.full((nwalkers,), fill, dtype=torch.int32, device="cuda")
+    prows = torch.full((nwalkers, cfg.maxhops + 1), fill, dtype=torch.int32, device="cuda") if paths else None
     st = gw.GwStats()
     rc = L.gw_walk_noalloc(ctypes.byref(cfg), ctypes.c_void_p(dg.beg_ptr), ctypes.c_void_p(dg.csr_ptr), dg.nverts,
                            dg.nedges, nwalkers, ctypes.c_void_p(hashes.data_ptr()), ctypes.c_void_p(lens.data_ptr()),
@@ -41,8 +41,10 @@ def test_noalloc_matches_gw_run_twice(gw, algo, maxhops, term, wps, p, q):
     ref_hashes = eng.hashes()
     n = eng.num_walkers()
     eng.close()
-    for _ in range(2):  # the second call reuses the scratch the first one left behind
-        (h, l, pr), st = _noalloc(gw, cfg, dg, n, paths=True)
+    # the second call reuses the scratch the first one left behind; its
+    # output buffers start filled with ones, as a reused caller buffer may be
+    for fill in (0, -1):
+        (h, l, pr), st = _noalloc(gw, cfg, dg, n, paths=True, fill=fill)
         assert np.array_equal(h, ref_hashes)
         assert np.array_equal(l, ref_lens)
         assert np.array_equal(pr, ref_paths)
