@@ -634,12 +634,6 @@ def prep_cpu_baseline(src, dst, V, target_s):
             "sample": "first %d of the samples, symmetrised + deduplicated + sorted" % k}
 
 
-def rank_seed(rank):
-    """Walk seed of a rank: every rank walks its own replica of the workload
-    (walkers are independent), so the per-GPU work stays fixed as N grows."""
-    return 42 + rank
-
-
 def reduce_rank_times(dist, ms, ms2, steps, e2e_steps, device):
     """Whole-job figures from every rank's own: the slowest rank's times (max)
     and all ranks' steps (sum), so value = all steps / the max time.  Every
@@ -654,25 +648,50 @@ def reduce_rank_times(dist, ms, ms2, steps, e2e_steps, device):
     return float(tmax[0]), float(tmax[1]), float(tsum[0]), float(tsum[1])
 
 
+def necessary_bytes(stats, walkers, paths):
+    """Bytes a walk step cannot avoid moving (oracle counts on a sample): the
+    32-B sector(s) of (beg[cur], beg[cur+1]), the sector of the accepted
+    candidate, the distinct sectors of the accepted trial's search of N(prev)
+    when its verdict needed one, the path entry (when recorded), and each
+    walker's hash and length.  Rejected trials need not read their
+    candidates (a warp decides them from positions), so they add nothing."""
+    b = 32 * (stats["off_sectors"] + stats["steps"] + stats["acc_sectors"]) + 12 * walkers
+    if paths:
+        b += 4 * (stats["steps"] + walkers)
+    return b
+
+
+def golden_checksum(config):
+    """The oracle's whole-run checksum of an in-core workload
+    (tests/golden/config_checksums.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "config_checksums.json")) as f:
+            return json.load(f).get(config)
+    except (OSError, ValueError):
+        return None
+
+
 def run_ours(args, wl):
+    """In-core workload: the graph resident in HBM (value) or copied from
+    pinned host blocks every step with the walks read back (e2e).  Under
+    torchrun every rank walks its own walker-id shard of the one population
+    on its own copy of the graph (no data-path collective)."""
+    import ctypes
     import torch
     import gowalker_b200 as gw
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    torch.cuda.set_device(local)
-    seed = rank_seed(rank)
+    dist, rank, world, local = init_dist()
+    dev = torch.device("cuda", local)
+    seed = 42
     paths = 1 if args.paths else 0
+    L = gw.load()
+    rate, rate_ms = ctypes.c_double(), ctypes.c_float()
+    if L.gw_philox_rate(local, 4096, ctypes.byref(rate), ctypes.byref(rate_ms)) != 0:
+        raise gw.GwError(-2, "gw_philox_rate failed")
 
     dg = build_graph(gw, wl)
+    total = dg.nverts * wl["wps"]
+    first, count = rank_shard(rank, world, total)
     cfgkw = dict(algorithm=wl["algo"], maxhops=wl["maxhops"], p=wl["p"], q=wl["q"], alpha=wl["alpha"],
                  term_prob=wl["term"], seed=seed, walkpersource=wl["wps"], record_paths=paths, device=local,
                  cache_size=1 << 40)
@@ -693,7 +712,7 @@ def run_ours(args, wl):
 
     # ---- device-resident runs
     for _ in range(args.warmup):
-        eng.init_walkers(wl["algo"], wl["wps"], seed)
+        eng.init_walkers(wl["algo"], wl["wps"], seed, first=first, count=count)
         eng.run()
     barrier()
     clocks = ClockSampler(local)
@@ -708,7 +727,7 @@ def run_ours(args, wl):
     variant = -1
     coop = [0, 0, 0, 0]
     for _ in range(args.steps):
-        eng.init_walkers(wl["algo"], wl["wps"], seed)
+        eng.init_walkers(wl["algo"], wl["wps"], seed, first=first, count=count)
         st = eng.run()
         for i, k in enumerate(("coop_small_steps", "coop_small_attempts", "coop_large_steps", "coop_large_attempts")):
             coop[i] += st[k]
@@ -722,9 +741,8 @@ def run_ours(args, wl):
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
     hash_sum, steps_last = eng.checksum()
-    nwalkers = eng.num_walkers()
 
-    # ---- end to end through the C ABI with host blocks
+    # ---- end to end through the C ABI: host blocks in, the walks out
     beg_t, csr_t, beg, csr = host_graph(dg)
     eng2 = gw.WalkEngine(**cfgkw)
     eng2.set_host_graph(beg_t, csr_t[: dg.nedges])
@@ -733,66 +751,91 @@ def run_ours(args, wl):
         h_w = torch.empty(dg.nedges, dtype=torch.float32, pin_memory=True)
         h_w.copy_(d_w)
         eng2.set_host_weights(h_w)
+    stride = wl["maxhops"] + 1
+    out_rows = torch.empty((count, stride) if paths else (1,), dtype=torch.int32, pin_memory=True)
+    out_lens = torch.empty(count, dtype=torch.int32, pin_memory=True)
+    out_hash = torch.empty(count, dtype=torch.int64, pin_memory=True)
     stream2 = torch.cuda.ExternalStream(eng2.stream_handle(), device=local)
-    for _ in range(max(1, args.warmup)):
+
+    def e2e_step():
         eng2.cache_reset()
-        eng2.init_walkers(wl["algo"], wl["wps"], seed)
-        eng2.run()
+        eng2.init_walkers(wl["algo"], wl["wps"], seed, first=first, count=count)
+        st2 = eng2.run()
+        if paths:
+            eng2._check(L.gw_get_paths(eng2.h, 0, count, ctypes.c_void_p(out_rows.data_ptr()),
+                                       ctypes.c_void_p(out_lens.data_ptr())))
+        else:
+            eng2._check(L.gw_path_lengths(eng2.h, 0, count, ctypes.c_void_p(out_lens.data_ptr())))
+        eng2._check(L.gw_path_hashes(eng2.h, 0, count, ctypes.c_void_p(out_hash.data_ptr())))
+        return st2
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
     barrier()
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(stream2)
-    e2e_steps = h2d = d2h = 0
+    e2e_steps = h2d = 0
     for _ in range(args.steps):
-        eng2.cache_reset()
-        eng2.init_walkers(wl["algo"], wl["wps"], seed)
-        st2 = eng2.run()
+        st2 = e2e_step()
         e2e_steps += st2["steps"]
         h2d += st2["h2d_bytes"]
-        d2h += st2["d2h_bytes"]
-        launches += 0
-    hs2, _ = eng2.checksum()
     f1.record(stream2)
     barrier()
     ms2 = f0.elapsed_time(f1)
+    d2h = count * (12 + (4 * stride if paths else 0))
+    hs2 = int(out_hash.numpy().view(np.uint64).sum(dtype=np.uint64))
     if hs2 != hash_sum:
         log("warning: e2e checksum differs from the device-resident run")
 
-    # max over ranks
+    # max over ranks; the population's checksum from the shards'
     ms, ms2, steps_all, e2e_all = reduce_rank_times(dist, ms, ms2, steps, e2e_steps, "cuda")
+    pop_hash = combine_hash_sums(dist, hash_sum, dev)
+    pop_steps = int(reduce_rank_times(dist, 0.0, 0.0, steps_last, 0, "cuda")[2])
 
     if rank == 0:
         peaks, peak_kind = measured_peaks()
         value = steps_all / (ms / 1000.0)
         line = {
             "metric": "walk steps/sec", "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "int32 gathers, fp32/fp64 accept compares", "data": "synthetic",
-            "config": {"workload": wl["name"], "vertices": dg.nverts, "edges": dg.nedges, "walkers": nwalkers,
+            "config": {"workload": wl["name"], "vertices": dg.nverts, "edges": dg.nedges, "walkers": total,
                        "csr_bytes": (dg.nverts + 1) * 8 + dg.nedges * 4,
                        "l2": "inputs larger than L2 (CSR %.2f GB vs 126 MB L2); no flush"
                              % (((dg.nverts + 1) * 8 + dg.nedges * 4) / 1e9),
-                       "paths_recorded": bool(paths), "walk_seed": "42+rank", "generator_seed": 1,
-                       "parallelism": "walker replicas per rank" if world > 1 else "1 GPU"},
+                       "paths_recorded": bool(paths), "walk_seed": seed, "generator_seed": 1,
+                       "parallelism": "walker-id shards, one per rank" if world > 1 else "1 GPU"},
             "gpu_launches": launches,
             "e2e": {"value": e2e_all / (ms2 / 1000.0), "unit": "steps/s",
-                    "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps},
-            "checksum": {"path_hash_sum": hash_sum, "steps_per_run": steps_last},
+                    "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h * world,
+                    "note": "per step: the CSR copied from pinned host blocks and validated, every walker run, "
+                            "then %s read back into pinned host memory"
+                            % ("every path row, length and hash" if paths else "every path length and hash")},
+            "checksum": {"path_hash_sum": pop_hash, "steps_per_run": pop_steps},
             "trials_per_step": trials / max(steps, 1),
             "kernel_variant": variant,
             "hard_steps": {"by_position": coop[0] // args.steps, "by_position_attempts": coop[1] // args.steps,
                            "by_search": coop[2] // args.steps, "by_search_attempts": coop[3] // args.steps},
         }
+        gold = golden_checksum(args.config)
+        if gold is not None and "path_hash_sum" in gold:
+            line["checksum"]["oracle_path_hash_sum"] = int(gold["path_hash_sum"])
+            line["checksum"]["matches_oracle"] = (pop_hash == int(gold["path_hash_sum"]) and
+                                                  pop_steps == gold["steps"])
         if clk:
             line["clocks"] = clk
-        # roofline of the step kernel from the oracle's exact sector counts on a sample
+        # roofline of the step kernel: the bytes a step cannot avoid (oracle
+        # counts on a sample of the workload) over the kernel's time
         from oracle import oracle as O
         O.lib()
         threads = os.cpu_count() or 1
         alias = O.build_alias(beg, h_w.numpy()) if h_w is not None else None
         s_steps, s_secs, s_stats, s_walk, s_desc = oracle_sample(O, beg, csr, wl, seed, args.cpu_seconds,
                                                                  threads=threads, alias=alias)
-        bpstep = algorithmic_bytes(s_stats, s_walk, paths, weighted=alias is not None) / max(s_steps, 1)
+        bpstep = necessary_bytes(s_stats, s_walk, paths) / max(s_steps, 1)
+        if alias is not None:
+            bpstep += 32.0  # the accepted candidate's alias-table entry
         kernel_s = kernel_ms / 1000.0 / args.steps
         steps_per_launch = steps / args.steps
         achieved = bpstep * steps_per_launch / kernel_s / 1e9
@@ -801,19 +844,25 @@ def run_ours(args, wl):
                             "frac": achieved / peaks["hbm_gbs"],
                             "traffic": (dram_ps * steps_per_launch) if dram_ps else None,
                             "peak_source": peak_kind,
-                            "algorithmic_bytes_per_step": bpstep, "kernel_ms_per_launch": kernel_ms / args.steps,
+                            "algorithmic_bytes_per_step": bpstep,
+                            "bytes_model": "offsets sector + accepted candidate sector + the accepted trial's "
+                                           "N(prev) search sectors + path entry + hash and length per walker",
+                            "sector_model_bytes_per_step": algorithmic_bytes(s_stats, s_walk, paths,
+                                                                             weighted=alias is not None)
+                                                           / max(s_steps, 1),
+                            "kernel_ms_per_launch": kernel_ms / args.steps,
                             "kernel": "k_walk_incore (weighted)" if h_w is not None else "k_walk_incore"}
         if dram_ps:
             line["roofline"]["dram_bytes_per_step"] = dram_ps
             line["roofline"]["dram_frac"] = dram_ps * steps_per_launch / kernel_s / 1e9 / peaks["hbm_gbs"]
-        if achieved > peaks["hbm_gbs"]:
-            line["roofline"]["note"] = (
-                "algorithmic bytes follow the reference step's sector model: one candidate sector per trial plus "
-                "the N(prev) search; hard steps decided from candidate positions skip those reads, so frac > 1 "
-                "and the kernel is bound by instruction issue (Philox per trial), not HBM; dram_frac is the "
-                "measured DRAM traffic (ncu, profiles/) over the peak")
+        trial_rate = trials / args.steps / kernel_s
+        line["issue_roofline"] = {"achieved": trial_rate, "peak": rate.value, "unit": "trials/s",
+                                  "frac": trial_rate / rate.value,
+                                  "peak_source": "measured in this run: gw_philox_rate, the step kernels' keyed "
+                                                 "Philox4x32-10 alone, best of 3 launches (%.1f ms)" % rate_ms.value,
+                                  "note": "every rejection trial evaluates at least one Philox draw"}
         line["cpu_baseline"] = {"value": s_steps / s_secs, "unit": "steps/s", "cores": threads, "kind": "port",
-                                "sample": s_desc}
+                                "cpu_model": cpu_model(), "sample": s_desc}
         print(json.dumps(line), flush=True)
     eng.close()
     eng2.close()

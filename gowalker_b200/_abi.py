@@ -24,7 +24,7 @@ EXPORTS = (
     "gw_version", "gw_status_string", "gw_config_default", "gw_create", "gw_destroy", "gw_last_error",
     "gw_set_config", "gw_stream", "gw_set_graph_meta", "gw_host_block", "gw_device_graph", "gw_cache_reset",
     "gw_host_weights", "gw_device_weights",
-    "gw_init_walkers", "gw_init_walker_range", "gw_run", "gw_num_walkers", "gw_get_paths", "gw_path_hashes", "gw_checksum",
+    "gw_init_walkers", "gw_init_walker_range", "gw_run", "gw_num_walkers", "gw_get_paths", "gw_path_lengths", "gw_path_hashes", "gw_checksum",
     "gw_bucket_counts", "gw_rmat_csr", "gw_web_csr", "gw_edges_csr", "gw_split_blocks", "gw_sa_choose_blocks",
     "gw_plain_choose_block", "gw_device_free", "gw_memcpy", "gw_walk_noalloc", "gw_philox_rate",
     "gw_mlp_forward", "gw_mlp_grad", "gw_mlp_train", "gw_host_alloc", "gw_host_free",
@@ -130,6 +130,7 @@ def load():
         "gw_num_walkers": ([vp, u64p], i32),
         "gw_get_paths": ([vp, u64, u64, vp, vp], i32),
         "gw_path_hashes": ([vp, u64, u64, vp], i32),
+        "gw_path_lengths": ([vp, u64, u64, vp], i32),
         "gw_checksum": ([vp, u64p, u64p], i32),
         "gw_bucket_counts": ([vp, vp], i32),
         "gw_rmat_csr": ([u32, u32, u64, u32p, u64, i32, u64, ctypes.POINTER(vp), ctypes.POINTER(vp), u64p], i32),

@@ -744,6 +744,28 @@ extern "C" int gw_run(gw_handle *h, uint32_t policy, gw_stats *stats)
 
 // ------------------------------------------------------------------ ABI: results
 
+namespace {
+// Zero every path-row entry past its walk's length (the kernels write a row
+// only up to the length; the rest holds whatever the buffer held before).
+__global__ void k_zero_tails(uint32_t *rows, const uint32_t *lens, uint64_t n, uint32_t stride)
+{
+    const uint64_t total = n * stride;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t row = i / stride;
+        if (i - row * stride >= __ldg(lens + row)) rows[i] = 0u;
+    }
+}
+}  // namespace
+
+extern "C" int gw_path_lengths(gw_handle *h, uint64_t first, uint64_t n, uint32_t *lens)
+{
+    if (!h || !lens) return GW_ERR_ARG;
+    if (!h->walkers_ready || !h->d_lens) return h->fail(GW_ERR_STATE, "no walk has run");
+    if (first + n > h->nwalkers) return h->fail(GW_ERR_ARG, "walker range out of bounds");
+    cudaSetDevice(h->cfg.device);
+    return h->cuda(cudaMemcpy(lens, h->d_lens + first, n * sizeof(uint32_t), cudaMemcpyDeviceToHost), "lengths D2H");
+}
+
 extern "C" int gw_get_paths(gw_handle *h, uint64_t first, uint64_t n, uint32_t *out, uint32_t *lens)
 {
     if (!h) return GW_ERR_ARG;
@@ -752,32 +774,24 @@ extern "C" int gw_get_paths(gw_handle *h, uint64_t first, uint64_t n, uint32_t *
     if (first + n > h->nwalkers) return h->fail(GW_ERR_ARG, "walker range out of bounds");
     cudaSetDevice(h->cfg.device);
     int st;
-    std::vector<uint32_t> own_lens;
-    uint32_t *L = lens;
-    if (!L && out && n) {  // the lengths are needed to zero the rows' tails
-        own_lens.resize(n);
-        L = own_lens.data();
+    if (out && n) {
+        // rows end with zeros past the walk's length: padded on the device,
+        // then one copy
+        k_zero_tails<<<h->num_sms * 8, 256, 0, h->s_compute>>>(h->d_paths + first * h->path_stride, h->d_lens + first,
+                                                              n, h->path_stride);
+        if ((st = h->cuda(cudaGetLastError(), "path padding"))) return st;
+        if ((st = h->cuda(cudaMemcpyAsync(out, h->d_paths + first * h->path_stride,
+                                          n * h->path_stride * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->s_compute),
+                          "paths D2H")))
+            return st;
     }
-    if (L && n) {
-        if ((st = h->cuda(cudaMemcpy(L, h->d_lens + first, n * sizeof(uint32_t), cudaMemcpyDeviceToHost),
+    if (lens && n) {
+        if ((st = h->cuda(cudaMemcpyAsync(lens, h->d_lens + first, n * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                          h->s_compute),
                           "lengths D2H")))
             return st;
     }
-    if (out && n) {
-        if ((st = h->cuda(cudaMemcpy(out, h->d_paths + first * h->path_stride,
-                                     n * h->path_stride * sizeof(uint32_t), cudaMemcpyDeviceToHost),
-                          "paths D2H")))
-            return st;
-        // The kernels write a row only up to the walk's length; the rest of
-        // the device row holds whatever the buffer held before, so the
-        // padding is made here.
-        const uint64_t stride = h->path_stride;
-        for (uint64_t i = 0; i < n; ++i) {
-            const uint64_t len = L[i] < stride ? L[i] : stride;
-            std::fill(out + i * stride + len, out + (i + 1) * stride, 0u);
-        }
-    }
-    return GW_OK;
+    return h->cuda(cudaStreamSynchronize(h->s_compute), "paths D2H");
 }
 
 extern "C" int gw_path_hashes(gw_handle *h, uint64_t first, uint64_t n, uint64_t *out)

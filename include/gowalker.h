@@ -229,6 +229,10 @@ int gw_num_walkers(gw_handle *h, uint64_t *n);
  * padded), lens = vertices per row.  Needs record_paths = GW_PATHS_FULL. */
 int gw_get_paths(gw_handle *h, uint64_t first, uint64_t n, uint32_t *out, uint32_t *lens);
 
+/* Vertices in each of walkers [first, first+n)'s paths (its steps + 1),
+ * whether or not paths were recorded. */
+int gw_path_lengths(gw_handle *h, uint64_t first, uint64_t n, uint32_t *lens);
+
 /* 64-bit FNV-1a hash of each walker's path over its 32-bit vertex ids. */
 int gw_path_hashes(gw_handle *h, uint64_t first, uint64_t n, uint64_t *out);
 

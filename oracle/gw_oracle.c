@@ -235,6 +235,9 @@ typedef struct {
     uint64_t off_sectors;    /* sectors of (beg[cur], beg[cur+1]) per step */
     uint64_t dead_ends;      /* walks stopped by the deg==0 rule */
     uint64_t terminated;     /* walks stopped by the termination draw */
+    uint64_t acc_sectors;    /* distinct sectors of the accepted trial's search of N(prev), when its
+                                verdict needed one: with the offsets and the accepted candidate, the
+                                bytes a step cannot avoid reading */
 } oracle_stats;
 
 /* Source vertex of walker `wid` (engine/walk.hpp init kernels). */
@@ -387,12 +390,17 @@ static uint32_t walk_from(const uint64_t *beg, const uint32_t *csr, const float 
                 continue;
             }
             int found;
-            if (prev != cur && ((rv < t_found) != (rv < t_notfound))) np = 1;
+            const int decides = (rv < t_found) != (rv < t_notfound);
+            if (prev != cur && decides) np = 1;
+            const uint64_t sec0 = st->search_sectors;
             if (prev == cur)
                 found = 1; /* x is drawn from N(cur) = N(prev): the search must succeed */
             else
                 found = search_sorted(csr, phead, ptail, x, &st->probes, &st->search_sectors);
-            if (found ? (rv < t_found) : (rv < t_notfound)) break;
+            if (found ? (rv < t_found) : (rv < t_notfound)) {
+                if (decides) st->acc_sectors += st->search_sectors - sec0;
+                break;
+            }
         }
         (void)pdeg;
         prev = cur;
@@ -471,6 +479,7 @@ static int walk_many(const uint64_t *beg, const uint32_t *csr, const float *apro
             stats->off_sectors += st.off_sectors;
             stats->dead_ends += st.dead_ends;
             stats->terminated += st.terminated;
+            stats->acc_sectors += st.acc_sectors;
         }
     }
     return 0;

@@ -66,6 +66,7 @@ class Stats(ctypes.Structure):
         ("off_sectors", ctypes.c_uint64),
         ("dead_ends", ctypes.c_uint64),
         ("terminated", ctypes.c_uint64),
+        ("acc_sectors", ctypes.c_uint64),
     ]
 
     def as_dict(self):
