@@ -1,22 +1,26 @@
 #!/usr/bin/env python3
 """Walk-engine benchmark: walk steps/s on one B200 (per rank), JSON on one line.
 
-Workload (default, `--config c2`): SOPR walks (reference transition rule,
-alpha 0.2), termination probability 0.15 per step, at most 20 steps, 4
-walkers per vertex, on a synthetic R-MAT graph of scale 24 (16,777,216
-vertices, edge factor 16, (a,b,c,d) = (0.57,0.19,0.19,0.05), generator seed 1,
-symmetrised, ~500 M directed edges, u32 ids, u64 offsets), in-core, walk seed
-42.  `--config c1` is the Node2vec scale-20 workload (p=2, q=0.5, length 80).
+Workload (default, `--config c3`): out-of-core Node2vec (p=0.5, q=2, length
+80, one walker per vertex, walk seed 42) on the 41.6 M-vertex, 1.47 B-edge
+directed R-MAT graph (scale 26, ids >= 41.6 M rejected, thinned to exactly
+1.47 B edges, generator seed 1), split into 64 equal-edge-mass blocks held in
+pinned host memory, device block cache capped at 1.5 GB.  Two arms run after
+one another on the same engine, K times each: GOWalker's block choice
+(plain) and the learned demand predictor (learned); value = the learned arm's
+steps/s, the plain arm beside it with both arms' H2D bytes per step, and the
+walks of both arms must be identical.
 
 One bench step = one full run of every walker of the workload (gw_run).
-  value : steps/s with the graph resident in HBM (gw_device_graph), timed with
-          CUDA events on the engine's launching stream.
-  e2e   : the same through the C ABI with the graph in pinned HOST blocks: each
-          step drops the device cache (gw_cache_reset), so the run copies the
-          CSR host->device, validates it, walks, and reads the counters back.
+Other workloads: `--config c2` (in-core SOPR, scale 24), `c1` (in-core
+Node2vec, scale 20), `c1w` (weighted), `c4`, `c5`, `c3s` (C3 at 1/16 size),
+`prep` (edge list -> CSR).  In-core lines time the graph resident in HBM
+(value) and end to end through the C ABI with the CSR copied from pinned host
+memory and the walks read back (e2e).
 
-Under torchrun each rank runs the workload with walk seed 42+rank (walkers are
-independent: no data-path collective); value = all ranks' steps / max time.
+Under torchrun every rank walks one walker-id shard of the same population
+(walkers are independent: no data-path collective); value = all ranks' steps
+/ the slowest rank's time.
 
 `--impl reference` times the oracle (the reference CPU step rule restated in
 C, OpenMP over all host threads) on a bounded sample of the same workload.
@@ -879,7 +883,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--config", default="c3", choices=sorted(WORKLOADS))
     ap.add_argument("--scale", type=int, default=None, help="override the graph scale (smaller smoke runs)")
     ap.add_argument("--paths", type=int, default=1, help="record full paths (1) or hashes only (0)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

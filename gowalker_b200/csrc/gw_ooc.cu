@@ -93,6 +93,7 @@ struct OocState {
     float *d_params_train = nullptr;
     cudaStream_t ts = nullptr;
     cudaEvent_t ev_gathered = nullptr, ev_trained = nullptr;
+    cudaGraphExec_t train_graph = nullptr;    // kTrainEpochs from a fresh initialisation + the loss read-back
     cudaGraphExec_t retrain_graph = nullptr;  // kRetrainEpochs of warm training + the loss read-back
     bool train_inflight = false;
     float *d_trace_x = nullptr, *d_trace_col = nullptr, *d_trace_y = nullptr;
@@ -185,6 +186,7 @@ void gw_handle::ooc_release()
     if (o.ev_gathered) cudaEventDestroy(o.ev_gathered);
     if (o.ev_trained) cudaEventDestroy(o.ev_trained);
     if (o.retrain_graph) cudaGraphExecDestroy(o.retrain_graph);
+    if (o.train_graph) cudaGraphExecDestroy(o.train_graph);
     for (float *p : {o.d_params, o.d_params_train, o.d_pred_res, o.d_train_ws, o.d_trace_x, o.d_trace_col, o.d_trace_y, o.d_train_x,
                      o.d_pred, o.d_emass, o.d_vfrac, o.d_prev_col, o.d_ema})
         cudaFree(p);
@@ -723,8 +725,24 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                                          : nullptr;
     bool stall_next = false;  // a learned choice moved no walker: the next decision is the plain rule's
     bool reverted = false;
-    uint64_t learned_steps = 0, learned_bytes = 0, plain_steps = 0, plain_bytes = 0;
+    // The judge: once the predictor decides, the last kJudgePlain of every
+    // kJudgePeriod iterations are decided by the plain rule, and each learned
+    // window's host-link bytes per step and time per step are compared with
+    // the plain windows on either side of it (the run's demand drifts, so
+    // only neighbouring windows are comparable).  Two losing windows in a row
+    // hand the run back to the plain rule.
+    struct JudgeWindow {
+        uint64_t steps = 0, bytes = 0;
+        double ms = 0.0;
+        uint32_t iters = 0;
+    };
+    constexpr uint32_t kJudgePeriod = 64, kJudgePlain = 16;
+    JudgeWindow win, last_learned_win, prev_plain_win;
+    int win_kind = -1;  // kind of the open window: 1 learned, 0 plain
+    bool have_learned_win = false, have_plain_win = false;
+    uint32_t judge_clock = 0, judge_losses = 0;
     uint64_t phase_steps_mark = 0, phase_bytes_mark = 0;
+    auto phase_time_mark = std::chrono::steady_clock::now();
     int last_phase = -1;
     double pred_err_sum = 0.0, persist_err_sum = 0.0;
     uint32_t pred_err_n = 0;
@@ -863,7 +881,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if (trace) cudaEventRecord(td0, ds);
         // learned: the plain rule's scores, each block's scaled by the
         // network's forecast growth of its demand
-        const bool learned_decides = learned_active && !stall_next;
+        const bool plain_window = (judge_clock % kJudgePeriod) >= kJudgePeriod - kJudgePlain;
+        const bool learned_decides = learned_active && !stall_next && !plain_window;
+        if (learned_active) judge_clock++;
         if ((st = cuda(launch_schedule(o.d_pairs, o.d_offsets + nbk, nb, o.d_cached, ncached, capacity, cfg.zero_threshold,
                                        learned_decides ? o.d_pred_res : nullptr, 1.f, o.d_dec, ds),
                        "schedule")))
@@ -918,18 +938,40 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             break;
         }
         const Decision d = *o.h_dec;
-        // judge: host-link bytes per step of each policy since it took over
+        // judge: the steps, host-link bytes and host time since the last
+        // decision belong to the window of the policy that took it
         const uint64_t steps_now = h_ctr[kCtrSteps];
-        if (last_phase >= 0) {
-            const uint64_t ds = steps_now - phase_steps_mark, db = h2d - phase_bytes_mark;
-            if (last_phase == 1) {
-                learned_steps += ds;
-                learned_bytes += db;
-            } else if (o.cached.size() >= capacity) {
-                plain_steps += ds;
-                plain_bytes += db;
+        const auto now = std::chrono::steady_clock::now();
+        if (last_phase >= 0 && o.cached.size() >= capacity && learned_iters > 0) {
+            if (last_phase != win_kind && win.iters > 0) {
+                // a window closes: a learned one waits for the plain one after it
+                if (win_kind == 1) {
+                    last_learned_win = win;
+                    have_learned_win = true;
+                } else {
+                    if (have_learned_win && have_plain_win && !reverted) {
+                        const double pb = (double)(prev_plain_win.bytes + win.bytes) /
+                                          (double)std::max<uint64_t>(prev_plain_win.steps + win.steps, 1);
+                        const double pm = (prev_plain_win.ms + win.ms) /
+                                          (double)std::max<uint64_t>(prev_plain_win.steps + win.steps, 1);
+                        const double lb = (double)last_learned_win.bytes / (double)std::max<uint64_t>(last_learned_win.steps, 1);
+                        const double lm = last_learned_win.ms / (double)std::max<uint64_t>(last_learned_win.steps, 1);
+                        judge_losses = (lb > pb || lm > 1.03 * pm) ? judge_losses + 1 : 0;
+                        if (judge_losses >= 2) reverted = true;
+                    }
+                    prev_plain_win = win;
+                    have_plain_win = true;
+                    have_learned_win = false;
+                }
+                win = JudgeWindow{};
             }
+            win_kind = last_phase;
+            win.steps += steps_now - phase_steps_mark;
+            win.bytes += h2d - phase_bytes_mark;
+            win.ms += std::chrono::duration<double, std::milli>(now - phase_time_mark).count();
+            win.iters++;
         }
+        phase_time_mark = now;
         // progress guard: a learned choice that moved no walker hands the
         // next decision to the plain rule and its rescue, which always make
         // some bucket runnable
@@ -960,12 +1002,6 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 pred_err_n++;
                 hist_pred.pop_front();
                 hist_col.pop_front();
-            }
-        }
-        if (learned_active) {
-            if (learned_iters >= 16 && plain_steps > 0 && learned_steps > 0 &&
-                (double)learned_bytes / (double)learned_steps > (double)plain_bytes / (double)plain_steps) {
-                reverted = true;  // the judge: learned moves more bytes per step than the plain rule
             }
         }
         nlive = d.live;
@@ -1099,37 +1135,30 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                     (st = cuda(cudaStreamWaitEvent(o.ts, o.ev_gathered, 0), "training wait")))
                     break;
                 launches++;
-                if (!o.trained) {
-                    // first training: from a fresh initialisation, on the stream
-                    if ((st = cuda(mlp_train(o.d_params_train, o.d_train_x, o.d_trace_y, kTraceIters * nb,
-                                             kTrainEpochs, kTrainLr, 0x6C6561726E6564ull, o.d_train_ws, nullptr, o.ts),
-                                   "predictor training")) ||
-                        (st = cuda(cudaMemcpyAsync(o.h_loss, loss_dev, sizeof(float), cudaMemcpyDeviceToHost, o.ts),
-                                   "loss")))
+                // first training from a fresh initialisation, then warm
+                // retraining of the weights in use: each a graph captured once
+                // (its pointers are the handle's fixed buffers), one launch
+                const bool first_fit = !o.trained;
+                cudaGraphExec_t &gx = first_fit ? o.train_graph : o.retrain_graph;
+                if (!gx) {
+                    cudaGraph_t g = nullptr;
+                    if ((st = cuda(cudaStreamBeginCapture(o.ts, cudaStreamCaptureModeThreadLocal), "capture"))) break;
+                    cudaError_t e1 = mlp_train(o.d_params_train, o.d_train_x, o.d_trace_y, kTraceIters * nb,
+                                               first_fit ? kTrainEpochs : kRetrainEpochs, kTrainLr,
+                                               first_fit ? 0x6C6561726E6564ull : 0ull, o.d_train_ws, nullptr, o.ts);
+                    if (e1 == cudaSuccess)
+                        e1 = cudaMemcpyAsync(o.h_loss, loss_dev, sizeof(float), cudaMemcpyDeviceToHost, o.ts);
+                    const cudaError_t e2 = cudaStreamEndCapture(o.ts, &g);
+                    if ((st = cuda(e1 != cudaSuccess ? e1 : e2, "training capture"))) {
+                        if (g) cudaGraphDestroy(g);
                         break;
-                    launches += 1 + 3 * kTrainEpochs;
-                } else {
-                    // warm retraining of the weights in use: one graph launch
-                    if (!o.retrain_graph) {
-                        cudaGraph_t g = nullptr;
-                        if ((st = cuda(cudaStreamBeginCapture(o.ts, cudaStreamCaptureModeThreadLocal), "capture")))
-                            break;
-                        cudaError_t e1 = mlp_train(o.d_params_train, o.d_train_x, o.d_trace_y, kTraceIters * nb,
-                                                   kRetrainEpochs, kTrainLr, 0ull, o.d_train_ws, nullptr, o.ts);
-                        if (e1 == cudaSuccess)
-                            e1 = cudaMemcpyAsync(o.h_loss, loss_dev, sizeof(float), cudaMemcpyDeviceToHost, o.ts);
-                        const cudaError_t e2 = cudaStreamEndCapture(o.ts, &g);
-                        if ((st = cuda(e1 != cudaSuccess ? e1 : e2, "training capture"))) {
-                            if (g) cudaGraphDestroy(g);
-                            break;
-                        }
-                        st = cuda(cudaGraphInstantiate(&o.retrain_graph, g, 0), "graph instantiate");
-                        cudaGraphDestroy(g);
-                        if (st) break;
                     }
-                    if ((st = cuda(cudaGraphLaunch(o.retrain_graph, o.ts), "predictor training"))) break;
-                    launches += 3 * kRetrainEpochs;
+                    st = cuda(cudaGraphInstantiate(&gx, g, 0), "graph instantiate");
+                    cudaGraphDestroy(g);
+                    if (st) break;
                 }
+                if ((st = cuda(cudaGraphLaunch(gx, o.ts), "predictor training"))) break;
+                launches += 1 + 3 * (first_fit ? kTrainEpochs : kRetrainEpochs);
                 if ((st = cuda(cudaEventRecord(o.ev_trained, o.ts), "event"))) break;
                 o.train_inflight = true;
                 next_train = trace_t + kRetrain;
