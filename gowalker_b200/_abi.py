@@ -57,7 +57,8 @@ class GwConfig(ctypes.Structure):
         ("strict_blocks", ctypes.c_uint32),
         ("prefetch", ctypes.c_uint32),
         ("compress_blocks", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 5),
+        ("learned_sync", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 4),
     ]
 
 

@@ -824,7 +824,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         const bool learned = policy == GW_POLICY_LEARNED;
         // a training that has finished (host-side query: never a wait) hands
         // its weights to the decisions from this iteration on
-        if (learned && o.train_inflight) {
+        const bool learned_on = learned && !reverted;  // once the judge reverts, the predictor does nothing
+        if (learned_on && o.train_inflight) {
+            if (cfg.learned_sync && (st = cuda(cudaEventSynchronize(o.ev_trained), "predictor training"))) break;
             const cudaError_t q = cudaEventQuery(o.ev_trained);
             if (q == cudaSuccess) {
                 if ((st = cuda(cudaMemcpyAsync(o.d_params, o.d_params_train, sizeof(float) * kMlpParams,
@@ -840,11 +842,12 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 cudaGetLastError();
             }
         }
-        const bool learned_active = learned && o.trained && !reverted;
-        // once trained the predictor keeps predicting (its error is measured)
-        // even after its judge has handed the choice back to the plain rule
-        const bool predicting = learned && o.trained;
-        const bool tracing = learned;  // features and demand go to the trace ring every iteration
+        const bool learned_active = learned_on && o.trained;
+        // until the judge reverts: features and demand go to the trace ring
+        // every iteration, and once trained the network forecasts (its error
+        // is measured in the windows where the plain rule decides too)
+        const bool predicting = learned_on && o.trained;
+        const bool tracing = learned_on;
         float *ring_x = o.d_trace_x + (uint64_t)(trace_t % kTraceRing) * nb * kMlpIn;
         float *ring_col = o.d_trace_col + (uint64_t)(trace_t % kTraceRing) * nb;
         if (tracing) {

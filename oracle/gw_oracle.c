@@ -892,3 +892,210 @@ int64_t oracle_sched_replay(const uint16_t *reqs, const uint32_t *nent, uint32_t
     free(live);
     return it;
 }
+
+/* ------------------------------------------------------------------ schedule study
+ *
+ * What other block policies would do on the same walks (the engine's
+ * lazy-residency rule, no prefetch): how much a better block choice or
+ * eviction could save, and what finishing the low-yield tail through mapped
+ * host memory saves.  Analysis only (the engine runs oracle_sched_replay's
+ * plain rule or its learned variant).
+ *   policy 0  GOWalker's choice (max_choose_blocks) and its rescue
+ *   policy 1  clairvoyant one-iteration yield: load the block (with the plain
+ *             rule's victim) whose load lets the walkers take the most steps
+ *             this iteration, computed exactly from the walks
+ *   policy 2  GOWalker's choice, clairvoyant eviction: evict the cached block
+ *             that the fewest waiting walkers need within their next 4 entries
+ * zt > 0: once the plain rule's best score is <= zt (the reference's zero
+ * threshold, engine/schedule.hpp:101,124 and apps/Node2vec.cu:100-108), stop
+ * loading; the remaining steps are counted in *zc_steps (they would run
+ * through mapped host memory). */
+static const uint16_t *st_reqs;
+static const uint32_t *st_nent;
+static uint32_t st_stride;
+#define SENT(w, k) (st_reqs[(uint64_t)(w) * st_stride + (k)])
+#define SBLK(w, k) ((uint32_t)(SENT(w, k) & 0x3FFFu))
+
+static uint32_t study_run(uint32_t *e, uint8_t *flag, uint32_t w, const uint8_t *res, int lazy, int commit, int *done)
+{
+    uint32_t ew = e[w], steps = 0;
+    *done = 0;
+    const uint32_t cb0 = SBLK(w, ew), pb0 = ew ? SBLK(w, ew - 1) : cb0;
+    if (!(res[cb0] && (res[pb0] || (lazy && !flag[w])))) return 0;
+    uint8_t fl = 0;
+    for (;;) {
+        const uint16_t ent = SENT(w, ew);
+        const uint32_t pb = ew ? SBLK(w, ew - 1) : (ent & 0x3FFFu);
+        if (ent & 0x4000u) {
+            *done = 1;
+            break;
+        }
+        if (!res[pb] && (!lazy || (ent & 0x8000u))) {
+            fl = 1;
+            break;
+        }
+        ew++;
+        steps++;
+        if (ew >= st_nent[w]) {
+            *done = 1;
+            break;
+        }
+        if (!res[SBLK(w, ew)]) break;
+    }
+    if (commit) {
+        e[w] = ew;
+        flag[w] = fl;
+    }
+    return steps + (uint32_t)(*done && steps == 0);
+}
+
+int64_t oracle_sched_study(const uint16_t *reqs, const uint32_t *nent, uint32_t count, uint32_t stride, uint32_t nb,
+                           uint32_t nslots, int lazy, int policy, uint64_t zt, uint64_t *loads, uint64_t *steps,
+                           uint64_t *zc_steps)
+{
+    if (nb == 0 || nb > 1024 || nslots < 2 || policy < 0 || policy > 2) return -1;
+    st_reqs = reqs;
+    st_nent = nent;
+    st_stride = stride;
+    const uint64_t nn = (uint64_t)nb * nb;
+    uint32_t *e = (uint32_t *)calloc(count, sizeof(uint32_t));
+    uint8_t *flag = (uint8_t *)calloc(count, 1);
+    uint64_t *pairs = (uint64_t *)calloc(nn, sizeof(uint64_t));
+    uint64_t *need = (uint64_t *)calloc(nb, sizeof(uint64_t));
+    uint32_t *live = (uint32_t *)malloc(sizeof(uint32_t) * (count ? count : 1));
+    uint32_t nlive = 0;
+    for (uint32_t w = 0; w < count; ++w) live[nlive++] = w;
+    uint8_t res[1024];
+    uint32_t cached[1024], ncached = 0;
+    memset(res, 0, sizeof(res));
+    *loads = *steps = *zc_steps = 0;
+    int64_t it = 0;
+    int stalled = 0; /* the last iteration moved no walker: the plain rule decides the next one */
+    for (;;) {
+        if (++it > (1 << 22)) {
+            it = -1;
+            break;
+        }
+        memset(pairs, 0, sizeof(uint64_t) * nn);
+        for (uint32_t k = 0; k < nlive; ++k) {
+            const uint32_t w = live[k], cb = SBLK(w, e[w]), pb = e[w] ? SBLK(w, e[w] - 1) : cb;
+            pairs[(uint64_t)pb * nb + cb]++;
+        }
+        if (nlive == 0) break;
+        const int full = ncached >= nslots;
+        int action, blk, pos, rblk, rpos;
+        plain_choice(pairs, nb, cached, ncached, nslots, 0, &action, &blk, &pos, &rblk, &rpos);
+        uint64_t plain_score = 0;
+        if (action) {
+            for (uint32_t j = 0; j < ncached; ++j) {
+                plain_score += pairs[(uint64_t)blk * nb + cached[j]] + pairs[(uint64_t)cached[j] * nb + blk];
+            }
+            if (full) {
+                uint64_t mn = 0xFFFFFFFFull;
+                for (uint32_t j = 0; j < ncached; ++j) {
+                    const uint64_t v = pairs[(uint64_t)blk * nb + cached[j]] + pairs[(uint64_t)cached[j] * nb + blk];
+                    if (v < mn) mn = v;
+                }
+                plain_score -= mn;
+            } else {
+                plain_score += pairs[(uint64_t)blk * nb + blk];
+            }
+        }
+        if (zt && plain_score <= zt) {
+            for (uint32_t k = 0; k < nlive; ++k) {
+                const uint32_t w = live[k];
+                *zc_steps += st_nent[w] - e[w] - ((SENT(w, st_nent[w] - 1) & 0x4000u) ? 1u : 0u);
+            }
+            break;
+        }
+        if (policy == 1 && action && !stalled) {
+            double by = -1.0;
+            int yi = -1, yp = -1;
+            for (uint32_t i = 0; i < nb; ++i) {
+                if (res[i]) continue;
+                int p = (int)ncached;
+                if (full) {
+                    uint64_t mn = 0xFFFFFFFFull;
+                    p = 0;
+                    for (uint32_t j = 0; j < ncached; ++j) {
+                        const uint64_t v = pairs[(uint64_t)i * nb + cached[j]] + pairs[(uint64_t)cached[j] * nb + i];
+                        if (v < mn) {
+                            mn = v;
+                            p = (int)j;
+                        }
+                    }
+                }
+                uint8_t r2[1024];
+                memcpy(r2, res, nb);
+                if (full) r2[cached[p]] = 0;
+                r2[i] = 1;
+                double y = 0.0;
+                int d;
+                for (uint32_t k = 0; k < nlive; ++k) {
+                    const uint32_t w = live[k], cb = SBLK(w, e[w]), pb = e[w] ? SBLK(w, e[w] - 1) : cb;
+                    if (cb == i || pb == i) y += study_run(e, flag, w, r2, lazy, 0, &d);
+                }
+                if (y > by) {
+                    by = y;
+                    yi = (int)i;
+                    yp = p;
+                }
+            }
+            if (yi >= 0 && by > 0) {
+                blk = yi;
+                pos = yp;
+            }
+        }
+        if (policy == 2 && action == 2 && !stalled) {
+            memset(need, 0, sizeof(uint64_t) * nb);
+            for (uint32_t k = 0; k < nlive; ++k) {
+                const uint32_t w = live[k];
+                for (uint32_t d = 0; d < 4 && e[w] + d < st_nent[w]; ++d) need[SBLK(w, e[w] + d)]++;
+            }
+            uint64_t mn = ~0ull;
+            for (uint32_t j = 0; j < ncached; ++j)
+                if (need[cached[j]] < mn) {
+                    mn = need[cached[j]];
+                    pos = (int)j;
+                }
+        }
+        int load = -1, lpos = -1;
+        if (action) {
+            load = blk;
+            lpos = action == 2 ? pos : -1;
+        } else if (rblk >= 0 && (ncached < nslots || rpos >= 0)) {
+            load = rblk;
+            lpos = ncached >= nslots ? rpos : -1;
+        } else {
+            it = -1;
+            break;
+        }
+        if (lpos >= 0) {
+            res[cached[lpos]] = 0;
+            cached[lpos] = (uint32_t)load;
+        } else {
+            cached[ncached++] = (uint32_t)load;
+        }
+        res[load] = 1;
+        (*loads)++;
+        uint32_t k2 = 0;
+        const uint64_t steps0 = *steps;
+        for (uint32_t k = 0; k < nlive; ++k) {
+            const uint32_t w = live[k], before = e[w];
+            int d;
+            study_run(e, flag, w, res, lazy, 1, &d);
+            *steps += e[w] - before;
+            if (!d) live[k2++] = w;
+        }
+        stalled = *steps == steps0 && k2 == nlive;
+        nlive = k2;
+    }
+    free(e);
+    free(flag);
+    free(pairs);
+    free(need);
+    free(live);
+    return it;
+}
+#undef SENT
+#undef SBLK

@@ -122,6 +122,10 @@ def lib():
                                           ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32), ctypes.c_uint64,
                                           ctypes.POINTER(SchedStats)]
         L.oracle_sched_replay.restype = ctypes.c_int64
+        L.oracle_sched_study.argtypes = [ctypes.POINTER(ctypes.c_uint16), u32p, ctypes.c_uint32, ctypes.c_uint32,
+                                         ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_uint64, u64p, u64p, u64p]
+        L.oracle_sched_study.restype = ctypes.c_int64
         L.oracle_walk_weighted.argtypes = [u64p, u32p, f32p, u32p, ctypes.c_uint32, ctypes.POINTER(Cfg),
                                            ctypes.c_uint32, ctypes.c_uint32, u32p, u32p, u64p, u32p,
                                            ctypes.POINTER(Stats), ctypes.c_int]
@@ -412,6 +416,24 @@ def sched_replay(reqs, nent, nb: int, nslots: int, prefetch: bool = True, lazy: 
     if it < 0:
         raise ValueError("schedule replay failed (bad arguments or no progress)")
     return st.as_dict(), (lg[:it].copy() if log else None)
+
+
+def sched_study(reqs, nent, nb: int, nslots: int, policy: int = 0, zero_threshold: int = 0, lazy: bool = True):
+    """Another block policy on the same walks (gw_oracle.c oracle_sched_study,
+    no prefetch): 0 GOWalker's choice, 1 clairvoyant one-iteration yield, 2
+    GOWalker's choice with clairvoyant eviction; zero_threshold > 0 stops
+    loading where the reference's zero rule does.  Returns a dict of
+    iterations, loads, steps taken by the block loads, and steps left to the
+    mapped-host tail."""
+    reqs = np.ascontiguousarray(reqs, dtype=np.uint16)
+    nent = np.ascontiguousarray(nent, dtype=np.uint32)
+    loads, steps, zc = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    it = lib().oracle_sched_study(reqs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), _p(nent, ctypes.c_uint32),
+                                  len(nent), reqs.shape[1], nb, nslots, int(lazy), policy, zero_threshold,
+                                  ctypes.byref(loads), ctypes.byref(steps), ctypes.byref(zc))
+    if it < 0:
+        raise ValueError("schedule study failed (bad arguments or no progress)")
+    return {"iterations": int(it), "loads": int(loads.value), "steps": int(steps.value), "zc_steps": int(zc.value)}
 
 
 def walk_traced(beg, csr, cfg: Cfg, wid: int, prev: int, cur: int, hop: int, cap: int = 1 << 16):

@@ -250,9 +250,13 @@ def test_trained_predictor_beats_carrying_demand_forward(gw, oracle, case):
     retrained every 16 iterations on the last 20, forecasts log1p(mean demand
     over the next 3 iterations) per block.  Both forecasts are scored by the
     engine against the realised demand (mean |error| on the log1p scale):
-    here the network's error is lower by 8-14 %.  (Its block choices do not
-    cut block loads on these graphs -- the judge hands the choice back to the
-    plain rule -- and the walks stay those of the oracle either way.)"""
+    here the network's error is lower by 8-14 %.  The run trains in step with
+    its decisions (learned_sync), so every forecast comes from the weights
+    fitted to the latest window; by default a training never delays a
+    decision and its weights arrive some iterations later.  (Its block
+    choices do not cut block loads on these graphs -- the judge hands the
+    choice back to the plain rule -- and the walks stay those of the oracle
+    either way.)"""
     from gowalker_b200.preprocess import split_equal_edge_mass
     if case == "sopr_single_source":
         beg, csr = graph(oracle, scale=13, ef=10, sym=True, cap=7000, seed=9)
@@ -264,7 +268,7 @@ def test_trained_predictor_beats_carrying_demand_forward(gw, oracle, case):
         wps, bound = 1, 0.95
     vb, eb = split_equal_edge_mass(beg, nb)
     eng = gw.WalkEngine(algorithm=algo, maxhops=maxhops, p=0.5, q=2.0, alpha=0.2, seed=5, record_paths=0,
-                        cache_size=cache_for(beg, eb, slots), **kw)
+                        cache_size=cache_for(beg, eb, slots), learned_sync=1, **kw)
     eng.set_host_graph(beg, csr, vb, eb)
     eng.init_walkers(algo, wps, 5)
     st = eng.run(gw.GW_POLICY_LEARNED)
