@@ -131,14 +131,26 @@ bool compress_block(const uint64_t *beg, const uint32_t *csr, uint32_t nv, uint6
     return true;
 }
 
+// Eight bytes of `base` from byte offset `off`, read as two aligned 32-bit
+// words (base 16-byte aligned): the low 40 bits or more are the bytes at off
+// onwards.  Neighbouring lanes read the same words, so a chunk's fields load
+// in one or two transactions instead of five byte loads per lane.
+__device__ __forceinline__ uint64_t load_bytes64(const uint8_t *__restrict__ base, uint64_t off)
+{
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(base + (off & ~3ull));
+    const uint64_t v = (uint64_t)__ldg(w) | ((uint64_t)__ldg(w + 1) << 32);
+    return v >> ((off & 3u) * 8u);
+}
+
 // Warp tasks: task t < nv decodes vertex t if it has at most 32 chunks;
 // task nv + g decodes split group g (32 chunks of a larger vertex).  Within a
 // chunk, lane i extracts delta i (lane 0 the first id) and a warp prefix sum
-// (mod 2^32) rebuilds the ids.
+// (mod 2^32) rebuilds the ids.  Every id written is checked against nverts
+// (the validation of a plain block copy, done here in the same pass).
 __global__ void k_decode_block(const uint8_t *__restrict__ src, uint64_t split_off, uint32_t nsplit,
                                uint64_t payload_off, uint64_t payload_bytes, uint32_t nv,
                                const uint64_t *__restrict__ beg, uint32_t v0, uint64_t e0, uint64_t ne,
-                               uint32_t *__restrict__ out, uint32_t *err)
+                               uint32_t nverts, uint32_t *__restrict__ out, uint32_t *err)
 {
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -146,6 +158,7 @@ __global__ void k_decode_block(const uint8_t *__restrict__ src, uint64_t split_o
     const uint32_t *split = reinterpret_cast<const uint32_t *>(src + split_off);
     const uint8_t *pay = src + payload_off;
     const uint64_t ntasks = (uint64_t)nv + nsplit;
+    bool bad_id = false;
     for (uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntasks; t += nwarps) {
         uint32_t v, c0;
         uint64_t pos;
@@ -176,8 +189,8 @@ __global__ void k_decode_block(const uint8_t *__restrict__ src, uint64_t split_o
                 bad = true;
                 break;
             }
-            const uint8_t *ch = pay + pos;
-            const uint32_t w = ch[0];
+            const uint64_t head = load_bytes64(pay, pos);  // width byte, then the first id
+            const uint32_t w = (uint32_t)head & 0xFFu;
             const uint64_t packed = ((uint64_t)(k - 1) * w + 7) >> 3;
             if (w > 32 || pos + 5 + packed > payload_bytes) {
                 bad = true;
@@ -185,12 +198,12 @@ __global__ void k_decode_block(const uint8_t *__restrict__ src, uint64_t split_o
             }
             uint32_t x = 0;
             if (lane == 0) {
-                x = (uint32_t)ch[1] | ((uint32_t)ch[2] << 8) | ((uint32_t)ch[3] << 16) | ((uint32_t)ch[4] << 24);
+                x = (uint32_t)(head >> 8);
             } else if (lane < k && w != 0) {
+                // bits [bp, bp + w) of the packed deltas: at most 39 bits from
+                // the byte holding bit bp, inside the 8-byte pad past the payload
                 const uint32_t bp = (lane - 1) * w;
-                const uint8_t *q = ch + 5 + (bp >> 3);  // up to 4 bytes past the field: the buffer is padded
-                const uint64_t acc = (uint64_t)q[0] | ((uint64_t)q[1] << 8) | ((uint64_t)q[2] << 16) |
-                                     ((uint64_t)q[3] << 24) | ((uint64_t)q[4] << 32);
+                const uint64_t acc = load_bytes64(pay, pos + 5 + (bp >> 3));
                 const uint64_t mask = (w == 32) ? 0xFFFFFFFFull : ((1ull << w) - 1);
                 const uint32_t z = (uint32_t)((acc >> (bp & 7u)) & mask);
                 x = (z >> 1) ^ (0u - (z & 1u));
@@ -200,20 +213,24 @@ __global__ void k_decode_block(const uint8_t *__restrict__ src, uint64_t split_o
                 const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
                 if (lane >= (uint32_t)o) x += y;
             }
-            if (lane < k) out[b0 - e0 + j + lane] = x;
+            if (lane < k) {
+                out[b0 - e0 + j + lane] = x;
+                bad_id |= x >= nverts;
+            }
             pos += 5 + packed;
         }
         if (bad && lane == 0) atomicOr(err, kErrBlock);
     }
+    if (__any_sync(0xFFFFFFFFu, bad_id) && lane == 0) atomicOr(err, kErrVertexRange);
 }
 
 cudaError_t launch_decode_block(const uint8_t *src, const CompressedBlock &cb, uint32_t nv, const uint64_t *beg,
-                                uint32_t v0, uint64_t e0, uint64_t ne, uint32_t *out, uint32_t *err, int num_sms,
-                                cudaStream_t s)
+                                uint32_t v0, uint64_t e0, uint64_t ne, uint32_t nverts, uint32_t *out, uint32_t *err,
+                                int num_sms, cudaStream_t s)
 {
     if (nv == 0) return cudaSuccess;
     k_decode_block<<<num_sms * 8, 256, 0, s>>>(src, cb.split_off, cb.nsplit, cb.payload_off, cb.payload_bytes, nv, beg,
-                                               v0, e0, ne, out, err);
+                                               v0, e0, ne, nverts, out, err);
     return cudaGetLastError();
 }
 

@@ -47,12 +47,13 @@ struct CompressedBlock {
 bool compress_block(const uint64_t *beg, const uint32_t *csr, uint32_t nv, uint64_t e0, uint64_t e1,
                     unsigned threads, CompressedBlock &out, std::string &why);
 
-// Decode a block copied to the device at `src` (the layout above) into `out`
-// (neighbour slot, indexed from e0).  beg: resident offsets of every vertex,
-// v0: the block's first vertex.  Any offset or payload read outside the
-// buffer sets kErrBlock in *err and skips the vertex.
+// Decode a block copied to the device at `src` (the layout above, 16-byte
+// aligned) into `out` (neighbour slot, indexed from e0).  beg: resident
+// offsets of every vertex, v0: the block's first vertex.  Any offset or
+// payload read outside the buffer sets kErrBlock in *err and skips the
+// vertex; an id >= nverts sets kErrVertexRange (the block's validation).
 cudaError_t launch_decode_block(const uint8_t *src, const CompressedBlock &cb, uint32_t nv, const uint64_t *beg,
-                                uint32_t v0, uint64_t e0, uint64_t ne, uint32_t *out, uint32_t *err, int num_sms,
-                                cudaStream_t s);
+                                uint32_t v0, uint64_t e0, uint64_t ne, uint32_t nverts, uint32_t *out, uint32_t *err,
+                                int num_sms, cudaStream_t s);
 
 }  // namespace gw

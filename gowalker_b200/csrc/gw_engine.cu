@@ -411,7 +411,7 @@ extern "C" int gw_host_weights(gw_handle *h, uint32_t blk, const float *w)
     h->weighted = all;
     h->resident = false;  // the next in-core run uploads the weights with the graph
     h->alias_ready = false;
-    h->ooc_invalidate(false);
+    h->ooc_release();  // the out-of-core slots and alias tables follow the weights
     return GW_OK;
 }
 
@@ -736,9 +736,6 @@ extern "C" int gw_run(gw_handle *h, uint32_t policy, gw_stats *stats)
     }
     if (!h->host_graph_complete())
         return h->fail(GW_ERR_STATE, "graph blocks missing: call gw_host_block for every block");
-    if (h->weighted)
-        return h->fail(GW_ERR_ARG, "weighted walks run in-core: the cache (%llu bytes) must hold the whole graph",
-                       (unsigned long long)h->cfg.cache_size);
     return h->run_ooc(policy, stats);
 }
 

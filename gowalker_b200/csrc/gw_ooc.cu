@@ -33,13 +33,22 @@ struct OocState {
     uint32_t nb = 0;
     uint32_t nslots = 0;
     uint64_t slot_csr_words = 0;
+    // words per slot: the neighbour list, then (weighted walks) the block's
+    // alias tables, one 8-byte entry per edge
+    uint64_t slot_stride_words = 0;
+    // weighted walks: every block's alias tables in pinned host memory, built
+    // on the device from its weights once per set-up and copied with the block
+    bool weighted = false;
+    std::vector<AliasEntry *> halias;
     uint64_t *d_beg = nullptr;     // offsets of every vertex (global, nverts+1): resident for the whole run
     uint32_t *slot_csr = nullptr;  // nslots * slot_csr_words: neighbour lists cached by block
     std::vector<int> slot_block;   // block held by each slot, -1 = free
     std::vector<int> block_slot;   // slot of each block, -1 = absent
     std::vector<uint32_t> cached;  // the scheduler's cached list (GOwalker_scheduler_t::buckets)
 
-    const uint32_t **h_blk_csr = nullptr;  // host block table (null = absent)
+    // block table, 2 * nb pointers: each block's neighbour list, then its
+    // alias tables (weighted walks); null = absent
+    const uint32_t **h_blk_csr = nullptr;
     const uint32_t **d_blk_csr = nullptr;  // the table the step kernels read
     // pinned copies of the table, alternating per push (a push may still be
     // in flight when the host edits the table for the next iteration), and
@@ -170,6 +179,8 @@ void gw_handle::ooc_release()
     for (void *p : o.staged) cudaFreeHost(p);
     for (auto &c : o.cblk)
         if (c.host) cudaFreeHost(c.host);
+    for (AliasEntry *p : o.halias)
+        if (p) cudaFreeHost(p);
     cudaFree(o.d_cstage[0]);
     cudaFree(o.d_cstage[1]);
     for (auto &p : o.h_snap)
@@ -258,6 +269,7 @@ static int ooc_setup(gw_handle *h)
     // a mode change of the block copies rebuilds the state; so does a set-up
     // that failed half-way
     if (h->ooc && (!h->ooc->ready || h->ooc->compressed != (h->cfg.compress_blocks != 0) ||
+                   h->ooc->weighted != h->weighted ||
                    (h->ooc->compressed && h->ooc->nstage != (h->cfg.prefetch ? 2u : 1u))))
         h->ooc_release();
     if (h->ooc && h->ooc->ready) return GW_OK;
@@ -276,7 +288,9 @@ static int ooc_setup(gw_handle *h)
     // fifth of the budget, and here an absent block's offsets stay readable.
     uint64_t beg_bytes = ((uint64_t)h->nverts + 1) * 8;
     o.slot_csr_words = (std::max<uint64_t>(maxe, 1) + 3) & ~3ull;  // keep slots 16-byte aligned
-    const uint64_t slot_bytes = o.slot_csr_words * 4;
+    o.weighted = h->weighted;
+    o.slot_stride_words = o.slot_csr_words * (o.weighted ? 3 : 1);
+    const uint64_t slot_bytes = o.slot_stride_words * 4;
     // Compressed blocks: encode every block once (host threads), and keep a
     // device buffer of the largest compressed block inside the cache budget.
     uint64_t cstage = 0;
@@ -310,11 +324,11 @@ static int ooc_setup(gw_handle *h)
         if ((st = h->cuda(cudaMalloc(&o.d_cstage[i], cstage), "compressed-block buffer"))) return st;
     beg_bytes = ((uint64_t)h->nverts + 1) * 8;
     if ((st = h->cuda(cudaMalloc(&o.d_beg, beg_bytes), "vertex offsets"))) return st;
-    if ((st = h->cuda(cudaMalloc(&o.slot_csr, o.nslots * o.slot_csr_words * 4), "slot neighbours"))) return st;
-    if ((st = h->cuda(cudaMalloc((void **)&o.d_blk_csr, nb * sizeof(void *)), "block table"))) return st;
-    if ((st = h->cuda(cudaMallocHost((void **)&o.h_blk_csr, nb * sizeof(void *)), "block table"))) return st;
+    if ((st = h->cuda(cudaMalloc(&o.slot_csr, o.nslots * o.slot_stride_words * 4), "slot neighbours"))) return st;
+    if ((st = h->cuda(cudaMalloc((void **)&o.d_blk_csr, 2 * nb * sizeof(void *)), "block table"))) return st;
+    if ((st = h->cuda(cudaMallocHost((void **)&o.h_blk_csr, 2 * nb * sizeof(void *)), "block table"))) return st;
     for (int k = 0; k < 2; ++k) {
-        if ((st = h->cuda(cudaHostAlloc((void **)&o.h_blk_pin[k], nb * sizeof(void *), cudaHostAllocMapped),
+        if ((st = h->cuda(cudaHostAlloc((void **)&o.h_blk_pin[k], 2 * nb * sizeof(void *), cudaHostAllocMapped),
                           "block table")))
             return st;
         if ((st = h->cuda(cudaHostGetDevicePointer((void **)&o.dm_blk_pin[k], (void *)o.h_blk_pin[k], 0),
@@ -477,6 +491,82 @@ struct EvRing {
     }
 };
 
+// Offsets of block b's vertices relative to its first edge (rel[v] =
+// beg[vstart + v] - estart, v <= nv): the alias builder indexes the block's
+// own edges from 0.
+__global__ void k_rel_offsets(const uint64_t *beg, uint32_t vstart, uint32_t nv, uint64_t estart, uint64_t *rel)
+{
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v <= nv; v += (uint64_t)gridDim.x * blockDim.x)
+        rel[v] = beg[vstart + v] - estart;
+}
+
+// Weighted walks: the alias tables of every block (Vose's method, the
+// in-core builder of gw_weighted.cu run block by block over the resident
+// offsets), copied into pinned host memory once; afterwards each load copies
+// a block's tables behind its neighbour list.  The scratch lives only for
+// the build.  A weight that is not positive and finite fails with
+// GW_ERR_GRAPH.
+static int ooc_build_alias(gw_handle *h, cudaStream_t s, uint64_t *h2d)
+{
+    OocState &o = *h->ooc;
+    const uint32_t nb = o.nb;
+    uint64_t maxe = 1, maxv = 1;
+    for (uint32_t b = 0; b < nb; ++b) {
+        maxe = std::max<uint64_t>(maxe, h->eblocks[b + 1] - h->eblocks[b]);
+        maxv = std::max<uint64_t>(maxv, (uint64_t)h->vblocks[b + 1] - h->vblocks[b]);
+    }
+    uint64_t *rel = nullptr;
+    float *dw = nullptr;
+    double *pd = nullptr;
+    uint32_t *q = nullptr;
+    AliasEntry *out = nullptr;
+    int st = GW_OK;
+    o.halias.assign(nb, nullptr);
+    do {
+        if ((st = h->cuda(cudaMalloc(&rel, (maxv + 1) * sizeof(uint64_t)), "alias build scratch")) ||
+            (st = h->cuda(cudaMalloc(&dw, maxe * sizeof(float)), "alias build scratch")) ||
+            (st = h->cuda(cudaMalloc(&pd, maxe * sizeof(double)), "alias build scratch")) ||
+            (st = h->cuda(cudaMalloc(&q, 2 * maxe * sizeof(uint32_t)), "alias build scratch")) ||
+            (st = h->cuda(cudaMalloc(&out, maxe * sizeof(AliasEntry)), "alias build scratch")))
+            break;
+        for (uint32_t b = 0; b < nb && !st; ++b) {
+            const uint64_t ne = h->eblocks[b + 1] - h->eblocks[b];
+            const uint32_t nv = h->vblocks[b + 1] - h->vblocks[b];
+            if (!ne) continue;
+            if ((st = h->cuda(cudaHostAlloc((void **)&o.halias[b], ne * sizeof(AliasEntry), cudaHostAllocDefault),
+                              "pinned alias tables")))
+                break;
+            k_rel_offsets<<<h->num_sms * 4, 256, 0, s>>>(o.d_beg, h->vblocks[b], nv, h->eblocks[b], rel);
+            if ((st = h->cuda(cudaGetLastError(), "alias build")) ||
+                (st = h->cuda(cudaMemcpyAsync(dw, h->host_w[b], ne * sizeof(float), cudaMemcpyHostToDevice, s),
+                              "block weights")) ||
+                (st = h->cuda(launch_build_alias(rel, dw, nv, pd, q, q + maxe, out, h->d_err, h->num_sms, s),
+                              "alias build")) ||
+                (st = h->cuda(cudaMemcpyAsync(o.halias[b], out, ne * sizeof(AliasEntry), cudaMemcpyDeviceToHost, s),
+                              "alias tables")))
+                break;
+            *h2d += ne * sizeof(float);
+            // the scratch is reused by the next block: finish this one first
+            if ((st = h->cuda(cudaStreamSynchronize(s), "alias build"))) break;
+        }
+        if (st) break;
+        uint32_t err = 0;
+        if ((st = h->cuda(cudaMemcpy(&err, h->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost), "error word"))) break;
+        if (err & kErrWeight) st = h->fail(GW_ERR_GRAPH, "an edge weight is not positive and finite");
+    } while (0);
+    cudaFree(rel);
+    cudaFree(dw);
+    cudaFree(pd);
+    cudaFree(q);
+    cudaFree(out);
+    if (st) {
+        for (AliasEntry *p : o.halias)
+            if (p) cudaFreeHost(p);
+        o.halias.clear();
+    }
+    return st;
+}
+
 int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
 {
     int st;
@@ -523,15 +613,15 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     std::fill(o.slot_block.begin(), o.slot_block.end(), -1);
     std::fill(o.block_slot.begin(), o.block_slot.end(), -1);
     o.cached.clear();
-    for (uint32_t b = 0; b < nb; ++b) o.h_blk_csr[b] = nullptr;
+    for (uint32_t b = 0; b < 2 * nb; ++b) o.h_blk_csr[b] = nullptr;
     const uint32_t **pin_last = o.h_blk_pin[0];
     uint32_t pin_last_idx = 0;
     auto push_tables = [&]() -> int {
         pin_last = o.h_blk_pin[o.pin_next];
         pin_last_idx = o.pin_next;
         o.pin_next ^= 1u;
-        memcpy((void *)pin_last, o.h_blk_csr, nb * sizeof(void *));
-        return cuda(cudaMemcpyAsync((void *)o.d_blk_csr, pin_last, nb * sizeof(void *), cudaMemcpyHostToDevice, s),
+        memcpy((void *)pin_last, o.h_blk_csr, 2 * nb * sizeof(void *));
+        return cuda(cudaMemcpyAsync((void *)o.d_blk_csr, pin_last, 2 * nb * sizeof(void *), cudaMemcpyHostToDevice, s),
                     "block table");
     };
     if ((st = push_tables())) return st;
@@ -544,20 +634,29 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     // for the re-bucketing following the decode that last read its buffer.
     auto upload_block = [&](uint32_t b, uint32_t *sc, cudaStream_t cs, uint32_t stage, uint64_t *bytes) -> int {
         const uint64_t ne = eblocks[b + 1] - eblocks[b];
+        if (o.weighted && ne) {
+            // the block's alias tables, uncompressed, behind its neighbour list
+            int e;
+            if ((e = cuda(cudaMemcpyAsync(sc + o.slot_csr_words, o.halias[b], ne * sizeof(AliasEntry),
+                                          cudaMemcpyHostToDevice, cs),
+                          "block alias tables")))
+                return e;
+        }
+        const uint64_t alias_bytes = o.weighted ? ne * sizeof(AliasEntry) : 0;
         if (!o.compressed) {
-            *bytes = ne * 4;
+            *bytes = ne * 4 + alias_bytes;
             if (!ne) return GW_OK;
             return cuda(cudaMemcpyAsync(sc, host_csr[b], ne * 4, cudaMemcpyHostToDevice, cs), "block neighbours");
         }
         const CompressedBlock &cb = o.cblk[b];
-        *bytes = cb.bytes;
+        *bytes = cb.bytes + alias_bytes;
         return cuda(cudaMemcpyAsync(o.d_cstage[stage], cb.host, cb.bytes, cudaMemcpyHostToDevice, cs), "compressed block");
     };
     auto decode_block = [&](uint32_t b, uint32_t *sc, cudaStream_t cs, uint32_t stage) -> int {
         if (!o.compressed) return GW_OK;
         launches++;
         return cuda(launch_decode_block(o.d_cstage[stage], o.cblk[b], vblocks[b + 1] - vblocks[b], o.d_beg, vblocks[b],
-                                        eblocks[b], eblocks[b + 1] - eblocks[b], sc, d_err, num_sms, cs),
+                                        eblocks[b], eblocks[b + 1] - eblocks[b], nverts, sc, d_err, num_sms, cs),
                     "block decode");
     };
     if ((st = cuda(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * kCtrCount, s), "memset"))) return st;
@@ -573,6 +672,16 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     }
     k_validate_offsets<<<num_sms * 4, 256, 0, s>>>(o.d_beg, nverts, o.d_vstart, o.d_estart, nb, d_err);
     launches++;
+    if (o.weighted) {
+        if (cfg.algorithm != GW_NODE2VEC)
+            return fail(GW_ERR_ARG, "weighted walks are Node2vec walks (algorithm %u given)", cfg.algorithm);
+        if (cfg.zero_copy && !cfg.prefetch)
+            return fail(GW_ERR_ARG, "the zero-copy tail reads unweighted blocks only");
+        if (o.halias.empty()) {
+            if ((st = ooc_build_alias(this, s, &h2d))) return st;
+            launches += 3 * nb;
+        }
+    }
 
     WalkerInit in{};
     in.mode = cfg.init_mode;
@@ -651,6 +760,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     consts_from_config(cfg, a.c);  // step constants as for the in-core kernel
     a.beg = o.d_beg;
     a.blk_csr = o.d_blk_csr;
+    a.blk_alias = o.weighted ? reinterpret_cast<const uint2 *const *>(o.d_blk_csr + nb) : nullptr;
     a.vstart = o.d_vstart;
     a.estart = o.d_estart;
     a.nb = nb;
@@ -665,7 +775,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     a.hashes = d_hashes;
     a.ctr = d_ctr;
     a.err = d_err;
-    const bool coop = needs_coop(cfg.algorithm, a.c);
+    const bool coop = !o.weighted && needs_coop(cfg.algorithm, a.c);
     // Lazy mode: a walker steps with only its current block resident until a
     // trial needs N(prev).  Node2vec thresholds do not depend on deg(prev);
     // SOPR/SOSR's do, and hard steps serve N(prev) to the whole warp, so
@@ -675,7 +785,8 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     // With prefetch the decision kernels (one CTA each) run beside the step
     // kernel: the step leaves one SM free for them, so the next block's copy
     // starts while the step runs instead of after it.
-    if (grid <= 0) grid = ooc_grid(sopr, paths, coop, cfg.prefetch && num_sms > 8 ? num_sms - 1 : num_sms);
+    if (grid <= 0)
+        grid = ooc_grid(sopr, paths, coop, cfg.prefetch && num_sms > 8 ? num_sms - 1 : num_sms, o.weighted);
 
     auto step = [&]() -> int {
         int e;
@@ -690,7 +801,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         a.order = o.w_ord[o.w_cur];
         a.keys = o.w_key[o.w_cur];
         if ((e = cuda(kring.begin(s, kernel_ms), "event"))) return e;
-        if ((e = cuda(launch_walk_ooc(a, sopr, coop, grid, s), "walk kernel"))) return e;
+        if ((e = cuda(launch_walk_ooc(a, sopr, coop, o.weighted, grid, s), "walk kernel"))) return e;
         if ((e = cuda(kring.end(s), "event"))) return e;
         launches += 2;
         return GW_OK;
@@ -784,20 +895,24 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 o.slot_block[freed] = -1;
                 o.block_slot[victim] = -1;
                 o.h_blk_csr[victim] = nullptr;
+                o.h_blk_csr[nb + victim] = nullptr;
                 o.cached[staged_pos] = (uint32_t)staged_block;
             } else {
                 o.cached.push_back((uint32_t)staged_block);
             }
             const uint32_t b = (uint32_t)staged_block;
-            uint32_t *sc = o.slot_csr + (uint64_t)staging_slot * o.slot_csr_words;
+            uint32_t *sc = o.slot_csr + (uint64_t)staging_slot * o.slot_stride_words;
             // a compressed block is expanded here, on the compute stream, so
             // the next block's copy overlaps this decode as well as the step
             if ((st = decode_block(b, sc, s, staged_stage))) break;
-            k_validate_block<<<num_sms * 4, 256, 0, s>>>(sc, eblocks[b + 1] - eblocks[b], nverts, d_err);
-            launches++;
+            if (!o.compressed) {  // a decoded block was checked by its decoder
+                k_validate_block<<<num_sms * 4, 256, 0, s>>>(sc, eblocks[b + 1] - eblocks[b], nverts, d_err);
+                launches++;
+            }
             o.slot_block[staging_slot] = (int)b;
             o.block_slot[b] = staging_slot;
             o.h_blk_csr[b] = sc;
+            o.h_blk_csr[nb + b] = o.weighted ? sc + o.slot_csr_words : nullptr;
             staging_slot = freed;
             if (staging_slot < 0)
                 for (uint32_t k = 0; k < o.nslots; ++k)
@@ -1052,7 +1167,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             // stream; it overlaps this iteration's step (everything on the
             // compute stream has finished: the decision read-back synced it)
             const uint32_t b = (uint32_t)todo.front().first;
-            uint32_t *sc = o.slot_csr + (uint64_t)staging_slot * o.slot_csr_words;
+            uint32_t *sc = o.slot_csr + (uint64_t)staging_slot * o.slot_stride_words;
             uint64_t bytes = 0;
             upload_stage ^= o.nstage == 2 ? 1u : 0u;
             staged_stage = upload_stage;
@@ -1087,6 +1202,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 slot = o.block_slot[victim];
                 o.block_slot[victim] = -1;
                 o.h_blk_csr[victim] = nullptr;
+                o.h_blk_csr[nb + victim] = nullptr;
                 o.cached[position] = (uint32_t)load_block;
             } else {
                 for (uint32_t k = 0; k < o.nslots; ++k)
@@ -1102,16 +1218,19 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             }
             const uint32_t b = (uint32_t)load_block;
             const uint64_t ne = eblocks[b + 1] - eblocks[b];
-            uint32_t *sc = o.slot_csr + (uint64_t)slot * o.slot_csr_words;
+            uint32_t *sc = o.slot_csr + (uint64_t)slot * o.slot_stride_words;
             uint64_t bytes = 0;
             if ((st = upload_block(b, sc, s, 0, &bytes)) || (st = decode_block(b, sc, s, 0))) break;
             h2d += bytes;
             loads++;
-            k_validate_block<<<num_sms * 4, 256, 0, s>>>(sc, ne, nverts, d_err);
-            launches++;
+            if (!o.compressed) {  // a decoded block was checked by its decoder
+                k_validate_block<<<num_sms * 4, 256, 0, s>>>(sc, ne, nverts, d_err);
+                launches++;
+            }
             o.slot_block[slot] = (int)b;
             o.block_slot[b] = slot;
             o.h_blk_csr[b] = sc;
+            o.h_blk_csr[nb + b] = o.weighted ? sc + o.slot_csr_words : nullptr;
         }
         if (st) break;
 

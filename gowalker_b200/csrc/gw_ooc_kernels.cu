@@ -360,7 +360,10 @@ __global__ void __launch_bounds__(1024) k_schedule(const uint32_t *__restrict__ 
     }
 }
 
-template <bool SOPR, bool PATHS, bool COOP>
+// W: weighted Node2vec -- the candidate is alias column r.x % deg, kept when
+// float(r.w >> 8) * 2^-24 < its probability, else its alias (the block's
+// alias tables sit behind its neighbour list), as in the in-core kernel.
+template <bool SOPR, bool PATHS, bool COOP, bool W = false>
 __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant__ OocStepArgs a)
 {
     __shared__ uint32_t s_vs[kMaxBlocks + 1];
@@ -384,6 +387,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
     uint32_t wid = 0, prev = 0, cur = 0, hop = 0, hop0 = 0, attempt = 0, pb = 0, cb = 0, deg = 0, pdeg = 0;
     uint64_t idx = 0, head = 0, phead = 0, h = 0;
     const uint32_t *ccsr = nullptr, *pcsr = nullptr;
+    const uint2 *calias = nullptr;  // W: the current block's alias tables
     U4 r{0, 0, 0, 0};
     StepThr t{0.f, 0.f, 0.f};
     uint32_t n_trials = 0;  // trials not yet added to s_ws
@@ -414,6 +418,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
             return;
         }
         ccsr = a.blk_csr[cb];
+        if constexpr (W) calias = a.blk_alias[cb];
         const uint64_t b0 = __ldg(a.beg + cur), b1 = __ldg(a.beg + cur + 1);
         head = b0 - a.estart[cb];
         deg = (uint32_t)(b1 - b0);
@@ -507,7 +512,12 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
 
         const uint32_t pos = r.x % deg;
         const float rv = rand_val(r.y, thr_max<SOPR>(a.c, t));
-        const uint32_t x = __ldg(ccsr + head + pos);
+        uint32_t col = pos;
+        if constexpr (W) {
+            const uint2 e = __ldg(calias + head + pos);
+            if (!(__uint2float_rn(r.w >> 8) * 0x1p-24f < __uint_as_float(e.x))) col = e.y;
+        }
+        const uint32_t x = __ldg(ccsr + head + col);
         n_trials++;
         const int verdict = pcsr != nullptr
                                 ? (accept_candidate<SOPR>(a.c, t, rv, x, prev, cur, CsrIndex{pcsr, {}, 0}, phead, pdeg) ? 1 : 0)
@@ -763,22 +773,23 @@ cudaError_t launch_schedule(const uint32_t *counts, const uint32_t *live, uint32
     return cudaGetLastError();
 }
 
-template <bool SOPR, bool PATHS, bool COOP>
+template <bool SOPR, bool PATHS, bool COOP, bool W = false>
 static int ooc_grid_for(int num_sms)
 {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_ooc<SOPR, PATHS, COOP>, kWalkThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_ooc<SOPR, PATHS, COOP, W>, kWalkThreads, 0);
     return (per_sm < 1 ? 1 : per_sm) * num_sms;
 }
 
-template <bool SOPR, bool PATHS, bool COOP>
+template <bool SOPR, bool PATHS, bool COOP, bool W = false>
 static void ooc_launch_one(const OocStepArgs &a, int grid, cudaStream_t s)
 {
-    k_walk_ooc<SOPR, PATHS, COOP><<<grid, kWalkThreads, 0, s>>>(a);
+    k_walk_ooc<SOPR, PATHS, COOP, W><<<grid, kWalkThreads, 0, s>>>(a);
 }
 
-int ooc_grid(bool sopr, bool paths, bool coop, int num_sms)
+int ooc_grid(bool sopr, bool paths, bool coop, int num_sms, bool weighted)
 {
+    if (weighted) return paths ? ooc_grid_for<false, true, false, true>(num_sms) : ooc_grid_for<false, false, false, true>(num_sms);
     const int v = (sopr ? 4 : 0) | (paths ? 2 : 0) | (coop ? 1 : 0);
     switch (v) {
     case 0: return ooc_grid_for<false, false, false>(num_sms);
@@ -792,8 +803,14 @@ int ooc_grid(bool sopr, bool paths, bool coop, int num_sms)
     }
 }
 
-cudaError_t launch_walk_ooc(const OocStepArgs &a, bool sopr, bool coop, int grid, cudaStream_t s)
+cudaError_t launch_walk_ooc(const OocStepArgs &a, bool sopr, bool coop, bool weighted, int grid, cudaStream_t s)
 {
+    if (weighted) {
+        if (sopr || coop || !a.blk_alias) return cudaErrorInvalidValue;  // weighted walks are Node2vec walks
+        if (a.paths) ooc_launch_one<false, true, false, true>(a, grid, s);
+        else ooc_launch_one<false, false, false, true>(a, grid, s);
+        return cudaGetLastError();
+    }
     const int v = (sopr ? 4 : 0) | (a.paths ? 2 : 0) | (coop ? 1 : 0);
     switch (v) {
     case 0: ooc_launch_one<false, false, false>(a, grid, s); break;

@@ -28,6 +28,7 @@ struct OocStepArgs {
     StepConsts c;
     const uint64_t *beg;             // [nverts+1] offsets of every vertex (global edge ids), resident
     const uint32_t *const *blk_csr;  // [nb] block neighbours, indexed from estart[b]; null = absent
+    const uint2 *const *blk_alias;   // [nb] weighted walks: block alias tables {prob bits, alias column}
     const uint32_t *vstart;          // [nb+1]
     const uint64_t *estart;          // [nb+1]
     uint32_t nb, nverts;
@@ -117,7 +118,7 @@ cudaError_t launch_gather_train(const float *ring_x, const float *ring_col, uint
 // level[i] = res[i] + x[i][0]
 cudaError_t launch_add_level(const float *res, const float *x, float *level, uint32_t nb, cudaStream_t s);
 
-int ooc_grid(bool sopr, bool paths, bool coop, int num_sms);
-cudaError_t launch_walk_ooc(const OocStepArgs &a, bool sopr, bool coop, int grid, cudaStream_t s);
+int ooc_grid(bool sopr, bool paths, bool coop, int num_sms, bool weighted = false);
+cudaError_t launch_walk_ooc(const OocStepArgs &a, bool sopr, bool coop, bool weighted, int grid, cudaStream_t s);
 
 }  // namespace gw

@@ -192,9 +192,13 @@ int gw_device_graph(gw_handle *h, const uint64_t *d_beg, const uint32_t *d_csr);
  * samples with them.  gw_host_weights borrows block blk's weights like
  * gw_host_block (every block with edges needs them before walks are
  * weighted); gw_device_weights gives the weights of a gw_device_graph graph
- * (NULL: unweighted again).  Weighted walks are Node2vec walks and run
- * in-core; a weight that is not positive and finite fails the run with
- * GW_ERR_GRAPH. */
+ * (NULL: unweighted again).  Weighted walks are Node2vec walks.
+ * Out-of-core, every block's alias tables are built on the device from its
+ * weights at the first run (scratch of 28 bytes per edge of the largest
+ * block, freed after) and copied behind its neighbour list with each load
+ * (8 bytes per edge, counted in h2d_bytes; the reference copies weights with
+ * every block, gpu/memory.hpp:134-137); the zero-copy tail is refused.  A
+ * weight that is not positive and finite fails the run with GW_ERR_GRAPH. */
 int gw_host_weights(gw_handle *h, uint32_t blk, const float *w);
 int gw_device_weights(gw_handle *h, const float *d_w);
 

@@ -91,7 +91,10 @@ def test_bad_weight_fails_with_graph_status(gw, oracle, bad):
     assert ei.value.status == -7
 
 
-def test_weighted_needs_node2vec_and_in_core(gw, oracle):
+def test_weighted_needs_node2vec(gw, oracle):
+    """Weighted walks are Node2vec walks, in-core and out-of-core; the
+    out-of-core zero-copy tail reads unweighted blocks only; a bad weight
+    fails an out-of-core run with the graph status too."""
     beg, csr = oracle.rmat_graph(11)
     w = np.ones(len(csr), np.float32)
     with pytest.raises(gw.GwError) as ei:
@@ -99,11 +102,61 @@ def test_weighted_needs_node2vec_and_in_core(gw, oracle):
     assert ei.value.status == -1
     from gowalker_b200.preprocess import split_equal_edge_mass
     vb, eb = split_equal_edge_mass(beg, 8)
-    eng = gw.WalkEngine(algorithm=0, maxhops=10, seed=1, walkpersource=1, cache_size=len(beg) * 8 + 4 * len(csr) // 2)
+    maxe = int(np.diff(eb.astype(np.int64)).max())
+    cache = len(beg) * 8 + 3 * ((maxe + 3) & ~3) * 12
+    for algo, zc, wv, status in ((1, 0, 1.0, -1), (0, 1, 1.0, -1), (0, 0, -1.0, -7)):
+        eng = gw.WalkEngine(algorithm=algo, maxhops=10, seed=1, walkpersource=1, cache_size=cache, zero_copy=zc)
+        eng.set_host_graph(beg, csr, vb, eb)
+        ww = w.copy()
+        ww[len(ww) // 3] = wv
+        eng.set_host_weights(ww)
+        eng.init_walkers(algo, 1, 1)
+        with pytest.raises(gw.GwError) as ei:
+            eng.run()
+        assert ei.value.status == status, (algo, zc, wv)
+        eng.close()
+
+
+@pytest.mark.parametrize("prefetch,compress,strict,slots", [(0, 0, 0, 3), (1, 1, 0, 4), (1, 0, 1, 5), (0, 1, 0, 2)])
+def test_out_of_core_weighted_matches_oracle(gw, oracle, prefetch, compress, strict, slots):
+    """Weighted Node2vec out-of-core: every block's alias tables are built on
+    the device from its weights once and copied behind its neighbour list
+    with each load (the reference copies weights with every block,
+    gpu/memory.hpp:134-137); the walks equal the oracle's weighted
+    restatement bit for bit whatever the cache size, prefetch, compression or
+    residency rule, and the H2D bytes carry the alias tables."""
+    from gowalker_b200.preprocess import split_equal_edge_mass
+    beg, csr = oracle.rmat_graph(14, 12, seed=6)
+    w = np.random.default_rng(7).lognormal(0.0, 1.0, len(csr)).astype(np.float32)
+    nb = 12
+    vb, eb = split_equal_edge_mass(beg, nb)
+    maxe = int(np.diff(eb.astype(np.int64)).max())
+    slot = ((maxe + 3) & ~3) * 12  # neighbour ids + alias tables
+    stage = 2 * (len(csr) * 4 // nb + (1 << 20)) if compress else 0
+    eng = gw.WalkEngine(algorithm=0, maxhops=25, p=0.5, q=2.0, seed=13, walkpersource=1, record_paths=1,
+                        cache_size=len(beg) * 8 + slots * slot + stage, prefetch=prefetch, compress_blocks=compress,
+                        strict_blocks=strict)
     eng.set_host_graph(beg, csr, vb, eb)
     eng.set_host_weights(w)
-    eng.init_walkers(0, 1, 1)
-    with pytest.raises(gw.GwError) as ei:
-        eng.run()
-    assert ei.value.status == -1
+    eng.init_walkers(0, 1, 13)
+    st = eng.run()
+    ref = oracle.walk(beg, csr, oracle.make_cfg(algo=0, maxhops=25, p=0.5, q=2.0, seed=13), 0, len(beg) - 1,
+                      paths=True, alias=oracle.build_alias(beg, w))
+    P, L = eng.paths()
+    assert st["block_loads"] > nb
+    assert np.array_equal(L, ref["lens"]) and np.array_equal(P, ref["paths"])
+    assert np.array_equal(eng.hashes(), ref["hashes"]) and st["steps"] == ref["stats"]["steps"]
+    # every load moves the block's alias tables (8 bytes per edge) with it
+    assert st["h2d_bytes"] > st["block_loads"] * 8 * min(np.diff(eb.astype(np.int64)))
+    # a second run reuses the tables; new weights rebuild them
+    eng.init_walkers(0, 1, 13)
+    eng.run()
+    assert np.array_equal(eng.hashes(), ref["hashes"])
+    w2 = np.ones(len(csr), np.float32)
+    eng.set_host_weights(w2)
+    eng.init_walkers(0, 1, 13)
+    eng.run()
+    ref2 = oracle.walk(beg, csr, oracle.make_cfg(algo=0, maxhops=25, p=0.5, q=2.0, seed=13), 0, len(beg) - 1,
+                       paths=False)
+    assert np.array_equal(eng.hashes(), ref2["hashes"])  # equal weights walk as unweighted
     eng.close()
