@@ -939,7 +939,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         const bool learned = policy == GW_POLICY_LEARNED;
         // a training that has finished (host-side query: never a wait) hands
         // its weights to the decisions from this iteration on
-        const bool learned_on = learned && !reverted;  // once the judge reverts, the predictor does nothing
+        // once the judge reverts, the predictor does nothing -- except in the
+        // evaluation mode (learned_sync), where it keeps forecasting and its
+        // forecasts keep being scored
+        const bool learned_on = learned && (!reverted || cfg.learned_sync);
         if (learned_on && o.train_inflight) {
             if (cfg.learned_sync && (st = cuda(cudaEventSynchronize(o.ev_trained), "predictor training"))) break;
             const cudaError_t q = cudaEventQuery(o.ev_trained);
@@ -957,7 +960,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 cudaGetLastError();
             }
         }
-        const bool learned_active = learned_on && o.trained;
+        const bool learned_active = learned_on && o.trained && !reverted;
         // until the judge reverts: features and demand go to the trace ring
         // every iteration, and once trained the network forecasts (its error
         // is measured in the windows where the plain rule decides too)

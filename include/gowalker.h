@@ -103,10 +103,12 @@ typedef struct gw_config {
     uint32_t compress_blocks; /* out-of-core: 1 = keep a compressed copy of every block's neighbour
                                  lists in pinned host memory (chunks of 32 ids, bit-packed deltas),
                                  copy that and decode it on the device: fewer host-link bytes */
-    uint32_t learned_sync;    /* learned policy: 1 = a decision waits for the predictor's training in
-                                 flight and uses its weights at once (fresher forecasts, decisions
-                                 that wait); 0 = training never delays a decision (weights adopted
-                                 when a training has finished) */
+    uint32_t learned_sync;    /* learned policy: 1 = evaluation mode: a decision waits for the
+                                 predictor's training in flight and uses its weights at once, and
+                                 the forecasts go on (and are scored) after the judge hands the run
+                                 back to the plain rule; 0 = training never delays a decision
+                                 (weights adopted when a training has finished) and the predictor
+                                 stops once reverted */
     uint32_t reserved[4];
 } gw_config;
 
