@@ -746,6 +746,34 @@ def run_ours(args, wl):
     ms = e0.elapsed_time(e1)
     hash_sum, steps_last = eng.checksum()
 
+    # ---- the plain form for comparison: one launch per hop, same walks
+    hop_arm = None
+    if args.launch_per_hop:
+        eng3 = gw.WalkEngine(**dict(cfgkw, launch_mode=gw.GW_LAUNCH_PER_HOP))
+        eng3.set_device_graph(dg.nverts, dg.nedges, dg.beg_ptr, dg.csr_ptr)
+        stream3 = torch.cuda.ExternalStream(eng3.stream_handle(), device=local)
+        for _ in range(args.warmup):
+            eng3.init_walkers(wl["algo"], wl["wps"], seed, first=first, count=count)
+            eng3.run()
+        barrier()
+        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        h0.record(stream3)
+        hop_steps = hop_kernel_ms = 0
+        for _ in range(args.steps):
+            eng3.init_walkers(wl["algo"], wl["wps"], seed, first=first, count=count)
+            st3 = eng3.run()
+            hop_steps += st3["steps"]
+            hop_kernel_ms += st3["kernel_ms"]
+        h1.record(stream3)
+        barrier()
+        hop_ms = h0.elapsed_time(h1)
+        hop_hash, _ = eng3.checksum()
+        eng3.close()
+        hop_ms, _, hop_all, _ = reduce_rank_times(dist, hop_ms, 0.0, hop_steps, 0, "cuda")
+        hop_arm = {"value": hop_all / (hop_ms / 1000.0), "unit": "steps/s", "ms_per_run": hop_ms / args.steps,
+                   "kernel_ms_per_run": hop_kernel_ms / args.steps, "launches_per_run": wl["maxhops"],
+                   "same_walks": hop_hash == hash_sum}
+
     # ---- end to end through the C ABI: host blocks in, the walks out
     beg_t, csr_t, beg, csr = host_graph(dg)
     eng2 = gw.WalkEngine(**cfgkw)
@@ -822,6 +850,9 @@ def run_ours(args, wl):
             "hard_steps": {"by_position": coop[0] // args.steps, "by_position_attempts": coop[1] // args.steps,
                            "by_search": coop[2] // args.steps, "by_search_attempts": coop[3] // args.steps},
         }
+        if hop_arm is not None:
+            hop_arm["persistent_over_per_hop"] = value / hop_arm["value"]
+            line["one_launch_per_hop"] = hop_arm
         gold = golden_checksum(args.config)
         if gold is not None and "path_hash_sum" in gold:
             line["checksum"]["oracle_path_hash_sum"] = int(gold["path_hash_sum"])
@@ -893,6 +924,9 @@ def main():
                          "one of GOWalker's rule, the learned predictor, SOWalker's annealing")
     ap.add_argument("--no-compress", action="store_true",
                     help="out-of-core: copy plain neighbour lists (default: compressed, decoded on the device)")
+    ap.add_argument("--launch-per-hop", action="store_true",
+                    help="in-core: also time the plain one-launch-per-hop form (same walks) beside the persistent "
+                         "kernel")
     ap.add_argument("--no-prefetch", action="store_true",
                     help="out-of-core: take each block choice in its own iteration (default: one iteration "
                          "ahead, the copy overlapped with the step)")

@@ -18,6 +18,7 @@ GW_POLICY_PLAIN, GW_POLICY_LEARNED, GW_POLICY_SA = 0, 1, 2
 GW_PATHS_NONE, GW_PATHS_FULL = 0, 1
 GW_EDGES_SYMMETRIC, GW_EDGES_SORT, GW_EDGES_DEDUP = 1, 2, 4
 GW_SPLIT_REFERENCE, GW_SPLIT_EQUAL_EDGES = 0, 1
+GW_LAUNCH_PERSISTENT, GW_LAUNCH_PER_HOP = 0, 1
 
 # Every symbol include/gowalker.h declares.
 EXPORTS = (
@@ -58,7 +59,8 @@ class GwConfig(ctypes.Structure):
         ("prefetch", ctypes.c_uint32),
         ("compress_blocks", ctypes.c_uint32),
         ("learned_sync", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 4),
+        ("launch_mode", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 3),
     ]
 
 

@@ -65,6 +65,7 @@ static bool config_ok(const gw_config &c, std::string &why)
     if (!(c.term_prob >= 0.0f) || !(c.term_prob < 1.0f)) { why = "term_prob must lie in [0, 1)"; return false; }
     if (c.init_mode > GW_INIT_RANDOM) { why = "unknown init_mode"; return false; }
     if (c.record_paths > GW_PATHS_FULL) { why = "unknown record_paths"; return false; }
+    if (c.launch_mode > GW_LAUNCH_PER_HOP) { why = "unknown launch_mode"; return false; }
     if (c.threadperblock != 0 && (c.threadperblock % 32 != 0 || c.threadperblock > 1024)) {
         why = "threadperblock must be a multiple of 32 up to 1024";
         return false;
@@ -630,6 +631,61 @@ int gw_handle::run_incore(gw_stats *stats)
     const bool sopr = cfg.algorithm != GW_NODE2VEC;
     const bool coop = !weighted && needs_coop(cfg.algorithm, a.c);
     a.alias = weighted ? reinterpret_cast<const uint2 *>(d_alias) : nullptr;
+    if (cfg.launch_mode == GW_LAUNCH_PER_HOP) {
+        // ---- the plain form: one launch per hop, walker state in memory
+        if (weighted) return fail(GW_ERR_ARG, "one launch per hop runs unweighted walks only");
+        HopState hs{};
+        const uint64_t n = nwalkers;
+        int rc = GW_OK;
+        if ((rc = cuda(cudaMalloc(&hs.prev, n * 4), "hop state")) || (rc = cuda(cudaMalloc(&hs.cur, n * 4), "hop state")) ||
+            (rc = cuda(cudaMalloc(&hs.hop, n * 4), "hop state")) || (rc = cuda(cudaMalloc(&hs.hash, n * 8), "hop state"))) {
+            cudaFree(hs.prev);
+            cudaFree(hs.cur);
+            cudaFree(hs.hop);
+            cudaFree(hs.hash);
+            return rc;
+        }
+        const uint32_t rounds = cfg.maxhops ? cfg.maxhops : 1;
+        if (!(rc = cuda(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * kCtrCount, s), "memset")) &&
+            !(rc = cuda(cudaEventRecord(ev_kernel0, s), "event"))) {
+            for (uint32_t k = 0; k < rounds && !rc; ++k) rc = cuda(launch_walk_hop(a, hs, sopr, k, num_sms, s), "hop launch");
+        }
+        if (!rc && !(rc = cuda(cudaEventRecord(ev_kernel1, s), "event")) &&
+            !(rc = cuda(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(unsigned long long) * kCtrCount, cudaMemcpyDeviceToHost, s),
+                        "counters D2H")) &&
+            !(rc = cuda(cudaMemcpyAsync(h_ctr + kCtrCount, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
+                        "error word D2H")) &&
+            !(rc = cuda(cudaEventRecord(ev_stop, s), "event")))
+            rc = cuda(cudaStreamSynchronize(s), "walk");
+        cudaStreamSynchronize(s);
+        cudaFree(hs.prev);
+        cudaFree(hs.cur);
+        cudaFree(hs.hop);
+        cudaFree(hs.hash);
+        if (rc) return rc;
+        last_hash_sum = h_ctr[kCtrHashSum];
+        last_steps = h_ctr[kCtrSteps];
+        if (stats) {
+            memset(stats, 0, sizeof(*stats));
+            stats->steps = h_ctr[kCtrSteps];
+            stats->trials = h_ctr[kCtrTrials];
+            stats->walkers = h_ctr[kCtrDone];
+            stats->h2d_bytes = h2d;
+            stats->d2h_bytes = sizeof(unsigned long long) * kCtrCount + sizeof(uint32_t);
+            stats->block_loads = h2d ? nblocks : 0;
+            stats->iterations = rounds;
+            stats->launches = rounds;
+            stats->kernel_variant = 0xFFFFFFFFu;
+            cudaEventElapsedTime(&stats->kernel_ms, ev_kernel0, ev_kernel1);
+            cudaEventElapsedTime(&stats->total_ms, ev_start, ev_stop);
+        }
+        const uint32_t errw = (uint32_t)h_ctr[kCtrCount];
+        if (errw) return fail(GW_ERR_DEVICE, "walk kernel error word 0x%x", errw);
+        if (h_ctr[kCtrDone] != nwalkers)
+            return fail(GW_ERR_DEVICE, "per-hop walk finished %llu of %llu walkers", (unsigned long long)h_ctr[kCtrDone],
+                        (unsigned long long)nwalkers);
+        return GW_OK;
+    }
     // kernel class for the autotuner: (sopr, paths, coop), weighted Node2vec apart
     const int combo = weighted ? 8 | (a.paths ? 2 : 0) : (sopr ? 4 : 0) | (a.paths ? 2 : 0) | (coop ? 1 : 0);
     auto grid_of = [&](int v, bool paths_on) {

@@ -111,6 +111,16 @@ cudaError_t launch_walk_incore(const IncoreArgs &a, bool sopr, bool coop, int va
 int incore_grid_weighted(bool paths, int variant, int num_sms);
 cudaError_t launch_walk_incore_weighted(const IncoreArgs &a, int variant, int grid, cudaStream_t s);
 
+// One launch per hop (gw_walk_hop.cu): walker state between launches.
+struct HopState {
+    uint32_t *prev, *cur, *hop;
+    uint64_t *hash;
+};
+// Launch `round` (0 .. maxhops-1) of the one-launch-per-hop walk: round 0
+// starts every walker; each advances every live walker by one step.
+cudaError_t launch_walk_hop(const IncoreArgs &a, const HopState &st, bool sopr, uint32_t round, int num_sms,
+                            cudaStream_t s);
+
 // Whether a run needs the warp-cooperative path for hard steps: always for
 // SOPR/SOSR (acceptance ~ deg(prev)/deg(cur) next to hubs); for Node2vec
 // only when max/min of {1/p, 1/q, 1} exceeds 8 (otherwise a step accepts

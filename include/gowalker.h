@@ -109,8 +109,15 @@ typedef struct gw_config {
                                  back to the plain rule; 0 = training never delays a decision
                                  (weights adopted when a training has finished) and the predictor
                                  stops once reverted */
-    uint32_t reserved[4];
+    uint32_t launch_mode;     /* in-core: GW_LAUNCH_PERSISTENT (default) or GW_LAUNCH_PER_HOP, the
+                                 plain form kept for comparison (unweighted walks only) */
+    uint32_t reserved[3];
 } gw_config;
+
+/* in-core launch modes */
+#define GW_LAUNCH_PERSISTENT 0u /* one persistent work-stealing kernel runs every walker to the end */
+#define GW_LAUNCH_PER_HOP 1u    /* one launch per hop, a thread per walker (the reference's grid-stride
+                                   loop, gpu/gpuwalk.hpp:193-205, cut at each hop); same walks */
 
 /* Per-run counters. */
 typedef struct gw_stats {

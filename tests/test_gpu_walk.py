@@ -345,3 +345,27 @@ def test_path_rows_zero_padded_after_longer_walks(gw, oracle):
     assert (L < 21).any()
     assert np.array_equal(L, ref["lens"]) and np.array_equal(P, ref["paths"])
     eng.close()
+
+
+@pytest.mark.parametrize("algo,maxhops,term,p,q,wps", [(0, 30, 0.0, 2.0, 0.5, 1), (1, 20, 0.15, 0.5, 2.0, 2),
+                                                      (2, 15, 0.15, 0.5, 2.0, 1), (0, 25, 0.0, 0.05, 20.0, 1)])
+def test_one_launch_per_hop_same_walks(gw, oracle, algo, maxhops, term, p, q, wps):
+    """The plain one-launch-per-hop form (GW_LAUNCH_PER_HOP: a thread per
+    walker, one launch per hop, state in memory) walks exactly the walks of
+    the persistent work-stealing kernel and of the oracle: paths, lengths,
+    hashes, steps and trials."""
+    beg, csr = oracle.rmat_graph(13, 16, seed=8)
+    runs = {}
+    for mode in (0, 1):
+        eng, st = run_engine(gw, beg, csr, algo, maxhops, wps=wps, p=p, q=q, term=term, seed=21, launch_mode=mode)
+        runs[mode] = (eng.paths(), eng.hashes(), st)
+        eng.close()
+    (P0, L0), H0, s0 = runs[0]
+    (P1, L1), H1, s1 = runs[1]
+    assert np.array_equal(P0, P1) and np.array_equal(L0, L1) and np.array_equal(H0, H1)
+    assert (s0["steps"], s0["trials"]) == (s1["steps"], s1["trials"])
+    assert s1["launches"] == maxhops
+    V = len(beg) - 1
+    ref = oracle.walk(beg, csr, oracle_cfg(oracle, algo, maxhops, wps, p, q, term=term, seed=21), 0, V * wps,
+                      paths=False)
+    assert np.array_equal(H1, ref["hashes"])
