@@ -739,6 +739,7 @@ def run_ours(args, wl):
         kernel_ms += st["kernel_ms"]
         trials += st["trials"]
         variant = st["kernel_variant"]
+        chunk = st["walker_chunk"]
         launches += st["launches"]
     e1.record(stream)
     barrier()
@@ -847,6 +848,7 @@ def run_ours(args, wl):
             "checksum": {"path_hash_sum": pop_hash, "steps_per_run": pop_steps},
             "trials_per_step": trials / max(steps, 1),
             "kernel_variant": variant,
+            "walker_chunk": chunk,
             "hard_steps": {"by_position": coop[0] // args.steps, "by_position_attempts": coop[1] // args.steps,
                            "by_search": coop[2] // args.steps, "by_search_attempts": coop[3] // args.steps},
         }

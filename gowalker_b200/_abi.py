@@ -84,7 +84,7 @@ class GwStats(ctypes.Structure):
         ("kernel_variant", ctypes.c_uint32),
         ("persist_error", ctypes.c_float),
         ("bucket_ms", ctypes.c_float),
-        ("reserved", ctypes.c_uint32 * 1),
+        ("walker_chunk", ctypes.c_uint32),
         ("coop_small_steps", ctypes.c_uint64),
         ("coop_small_attempts", ctypes.c_uint64),
         ("coop_large_steps", ctypes.c_uint64),

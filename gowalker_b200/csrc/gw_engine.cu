@@ -695,26 +695,33 @@ int gw_handle::run_incore(gw_stats *stats)
         return weighted ? launch_walk_incore_weighted(x, v, g, s) : launch_walk_incore(x, sopr, coop, v, g, s);
     };
     int variant = tuned_variant[combo];
+    // Walkers per warp claim: few lanes idle at the end of a run with small
+    // claims, fewer atomics with large ones; the autotuner picks among these.
+    static const uint32_t kChunks[] = {16, 64, 256};
     if (cfg.blockpergrid == 0 && variant < 0) {
-        // Autotuner: time each register-cap variant on this run's walkers
-        // (their outputs are rewritten by the full run below) and keep the
-        // fastest for every later run of this kernel class.  Runs of up to
-        // 2^22 walkers are timed whole: with few walkers per lane the tail of
-        // the last round decides, and a part of the run would misrank the
-        // variants.  Larger runs are timed on every 16th walker id, which
-        // keeps the run's mix of source degrees (R-MAT ids are not random in
-        // degree, so a contiguous range would not).  Variants run in a
-        // forward then a reverse pass and keep their best time, so none
-        // gains from the caches the previous one warmed.
+        // Autotuner: time each register-cap variant with each claim size on
+        // this run's walkers (their outputs are rewritten by the full run
+        // below) and keep the fastest pair for every later run of this kernel
+        // class.  Runs of up to 2^22 walkers are timed whole: with few walkers
+        // per lane the tail of the last round decides, and a part of the run
+        // would misrank the candidates.  Larger runs are timed on every 16th
+        // walker id, which keeps the run's mix of source degrees (R-MAT ids
+        // are not random in degree, so a contiguous range would not).  The
+        // candidates run in a forward then a reverse pass and keep their best
+        // time, so none gains from the caches the previous one warmed.
         const uint32_t stride = nwalkers > (1ull << 22) ? 16u : 1u;
         IncoreArgs c = a;
         c.wid_base = wid_first;
         c.wid_stride = stride;
         c.nwalkers = (uint32_t)(nwalkers / stride);
+        constexpr int kCand = kIncoreVariants * 3;
         float best = 1e30f;
-        for (int v = 0; v < kIncoreVariants; ++v) tuned_ms[combo][v] = 1e30f;
-        for (int i = 0; i < 2 * kIncoreVariants; ++i) {
-            const int v = i < kIncoreVariants ? i : 2 * kIncoreVariants - 1 - i;
+        float cand_ms[kCand];
+        for (float &m : cand_ms) m = 1e30f;
+        for (int i = 0; i < 2 * kCand; ++i) {
+            const int k = i < kCand ? i : 2 * kCand - 1 - i;
+            const int v = k / 3;
+            c.chunk = kChunks[k % 3];
             if ((st = cuda(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * kCtrCount, s), "memset"))) return st;
             if ((st = cuda(cudaEventRecord(ev_kernel0, s), "event"))) return st;
             if ((st = cuda(launch(c, v, grid_of(v, c.paths != nullptr)), "walk kernel launch (tuning)")))
@@ -723,16 +730,21 @@ int gw_handle::run_incore(gw_stats *stats)
             if ((st = cuda(cudaEventSynchronize(ev_kernel1), "tuning"))) return st;
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ev_kernel0, ev_kernel1);
-            tuned_ms[combo][v] = std::min(tuned_ms[combo][v], ms);
-            if (ms < best) {
-                best = ms;
-                variant = v;
+            cand_ms[k] = std::min(cand_ms[k], ms);
+        }
+        for (int k = 0; k < kCand; ++k) {
+            tuned_ms[combo][k / 3] = std::min(k % 3 == 0 ? 1e30f : tuned_ms[combo][k / 3], cand_ms[k]);
+            if (cand_ms[k] < best) {
+                best = cand_ms[k];
+                variant = k / 3;
+                tuned_chunk[combo] = kChunks[k % 3];
             }
         }
         tuned_variant[combo] = variant;
     }
     if (variant < 0) variant = 1;
     last_variant = variant;
+    a.chunk = tuned_chunk[combo] ? tuned_chunk[combo] : kChunk;
     if ((st = cuda(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long) * kCtrCount, s), "memset"))) return st;
     int grid = (int)cfg.blockpergrid;
     if (grid <= 0) grid = grid_of(variant, a.paths != nullptr);
@@ -761,6 +773,7 @@ int gw_handle::run_incore(gw_stats *stats)
         stats->iterations = 1;
         stats->launches = 1;
         stats->kernel_variant = (uint32_t)variant;
+        stats->walker_chunk = a.chunk;
         stats->coop_small_steps = h_ctr[kCtrCoopSmall];
         stats->coop_small_attempts = h_ctr[kCtrCoopSmallAtt];
         stats->coop_large_steps = h_ctr[kCtrCoopLarge];

@@ -82,6 +82,7 @@ struct gw_handle {
     // (sopr, paths, coop) and the measured times of each variant
     int tuned_variant[16] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
     float tuned_ms[16][gw::kIncoreVariants] = {};
+    uint32_t tuned_chunk[16] = {};  // walkers per warp claim the autotuner picked per kernel class
     int last_variant = -1;
 
     // out-of-core state (gw_ooc.cu)

@@ -73,6 +73,7 @@ struct IncoreArgs {
     uint32_t wid_base;
     uint32_t wid_stride;       // 1 for a run; > 1 for the autotuner's sample
     uint32_t out_base;         // first walker id of the population: outputs are indexed by wid - out_base
+    uint32_t chunk;            // walkers a warp claims per atomic (0: kChunk); the autotuner picks it
     uint32_t *paths;           // rows indexed by walker id, or null
     uint32_t stride;           // maxhops + 1
     uint32_t *lens;            // vertices per path

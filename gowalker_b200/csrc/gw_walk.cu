@@ -44,6 +44,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const __grid
     const uint64_t *__restrict__ beg = a.beg;
     const uint32_t *__restrict__ csr = a.ix.csr;
     const uint32_t maxhops = a.c.maxhops;
+    const uint32_t chunk = a.chunk ? a.chunk : kChunk;
 
     uint32_t q_next = 0, q_end = 0;  // warp-uniform claimed range
     bool exhausted = false;          // warp-uniform
@@ -80,14 +81,14 @@ __global__ void __launch_bounds__(kWalkThreads, MINB) k_walk_incore(const __grid
             if (need == 0 || exhausted) break;
             if (q_next >= q_end) {
                 unsigned long long base = 0;
-                if (lane == 0) base = atomicAdd(&a.ctr[kCtrCursor], (unsigned long long)kChunk);
+                if (lane == 0) base = atomicAdd(&a.ctr[kCtrCursor], (unsigned long long)chunk);
                 base = __shfl_sync(0xFFFFFFFFu, base, 0);
                 if (base >= a.nwalkers) {
                     exhausted = true;
                     break;
                 }
                 q_next = (uint32_t)base;
-                q_end = (uint32_t)min(base + kChunk, (unsigned long long)a.nwalkers);
+                q_end = (uint32_t)min(base + chunk, (unsigned long long)a.nwalkers);
             }
             const uint32_t avail = q_end - q_next;
             const uint32_t rank = __popc(need & lt_mask);

@@ -141,7 +141,7 @@ typedef struct gw_stats {
     float persist_error;         /* learned: the same error of the forecast without the network
                                     (this iteration's demand carried forward) */
     float bucket_ms;             /* out-of-core: time re-bucketing walkers (CUDA events) */
-    uint32_t reserved[1];
+    uint32_t walker_chunk;       /* in-core: walkers a warp claims per atomic (the autotuner's pick) */
     uint64_t coop_small_steps;   /* hard steps decided from candidate positions (in-core) */
     uint64_t coop_small_attempts;
     uint64_t coop_large_steps;   /* hard steps evaluated with candidate loads (in-core) */
