@@ -20,6 +20,7 @@ enum Counter : int {
     kCtrCoopSmallAtt = 6,  // attempts those steps took
     kCtrCoopLarge = 7,     // hard steps evaluated with candidate loads and searches
     kCtrCoopLargeAtt = 8,  // attempts those steps took
+    kCtrZcSectors = 9,     // out-of-core zero-copy tail: 32-byte sectors read from mapped host memory
     kCtrCount = 12
 };
 

@@ -87,6 +87,7 @@ struct OocState {
     bool compressed = false;
     std::vector<CompressedBlock> cblk;
     uint8_t *d_cstage[2] = {nullptr, nullptr};  // prefetch uploads alternate: one may wait for its decode
+    uint8_t *d_mapped = nullptr;                // zero-copy tail: 1 per block read through mapped host memory
     uint32_t nstage = 0;
 
     bool ready = false;
@@ -181,6 +182,7 @@ void gw_handle::ooc_release()
         if (c.host) cudaFreeHost(c.host);
     for (AliasEntry *p : o.halias)
         if (p) cudaFreeHost(p);
+    cudaFree(o.d_mapped);
     cudaFree(o.d_cstage[0]);
     cudaFree(o.d_cstage[1]);
     for (auto &p : o.h_snap)
@@ -675,8 +677,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     if (o.weighted) {
         if (cfg.algorithm != GW_NODE2VEC)
             return fail(GW_ERR_ARG, "weighted walks are Node2vec walks (algorithm %u given)", cfg.algorithm);
-        if (cfg.zero_copy && !cfg.prefetch)
-            return fail(GW_ERR_ARG, "the zero-copy tail reads unweighted blocks only");
+        if (cfg.zero_copy) return fail(GW_ERR_ARG, "the zero-copy tail reads unweighted blocks only");
         if (o.halias.empty()) {
             if ((st = ooc_build_alias(this, s, &h2d))) return st;
             launches += 3 * nb;
@@ -1133,19 +1134,36 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             todo.emplace_back(d.block, d.action == 2 ? d.position : -1);
             last_phase = learned_decides ? 1 : 0;
             if (learned_decides) learned_iters++;
-        } else if (cfg.zero_copy && !prefetch) {
-            // ---- zero-copy tail: every absent block read through mapped host memory
+        } else if (cfg.zero_copy) {
+            // ---- zero-copy tail (GOWalker's zero mode, engine/engine.hpp:593-634):
+            // no block scores above zero_threshold, so every remaining walker
+            // runs to its end reading the absent blocks through mapped host
+            // memory; those reads are counted (32-byte sectors) into h2d_bytes.
+            // With prefetch this iteration's step has run already.
             if ((st = ooc_map_host(this))) break;
+            std::vector<uint8_t> mapped(nb, 0);
             for (uint32_t b = 0; b < nb; ++b)
-                if (o.block_slot[b] < 0) o.h_blk_csr[b] = o.map_csr[b];
+                if (o.block_slot[b] < 0) {
+                    o.h_blk_csr[b] = o.map_csr[b];
+                    mapped[b] = 1;
+                }
+            if (!o.d_mapped && (st = cuda(cudaMalloc(&o.d_mapped, nb), "mapped-block flags"))) break;
+            if ((st = cuda(cudaMemcpyAsync(o.d_mapped, mapped.data(), nb, cudaMemcpyHostToDevice, s), "mapped flags")))
+                break;
             if ((st = push_tables())) break;
             unsigned long long before[kCtrCount];
-            memcpy(before, h_ctr, sizeof(before));
-            if ((st = step())) break;
+            if ((st = cuda(cudaMemcpyAsync(before, d_ctr, sizeof(before), cudaMemcpyDeviceToHost, s), "counters")) ||
+                (st = cuda(cudaStreamSynchronize(s), "counters")))
+                break;
+            a.mapped = o.d_mapped;
+            st = step();
+            a.mapped = nullptr;
+            if (st) break;
             if ((st = cuda(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(before), cudaMemcpyDeviceToHost, s), "counters")))
                 break;
             if ((st = cuda(cudaStreamSynchronize(s), "zero-copy"))) break;
             zc_steps += h_ctr[kCtrSteps] - before[kCtrSteps];
+            h2d += 32ull * (h_ctr[kCtrZcSectors] - before[kCtrZcSectors]);
             // restore the table to device slots only
             for (uint32_t b = 0; b < nb; ++b)
                 if (o.block_slot[b] < 0) o.h_blk_csr[b] = nullptr;

@@ -363,10 +363,21 @@ __global__ void __launch_bounds__(1024) k_schedule(const uint32_t *__restrict__ 
 // W: weighted Node2vec -- the candidate is alias column r.x % deg, kept when
 // float(r.w >> 8) * 2^-24 < its probability, else its alias (the block's
 // alias tables sit behind its neighbour list), as in the in-core kernel.
-template <bool SOPR, bool PATHS, bool COOP, bool W = false>
+// ZC: the zero-copy tail -- the blocks marked in a.mapped are read through
+// mapped host memory; every read of one is counted as a 32-byte sector in
+// kCtrZcSectors (an upper bound of the host-link bytes: each probe of a
+// binary search counts as its own sector).
+template <bool SOPR, bool PATHS, bool COOP, bool W = false, bool ZC = false>
 __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant__ OocStepArgs a)
 {
     __shared__ uint32_t s_vs[kMaxBlocks + 1];
+    __shared__ uint8_t s_mapped[ZC ? kMaxBlocks : 1];
+    if constexpr (ZC)
+        for (uint32_t i = threadIdx.x; i < a.nb; i += blockDim.x) s_mapped[i] = a.mapped[i];
+    uint32_t zc_sectors = 0;
+    // sectors of a plain binary search over n ids plus the final read: at most
+    // bit_length(n) + 1
+    auto search_sectors = [](uint32_t n) { return 33u - (uint32_t)__clz(n); };
     __shared__ uint32_t s_iv[kWalkThreads / 32][kCoopScratchWords];
     __shared__ unsigned long long s_ws[kWalkThreads / 32][kWsCount];  // per-warp statistics
     for (uint32_t i = threadIdx.x; i <= a.nb; i += blockDim.x) s_vs[i] = a.vstart[i];
@@ -499,6 +510,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
                 __shfl_sync(0xFFFFFFFFu, cur, L), pix, ph, __shfl_sync(0xFFFFFFFFu, pdeg, L), s_iv[warp], &xs);
             if (lane == (uint32_t)L) {
                 n_trials += astar - p0;
+                if constexpr (ZC)  // every attempt: a candidate and, at most, a search of N(prev)
+                    zc_sectors += (astar - p0) * ((s_mapped[cb] ? 1u : 0u) + (s_mapped[pb] ? search_sectors(pdeg) : 0u));
                 if (astar >= kMaxAttempts) {
                     atomicOr(a.err, kErrTrials);
                     finish();
@@ -519,6 +532,13 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
         }
         const uint32_t x = __ldg(ccsr + head + col);
         n_trials++;
+        if constexpr (ZC) {
+            if (s_mapped[cb]) zc_sectors += 1u;
+            // accept_candidate searches N(prev) when neither the rand value
+            // nor x == prev (nor prev == cur) decides the trial
+            if (pcsr != nullptr && s_mapped[pb] && !(rv <= thr_min<SOPR>(a.c, t)) && x != prev && prev != cur)
+                zc_sectors += search_sectors(pdeg);
+        }
         const int verdict = pcsr != nullptr
                                 ? (accept_candidate<SOPR>(a.c, t, rv, x, prev, cur, CsrIndex{pcsr, {}, 0}, phead, pdeg) ? 1 : 0)
                                 : accept_without_prev<SOPR>(a.c, t, rv, x, prev, cur);
@@ -597,6 +617,10 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
         atomicAdd(&a.ctr[kCtrTrials], s_ws[warp][kWsTrials]);
         atomicAdd(&a.ctr[kCtrDone], s_ws[warp][kWsDone]);
         atomicAdd(&a.ctr[kCtrHashSum], s_ws[warp][kWsHash]);
+    }
+    if constexpr (ZC) {
+        const unsigned long long zs = warp_sum((unsigned long long)zc_sectors);
+        if (lane == 0 && zs) atomicAdd(&a.ctr[kCtrZcSectors], zs);
     }
 }
 
@@ -784,7 +808,8 @@ static int ooc_grid_for(int num_sms)
 template <bool SOPR, bool PATHS, bool COOP, bool W = false>
 static void ooc_launch_one(const OocStepArgs &a, int grid, cudaStream_t s)
 {
-    k_walk_ooc<SOPR, PATHS, COOP, W><<<grid, kWalkThreads, 0, s>>>(a);
+    if (a.mapped) k_walk_ooc<SOPR, PATHS, COOP, W, true><<<grid, kWalkThreads, 0, s>>>(a);
+    else k_walk_ooc<SOPR, PATHS, COOP, W><<<grid, kWalkThreads, 0, s>>>(a);
 }
 
 int ooc_grid(bool sopr, bool paths, bool coop, int num_sms, bool weighted)

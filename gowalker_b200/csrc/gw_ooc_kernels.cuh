@@ -33,6 +33,7 @@ struct OocStepArgs {
     const uint64_t *estart;          // [nb+1]
     uint32_t nb, nverts;
     uint32_t lazy;                   // 1: a walker runs with only its current block resident
+    const uint8_t *mapped;           // [nb] zero-copy tail: 1 = read through mapped host memory (counted)
     WalkerRec *recs;                 // one record per walker, never moved
     const uint32_t *order;           // record of each bucket-sorted position
     uint32_t *keys;                  // bucket of each sorted position; kNoBucket once finished

@@ -312,3 +312,39 @@ def test_block_schedule_matches_cpu_replay(gw, oracle, algo, prefetch, strict, s
     rs, _ = oracle.sched_replay(reqs, nent, nb, slots, prefetch=bool(prefetch), lazy=lazy)
     assert (st["iterations"], st["block_loads"], st["steps"]) == (rs["iterations"], rs["loads"], rs["steps"])
     assert rs["loads"] > 2 * nb
+
+
+@pytest.mark.parametrize("algo,compress", [(0, 0), (0, 1), (1, 0)])
+def test_zero_copy_tail_with_prefetch(gw, oracle, algo, compress):
+    """GOWalker's zero mode with the block copies prefetched: once no block
+    scores above zero_threshold (engine/schedule.hpp:101,124), every
+    remaining walker runs to its end reading the absent blocks through mapped
+    host memory (engine/engine.hpp:593-634).  Same walks as the oracle, fewer
+    block loads than without the tail, and the mapped reads are counted into
+    the host-to-device bytes."""
+    from gowalker_b200.preprocess import split_equal_edge_mass
+    beg, csr = graph(oracle, scale=14, ef=8, cap=12000, seed=33)
+    vb, eb = split_equal_edge_mass(beg, 16)
+    term = 0.15 if algo else 0.0
+    res = {}
+    for zc in (0, 1):
+        stage = 2 * (len(csr) * 4 // 16 + (1 << 16)) if compress else 0
+        eng = gw.WalkEngine(algorithm=algo, maxhops=30, p=0.5, q=2.0, alpha=0.2, term_prob=term, seed=4,
+                            walkpersource=1, record_paths=0, cache_size=cache_for(beg, eb, 6) + stage, prefetch=1,
+                            compress_blocks=compress, zero_copy=zc, zero_threshold=60 if zc else 0)
+        eng.set_host_graph(beg, csr, vb, eb)
+        eng.init_walkers(algo, 1, 4)
+        st = eng.run()
+        res[zc] = (eng.hashes(), st)
+        eng.close()
+    ref = oracle.walk(beg, csr, oracle.make_cfg(algo=algo, maxhops=30, p=0.5, q=2.0, alpha=0.2, term_prob=term, seed=4),
+                      0, len(beg) - 1, paths=False)
+    for zc in (0, 1):
+        assert np.array_equal(res[zc][0], ref["hashes"]), zc
+    s0, s1 = res[0][1], res[1][1]
+    assert s1["zero_copy_steps"] > 0 and s0["zero_copy_steps"] == 0
+    assert s1["block_loads"] < s0["block_loads"]
+    assert s1["steps"] == s0["steps"] == ref["stats"]["steps"]
+    # the tail's mapped reads (at least one 32-byte sector per tail step's
+    # candidate from an absent block) are in the host-to-device bytes
+    assert s1["h2d_bytes"] > 0
