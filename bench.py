@@ -390,10 +390,14 @@ def run_ooc_bench(args, wl):
     vb, eb = split_equal_edge_mass(beg, wl["nblocks"])
     arms = ["plain", "learned"] if args.policy == "pair" else [args.policy]
     V = len(beg) - 1
+    # GOWalker's zero mode: its threshold is blocksize / 128 / 24 walkers
+    # (apps/Node2vec.cu:100-108), the block size here the largest block's bytes
+    zero_threshold = int(4 * int(np.diff(eb.astype(np.int64)).max()) / 128 / 24) if args.zero_copy else 0
     first, count = rank_shard(rank, world, V * wl["wps"])
     eng = gw.WalkEngine(algorithm=wl["algo"], maxhops=wl["maxhops"], p=wl["p"], q=wl["q"], alpha=wl["alpha"],
                         term_prob=wl["term"], seed=42, walkpersource=wl["wps"], record_paths=0,
-                        cache_size=wl["cache"], zero_copy=0, strict_blocks=1 if args.strict_blocks else 0,
+                        cache_size=wl["cache"], zero_copy=1 if args.zero_copy else 0, zero_threshold=zero_threshold,
+                        strict_blocks=1 if args.strict_blocks else 0,
                         prefetch=0 if args.no_prefetch else 1, compress_blocks=0 if args.no_compress else 1,
                         device=local)
     eng.set_host_graph(beg_t, csr_t[: len(csr)], vb, eb)
@@ -447,6 +451,7 @@ def run_ooc_bench(args, wl):
             steps_per_run=steps_all / args.steps, block_loads_per_run=sum(s["block_loads"] for s in sts) / args.steps,
             iterations_per_run=sum(s["iterations"] for s in sts) / args.steps,
             launches=sum(s["launches"] for s in sts), path_hash_sum=str(hsum),
+            zero_copy_steps_per_run=sum(s["zero_copy_steps"] for s in sts) / args.steps,
             kernel_ms_per_run=sum(s["kernel_ms"] for s in sts) / args.steps,
             bucket_ms_per_run=sum(s["bucket_ms"] for s in sts) / args.steps,
             learned_iterations_per_run=sum(s["learned_iterations"] for s in sts) / args.steps,
@@ -469,6 +474,7 @@ def run_ooc_bench(args, wl):
                            "residency": "both blocks (reference rule)" if args.strict_blocks else
                                         "current block until N(prev) is needed",
                            "prefetch": not args.no_prefetch, "compressed_blocks": not args.no_compress,
+                           "zero_copy_tail": {"on": bool(args.zero_copy), "zero_threshold_walkers": zero_threshold},
                            "vertices": V, "edges": len(csr), "blocks": wl["nblocks"], "cache_bytes": wl["cache"],
                            "walkers": V * wl["wps"], "graph_in": "pinned host memory",
                            "l2": "every run copies the graph's blocks from the host into a 1.5 GB-class device "
@@ -926,6 +932,9 @@ def main():
                          "one of GOWalker's rule, the learned predictor, SOWalker's annealing")
     ap.add_argument("--no-compress", action="store_true",
                     help="out-of-core: copy plain neighbour lists (default: compressed, decoded on the device)")
+    ap.add_argument("--zero-copy", action="store_true",
+                    help="out-of-core: GOWalker's zero mode -- once no block scores above blocksize/3072 walkers, "
+                         "finish every walker reading mapped host memory")
     ap.add_argument("--launch-per-hop", action="store_true",
                     help="in-core: also time the plain one-launch-per-hop form (same walks) beside the persistent "
                          "kernel")
