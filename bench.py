@@ -7,9 +7,10 @@ directed R-MAT graph (scale 26, ids >= 41.6 M rejected, thinned to exactly
 1.47 B edges, generator seed 1), split into 64 equal-edge-mass blocks held in
 pinned host memory, device block cache capped at 1.5 GB.  Two arms run after
 one another on the same engine, K times each: GOWalker's block choice
-(plain) and the learned demand predictor (learned); value = the learned arm's
-steps/s, the plain arm beside it with both arms' H2D bytes per step, and the
-walks of both arms must be identical.
+(plain) and the learned demand predictor (learned), both with GOWalker's zero
+mode (the tail read through mapped host memory, `--no-zero-copy` to turn it
+off); value = the learned arm's steps/s, the plain arm beside it with both
+arms' H2D bytes per step, and the walks of both arms must be identical.
 
 One bench step = one full run of every walker of the workload (gw_run).
 Other workloads: `--config c2` (in-core SOPR, scale 24), `c1` (in-core
@@ -932,9 +933,10 @@ def main():
                          "one of GOWalker's rule, the learned predictor, SOWalker's annealing")
     ap.add_argument("--no-compress", action="store_true",
                     help="out-of-core: copy plain neighbour lists (default: compressed, decoded on the device)")
-    ap.add_argument("--zero-copy", action="store_true",
-                    help="out-of-core: GOWalker's zero mode -- once no block scores above blocksize/3072 walkers, "
-                         "finish every walker reading mapped host memory")
+    ap.add_argument("--no-zero-copy", dest="zero_copy", action="store_false",
+                    help="out-of-core: keep loading blocks to the end (default: GOWalker's zero mode -- once no "
+                         "block scores above blocksize/3072 walkers, every walker finishes reading mapped host "
+                         "memory)")
     ap.add_argument("--launch-per-hop", action="store_true",
                     help="in-core: also time the plain one-launch-per-hop form (same walks) beside the persistent "
                          "kernel")
