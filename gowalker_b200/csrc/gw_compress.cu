@@ -131,22 +131,68 @@ bool compress_block(const uint64_t *beg, const uint32_t *csr, uint32_t nv, uint6
     return true;
 }
 
-// Eight bytes of `base` from byte offset `off`, read as two aligned 32-bit
-// words (base 16-byte aligned): the low 40 bits or more are the bytes at off
-// onwards.  Neighbouring lanes read the same words, so a chunk's fields load
-// in one or two transactions instead of five byte loads per lane.
-__device__ __forceinline__ uint64_t load_bytes64(const uint8_t *__restrict__ base, uint64_t off)
+// One chunk of k ids at byte `pos` of the payload, decoded by the warp: the
+// lanes load the chunk's bytes as 34 aligned 32-bit words in one coalesced
+// round (lane i: words i and, for lanes 0-1, i + 32; a chunk spans at most
+// 3 + 5 + 124 bytes), then every lane takes its delta's bits from the words
+// by shuffles -- no lane waits for a second dependent load.  Words past the
+// buffer end (`limit` words from `pay`) read as zero.  Returns the next
+// chunk's position; sets *bad on a malformed chunk.
+__device__ __forceinline__ uint64_t decode_chunk(const uint8_t *__restrict__ pay, uint64_t pos, uint32_t k,
+                                                 uint64_t payload_bytes, uint64_t limit, uint32_t lane,
+                                                 uint32_t *__restrict__ row, uint32_t nverts, bool &bad_id, bool &bad)
 {
-    const uint32_t *w = reinterpret_cast<const uint32_t *>(base + (off & ~3ull));
-    const uint64_t v = (uint64_t)__ldg(w) | ((uint64_t)__ldg(w + 1) << 32);
-    return v >> ((off & 3u) * 8u);
+    const uint64_t w0 = pos >> 2;
+    const uint32_t sh = (uint32_t)(pos & 3u) * 8u;
+    const uint32_t *__restrict__ words = reinterpret_cast<const uint32_t *>(pay);
+    const uint32_t wa = (w0 + lane < limit) ? __ldg(words + w0 + lane) : 0u;
+    const uint32_t wb = (lane < 2u && w0 + 32u + lane < limit) ? __ldg(words + w0 + 32u + lane) : 0u;
+    auto word = [&](uint32_t q) {  // word q of the window (q < 34), from the lane holding it
+        const uint32_t x = __shfl_sync(0xFFFFFFFFu, wa, q & 31u);
+        const uint32_t y = __shfl_sync(0xFFFFFFFFu, wb, q & 31u);
+        return q < 32u ? x : y;
+    };
+    const uint64_t head = (((uint64_t)word(1) << 32) | word(0)) >> sh;  // width byte, then the first id
+    const uint32_t w = (uint32_t)head & 0xFFu;
+    const uint64_t packed = ((uint64_t)(k - 1) * w + 7) >> 3;
+    if (w > 32 || pos + 5 + packed > payload_bytes) {
+        bad = true;
+        return pos;
+    }
+    // every lane shuffles (the same control flow), lanes 1 .. k-1 keep a delta
+    const uint32_t bp = lane ? (lane - 1) * w : 0u;
+    const uint32_t bo = sh + 40u + bp;  // bit offset of the delta from word 0
+    const uint32_t q = bo >> 5;
+    const uint64_t acc = ((uint64_t)word(q + 1) << 32) | word(q);
+    uint32_t x;
+    if (lane == 0) {
+        x = (uint32_t)(head >> 8);
+    } else if (lane < k && w != 0) {
+        const uint64_t mask = (w == 32) ? 0xFFFFFFFFull : ((1ull << w) - 1);
+        const uint32_t z = (uint32_t)((acc >> (bo & 31u)) & mask);
+        x = (z >> 1) ^ (0u - (z & 1u));
+    } else {
+        x = 0;
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane < k) {
+        row[lane] = x;
+        bad_id |= x >= nverts;
+    }
+    return pos + 5 + packed;
 }
 
-// Warp tasks: task t < nv decodes vertex t if it has at most 32 chunks;
-// task nv + g decodes split group g (32 chunks of a larger vertex).  Within a
-// chunk, lane i extracts delta i (lane 0 the first id) and a warp prefix sum
-// (mod 2^32) rebuilds the ids.  Every id written is checked against nverts
-// (the validation of a plain block copy, done here in the same pass).
+// Warp tasks: task t < ntv decodes vertices [32t, 32t + 32) that have at most
+// 32 chunks (lane i loads vertex 32t + i's payload offset and neighbour
+// range, coalesced, and the warp walks the 32 in turn); task ntv + g decodes
+// split group g (32 chunks of a larger vertex).  Within a chunk, lane i
+// extracts delta i (lane 0 the first id) and a warp prefix sum (mod 2^32)
+// rebuilds the ids.  Every id written is checked against nverts (the
+// validation of a plain block copy, done here in the same pass).
 __global__ void k_decode_block(const uint8_t *__restrict__ src, uint64_t split_off, uint32_t nsplit,
                                uint64_t payload_off, uint64_t payload_bytes, uint32_t nv,
                                const uint64_t *__restrict__ beg, uint32_t v0, uint64_t e0, uint64_t ne,
@@ -157,70 +203,72 @@ __global__ void k_decode_block(const uint8_t *__restrict__ src, uint64_t split_o
     const uint32_t *voff = reinterpret_cast<const uint32_t *>(src);
     const uint32_t *split = reinterpret_cast<const uint32_t *>(src + split_off);
     const uint8_t *pay = src + payload_off;
-    const uint64_t ntasks = (uint64_t)nv + nsplit;
-    bool bad_id = false;
+    const uint64_t limit = (payload_bytes + 8) >> 2;  // whole words of payload and padding
+    const uint64_t ntv = ((uint64_t)nv + 31) >> 5;
+    const uint64_t ntasks = ntv + nsplit;
+    bool bad_id = false, bad = false;
     for (uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntasks; t += nwarps) {
-        uint32_t v, c0;
-        uint64_t pos;
-        if (t < nv) {
-            v = (uint32_t)t;
-            c0 = 0;
-            pos = __ldg(voff + v);
+        if (t < ntv) {
+            const uint64_t vi = (t << 5) + lane;
+            uint64_t mpos = 0, mb0 = 0, mb1 = 0;
+            if (vi < nv) {
+                mpos = __ldg(voff + vi);
+                mb0 = __ldg(beg + v0 + vi);
+                mb1 = __ldg(beg + v0 + vi + 1);
+            }
+            const uint32_t nvt = (uint32_t)min((uint64_t)32, (uint64_t)nv - (t << 5));
+            for (uint32_t j = 0; j < nvt; ++j) {
+                uint64_t pos = __shfl_sync(0xFFFFFFFFu, mpos, j);
+                const uint64_t b0 = __shfl_sync(0xFFFFFFFFu, mb0, j), b1 = __shfl_sync(0xFFFFFFFFu, mb1, j);
+                if (b1 < b0 || b0 < e0 || b1 - e0 > ne) {
+                    bad = true;
+                    continue;
+                }
+                const uint64_t d = b1 - b0;
+                const uint64_t nch = (d + kChunkIds - 1) / kChunkIds;
+                if (nch > kChunkIds) continue;  // decoded by its split groups
+                bool vbad = false;
+                for (uint64_t c = 0; c < nch && !vbad; ++c) {
+                    const uint32_t k = (uint32_t)min((uint64_t)kChunkIds, d - c * kChunkIds);
+                    if (pos + 5 > payload_bytes) {
+                        vbad = true;
+                        break;
+                    }
+                    pos = decode_chunk(pay, pos, k, payload_bytes, limit, lane, out + (b0 - e0) + c * kChunkIds, nverts,
+                                       bad_id, vbad);
+                }
+                bad |= vbad;
+            }
         } else {
-            const uint64_t g = t - nv;
-            v = __ldg(split + 3 * g);
-            c0 = __ldg(split + 3 * g + 1);
-            pos = __ldg(split + 3 * g + 2);
+            const uint64_t g = t - ntv;
+            const uint32_t v = __ldg(split + 3 * g), c0 = __ldg(split + 3 * g + 1);
+            uint64_t pos = __ldg(split + 3 * g + 2);
             if (v >= nv) {
-                if (lane == 0) atomicOr(err, kErrBlock);
+                bad = true;
                 continue;
             }
-        }
-        const uint64_t b0 = __ldg(beg + v0 + v), b1 = __ldg(beg + v0 + v + 1);
-        bool bad = b1 < b0 || b0 < e0 || b1 - e0 > ne;
-        const uint64_t d = bad ? 0 : b1 - b0;
-        const uint64_t nch = (d + kChunkIds - 1) / kChunkIds;
-        if (t < nv && nch > kChunkIds) continue;  // decoded by its split groups
-        const uint64_t c1 = min(nch, (uint64_t)c0 + kChunkIds);
-        for (uint64_t c = c0; c < c1; ++c) {
-            const uint64_t j = c * kChunkIds;
-            const uint32_t k = (uint32_t)min((uint64_t)kChunkIds, d - j);
-            if (pos + 5 > payload_bytes) {
+            const uint64_t b0 = __ldg(beg + v0 + v), b1 = __ldg(beg + v0 + v + 1);
+            if (b1 < b0 || b0 < e0 || b1 - e0 > ne) {
                 bad = true;
-                break;
+                continue;
             }
-            const uint64_t head = load_bytes64(pay, pos);  // width byte, then the first id
-            const uint32_t w = (uint32_t)head & 0xFFu;
-            const uint64_t packed = ((uint64_t)(k - 1) * w + 7) >> 3;
-            if (w > 32 || pos + 5 + packed > payload_bytes) {
-                bad = true;
-                break;
+            const uint64_t d = b1 - b0;
+            const uint64_t nch = (d + kChunkIds - 1) / kChunkIds;
+            const uint64_t c1 = min(nch, (uint64_t)c0 + kChunkIds);
+            bool vbad = false;
+            for (uint64_t c = c0; c < c1 && !vbad; ++c) {
+                const uint32_t k = (uint32_t)min((uint64_t)kChunkIds, d - c * kChunkIds);
+                if (pos + 5 > payload_bytes) {
+                    vbad = true;
+                    break;
+                }
+                pos = decode_chunk(pay, pos, k, payload_bytes, limit, lane, out + (b0 - e0) + c * kChunkIds, nverts,
+                                   bad_id, vbad);
             }
-            uint32_t x = 0;
-            if (lane == 0) {
-                x = (uint32_t)(head >> 8);
-            } else if (lane < k && w != 0) {
-                // bits [bp, bp + w) of the packed deltas: at most 39 bits from
-                // the byte holding bit bp, inside the 8-byte pad past the payload
-                const uint32_t bp = (lane - 1) * w;
-                const uint64_t acc = load_bytes64(pay, pos + 5 + (bp >> 3));
-                const uint64_t mask = (w == 32) ? 0xFFFFFFFFull : ((1ull << w) - 1);
-                const uint32_t z = (uint32_t)((acc >> (bp & 7u)) & mask);
-                x = (z >> 1) ^ (0u - (z & 1u));
-            }
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-                if (lane >= (uint32_t)o) x += y;
-            }
-            if (lane < k) {
-                out[b0 - e0 + j + lane] = x;
-                bad_id |= x >= nverts;
-            }
-            pos += 5 + packed;
+            bad |= vbad;
         }
-        if (bad && lane == 0) atomicOr(err, kErrBlock);
     }
+    if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(err, kErrBlock);
     if (__any_sync(0xFFFFFFFFu, bad_id) && lane == 0) atomicOr(err, kErrVertexRange);
 }
 
