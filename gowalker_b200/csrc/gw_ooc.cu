@@ -1001,13 +1001,13 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         }
         // ---- plain block choice on the device (decision, fallback and rescue), read back
         if (trace) cudaEventRecord(td0, ds);
-        // learned: the plain rule's scores, each block's scaled by the
-        // network's forecast growth of its demand
+        // learned: the plain rule's choice; with a full cache the victim is
+        // the cached block with the lowest forecast of incident walkers
         const bool plain_window = (judge_clock % kJudgePeriod) >= kJudgePeriod - kJudgePlain;
         const bool learned_decides = learned_active && !stall_next && !plain_window;
         if (learned_active) judge_clock++;
         if ((st = cuda(launch_schedule(o.d_pairs, o.d_offsets + nbk, nb, o.d_cached, ncached, capacity, cfg.zero_threshold,
-                                       learned_decides ? o.d_pred_res : nullptr, 1.f, o.d_dec, ds),
+                                       learned_decides ? o.d_pred : nullptr, 1.f, o.d_dec, ds),
                        "schedule")))
             break;
         launches++;

@@ -242,8 +242,10 @@ __global__ void __launch_bounds__(kScanThreads) k_runnable(const uint32_t *__res
 // would switch to it): the fullest bucket with an absent block; load its first
 // absent block, evicting the cached block with the fewest incident walkers
 // outside that bucket -- after at most two rescues the bucket runs, so every
-// run ends.  `pred` (optional) replaces the scores by predicted demand scaled
-// by pred_weight: the learned policy.
+// run ends.  `pred` (optional, the learned policy): each block's forecast of
+// log1p(incident walkers over the next iterations); with a full cache the
+// chosen block then replaces the cached block with the lowest forecast
+// instead of the one with the smallest link (pred_weight is unused).
 __global__ void __launch_bounds__(1024) k_schedule(const uint32_t *__restrict__ counts,
                                                    const uint32_t *__restrict__ live, uint32_t nb,
                                                    const uint32_t *__restrict__ cached, uint32_t ncached,
@@ -307,8 +309,6 @@ __global__ void __launch_bounds__(1024) k_schedule(const uint32_t *__restrict__ 
             score = all - (key >> 32);
             pos = (uint32_t)key;
         }
-        // learned: scale by the forecast growth of block i's demand, e^pred
-        if (pred) score = (unsigned long long)((double)score * exp((double)fminf(fmaxf(pred_weight * pred[i], -4.f), 4.f)));
         if (lane == 0) {
             s_pos[i] = pos;
             atomicMax(&s_best, (score << 11) | (2047u - i));
@@ -332,6 +332,16 @@ __global__ void __launch_bounds__(1024) k_schedule(const uint32_t *__restrict__ 
             d.action = full ? 2 : 1;
             d.block = bi;
             d.position = full ? (int32_t)s_pos[bi] : (int32_t)ncached;
+            if (full && pred) {
+                // learned eviction: the cached block with the lowest forecast
+                // of incident walkers over the next iterations (first on ties)
+                float mn = 3.0e38f;
+                for (uint32_t j = 0; j < ncached; ++j)
+                    if (pred[s_list[j]] < mn) {
+                        mn = pred[s_list[j]];
+                        d.position = (int32_t)j;
+                    }
+            }
         } else {
             d.action = 0;
             d.block = -1;
@@ -670,15 +680,17 @@ __global__ void __launch_bounds__(1024) k_features(const FeatureArgs f)
         x[13] = log1pf((float)(row + col - diag));
         x[14] = log1pf((float)(row - diag));
         x[15] = log1pf((float)(col - diag));
-        f.col[i] = colf;
+        f.col[i] = (float)(row + col - diag);  // incident walkers: the forecast's quantity
     }
 }
 
 // Training set from the trace ring (ring slots of kMlpIn features and of
-// demand per block; iteration t lives in slot t % ring): samples t0 .. t0+T-1
-// gathered in order, with targets y = log1p(mean demand over the next k
-// iterations) - x[0] (x[0] = log1p of the demand then), so the network
-// learns the change of log demand and an untrained one forecasts no change.
+// incident walkers per block -- walkers whose current or previous block it
+// is; iteration t lives in slot t % ring): samples t0 .. t0+T-1 gathered in
+// order, with targets y = log1p(mean incident walkers over the next k
+// iterations) - x[13] (x[13] = log1p of the incident walkers then), so the
+// network learns the change of that log demand and an untrained one
+// forecasts no change.
 __global__ void k_gather_train(const float *ring_x, const float *ring_col, uint32_t t0, uint32_t ring, uint32_t T,
                                uint32_t k, uint32_t nb, float *train_x, float *y)
 {
@@ -691,14 +703,14 @@ __global__ void k_gather_train(const float *ring_x, const float *ring_col, uint3
     for (int f = 0; f < 16; ++f) xd[f] = xs[f];
     float s = 0.f;
     for (uint32_t d = 1; d <= k; ++d) s += ring_col[(uint64_t)((t + d) % ring) * nb + i];
-    y[idx] = log1pf(s / (float)k) - xs[0];
+    y[idx] = log1pf(s / (float)k) - xs[13];
 }
 
-// level[i] = res[i] + x[i][0]: the forecast change back to log demand.
+// level[i] = res[i] + x[i][13]: the forecast change back to log incident walkers.
 __global__ void k_add_level(const float *res, const float *x, float *level, uint32_t nb)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nb) level[i] = res[i] + x[(uint64_t)i * 16];
+    if (i < nb) level[i] = res[i] + x[(uint64_t)i * 16 + 13];
 }
 
 

@@ -906,6 +906,11 @@ int64_t oracle_sched_replay(const uint16_t *reqs, const uint32_t *nent, uint32_t
  *             this iteration, computed exactly from the walks
  *   policy 2  GOWalker's choice, clairvoyant eviction: evict the cached block
  *             that the fewest waiting walkers need within their next 4 entries
+ *   policy 3  GOWalker's choice, evicting the cached block with the fewest
+ *             incident walkers (current or previous block) now
+ *   policy 4  GOWalker's choice, evicting the lowest running average of steps
+ *             taken in the block (weight 1/2 per iteration)
+ *   policy 5  GOWalker's choice, evicting the block unused the longest
  * zt > 0: once the plain rule's best score is <= zt (the reference's zero
  * threshold, engine/schedule.hpp:101,124 and apps/Node2vec.cu:100-108), stop
  * loading; the remaining steps are counted in *zc_steps (they would run
@@ -916,7 +921,8 @@ static uint32_t st_stride;
 #define SENT(w, k) (st_reqs[(uint64_t)(w) * st_stride + (k)])
 #define SBLK(w, k) ((uint32_t)(SENT(w, k) & 0x3FFFu))
 
-static uint32_t study_run(uint32_t *e, uint8_t *flag, uint32_t w, const uint8_t *res, int lazy, int commit, int *done)
+static uint32_t study_run(uint32_t *e, uint8_t *flag, uint32_t w, const uint8_t *res, int lazy, int commit, int *done,
+                          uint64_t *usage)
 {
     uint32_t ew = e[w], steps = 0;
     *done = 0;
@@ -934,6 +940,7 @@ static uint32_t study_run(uint32_t *e, uint8_t *flag, uint32_t w, const uint8_t 
             fl = 1;
             break;
         }
+        if (usage) usage[ent & 0x3FFFu]++;
         ew++;
         steps++;
         if (ew >= st_nent[w]) {
@@ -953,7 +960,7 @@ int64_t oracle_sched_study(const uint16_t *reqs, const uint32_t *nent, uint32_t 
                            uint32_t nslots, int lazy, int policy, uint64_t zt, uint64_t *loads, uint64_t *steps,
                            uint64_t *zc_steps)
 {
-    if (nb == 0 || nb > 1024 || nslots < 2 || policy < 0 || policy > 2) return -1;
+    if (nb == 0 || nb > 1024 || nslots < 2 || policy < 0 || policy > 5) return -1;
     st_reqs = reqs;
     st_nent = nent;
     st_stride = stride;
@@ -962,6 +969,9 @@ int64_t oracle_sched_study(const uint16_t *reqs, const uint32_t *nent, uint32_t 
     uint8_t *flag = (uint8_t *)calloc(count, 1);
     uint64_t *pairs = (uint64_t *)calloc(nn, sizeof(uint64_t));
     uint64_t *need = (uint64_t *)calloc(nb, sizeof(uint64_t));
+    uint64_t *usage = (uint64_t *)calloc(nb, sizeof(uint64_t));   /* steps taken in each block, this iteration */
+    double *use_ema = (double *)calloc(nb, sizeof(double));        /* their running average */
+    int64_t *last_use = (int64_t *)calloc(nb, sizeof(int64_t));    /* last iteration with steps in the block */
     uint32_t *live = (uint32_t *)malloc(sizeof(uint32_t) * (count ? count : 1));
     uint32_t nlive = 0;
     for (uint32_t w = 0; w < count; ++w) live[nlive++] = w;
@@ -1033,7 +1043,7 @@ int64_t oracle_sched_study(const uint16_t *reqs, const uint32_t *nent, uint32_t 
                 int d;
                 for (uint32_t k = 0; k < nlive; ++k) {
                     const uint32_t w = live[k], cb = SBLK(w, e[w]), pb = e[w] ? SBLK(w, e[w] - 1) : cb;
-                    if (cb == i || pb == i) y += study_run(e, flag, w, r2, lazy, 0, &d);
+                    if (cb == i || pb == i) y += study_run(e, flag, w, r2, lazy, 0, &d, NULL);
                 }
                 if (y > by) {
                     by = y;
@@ -1059,6 +1069,29 @@ int64_t oracle_sched_study(const uint16_t *reqs, const uint32_t *nent, uint32_t 
                     pos = (int)j;
                 }
         }
+        if (policy >= 3 && action == 2 && !stalled) {
+            /* 3: the fewest walkers at or from the block now; 4: the lowest
+               running average of steps taken in it; 5: the longest unused */
+            double mn = 1e300;
+            for (uint32_t j = 0; j < ncached; ++j) {
+                const uint32_t c = cached[j];
+                double v;
+                if (policy == 3) {
+                    uint64_t inc = 0;
+                    for (uint32_t k = 0; k < nb; ++k)
+                        inc += pairs[(uint64_t)c * nb + k] + (k != c ? pairs[(uint64_t)k * nb + c] : 0);
+                    v = (double)inc;
+                } else if (policy == 4) {
+                    v = use_ema[c];
+                } else {
+                    v = (double)last_use[c];
+                }
+                if (v < mn) {
+                    mn = v;
+                    pos = (int)j;
+                }
+            }
+        }
         int load = -1, lpos = -1;
         if (action) {
             load = blk;
@@ -1080,16 +1113,24 @@ int64_t oracle_sched_study(const uint16_t *reqs, const uint32_t *nent, uint32_t 
         (*loads)++;
         uint32_t k2 = 0;
         const uint64_t steps0 = *steps;
+        memset(usage, 0, sizeof(uint64_t) * nb);
         for (uint32_t k = 0; k < nlive; ++k) {
             const uint32_t w = live[k], before = e[w];
             int d;
-            study_run(e, flag, w, res, lazy, 1, &d);
+            study_run(e, flag, w, res, lazy, 1, &d, usage);
             *steps += e[w] - before;
             if (!d) live[k2++] = w;
         }
         stalled = *steps == steps0 && k2 == nlive;
         nlive = k2;
+        for (uint32_t b = 0; b < nb; ++b) {
+            use_ema[b] = 0.5 * use_ema[b] + 0.5 * (double)usage[b];
+            if (usage[b]) last_use[b] = it;
+        }
     }
+    free(usage);
+    free(use_ema);
+    free(last_use);
     free(e);
     free(flag);
     free(pairs);

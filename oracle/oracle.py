@@ -421,7 +421,9 @@ def sched_replay(reqs, nent, nb: int, nslots: int, prefetch: bool = True, lazy: 
 def sched_study(reqs, nent, nb: int, nslots: int, policy: int = 0, zero_threshold: int = 0, lazy: bool = True):
     """Another block policy on the same walks (gw_oracle.c oracle_sched_study,
     no prefetch): 0 GOWalker's choice, 1 clairvoyant one-iteration yield, 2
-    GOWalker's choice with clairvoyant eviction; zero_threshold > 0 stops
+    GOWalker's choice with clairvoyant eviction, 3-5 GOWalker's choice
+    evicting the fewest incident walkers / the lowest average use / the least
+    recently used block; zero_threshold > 0 stops
     loading where the reference's zero rule does.  Returns a dict of
     iterations, loads, steps taken by the block loads, and steps left to the
     mapped-host tail."""
