@@ -186,6 +186,51 @@ __device__ __forceinline__ uint64_t decode_chunk(const uint8_t *__restrict__ pay
     return pos + 5 + packed;
 }
 
+// The same chunk decode from a warp's shared-memory copy of the payload
+// words [base, base + staged): every lane reads the words it needs directly.
+// `end` is the byte just past the staged vertices' chunks; a chunk reaching
+// past it is malformed.  Reads stay inside the staged words plus a 36-word
+// tail (lanes past k read words they do not use).
+__device__ __forceinline__ uint64_t decode_chunk_sm(const uint32_t *sm, uint64_t base, uint64_t pos, uint64_t end,
+                                                    uint32_t k, uint32_t lane, uint32_t *__restrict__ row,
+                                                    uint32_t nverts, bool &bad_id, bool &bad)
+{
+    const uint32_t off = (uint32_t)((pos >> 2) - base);
+    const uint32_t sh = (uint32_t)(pos & 3u) * 8u;
+    const uint64_t head = (((uint64_t)sm[off + 1] << 32) | sm[off]) >> sh;
+    const uint32_t w = (uint32_t)head & 0xFFu;
+    const uint64_t packed = ((uint64_t)(k - 1) * w + 7) >> 3;
+    if (w > 32 || pos + 5 + packed > end) {
+        bad = true;
+        return pos;
+    }
+    const uint32_t bp = lane ? (lane - 1) * w : 0u;
+    const uint32_t bo = sh + 40u + bp;
+    const uint32_t q = off + (bo >> 5);
+    uint32_t x = 0;
+    if (lane == 0) {
+        x = (uint32_t)(head >> 8);
+    } else if (lane < k && w != 0) {
+        const uint64_t acc = ((uint64_t)sm[q + 1] << 32) | sm[q];
+        const uint64_t mask = (w == 32) ? 0xFFFFFFFFull : ((1ull << w) - 1);
+        const uint32_t z = (uint32_t)((acc >> (bo & 31u)) & mask);
+        x = (z >> 1) ^ (0u - (z & 1u));
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane < k) {
+        row[lane] = x;
+        bad_id |= x >= nverts;
+    }
+    return pos + 5 + packed;
+}
+
+constexpr uint32_t kStageWords = 1024;  // a warp's shared-memory copy of one vertex batch's payload (4 KB)
+constexpr uint32_t kDecodeThreads = 256;
+
 // Warp tasks: task t < ntv decodes vertices [32t, 32t + 32) that have at most
 // 32 chunks (lane i loads vertex 32t + i's payload offset and neighbour
 // range, coalesced, and the warp walks the 32 in turn); task ntv + g decodes
@@ -193,11 +238,15 @@ __device__ __forceinline__ uint64_t decode_chunk(const uint8_t *__restrict__ pay
 // extracts delta i (lane 0 the first id) and a warp prefix sum (mod 2^32)
 // rebuilds the ids.  Every id written is checked against nverts (the
 // validation of a plain block copy, done here in the same pass).
-__global__ void k_decode_block(const uint8_t *__restrict__ src, uint64_t split_off, uint32_t nsplit,
-                               uint64_t payload_off, uint64_t payload_bytes, uint32_t nv,
-                               const uint64_t *__restrict__ beg, uint32_t v0, uint64_t e0, uint64_t ne,
-                               uint32_t nverts, uint32_t *__restrict__ out, uint32_t *err)
+__global__ void __launch_bounds__(kDecodeThreads)
+    k_decode_block(const uint8_t *__restrict__ src, uint64_t split_off, uint32_t nsplit, uint64_t payload_off,
+                   uint64_t payload_bytes, uint32_t nv, const uint64_t *__restrict__ beg, uint32_t v0, uint64_t e0,
+                   uint64_t ne, uint32_t nverts, uint32_t *__restrict__ out, uint32_t *err)
 {
+    // a vertex batch's payload bytes are contiguous: a warp copies them into
+    // shared memory with coalesced, independent loads, then decodes from there
+    __shared__ uint32_t s_stage[kDecodeThreads / 32][kStageWords + 36];
+    uint32_t *sm = s_stage[threadIdx.x >> 5];
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const uint32_t *voff = reinterpret_cast<const uint32_t *>(src);
@@ -217,6 +266,17 @@ __global__ void k_decode_block(const uint8_t *__restrict__ src, uint64_t split_o
                 mb1 = __ldg(beg + v0 + vi + 1);
             }
             const uint32_t nvt = (uint32_t)min((uint64_t)32, (uint64_t)nv - (t << 5));
+            // the batch's payload: [first vertex's offset, the next batch's)
+            const uint64_t p0 = __shfl_sync(0xFFFFFFFFu, mpos, 0);
+            const uint64_t p1 = __ldg(voff + (t << 5) + nvt);
+            const uint64_t base = p0 >> 2;
+            const uint64_t nwords = p1 > p0 ? ((p1 + 3) >> 2) - base + 2 : 0;
+            const bool staged = p1 >= p0 && p1 <= payload_bytes && nwords <= kStageWords;
+            if (staged) {
+                for (uint32_t i = lane; i < nwords; i += 32)
+                    sm[i] = (base + i < limit) ? __ldg(reinterpret_cast<const uint32_t *>(pay) + base + i) : 0u;
+                __syncwarp();
+            }
             for (uint32_t j = 0; j < nvt; ++j) {
                 uint64_t pos = __shfl_sync(0xFFFFFFFFu, mpos, j);
                 const uint64_t b0 = __shfl_sync(0xFFFFFFFFu, mb0, j), b1 = __shfl_sync(0xFFFFFFFFu, mb1, j);
@@ -230,15 +290,24 @@ __global__ void k_decode_block(const uint8_t *__restrict__ src, uint64_t split_o
                 bool vbad = false;
                 for (uint64_t c = 0; c < nch && !vbad; ++c) {
                     const uint32_t k = (uint32_t)min((uint64_t)kChunkIds, d - c * kChunkIds);
-                    if (pos + 5 > payload_bytes) {
-                        vbad = true;
-                        break;
+                    uint32_t *row = out + (b0 - e0) + c * kChunkIds;
+                    if (staged) {
+                        if (pos < p0 || pos + 5 > p1) {
+                            vbad = true;
+                            break;
+                        }
+                        pos = decode_chunk_sm(sm, base, pos, p1, k, lane, row, nverts, bad_id, vbad);
+                    } else {
+                        if (pos + 5 > payload_bytes) {
+                            vbad = true;
+                            break;
+                        }
+                        pos = decode_chunk(pay, pos, k, payload_bytes, limit, lane, row, nverts, bad_id, vbad);
                     }
-                    pos = decode_chunk(pay, pos, k, payload_bytes, limit, lane, out + (b0 - e0) + c * kChunkIds, nverts,
-                                       bad_id, vbad);
                 }
                 bad |= vbad;
             }
+            __syncwarp();  // the next batch overwrites the staged words
         } else {
             const uint64_t g = t - ntv;
             const uint32_t v = __ldg(split + 3 * g), c0 = __ldg(split + 3 * g + 1);
@@ -277,8 +346,8 @@ cudaError_t launch_decode_block(const uint8_t *src, const CompressedBlock &cb, u
                                 int num_sms, cudaStream_t s)
 {
     if (nv == 0) return cudaSuccess;
-    k_decode_block<<<num_sms * 8, 256, 0, s>>>(src, cb.split_off, cb.nsplit, cb.payload_off, cb.payload_bytes, nv, beg,
-                                               v0, e0, ne, nverts, out, err);
+    k_decode_block<<<num_sms * 4, kDecodeThreads, 0, s>>>(src, cb.split_off, cb.nsplit, cb.payload_off,
+                                                         cb.payload_bytes, nv, beg, v0, e0, ne, nverts, out, err);
     return cudaGetLastError();
 }
 
