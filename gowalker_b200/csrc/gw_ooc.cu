@@ -29,6 +29,24 @@
 
 namespace gw {
 
+// What makes two out-of-core runs the same workload, for the learned
+// policy's judge: the graph stays as set, so the walkers, walk parameters
+// and engine options decide.
+struct RunSignature {
+    uint64_t nwalkers = 0, seed = 0, cache_size = 0;
+    uint32_t wid_first = 0, algorithm = 0, maxhops = 0, wps = 0, numwalks = 0, init_mode = 0;
+    float p = 0.f, q = 0.f, alpha = 0.f, term = 0.f;
+    uint32_t zero_copy = 0, zero_threshold = 0, prefetch = 0, compress = 0, strict = 0;
+    bool operator==(const RunSignature &o) const
+    {
+        return nwalkers == o.nwalkers && seed == o.seed && cache_size == o.cache_size && wid_first == o.wid_first &&
+               algorithm == o.algorithm && maxhops == o.maxhops && wps == o.wps && numwalks == o.numwalks &&
+               init_mode == o.init_mode && p == o.p && q == o.q && alpha == o.alpha && term == o.term &&
+               zero_copy == o.zero_copy && zero_threshold == o.zero_threshold && prefetch == o.prefetch &&
+               compress == o.compress && strict == o.strict;
+    }
+};
+
 struct OocState {
     uint32_t nb = 0;
     uint32_t nslots = 0;
@@ -106,6 +124,11 @@ struct OocState {
     cudaGraphExec_t train_graph = nullptr;    // kTrainEpochs from a fresh initialisation + the loss read-back
     cudaGraphExec_t retrain_graph = nullptr;  // kRetrainEpochs of warm training + the loss read-back
     bool train_inflight = false;
+    // the judge's record: the last plain run of a workload, and a learned
+    // run that lost to it
+    bool have_plain = false, learned_lost = false;
+    RunSignature plain_sig, lost_sig;
+    double plain_bytes_per_step = 0.0, plain_ms_per_step = 0.0;
     float *d_trace_x = nullptr, *d_trace_col = nullptr, *d_trace_y = nullptr;
     float *d_train_x = nullptr, *d_pred = nullptr, *d_pred_res = nullptr;  // forecast log demand, its change
     float *d_emass = nullptr, *d_vfrac = nullptr, *d_prev_col = nullptr, *d_ema = nullptr;
@@ -569,6 +592,30 @@ static int ooc_build_alias(gw_handle *h, cudaStream_t s, uint64_t *h2d)
     return st;
 }
 
+static RunSignature run_signature(const gw_handle *h)
+{
+    RunSignature r;
+    r.nwalkers = h->nwalkers;
+    r.seed = h->cfg.seed;
+    r.cache_size = h->cfg.cache_size;
+    r.wid_first = h->wid_first;
+    r.algorithm = h->cfg.algorithm;
+    r.maxhops = h->cfg.maxhops;
+    r.wps = h->cfg.walkpersource;
+    r.numwalks = h->cfg.numwalks;
+    r.init_mode = h->cfg.init_mode;
+    r.p = h->cfg.p;
+    r.q = h->cfg.q;
+    r.alpha = h->cfg.alpha;
+    r.term = h->cfg.term_prob;
+    r.zero_copy = h->cfg.zero_copy;
+    r.zero_threshold = h->cfg.zero_threshold;
+    r.prefetch = h->cfg.prefetch;
+    r.compress = h->cfg.compress_blocks;
+    r.strict = h->cfg.strict_blocks;
+    return r;
+}
+
 int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
 {
     int st;
@@ -837,24 +884,15 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                                          : nullptr;
     bool stall_next = false;  // a learned choice moved no walker: the next decision is the plain rule's
     bool reverted = false;
-    // The judge: once the predictor decides, the last kJudgePlain of every
-    // kJudgePeriod iterations are decided by the plain rule, and each learned
-    // window's host-link bytes per step and time per step are compared with
-    // the plain windows on either side of it (the run's demand drifts, so
-    // only neighbouring windows are comparable).  Two losing windows in a row
-    // hand the run back to the plain rule.
-    struct JudgeWindow {
-        uint64_t steps = 0, bytes = 0;
-        double ms = 0.0;
-        uint32_t iters = 0;
-    };
-    constexpr uint32_t kJudgePeriod = 64, kJudgePlain = 16;
-    JudgeWindow win, last_learned_win, prev_plain_win;
-    int win_kind = -1;  // kind of the open window: 1 learned, 0 plain
-    bool have_learned_win = false, have_plain_win = false;
-    uint32_t judge_clock = 0, judge_losses = 0;
-    uint64_t phase_steps_mark = 0, phase_bytes_mark = 0;
-    auto phase_time_mark = std::chrono::steady_clock::now();
+    // The judge works run by run: a learned run is compared, when it ends,
+    // with the last plain run of the same workload on this handle (host-link
+    // bytes per step and time per step); a learned run that lost hands every
+    // later learned run of that workload to the plain rule.  A whole run is
+    // the only fair unit: a better eviction may load more blocks early and
+    // win at the end, where fewer walkers are left to the mapped tail.
+    const RunSignature sig = run_signature(this);
+    if (policy == GW_POLICY_LEARNED && o.learned_lost && o.lost_sig == sig) reverted = true;
+    uint64_t phase_steps_mark = 0;
     int last_phase = -1;
     double pred_err_sum = 0.0, persist_err_sum = 0.0;
     uint32_t pred_err_n = 0;
@@ -1003,9 +1041,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if (trace) cudaEventRecord(td0, ds);
         // learned: the plain rule's choice; with a full cache the victim is
         // the cached block with the lowest forecast of incident walkers
-        const bool plain_window = (judge_clock % kJudgePeriod) >= kJudgePeriod - kJudgePlain;
-        const bool learned_decides = learned_active && !stall_next && !plain_window;
-        if (learned_active) judge_clock++;
+        const bool learned_decides = learned_active && !stall_next;
         if ((st = cuda(launch_schedule(o.d_pairs, o.d_offsets + nbk, nb, o.d_cached, ncached, capacity, cfg.zero_threshold,
                                        learned_decides ? o.d_pred : nullptr, 1.f, o.d_dec, ds),
                        "schedule")))
@@ -1060,47 +1096,13 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             break;
         }
         const Decision d = *o.h_dec;
-        // judge: the steps, host-link bytes and host time since the last
-        // decision belong to the window of the policy that took it
         const uint64_t steps_now = h_ctr[kCtrSteps];
-        const auto now = std::chrono::steady_clock::now();
-        if (last_phase >= 0 && o.cached.size() >= capacity && learned_iters > 0) {
-            if (last_phase != win_kind && win.iters > 0) {
-                // a window closes: a learned one waits for the plain one after it
-                if (win_kind == 1) {
-                    last_learned_win = win;
-                    have_learned_win = true;
-                } else {
-                    if (have_learned_win && have_plain_win && !reverted) {
-                        const double pb = (double)(prev_plain_win.bytes + win.bytes) /
-                                          (double)std::max<uint64_t>(prev_plain_win.steps + win.steps, 1);
-                        const double pm = (prev_plain_win.ms + win.ms) /
-                                          (double)std::max<uint64_t>(prev_plain_win.steps + win.steps, 1);
-                        const double lb = (double)last_learned_win.bytes / (double)std::max<uint64_t>(last_learned_win.steps, 1);
-                        const double lm = last_learned_win.ms / (double)std::max<uint64_t>(last_learned_win.steps, 1);
-                        judge_losses = (lb > pb || lm > 1.03 * pm) ? judge_losses + 1 : 0;
-                        if (judge_losses >= 2) reverted = true;
-                    }
-                    prev_plain_win = win;
-                    have_plain_win = true;
-                    have_learned_win = false;
-                }
-                win = JudgeWindow{};
-            }
-            win_kind = last_phase;
-            win.steps += steps_now - phase_steps_mark;
-            win.bytes += h2d - phase_bytes_mark;
-            win.ms += std::chrono::duration<double, std::milli>(now - phase_time_mark).count();
-            win.iters++;
-        }
-        phase_time_mark = now;
         // progress guard: a learned choice that moved no walker hands the
         // next decision to the plain rule and its rescue, which always make
         // some bucket runnable
         const bool learned_stalled = last_phase == 1 && steps_now == phase_steps_mark;
         stall_next = learned_stalled;
         phase_steps_mark = steps_now;
-        phase_bytes_mark = h2d;
         last_phase = -1;
         if (predicting) {
             // Each prediction is scored once the kHorizon iterations it
@@ -1385,6 +1387,25 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     if (h_ctr[kCtrDone] != nwalkers)
         return fail(GW_ERR_DEVICE, "out-of-core run finished %llu of %llu walkers", (unsigned long long)h_ctr[kCtrDone],
                     (unsigned long long)nwalkers);
+    // the judge: a plain run sets the bar; a learned run with more
+    // host-link bytes per step, or more than 2 % more time per step, than
+    // the last plain run of the same workload hands that workload's later
+    // learned runs to the plain rule
+    float run_ms = 0.f;
+    cudaEventElapsedTime(&run_ms, ev_start, ev_stop);
+    const double steps_d = (double)std::max<uint64_t>(h_ctr[kCtrSteps], 1);
+    if (policy == GW_POLICY_PLAIN) {
+        o.have_plain = true;
+        o.plain_sig = sig;
+        o.plain_bytes_per_step = (double)h2d / steps_d;
+        o.plain_ms_per_step = (double)run_ms / steps_d;
+    } else if (policy == GW_POLICY_LEARNED && !reverted && o.have_plain && o.plain_sig == sig) {
+        if ((double)h2d / steps_d > o.plain_bytes_per_step * 1.0005 ||
+            (double)run_ms / steps_d > o.plain_ms_per_step * 1.02) {
+            o.learned_lost = true;
+            o.lost_sig = sig;
+        }
+    }
     return GW_OK;
 }
 
