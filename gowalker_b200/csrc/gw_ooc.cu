@@ -640,7 +640,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     double t_sched = 0.0, t_runnable = 0.0;
     bool tcp_live[2] = {false, false}, tin_live = false;
     uint32_t tcp_next = 0;
-    double t_install = 0.0, t_copy = 0.0, t_decision = 0.0;
+    double t_install = 0.0, t_copy = 0.0, t_decision = 0.0, t_zero = 0.0;
     if (trace) {
         cudaEventCreate(&td0);
         cudaEventCreate(&td1);
@@ -999,10 +999,13 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 cudaGetLastError();
             }
         }
-        const bool learned_active = learned_on && o.trained && !reverted;
+        // the learned rule decides from the first iteration: until the network
+        // is trained its forecast is this iteration's incident count carried
+        // forward (what an untrained network, whose output layer starts at
+        // zero, forecasts too)
+        const bool learned_active = learned_on && !reverted;
         // until the judge reverts: features and demand go to the trace ring
-        // every iteration, and once trained the network forecasts (its error
-        // is measured in the windows where the plain rule decides too)
+        // every iteration, and once trained the network forecasts
         const bool predicting = learned_on && o.trained;
         const bool tracing = learned_on;
         float *ring_x = o.d_trace_x + (uint64_t)(trace_t % kTraceRing) * nb * kMlpIn;
@@ -1042,8 +1045,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         // learned: the plain rule's choice; with a full cache the victim is
         // the cached block with the lowest forecast of incident walkers
         const bool learned_decides = learned_active && !stall_next;
+        const float *forecast = learned_decides ? (o.trained ? o.d_pred : ring_col) : nullptr;
         if ((st = cuda(launch_schedule(o.d_pairs, o.d_offsets + nbk, nb, o.d_cached, ncached, capacity, cfg.zero_threshold,
-                                       learned_decides ? o.d_pred : nullptr, 1.f, o.d_dec, ds),
+                                       forecast, 1.f, o.d_dec, ds),
                        "schedule")))
             break;
         launches++;
@@ -1158,12 +1162,14 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 (st = cuda(cudaStreamSynchronize(s), "counters")))
                 break;
             a.mapped = o.d_mapped;
+            const auto tz0 = std::chrono::steady_clock::now();
             st = step();
             a.mapped = nullptr;
             if (st) break;
             if ((st = cuda(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(before), cudaMemcpyDeviceToHost, s), "counters")))
                 break;
             if ((st = cuda(cudaStreamSynchronize(s), "zero-copy"))) break;
+            t_zero += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tz0).count();
             zc_steps += h_ctr[kCtrSteps] - before[kCtrSteps];
             h2d += 32ull * (h_ctr[kCtrZcSectors] - before[kCtrZcSectors]);
             // restore the table to device slots only
@@ -1374,8 +1380,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             fprintf(stderr,
                     "[gowalker] out-of-core run: %u iterations, %.1f ms total, step %.1f, re-bucketing %.1f, "
                     "install %.1f, prefetch copies %.1f (copy stream), host blocked on decisions %.1f ms "
-                    "(decision kernels and read-back %.1f), runnable-bucket pass %.1f ms\n",
-                    iters, stats->total_ms, kernel_ms, bucket_ms, t_install, t_copy, t_decision, t_sched, t_runnable);
+                    "(decision kernels and read-back %.1f), runnable-bucket pass %.1f ms, zero-copy tail %.1f ms "
+                    "(%llu steps), %u block loads, %u learned iterations\n",
+                    iters, stats->total_ms, kernel_ms, bucket_ms, t_install, t_copy, t_decision, t_sched, t_runnable,
+                    t_zero, (unsigned long long)zc_steps, (unsigned)loads, learned_iters);
         stats->learned_iterations = learned_iters;
         stats->policy_reverted = reverted ? 1u : 0u;
         stats->train_loss = (policy == GW_POLICY_LEARNED && o.h_loss) ? *o.h_loss : 0.f;

@@ -664,6 +664,7 @@ int oracle_walk_reqs(const uint64_t *beg, const uint32_t *csr, uint32_t nverts, 
 typedef struct {
     uint64_t iterations, loads, steps, parks, rescues;
     uint64_t finished;
+    uint64_t zc_steps; /* steps left to the mapped-host tail (zero mode) */
 } oracle_sched_stats;
 
 /* Plain block choice, GOwalker_scheduler_t::max_choose_blocks
@@ -756,8 +757,8 @@ static void plain_choice(const uint64_t *pairs, uint32_t nb, const uint32_t *cac
  * iteration the loaded block, the cached position it replaced (-1 append)
  * and the steps taken.  Returns the iteration count or -1. */
 int64_t oracle_sched_replay(const uint16_t *reqs, const uint32_t *nent, uint32_t count, uint32_t stride, uint32_t nb,
-                            uint32_t nslots, int prefetch, int lazy, uint64_t zero_threshold, int32_t *log,
-                            uint64_t log_cap, oracle_sched_stats *out)
+                            uint32_t nslots, int prefetch, int lazy, uint64_t zero_threshold, int evict_incident,
+                            int zero_tail, int32_t *log, uint64_t log_cap, oracle_sched_stats *out)
 {
     if (nb == 0 || nb > 1024 || nslots < (prefetch ? 3u : 2u)) return -1;
     memset(out, 0, sizeof(*out));
@@ -807,9 +808,28 @@ int64_t oracle_sched_replay(const uint16_t *reqs, const uint32_t *nent, uint32_t
         }
         int action, blk, pos, rblk, rpos;
         plain_choice(pairs, nb, cached, ncached, capacity, zero_threshold, &action, &blk, &pos, &rblk, &rpos);
+        if (evict_incident && action == 2) {
+            /* the cached block with the fewest incident walkers (first on ties) */
+            uint64_t mn = ~0ull;
+            for (uint32_t j = 0; j < ncached; ++j) {
+                const uint32_t c = cached[j];
+                uint64_t inc = 0;
+                for (uint32_t k = 0; k < nb; ++k)
+                    inc += pairs[(uint64_t)c * nb + k] + (k != c ? pairs[(uint64_t)k * nb + c] : 0);
+                if (inc < mn) {
+                    mn = inc;
+                    pos = (int)j;
+                }
+            }
+        }
         const uint32_t live_at_decision = nlive;
+        /* zero mode: nothing scores above the threshold -- the rest finishes
+           through mapped host memory (with prefetch, after this iteration's step) */
+        const int tail = zero_tail && !action && live_at_decision > 0;
         int load = -1, lpos = -1;
-        if (action) {
+        if (tail) {
+            /* no load */
+        } else if (action) {
             load = blk;
             lpos = action == 2 ? pos : -1;
         } else if (rblk >= 0 && (ncached < capacity || rpos >= 0)) {
@@ -818,6 +838,11 @@ int64_t oracle_sched_replay(const uint16_t *reqs, const uint32_t *nent, uint32_t
             out->rescues++;
         }
         if (!prefetch && live_at_decision == 0) break;
+        if (tail && !prefetch) {
+            for (uint32_t k = 0; k < nlive; ++k) out->zc_steps += nent[live[k]] - e[live[k]] -
+                                                                 ((reqs[(uint64_t)live[k] * stride + nent[live[k]] - 1] & 0x4000u) ? 1u : 0u);
+            break;
+        }
         if (!prefetch && load >= 0) {
             /* loaded before this iteration's step */
             if (lpos >= 0) {
@@ -875,6 +900,11 @@ int64_t oracle_sched_replay(const uint16_t *reqs, const uint32_t *nent, uint32_t
             log[3 * (it - 1) + 2] = (int32_t)(out->steps - steps_before);
         }
         if (load >= 0) out->loads++;
+        if (prefetch && tail) {
+            for (uint32_t k = 0; k < nlive; ++k) out->zc_steps += nent[live[k]] - e[live[k]] -
+                                                                 ((reqs[(uint64_t)live[k] * stride + nent[live[k]] - 1] & 0x4000u) ? 1u : 0u);
+            break;
+        }
         if (prefetch) {
             if (live_at_decision == 0) break;
             staged = load;

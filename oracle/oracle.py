@@ -74,7 +74,8 @@ class Stats(ctypes.Structure):
 
 
 class SchedStats(ctypes.Structure):
-    _fields_ = [(n, ctypes.c_uint64) for n in ("iterations", "loads", "steps", "parks", "rescues", "finished")]
+    _fields_ = [(n, ctypes.c_uint64) for n in ("iterations", "loads", "steps", "parks", "rescues", "finished",
+                                               "zc_steps")]
 
     def as_dict(self):
         return {name: int(getattr(self, name)) for name, _ in self._fields_}
@@ -119,8 +120,8 @@ def lib():
         L.oracle_walk_reqs.restype = ctypes.c_int
         L.oracle_sched_replay.argtypes = [ctypes.POINTER(ctypes.c_uint16), u32p, ctypes.c_uint32, ctypes.c_uint32,
                                           ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
-                                          ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32), ctypes.c_uint64,
-                                          ctypes.POINTER(SchedStats)]
+                                          ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32),
+                                          ctypes.c_uint64, ctypes.POINTER(SchedStats)]
         L.oracle_sched_replay.restype = ctypes.c_int64
         L.oracle_sched_study.argtypes = [ctypes.POINTER(ctypes.c_uint16), u32p, ctypes.c_uint32, ctypes.c_uint32,
                                          ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
@@ -400,10 +401,13 @@ def walk_requirements(beg, csr, cfg: Cfg, vstart, wid_begin: int, count: int, nt
 
 
 def sched_replay(reqs, nent, nb: int, nslots: int, prefetch: bool = True, lazy: bool = True,
-                 zero_threshold: int = 0, log: bool = False):
+                 zero_threshold: int = 0, log: bool = False, evict_incident: bool = False, zero_tail: bool = False):
     """The out-of-core engine's plain block schedule replayed on the CPU
-    (gw_oracle.c oracle_sched_replay).  Returns (stats dict, per-iteration log
-    of (loaded block, replaced position, steps) or None)."""
+    (gw_oracle.c oracle_sched_replay).  evict_incident: the victim is the
+    cached block with the fewest incident walkers; zero_tail: GOWalker's zero
+    mode (the rest through mapped host memory once nothing scores above
+    zero_threshold; those steps in stats["zc_steps"]).  Returns (stats dict,
+    per-iteration log of (loaded block, replaced position, steps) or None)."""
     reqs = np.ascontiguousarray(reqs, dtype=np.uint16)
     nent = np.ascontiguousarray(nent, dtype=np.uint32)
     cap = 1 << 22 if log else 0
@@ -411,7 +415,7 @@ def sched_replay(reqs, nent, nb: int, nslots: int, prefetch: bool = True, lazy: 
     st = SchedStats()
     it = lib().oracle_sched_replay(reqs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), _p(nent, ctypes.c_uint32),
                                    len(nent), reqs.shape[1], nb, nslots, int(prefetch), int(lazy), zero_threshold,
-                                   lg.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) if log else None, cap,
+                                   int(evict_incident), int(zero_tail), lg.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) if log else None, cap,
                                    ctypes.byref(st))
     if it < 0:
         raise ValueError("schedule replay failed (bad arguments or no progress)")
