@@ -394,13 +394,14 @@ def run_ooc_bench(args, wl):
     # GOWalker's zero mode: its threshold is blocksize / 128 / 24 walkers
     # (apps/Node2vec.cu:100-108), the block size here the largest block's bytes
     zero_threshold = int(4 * int(np.diff(eb.astype(np.int64)).max()) / 128 / 24) if args.zero_copy else 0
+    zero_threshold = int(zero_threshold * args.zero_scale)
     first, count = rank_shard(rank, world, V * wl["wps"])
     eng = gw.WalkEngine(algorithm=wl["algo"], maxhops=wl["maxhops"], p=wl["p"], q=wl["q"], alpha=wl["alpha"],
                         term_prob=wl["term"], seed=42, walkpersource=wl["wps"], record_paths=0,
                         cache_size=wl["cache"], zero_copy=1 if args.zero_copy else 0, zero_threshold=zero_threshold,
                         strict_blocks=1 if args.strict_blocks else 0,
                         prefetch=0 if args.no_prefetch else 1, compress_blocks=0 if args.no_compress else 1,
-                        device=local)
+                        learned_mode=args.learned_mode, device=local)
     eng.set_host_graph(beg_t, csr_t[: len(csr)], vb, eb)
     stream = torch.cuda.ExternalStream(eng.stream_handle(), device=local)
     h_hash = np.zeros(count, dtype=np.uint64)
@@ -476,6 +477,9 @@ def run_ooc_bench(args, wl):
                                         "current block until N(prev) is needed",
                            "prefetch": not args.no_prefetch, "compressed_blocks": not args.no_compress,
                            "zero_copy_tail": {"on": bool(args.zero_copy), "zero_threshold_walkers": zero_threshold},
+                           "learned_mode": {1: "forecast eviction", 2: "zero-copy switch priced by measured costs",
+                                            3: "forecast eviction and zero-copy switch"}[
+                               args.learned_mode or gw.GW_LEARNED_DEFAULT],
                            "vertices": V, "edges": len(csr), "blocks": wl["nblocks"], "cache_bytes": wl["cache"],
                            "walkers": V * wl["wps"], "graph_in": "pinned host memory",
                            "l2": "every run copies the graph's blocks from the host into a 1.5 GB-class device "
@@ -937,6 +941,11 @@ def main():
                     help="out-of-core: keep loading blocks to the end (default: GOWalker's zero mode -- once no "
                          "block scores above blocksize/3072 walkers, every walker finishes reading mapped host "
                          "memory)")
+    ap.add_argument("--learned-mode", type=int, default=0,
+                    help="out-of-core learned policy parts: 1 forecast eviction, 2 zero-copy switch priced by "
+                         "measured costs, 3 both (default 0: the library's default, the switch)")
+    ap.add_argument("--zero-scale", type=float, default=1.0,
+                    help="out-of-core: multiply GOWalker's zero-mode threshold by this factor (default 1)")
     ap.add_argument("--launch-per-hop", action="store_true",
                     help="in-core: also time the plain one-launch-per-hop form (same walks) beside the persistent "
                          "kernel")

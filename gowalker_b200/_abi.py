@@ -19,6 +19,8 @@ GW_PATHS_NONE, GW_PATHS_FULL = 0, 1
 GW_EDGES_SYMMETRIC, GW_EDGES_SORT, GW_EDGES_DEDUP = 1, 2, 4
 GW_SPLIT_REFERENCE, GW_SPLIT_EQUAL_EDGES = 0, 1
 GW_LAUNCH_PERSISTENT, GW_LAUNCH_PER_HOP = 0, 1
+GW_LEARNED_EVICT, GW_LEARNED_ZERO_SWITCH = 1, 2
+GW_LEARNED_DEFAULT = GW_LEARNED_ZERO_SWITCH
 
 # Every symbol include/gowalker.h declares.
 EXPORTS = (
@@ -60,7 +62,8 @@ class GwConfig(ctypes.Structure):
         ("compress_blocks", ctypes.c_uint32),
         ("learned_sync", ctypes.c_uint32),
         ("launch_mode", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 3),
+        ("learned_mode", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 2),
     ]
 
 

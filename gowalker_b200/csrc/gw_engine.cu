@@ -66,6 +66,7 @@ static bool config_ok(const gw_config &c, std::string &why)
     if (c.init_mode > GW_INIT_RANDOM) { why = "unknown init_mode"; return false; }
     if (c.record_paths > GW_PATHS_FULL) { why = "unknown record_paths"; return false; }
     if (c.launch_mode > GW_LAUNCH_PER_HOP) { why = "unknown launch_mode"; return false; }
+    if (c.learned_mode & ~(GW_LEARNED_EVICT | GW_LEARNED_ZERO_SWITCH)) { why = "unknown learned_mode bits"; return false; }
     if (c.threadperblock != 0 && (c.threadperblock % 32 != 0 || c.threadperblock > 1024)) {
         why = "threadperblock must be a multiple of 32 up to 1024";
         return false;

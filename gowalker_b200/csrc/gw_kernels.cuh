@@ -21,6 +21,8 @@ enum Counter : int {
     kCtrCoopLarge = 7,     // hard steps evaluated with candidate loads and searches
     kCtrCoopLargeAtt = 8,  // attempts those steps took
     kCtrZcSectors = 9,     // out-of-core zero-copy tail: 32-byte sectors read from mapped host memory
+    kCtrModelSectors = 10, // out-of-core, blocks resident: the sectors those steps would read from mapped memory
+    kCtrRunnable = 11,     // out-of-core: walkers handed to the step kernels (sum over launches)
     kCtrCount = 12
 };
 

@@ -36,14 +36,14 @@ struct RunSignature {
     uint64_t nwalkers = 0, seed = 0, cache_size = 0;
     uint32_t wid_first = 0, algorithm = 0, maxhops = 0, wps = 0, numwalks = 0, init_mode = 0;
     float p = 0.f, q = 0.f, alpha = 0.f, term = 0.f;
-    uint32_t zero_copy = 0, zero_threshold = 0, prefetch = 0, compress = 0, strict = 0;
+    uint32_t zero_copy = 0, zero_threshold = 0, prefetch = 0, compress = 0, strict = 0, learned_mode = 0;
     bool operator==(const RunSignature &o) const
     {
         return nwalkers == o.nwalkers && seed == o.seed && cache_size == o.cache_size && wid_first == o.wid_first &&
                algorithm == o.algorithm && maxhops == o.maxhops && wps == o.wps && numwalks == o.numwalks &&
                init_mode == o.init_mode && p == o.p && q == o.q && alpha == o.alpha && term == o.term &&
                zero_copy == o.zero_copy && zero_threshold == o.zero_threshold && prefetch == o.prefetch &&
-               compress == o.compress && strict == o.strict;
+               compress == o.compress && strict == o.strict && learned_mode == o.learned_mode;
     }
 };
 
@@ -128,7 +128,10 @@ struct OocState {
     // run that lost to it
     bool have_plain = false, learned_lost = false;
     RunSignature plain_sig, lost_sig;
-    double plain_bytes_per_step = 0.0, plain_ms_per_step = 0.0;
+    double plain_ms_per_step = 0.0;
+    // the last zero-copy tail's time per mapped sector (seconds; 0 = none
+    // timed yet): the learned switch's price of a mapped read on this link
+    double tail_s_per_sector = 0.0;
     float *d_trace_x = nullptr, *d_trace_col = nullptr, *d_trace_y = nullptr;
     float *d_train_x = nullptr, *d_pred = nullptr, *d_pred_res = nullptr;  // forecast log demand, its change
     float *d_emass = nullptr, *d_vfrac = nullptr, *d_prev_col = nullptr, *d_ema = nullptr;
@@ -613,6 +616,7 @@ static RunSignature run_signature(const gw_handle *h)
     r.prefetch = h->cfg.prefetch;
     r.compress = h->cfg.compress_blocks;
     r.strict = h->cfg.strict_blocks;
+    r.learned_mode = h->cfg.learned_mode;
     return r;
 }
 
@@ -627,7 +631,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     cudaStream_t s = s_compute;
     const bool sopr = cfg.algorithm != GW_NODE2VEC;
     const bool paths = cfg.record_paths == GW_PATHS_FULL;
-    uint64_t h2d = 0, loads = 0, zc_steps = 0;
+    uint64_t h2d = 0, loads = 0, zc_steps = 0, zc_sectors = 0;
     uint32_t iters = 0, launches = 0;
     float kernel_ms = 0.f, bucket_ms = 0.f;
     // GOWALKER_TRACE: per-run phase totals on stderr (install = wait for the
@@ -885,13 +889,30 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     bool stall_next = false;  // a learned choice moved no walker: the next decision is the plain rule's
     bool reverted = false;
     // The judge works run by run: a learned run is compared, when it ends,
-    // with the last plain run of the same workload on this handle (host-link
-    // bytes per step and time per step); a learned run that lost hands every
+    // with the last plain run of the same workload on this handle (time per
+    // step); a learned run that lost hands every
     // later learned run of that workload to the plain rule.  A whole run is
     // the only fair unit: a better eviction may load more blocks early and
     // win at the end, where fewer walkers are left to the mapped tail.
     const RunSignature sig = run_signature(this);
     if (policy == GW_POLICY_LEARNED && o.learned_lost && o.lost_sig == sig) reverted = true;
+    const uint32_t lmode = cfg.learned_mode ? cfg.learned_mode : GW_LEARNED_DEFAULT;
+    // The learned zero-mode switch prices the next load against the tail:
+    // the walkers it makes runnable (the plain rule's score) x steps a
+    // runnable walker takes per iteration (rho, over the last kRhoWindow
+    // iterations) x mapped sectors per step (sigma, modelled by the step
+    // kernels on this run's resident steps) x time per mapped sector (tau,
+    // timed on this handle's last tail) against the time of an iteration
+    // (host clock between decisions, averaged).  Until a tail has been
+    // timed, GOWalker's zero_threshold decides.
+    const bool cost_switch = policy == GW_POLICY_LEARNED && !reverted && (lmode & GW_LEARNED_ZERO_SWITCH) &&
+                             cfg.zero_copy && o.tail_s_per_sector > 0.0;
+    constexpr uint32_t kRhoWindow = 16;
+    std::deque<std::pair<uint64_t, uint64_t>> rho_hist;  // (steps, runnable) at each decision
+    double iter_ms_avg = 0.0;
+    std::chrono::steady_clock::time_point t_last_dec{};
+    bool have_last_dec = false;
+    uint32_t switch_iter = 0;
     uint64_t phase_steps_mark = 0;
     int last_phase = -1;
     double pred_err_sum = 0.0, persist_err_sum = 0.0;
@@ -1006,8 +1027,8 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         const bool learned_active = learned_on && !reverted;
         // until the judge reverts: features and demand go to the trace ring
         // every iteration, and once trained the network forecasts
-        const bool predicting = learned_on && o.trained;
-        const bool tracing = learned_on;
+        const bool tracing = learned_on && (lmode & GW_LEARNED_EVICT);
+        const bool predicting = tracing && o.trained;
         float *ring_x = o.d_trace_x + (uint64_t)(trace_t % kTraceRing) * nb * kMlpIn;
         float *ring_col = o.d_trace_col + (uint64_t)(trace_t % kTraceRing) * nb;
         if (tracing) {
@@ -1045,8 +1066,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         // learned: the plain rule's choice; with a full cache the victim is
         // the cached block with the lowest forecast of incident walkers
         const bool learned_decides = learned_active && !stall_next;
-        const float *forecast = learned_decides ? (o.trained ? o.d_pred : ring_col) : nullptr;
-        if ((st = cuda(launch_schedule(o.d_pairs, o.d_offsets + nbk, nb, o.d_cached, ncached, capacity, cfg.zero_threshold,
+        const float *forecast =
+            learned_decides && (lmode & GW_LEARNED_EVICT) ? (o.trained ? o.d_pred : ring_col) : nullptr;
+        if ((st = cuda(launch_schedule(o.d_pairs, o.d_offsets + nbk, nb, o.d_cached, ncached, capacity,
+                                       cost_switch ? 0u : cfg.zero_threshold,
                                        forecast, 1.f, o.d_dec, ds),
                        "schedule")))
             break;
@@ -1101,6 +1124,30 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         }
         const Decision d = *o.h_dec;
         const uint64_t steps_now = h_ctr[kCtrSteps];
+        // ---- learned zero-mode switch (prices: see cost_switch above)
+        bool zero_now = false;
+        if (cost_switch) {
+            const auto tnow = std::chrono::steady_clock::now();
+            if (have_last_dec) {
+                const double ms = std::chrono::duration<double, std::milli>(tnow - t_last_dec).count();
+                iter_ms_avg = iter_ms_avg > 0.0 ? iter_ms_avg + (ms - iter_ms_avg) / 8.0 : ms;
+            }
+            t_last_dec = tnow;
+            have_last_dec = true;
+            rho_hist.emplace_back(steps_now, h_ctr[kCtrRunnable]);
+            if (rho_hist.size() > kRhoWindow + 1) rho_hist.pop_front();
+            const uint64_t dsteps = steps_now - rho_hist.front().first;
+            const uint64_t drun = h_ctr[kCtrRunnable] - rho_hist.front().second;
+            if ((d.action == 1 || d.action == 2) && rho_hist.size() > kRhoWindow && drun > 0 && steps_now > 0) {
+                const double rho = (double)dsteps / (double)drun;
+                const double sigma = (double)h_ctr[kCtrModelSectors] / (double)steps_now;
+                const double load_gain_ms = (double)d.score * rho * sigma * o.tail_s_per_sector * 1e3;
+                if (load_gain_ms < iter_ms_avg) {
+                    zero_now = true;
+                    switch_iter = iters;
+                }
+            }
+        }
         // progress guard: a learned choice that moved no walker hands the
         // next decision to the plain rule and its rescue, which always make
         // some bucket runnable
@@ -1136,16 +1183,17 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         if (nlive == 0) break;
 
         std::vector<std::pair<int, int>> todo;  // (block, cached position or -1)
-        if (d.action == 1 || d.action == 2) {
+        if ((d.action == 1 || d.action == 2) && !zero_now) {
             todo.emplace_back(d.block, d.action == 2 ? d.position : -1);
             last_phase = learned_decides ? 1 : 0;
-            if (learned_decides) learned_iters++;
+            if (learned_decides && (lmode & GW_LEARNED_EVICT)) learned_iters++;
         } else if (cfg.zero_copy) {
             // ---- zero-copy tail (GOWalker's zero mode, engine/engine.hpp:593-634):
             // no block scores above zero_threshold, so every remaining walker
             // runs to its end reading the absent blocks through mapped host
             // memory; those reads are counted (32-byte sectors) into h2d_bytes.
             // With prefetch this iteration's step has run already.
+            if (zero_now) learned_iters++;
             if ((st = ooc_map_host(this))) break;
             std::vector<uint8_t> mapped(nb, 0);
             for (uint32_t b = 0; b < nb; ++b)
@@ -1169,9 +1217,16 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             if ((st = cuda(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(before), cudaMemcpyDeviceToHost, s), "counters")))
                 break;
             if ((st = cuda(cudaStreamSynchronize(s), "zero-copy"))) break;
-            t_zero += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tz0).count();
+            const double tail_ms =
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tz0).count();
+            t_zero += tail_ms;
             zc_steps += h_ctr[kCtrSteps] - before[kCtrSteps];
+            // the price of a mapped sector on this link (a short tail,
+            // latency-bound, overprices it: the switch then comes later)
+            if (h_ctr[kCtrZcSectors] - before[kCtrZcSectors] >= (1ull << 16))
+                o.tail_s_per_sector = tail_ms * 1e-3 / (double)(h_ctr[kCtrZcSectors] - before[kCtrZcSectors]);
             h2d += 32ull * (h_ctr[kCtrZcSectors] - before[kCtrZcSectors]);
+            zc_sectors += h_ctr[kCtrZcSectors] - before[kCtrZcSectors];
             // restore the table to device slots only
             for (uint32_t b = 0; b < nb; ++b)
                 if (o.block_slot[b] < 0) o.h_blk_csr[b] = nullptr;
@@ -1381,9 +1436,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                     "[gowalker] out-of-core run: %u iterations, %.1f ms total, step %.1f, re-bucketing %.1f, "
                     "install %.1f, prefetch copies %.1f (copy stream), host blocked on decisions %.1f ms "
                     "(decision kernels and read-back %.1f), runnable-bucket pass %.1f ms, zero-copy tail %.1f ms "
-                    "(%llu steps), %u block loads, %u learned iterations\n",
+                    "(%llu steps, %llu mapped sectors%s), %u block loads, %u learned iterations\n",
                     iters, stats->total_ms, kernel_ms, bucket_ms, t_install, t_copy, t_decision, t_sched, t_runnable,
-                    t_zero, (unsigned long long)zc_steps, (unsigned)loads, learned_iters);
+                    t_zero, (unsigned long long)zc_steps, (unsigned long long)zc_sectors,
+                    switch_iter ? ", entered by the learned switch" : "", (unsigned)loads, learned_iters);
         stats->learned_iterations = learned_iters;
         stats->policy_reverted = reverted ? 1u : 0u;
         stats->train_loss = (policy == GW_POLICY_LEARNED && o.h_loss) ? *o.h_loss : 0.f;
@@ -1395,21 +1451,21 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     if (h_ctr[kCtrDone] != nwalkers)
         return fail(GW_ERR_DEVICE, "out-of-core run finished %llu of %llu walkers", (unsigned long long)h_ctr[kCtrDone],
                     (unsigned long long)nwalkers);
-    // the judge: a plain run sets the bar; a learned run with more
-    // host-link bytes per step, or more than 2 % more time per step, than
-    // the last plain run of the same workload hands that workload's later
-    // learned runs to the plain rule
+    // the judge: a plain run sets the bar; a learned run with more than 2 %
+    // more time per step than the last plain run of the same workload hands
+    // that workload's later learned runs to the plain rule.  Time, not
+    // host-link bytes: a 32-byte mapped read costs the link about as long as
+    // 140 bytes of a bulk copy, so a schedule that loads more and reads
+    // fewer mapped sectors can move more bytes and still finish first.
     float run_ms = 0.f;
     cudaEventElapsedTime(&run_ms, ev_start, ev_stop);
     const double steps_d = (double)std::max<uint64_t>(h_ctr[kCtrSteps], 1);
     if (policy == GW_POLICY_PLAIN) {
         o.have_plain = true;
         o.plain_sig = sig;
-        o.plain_bytes_per_step = (double)h2d / steps_d;
         o.plain_ms_per_step = (double)run_ms / steps_d;
     } else if (policy == GW_POLICY_LEARNED && !reverted && o.have_plain && o.plain_sig == sig) {
-        if ((double)h2d / steps_d > o.plain_bytes_per_step * 1.0005 ||
-            (double)run_ms / steps_d > o.plain_ms_per_step * 1.02) {
+        if ((double)run_ms / steps_d > o.plain_ms_per_step * 1.02) {
             o.learned_lost = true;
             o.lost_sig = sig;
         }

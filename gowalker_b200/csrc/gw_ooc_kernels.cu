@@ -376,7 +376,9 @@ __global__ void __launch_bounds__(1024) k_schedule(const uint32_t *__restrict__ 
 // ZC: the zero-copy tail -- the blocks marked in a.mapped are read through
 // mapped host memory; every read of one is counted as a 32-byte sector in
 // kCtrZcSectors (an upper bound of the host-link bytes: each probe of a
-// binary search counts as its own sector).
+// binary search counts as its own sector).  Without ZC the same count is
+// taken as if every block were mapped (kCtrModelSectors): what these steps
+// would cost in the zero-copy tail, the learned policy's switch estimate.
 template <bool SOPR, bool PATHS, bool COOP, bool W = false, bool ZC = false>
 __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant__ OocStepArgs a)
 {
@@ -400,6 +402,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
     const uint32_t nrun = *a.nrun;
     const uint32_t total = a.run_pre[nrun];
     const uint32_t maxhops = a.c.maxhops;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.ctr[kCtrRunnable], (unsigned long long)total);
 
     uint32_t q_next = 0, q_end = 0;
     bool exhausted = false;
@@ -522,6 +525,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
                 n_trials += astar - p0;
                 if constexpr (ZC)  // every attempt: a candidate and, at most, a search of N(prev)
                     zc_sectors += (astar - p0) * ((s_mapped[cb] ? 1u : 0u) + (s_mapped[pb] ? search_sectors(pdeg) : 0u));
+                else
+                    zc_sectors += (astar - p0) * (1u + search_sectors(pdeg));
                 if (astar >= kMaxAttempts) {
                     atomicOr(a.err, kErrTrials);
                     finish();
@@ -542,11 +547,12 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
         }
         const uint32_t x = __ldg(ccsr + head + col);
         n_trials++;
-        if constexpr (ZC) {
-            if (s_mapped[cb]) zc_sectors += 1u;
+        {
             // accept_candidate searches N(prev) when neither the rand value
             // nor x == prev (nor prev == cur) decides the trial
-            if (pcsr != nullptr && s_mapped[pb] && !(rv <= thr_min<SOPR>(a.c, t)) && x != prev && prev != cur)
+            const bool cm = ZC ? s_mapped[cb] != 0 : true, pm = ZC ? s_mapped[pb] != 0 : true;
+            if (cm) zc_sectors += 1u;
+            if (pcsr != nullptr && pm && !(rv <= thr_min<SOPR>(a.c, t)) && x != prev && prev != cur)
                 zc_sectors += search_sectors(pdeg);
         }
         const int verdict = pcsr != nullptr
@@ -628,9 +634,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_ooc(const __grid_constant
         atomicAdd(&a.ctr[kCtrDone], s_ws[warp][kWsDone]);
         atomicAdd(&a.ctr[kCtrHashSum], s_ws[warp][kWsHash]);
     }
-    if constexpr (ZC) {
+    {
         const unsigned long long zs = warp_sum((unsigned long long)zc_sectors);
-        if (lane == 0 && zs) atomicAdd(&a.ctr[kCtrZcSectors], zs);
+        if (lane == 0 && zs) atomicAdd(&a.ctr[ZC ? kCtrZcSectors : kCtrModelSectors], zs);
     }
 }
 

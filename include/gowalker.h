@@ -64,7 +64,11 @@ extern "C" {
 /* block-choice policies */
 #define GW_POLICY_PLAIN 0u   /* GOwalker_scheduler_t::max_choose_blocks
                                 (engine/schedule.hpp:70-138) on the device */
-#define GW_POLICY_LEARNED 1u /* MLP demand predictor, plain policy as fallback */
+#define GW_POLICY_LEARNED 1u /* GOWalker's choice with learned parts (gw_config.learned_mode): the
+                                zero-copy switch priced by measured costs, and eviction by the MLP's
+                                forecast of incident walkers; judged run by run against the last plain
+                                run of the same workload (more than 2 % more time per step loses, and
+                                later learned runs of that workload are plain) */
 #define GW_POLICY_SA 2u      /* SOwalker_scheduler_t::choose_blocks (engine/schedule.hpp:455-593):
                                 an annealed block set, loaded block by block */
 
@@ -111,8 +115,20 @@ typedef struct gw_config {
                                  stops once reverted */
     uint32_t launch_mode;     /* in-core: GW_LAUNCH_PERSISTENT (default) or GW_LAUNCH_PER_HOP, the
                                  plain form kept for comparison (unweighted walks only) */
-    uint32_t reserved[3];
+    uint32_t learned_mode;    /* learned policy parts: GW_LEARNED_EVICT | GW_LEARNED_ZERO_SWITCH;
+                                 0 = GW_LEARNED_DEFAULT */
+    uint32_t reserved[2];
 } gw_config;
+
+/* learned policy parts (gw_config.learned_mode) */
+#define GW_LEARNED_EVICT 1u        /* with a full cache, evict the cached block with the lowest forecast of
+                                      incident walkers (GOWalker's choice of the block to load is kept) */
+#define GW_LEARNED_ZERO_SWITCH 2u  /* zero-copy tail: switch when the next load's walkers, times the steps a
+                                      runnable walker takes per iteration, times the mapped sectors a step
+                                      reads, times the measured time per mapped sector, is below the
+                                      measured time of an iteration (in place of the fixed zero_threshold,
+                                      which is used until this handle has timed a zero-copy tail) */
+#define GW_LEARNED_DEFAULT GW_LEARNED_ZERO_SWITCH
 
 /* in-core launch modes */
 #define GW_LAUNCH_PERSISTENT 0u /* one persistent work-stealing kernel runs every walker to the end */
@@ -132,7 +148,8 @@ typedef struct gw_stats {
     uint32_t launches;        /* kernels launched by this run */
     float kernel_ms;          /* time inside the step kernels (CUDA events) */
     float total_ms;           /* whole run (CUDA events) */
-    uint32_t learned_iterations; /* iterations decided by the predictor */
+    uint32_t learned_iterations; /* decisions the learned parts changed or took: forecast evictions,
+                                    and the switch to the zero-copy tail */
     uint32_t policy_reverted;    /* 1 when the judge sent the run back to the plain policy */
     float train_loss;            /* predictor training loss (mean squared, log1p scale) */
     float pred_error;            /* learned: mean |prediction - realised target| per block, the target

@@ -22,13 +22,13 @@ def cache_for(beg, eb, slots):
 
 
 def run_ooc(gw, beg, csr, nblocks, slots, algo=0, maxhops=20, wps=1, p=0.5, q=2.0, alpha=0.2, term=0.0, seed=5,
-            zero_copy=0, zero_threshold=0, paths=1, policy=0):
+            zero_copy=0, zero_threshold=0, paths=1, policy=0, learned_mode=0):
     from gowalker_b200.preprocess import split_equal_edge_mass
     vb, eb = split_equal_edge_mass(beg, nblocks)
     cache = cache_for(beg, eb, slots)
     eng = gw.WalkEngine(algorithm=algo, maxhops=maxhops, p=p, q=q, alpha=alpha, term_prob=term, seed=seed,
                         walkpersource=wps, record_paths=paths, cache_size=cache, zero_copy=zero_copy,
-                        zero_threshold=zero_threshold)
+                        zero_threshold=zero_threshold, learned_mode=learned_mode)
     eng.set_host_graph(beg, csr, vb, eb)
     eng.init_walkers(algo, wps, seed)
     st = eng.run(policy)
@@ -75,7 +75,8 @@ def test_ooc_learned_policy_same_walks(gw, oracle):
     the walks stay those of the plain policy and of the oracle."""
     beg, csr = graph(oracle, scale=14, ef=8, sym=False, cap=12000, seed=8)
     e1, s1 = run_ooc(gw, beg, csr, 16, 4, algo=0, maxhops=30, paths=0, policy=0)
-    e2, s2 = run_ooc(gw, beg, csr, 16, 4, algo=0, maxhops=30, paths=0, policy=1)
+    e2, s2 = run_ooc(gw, beg, csr, 16, 4, algo=0, maxhops=30, paths=0, policy=1,
+                     learned_mode=gw.GW_LEARNED_EVICT | gw.GW_LEARNED_ZERO_SWITCH)
     h1, h2 = e1.hashes(), e2.hashes()
     assert np.array_equal(h1, h2)
     V = len(beg) - 1
@@ -91,6 +92,33 @@ def test_ooc_learned_policy_same_walks(gw, oracle):
     assert np.array_equal(e2.hashes(), h1)
     e1.close()
     e2.close()
+
+
+def test_learned_zero_switch(gw, oracle):
+    """The learned zero-copy switch.  On a fresh handle no tail has been
+    timed, so the learned run (default parts: the switch alone) takes exactly
+    the plain schedule -- GOWalker's zero_threshold -- and times its tail;
+    the next learned run prices each load against that tail and may switch
+    at another iteration.  Every run walks the oracle's walks."""
+    beg, csr = graph(oracle, scale=15, ef=10, sym=False, cap=20000, seed=12)
+    V = len(beg) - 1
+    ref = oracle.walk(beg, csr, oracle.make_cfg(algo=0, maxhops=40, p=0.5, q=2.0, seed=5), 0, V, paths=False)
+    e0, s0 = run_ooc(gw, beg, csr, 16, 4, algo=0, maxhops=40, paths=0, policy=0, zero_copy=1, zero_threshold=300)
+    e1, s1 = run_ooc(gw, beg, csr, 16, 4, algo=0, maxhops=40, paths=0, policy=1, zero_copy=1, zero_threshold=300)
+    assert np.array_equal(e0.hashes(), ref["hashes"])
+    assert np.array_equal(e1.hashes(), ref["hashes"])
+    assert s0["zero_copy_steps"] > 0
+    for k in ("iterations", "block_loads", "zero_copy_steps", "h2d_bytes"):
+        assert s1[k] == s0[k], k
+    assert s1["learned_iterations"] == 0
+    e1.init_walkers(0, 1, 5)
+    s2 = e1.run(gw.GW_POLICY_LEARNED)
+    assert np.array_equal(e1.hashes(), ref["hashes"])
+    assert s2["steps"] == s0["steps"] and s2["learned_iterations"] <= 1
+    if s2["learned_iterations"] == 1:
+        assert s2["zero_copy_steps"] > 0
+    e0.close()
+    e1.close()
 
 
 def test_ooc_rejects_tiny_cache(gw, oracle):
@@ -268,7 +296,8 @@ def test_trained_predictor_beats_carrying_demand_forward(gw, oracle, case):
         wps, bound = 1, 0.95
     vb, eb = split_equal_edge_mass(beg, nb)
     eng = gw.WalkEngine(algorithm=algo, maxhops=maxhops, p=0.5, q=2.0, alpha=0.2, seed=5, record_paths=0,
-                        cache_size=cache_for(beg, eb, slots), learned_sync=1, **kw)
+                        cache_size=cache_for(beg, eb, slots), learned_sync=1, learned_mode=gw.GW_LEARNED_EVICT,
+                        **kw)
     eng.set_host_graph(beg, csr, vb, eb)
     eng.init_walkers(algo, wps, 5)
     st = eng.run(gw.GW_POLICY_LEARNED)
