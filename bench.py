@@ -477,9 +477,10 @@ def run_ooc_bench(args, wl):
                                         "current block until N(prev) is needed",
                            "prefetch": not args.no_prefetch, "compressed_blocks": not args.no_compress,
                            "zero_copy_tail": {"on": bool(args.zero_copy), "zero_threshold_walkers": zero_threshold},
-                           "learned_mode": {1: "forecast eviction", 2: "zero-copy switch priced by measured costs",
-                                            3: "forecast eviction and zero-copy switch"}[
-                               args.learned_mode or gw.GW_LEARNED_DEFAULT],
+                           "learned_mode": {0: "automatic: forecast eviction and zero-copy switch, then the "
+                                               "switch alone, then the faster",
+                                            1: "forecast eviction", 2: "zero-copy switch priced by measured costs",
+                                            3: "forecast eviction and zero-copy switch"}[args.learned_mode],
                            "vertices": V, "edges": len(csr), "blocks": wl["nblocks"], "cache_bytes": wl["cache"],
                            "walkers": V * wl["wps"], "graph_in": "pinned host memory",
                            "l2": "every run copies the graph's blocks from the host into a 1.5 GB-class device "
@@ -943,7 +944,8 @@ def main():
                          "memory)")
     ap.add_argument("--learned-mode", type=int, default=0,
                     help="out-of-core learned policy parts: 1 forecast eviction, 2 zero-copy switch priced by "
-                         "measured costs, 3 both (default 0: the library's default, the switch)")
+                         "measured costs, 3 both (default 0: automatic -- both, then the switch alone, then the "
+                         "faster)")
     ap.add_argument("--zero-scale", type=float, default=1.0,
                     help="out-of-core: multiply GOWalker's zero-mode threshold by this factor (default 1)")
     ap.add_argument("--launch-per-hop", action="store_true",

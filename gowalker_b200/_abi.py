@@ -20,7 +20,7 @@ GW_EDGES_SYMMETRIC, GW_EDGES_SORT, GW_EDGES_DEDUP = 1, 2, 4
 GW_SPLIT_REFERENCE, GW_SPLIT_EQUAL_EDGES = 0, 1
 GW_LAUNCH_PERSISTENT, GW_LAUNCH_PER_HOP = 0, 1
 GW_LEARNED_EVICT, GW_LEARNED_ZERO_SWITCH = 1, 2
-GW_LEARNED_DEFAULT = GW_LEARNED_ZERO_SWITCH
+GW_LEARNED_AUTO = 0
 
 # Every symbol include/gowalker.h declares.
 EXPORTS = (
@@ -92,10 +92,12 @@ class GwStats(ctypes.Structure):
         ("coop_small_attempts", ctypes.c_uint64),
         ("coop_large_steps", ctypes.c_uint64),
         ("coop_large_attempts", ctypes.c_uint64),
+        ("learned_parts", ctypes.c_uint32),
+        ("reserved2", ctypes.c_uint32),
     ]
 
     def as_dict(self):
-        return {n: (getattr(self, n) if n != "reserved" else None) for n, _ in self._fields_ if n != "reserved"}
+        return {n: getattr(self, n) for n, _ in self._fields_ if not n.startswith("reserved")}
 
 
 _LIB = None

@@ -132,6 +132,10 @@ struct OocState {
     // the last zero-copy tail's time per mapped sector (seconds; 0 = none
     // timed yet): the learned switch's price of a mapped read on this link
     double tail_s_per_sector = 0.0;
+    // learned_mode 0 (automatic): time per step of each set of learned parts
+    // tried on the workload `auto_sig` (index = the parts' bits; < 0 = untried)
+    RunSignature auto_sig;
+    double auto_ms_per_step[4] = {-1.0, -1.0, -1.0, -1.0};
     float *d_trace_x = nullptr, *d_trace_col = nullptr, *d_trace_y = nullptr;
     float *d_train_x = nullptr, *d_pred = nullptr, *d_pred_res = nullptr;  // forecast log demand, its change
     float *d_emass = nullptr, *d_vfrac = nullptr, *d_prev_col = nullptr, *d_ema = nullptr;
@@ -896,23 +900,43 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     // win at the end, where fewer walkers are left to the mapped tail.
     const RunSignature sig = run_signature(this);
     if (policy == GW_POLICY_LEARNED && o.learned_lost && o.lost_sig == sig) reverted = true;
-    const uint32_t lmode = cfg.learned_mode ? cfg.learned_mode : GW_LEARNED_DEFAULT;
-    // The learned zero-mode switch prices the next load against the tail:
-    // the walkers it makes runnable (the plain rule's score) x steps a
-    // runnable walker takes per iteration (rho, over the last kRhoWindow
-    // iterations) x mapped sectors per step (sigma, modelled by the step
-    // kernels on this run's resident steps) x time per mapped sector (tau,
-    // timed on this handle's last tail) against the time of an iteration
-    // (host clock between decisions, averaged).  Until a tail has been
-    // timed, GOWalker's zero_threshold decides.
+    // learned parts: the caller's, or (learned_mode 0) tried run by run --
+    // the forecast eviction with the switch, then the switch alone -- and
+    // from then on the faster of the two on this workload
+    const bool auto_mode = cfg.learned_mode == 0;
+    if (auto_mode && !(o.auto_sig == sig)) {
+        o.auto_sig = sig;
+        for (double &x : o.auto_ms_per_step) x = -1.0;
+    }
+    uint32_t lmode = cfg.learned_mode;
+    if (auto_mode) {
+        const uint32_t both = GW_LEARNED_EVICT | GW_LEARNED_ZERO_SWITCH, sw = GW_LEARNED_ZERO_SWITCH;
+        if (o.auto_ms_per_step[both] < 0.0) lmode = both;
+        else if (o.auto_ms_per_step[sw] < 0.0) lmode = sw;
+        else lmode = o.auto_ms_per_step[both] <= o.auto_ms_per_step[sw] ? both : sw;
+    }
+    // The learned zero-mode switch prices the next iteration against the
+    // tail.  The next load makes `score` walkers runnable (the plain rule's
+    // score); they take rho steps each (steps per runnable walker over the
+    // last kSwitchWindow iterations); in the tail each step would read sigma
+    // mapped sectors (modelled by the step kernels on this run's resident
+    // steps) at tau seconds a sector (timed on this handle's last tail).  An
+    // iteration's price is its time (host clock between decisions, averaged
+    // over the same window): switching saves all of it.  The switch is taken once score * rho * sigma * tau stays below that
+    // price for kSwitchRun decisions in a row, and only while the tail's
+    // upper bound (every live walker walking to maxhops, at most what is
+    // left of the population's steps) would take no longer than the run
+    // so far.  Until a tail has been timed, GOWalker's zero_threshold decides.
     const bool cost_switch = policy == GW_POLICY_LEARNED && !reverted && (lmode & GW_LEARNED_ZERO_SWITCH) &&
                              cfg.zero_copy && o.tail_s_per_sector > 0.0;
-    constexpr uint32_t kRhoWindow = 16;
-    std::deque<std::pair<uint64_t, uint64_t>> rho_hist;  // (steps, runnable) at each decision
-    double iter_ms_avg = 0.0;
-    std::chrono::steady_clock::time_point t_last_dec{};
-    bool have_last_dec = false;
-    uint32_t switch_iter = 0;
+    constexpr uint32_t kSwitchWindow = 16, kSwitchRun = 4;
+    struct SwitchSample {
+        uint64_t steps, runnable;
+        double host_ms;
+    };
+    std::deque<SwitchSample> sw_hist;
+    const auto t_run0 = std::chrono::steady_clock::now();
+    uint32_t sw_ok = 0, switch_iter = 0;
     uint64_t phase_steps_mark = 0;
     int last_phase = -1;
     double pred_err_sum = 0.0, persist_err_sum = 0.0;
@@ -1127,25 +1151,27 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         // ---- learned zero-mode switch (prices: see cost_switch above)
         bool zero_now = false;
         if (cost_switch) {
-            const auto tnow = std::chrono::steady_clock::now();
-            if (have_last_dec) {
-                const double ms = std::chrono::duration<double, std::milli>(tnow - t_last_dec).count();
-                iter_ms_avg = iter_ms_avg > 0.0 ? iter_ms_avg + (ms - iter_ms_avg) / 8.0 : ms;
-            }
-            t_last_dec = tnow;
-            have_last_dec = true;
-            rho_hist.emplace_back(steps_now, h_ctr[kCtrRunnable]);
-            if (rho_hist.size() > kRhoWindow + 1) rho_hist.pop_front();
-            const uint64_t dsteps = steps_now - rho_hist.front().first;
-            const uint64_t drun = h_ctr[kCtrRunnable] - rho_hist.front().second;
-            if ((d.action == 1 || d.action == 2) && rho_hist.size() > kRhoWindow && drun > 0 && steps_now > 0) {
-                const double rho = (double)dsteps / (double)drun;
+            const double host_ms =
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_run0).count();
+            sw_hist.push_back({steps_now, h_ctr[kCtrRunnable], host_ms});
+            if (sw_hist.size() > kSwitchWindow + 1) sw_hist.pop_front();
+            const SwitchSample &w0 = sw_hist.front();
+            const uint64_t drun = h_ctr[kCtrRunnable] - w0.runnable;
+            bool ok = false;
+            if ((d.action == 1 || d.action == 2) && sw_hist.size() > kSwitchWindow && drun > 0 && steps_now > 0) {
+                const double rho = (double)(steps_now - w0.steps) / (double)drun;
                 const double sigma = (double)h_ctr[kCtrModelSectors] / (double)steps_now;
-                const double load_gain_ms = (double)d.score * rho * sigma * o.tail_s_per_sector * 1e3;
-                if (load_gain_ms < iter_ms_avg) {
-                    zero_now = true;
-                    switch_iter = iters;
-                }
+                const double sector_ms = sigma * o.tail_s_per_sector * 1e3;  // per tail step
+                const double iter_price_ms = (host_ms - w0.host_ms) / kSwitchWindow;
+                const double total_steps = (double)nwalkers * (double)cfg.maxhops;
+                const double tail_upper_ms =
+                    std::min((double)d.live * (double)cfg.maxhops, std::max(total_steps - (double)steps_now, 0.0)) * sector_ms;
+                ok = (double)d.score * rho * sector_ms < iter_price_ms && tail_upper_ms < host_ms;
+            }
+            sw_ok = ok ? sw_ok + 1 : 0;
+            if (sw_ok >= kSwitchRun) {
+                zero_now = true;
+                switch_iter = iters;
             }
         }
         // progress guard: a learned choice that moved no walker hands the
@@ -1223,7 +1249,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             zc_steps += h_ctr[kCtrSteps] - before[kCtrSteps];
             // the price of a mapped sector on this link (a short tail,
             // latency-bound, overprices it: the switch then comes later)
-            if (h_ctr[kCtrZcSectors] - before[kCtrZcSectors] >= (1ull << 16))
+            if (h_ctr[kCtrZcSectors] - before[kCtrZcSectors] >= (1ull << 12))
                 o.tail_s_per_sector = tail_ms * 1e-3 / (double)(h_ctr[kCtrZcSectors] - before[kCtrZcSectors]);
             h2d += 32ull * (h_ctr[kCtrZcSectors] - before[kCtrZcSectors]);
             zc_sectors += h_ctr[kCtrZcSectors] - before[kCtrZcSectors];
@@ -1442,6 +1468,7 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                     switch_iter ? ", entered by the learned switch" : "", (unsigned)loads, learned_iters);
         stats->learned_iterations = learned_iters;
         stats->policy_reverted = reverted ? 1u : 0u;
+        stats->learned_parts = policy == GW_POLICY_LEARNED && !reverted ? lmode : 0u;
         stats->train_loss = (policy == GW_POLICY_LEARNED && o.h_loss) ? *o.h_loss : 0.f;
         stats->pred_error = pred_err_n ? (float)(pred_err_sum / pred_err_n) : 0.f;
         stats->persist_error = pred_err_n ? (float)(persist_err_sum / pred_err_n) : 0.f;
@@ -1464,8 +1491,24 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         o.have_plain = true;
         o.plain_sig = sig;
         o.plain_ms_per_step = (double)run_ms / steps_d;
-    } else if (policy == GW_POLICY_LEARNED && !reverted && o.have_plain && o.plain_sig == sig) {
-        if ((double)run_ms / steps_d > o.plain_ms_per_step * 1.02) {
+    } else if (policy == GW_POLICY_LEARNED && !reverted) {
+        // automatic parts: a run counts for its parts unless its tail came
+        // at GOWalker's threshold because no tail had been timed yet
+        if (auto_mode && (cost_switch || !cfg.zero_copy || zc_steps == 0))
+            o.auto_ms_per_step[lmode] = (double)run_ms / steps_d;
+    }
+    // in automatic mode the judge waits until both sets of parts have run,
+    // and then compares the faster
+    double learned_ms_per_step = (double)run_ms / steps_d;
+    bool judge_now = policy == GW_POLICY_LEARNED && !reverted && o.have_plain && o.plain_sig == sig;
+    if (judge_now && auto_mode) {
+        const double a = o.auto_ms_per_step[GW_LEARNED_EVICT | GW_LEARNED_ZERO_SWITCH],
+                     b = o.auto_ms_per_step[GW_LEARNED_ZERO_SWITCH];
+        judge_now = a >= 0.0 && b >= 0.0;
+        learned_ms_per_step = std::min(a, b);
+    }
+    if (judge_now) {
+        if (learned_ms_per_step > o.plain_ms_per_step * 1.02) {
             o.learned_lost = true;
             o.lost_sig = sig;
         }

@@ -115,8 +115,9 @@ typedef struct gw_config {
                                  stops once reverted */
     uint32_t launch_mode;     /* in-core: GW_LAUNCH_PERSISTENT (default) or GW_LAUNCH_PER_HOP, the
                                  plain form kept for comparison (unweighted walks only) */
-    uint32_t learned_mode;    /* learned policy parts: GW_LEARNED_EVICT | GW_LEARNED_ZERO_SWITCH;
-                                 0 = GW_LEARNED_DEFAULT */
+    uint32_t learned_mode;    /* learned policy parts: GW_LEARNED_EVICT | GW_LEARNED_ZERO_SWITCH, or
+                                 GW_LEARNED_AUTO (0, default): both parts on the first learned run of
+                                 a workload, the switch alone on the next, then the faster */
     uint32_t reserved[2];
 } gw_config;
 
@@ -128,7 +129,7 @@ typedef struct gw_config {
                                       reads, times the measured time per mapped sector, is below the
                                       measured time of an iteration (in place of the fixed zero_threshold,
                                       which is used until this handle has timed a zero-copy tail) */
-#define GW_LEARNED_DEFAULT GW_LEARNED_ZERO_SWITCH
+#define GW_LEARNED_AUTO 0u
 
 /* in-core launch modes */
 #define GW_LAUNCH_PERSISTENT 0u /* one persistent work-stealing kernel runs every walker to the end */
@@ -163,6 +164,8 @@ typedef struct gw_stats {
     uint64_t coop_small_attempts;
     uint64_t coop_large_steps;   /* hard steps evaluated with candidate loads (in-core) */
     uint64_t coop_large_attempts;
+    uint32_t learned_parts;      /* learned out-of-core runs: the GW_LEARNED_* parts this run used */
+    uint32_t reserved2;
 } gw_stats;
 
 /* ------------------------------------------------------------------ basics */
