@@ -457,7 +457,17 @@ def run_ooc_bench(args, wl):
             kernel_ms_per_run=sum(s["kernel_ms"] for s in sts) / args.steps,
             bucket_ms_per_run=sum(s["bucket_ms"] for s in sts) / args.steps,
             learned_iterations_per_run=sum(s["learned_iterations"] for s in sts) / args.steps,
-            reverted_runs=sum(s["policy_reverted"] for s in sts))
+            reverted_runs=sum(s["policy_reverted"] for s in sts),
+            learned_parts=[s["learned_parts"] for s in sts])
+        # the copy stream: busy time of the block copies, and the block bytes
+        # (H2D bytes less the mapped sectors of the tail) over that time
+        copy_ms = sum(s["copy_ms"] for s in sts)
+        block_bytes = sum(s["h2d_bytes"] - 32 * s["zero_copy_sectors"] for s in sts)
+        res[arm]["copy_stream"] = {
+            "busy_ms_per_run": copy_ms / args.steps,
+            "busy_frac": copy_ms / max(sum(ev[0].elapsed_time(ev[1]) for ev, _, _ in rec[arm]), 1e-9),
+            "block_gb_per_s_while_busy": block_bytes / max(copy_ms / 1e3, 1e-9) / 1e9,
+            "nominal_pcie_gen5_x16_gbs": PCIE_GEN5_X16_GBS}
         if arm == "learned":
             res[arm]["pred_error"] = sts[-1]["pred_error"]
             res[arm]["persist_error"] = sts[-1]["persist_error"]

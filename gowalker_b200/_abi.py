@@ -93,7 +93,8 @@ class GwStats(ctypes.Structure):
         ("coop_large_steps", ctypes.c_uint64),
         ("coop_large_attempts", ctypes.c_uint64),
         ("learned_parts", ctypes.c_uint32),
-        ("reserved2", ctypes.c_uint32),
+        ("copy_ms", ctypes.c_float),
+        ("zero_copy_sectors", ctypes.c_uint64),
     ]
 
     def as_dict(self):

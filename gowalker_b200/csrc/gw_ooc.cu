@@ -654,10 +654,12 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         cudaEventCreate(&td1);
         cudaEventCreate(&tin0);
         cudaEventCreate(&tin1);
-        for (auto &pr : tcp) {
-            cudaEventCreate(&pr[0]);
-            cudaEventCreate(&pr[1]);
-        }
+    }
+    // prefetch copies are timed on the copy stream in every run
+    // (gw_stats.copy_ms): two event pairs, each read when it comes round
+    for (auto &pr : tcp) {
+        cudaEventCreate(&pr[0]);
+        cudaEventCreate(&pr[1]);
     }
     EvRing bring, kring, rring;  // re-bucketing, step kernel, runnable pass (trace)
     bring.create();
@@ -686,9 +688,8 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     // plain copy into the slot, or the compressed copy into the staging
     // buffer `stage`; decode_block then expands a compressed one into the
     // slot.  A prefetched block is uploaded on the copy stream and decoded on
-    // the compute stream when it is installed; the two staging buffers
-    // alternate, and an upload is issued only after the decision that waited
-    // for the re-bucketing following the decode that last read its buffer.
+    // the decode stream right behind it; the two staging buffers alternate,
+    // and an upload waits for the decode that last read its buffer.
     auto upload_block = [&](uint32_t b, uint32_t *sc, cudaStream_t cs, uint32_t stage, uint64_t *bytes) -> int {
         const uint64_t ne = eblocks[b + 1] - eblocks[b];
         if (o.weighted && ne) {
@@ -957,6 +958,22 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     }
     cudaEvent_t staged_ev = nullptr;
     if (prefetch) cudaEventCreateWithFlags(&staged_ev, cudaEventDisableTiming);
+    // A prefetched compressed block is decoded on a stream of its own right
+    // behind its copy, so neither the compute stream (install, step,
+    // re-bucketing) nor the next copy waits for the decode.  The decode
+    // writes the staging slot, which no step reads (it left the block table
+    // when its block was evicted, before the step that precedes the decision
+    // this copy follows); the next upload into the same compressed-copy
+    // buffer waits for the decode that last read it.
+    cudaStream_t s_dec = nullptr;
+    cudaEvent_t ev_up = nullptr, ev_decoded[2] = {nullptr, nullptr};
+    bool decoded_rec[2] = {false, false};
+    if (prefetch && o.compressed) {
+        cudaStreamCreateWithFlags(&s_dec, cudaStreamNonBlocking);
+        cudaEventCreateWithFlags(&ev_up, cudaEventDisableTiming);
+        for (auto &e : ev_decoded) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    }
+    bool staged_decoded = false;
     // Decisions run on their own stream when prefetching: they read the
     // counts of the last re-bucketing (ev_buck) and never wait for a copy,
     // so the next block's upload queues right behind the one in flight.
@@ -986,9 +1003,9 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             }
             const uint32_t b = (uint32_t)staged_block;
             uint32_t *sc = o.slot_csr + (uint64_t)staging_slot * o.slot_stride_words;
-            // a compressed block is expanded here, on the compute stream, so
-            // the next block's copy overlaps this decode as well as the step
-            if ((st = decode_block(b, sc, s, staged_stage))) break;
+            // a compressed block was expanded on the decode stream (staged_ev
+            // follows its decode), else it is expanded here
+            if (!staged_decoded && (st = decode_block(b, sc, s, staged_stage))) break;
             if (!o.compressed) {  // a decoded block was checked by its decoder
                 k_validate_block<<<num_sms * 4, 256, 0, s>>>(sc, eblocks[b + 1] - eblocks[b], nverts, d_err);
                 launches++;
@@ -1133,12 +1150,6 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 t_install += ms;
                 tin_live = false;
             }
-            for (int k = 0; k < 2; ++k)
-                if (tcp_live[k] && cudaEventQuery(tcp[k][1]) == cudaSuccess &&
-                    cudaEventElapsedTime(&ms, tcp[k][0], tcp[k][1]) == cudaSuccess) {
-                    t_copy += ms;
-                    tcp_live[k] = false;
-                }
             cudaGetLastError();  // a query of work still in flight is not an error of the run
         }
         if ((uint32_t)h_ctr[kCtrCount] != 0) {
@@ -1281,22 +1292,33 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
             uint64_t bytes = 0;
             upload_stage ^= o.nstage == 2 ? 1u : 0u;
             staged_stage = upload_stage;
-            if (trace) {
-                if (tcp_live[tcp_next]) {  // still unread: wait for it
-                    cudaEventSynchronize(tcp[tcp_next][1]);
-                    float ms = 0.f;
-                    if (cudaEventElapsedTime(&ms, tcp[tcp_next][0], tcp[tcp_next][1]) == cudaSuccess) t_copy += ms;
-                    tcp_live[tcp_next] = false;
-                }
-                cudaEventRecord(tcp[tcp_next][0], s_copy);
+            if (tcp_live[tcp_next]) {  // the copy two uploads ago: read its time
+                cudaEventSynchronize(tcp[tcp_next][1]);
+                float ms = 0.f;
+                if (cudaEventElapsedTime(&ms, tcp[tcp_next][0], tcp[tcp_next][1]) == cudaSuccess) t_copy += ms;
+                tcp_live[tcp_next] = false;
             }
+            if (s_dec && decoded_rec[upload_stage] &&
+                (st = cuda(cudaStreamWaitEvent(s_copy, ev_decoded[upload_stage], 0), "decode wait")))
+                break;
+            cudaEventRecord(tcp[tcp_next][0], s_copy);
             if ((st = upload_block(b, sc, s_copy, upload_stage, &bytes))) break;
-            if (trace) {
-                cudaEventRecord(tcp[tcp_next][1], s_copy);
-                tcp_live[tcp_next] = true;
-                tcp_next ^= 1u;
+            cudaEventRecord(tcp[tcp_next][1], s_copy);
+            tcp_live[tcp_next] = true;
+            tcp_next ^= 1u;
+            if (s_dec) {
+                if ((st = cuda(cudaEventRecord(ev_up, s_copy), "event")) ||
+                    (st = cuda(cudaStreamWaitEvent(s_dec, ev_up, 0), "copy wait")) ||
+                    (st = decode_block(b, sc, s_dec, upload_stage)) ||
+                    (st = cuda(cudaEventRecord(ev_decoded[upload_stage], s_dec), "event")) ||
+                    (st = cuda(cudaEventRecord(staged_ev, s_dec), "event")))
+                    break;
+                decoded_rec[upload_stage] = true;
+                staged_decoded = true;
+            } else {
+                if ((st = cuda(cudaEventRecord(staged_ev, s_copy), "event"))) break;
+                staged_decoded = false;
             }
-            if ((st = cuda(cudaEventRecord(staged_ev, s_copy), "event"))) break;
             h2d += bytes;
             loads++;
             staged_block = (int)b;
@@ -1411,6 +1433,17 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         cudaStreamSynchronize(s_copy);  // a staged copy may still be in flight
         cudaEventDestroy(staged_ev);
     }
+    for (int k = 0; k < 2; ++k) {
+        float ms = 0.f;
+        if (tcp_live[k] && cudaEventElapsedTime(&ms, tcp[k][0], tcp[k][1]) == cudaSuccess) t_copy += ms;
+        tcp_live[k] = false;
+    }
+    if (s_dec) {
+        cudaStreamSynchronize(s_dec);  // and its decode
+        cudaStreamDestroy(s_dec);
+        cudaEventDestroy(ev_up);
+        for (auto &e : ev_decoded) cudaEventDestroy(e);
+    }
     if (ds != s) {
         cudaStreamSynchronize(ds);
         cudaStreamDestroy(ds);
@@ -1435,10 +1468,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         cudaEventDestroy(td1);
         cudaEventDestroy(tin0);
         cudaEventDestroy(tin1);
-        for (auto &pr : tcp) {
-            cudaEventDestroy(pr[0]);
-            cudaEventDestroy(pr[1]);
-        }
+    }
+    for (auto &pr : tcp) {
+        cudaEventDestroy(pr[0]);
+        cudaEventDestroy(pr[1]);
     }
     if (st) return st;
     last_hash_sum = h_ctr[kCtrHashSum];
@@ -1469,6 +1502,8 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         stats->learned_iterations = learned_iters;
         stats->policy_reverted = reverted ? 1u : 0u;
         stats->learned_parts = policy == GW_POLICY_LEARNED && !reverted ? lmode : 0u;
+        stats->copy_ms = (float)t_copy;
+        stats->zero_copy_sectors = zc_sectors;
         stats->train_loss = (policy == GW_POLICY_LEARNED && o.h_loss) ? *o.h_loss : 0.f;
         stats->pred_error = pred_err_n ? (float)(pred_err_sum / pred_err_n) : 0.f;
         stats->persist_error = pred_err_n ? (float)(persist_err_sum / pred_err_n) : 0.f;

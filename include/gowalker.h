@@ -165,7 +165,10 @@ typedef struct gw_stats {
     uint64_t coop_large_steps;   /* hard steps evaluated with candidate loads (in-core) */
     uint64_t coop_large_attempts;
     uint32_t learned_parts;      /* learned out-of-core runs: the GW_LEARNED_* parts this run used */
-    uint32_t reserved2;
+    float copy_ms;               /* out-of-core with prefetch: time the copy stream spent on block copies
+                                    (CUDA events around each upload) */
+    uint64_t zero_copy_sectors;  /* 32-byte sectors the zero-copy tail read from mapped host memory (in
+                                    h2d_bytes at 32 bytes each) */
 } gw_stats;
 
 /* ------------------------------------------------------------------ basics */
