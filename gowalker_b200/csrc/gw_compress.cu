@@ -128,69 +128,26 @@ bool compress_block(const uint64_t *beg, const uint32_t *csr, uint32_t nv, uint6
     run([&](uint32_t a, uint32_t b) {
         for (uint32_t v = a; v < b; ++v) encode_vertex(csr + (beg[v] - e0), beg[v + 1] - beg[v], pay + off[v]);
     });
+    // pieces of about equal payload, cut at multiples of 32 vertices
+    out.piece_v[0] = 0;
+    out.piece_v[kPieces] = nv;
+    for (uint32_t k = 1; k < kPieces; ++k) {
+        const uint64_t target = payload * k / kPieces;
+        uint32_t v = (uint32_t)(std::lower_bound(off.begin(), off.begin() + nv, target) - off.begin());
+        v &= ~31u;
+        out.piece_v[k] = std::max(v, out.piece_v[k - 1]);
+    }
+    for (uint32_t k = 0; k <= kPieces; ++k) out.piece_g[k] = (uint32_t)gstart[out.piece_v[k]];
     return true;
 }
 
-// One chunk of k ids at byte `pos` of the payload, decoded by the warp: the
-// lanes load the chunk's bytes as 34 aligned 32-bit words in one coalesced
-// round (lane i: words i and, for lanes 0-1, i + 32; a chunk spans at most
-// 3 + 5 + 124 bytes), then every lane takes its delta's bits from the words
-// by shuffles -- no lane waits for a second dependent load.  Words past the
-// buffer end (`limit` words from `pay`) read as zero.  Returns the next
-// chunk's position; sets *bad on a malformed chunk.
-__device__ __forceinline__ uint64_t decode_chunk(const uint8_t *__restrict__ pay, uint64_t pos, uint32_t k,
-                                                 uint64_t payload_bytes, uint64_t limit, uint32_t lane,
-                                                 uint32_t *__restrict__ row, uint32_t nverts, bool &bad_id, bool &bad)
-{
-    const uint64_t w0 = pos >> 2;
-    const uint32_t sh = (uint32_t)(pos & 3u) * 8u;
-    const uint32_t *__restrict__ words = reinterpret_cast<const uint32_t *>(pay);
-    const uint32_t wa = (w0 + lane < limit) ? __ldg(words + w0 + lane) : 0u;
-    const uint32_t wb = (lane < 2u && w0 + 32u + lane < limit) ? __ldg(words + w0 + 32u + lane) : 0u;
-    auto word = [&](uint32_t q) {  // word q of the window (q < 34), from the lane holding it
-        const uint32_t x = __shfl_sync(0xFFFFFFFFu, wa, q & 31u);
-        const uint32_t y = __shfl_sync(0xFFFFFFFFu, wb, q & 31u);
-        return q < 32u ? x : y;
-    };
-    const uint64_t head = (((uint64_t)word(1) << 32) | word(0)) >> sh;  // width byte, then the first id
-    const uint32_t w = (uint32_t)head & 0xFFu;
-    const uint64_t packed = ((uint64_t)(k - 1) * w + 7) >> 3;
-    if (w > 32 || pos + 5 + packed > payload_bytes) {
-        bad = true;
-        return pos;
-    }
-    // every lane shuffles (the same control flow), lanes 1 .. k-1 keep a delta
-    const uint32_t bp = lane ? (lane - 1) * w : 0u;
-    const uint32_t bo = sh + 40u + bp;  // bit offset of the delta from word 0
-    const uint32_t q = bo >> 5;
-    const uint64_t acc = ((uint64_t)word(q + 1) << 32) | word(q);
-    uint32_t x;
-    if (lane == 0) {
-        x = (uint32_t)(head >> 8);
-    } else if (lane < k && w != 0) {
-        const uint64_t mask = (w == 32) ? 0xFFFFFFFFull : ((1ull << w) - 1);
-        const uint32_t z = (uint32_t)((acc >> (bo & 31u)) & mask);
-        x = (z >> 1) ^ (0u - (z & 1u));
-    } else {
-        x = 0;
-    }
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-        if (lane >= (uint32_t)o) x += y;
-    }
-    if (lane < k) {
-        row[lane] = x;
-        bad_id |= x >= nverts;
-    }
-    return pos + 5 + packed;
-}
-
-// The same chunk decode from a warp's shared-memory copy of the payload
-// words [base, base + staged): every lane reads the words it needs directly.
-// `end` is the byte just past the staged vertices' chunks; a chunk reaching
-// past it is malformed.  Reads stay inside the staged words plus a 36-word
-// tail (lanes past k read words they do not use).
+// One chunk of k ids at byte `pos` of the payload, decoded by the warp from
+// its shared-memory window of the payload words [base, base + kWindowWords):
+// lane 0 takes the first id, lane i < k delta i (its bits read straight from
+// the window), and a warp prefix sum (mod 2^32) rebuilds the ids.  `end` is
+// the byte past the chunks this task may read; a chunk reaching past it is
+// malformed.  A chunk spans at most 3 + 5 + 124 bytes, so its words lie in
+// [off, off + 35) with off = pos / 4 - base; the caller keeps off <= kSlideAt.
 __device__ __forceinline__ uint64_t decode_chunk_sm(const uint32_t *sm, uint64_t base, uint64_t pos, uint64_t end,
                                                     uint32_t k, uint32_t lane, uint32_t *__restrict__ row,
                                                     uint32_t nverts, bool &bad_id, bool &bad)
@@ -228,35 +185,51 @@ __device__ __forceinline__ uint64_t decode_chunk_sm(const uint32_t *sm, uint64_t
     return pos + 5 + packed;
 }
 
-constexpr uint32_t kStageWords = 1024;  // a warp's shared-memory copy of one vertex batch's payload (4 KB)
+constexpr uint32_t kWindowWords = 1024 + 36;  // a warp's shared-memory window of the payload (4.1 KB)
+constexpr uint32_t kSlideAt = 1024;           // a chunk starting past this word of the window slides it
 constexpr uint32_t kDecodeThreads = 256;
 
 // Warp tasks: task t < ntv decodes vertices [32t, 32t + 32) that have at most
 // 32 chunks (lane i loads vertex 32t + i's payload offset and neighbour
 // range, coalesced, and the warp walks the 32 in turn); task ntv + g decodes
-// split group g (32 chunks of a larger vertex).  Within a chunk, lane i
-// extracts delta i (lane 0 the first id) and a warp prefix sum (mod 2^32)
-// rebuilds the ids.  Every id written is checked against nverts (the
-// validation of a plain block copy, done here in the same pass).
+// split group g (32 chunks of a larger vertex).  A task's chunks are read
+// from a window of the payload in shared memory, filled by the warp with
+// coalesced, independent loads and slid forward when the next chunk would
+// run past it, so the only dependent chain -- each chunk's position follows
+// from the previous chunk's width byte -- runs through shared memory.  Every
+// id written is checked against nverts (the validation of a plain block
+// copy, done here in the same pass).
 __global__ void __launch_bounds__(kDecodeThreads)
     k_decode_block(const uint8_t *__restrict__ src, uint64_t split_off, uint32_t nsplit, uint64_t payload_off,
                    uint64_t payload_bytes, uint32_t nv, const uint64_t *__restrict__ beg, uint32_t v0, uint64_t e0,
-                   uint64_t ne, uint32_t nverts, uint32_t *__restrict__ out, uint32_t *err)
+                   uint64_t ne, uint32_t nverts, uint32_t *__restrict__ out, uint32_t *err, uint64_t t_lo,
+                   uint64_t t_hi, uint64_t g_lo, uint64_t g_hi)
 {
-    // a vertex batch's payload bytes are contiguous: a warp copies them into
-    // shared memory with coalesced, independent loads, then decodes from there
-    __shared__ uint32_t s_stage[kDecodeThreads / 32][kStageWords + 36];
-    uint32_t *sm = s_stage[threadIdx.x >> 5];
+    __shared__ uint32_t s_win[kDecodeThreads / 32][kWindowWords];
+    uint32_t *sm = s_win[threadIdx.x >> 5];
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const uint32_t *voff = reinterpret_cast<const uint32_t *>(src);
     const uint32_t *split = reinterpret_cast<const uint32_t *>(src + split_off);
-    const uint8_t *pay = src + payload_off;
+    const uint32_t *pay_words = reinterpret_cast<const uint32_t *>(src + payload_off);
     const uint64_t limit = (payload_bytes + 8) >> 2;  // whole words of payload and padding
     const uint64_t ntv = ((uint64_t)nv + 31) >> 5;
-    const uint64_t ntasks = ntv + nsplit;
+    // this launch's tasks: vertex batches [t_lo, t_hi), then split groups [g_lo, g_hi)
+    const uint64_t nbt = t_hi - t_lo;
+    const uint64_t ntasks = nbt + (g_hi - g_lo);
     bool bad_id = false, bad = false;
-    for (uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntasks; t += nwarps) {
+    uint64_t base = ~0ull;  // first payload word in the window (~0: empty)
+    // make the window hold the chunk at byte `pos` (warp-uniform)
+    auto cover = [&](uint64_t pos) {
+        const uint64_t w = pos >> 2;
+        if (base != ~0ull && w >= base && w - base <= kSlideAt) return;
+        __syncwarp();  // every lane is done with the old window
+        base = w;
+        for (uint32_t i = lane; i < kWindowWords; i += 32) sm[i] = (base + i < limit) ? __ldg(pay_words + base + i) : 0u;
+        __syncwarp();
+    };
+    for (uint64_t task = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; task < ntasks; task += nwarps) {
+        const uint64_t t = task < nbt ? t_lo + task : ntv + g_lo + (task - nbt);
         if (t < ntv) {
             const uint64_t vi = (t << 5) + lane;
             uint64_t mpos = 0, mb0 = 0, mb1 = 0;
@@ -269,14 +242,78 @@ __global__ void __launch_bounds__(kDecodeThreads)
             // the batch's payload: [first vertex's offset, the next batch's)
             const uint64_t p0 = __shfl_sync(0xFFFFFFFFu, mpos, 0);
             const uint64_t p1 = __ldg(voff + (t << 5) + nvt);
-            const uint64_t base = p0 >> 2;
-            const uint64_t nwords = p1 > p0 ? ((p1 + 3) >> 2) - base + 2 : 0;
-            const bool staged = p1 >= p0 && p1 <= payload_bytes && nwords <= kStageWords;
-            if (staged) {
-                for (uint32_t i = lane; i < nwords; i += 32)
-                    sm[i] = (base + i < limit) ? __ldg(reinterpret_cast<const uint32_t *>(pay) + base + i) : 0u;
-                __syncwarp();
+            if (p1 < p0 || p1 > payload_bytes) {
+                bad = true;
+                continue;
             }
+            // every chunk of the batch reads words [p0 / 4, p1 / 4 + 2)
+            const uint64_t b_base = p0 >> 2, nwords = ((p1 + 3) >> 2) - b_base + 2;
+            if (nwords <= kWindowWords) {
+                // ---- the whole batch in the window: one fill, then each lane
+                // decodes its own vertex when it has one chunk (most do), and
+                // the warp decodes the chunks of the batch's larger vertices
+                __syncwarp();
+                base = b_base;
+                for (uint32_t i = lane; i < nwords; i += 32)
+                    sm[i] = (base + i < limit) ? __ldg(pay_words + base + i) : 0u;
+                __syncwarp();
+                const bool mine = (uint64_t)lane < nvt;
+                const bool range_ok = !mine || (mb1 >= mb0 && mb0 >= e0 && mb1 - e0 <= ne);
+                bad |= !range_ok;
+                const uint64_t d = (mine && range_ok) ? mb1 - mb0 : 0;
+                if (d >= 1 && d <= kChunkIds) {
+                    if (mpos < p0 || mpos + 5 > p1) {
+                        bad = true;
+                    } else {
+                        const uint32_t off = (uint32_t)((mpos >> 2) - base);
+                        const uint32_t sh = (uint32_t)(mpos & 3u) * 8u;
+                        const uint64_t head = (((uint64_t)sm[off + 1] << 32) | sm[off]) >> sh;
+                        const uint32_t w = (uint32_t)head & 0xFFu;
+                        if (w > 32 || mpos + 5 + (((d - 1) * w + 7) >> 3) > p1) {
+                            bad = true;
+                        } else {
+                            uint32_t *row = out + (mb0 - e0);
+                            uint32_t x = (uint32_t)(head >> 8);
+                            row[0] = x;
+                            bool over = x >= nverts;
+                            const uint64_t mask = (w == 32) ? 0xFFFFFFFFull : ((1ull << w) - 1);
+                            uint32_t bit = sh + 40u;  // from word `off`
+                            for (uint32_t i = 1; i < (uint32_t)d; ++i, bit += w) {
+                                const uint32_t q = off + (bit >> 5);
+                                const uint64_t acc = ((uint64_t)sm[q + 1] << 32) | sm[q];
+                                const uint32_t z = (uint32_t)((acc >> (bit & 31u)) & mask);
+                                x += (z >> 1) ^ (0u - (z & 1u));
+                                row[i] = x;
+                                over |= x >= nverts;
+                            }
+                            bad_id |= over;
+                        }
+                    }
+                }
+                // vertices of 2..32 chunks, one after another, a chunk per warp step
+                for (unsigned mm = __ballot_sync(0xFFFFFFFFu, d > kChunkIds && d <= (uint64_t)kChunkIds * kChunkIds);
+                     mm; mm &= mm - 1) {
+                    const int j = __ffs(mm) - 1;
+                    uint64_t pos = __shfl_sync(0xFFFFFFFFu, mpos, j);
+                    const uint64_t b0 = __shfl_sync(0xFFFFFFFFu, mb0, j);
+                    const uint64_t dj = __shfl_sync(0xFFFFFFFFu, d, j);
+                    const uint64_t nch = (dj + kChunkIds - 1) / kChunkIds;
+                    bool vbad = false;
+                    for (uint64_t c = 0; c < nch && !vbad; ++c) {
+                        const uint32_t k = (uint32_t)min((uint64_t)kChunkIds, dj - c * kChunkIds);
+                        if (pos < p0 || pos + 5 > p1) {
+                            vbad = true;
+                            break;
+                        }
+                        pos = decode_chunk_sm(sm, base, pos, p1, k, lane, out + (b0 - e0) + c * kChunkIds, nverts,
+                                              bad_id, vbad);
+                    }
+                    bad |= vbad;
+                }
+                base = ~0ull;  // the window holds this batch's words only
+                continue;
+            }
+            // ---- a batch larger than the window: vertex by vertex, sliding it
             for (uint32_t j = 0; j < nvt; ++j) {
                 uint64_t pos = __shfl_sync(0xFFFFFFFFu, mpos, j);
                 const uint64_t b0 = __shfl_sync(0xFFFFFFFFu, mb0, j), b1 = __shfl_sync(0xFFFFFFFFu, mb1, j);
@@ -290,24 +327,16 @@ __global__ void __launch_bounds__(kDecodeThreads)
                 bool vbad = false;
                 for (uint64_t c = 0; c < nch && !vbad; ++c) {
                     const uint32_t k = (uint32_t)min((uint64_t)kChunkIds, d - c * kChunkIds);
-                    uint32_t *row = out + (b0 - e0) + c * kChunkIds;
-                    if (staged) {
-                        if (pos < p0 || pos + 5 > p1) {
-                            vbad = true;
-                            break;
-                        }
-                        pos = decode_chunk_sm(sm, base, pos, p1, k, lane, row, nverts, bad_id, vbad);
-                    } else {
-                        if (pos + 5 > payload_bytes) {
-                            vbad = true;
-                            break;
-                        }
-                        pos = decode_chunk(pay, pos, k, payload_bytes, limit, lane, row, nverts, bad_id, vbad);
+                    if (pos < p0 || pos + 5 > p1) {
+                        vbad = true;
+                        break;
                     }
+                    cover(pos);
+                    pos = decode_chunk_sm(sm, base, pos, p1, k, lane, out + (b0 - e0) + c * kChunkIds, nverts, bad_id,
+                                          vbad);
                 }
                 bad |= vbad;
             }
-            __syncwarp();  // the next batch overwrites the staged words
         } else {
             const uint64_t g = t - ntv;
             const uint32_t v = __ldg(split + 3 * g), c0 = __ldg(split + 3 * g + 1);
@@ -331,8 +360,9 @@ __global__ void __launch_bounds__(kDecodeThreads)
                     vbad = true;
                     break;
                 }
-                pos = decode_chunk(pay, pos, k, payload_bytes, limit, lane, out + (b0 - e0) + c * kChunkIds, nverts,
-                                   bad_id, vbad);
+                cover(pos);
+                pos = decode_chunk_sm(sm, base, pos, payload_bytes, k, lane, out + (b0 - e0) + c * kChunkIds, nverts,
+                                      bad_id, vbad);
             }
             bad |= vbad;
         }
@@ -343,11 +373,20 @@ __global__ void __launch_bounds__(kDecodeThreads)
 
 cudaError_t launch_decode_block(const uint8_t *src, const CompressedBlock &cb, uint32_t nv, const uint64_t *beg,
                                 uint32_t v0, uint64_t e0, uint64_t ne, uint32_t nverts, uint32_t *out, uint32_t *err,
-                                int num_sms, cudaStream_t s)
+                                int num_sms, cudaStream_t s, int piece)
 {
     if (nv == 0) return cudaSuccess;
+    uint64_t t_lo = 0, t_hi = ((uint64_t)nv + 31) >> 5, g_lo = 0, g_hi = cb.nsplit;
+    if (piece >= 0) {
+        t_lo = cb.piece_v[piece] >> 5;
+        t_hi = ((uint64_t)cb.piece_v[piece + 1] + 31) >> 5;
+        g_lo = cb.piece_g[piece];
+        g_hi = cb.piece_g[piece + 1];
+        if (t_hi <= t_lo && g_hi <= g_lo) return cudaSuccess;
+    }
     k_decode_block<<<num_sms * 4, kDecodeThreads, 0, s>>>(src, cb.split_off, cb.nsplit, cb.payload_off,
-                                                         cb.payload_bytes, nv, beg, v0, e0, ne, nverts, out, err);
+                                                         cb.payload_bytes, nv, beg, v0, e0, ne, nverts, out, err, t_lo,
+                                                         t_hi, g_lo, g_hi);
     return cudaGetLastError();
 }
 

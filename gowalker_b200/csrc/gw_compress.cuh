@@ -30,6 +30,10 @@
 namespace gw {
 
 constexpr uint32_t kChunkIds = 32;
+// A prefetched block is copied and decoded in kPieces vertex ranges of about
+// equal payload (each a multiple of 32 vertices), so all but the last piece's
+// decode overlap the copy of the pieces after it.
+constexpr uint32_t kPieces = 4;
 
 struct CompressedBlock {
     uint8_t *host = nullptr;   // pinned (cudaHostAlloc), owned by the handle
@@ -38,6 +42,8 @@ struct CompressedBlock {
     uint32_t nsplit = 0;
     uint64_t payload_off = 0;  // start of the payload in the buffer
     uint64_t payload_bytes = 0;
+    uint32_t piece_v[kPieces + 1] = {};  // first vertex of each piece (piece_v[kPieces] = nv)
+    uint32_t piece_g[kPieces + 1] = {};  // first split group of each piece
 };
 
 // Encode block [beg[0], beg[nv]) (global edge ids; csr indexed from beg[0]).
@@ -52,8 +58,11 @@ bool compress_block(const uint64_t *beg, const uint32_t *csr, uint32_t nv, uint6
 // offsets of every vertex, v0: the block's first vertex.  Any offset or
 // payload read outside the buffer sets kErrBlock in *err and skips the
 // vertex; an id >= nverts sets kErrVertexRange (the block's validation).
+// piece < 0: the whole block; else only piece `piece`'s vertices, which need
+// only the split table, their offsets [piece_v[piece], piece_v[piece + 1]]
+// and their payload bytes (plus 8) in place.
 cudaError_t launch_decode_block(const uint8_t *src, const CompressedBlock &cb, uint32_t nv, const uint64_t *beg,
                                 uint32_t v0, uint64_t e0, uint64_t ne, uint32_t nverts, uint32_t *out, uint32_t *err,
-                                int num_sms, cudaStream_t s);
+                                int num_sms, cudaStream_t s, int piece = -1);
 
 }  // namespace gw

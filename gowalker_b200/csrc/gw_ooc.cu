@@ -710,6 +710,49 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         *bytes = cb.bytes + alias_bytes;
         return cuda(cudaMemcpyAsync(o.d_cstage[stage], cb.host, cb.bytes, cudaMemcpyHostToDevice, cs), "compressed block");
     };
+    // A prefetched compressed block: the split table, then each piece's
+    // offsets and payload, each piece decoded on `ds_dec` as soon as its
+    // bytes have landed (an event per piece), so only the last piece's decode
+    // follows the whole copy.
+    auto upload_decode_pieces = [&](uint32_t b, uint32_t *sc, cudaStream_t cs, cudaStream_t ds_dec, cudaEvent_t ev,
+                                    uint32_t stage, uint64_t *bytes) -> int {
+        const uint64_t ne = eblocks[b + 1] - eblocks[b];
+        const CompressedBlock &cb = o.cblk[b];
+        const uint32_t nv = vblocks[b + 1] - vblocks[b];
+        uint8_t *dst = o.d_cstage[stage];
+        const uint32_t *hvoff = reinterpret_cast<const uint32_t *>(cb.host);
+        int e;
+        *bytes = 0;
+        auto put = [&](uint64_t lo, uint64_t hi, const char *what) -> int {
+            if (hi <= lo) return GW_OK;
+            *bytes += hi - lo;
+            return cuda(cudaMemcpyAsync(dst + lo, cb.host + lo, hi - lo, cudaMemcpyHostToDevice, cs), what);
+        };
+        if (o.weighted && ne) {
+            if ((e = cuda(cudaMemcpyAsync(sc + o.slot_csr_words, o.halias[b], ne * sizeof(AliasEntry),
+                                          cudaMemcpyHostToDevice, cs),
+                          "block alias tables")))
+                return e;
+            *bytes += ne * sizeof(AliasEntry);
+        }
+        if ((e = put(cb.split_off, cb.payload_off, "compressed block split table"))) return e;
+        for (uint32_t k = 0; k < kPieces; ++k) {
+            const uint32_t va = cb.piece_v[k], vb = cb.piece_v[k + 1];
+            if (va == vb) continue;
+            if ((e = put(4ull * va, 4ull * (vb + 1), "compressed block offsets")) ||
+                (e = put(cb.payload_off + hvoff[va], std::min(cb.payload_off + hvoff[vb] + 8, cb.bytes),
+                         "compressed block payload")))
+                return e;
+            if ((e = cuda(cudaEventRecord(ev, cs), "event")) || (e = cuda(cudaStreamWaitEvent(ds_dec, ev, 0), "event")))
+                return e;
+            launches++;
+            if ((e = cuda(launch_decode_block(dst, cb, nv, o.d_beg, vblocks[b], eblocks[b], ne, nverts, sc, d_err,
+                                              num_sms, ds_dec, (int)k),
+                          "block decode")))
+                return e;
+        }
+        return GW_OK;
+    };
     auto decode_block = [&](uint32_t b, uint32_t *sc, cudaStream_t cs, uint32_t stage) -> int {
         if (!o.compressed) return GW_OK;
         launches++;
@@ -958,8 +1001,8 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     }
     cudaEvent_t staged_ev = nullptr;
     if (prefetch) cudaEventCreateWithFlags(&staged_ev, cudaEventDisableTiming);
-    // A prefetched compressed block is decoded on a stream of its own right
-    // behind its copy, so neither the compute stream (install, step,
+    // A prefetched compressed block is decoded on a stream of its own, piece
+    // by piece behind its copy, so neither the compute stream (install, step,
     // re-bucketing) nor the next copy waits for the decode.  The decode
     // writes the staging slot, which no step reads (it left the block table
     // when its block was evicted, before the step that precedes the decision
@@ -1302,15 +1345,14 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 (st = cuda(cudaStreamWaitEvent(s_copy, ev_decoded[upload_stage], 0), "decode wait")))
                 break;
             cudaEventRecord(tcp[tcp_next][0], s_copy);
-            if ((st = upload_block(b, sc, s_copy, upload_stage, &bytes))) break;
+            if (s_dec) st = upload_decode_pieces(b, sc, s_copy, s_dec, ev_up, upload_stage, &bytes);
+            else st = upload_block(b, sc, s_copy, upload_stage, &bytes);
+            if (st) break;
             cudaEventRecord(tcp[tcp_next][1], s_copy);
             tcp_live[tcp_next] = true;
             tcp_next ^= 1u;
             if (s_dec) {
-                if ((st = cuda(cudaEventRecord(ev_up, s_copy), "event")) ||
-                    (st = cuda(cudaStreamWaitEvent(s_dec, ev_up, 0), "copy wait")) ||
-                    (st = decode_block(b, sc, s_dec, upload_stage)) ||
-                    (st = cuda(cudaEventRecord(ev_decoded[upload_stage], s_dec), "event")) ||
+                if ((st = cuda(cudaEventRecord(ev_decoded[upload_stage], s_dec), "event")) ||
                     (st = cuda(cudaEventRecord(staged_ev, s_dec), "event")))
                     break;
                 decoded_rec[upload_stage] = true;
