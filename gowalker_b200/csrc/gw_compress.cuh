@@ -59,8 +59,7 @@ bool compress_block(const uint64_t *beg, const uint32_t *csr, uint32_t nv, uint6
 // payload read outside the buffer sets kErrBlock in *err and skips the
 // vertex; an id >= nverts sets kErrVertexRange (the block's validation).
 // piece < 0: the whole block; else only piece `piece`'s vertices, which need
-// only the split table, their offsets [piece_v[piece], piece_v[piece + 1]]
-// and their payload bytes (plus 8) in place.
+// only the offsets, the split table and their payload bytes (plus 8) in place.
 cudaError_t launch_decode_block(const uint8_t *src, const CompressedBlock &cb, uint32_t nv, const uint64_t *beg,
                                 uint32_t v0, uint64_t e0, uint64_t ne, uint32_t nverts, uint32_t *out, uint32_t *err,
                                 int num_sms, cudaStream_t s, int piece = -1);
