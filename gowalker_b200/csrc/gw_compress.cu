@@ -12,13 +12,17 @@ namespace gw {
 static inline uint32_t zigzag(uint32_t d) { return (d << 1) ^ (uint32_t)((int32_t)d >> 31); }
 static inline uint32_t bit_length(uint32_t x) { return x ? 32u - (uint32_t)__builtin_clz(x) : 0u; }
 
-// Width of the chunk ids[0, k): bits of the largest zigzag delta (an OR has
-// the same bit length as the maximum).
-static inline uint32_t chunk_width(const uint32_t *ids, uint32_t k)
+// Code of the chunk ids[0, k): the deltas as they are when that is narrower
+// (a sorted list: one bit less), else zigzag-coded; returns the width byte
+// (bit width | kPlainDeltas) -- an OR has the same bit length as the maximum.
+static inline uint32_t chunk_code(const uint32_t *ids, uint32_t k)
 {
-    uint32_t m = 0;
-    for (uint32_t i = 1; i < k; ++i) m |= zigzag(ids[i] - ids[i - 1]);
-    return bit_length(m);
+    uint32_t mz = 0, mr = 0;
+    for (uint32_t i = 1; i < k; ++i) {
+        mz |= zigzag(ids[i] - ids[i - 1]);
+        mr |= ids[i] - ids[i - 1];
+    }
+    return bit_length(mr) < bit_length(mz) ? bit_length(mr) | kPlainDeltas : bit_length(mz);
 }
 
 // Bytes of a vertex's chunks; with `group` non-null, also the byte offset
@@ -29,7 +33,7 @@ static uint64_t vertex_bytes(const uint32_t *ids, uint64_t d, uint64_t *group)
     for (uint64_t j = 0; j < d; j += kChunkIds, ++c) {
         if (group && c % kChunkIds == 0) group[c / kChunkIds] = s;
         const uint32_t k = (uint32_t)std::min<uint64_t>(kChunkIds, d - j);
-        s += 5 + ((uint64_t)(k - 1) * chunk_width(ids + j, k) + 7) / 8;
+        s += 5 + ((uint64_t)(k - 1) * (chunk_code(ids + j, k) & kWidthMask) + 7) / 8;
     }
     return s;
 }
@@ -42,13 +46,15 @@ static void encode_vertex(const uint32_t *ids, uint64_t d, uint8_t *p)
     for (uint64_t j = 0; j < d; j += kChunkIds) {
         const uint32_t k = (uint32_t)std::min<uint64_t>(kChunkIds, d - j);
         const uint32_t *c = ids + j;
-        const uint32_t w = chunk_width(c, k);
-        *p++ = (uint8_t)w;
+        const uint32_t code = chunk_code(c, k), w = code & kWidthMask;
+        const bool plain = (code & kPlainDeltas) != 0;
+        *p++ = (uint8_t)code;
         for (int b = 0; b < 4; ++b) *p++ = (uint8_t)(c[0] >> (8 * b));
         uint64_t acc = 0;
         uint32_t nbits = 0;
         for (uint32_t i = 1; i < k; ++i) {
-            acc |= (uint64_t)zigzag(c[i] - c[i - 1]) << nbits;
+            const uint32_t dl = c[i] - c[i - 1];
+            acc |= (uint64_t)(plain ? dl : zigzag(dl)) << nbits;
             nbits += w;
             while (nbits >= 8) {
                 *p++ = (uint8_t)acc;
@@ -155,9 +161,10 @@ __device__ __forceinline__ uint64_t decode_chunk_sm(const uint32_t *sm, uint64_t
     const uint32_t off = (uint32_t)((pos >> 2) - base);
     const uint32_t sh = (uint32_t)(pos & 3u) * 8u;
     const uint64_t head = (((uint64_t)sm[off + 1] << 32) | sm[off]) >> sh;
-    const uint32_t w = (uint32_t)head & 0xFFu;
+    const uint32_t code = (uint32_t)head & 0xFFu, w = code & kWidthMask;
+    const uint32_t zz = (code & kPlainDeltas) ? 0u : 1u;  // zigzag-coded deltas
     const uint64_t packed = ((uint64_t)(k - 1) * w + 7) >> 3;
-    if (w > 32 || pos + 5 + packed > end) {
+    if (w > 32 || (code & ~(kWidthMask | kPlainDeltas)) || pos + 5 + packed > end) {
         bad = true;
         return pos;
     }
@@ -171,7 +178,7 @@ __device__ __forceinline__ uint64_t decode_chunk_sm(const uint32_t *sm, uint64_t
         const uint64_t acc = ((uint64_t)sm[q + 1] << 32) | sm[q];
         const uint64_t mask = (w == 32) ? 0xFFFFFFFFull : ((1ull << w) - 1);
         const uint32_t z = (uint32_t)((acc >> (bo & 31u)) & mask);
-        x = (z >> 1) ^ (0u - (z & 1u));
+        x = zz ? (z >> 1) ^ (0u - (z & 1u)) : z;
     }
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -268,8 +275,10 @@ __global__ void __launch_bounds__(kDecodeThreads)
                         const uint32_t off = (uint32_t)((mpos >> 2) - base);
                         const uint32_t sh = (uint32_t)(mpos & 3u) * 8u;
                         const uint64_t head = (((uint64_t)sm[off + 1] << 32) | sm[off]) >> sh;
-                        const uint32_t w = (uint32_t)head & 0xFFu;
-                        if (w > 32 || mpos + 5 + (((d - 1) * w + 7) >> 3) > p1) {
+                        const uint32_t code = (uint32_t)head & 0xFFu, w = code & kWidthMask;
+                        const bool zz = (code & kPlainDeltas) == 0;
+                        if (w > 32 || (code & ~(kWidthMask | kPlainDeltas)) ||
+                            mpos + 5 + (((d - 1) * w + 7) >> 3) > p1) {
                             bad = true;
                         } else {
                             uint32_t *row = out + (mb0 - e0);
@@ -282,7 +291,7 @@ __global__ void __launch_bounds__(kDecodeThreads)
                                 const uint32_t q = off + (bit >> 5);
                                 const uint64_t acc = ((uint64_t)sm[q + 1] << 32) | sm[q];
                                 const uint32_t z = (uint32_t)((acc >> (bit & 31u)) & mask);
-                                x += (z >> 1) ^ (0u - (z & 1u));
+                                x += zz ? (z >> 1) ^ (0u - (z & 1u)) : z;
                                 row[i] = x;
                                 over |= x >= nverts;
                             }

@@ -12,14 +12,17 @@
 //                         32 chunks in sequence (hub vertices have 10^5+)
 //   (pad to 16 bytes)
 //   payload               per vertex, ceil(deg / 32) chunks of up to 32 ids:
-//                           u8  w       bit width of the chunk's deltas
+//                           u8  code    bit width w of the chunk's deltas (bits
+//                                       0-5), kPlainDeltas (bit 7) when they are
+//                                       stored as they are, else zigzag-coded
 //                           u32 first   first id (little endian, unaligned)
-//                           (k-1) deltas, zigzag-coded, packed LSB first at w bits
+//                           (k-1) deltas, packed LSB first at w bits
 //   8 bytes of padding    so a decoder may read up to 5 bytes past a field
 //
-// Deltas are id[i] - id[i-1] modulo 2^32, zigzag-coded, so any neighbour order
-// (sorted or not, duplicates included) round-trips exactly; sorted lists give
-// small deltas.  The offsets of every vertex are resident on the device, so
+// Deltas are id[i] - id[i-1] modulo 2^32, zigzag-coded unless every delta of
+// the chunk is narrower as it is, so any neighbour order (sorted or not,
+// duplicates included) round-trips exactly; sorted lists give small deltas
+// and need no sign bit.  The offsets of every vertex are resident on the device, so
 // the decoder knows each vertex's degree and output position without them
 // crossing the link again.
 #pragma once
@@ -30,6 +33,8 @@
 namespace gw {
 
 constexpr uint32_t kChunkIds = 32;
+constexpr uint32_t kWidthMask = 0x3Fu;    // bit width in a chunk's code byte
+constexpr uint32_t kPlainDeltas = 0x80u;  // deltas stored as they are (a sorted chunk: one bit less each)
 // A prefetched block is copied and decoded in kPieces vertex ranges of about
 // equal payload (each a multiple of 32 vertices), so all but the last piece's
 // decode overlap the copy of the pieces after it.
