@@ -16,7 +16,7 @@
 // file builds the alias tables.
 //
 // Alias tables (Vose's method, per vertex: one thread each, a CTA for each
-// vertex above 256 neighbours): the weights are
+// vertex above 256 neighbours, below): the weights are
 // summed in double in index order, scaled to p_i = w_i * deg / sum, split
 // into a queue of p < 1 and a queue of p >= 1 in index order; repeatedly the
 // next small s takes the front large l as its alias (prob[s] = (float)p_s)
@@ -31,8 +31,7 @@
 
 namespace gw {
 
-constexpr uint64_t kHubDeg = 256;            // vertices above this degree get a CTA each
-constexpr uint64_t kHubSmemEntries = 20480;  // their probabilities in shared memory up to this degree (160 KB)
+constexpr uint64_t kHubDeg = 256;  // vertices above this degree get a CTA each
 
 // Vose's loop for one vertex whose probabilities p[0, d) are scaled; the
 // queues hold indices in the order they are pushed.  p and the queues may be
@@ -89,45 +88,176 @@ __global__ void k_build_alias(const uint64_t *__restrict__ beg, const float *__r
     }
 }
 
-// Vertices of degree above kHubDeg: one CTA each.  The sum stays one
-// sequential chain of double additions in index order (thread 0) and the
-// loop stays Vose's serial loop, so the tables equal the small-vertex path's;
-// the CTA scales the probabilities in parallel and the loop runs on
-// shared-memory probabilities (up to kHubSmemEntries), where a serial chain
-// of dependent accesses costs far less than in global memory.
+// Vertices of degree above kHubDeg: one CTA each, with every memory access
+// of Vose's serial loop sequential so that a warp can fetch it 32 entries
+// ahead.  Vose's small queue is the initial smalls (index order) followed by
+// the larges that dropped below 1, in the order they dropped; the large queue
+// is the initial larges (index order), each one's probability untouched
+// until it becomes the current large.  So the loop reads three streams in
+// order -- initial smalls, initial larges, and the dropped larges (written
+// behind the consumed larges in the same array, each with its residual) --
+// and keeps the current large's residual in a register.  The warp runs the
+// loop in lockstep (every lane holds the same values; lane 0 writes), so the
+// sequence of double operations is exactly Vose's, as in the one-thread path
+// and the oracle.  The weight sum is the same in-order chain, fed 32 weights
+// at a time; the scaling and the split into the two queues run on the CTA.
 __global__ void __launch_bounds__(128)
     k_build_alias_hubs(const uint64_t *__restrict__ beg, const float *__restrict__ w, uint32_t nverts,
                        double *__restrict__ pd, uint32_t *__restrict__ qs, uint32_t *__restrict__ ql,
                        AliasEntry *__restrict__ out, uint32_t *err)
 {
-    extern __shared__ double s_p[];
     __shared__ double s_sum;
     __shared__ int s_bad;
+    __shared__ uint32_t s_cnt[2][4];  // per warp: smalls, larges of the current 128 indices
+    __shared__ uint32_t s_tot[2];     // smalls, larges so far
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    constexpr uint32_t kNone = 0xFFFFFFFFu;
     for (uint64_t v = blockIdx.x; v < nverts; v += gridDim.x) {
         const uint64_t h = beg[v], d = beg[v + 1] - h;
         if (d <= kHubDeg) continue;  // uniform over the CTA
-        if (threadIdx.x == 0) {
+        if (warp == 0) {
+            // the weight sum, one in-order chain of double additions
             double sum = 0.0;
             bool bad = false;
-            for (uint64_t i = 0; i < d; ++i) {
-                const float wi = w[h + i];
-                bad |= !(wi > 0.f && wi < __int_as_float(0x7F800000));
-                sum = __dadd_rn(sum, (double)wi);
+            float wn = lane < d ? w[h + lane] : 1.f;
+            for (uint64_t b = 0; b < d; b += 32) {
+                const float wc = wn;
+                wn = (b + 32 + lane < d) ? w[h + b + 32 + lane] : 1.f;  // the next 32, in flight meanwhile
+                bad |= !(wc > 0.f && wc < __int_as_float(0x7F800000));
+                const uint32_t n = (uint32_t)min((uint64_t)32, d - b);
+                for (uint32_t j = 0; j < n; ++j) sum = __dadd_rn(sum, (double)__shfl_sync(0xFFFFFFFFu, wc, j));
             }
-            s_sum = sum;
-            s_bad = bad ? 1 : 0;
+            bad = __any_sync(0xFFFFFFFFu, bad);
+            if (lane == 0) {
+                s_sum = sum;
+                s_bad = bad ? 1 : 0;
+                s_tot[0] = s_tot[1] = 0;
+            }
         }
         __syncthreads();
         if (s_bad) {
             if (threadIdx.x == 0) atomicOr(err, kErrWeight);
             for (uint64_t i = threadIdx.x; i < d; i += blockDim.x) out[h + i] = AliasEntry{1.f, (uint32_t)i};
-        } else {
-            double *p = d <= kHubSmemEntries ? s_p : pd + h;
-            const double sum = s_sum;
-            for (uint64_t i = threadIdx.x; i < d; i += blockDim.x)
-                p[i] = __ddiv_rn(__dmul_rn((double)w[h + i], (double)d), sum);
             __syncthreads();
-            if (threadIdx.x == 0) vose_loop(d, p, qs + h, ql + h, out + h);
+            continue;
+        }
+        // scale, and split the indices into the two queues in index order
+        const double sum = s_sum;
+        for (uint64_t b = 0; b < d; b += blockDim.x) {
+            const uint64_t i = b + threadIdx.x;
+            double p = 0.0;
+            if (i < d) {
+                p = __ddiv_rn(__dmul_rn((double)w[h + i], (double)d), sum);
+                pd[h + i] = p;
+            }
+            const bool sm = i < d && p < 1.0, lg = i < d && !(p < 1.0);
+            const unsigned bs = __ballot_sync(0xFFFFFFFFu, sm), bl = __ballot_sync(0xFFFFFFFFu, lg);
+            if (lane == 0) {
+                s_cnt[0][warp] = __popc(bs);
+                s_cnt[1][warp] = __popc(bl);
+            }
+            __syncthreads();
+            uint32_t os = s_tot[0], ol = s_tot[1];
+            for (uint32_t k = 0; k < warp; ++k) {
+                os += s_cnt[0][k];
+                ol += s_cnt[1][k];
+            }
+            const unsigned lt = (1u << lane) - 1u;
+            if (sm) qs[h + os + __popc(bs & lt)] = (uint32_t)i;
+            if (lg) ql[h + ol + __popc(bl & lt)] = (uint32_t)i;
+            __syncthreads();
+            if (threadIdx.x == 0)
+                for (uint32_t k = 0; k < blockDim.x / 32; ++k) {
+                    s_tot[0] += s_cnt[0][k];
+                    s_tot[1] += s_cnt[1][k];
+                }
+            __syncthreads();
+        }
+        const uint32_t ns0 = s_tot[0], nl = s_tot[1];
+        if (warp == 0) {
+            // Vose's loop.  The two initial queues are read in order, 32
+            // entries at a time, the next 32 fetched ahead: their indices when
+            // a chunk is entered, their probabilities 16 entries later (the
+            // indices have landed by then).
+            uint32_t sb_i = 0, lb_i = 0, ab_i = 0, sn_i = 0, ln_i = 0;
+            double sb_p = 0.0, lb_p = 0.0, ab_p = 0.0, sn_p = 0.0, ln_p = 0.0;
+            uint32_t sbase = kNone, lbase = kNone, abase = kNone, avalid = 0;
+            auto get_s = [&](uint32_t k, uint32_t &idx, double &p) {  // initial small k < ns0, k = 0, 1, 2, ...
+                if (sbase == kNone) {
+                    sbase = k;
+                    sb_i = k + lane < ns0 ? qs[h + k + lane] : 0u;
+                    sb_p = k + lane < ns0 ? pd[h + sb_i] : 0.0;
+                    sn_i = k + 32 + lane < ns0 ? qs[h + k + 32 + lane] : 0u;
+                } else if (k == sbase + 32) {
+                    sbase = k;
+                    sb_i = sn_i;
+                    sb_p = sn_p;
+                    sn_i = k + 32 + lane < ns0 ? qs[h + k + 32 + lane] : 0u;
+                }
+                if (k == sbase + 16) sn_p = sbase + 32 + lane < ns0 ? pd[h + sn_i] : 0.0;
+                idx = __shfl_sync(0xFFFFFFFFu, sb_i, k - sbase);
+                p = __shfl_sync(0xFFFFFFFFu, sb_p, k - sbase);
+            };
+            auto get_l = [&](uint32_t k, uint32_t &idx, double &p) {  // initial large k < nl, k = 0, 1, 2, ...
+                if (lbase == kNone) {
+                    lbase = k;
+                    lb_i = k + lane < nl ? ql[h + k + lane] : 0u;
+                    lb_p = k + lane < nl ? pd[h + lb_i] : 0.0;
+                    ln_i = k + 32 + lane < nl ? ql[h + k + 32 + lane] : 0u;
+                } else if (k == lbase + 32) {
+                    lbase = k;
+                    lb_i = ln_i;
+                    lb_p = ln_p;
+                    ln_i = k + 32 + lane < nl ? ql[h + k + 32 + lane] : 0u;
+                }
+                if (k == lbase + 16) ln_p = lbase + 32 + lane < nl ? pd[h + ln_i] : 0.0;
+                idx = __shfl_sync(0xFFFFFFFFu, lb_i, k - lbase);
+                p = __shfl_sync(0xFFFFFFFFu, lb_p, k - lbase);
+            };
+            uint32_t na = 0;                                          // dropped larges so far (== larges consumed)
+            auto get_a = [&](uint32_t k, uint32_t &idx, double &p) {  // dropped large k < na
+                if (abase == kNone || k >= abase + avalid) {
+                    __syncwarp();  // lane 0's writes of the entries are visible
+                    abase = k;
+                    avalid = min(32u, na - k);
+                    ab_i = lane < avalid ? ql[h + k + lane] : 0u;
+                    ab_p = lane < avalid ? pd[h + ab_i] : 0.0;
+                }
+                idx = __shfl_sync(0xFFFFFFFFu, ab_i, k - abase);
+                p = __shfl_sync(0xFFFFFFFFu, ab_p, k - abase);
+            };
+            uint32_t hs = 0, hl = 0, lidx = 0;
+            double r = 0.0;
+            if (nl) get_l(0, lidx, r);
+            while (hs < ns0 + na && hl < nl) {
+                uint32_t sidx;
+                double ps;
+                if (hs < ns0) get_s(hs, sidx, ps);
+                else get_a(hs - ns0, sidx, ps);
+                ++hs;
+                if (lane == 0) out[h + sidx] = AliasEntry{__double2float_rn(ps), lidx};
+                r = __dsub_rn(__dadd_rn(r, ps), 1.0);
+                if (r < 1.0) {
+                    // the large drops into the small queue, behind the consumed larges
+                    if (lane == 0) {
+                        pd[h + lidx] = r;
+                        ql[h + na] = lidx;
+                    }
+                    ++na;
+                    if (++hl < nl) get_l(hl, lidx, r);
+                }
+            }
+            __syncwarp();
+            // what is left keeps its own column: the larges from the current
+            // one on, and the smalls not consumed
+            for (uint32_t k = hl + lane; k < nl; k += 32) {
+                const uint32_t i = ql[h + k];
+                out[h + i] = AliasEntry{1.f, i};
+            }
+            for (uint32_t k = hs + lane; k < ns0 + na; k += 32) {
+                const uint32_t i = k < ns0 ? qs[h + k] : ql[h + (k - ns0)];
+                out[h + i] = AliasEntry{1.f, i};
+            }
         }
         __syncthreads();
     }
@@ -139,11 +269,7 @@ cudaError_t launch_build_alias(const uint64_t *beg, const float *w, uint32_t nve
     k_build_alias<<<num_sms * 8, 128, 0, s>>>(beg, w, nverts, pd, qs, ql, out, err);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const size_t smem = kHubSmemEntries * sizeof(double);
-    if ((e = cudaFuncSetAttribute(k_build_alias_hubs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
-        cudaSuccess)
-        return e;
-    k_build_alias_hubs<<<num_sms * 2, 128, smem, s>>>(beg, w, nverts, pd, qs, ql, out, err);
+    k_build_alias_hubs<<<num_sms * 4, 128, 0, s>>>(beg, w, nverts, pd, qs, ql, out, err);
     return cudaGetLastError();
 }
 
