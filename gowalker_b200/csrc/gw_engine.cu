@@ -546,12 +546,13 @@ int gw_handle::build_alias(cudaStream_t s)
     double *pd = nullptr;
     uint32_t *q = nullptr;
     if ((st = cuda(cudaMalloc(&pd, (nedges ? nedges : 1) * sizeof(double)), "alias scratch"))) return st;
-    if ((st = cuda(cudaMalloc(&q, 2 * (nedges ? nedges : 1) * sizeof(uint32_t)), "alias scratch"))) {
+    if ((st = cuda(cudaMalloc(&q, (2 * (nedges ? nedges : 1) + nverts + 2) * sizeof(uint32_t)), "alias scratch"))) {
         cudaFree(pd);
         return st;
     }
     st = cuda(cudaMemsetAsync(d_err, 0, sizeof(uint32_t), s), "memset");
-    if (!st) st = cuda(launch_build_alias(dev_beg, dev_w, nverts, pd, q, q + nedges, d_alias, d_err, num_sms, s),
+    if (!st) st = cuda(launch_build_alias(dev_beg, dev_w, nverts, pd, q, q + nedges,
+                                                      q + 2 * (nedges ? nedges : 1), d_alias, d_err, num_sms, s),
                        "alias build");
     if (!st) st = cuda(cudaMemcpyAsync(h_ctr + kCtrCount, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "D2H");
     if (!st) st = cuda(cudaStreamSynchronize(s), "alias build");

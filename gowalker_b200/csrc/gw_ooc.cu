@@ -558,7 +558,7 @@ static int ooc_build_alias(gw_handle *h, cudaStream_t s, uint64_t *h2d)
         if ((st = h->cuda(cudaMalloc(&rel, (maxv + 1) * sizeof(uint64_t)), "alias build scratch")) ||
             (st = h->cuda(cudaMalloc(&dw, maxe * sizeof(float)), "alias build scratch")) ||
             (st = h->cuda(cudaMalloc(&pd, maxe * sizeof(double)), "alias build scratch")) ||
-            (st = h->cuda(cudaMalloc(&q, 2 * maxe * sizeof(uint32_t)), "alias build scratch")) ||
+            (st = h->cuda(cudaMalloc(&q, (2 * maxe + maxv + 2) * sizeof(uint32_t)), "alias build scratch")) ||
             (st = h->cuda(cudaMalloc(&out, maxe * sizeof(AliasEntry)), "alias build scratch")))
             break;
         for (uint32_t b = 0; b < nb && !st; ++b) {
@@ -572,7 +572,7 @@ static int ooc_build_alias(gw_handle *h, cudaStream_t s, uint64_t *h2d)
             if ((st = h->cuda(cudaGetLastError(), "alias build")) ||
                 (st = h->cuda(cudaMemcpyAsync(dw, h->host_w[b], ne * sizeof(float), cudaMemcpyHostToDevice, s),
                               "block weights")) ||
-                (st = h->cuda(launch_build_alias(rel, dw, nv, pd, q, q + maxe, out, h->d_err, h->num_sms, s),
+                (st = h->cuda(launch_build_alias(rel, dw, nv, pd, q, q + maxe, q + 2 * maxe, out, h->d_err, h->num_sms, s),
                               "alias build")) ||
                 (st = h->cuda(cudaMemcpyAsync(o.halias[b], out, ne * sizeof(AliasEntry), cudaMemcpyDeviceToHost, s),
                               "alias tables")))

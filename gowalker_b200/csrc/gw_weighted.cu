@@ -101,20 +101,47 @@ __global__ void k_build_alias(const uint64_t *__restrict__ beg, const float *__r
 // sequence of double operations is exactly Vose's, as in the one-thread path
 // and the oracle.  The weight sum is the same in-order chain, fed 32 weights
 // at a time; the scaling and the split into the two queues run on the CTA.
+// The vertices of degree in (lo, hi], appended to the list work[2 + i]
+// (work[0] counts it) that the CTAs of k_build_alias_hubs take one vertex at
+// a time from (work[1]): R-MAT hubs sit at ids with many zero bits, so a
+// fixed stride would give a few CTAs most of the work.  Listing the largest
+// first lets their serial loops start first.
+__global__ void k_list_hubs(const uint64_t *__restrict__ beg, uint32_t nverts, uint64_t lo, uint64_t hi,
+                            uint32_t *__restrict__ work)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < nverts; b += stride) {
+        const uint64_t v = b + threadIdx.x;
+        const bool hub = v < nverts && beg[v + 1] - beg[v] > lo && beg[v + 1] - beg[v] <= hi;
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, hub);
+        uint32_t base = 0;
+        if (lane == 0 && m) base = atomicAdd(work, (uint32_t)__popc(m));
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (hub) work[2 + base + __popc(m & ((1u << lane) - 1u))] = (uint32_t)v;
+    }
+}
+
 __global__ void __launch_bounds__(128)
-    k_build_alias_hubs(const uint64_t *__restrict__ beg, const float *__restrict__ w, uint32_t nverts,
+    k_build_alias_hubs(const uint64_t *__restrict__ beg, const float *__restrict__ w, uint32_t *__restrict__ work,
                        double *__restrict__ pd, uint32_t *__restrict__ qs, uint32_t *__restrict__ ql,
                        AliasEntry *__restrict__ out, uint32_t *err)
 {
+    __shared__ uint32_t s_next;
     __shared__ double s_sum;
     __shared__ int s_bad;
     __shared__ uint32_t s_cnt[2][4];  // per warp: smalls, larges of the current 128 indices
     __shared__ uint32_t s_tot[2];     // smalls, larges so far
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     constexpr uint32_t kNone = 0xFFFFFFFFu;
-    for (uint64_t v = blockIdx.x; v < nverts; v += gridDim.x) {
+    const uint32_t nhubs = work[0];
+    for (;;) {
+        __syncthreads();  // the previous vertex is done with s_next and the shared sums
+        if (threadIdx.x == 0) s_next = atomicAdd(work + 1, 1u);
+        __syncthreads();
+        if (s_next >= nhubs) break;
+        const uint64_t v = work[2 + s_next];
         const uint64_t h = beg[v], d = beg[v + 1] - h;
-        if (d <= kHubDeg) continue;  // uniform over the CTA
         if (warp == 0) {
             // the weight sum, one in-order chain of double additions
             double sum = 0.0;
@@ -181,7 +208,7 @@ __global__ void __launch_bounds__(128)
             // indices have landed by then).
             uint32_t sb_i = 0, lb_i = 0, ab_i = 0, sn_i = 0, ln_i = 0;
             double sb_p = 0.0, lb_p = 0.0, ab_p = 0.0, sn_p = 0.0, ln_p = 0.0;
-            uint32_t sbase = kNone, lbase = kNone, abase = kNone, avalid = 0;
+            uint32_t sbase = kNone, lbase = kNone, abase = kNone;
             auto get_s = [&](uint32_t k, uint32_t &idx, double &p) {  // initial small k < ns0, k = 0, 1, 2, ...
                 if (sbase == kNone) {
                     sbase = k;
@@ -214,14 +241,22 @@ __global__ void __launch_bounds__(128)
                 idx = __shfl_sync(0xFFFFFFFFu, lb_i, k - lbase);
                 p = __shfl_sync(0xFFFFFFFFu, lb_p, k - lbase);
             };
-            uint32_t na = 0;                                          // dropped larges so far (== larges consumed)
+            // dropped larges: the last 32 in a register ring (entry j in lane
+            // j % 32), older ones from memory, 32 at a time
+            uint32_t na = 0;  // dropped larges so far (== larges consumed)
+            uint32_t ring_i = 0;
+            double ring_p = 0.0;
             auto get_a = [&](uint32_t k, uint32_t &idx, double &p) {  // dropped large k < na
-                if (abase == kNone || k >= abase + avalid) {
+                if (na - k <= 32u) {
+                    idx = __shfl_sync(0xFFFFFFFFu, ring_i, k & 31u);
+                    p = __shfl_sync(0xFFFFFFFFu, ring_p, k & 31u);
+                    return;
+                }
+                if (abase == kNone || k < abase || k >= abase + 32u) {
                     __syncwarp();  // lane 0's writes of the entries are visible
-                    abase = k;
-                    avalid = min(32u, na - k);
-                    ab_i = lane < avalid ? ql[h + k + lane] : 0u;
-                    ab_p = lane < avalid ? pd[h + ab_i] : 0.0;
+                    abase = k;     // k + 32 < na: all 32 are written
+                    ab_i = ql[h + k + lane];
+                    ab_p = pd[h + ab_i];
                 }
                 idx = __shfl_sync(0xFFFFFFFFu, ab_i, k - abase);
                 p = __shfl_sync(0xFFFFFFFFu, ab_p, k - abase);
@@ -242,6 +277,10 @@ __global__ void __launch_bounds__(128)
                     if (lane == 0) {
                         pd[h + lidx] = r;
                         ql[h + na] = lidx;
+                    }
+                    if (lane == (na & 31u)) {
+                        ring_i = lidx;
+                        ring_p = r;
                     }
                     ++na;
                     if (++hl < nl) get_l(hl, lidx, r);
@@ -264,12 +303,16 @@ __global__ void __launch_bounds__(128)
 }
 
 cudaError_t launch_build_alias(const uint64_t *beg, const float *w, uint32_t nverts, double *pd, uint32_t *qs,
-                               uint32_t *ql, AliasEntry *out, uint32_t *err, int num_sms, cudaStream_t s)
+                               uint32_t *ql, uint32_t *work, AliasEntry *out, uint32_t *err, int num_sms, cudaStream_t s)
 {
     k_build_alias<<<num_sms * 8, 128, 0, s>>>(beg, w, nverts, pd, qs, ql, out, err);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_build_alias_hubs<<<num_sms * 4, 128, 0, s>>>(beg, w, nverts, pd, qs, ql, out, err);
+    if ((e = cudaMemsetAsync(work, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
+    k_list_hubs<<<num_sms * 4, 256, 0, s>>>(beg, nverts, 16 * kHubDeg, ~0ull, work);
+    k_list_hubs<<<num_sms * 4, 256, 0, s>>>(beg, nverts, kHubDeg, 16 * kHubDeg, work);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_build_alias_hubs<<<num_sms * 4, 128, 0, s>>>(beg, w, work, pd, qs, ql, out, err);
     return cudaGetLastError();
 }
 

@@ -15,9 +15,11 @@ struct AliasEntry {
 static_assert(sizeof(AliasEntry) == 8, "one 8-byte load per trial");
 
 // Alias tables of every vertex's out-edges from its weights (w[e] per edge).
-// pd, qs, ql: scratch of nedges doubles / u32 / u32.  A weight that is not
-// positive and finite sets kErrWeight (that vertex gets a uniform table).
+// pd, qs, ql: scratch of nedges doubles / u32 / u32; work: nverts + 2 u32.
+// A weight that is not positive and finite sets kErrWeight (that vertex gets
+// a uniform table).
 cudaError_t launch_build_alias(const uint64_t *beg, const float *w, uint32_t nverts, double *pd, uint32_t *qs,
-                               uint32_t *ql, AliasEntry *out, uint32_t *err, int num_sms, cudaStream_t s);
+                               uint32_t *ql, uint32_t *work, AliasEntry *out, uint32_t *err, int num_sms,
+                               cudaStream_t s);
 
 }  // namespace gw
