@@ -889,8 +889,49 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     if (grid <= 0)
         grid = ooc_grid(sopr, paths, coop, cfg.prefetch && num_sms > 8 ? num_sms - 1 : num_sms, o.weighted);
 
+    // The step of an iteration -- runnable pass, cursor reset, step kernel --
+    // is captured once per run and sorted-index parity as a CUDA graph, like
+    // the re-bucketing after it (the step kernel's arguments differ only by
+    // that parity).  The zero-copy tail's launch and traced runs (events
+    // around the runnable pass) launch the kernels one by one.
+    cudaGraphExec_t sgraph[2] = {nullptr, nullptr};
+    auto step_ops = [&](uint32_t c) -> int {
+        int e;
+        if ((e = cuda(launch_runnable(o.d_counts, o.d_offsets, o.d_blk_csr, nb, a.lazy, o.d_run_pre, o.d_run_off,
+                                      o.d_nrun, s),
+                      "runnable")))
+            return e;
+        if ((e = cuda(cudaMemsetAsync(d_ctr + kCtrCursor, 0, sizeof(unsigned long long), s), "memset"))) return e;
+        OocStepArgs ac = a;
+        ac.recs = o.w_rec;
+        ac.order = o.w_ord[c];
+        ac.keys = o.w_key[c];
+        return cuda(launch_walk_ooc(ac, sopr, coop, o.weighted, grid, s), "walk kernel");
+    };
     auto step = [&]() -> int {
         int e;
+        if (!trace && !a.mapped) {
+            const uint32_t c = o.w_cur;
+            if (!sgraph[c]) {
+                cudaGraph_t g = nullptr;
+                if ((e = cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture"))) return e;
+                const int eo = step_ops(c);
+                const cudaError_t ec = cudaStreamEndCapture(s, &g);
+                if (eo) {
+                    if (g) cudaGraphDestroy(g);
+                    return eo;
+                }
+                if ((e = cuda(ec, "capture"))) return e;
+                e = cuda(cudaGraphInstantiate(&sgraph[c], g, 0), "graph instantiate");
+                cudaGraphDestroy(g);
+                if (e) return e;
+            }
+            if ((e = cuda(kring.begin(s, kernel_ms), "event"))) return e;
+            if ((e = cuda(cudaGraphLaunch(sgraph[c], s), "step graph"))) return e;
+            if ((e = cuda(kring.end(s), "event"))) return e;
+            launches += 2;
+            return GW_OK;
+        }
         if (trace) rring.begin(s, t_runnable_f);
         if ((e = cuda(launch_runnable(o.d_counts, o.d_offsets, o.d_blk_csr, nb, a.lazy, o.d_run_pre, o.d_run_off,
                                       o.d_nrun, s),
@@ -1495,6 +1536,8 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
     // the next run's first decision
     if (o.ts) cudaStreamSynchronize(o.ts);
     for (auto &g : bgraph)
+        if (g) cudaGraphExecDestroy(g);
+    for (auto &g : sgraph)
         if (g) cudaGraphExecDestroy(g);
     cudaEventDestroy(ev_buck);
     cudaEventDestroy(ev_dec);

@@ -147,7 +147,8 @@ typedef struct gw_stats {
     uint64_t zero_copy_steps; /* steps taken in the mapped-host tail mode */
     uint32_t iterations;      /* scheduler iterations */
     uint32_t launches;        /* kernels launched by this run */
-    float kernel_ms;          /* time inside the step kernels (CUDA events) */
+    float kernel_ms;          /* time inside the step kernels (CUDA events; out-of-core untraced
+                                 runs include each iteration's runnable-bucket pass) */
     float total_ms;           /* whole run (CUDA events) */
     uint32_t learned_iterations; /* decisions the learned parts changed or took: forecast evictions,
                                     and the switch to the zero-copy tail */
