@@ -711,9 +711,10 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
         return cuda(cudaMemcpyAsync(o.d_cstage[stage], cb.host, cb.bytes, cudaMemcpyHostToDevice, cs), "compressed block");
     };
     // A prefetched compressed block: its header (vertex offsets and split
-    // table) in one copy, then each piece's payload, each piece decoded on
-    // `ds_dec` as soon as its bytes have landed (an event per piece), so only
-    // the last piece's decode follows the whole copy.
+    // table) with the first piece's payload in one copy, then each further
+    // piece's payload, each piece decoded on `ds_dec` as soon as its bytes
+    // have landed (an event per piece), so only the last piece's decode
+    // follows the whole copy.
     auto upload_decode_pieces = [&](uint32_t b, uint32_t *sc, cudaStream_t cs, cudaStream_t ds_dec, cudaEvent_t ev,
                                     uint32_t stage, uint64_t *bytes) -> int {
         const uint64_t ne = eblocks[b + 1] - eblocks[b];
@@ -735,15 +736,16 @@ int gw_handle::run_ooc(uint32_t policy, gw_stats *stats)
                 return e;
             *bytes += ne * sizeof(AliasEntry);
         }
-        if ((e = put(0, cb.payload_off, "compressed block offsets and split table"))) return e;
+        // the header and the first piece are contiguous: one copy
+        uint64_t done = 0;
         for (uint32_t k = 0; k < kPieces; ++k) {
             const uint32_t va = cb.piece_v[k], vb = cb.piece_v[k + 1];
             if (va == vb) continue;
             // the payload of the piece, plus the 8 bytes a decoder may read past it
-            if ((e = put(cb.payload_off + hvoff[va],
-                         k + 1 == kPieces ? cb.bytes : std::min(cb.payload_off + hvoff[vb] + 8, cb.bytes),
-                         "compressed block payload")))
-                return e;
+            const uint64_t lo = done ? cb.payload_off + hvoff[va] : 0;
+            const uint64_t hi = k + 1 == kPieces ? cb.bytes : std::min(cb.payload_off + hvoff[vb] + 8, cb.bytes);
+            if ((e = put(lo, hi, "compressed block payload"))) return e;
+            done = hi;
             if ((e = cuda(cudaEventRecord(ev, cs), "event")) || (e = cuda(cudaStreamWaitEvent(ds_dec, ev, 0), "event")))
                 return e;
             launches++;
