@@ -12,9 +12,10 @@ namespace gw {
 static inline uint32_t zigzag(uint32_t d) { return (d << 1) ^ (uint32_t)((int32_t)d >> 31); }
 static inline uint32_t bit_length(uint32_t x) { return x ? 32u - (uint32_t)__builtin_clz(x) : 0u; }
 
-// Code of the chunk ids[0, k): the deltas as they are when that is narrower
-// (a sorted list: one bit less), else zigzag-coded; returns the width byte
-// (bit width | kPlainDeltas) -- an OR has the same bit length as the maximum.
+// Code byte of the chunk ids[0, k): the deltas as they are when that is
+// narrower (a sorted list: one bit less; at most 31 bits then), else
+// zigzag-coded -- an OR has the same bit length as the maximum -- and the
+// first id in as few bytes as hold it.
 static inline uint32_t chunk_code(const uint32_t *ids, uint32_t k)
 {
     uint32_t mz = 0, mr = 0;
@@ -22,7 +23,9 @@ static inline uint32_t chunk_code(const uint32_t *ids, uint32_t k)
         mz |= zigzag(ids[i] - ids[i - 1]);
         mr |= ids[i] - ids[i - 1];
     }
-    return bit_length(mr) < bit_length(mz) ? bit_length(mr) | kPlainDeltas : bit_length(mz);
+    const uint32_t c = bit_length(mr) < bit_length(mz) ? 32u + bit_length(mr) : bit_length(mz);
+    const uint32_t fb = std::max(1u, (bit_length(ids[0]) + 7u) / 8u);
+    return c | ((fb - 1u) << 6);
 }
 
 // Bytes of a vertex's chunks; with `group` non-null, also the byte offset
@@ -33,7 +36,7 @@ static uint64_t vertex_bytes(const uint32_t *ids, uint64_t d, uint64_t *group)
     for (uint64_t j = 0; j < d; j += kChunkIds, ++c) {
         if (group && c % kChunkIds == 0) group[c / kChunkIds] = s;
         const uint32_t k = (uint32_t)std::min<uint64_t>(kChunkIds, d - j);
-        s += 5 + ((uint64_t)(k - 1) * (chunk_code(ids + j, k) & kWidthMask) + 7) / 8;
+        s += chunk_bytes(chunk_code(ids + j, k), k);
     }
     return s;
 }
@@ -46,10 +49,10 @@ static void encode_vertex(const uint32_t *ids, uint64_t d, uint8_t *p)
     for (uint64_t j = 0; j < d; j += kChunkIds) {
         const uint32_t k = (uint32_t)std::min<uint64_t>(kChunkIds, d - j);
         const uint32_t *c = ids + j;
-        const uint32_t code = chunk_code(c, k), w = code & kWidthMask;
-        const bool plain = (code & kPlainDeltas) != 0;
+        const uint32_t code = chunk_code(c, k), w = chunk_width(code);
+        const bool plain = chunk_plain(code);
         *p++ = (uint8_t)code;
-        for (int b = 0; b < 4; ++b) *p++ = (uint8_t)(c[0] >> (8 * b));
+        for (uint32_t b = 0; b < chunk_first_bytes(code); ++b) *p++ = (uint8_t)(c[0] >> (8 * b));
         uint64_t acc = 0;
         uint32_t nbits = 0;
         for (uint32_t i = 1; i < k; ++i) {
@@ -152,7 +155,8 @@ bool compress_block(const uint64_t *beg, const uint32_t *csr, uint32_t nv, uint6
 // lane 0 takes the first id, lane i < k delta i (its bits read straight from
 // the window), and a warp prefix sum (mod 2^32) rebuilds the ids.  `end` is
 // the byte past the chunks this task may read; a chunk reaching past it is
-// malformed.  A chunk spans at most 3 + 5 + 124 bytes, so its words lie in
+// malformed.  A chunk spans at most 3 + 5 + 124 bytes (alignment, code and
+// first id, deltas), so its words lie in
 // [off, off + 35) with off = pos / 4 - base; the caller keeps off <= kSlideAt.
 __device__ __forceinline__ uint64_t decode_chunk_sm(const uint32_t *sm, uint64_t base, uint64_t pos, uint64_t end,
                                                     uint32_t k, uint32_t lane, uint32_t *__restrict__ row,
@@ -161,19 +165,19 @@ __device__ __forceinline__ uint64_t decode_chunk_sm(const uint32_t *sm, uint64_t
     const uint32_t off = (uint32_t)((pos >> 2) - base);
     const uint32_t sh = (uint32_t)(pos & 3u) * 8u;
     const uint64_t head = (((uint64_t)sm[off + 1] << 32) | sm[off]) >> sh;
-    const uint32_t code = (uint32_t)head & 0xFFu, w = code & kWidthMask;
-    const uint32_t zz = (code & kPlainDeltas) ? 0u : 1u;  // zigzag-coded deltas
-    const uint64_t packed = ((uint64_t)(k - 1) * w + 7) >> 3;
-    if (w > 32 || (code & ~(kWidthMask | kPlainDeltas)) || pos + 5 + packed > end) {
+    const uint32_t code = (uint32_t)head & 0xFFu, w = chunk_width(code), fb = chunk_first_bytes(code);
+    const uint32_t zz = chunk_plain(code) ? 0u : 1u;  // zigzag-coded deltas
+    const uint64_t size = chunk_bytes(code, k);
+    if (pos + size > end) {
         bad = true;
         return pos;
     }
     const uint32_t bp = lane ? (lane - 1) * w : 0u;
-    const uint32_t bo = sh + 40u + bp;
+    const uint32_t bo = sh + 8u + 8u * fb + bp;
     const uint32_t q = off + (bo >> 5);
     uint32_t x = 0;
     if (lane == 0) {
-        x = (uint32_t)(head >> 8);
+        x = (uint32_t)((head >> 8) & (0xFFFFFFFFull >> (32u - 8u * fb)));
     } else if (lane < k && w != 0) {
         const uint64_t acc = ((uint64_t)sm[q + 1] << 32) | sm[q];
         const uint64_t mask = (w == 32) ? 0xFFFFFFFFull : ((1ull << w) - 1);
@@ -189,7 +193,7 @@ __device__ __forceinline__ uint64_t decode_chunk_sm(const uint32_t *sm, uint64_t
         row[lane] = x;
         bad_id |= x >= nverts;
     }
-    return pos + 5 + packed;
+    return pos + size;
 }
 
 constexpr uint32_t kWindowWords = 1024 + 36;  // a warp's shared-memory window of the payload (4.1 KB)
@@ -269,24 +273,24 @@ __global__ void __launch_bounds__(kDecodeThreads)
                 bad |= !range_ok;
                 const uint64_t d = (mine && range_ok) ? mb1 - mb0 : 0;
                 if (d >= 1 && d <= kChunkIds) {
-                    if (mpos < p0 || mpos + 5 > p1) {
+                    if (mpos < p0 || mpos + 2 > p1) {
                         bad = true;
                     } else {
                         const uint32_t off = (uint32_t)((mpos >> 2) - base);
                         const uint32_t sh = (uint32_t)(mpos & 3u) * 8u;
                         const uint64_t head = (((uint64_t)sm[off + 1] << 32) | sm[off]) >> sh;
-                        const uint32_t code = (uint32_t)head & 0xFFu, w = code & kWidthMask;
-                        const bool zz = (code & kPlainDeltas) == 0;
-                        if (w > 32 || (code & ~(kWidthMask | kPlainDeltas)) ||
-                            mpos + 5 + (((d - 1) * w + 7) >> 3) > p1) {
+                        const uint32_t code = (uint32_t)head & 0xFFu, w = chunk_width(code);
+                        const uint32_t fb = chunk_first_bytes(code);
+                        const bool zz = !chunk_plain(code);
+                        if (mpos + chunk_bytes(code, (uint32_t)d) > p1) {
                             bad = true;
                         } else {
                             uint32_t *row = out + (mb0 - e0);
-                            uint32_t x = (uint32_t)(head >> 8);
+                            uint32_t x = (uint32_t)((head >> 8) & (0xFFFFFFFFull >> (32u - 8u * fb)));
                             row[0] = x;
                             bool over = x >= nverts;
                             const uint64_t mask = (w == 32) ? 0xFFFFFFFFull : ((1ull << w) - 1);
-                            uint32_t bit = sh + 40u;  // from word `off`
+                            uint32_t bit = sh + 8u + 8u * fb;  // from word `off`
                             for (uint32_t i = 1; i < (uint32_t)d; ++i, bit += w) {
                                 const uint32_t q = off + (bit >> 5);
                                 const uint64_t acc = ((uint64_t)sm[q + 1] << 32) | sm[q];
@@ -310,7 +314,7 @@ __global__ void __launch_bounds__(kDecodeThreads)
                     bool vbad = false;
                     for (uint64_t c = 0; c < nch && !vbad; ++c) {
                         const uint32_t k = (uint32_t)min((uint64_t)kChunkIds, dj - c * kChunkIds);
-                        if (pos < p0 || pos + 5 > p1) {
+                        if (pos < p0 || pos + 2 > p1) {
                             vbad = true;
                             break;
                         }
@@ -336,7 +340,7 @@ __global__ void __launch_bounds__(kDecodeThreads)
                 bool vbad = false;
                 for (uint64_t c = 0; c < nch && !vbad; ++c) {
                     const uint32_t k = (uint32_t)min((uint64_t)kChunkIds, d - c * kChunkIds);
-                    if (pos < p0 || pos + 5 > p1) {
+                    if (pos < p0 || pos + 2 > p1) {
                         vbad = true;
                         break;
                     }
@@ -365,7 +369,7 @@ __global__ void __launch_bounds__(kDecodeThreads)
             bool vbad = false;
             for (uint64_t c = c0; c < c1 && !vbad; ++c) {
                 const uint32_t k = (uint32_t)min((uint64_t)kChunkIds, d - c * kChunkIds);
-                if (pos + 5 > payload_bytes) {
+                if (pos + 2 > payload_bytes) {
                     vbad = true;
                     break;
                 }

@@ -12,17 +12,19 @@
 //                         32 chunks in sequence (hub vertices have 10^5+)
 //   (pad to 16 bytes)
 //   payload               per vertex, ceil(deg / 32) chunks of up to 32 ids:
-//                           u8  code    bit width w of the chunk's deltas (bits
-//                                       0-5), kPlainDeltas (bit 7) when they are
-//                                       stored as they are, else zigzag-coded
-//                           u32 first   first id (little endian, unaligned)
+//                           u8  code    bits 0-5: c, the deltas' width w = c
+//                                       zigzag-coded (c <= 32) or w = c - 32
+//                                       stored as they are (c > 32: a sorted
+//                                       chunk, one bit less each); bits 6-7:
+//                                       the first id's bytes - 1
+//                           first id    1-4 bytes, little endian, unaligned
 //                           (k-1) deltas, packed LSB first at w bits
 //   8 bytes of padding    so a decoder may read up to 5 bytes past a field
 //
 // Deltas are id[i] - id[i-1] modulo 2^32, zigzag-coded unless every delta of
 // the chunk is narrower as it is, so any neighbour order (sorted or not,
 // duplicates included) round-trips exactly; sorted lists give small deltas
-// and need no sign bit.  The offsets of every vertex are resident on the device, so
+// and need no sign bit, and a sorted list's first id is its smallest.  The offsets of every vertex are resident on the device, so
 // the decoder knows each vertex's degree and output position without them
 // crossing the link again.
 #pragma once
@@ -33,8 +35,19 @@
 namespace gw {
 
 constexpr uint32_t kChunkIds = 32;
-constexpr uint32_t kWidthMask = 0x3Fu;    // bit width in a chunk's code byte
-constexpr uint32_t kPlainDeltas = 0x80u;  // deltas stored as they are (a sorted chunk: one bit less each)
+// A chunk's code byte (layout above): width, whether the deltas are plain,
+// bytes of the first id, bytes of the whole chunk of k ids.
+__host__ __device__ inline uint32_t chunk_width(uint32_t code)
+{
+    const uint32_t c = code & 63u;
+    return c > 32u ? c - 32u : c;
+}
+__host__ __device__ inline bool chunk_plain(uint32_t code) { return (code & 63u) > 32u; }
+__host__ __device__ inline uint32_t chunk_first_bytes(uint32_t code) { return (code >> 6) + 1u; }
+__host__ __device__ inline uint64_t chunk_bytes(uint32_t code, uint32_t k)
+{
+    return 1u + chunk_first_bytes(code) + (((uint64_t)(k - 1) * chunk_width(code) + 7) >> 3);
+}
 // A prefetched block is copied and decoded in kPieces vertex ranges of about
 // equal payload (each a multiple of 32 vertices), so all but the last piece's
 // decode overlap the copy of the pieces after it.
