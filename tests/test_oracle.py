@@ -422,3 +422,29 @@ def test_max_choose_blocks_matches_reference(oracle, tmp_path, nb):
         assert got == want, (cached, nslots, zt)
         acts.add(got[0])
     assert acts == {0, 1, 2}
+
+
+def test_schedule_replay_zero_mode_and_incident_eviction(oracle):
+    """The CPU schedule replay's options: GOWalker's zero mode ends the
+    loading at the first iteration whose best score is at or below the
+    threshold and leaves every remaining step to the mapped tail (loaded plus
+    tail steps = every step of the walks, for any threshold and either
+    eviction rule), and a higher threshold loads no more blocks."""
+    beg, csr = oracle.rmat_graph(13, 12, seed=5)
+    nb = 16
+    vb, eb = oracle.split_equal_edge_mass(beg, nb)
+    cfg = oracle.make_cfg(algo=0, maxhops=40, p=0.5, q=2.0, seed=9)
+    reqs, nent = oracle.walk_requirements(beg, csr, cfg, vb, 0, len(beg) - 1)
+    total = oracle.walk(beg, csr, cfg, 0, len(beg) - 1, paths=False)["stats"]["steps"]
+    loads = {}
+    for ev in (False, True):
+        for zt in (0, 40, 200):
+            for pf in (False, True):
+                st, _ = oracle.sched_replay(reqs, nent, nb, 5, prefetch=pf, zero_threshold=zt, evict_incident=ev,
+                                            zero_tail=zt > 0)
+                assert st["steps"] + st["zc_steps"] == total, (ev, zt, pf)
+                assert (st["zc_steps"] > 0) == (zt > 0) or zt == 0
+                loads[(ev, zt, pf)] = st["loads"]
+    for ev in (False, True):
+        for pf in (False, True):
+            assert loads[(ev, 200, pf)] <= loads[(ev, 40, pf)] <= loads[(ev, 0, pf)]
