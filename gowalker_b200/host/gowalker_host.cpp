@@ -514,7 +514,9 @@ static void print_help()
            "- zero:          finish stragglers through mapped host memory (zero_threshold per block size)\n"
            "- GOWalker / SOWalker: block choice by the GOWalker rule or by SOWalker's annealed block set\n"
            "  (both on the device); gpu cpu walkaware: accepted, no effect\n"
-           "- learned:       block choice by the trained demand predictor (plain rule as fallback)\n"
+           "- learned:       GOWalker's block choice with learned parts: the zero-copy switch priced by\n"
+           "                 measured costs and eviction by a trained forecast (chosen run by run; the\n"
+           "                 plain rule judges)\n"
            "- termination F: stop each walk with probability F per step (SOPR/SOSR workloads)\n"
            "- seed N, device N, keepblocks, persource, paths FILE, pathsbin FILE\n"
            "- h:             print this message\n");
